@@ -1,0 +1,231 @@
+/*
+ * skema_c.h -- C ABI of the B200 SketchySVD sketch update.
+ *
+ * This is the drop-in boundary for Skema's streaming SketchySVD path. Every
+ * entry point names the reference interface it replaces (paths are relative
+ * to the jeremy-myers/skema source tree). The header is plain C: no C++
+ * types, no torch types, no exceptions. Every call returns an int status
+ * (skema_status); the message of the last failure on a context is returned
+ * by skema_last_error().
+ *
+ * Conventions
+ *   - Dense matrices are described by (pointer, leading dimension, layout).
+ *     SKEMA_COL_MAJOR is the reference's Kokkos::LayoutLeft
+ *     (src/Skema_Utils.hpp:12); SKEMA_ROW_MAJOR is also accepted.
+ *   - `mem` says where caller buffers live: SKEMA_MEM_DEVICE (CUDA device
+ *     pointers on the context's device) or SKEMA_MEM_HOST (host pointers;
+ *     the library stages the data through device memory it owns).
+ *   - One context = one CUDA stream. Calls on one context must be serialised
+ *     by the caller; separate contexts are independent.
+ *   - The context owns the random maps, the sketches X, Y, Z and all
+ *     workspaces. Outputs go to caller-provided buffers.
+ */
+#ifndef SKEMA_C_H
+#define SKEMA_C_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+typedef enum {
+  SKEMA_OK = 0,
+  SKEMA_EINVAL = 1,       /* bad argument or shape                          */
+  SKEMA_ENOMEM = 2,       /* device or host allocation failed               */
+  SKEMA_ECUDA = 3,        /* a CUDA runtime call failed                     */
+  SKEMA_ENOTPD = 4,       /* Cholesky failed even after the shifted retry   */
+  SKEMA_ETIMEOUT = 5,     /* a bounded device-side wait ran out             */
+  SKEMA_ESTATE = 6,       /* call not valid in the context's current state  */
+  SKEMA_EUNSUPPORTED = 7, /* combination not provided by this build         */
+  SKEMA_ENOKERNEL = 8     /* no CUDA device / kernel image for this device  */
+} skema_status;
+
+/* ---- enums mirroring src/Skema_Utils.hpp:38-80 ------------------------- */
+enum { SKEMA_MAP_GAUSS = 0, SKEMA_MAP_SPARSE_SIGN = 1 };    /* DimRedux_Map */
+enum { SKEMA_KERNEL_NONE = 0, SKEMA_KERNEL_GAUSSRBF = 1 };  /* Kernel_Map   */
+/* Arithmetic of the sketch contractions (new; the reference is FP64 only). */
+enum { SKEMA_PREC_FP32 = 0, SKEMA_PREC_BF16 = 1, SKEMA_PREC_FP8 = 2 };
+/* Which map, in the order of AlgParams::seeds (src/Skema_SketchySVD.cpp:37,54,70,87). */
+enum { SKEMA_UPSILON = 0, SKEMA_OMEGA = 1, SKEMA_PHI = 2, SKEMA_PSI = 3 };
+enum { SKEMA_COL_MAJOR = 0, SKEMA_ROW_MAJOR = 1 };
+enum { SKEMA_MEM_DEVICE = 0, SKEMA_MEM_HOST = 1 };
+/* Which sketch, for skema_get_sketch / skema_set_sketch. */
+enum { SKEMA_SKETCH_X = 0, SKEMA_SKETCH_Y = 1, SKEMA_SKETCH_Z = 2 };
+
+/*
+ * Sketch fields of Skema::AlgParams (src/Skema_AlgParams.hpp:12-90), with the
+ * same names and meaning. Defaults come from skema_params_init().
+ */
+typedef struct {
+  int64_t matrix_m;           /* rows of A (points N for a kernel input)      */
+  int64_t matrix_n;           /* cols of A (N for a kernel input)             */
+  int64_t rank;               /* r                                            */
+  int64_t sketch_range;       /* k; 4r+1 when < rank (Skema_SketchySVD.cpp:20) */
+  int64_t sketch_core;        /* s; 2k+1 when < rank (Skema_SketchySVD.cpp:23) */
+  int64_t window;             /* rows per streaming window                    */
+  double sketch_eta;          /* X = nu*X + eta*x  (Skema_SketchySVD.cpp:187) */
+  double sketch_nu;
+  int32_t seeds[4];           /* Upsilon, Omega, Phi, Psi                     */
+  int32_t dim_redux;          /* SKEMA_MAP_*                                  */
+  int32_t issparse;           /* input is CSR                                 */
+  int32_t issymmetric;        /* with !force_three_sketch: SketchySPD         */
+  int32_t force_three_sketch;
+  int32_t kernel_func;        /* SKEMA_KERNEL_*                               */
+  double kernel_gamma;
+  int32_t precision;          /* SKEMA_PREC_* (new)                           */
+  int32_t device;             /* CUDA device ordinal                          */
+} skema_params;
+
+typedef struct skema_ctx skema_ctx;
+
+/* Fill p with AlgParams' defaults (src/Skema_AlgParams.cpp:10-57; eta/nu 1.0
+ * from src/Skema_AlgParams.cpp:275-278). */
+int skema_params_init(skema_params* p);
+
+/* SketchySVD<MatrixType,DimReduxT>::SketchySVD(const AlgParams&)
+ * (src/Skema_SketchySVD.cpp:16-117) or SketchySPD::SketchySPD
+ * (src/Skema_SketchySVD.cpp:759-788) when issymmetric && !force_three_sketch.
+ * Generates the four maps (GaussDimRedux ctor src/Skema_DimRedux.hpp:98-128,
+ * SparseSignDimRedux ctor src/Skema_DimRedux.hpp:191-268) on the device with
+ * the orientation rules of src/Skema_SketchySVD.cpp:30-95, and allocates
+ * zeroed sketches X (k x n), Y (m x k), Z (s x s). */
+int skema_create(const skema_params* p, skema_ctx** out);
+
+/* ~SketchySVD(): frees every device buffer the context owns. */
+int skema_destroy(skema_ctx* ctx);
+
+/* Message of the last failed call on ctx ("" if none). A NULL ctx returns the
+ * message of the last failed skema_create on this thread. */
+const char* skema_last_error(const skema_ctx* ctx);
+
+/* Resolved sketch sizes (range k, core s) and whether the context runs the
+ * one-sketch SketchySPD variant. */
+int skema_get_dims(const skema_ctx* ctx, int64_t* range, int64_t* core, int32_t* spd);
+
+/* Zero X, Y, Z: the start of SketchySVD::linear_update
+ * (src/Skema_SketchySVD.cpp:131-133). */
+int skema_reset(skema_ctx* ctx);
+
+/* SketchySVD<matrix_type,*>::linear_update + update
+ * (src/Skema_SketchySVD.cpp:120-246, 256-293) for rows [row0, row0+nrows)
+ * of a dense A. The rows are split into windows of params.window rows
+ * (last window partial, :167-173); per window the update is
+ *   X = nu*X + eta*(Upsilon_w A_w),  Y(w,:) = nu*Y(w,:) + eta*(A_w Omega^T),
+ *   Z = nu*Z + eta*(Phi_w A_w Psi^T).
+ * A points at row row0 of a block with leading dimension ld. Unlike the
+ * reference, the sketches are not re-zeroed here: call skema_reset first to
+ * get linear_update's semantics, or stream several row blocks in order. */
+int skema_linear_update_dense(skema_ctx* ctx, const float* A, int64_t ld,
+                              int32_t layout, int64_t row0, int64_t nrows,
+                              int32_t mem);
+
+/* SketchySVD<crs_matrix_type,*>::linear_update + update
+ * (src/Skema_SketchySVD.cpp:120-246, 296-335) with the CRS window of
+ * Window::get (src/Skema_Window.hpp:50-78). rowptr has nrows+1 entries
+ * (absolute offsets into col/val, rowptr[0] need not be 0); col holds int32
+ * column indices in [0, matrix_n). Duplicate column entries in a row are
+ * summed, as KokkosSparse does. */
+int skema_linear_update_csr(skema_ctx* ctx, const int64_t* rowptr,
+                            const int32_t* col, const float* val, int64_t row0,
+                            int64_t nrows, int32_t mem);
+
+/* GaussRBFWindow::get + GaussRBF::compute (src/Skema_Window.hpp:90-107,
+ * src/Skema_Kernel.cpp:6-81) feeding linear_update: rows [row0,row0+nrows)
+ * of K(i,j) = exp(-gamma*||x_i - x_j||^2) with K(i,i) = 1, generated on the
+ * device one window at a time (the whole K is never formed). pts is npts x d
+ * (npts == matrix_m == matrix_n). */
+int skema_linear_update_rbf(skema_ctx* ctx, const float* pts, int64_t ld,
+                            int32_t layout, int64_t npts, int64_t d,
+                            int64_t row0, int64_t nrows, int32_t mem);
+
+/* SketchySVD::low_rank_approx + initial_approx
+ * (src/Skema_SketchySVD.cpp:338-664), computed on the device in FP64 with
+ * CholeskyQR2 in place of dgeqrf/dorgqr, triangular solves in place of the
+ * dgels calls on T1/T2, and a one-sided Jacobi SVD in place of dgesvd.
+ * Outputs: U (m x rank), S (rank), V (n x rank), column-major. Singular
+ * vectors equal LAPACK's up to sign. Any output pointer may be NULL. */
+int skema_low_rank_approx(skema_ctx* ctx, double* U, double* S, double* V,
+                          int32_t mem);
+
+/* Copy one sketch out of / into the context (the reference only exposes them
+ * through its debug dumps, src/Skema_SketchySVD.cpp:192-206, 235-245).
+ * X is k x n, Y is m x k, Z is s x s; `layout` is the layout of buf. */
+int skema_get_sketch(skema_ctx* ctx, int32_t which, float* buf, int64_t ld,
+                     int32_t layout, int32_t mem);
+int skema_set_sketch(skema_ctx* ctx, int32_t which, const float* buf,
+                     int64_t ld, int32_t layout, int32_t mem);
+
+/* Map dump/import (the --debug-file dumps of src/Skema_DimRedux.hpp:124-127,
+ * 264-267). The map is described in its stored orientation (nrow x ncol of
+ * the DimRedux ctor). Gauss: values as double, column-major nrow x ncol.
+ * SparseSign: zeta entries per stored row, indices int32 and values double
+ * (+-1), row r at [r*zeta, (r+1)*zeta). Query shapes with buffers NULL. */
+int skema_map_info(const skema_ctx* ctx, int32_t which, int64_t* nrow,
+                   int64_t* ncol, int32_t* zeta, int32_t* transposed);
+int skema_map_export(skema_ctx* ctx, int32_t which, double* values,
+                     int32_t* indices);
+int skema_map_import(skema_ctx* ctx, int32_t which, const double* values,
+                     const int32_t* indices);
+
+/* Standalone RBF-kernel sketch (new; no reference counterpart beyond
+ * GaussRBF::compute, src/Skema_Kernel.cpp:6-81):
+ *   Y = K Omega^T,  K(i,j) = exp(-gamma*||x_i - x_j||^2), K(i,i) = 1,
+ * with pts N x d (row-major), Omega k x N (row-major), Y N x k (row-major),
+ * all device pointers, on ctx's stream. */
+int skema_rbf_sketch_fwd(skema_ctx* ctx, const float* pts, int64_t npts,
+                         int64_t d, double gamma, const float* omega,
+                         int64_t k, float* Y);
+
+/* Vector-Jacobian product of skema_rbf_sketch_fwd: given Ybar = dL/dY
+ * (N x k, row-major), returns dL/dpts (N x d, row-major, overwritten) and
+ * dL/dgamma (one double, device pointer). Kernel tiles are recomputed, never
+ * stored. */
+int skema_rbf_sketch_vjp(skema_ctx* ctx, const float* pts, int64_t npts,
+                         int64_t d, double gamma, const float* omega,
+                         int64_t k, const float* Ybar, float* dpts,
+                         double* dgamma);
+
+/* Wait for all work queued on ctx's stream. */
+int skema_synchronize(skema_ctx* ctx);
+
+/* Use an external CUDA stream (cudaStream_t passed as void*; NULL restores
+ * the context's own stream). */
+int skema_set_stream(skema_ctx* ctx, void* stream);
+
+/* Number of this library's kernels launched on ctx so far (for accounting). */
+int64_t skema_launch_count(const skema_ctx* ctx);
+
+/* Device-side stage timers, the counterpart of the reference's
+ * timings["update"][...] / timings["approx"][...] maps
+ * (src/Skema_SketchySVD.cpp:101-116), measured with CUDA events on the
+ * context's stream. skema_timing_enable(ctx, 1) clears and starts them;
+ * skema_timing_get synchronises and returns the accumulated milliseconds and
+ * number of timed launches of one stage:
+ *   "update.omega"   Y = A Omega^T (the streaming Y kernel of the sparse path)
+ *   "update.psi"     T = A Psi^T
+ *   "update.upsilon" X += Upsilon_w A_w
+ *   "update.phi"     Z += Phi_w T
+ *   "update.entries" the sparse-sign X/Z entry kernel
+ *   "update.window"  kernel-window generation
+ *   "update.fused"   the fused tensor-core window kernel
+ *   "update.daxpy"   sketch scaling by nu
+ * Unknown names give SKEMA_EINVAL. */
+int skema_timing_enable(skema_ctx* ctx, int32_t on);
+int skema_timing_get(skema_ctx* ctx, const char* stage, double* ms, int64_t* count);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SKEMA_C_H */

@@ -1,0 +1,26 @@
+"""B200 SketchySVD sketch update: a CUDA library for sm_100a behind a C ABI
+(include/skema_c.h), with a Python mirror of Skema's SketchySVD interface."""
+from ._lib import SkemaError, load
+from .sketchy import (
+    AlgParams,
+    GaussDimRedux,
+    SketchySPD,
+    SketchySVD,
+    SparseSignDimRedux,
+    rbf_sketch_fwd,
+    rbf_sketch_vjp,
+    sketchysvd,
+)
+
+__all__ = [
+    "AlgParams",
+    "GaussDimRedux",
+    "SparseSignDimRedux",
+    "SketchySVD",
+    "SketchySPD",
+    "sketchysvd",
+    "rbf_sketch_fwd",
+    "rbf_sketch_vjp",
+    "SkemaError",
+    "load",
+]

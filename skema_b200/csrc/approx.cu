@@ -1,0 +1,549 @@
+// approx.cu -- SketchySVD::initial_approx + low_rank_approx
+// (src/Skema_SketchySVD.cpp:338-664) on the device, in FP64.
+//
+//   P = orth(X^T)          (reference: dgeqrf+dorgqr, :355-357)
+//   Q = orth(Y)            (:381-383; here Y is not overwritten)
+//   [U1, T1] = qr(Phi~ Q)  (:409, :453)
+//   [U2, T2] = qr(Psi~ P)  (:430, :476)
+//   Z2 = U1^T Z U2         (:500, :515)
+//   Z2 = T1 \ Z2           (dgels on the triangular T1, :532)
+//   C  = (T2 \ Z2^T)^T     (:549-562)
+//   [Uc, S, Vc] = svd(C)   (dgesvd, :609)
+//   U = Q Uc(:, 1:r), V = P Vc(:, 1:r), S(1:r)   (:627, :645, :657-660)
+//
+// orth/qr use CholeskyQR2 (Gram on the device, Cholesky in one CTA, triangular
+// solve of the rows), with the shifted CholeskyQR pre-pass of Fukaya,
+// Kannan, Nakatsukasa, Yamamoto and Yanagisawa (SIAM J. Sci. Comput. 2020)
+// when the Gram matrix is not numerically positive definite. The Q factor
+// equals Householder's up to column signs, so S is unchanged and U, V match
+// LAPACK's up to sign. The SVD of the k x k core is a one-sided (Hestenes)
+// Jacobi SVD with round-robin pair ordering in one CTA.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "internal.h"
+
+namespace skema {
+
+namespace {
+
+// ---------------------------------------------------------------- DGEMM ----
+// C(i,j) = alpha * sum A(i,kk) B(kk,j) + beta*C(i,j); A, B may be float or
+// double; FP64 accumulation. 64x64 tile, 4x4 per thread, split-K atomic.
+template <typename TA, typename TB, bool ATOMIC>
+__global__ void __launch_bounds__(256)
+    dgemm_kernel(int64_t M, int64_t N, int64_t K, double alpha, const TA* __restrict__ A,
+                 int64_t ars, int64_t acs, const TB* __restrict__ B, int64_t brs, int64_t bcs,
+                 double beta, double* __restrict__ C, int64_t crs, int64_t ccs, int64_t kchunk) {
+  __shared__ double As[8][64 + 1];
+  __shared__ double Bs[8][64 + 1];
+  const int tid = threadIdx.x;
+  const int64_t m0 = (int64_t)blockIdx.x * 64, n0 = (int64_t)blockIdx.y * 64;
+  const int64_t kb = (int64_t)blockIdx.z * kchunk, ke = min(K, kb + kchunk);
+  if (kb >= ke) return;
+  const bool am = (ars == 1);
+  const bool bn = (bcs == 1);
+  // 512 elements per operand tile: 2 per thread
+  int la_m[2], la_k[2], lb_n[2], lb_k[2];
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    const int e = tid + 256 * q;
+    if (am) { la_m[q] = e & 63; la_k[q] = e >> 6; } else { la_k[q] = e & 7; la_m[q] = e >> 3; }
+    if (bn) { lb_n[q] = e & 63; lb_k[q] = e >> 6; } else { lb_k[q] = e & 7; lb_n[q] = e >> 3; }
+  }
+  const int tx = tid & 15, ty = tid >> 4;
+  double acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+  for (int64_t k0 = kb; k0 < ke; k0 += 8) {
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      const int64_t gm = m0 + la_m[q], gk = k0 + la_k[q];
+      As[la_k[q]][la_m[q]] = (gm < M && gk < ke) ? (double)A[gm * ars + gk * acs] : 0.0;
+      const int64_t gn = n0 + lb_n[q], gk2 = k0 + lb_k[q];
+      Bs[lb_k[q]][lb_n[q]] = (gn < N && gk2 < ke) ? (double)B[gk2 * brs + gn * bcs] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < 8; ++kk) {
+      double a[4], b[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        a[u] = As[kk][ty + 16 * u];
+        b[u] = Bs[kk][tx + 16 * u];
+      }
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int64_t gm = m0 + ty + 16 * i;
+    if (gm >= M) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int64_t gn = n0 + tx + 16 * j;
+      if (gn >= N) continue;
+      double* cp = C + gm * crs + gn * ccs;
+      if (ATOMIC)
+        atomicAdd(cp, alpha * acc[i][j]);
+      else
+        *cp = (beta == 0.0) ? alpha * acc[i][j] : fma(beta, *cp, alpha * acc[i][j]);
+    }
+  }
+}
+
+template <typename TA, typename TB>
+void dgemm(skema_ctx* c, int64_t M, int64_t N, int64_t K, double alpha, const TA* A, int64_t ars,
+           int64_t acs, const TB* B, int64_t brs, int64_t bcs, double beta, double* C, int64_t crs,
+           int64_t ccs, bool allow_split = true);
+
+__global__ void dscale_kernel(double* C, int64_t crs, int64_t ccs, int64_t M, int64_t N, double b) {
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < M * N;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = q % M, j = q / M;
+    double* p = C + i * crs + j * ccs;
+    *p = (b == 0.0) ? 0.0 : b * *p;
+  }
+}
+
+template <typename TA, typename TB>
+void dgemm(skema_ctx* c, int64_t M, int64_t N, int64_t K, double alpha, const TA* A, int64_t ars,
+           int64_t acs, const TB* B, int64_t brs, int64_t bcs, double beta, double* C, int64_t crs,
+           int64_t ccs, bool allow_split) {
+  if (M <= 0 || N <= 0) return;
+  const int64_t tiles = ((M + 63) / 64) * ((N + 63) / 64);
+  int64_t split = 1;
+  if (allow_split && tiles < 2 * c->sm_count && K >= 512)
+    split = std::min<int64_t>((2 * c->sm_count + tiles - 1) / tiles, K / 256);
+  if (split > 1) {
+    dscale_kernel<<<(int)std::min<int64_t>((M * N + 255) / 256, 4096), 256, 0, c->stream>>>(
+        C, crs, ccs, M, N, beta);
+    SKEMA_LAUNCHED(c);
+  }
+  int64_t kchunk = (K + split - 1) / split;
+  kchunk = (kchunk + 7) / 8 * 8;
+  const int64_t gz = std::max<int64_t>(1, (K + kchunk - 1) / kchunk);
+  if ((N + 63) / 64 > 65535) fail(SKEMA_EUNSUPPORTED, "dgemm: N too large");
+  dim3 grid((unsigned)((M + 63) / 64), (unsigned)((N + 63) / 64), (unsigned)gz);
+  if (split > 1)
+    dgemm_kernel<TA, TB, true><<<grid, 256, 0, c->stream>>>(M, N, K, alpha, A, ars, acs, B, brs,
+                                                            bcs, beta, C, crs, ccs, kchunk);
+  else
+    dgemm_kernel<TA, TB, false><<<grid, 256, 0, c->stream>>>(M, N, K, alpha, A, ars, acs, B, brs,
+                                                             bcs, beta, C, crs, ccs, kchunk);
+  SKEMA_LAUNCHED(c);
+}
+
+// ----------------------------------------------------- conversions ----------
+__global__ void f2d_kernel(const float* __restrict__ S, int64_t srs, int64_t scs,
+                           double* __restrict__ D, int64_t drs, int64_t dcs, int64_t M, int64_t N) {
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < M * N;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    int64_t i, j;
+    if (drs == 1) { i = q % M; j = q / M; } else { i = q / N; j = q % N; }
+    D[i * drs + j * dcs] = (double)S[i * srs + j * scs];
+  }
+}
+
+// ----------------------------------------------------------- Cholesky -------
+// In place on the lower triangle of the column-major k x k G (one CTA).
+// status[0] = 0 ok, j+1 if the j-th pivot was not positive.
+__global__ void cholesky_kernel(double* G, int64_t k, int* status) {
+  __shared__ double piv;
+  __shared__ int bad;
+  if (threadIdx.x == 0) bad = 0;
+  __syncthreads();
+  for (int64_t j = 0; j < k; ++j) {
+    if (threadIdx.x == 0) {
+      const double d = G[j + j * k];
+      if (!(d > 0.0) && !bad) bad = (int)(j + 1);
+      piv = (d > 0.0) ? sqrt(d) : 1.0;
+      G[j + j * k] = piv;
+    }
+    __syncthreads();
+    if (bad) break;
+    for (int64_t i = j + 1 + threadIdx.x; i < k; i += blockDim.x) G[i + j * k] /= piv;
+    __syncthreads();
+    // trailing update of the lower triangle: G(a, b) -= L(a, j) L(b, j), b > j, a >= b
+    const int64_t rem = k - j - 1;
+    for (int64_t q = threadIdx.x; q < rem * rem; q += blockDim.x) {
+      const int64_t a = j + 1 + q % rem, b = j + 1 + q / rem;
+      if (a >= b) G[a + b * k] -= G[a + j * k] * G[b + j * k];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) status[0] = bad;
+}
+
+// R (upper, column-major k x k) = L^T from the factored lower triangle of G.
+__global__ void lower_to_upper_kernel(const double* G, double* R, int64_t k) {
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < k * k;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = q % k, j = q / k;
+    R[i + j * k] = (i <= j) ? G[j + i * k] : 0.0;
+  }
+}
+
+// Solve R X = B in place for upper-triangular R (column-major k x k) and B
+// (k x nrhs, column stride ldb): one warp per right-hand side.
+__global__ void trsm_upper_kernel(const double* __restrict__ R, int64_t k, double* B, int64_t ldb,
+                                  int64_t nrhs) {
+  const int lane = threadIdx.x & 31;
+  const int64_t col = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (col >= nrhs) return;
+  double* x = B + col * ldb;
+  for (int64_t i = k - 1; i >= 0; --i) {
+    double s = 0.0;
+    for (int64_t l = i + 1 + lane; l < k; l += 32) s += R[i + l * k] * x[l];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) x[i] = (x[i] - s) / R[i + i * k];
+    __syncwarp();
+  }
+}
+
+// D = S^T for column-major k x k matrices.
+__global__ void dtranspose_kernel(const double* __restrict__ S, double* __restrict__ D, int64_t k) {
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < k * k;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = q % k, j = q / k;
+    D[i + j * k] = S[j + i * k];
+  }
+}
+
+__global__ void identity_kernel(double* I, int64_t k) {
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < k * k;
+       q += (int64_t)gridDim.x * blockDim.x)
+    I[q] = (q % k == q / k) ? 1.0 : 0.0;
+}
+
+// G(j, j) += shift
+__global__ void shift_diag_kernel(double* G, int64_t k, const double* fro2, double factor) {
+  const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (j < k) G[j + j * k] += factor * fro2[0];
+}
+
+__global__ void trace_kernel(const double* G, int64_t k, double* out) {
+  __shared__ double red[256];
+  double s = 0.0;
+  for (int64_t j = threadIdx.x; j < k; j += blockDim.x) s += G[j + j * k];
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int st = 128; st > 0; st >>= 1) {
+    if (threadIdx.x < st) red[threadIdx.x] += red[threadIdx.x + st];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[0] = red[0];
+}
+
+// --------------------------------------------------- sparse-sign maps ------
+// out(r, :) = sum_t sign_rt Q(c_rt, :) for a row-sparse map (R x m, zeta per
+// row); Q is m x k column-major (ldq), out R x k column-major (ldo).
+__global__ void rowsparse_apply_kernel(const uint32_t* __restrict__ mp, int zeta, int64_t R,
+                                       const double* __restrict__ Q, int64_t ldq, int64_t k,
+                                       double* __restrict__ out, int64_t ldo) {
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < R * k;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = q % R, j = q / R;
+    double a = 0.0;
+    for (int t = 0; t < zeta; ++t) {
+      const uint32_t w = mp[r * zeta + t];
+      const double v = Q[(int64_t)(w & 0x7fffffffu) + j * ldq];
+      a += (w >> 31) ? -v : v;
+    }
+    out[r + j * ldo] = a;
+  }
+}
+
+// out(c_jt, :) += sign_jt P(j, :) for a stored-transposed map (n rows, zeta
+// entries over R columns); out is R x k column-major, zeroed by the caller.
+__global__ void colsparse_apply_kernel(const uint32_t* __restrict__ mp, int zeta, int64_t n,
+                                       const double* __restrict__ P, int64_t ldp, int64_t k,
+                                       double* __restrict__ out, int64_t ldo) {
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n * k;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t j = q % n, col = q / n;
+    const double v = P[j + col * ldp];
+    for (int t = 0; t < zeta; ++t) {
+      const uint32_t w = mp[j * zeta + t];
+      atomicAdd(out + (int64_t)(w & 0x7fffffffu) + col * ldo, (w >> 31) ? -v : v);
+    }
+  }
+}
+
+// ------------------------------------------------------ Jacobi SVD ---------
+// One-sided Jacobi on the column-major k x k A (overwritten by A V = U S),
+// V accumulated (column-major k x k). One CTA; each warp rotates pairs.
+__global__ void __launch_bounds__(1024) jacobi_svd_kernel(double* A, double* V, int64_t k,
+                                                          int max_sweeps, double tol,
+                                                          int* sweeps_out) {
+  __shared__ unsigned long long off_max;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  for (int64_t q = threadIdx.x; q < k * k; q += blockDim.x) V[q] = (q % k == q / k) ? 1.0 : 0.0;
+  const int64_t kp = (k + 1) & ~(int64_t)1;  // even number of players
+  int sweep = 0;
+  for (; sweep < max_sweeps; ++sweep) {
+    if (threadIdx.x == 0) off_max = 0ull;
+    __syncthreads();
+    for (int64_t round = 0; round < kp - 1; ++round) {
+      for (int64_t pr = warp; pr < kp / 2; pr += nwarp) {
+        int64_t p, qq;
+        if (pr == 0) {
+          p = round;
+          qq = kp - 1;
+        } else {
+          p = (round + pr) % (kp - 1);
+          qq = (round - pr + (kp - 1)) % (kp - 1);
+        }
+        if (p > qq) { const int64_t t = p; p = qq; qq = t; }
+        if (qq >= k) continue;  // bye
+        double* ap = A + p * k;
+        double* aq = A + qq * k;
+        double al = 0.0, be = 0.0, ga = 0.0;
+        for (int64_t i = lane; i < k; i += 32) {
+          const double x = ap[i], y = aq[i];
+          al += x * x;
+          be += y * y;
+          ga += x * y;
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+          al += __shfl_xor_sync(0xffffffffu, al, o);
+          be += __shfl_xor_sync(0xffffffffu, be, o);
+          ga += __shfl_xor_sync(0xffffffffu, ga, o);
+        }
+        const double den = sqrt(al * be);
+        if (den == 0.0 || fabs(ga) <= tol * den) continue;
+        const double rel = fabs(ga) / den;
+        if (lane == 0) atomicMax(&off_max, (unsigned long long)__double_as_longlong(rel));
+        const double zeta = (be - al) / (2.0 * ga);
+        const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+        const double cs = 1.0 / sqrt(1.0 + t * t), sn = cs * t;
+        for (int64_t i = lane; i < k; i += 32) {
+          const double x = ap[i], y = aq[i];
+          ap[i] = cs * x - sn * y;
+          aq[i] = sn * x + cs * y;
+        }
+        double* vp = V + p * k;
+        double* vq = V + qq * k;
+        for (int64_t i = lane; i < k; i += 32) {
+          const double x = vp[i], y = vq[i];
+          vp[i] = cs * x - sn * y;
+          vq[i] = sn * x + cs * y;
+        }
+      }
+      __syncthreads();
+    }
+    __syncthreads();
+    if (off_max == 0ull) break;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) sweeps_out[0] = sweep;
+}
+
+// sigma_j = ||a_j||, ranks by descending sigma (ties by index), then
+// U(:, rank) = a_j / sigma_j, Vout(:, rank) = v_j, S(rank) = sigma_j.
+__global__ void svd_finish_kernel(const double* A, const double* V, int64_t k, double* U,
+                                  double* Vout, double* S, double* sig) {
+  for (int64_t j = threadIdx.x; j < k; j += blockDim.x) {
+    double s = 0.0;
+    for (int64_t i = 0; i < k; ++i) s += A[i + j * k] * A[i + j * k];
+    sig[j] = sqrt(s);
+  }
+  __syncthreads();
+  for (int64_t j = threadIdx.x; j < k; j += blockDim.x) {
+    int64_t rank = 0;
+    const double sj = sig[j];
+    for (int64_t l = 0; l < k; ++l)
+      if (sig[l] > sj || (sig[l] == sj && l < j)) ++rank;
+    S[rank] = sj;
+    const double inv = sj > 0.0 ? 1.0 / sj : 0.0;
+    for (int64_t i = 0; i < k; ++i) {
+      U[i + rank * k] = A[i + j * k] * inv;
+      Vout[i + rank * k] = V[i + j * k];
+    }
+  }
+}
+
+// ------------------------------------------------------------ helpers ------
+struct DevBuf {
+  void* p = nullptr;
+  explicit DevBuf(size_t bytes) { SKEMA_CUDA(cudaMalloc(&p, std::max<size_t>(bytes, 16))); }
+  ~DevBuf() {
+    if (p) cudaFree(p);
+  }
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  double* d() const { return (double*)p; }
+};
+
+int g1(const skema_ctx* c, int64_t total) {
+  return (int)std::max<int64_t>(1, std::min<int64_t>((total + 255) / 256, (int64_t)c->sm_count * 16));
+}
+
+// In-place CholeskyQR2 (+ shifted pre-pass if needed) of the column-major
+// rows x k matrix Qm (ld = rows). On return Rout (k x k, upper, column-major)
+// holds R with Q_in = Q_out R.
+void cholqr(skema_ctx* c, double* Qm, int64_t rows, int64_t k, double* Rout, double* work,
+            int* dstatus) {
+  double* G = work;            // k x k
+  double* R = work + k * k;    // k x k
+  double* Racc = work + 2 * k * k;
+  double* fro2 = work + 3 * k * k;
+  identity_kernel<<<g1(c, k * k), 256, 0, c->stream>>>(Racc, k);
+  SKEMA_LAUNCHED(c);
+  int passes_left = 2;
+  bool shifted = false;
+  while (passes_left > 0) {
+    // G = Q^T Q
+    dgemm<double, double>(c, k, k, rows, 1.0, Qm, rows, 1, Qm, 1, rows, 0.0, G, 1, k);
+    cholesky_kernel<<<1, 1024, 0, c->stream>>>(G, k, dstatus);
+    SKEMA_LAUNCHED(c);
+    int st = 0;
+    SKEMA_CUDA(cudaMemcpyAsync(&st, dstatus, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    SKEMA_CUDA(cudaStreamSynchronize(c->stream));
+    if (st != 0) {
+      if (shifted) fail(SKEMA_ENOTPD, "Cholesky of the Gram matrix failed after the shifted pass");
+      // shifted CholeskyQR: G + s I with s = 11 (rows*k + k(k+1)) u ||Q||_F^2
+      dgemm<double, double>(c, k, k, rows, 1.0, Qm, rows, 1, Qm, 1, rows, 0.0, G, 1, k);
+      trace_kernel<<<1, 256, 0, c->stream>>>(G, k, fro2);
+      SKEMA_LAUNCHED(c);
+      const double u = 1.1102230246251565e-16;
+      shift_diag_kernel<<<(int)((k + 255) / 256), 256, 0, c->stream>>>(
+          G, k, fro2, 11.0 * ((double)rows * k + (double)k * (k + 1)) * u);
+      SKEMA_LAUNCHED(c);
+      cholesky_kernel<<<1, 1024, 0, c->stream>>>(G, k, dstatus);
+      SKEMA_LAUNCHED(c);
+      SKEMA_CUDA(cudaMemcpyAsync(&st, dstatus, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+      SKEMA_CUDA(cudaStreamSynchronize(c->stream));
+      if (st != 0) fail(SKEMA_ENOTPD, "shifted Cholesky of the Gram matrix failed");
+      shifted = true;
+      passes_left = 3;  // shifted pass + CholeskyQR2
+    }
+    lower_to_upper_kernel<<<g1(c, k * k), 256, 0, c->stream>>>(G, R, k);
+    SKEMA_LAUNCHED(c);
+    // Q <- Q R^{-1}: solve R^T Q^T = ... via rows: transpose form R^T x = q_row
+    // done as Q^T <- R^{-T} Q^T; equivalently solve with the inverse:
+    // Rinv = R^{-1} (upper) then Q <- Q Rinv.
+    identity_kernel<<<g1(c, k * k), 256, 0, c->stream>>>(G, k);
+    SKEMA_LAUNCHED(c);
+    trsm_upper_kernel<<<(int)((k * 32 + 255) / 256), 256, 0, c->stream>>>(R, k, G, k, k);
+    SKEMA_LAUNCHED(c);
+    // Qm <- Qm * Rinv  (rows x k) via a temporary in Rout's slot? use work tail
+    double* Qtmp = work + 3 * k * k + 8;
+    dgemm<double, double>(c, rows, k, k, 1.0, Qm, 1, rows, G, 1, k, 0.0, Qtmp, 1, rows, false);
+    SKEMA_CUDA(cudaMemcpyAsync(Qm, Qtmp, sizeof(double) * (size_t)(rows * k),
+                               cudaMemcpyDeviceToDevice, c->stream));
+    // Racc <- R * Racc
+    double* tmp = Rout;
+    dgemm<double, double>(c, k, k, k, 1.0, R, 1, k, Racc, 1, k, 0.0, tmp, 1, k, false);
+    SKEMA_CUDA(cudaMemcpyAsync(Racc, tmp, sizeof(double) * (size_t)(k * k),
+                               cudaMemcpyDeviceToDevice, c->stream));
+    --passes_left;
+  }
+  SKEMA_CUDA(cudaMemcpyAsync(Rout, Racc, sizeof(double) * (size_t)(k * k), cudaMemcpyDeviceToDevice,
+                             c->stream));
+}
+
+size_t cholqr_work_doubles(int64_t rows, int64_t k) { return (size_t)(3 * k * k + 8 + rows * k); }
+
+// out (R x k, column-major ld R) = Map~ (R x cols) * Qm (cols x k, column-major ld cols)
+void apply_map(skema_ctx* c, const Map& mp, const double* Qm, int64_t cols, int64_t k, double* out) {
+  const int64_t R = mp.lrows;
+  if (mp.kind == SKEMA_MAP_GAUSS) {
+    dgemm<float, double>(c, R, k, cols, 1.0, mp.f32, mp.rs, mp.cs, Qm, 1, cols, 0.0, out, 1, R);
+    return;
+  }
+  if (!mp.transposed) {
+    rowsparse_apply_kernel<<<g1(c, R * k), 256, 0, c->stream>>>(mp.packed, mp.zeta, R, Qm, cols, k,
+                                                                 out, R);
+    SKEMA_LAUNCHED(c);
+  } else {
+    SKEMA_CUDA(cudaMemsetAsync(out, 0, sizeof(double) * (size_t)(R * k), c->stream));
+    colsparse_apply_kernel<<<g1(c, cols * k), 256, 0, c->stream>>>(mp.packed, mp.zeta, cols, Qm,
+                                                                    cols, k, out, R);
+    SKEMA_LAUNCHED(c);
+  }
+}
+
+}  // namespace
+
+void low_rank_approx(skema_ctx* c, double* Uout, double* Sout, double* Vout) {
+  const int64_t m = c->m, n = c->n, k = c->k, s = c->s, r = c->p.rank;
+  y_materialize(c);
+  DevBuf bQ(sizeof(double) * (size_t)(m * k));
+  DevBuf bP(sizeof(double) * (size_t)(n * k));
+  DevBuf bW(sizeof(double) * cholqr_work_doubles(std::max(m, std::max(n, s)), k));
+  DevBuf bU1(sizeof(double) * (size_t)(s * k));
+  DevBuf bU2(sizeof(double) * (size_t)(s * k));
+  DevBuf bsmall(sizeof(double) * (size_t)(8 * k * k + s * s + k * s + 4 * k + 64));
+  DevBuf bstat(sizeof(int) * 4);
+  double* Q = bQ.d();
+  double* P = bP.d();
+  double* W = bW.d();
+  double* U1 = bU1.d();
+  double* U2 = bU2.d();
+  double* T1 = bsmall.d();
+  double* T2 = T1 + k * k;
+  double* Z1 = T2 + k * k;         // k x s
+  double* Z2 = Z1 + k * s;         // k x k
+  double* Z2t = Z2 + k * k;        // k x k
+  double* Uc = Z2t + k * k;        // k x k
+  double* Vc = Uc + k * k;         // k x k
+  double* Sv = Vc + k * k;         // k
+  double* sig = Sv + k;            // k
+  double* Zd = sig + k;            // s x s
+  int* st = (int*)bstat.p;
+
+  // Q = Y (m x k, column-major, FP64); P = X^T (n x k, column-major)
+  f2d_kernel<<<g1(c, m * k), 256, 0, c->stream>>>(c->Y, k, 1, Q, 1, m, m, k);
+  SKEMA_LAUNCHED(c);
+  f2d_kernel<<<g1(c, n * k), 256, 0, c->stream>>>(c->X, 1, n, P, 1, n, n, k);
+  SKEMA_LAUNCHED(c);
+  f2d_kernel<<<g1(c, s * s), 256, 0, c->stream>>>(c->Z, s, 1, Zd, 1, s, s, s);
+  SKEMA_LAUNCHED(c);
+  cholqr(c, P, n, k, T1, W, st);  // T1 used as scratch R here
+  cholqr(c, Q, m, k, T1, W, st);
+  // U1 = Phi~ Q (s x k), U2 = Psi~ P (s x k)
+  apply_map(c, c->phi, Q, m, k, U1);
+  apply_map(c, c->psi, P, n, k, U2);
+  cholqr(c, U1, s, k, T1, W, st);
+  cholqr(c, U2, s, k, T2, W, st);
+  // Z1 = U1^T Z (k x s); Z2 = Z1 U2 (k x k)
+  dgemm<double, double>(c, k, s, s, 1.0, U1, s, 1, Zd, 1, s, 0.0, Z1, 1, k);
+  dgemm<double, double>(c, k, k, s, 1.0, Z1, 1, k, U2, 1, s, 0.0, Z2, 1, k);
+  // Z2 = T1 \ Z2
+  trsm_upper_kernel<<<(int)((k * 32 + 255) / 256), 256, 0, c->stream>>>(T1, k, Z2, k, k);
+  SKEMA_LAUNCHED(c);
+  // C^T = T2 \ Z2^T
+  dtranspose_kernel<<<g1(c, k * k), 256, 0, c->stream>>>(Z2, Z2t, k);
+  SKEMA_LAUNCHED(c);
+  trsm_upper_kernel<<<(int)((k * 32 + 255) / 256), 256, 0, c->stream>>>(T2, k, Z2t, k, k);
+  SKEMA_LAUNCHED(c);
+  // C = (Z2t)^T: copy into Uc's slot as the Jacobi working matrix
+  double* C = Uc;
+  {
+    double* Cw = W;  // k x k working copy
+    dtranspose_kernel<<<g1(c, k * k), 256, 0, c->stream>>>(Z2t, Cw, k);
+    SKEMA_LAUNCHED(c);
+    jacobi_svd_kernel<<<1, 1024, 0, c->stream>>>(Cw, Vc, k, 60, 1e-15, st + 1);
+    SKEMA_LAUNCHED(c);
+    svd_finish_kernel<<<1, 256, 0, c->stream>>>(Cw, Vc, k, C, Z2 /*Vout*/, Sv, sig);
+    SKEMA_LAUNCHED(c);
+  }
+  // U = Q Uc(:, 1:r), V = P Vc(:, 1:r), S = S(1:r)
+  if (Uout) dgemm<double, double>(c, m, r, k, 1.0, Q, 1, m, C, 1, k, 0.0, Uout, 1, m, false);
+  if (Vout) dgemm<double, double>(c, n, r, k, 1.0, P, 1, n, Z2, 1, k, 0.0, Vout, 1, n, false);
+  if (Sout)
+    SKEMA_CUDA(cudaMemcpyAsync(Sout, Sv, sizeof(double) * (size_t)r, cudaMemcpyDeviceToDevice, c->stream));
+  SKEMA_CUDA(cudaStreamSynchronize(c->stream));
+}
+
+}  // namespace skema

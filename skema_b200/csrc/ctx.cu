@@ -1,0 +1,679 @@
+// ctx.cu -- the C ABI of include/skema_c.h: context lifecycle, parameter
+// resolution, map orientation, sketch import/export and dispatch of the
+// linear update to the kernels of the other translation units.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+
+#include "internal.h"
+
+namespace skema {
+
+static thread_local std::string g_create_error;
+
+void fail(int status, const std::string& msg) { throw Error{status, msg}; }
+
+void cuda_check(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) {
+    const int st = (e == cudaErrorMemoryAllocation) ? SKEMA_ENOMEM
+                   : (e == cudaErrorNoDevice || e == cudaErrorNoKernelImageForDevice ||
+                      e == cudaErrorInsufficientDriver)
+                       ? SKEMA_ENOKERNEL
+                       : SKEMA_ECUDA;
+    fail(st, std::string(what) + ": " + cudaGetErrorString(e));
+  }
+}
+
+void* workspace(skema_ctx* c, size_t bytes) {
+  if (bytes <= c->ws_bytes) return c->ws;
+  if (c->ws) {
+    SKEMA_CUDA(cudaStreamSynchronize(c->stream));
+    SKEMA_CUDA(cudaFree(c->ws));
+    c->ws = nullptr;
+    c->ws_bytes = 0;
+  }
+  const size_t b = std::max<size_t>(bytes, 1 << 20);
+  SKEMA_CUDA(cudaMalloc(&c->ws, b));
+  c->ws_bytes = b;
+  return c->ws;
+}
+
+void* staging(skema_ctx* c, size_t bytes) {
+  if (bytes <= c->stage_bytes) return c->stage;
+  if (c->stage) {
+    SKEMA_CUDA(cudaStreamSynchronize(c->stream));
+    SKEMA_CUDA(cudaFree(c->stage));
+    c->stage = nullptr;
+    c->stage_bytes = 0;
+  }
+  const size_t b = std::max<size_t>(bytes, 1 << 20);
+  SKEMA_CUDA(cudaMalloc(&c->stage, b));
+  c->stage_bytes = b;
+  return c->stage;
+}
+
+bool y_rows_clean(const skema_ctx* c, int64_t a, int64_t b) {
+  for (const Interval& iv : c->y_written)
+    if (iv.a < b && a < iv.b) return false;
+  return true;
+}
+
+void y_rows_mark(skema_ctx* c, int64_t a, int64_t b) {
+  if (a >= b) return;
+  std::vector<Interval>& v = c->y_written;
+  v.push_back({a, b});
+  std::sort(v.begin(), v.end(), [](const Interval& x, const Interval& y) { return x.a < y.a; });
+  std::vector<Interval> out;
+  for (const Interval& iv : v) {
+    if (!out.empty() && iv.a <= out.back().b)
+      out.back().b = std::max(out.back().b, iv.b);
+    else
+      out.push_back(iv);
+  }
+  v.swap(out);
+}
+
+void y_materialize(skema_ctx* c) {
+  int64_t at = 0;
+  for (const Interval& iv : c->y_written) {
+    if (iv.a > at)
+      SKEMA_CUDA(cudaMemsetAsync(c->Y + at * c->k, 0, sizeof(float) * (size_t)((iv.a - at) * c->k),
+                                 c->stream));
+    at = std::max(at, iv.b);
+  }
+  if (at < c->m)
+    SKEMA_CUDA(cudaMemsetAsync(c->Y + at * c->k, 0, sizeof(float) * (size_t)((c->m - at) * c->k),
+                               c->stream));
+  c->y_written.assign(1, Interval{0, c->m});
+}
+
+const char* const kStageNames[ST_COUNT] = {"update.omega",   "update.psi",    "update.upsilon",
+                                            "update.phi",     "update.entries", "update.window",
+                                            "update.fused",   "update.daxpy"};
+
+static cudaEvent_t pool_event(skema_ctx* c) {
+  if (!c->event_pool.empty()) {
+    cudaEvent_t e = c->event_pool.back();
+    c->event_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  SKEMA_CUDA(cudaEventCreate(&e));
+  return e;
+}
+
+StageScope::StageScope(skema_ctx* c, int stage) : c_(c), stage_(stage) {
+  if (!c_->timing) return;
+  a_ = pool_event(c_);
+  SKEMA_CUDA(cudaEventRecord(a_, c_->stream));
+}
+
+StageScope::~StageScope() {
+  if (!a_) return;
+  cudaEvent_t b = nullptr;
+  if (!c_->event_pool.empty()) {
+    b = c_->event_pool.back();
+    c_->event_pool.pop_back();
+  } else if (cudaEventCreate(&b) != cudaSuccess) {
+    return;
+  }
+  if (cudaEventRecord(b, c_->stream) != cudaSuccess) return;
+  c_->pending.push_back(PendingTimer{stage_, a_, b});
+}
+
+static void drain_timers(skema_ctx* c) {
+  if (c->pending.empty()) return;
+  SKEMA_CUDA(cudaStreamSynchronize(c->stream));
+  for (const PendingTimer& t : c->pending) {
+    float ms = 0.f;
+    SKEMA_CUDA(cudaEventElapsedTime(&ms, t.a, t.b));
+    c->stage_ms[t.stage] += ms;
+    c->stage_n[t.stage] += 1;
+    c->event_pool.push_back(t.a);
+    c->event_pool.push_back(t.b);
+  }
+  c->pending.clear();
+}
+
+static void free_all(skema_ctx* c) {
+  for (const PendingTimer& t : c->pending) {
+    cudaEventDestroy(t.a);
+    cudaEventDestroy(t.b);
+  }
+  c->pending.clear();
+  for (cudaEvent_t e : c->event_pool) cudaEventDestroy(e);
+  c->event_pool.clear();
+  map_free(c->ups);
+  map_free(c->omg);
+  map_free(c->phi);
+  map_free(c->psi);
+  if (c->X) cudaFree(c->X);
+  if (c->Y) cudaFree(c->Y);
+  if (c->Z) cudaFree(c->Z);
+  if (c->ws) cudaFree(c->ws);
+  if (c->stage) cudaFree(c->stage);
+  c->X = c->Y = c->Z = nullptr;
+  c->ws = c->stage = nullptr;
+  if (c->own_stream) cudaStreamDestroy(c->own_stream);
+  c->own_stream = nullptr;
+}
+
+// Runs f, converting library errors into a status and remembering the message.
+template <typename F>
+static int guarded(skema_ctx* c, F&& f) {
+  if (!c) return SKEMA_EINVAL;
+  try {
+    SKEMA_CUDA(cudaSetDevice(c->dev));
+    f();
+    c->err.clear();
+    return SKEMA_OK;
+  } catch (const Error& e) {
+    c->err = e.msg;
+    return e.status;
+  } catch (const std::bad_alloc&) {
+    c->err = "host allocation failed";
+    return SKEMA_ENOMEM;
+  } catch (...) {
+    c->err = "unexpected C++ exception";
+    return SKEMA_ECUDA;
+  }
+}
+
+static void set_map(Map& mp, int kind, int64_t nrow, int64_t ncol, bool transposed,
+                    int32_t seed) {
+  mp.kind = kind;
+  mp.nrow = nrow;
+  mp.ncol = ncol;
+  mp.transposed = transposed;
+  mp.lrows = transposed ? ncol : nrow;
+  mp.lcols = transposed ? nrow : ncol;
+  mp.seed = (uint32_t)seed;
+}
+
+// Orientation rules of SketchySVD's ctor (src/Skema_SketchySVD.cpp:30-95) and
+// SketchySPD's ctor (src/Skema_SketchySVD.cpp:769-775).
+static void plan_maps(skema_ctx* c) {
+  const skema_params& p = c->p;
+  const int kind = p.dim_redux;
+  if (c->spd) {
+    // Omega(ncol, range, seeds[0]) applied as Y = A * Omega (:896-903):
+    // logical Omega~ = stored^T (k x n).
+    set_map(c->omg, kind, c->n, c->k, true, p.seeds[0]);
+    return;
+  }
+  const bool gauss_sparse = p.issparse && kind == SKEMA_MAP_GAUSS;
+  const bool omega_t = p.issparse != 0;
+  set_map(c->ups, kind, gauss_sparse ? c->m : c->k, gauss_sparse ? c->k : c->m, gauss_sparse,
+          p.seeds[0]);
+  set_map(c->omg, kind, omega_t ? c->n : c->k, omega_t ? c->k : c->n, omega_t, p.seeds[1]);
+  set_map(c->phi, kind, gauss_sparse ? c->m : c->s, gauss_sparse ? c->s : c->m, gauss_sparse,
+          p.seeds[2]);
+  set_map(c->psi, kind, omega_t ? c->n : c->s, omega_t ? c->s : c->n, omega_t, p.seeds[3]);
+}
+
+static void check_dense_args(const void* A, int64_t ld, int32_t layout, int64_t rows,
+                             int64_t cols, int32_t mem) {
+  if (layout != SKEMA_COL_MAJOR && layout != SKEMA_ROW_MAJOR) fail(SKEMA_EINVAL, "bad layout");
+  if (mem != SKEMA_MEM_DEVICE && mem != SKEMA_MEM_HOST) fail(SKEMA_EINVAL, "bad mem kind");
+  if (rows > 0 && cols > 0 && !A) fail(SKEMA_EINVAL, "null matrix pointer");
+  const int64_t need = (layout == SKEMA_COL_MAJOR) ? rows : cols;
+  if (rows > 0 && cols > 0 && ld < need) fail(SKEMA_EINVAL, "leading dimension too small");
+}
+
+}  // namespace skema
+
+using namespace skema;
+
+extern "C" {
+
+int skema_params_init(skema_params* p) {
+  if (!p) return SKEMA_EINVAL;
+  std::memset(p, 0, sizeof(*p));
+  p->matrix_m = 0;
+  p->matrix_n = 0;
+  p->rank = 1;
+  p->sketch_range = 1;
+  p->sketch_core = 1;
+  p->window = 1;
+  p->sketch_eta = 1.0;
+  p->sketch_nu = 1.0;
+  p->seeds[0] = 0;
+  p->seeds[1] = 1;
+  p->seeds[2] = 2;
+  p->seeds[3] = 3;
+  p->dim_redux = SKEMA_MAP_GAUSS;
+  p->issparse = 0;
+  p->issymmetric = 0;
+  p->force_three_sketch = 0;
+  p->kernel_func = SKEMA_KERNEL_NONE;
+  p->kernel_gamma = 1.0;
+  p->precision = SKEMA_PREC_FP32;
+  p->device = 0;
+  return SKEMA_OK;
+}
+
+int skema_create(const skema_params* p, skema_ctx** out) {
+  g_create_error.clear();
+  if (!p || !out) {
+    g_create_error = "null argument";
+    return SKEMA_EINVAL;
+  }
+  *out = nullptr;
+  skema_ctx* c = new (std::nothrow) skema_ctx();
+  if (!c) return SKEMA_ENOMEM;
+  c->p = *p;
+  try {
+    if (p->matrix_m <= 0 || p->matrix_n <= 0) fail(SKEMA_EINVAL, "matrix_m and matrix_n must be > 0");
+    if (p->rank < 1) fail(SKEMA_EINVAL, "rank must be >= 1");
+    if (p->window < 1) fail(SKEMA_EINVAL, "window must be >= 1");
+    if (p->dim_redux != SKEMA_MAP_GAUSS && p->dim_redux != SKEMA_MAP_SPARSE_SIGN)
+      fail(SKEMA_EINVAL, "dim_redux must be gauss or sparse-sign");
+    if (p->kernel_func != SKEMA_KERNEL_NONE && p->kernel_func != SKEMA_KERNEL_GAUSSRBF)
+      fail(SKEMA_EINVAL, "kernel_func must be none or gaussrbf");
+    if (p->precision < SKEMA_PREC_FP32 || p->precision > SKEMA_PREC_FP8)
+      fail(SKEMA_EINVAL, "precision must be fp32, bf16 or fp8");
+    if (p->kernel_func == SKEMA_KERNEL_GAUSSRBF && p->issparse)
+      fail(SKEMA_EUNSUPPORTED, "Gauss RBF kernel on a sparse input (the reference exits here too)");
+    if (p->kernel_func == SKEMA_KERNEL_GAUSSRBF && p->matrix_m != p->matrix_n)
+      fail(SKEMA_EINVAL, "kernel input needs matrix_n == matrix_m");
+    if (!(p->kernel_gamma >= 0.0)) fail(SKEMA_EINVAL, "kernel_gamma must be >= 0");
+    c->m = p->matrix_m;
+    c->n = p->matrix_n;
+    // range/core defaults (src/Skema_SketchySVD.cpp:20-24)
+    c->k = p->sketch_range < p->rank ? 4 * p->rank + 1 : p->sketch_range;
+    c->s = p->sketch_core < p->rank ? 2 * c->k + 1 : p->sketch_core;
+    c->w = p->window;
+    c->spd = p->issymmetric && !p->force_three_sketch;
+    if (c->n >= (int64_t(1) << 31) || c->m >= (int64_t(1) << 40) || c->k >= (1 << 20) ||
+        c->s >= (1 << 20))
+      fail(SKEMA_EINVAL, "dimension out of supported range");
+    int ndev = 0;
+    cuda_check(cudaGetDeviceCount(&ndev), "cudaGetDeviceCount");
+    if (p->device < 0 || p->device >= ndev) fail(SKEMA_EINVAL, "device ordinal out of range");
+    c->dev = p->device;
+    SKEMA_CUDA(cudaSetDevice(c->dev));
+    cudaDeviceProp prop;
+    SKEMA_CUDA(cudaGetDeviceProperties(&prop, c->dev));
+    c->sm_count = prop.multiProcessorCount;
+    c->cc_major = prop.major;
+    c->cc_minor = prop.minor;
+    if (prop.major != 10) fail(SKEMA_ENOKERNEL, "this build carries sm_100a code only");
+    SKEMA_CUDA(cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking));
+    c->stream = c->own_stream;
+    plan_maps(c);
+    if (c->spd) {
+      map_generate(c, c->omg, p->precision);
+    } else {
+      map_generate(c, c->ups, p->precision);
+      map_generate(c, c->omg, p->precision);
+      map_generate(c, c->phi, p->precision);
+      map_generate(c, c->psi, p->precision);
+      if (p->dim_redux == SKEMA_MAP_SPARSE_SIGN) {
+        map_build_inverse(c, c->ups);
+        map_build_inverse(c, c->phi);
+      }
+    }
+    if (!c->spd) {
+      SKEMA_CUDA(cudaMalloc(&c->X, sizeof(float) * (size_t)(c->k * c->n)));
+      SKEMA_CUDA(cudaMalloc(&c->Z, sizeof(float) * (size_t)(c->s * c->s)));
+    }
+    SKEMA_CUDA(cudaMalloc(&c->Y, sizeof(float) * (size_t)(c->m * c->k)));
+    if (c->X) SKEMA_CUDA(cudaMemsetAsync(c->X, 0, sizeof(float) * (size_t)(c->k * c->n), c->stream));
+    if (c->Z) SKEMA_CUDA(cudaMemsetAsync(c->Z, 0, sizeof(float) * (size_t)(c->s * c->s), c->stream));
+    SKEMA_CUDA(cudaMemsetAsync(c->Y, 0, sizeof(float) * (size_t)(c->m * c->k), c->stream));
+    SKEMA_CUDA(cudaStreamSynchronize(c->stream));
+  } catch (const Error& e) {
+    g_create_error = e.msg;
+    free_all(c);
+    delete c;
+    return e.status;
+  } catch (const std::bad_alloc&) {
+    g_create_error = "host allocation failed";
+    free_all(c);
+    delete c;
+    return SKEMA_ENOMEM;
+  }
+  *out = c;
+  return SKEMA_OK;
+}
+
+int skema_destroy(skema_ctx* c) {
+  if (!c) return SKEMA_OK;
+  cudaSetDevice(c->dev);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  free_all(c);
+  delete c;
+  return SKEMA_OK;
+}
+
+const char* skema_last_error(const skema_ctx* c) {
+  if (!c) return g_create_error.c_str();
+  return c->err.c_str();
+}
+
+int skema_get_dims(const skema_ctx* c, int64_t* range, int64_t* core, int32_t* spd) {
+  if (!c) return SKEMA_EINVAL;
+  if (range) *range = c->k;
+  if (core) *core = c->s;
+  if (spd) *spd = c->spd ? 1 : 0;
+  return SKEMA_OK;
+}
+
+int skema_reset(skema_ctx* c) {
+  return guarded(c, [&] {
+    if (c->X) SKEMA_CUDA(cudaMemsetAsync(c->X, 0, sizeof(float) * (size_t)(c->k * c->n), c->stream));
+    if (c->Z) SKEMA_CUDA(cudaMemsetAsync(c->Z, 0, sizeof(float) * (size_t)(c->s * c->s), c->stream));
+    // Y is zeroed lazily: the update kernels treat rows not written since the
+    // reset as zero (write-only), and y_materialize() clears the rest before
+    // Y is read back or factorised.
+    c->y_written.clear();
+  });
+}
+
+int skema_linear_update_dense(skema_ctx* c, const float* A, int64_t ld, int32_t layout,
+                              int64_t row0, int64_t nrows, int32_t mem) {
+  return guarded(c, [&] {
+    if (c->p.kernel_func != SKEMA_KERNEL_NONE)
+      fail(SKEMA_ESTATE, "context expects kernel points: use skema_linear_update_rbf");
+    if (c->p.issparse) fail(SKEMA_ESTATE, "context was created for a CSR input");
+    if (row0 < 0 || nrows < 0 || row0 + nrows > c->m) fail(SKEMA_EINVAL, "row range outside A");
+    check_dense_args(A, ld, layout, nrows, c->n, mem);
+    if (nrows == 0) return;
+    if (mem == SKEMA_MEM_DEVICE) {
+      Mat a{A, layout == SKEMA_COL_MAJOR ? 1 : ld, layout == SKEMA_COL_MAJOR ? ld : 1};
+      dense_update(c, a, row0, nrows);
+      return;
+    }
+    // Host input: stage window by window (the device path then sees a
+    // column-major w x n block with ld = w).
+    const int64_t W = c->w;
+    const size_t win_bytes = sizeof(float) * (size_t)(std::min(W, nrows) * c->n);
+    float* buf = (float*)staging(c, win_bytes);
+    for (int64_t r = 0; r < nrows; r += W) {
+      const int64_t wr = std::min(W, nrows - r);
+      if (layout == SKEMA_COL_MAJOR) {
+        SKEMA_CUDA(cudaMemcpy2DAsync(buf, sizeof(float) * wr, A + r, sizeof(float) * ld,
+                                     sizeof(float) * wr, c->n, cudaMemcpyHostToDevice, c->stream));
+        Mat a{buf, 1, wr};
+        dense_update(c, a, row0 + r, wr);
+      } else {
+        SKEMA_CUDA(cudaMemcpy2DAsync(buf, sizeof(float) * c->n, A + r * ld, sizeof(float) * ld,
+                                     sizeof(float) * c->n, wr, cudaMemcpyHostToDevice, c->stream));
+        Mat a{buf, c->n, 1};
+        dense_update(c, a, row0 + r, wr);
+      }
+    }
+  });
+}
+
+int skema_linear_update_csr(skema_ctx* c, const int64_t* rowptr, const int32_t* col,
+                            const float* val, int64_t row0, int64_t nrows, int32_t mem) {
+  return guarded(c, [&] {
+    if (!c->p.issparse) fail(SKEMA_ESTATE, "context was created for a dense input");
+    if (row0 < 0 || nrows < 0 || row0 + nrows > c->m) fail(SKEMA_EINVAL, "row range outside A");
+    if (mem != SKEMA_MEM_DEVICE && mem != SKEMA_MEM_HOST) fail(SKEMA_EINVAL, "bad mem kind");
+    if (nrows == 0) return;
+    if (!rowptr) fail(SKEMA_EINVAL, "null rowptr");
+    if (mem == SKEMA_MEM_DEVICE) {
+      csr_update(c, rowptr, col, val, 0, row0, nrows);
+      return;
+    }
+    const int64_t base = rowptr[0];
+    const int64_t nnz = rowptr[nrows] - base;
+    if (nnz < 0) fail(SKEMA_EINVAL, "rowptr is decreasing");
+    for (int64_t i = 0; i < nrows; ++i)
+      if (rowptr[i + 1] < rowptr[i]) fail(SKEMA_EINVAL, "rowptr is decreasing");
+    if (nnz > 0 && (!col || !val)) fail(SKEMA_EINVAL, "null col/val");
+    const size_t rp_bytes = sizeof(int64_t) * (size_t)(nrows + 1);
+    const size_t rp_pad = (rp_bytes + 255) / 256 * 256;
+    const size_t c_bytes = sizeof(int32_t) * (size_t)nnz;
+    const size_t c_pad = (c_bytes + 255) / 256 * 256;
+    char* buf = (char*)staging(c, rp_pad + c_pad + sizeof(float) * (size_t)nnz + 256);
+    int64_t* d_rp = (int64_t*)buf;
+    int32_t* d_col = (int32_t*)(buf + rp_pad);
+    float* d_val = (float*)(buf + rp_pad + c_pad);
+    SKEMA_CUDA(cudaMemcpyAsync(d_rp, rowptr, rp_bytes, cudaMemcpyHostToDevice, c->stream));
+    if (nnz > 0) {
+      SKEMA_CUDA(cudaMemcpyAsync(d_col, col + base, c_bytes, cudaMemcpyHostToDevice, c->stream));
+      SKEMA_CUDA(cudaMemcpyAsync(d_val, val + base, sizeof(float) * (size_t)nnz,
+                                 cudaMemcpyHostToDevice, c->stream));
+    }
+    csr_update(c, d_rp, d_col, d_val, base, row0, nrows);
+  });
+}
+
+int skema_linear_update_rbf(skema_ctx* c, const float* pts, int64_t ld, int32_t layout,
+                            int64_t npts, int64_t d, int64_t row0, int64_t nrows, int32_t mem) {
+  return guarded(c, [&] {
+    if (c->p.kernel_func != SKEMA_KERNEL_GAUSSRBF)
+      fail(SKEMA_ESTATE, "context was not created with kernel_func = gaussrbf");
+    if (npts != c->m) fail(SKEMA_EINVAL, "npts must equal matrix_m");
+    if (d <= 0) fail(SKEMA_EINVAL, "d must be > 0");
+    if (row0 < 0 || nrows < 0 || row0 + nrows > c->m) fail(SKEMA_EINVAL, "row range outside K");
+    check_dense_args(pts, ld, layout, npts, d, mem);
+    if (nrows == 0) return;
+    if (mem == SKEMA_MEM_DEVICE) {
+      Mat P{pts, layout == SKEMA_COL_MAJOR ? 1 : ld, layout == SKEMA_COL_MAJOR ? ld : 1};
+      rbf_update(c, P, npts, d, row0, nrows);
+      return;
+    }
+    float* buf = (float*)staging(c, sizeof(float) * (size_t)(npts * d));
+    if (layout == SKEMA_COL_MAJOR) {
+      SKEMA_CUDA(cudaMemcpy2DAsync(buf, sizeof(float) * npts, pts, sizeof(float) * ld,
+                                   sizeof(float) * npts, d, cudaMemcpyHostToDevice, c->stream));
+      rbf_update(c, Mat{buf, 1, npts}, npts, d, row0, nrows);
+    } else {
+      SKEMA_CUDA(cudaMemcpy2DAsync(buf, sizeof(float) * d, pts, sizeof(float) * ld,
+                                   sizeof(float) * d, npts, cudaMemcpyHostToDevice, c->stream));
+      rbf_update(c, Mat{buf, d, 1}, npts, d, row0, nrows);
+    }
+  });
+}
+
+int skema_low_rank_approx(skema_ctx* c, double* U, double* S, double* V, int32_t mem) {
+  return guarded(c, [&] {
+    if (c->spd) fail(SKEMA_EUNSUPPORTED, "the SketchySPD fixed-rank approximation is not provided");
+    if (mem != SKEMA_MEM_DEVICE && mem != SKEMA_MEM_HOST) fail(SKEMA_EINVAL, "bad mem kind");
+    if (c->k > c->n || c->k > c->m) fail(SKEMA_EINVAL, "range must not exceed min(m, n)");
+    if (c->s < c->k) fail(SKEMA_EINVAL, "core must be >= range");
+    const int64_t r = c->p.rank;
+    if (r > c->k) fail(SKEMA_EINVAL, "rank must not exceed range");
+    if (mem == SKEMA_MEM_DEVICE) {
+      low_rank_approx(c, U, S, V);
+      return;
+    }
+    const size_t ub = sizeof(double) * (size_t)(c->m * r), vb = sizeof(double) * (size_t)(c->n * r);
+    char* buf = (char*)staging(c, ub + vb + sizeof(double) * (size_t)r + 512);
+    double* dU = (double*)buf;
+    double* dV = (double*)(buf + (ub + 255) / 256 * 256);
+    double* dS = (double*)(buf + (ub + 255) / 256 * 256 + (vb + 255) / 256 * 256);
+    low_rank_approx(c, U ? dU : nullptr, S ? dS : nullptr, V ? dV : nullptr);
+    if (U) SKEMA_CUDA(cudaMemcpyAsync(U, dU, ub, cudaMemcpyDeviceToHost, c->stream));
+    if (V) SKEMA_CUDA(cudaMemcpyAsync(V, dV, vb, cudaMemcpyDeviceToHost, c->stream));
+    if (S) SKEMA_CUDA(cudaMemcpyAsync(S, dS, sizeof(double) * (size_t)r, cudaMemcpyDeviceToHost, c->stream));
+    SKEMA_CUDA(cudaStreamSynchronize(c->stream));
+  });
+}
+
+static void sketch_shape(const skema_ctx* c, int32_t which, float** p, int64_t* rows, int64_t* cols) {
+  switch (which) {
+    case SKEMA_SKETCH_X:
+      *p = c->X, *rows = c->k, *cols = c->n;
+      break;
+    case SKEMA_SKETCH_Y:
+      *p = c->Y, *rows = c->m, *cols = c->k;
+      break;
+    case SKEMA_SKETCH_Z:
+      *p = c->Z, *rows = c->s, *cols = c->s;
+      break;
+    default:
+      fail(SKEMA_EINVAL, "which must be X, Y or Z");
+  }
+  if (!*p) fail(SKEMA_ESTATE, "this context has no such sketch (SketchySPD keeps Y only)");
+}
+
+int skema_get_sketch(skema_ctx* c, int32_t which, float* buf, int64_t ld, int32_t layout,
+                     int32_t mem) {
+  return guarded(c, [&] {
+    float* src;
+    int64_t rows, cols;
+    sketch_shape(c, which, &src, &rows, &cols);
+    check_dense_args(buf, ld, layout, rows, cols, mem);
+    if (which == SKEMA_SKETCH_Y) y_materialize(c);
+    const cudaMemcpyKind kind = mem == SKEMA_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+    if (layout == SKEMA_ROW_MAJOR) {
+      SKEMA_CUDA(cudaMemcpy2DAsync(buf, sizeof(float) * ld, src, sizeof(float) * cols,
+                                   sizeof(float) * cols, rows, kind, c->stream));
+    } else if (mem == SKEMA_MEM_DEVICE) {
+      copy_block(c, Mat{src, cols, 1}, MatOut{buf, 1, ld}, rows, cols);
+    } else {
+      float* tmp = (float*)staging(c, sizeof(float) * (size_t)(rows * cols));
+      copy_block(c, Mat{src, cols, 1}, MatOut{tmp, 1, rows}, rows, cols);
+      SKEMA_CUDA(cudaMemcpy2DAsync(buf, sizeof(float) * ld, tmp, sizeof(float) * rows,
+                                   sizeof(float) * rows, cols, cudaMemcpyDeviceToHost, c->stream));
+    }
+    if (mem == SKEMA_MEM_HOST) SKEMA_CUDA(cudaStreamSynchronize(c->stream));
+  });
+}
+
+int skema_set_sketch(skema_ctx* c, int32_t which, const float* buf, int64_t ld, int32_t layout,
+                     int32_t mem) {
+  return guarded(c, [&] {
+    float* dst;
+    int64_t rows, cols;
+    sketch_shape(c, which, &dst, &rows, &cols);
+    check_dense_args(buf, ld, layout, rows, cols, mem);
+    const cudaMemcpyKind kind = mem == SKEMA_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+    if (layout == SKEMA_ROW_MAJOR) {
+      SKEMA_CUDA(cudaMemcpy2DAsync(dst, sizeof(float) * cols, buf, sizeof(float) * ld,
+                                   sizeof(float) * cols, rows, kind, c->stream));
+    } else if (mem == SKEMA_MEM_DEVICE) {
+      copy_block(c, Mat{buf, 1, ld}, MatOut{dst, cols, 1}, rows, cols);
+    } else {
+      float* tmp = (float*)staging(c, sizeof(float) * (size_t)(rows * cols));
+      SKEMA_CUDA(cudaMemcpy2DAsync(tmp, sizeof(float) * rows, buf, sizeof(float) * ld,
+                                   sizeof(float) * rows, cols, cudaMemcpyHostToDevice, c->stream));
+      copy_block(c, Mat{tmp, 1, rows}, MatOut{dst, cols, 1}, rows, cols);
+    }
+    if (which == SKEMA_SKETCH_Y) {
+      c->y_written.clear();
+      y_rows_mark(c, 0, c->m);
+    }
+    SKEMA_CUDA(cudaStreamSynchronize(c->stream));
+  });
+}
+
+static Map* map_of(skema_ctx* c, int32_t which) {
+  Map* mp = nullptr;
+  switch (which) {
+    case SKEMA_UPSILON: mp = &c->ups; break;
+    case SKEMA_OMEGA: mp = &c->omg; break;
+    case SKEMA_PHI: mp = &c->phi; break;
+    case SKEMA_PSI: mp = &c->psi; break;
+    default: fail(SKEMA_EINVAL, "which must be UPSILON, OMEGA, PHI or PSI");
+  }
+  if (mp->nrow == 0) fail(SKEMA_ESTATE, "this context has no such map (SketchySPD keeps Omega only)");
+  return mp;
+}
+
+int skema_map_info(const skema_ctx* cc, int32_t which, int64_t* nrow, int64_t* ncol,
+                   int32_t* zeta, int32_t* transposed) {
+  skema_ctx* c = const_cast<skema_ctx*>(cc);
+  return guarded(c, [&] {
+    Map* mp = map_of(c, which);
+    if (nrow) *nrow = mp->nrow;
+    if (ncol) *ncol = mp->ncol;
+    if (zeta) *zeta = mp->kind == SKEMA_MAP_SPARSE_SIGN ? mp->zeta : 0;
+    // The reference's init_transposed flag: SketchySPD's Omega is built
+    // without it even though it is applied as A * Omega.
+    if (transposed) *transposed = (mp->transposed && !c->spd) ? 1 : 0;
+  });
+}
+
+}  // extern "C"
+
+namespace skema {
+void map_export(skema_ctx* c, Map& mp, double* values, int32_t* indices);
+void map_import(skema_ctx* c, Map& mp, const double* values, const int32_t* indices);
+}  // namespace skema
+
+extern "C" {
+
+int skema_map_export(skema_ctx* c, int32_t which, double* values, int32_t* indices) {
+  return guarded(c, [&] {
+    Map* mp = map_of(c, which);
+    map_export(c, *mp, values, indices);
+  });
+}
+
+int skema_map_import(skema_ctx* c, int32_t which, const double* values, const int32_t* indices) {
+  return guarded(c, [&] {
+    Map* mp = map_of(c, which);
+    map_import(c, *mp, values, indices);
+  });
+}
+
+int skema_rbf_sketch_fwd(skema_ctx* c, const float* pts, int64_t npts, int64_t d, double gamma,
+                         const float* omega, int64_t k, float* Y) {
+  return guarded(c, [&] {
+    if (npts <= 0 || d <= 0 || k <= 0) fail(SKEMA_EINVAL, "npts, d and k must be > 0");
+    if (!pts || !omega || !Y) fail(SKEMA_EINVAL, "null pointer");
+    if (!(gamma >= 0.0)) fail(SKEMA_EINVAL, "gamma must be >= 0");
+    rbf_fwd(c, pts, npts, d, gamma, omega, k, Y);
+  });
+}
+
+int skema_rbf_sketch_vjp(skema_ctx* c, const float* pts, int64_t npts, int64_t d, double gamma,
+                         const float* omega, int64_t k, const float* Ybar, float* dpts,
+                         double* dgamma) {
+  return guarded(c, [&] {
+    if (npts <= 0 || d <= 0 || k <= 0) fail(SKEMA_EINVAL, "npts, d and k must be > 0");
+    if (!pts || !omega || !Ybar || !dpts || !dgamma) fail(SKEMA_EINVAL, "null pointer");
+    if (!(gamma >= 0.0)) fail(SKEMA_EINVAL, "gamma must be >= 0");
+    rbf_vjp(c, pts, npts, d, gamma, omega, k, Ybar, dpts, dgamma);
+  });
+}
+
+int skema_synchronize(skema_ctx* c) {
+  return guarded(c, [&] { SKEMA_CUDA(cudaStreamSynchronize(c->stream)); });
+}
+
+int skema_set_stream(skema_ctx* c, void* stream) {
+  return guarded(c, [&] {
+    SKEMA_CUDA(cudaStreamSynchronize(c->stream));
+    c->stream = stream ? (cudaStream_t)stream : c->own_stream;
+  });
+}
+
+int64_t skema_launch_count(const skema_ctx* c) { return c ? c->launches : -1; }
+
+int skema_timing_enable(skema_ctx* c, int32_t on) {
+  return guarded(c, [&] {
+    drain_timers(c);
+    for (int i = 0; i < ST_COUNT; ++i) {
+      c->stage_ms[i] = 0.0;
+      c->stage_n[i] = 0;
+    }
+    c->timing = on != 0;
+  });
+}
+
+int skema_timing_get(skema_ctx* c, const char* stage, double* ms, int64_t* count) {
+  return guarded(c, [&] {
+    if (!stage) fail(SKEMA_EINVAL, "null stage name");
+    drain_timers(c);
+    for (int i = 0; i < ST_COUNT; ++i) {
+      if (std::strcmp(stage, kStageNames[i]) == 0) {
+        if (ms) *ms = c->stage_ms[i];
+        if (count) *count = c->stage_n[i];
+        return;
+      }
+    }
+    fail(SKEMA_EINVAL, std::string("unknown stage ") + stage);
+  });
+}
+
+}  // extern "C"

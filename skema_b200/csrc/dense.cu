@@ -1,0 +1,109 @@
+// dense.cu -- SketchySVD::linear_update over a dense input
+// (src/Skema_SketchySVD.cpp:120-246) with update(dense, Gauss)
+// (src/Skema_SketchySVD.cpp:256-268), FP32 form, and the dispatch to the
+// SparseSign, SketchySPD and tensor-core forms.
+//
+// Per window A_w (rows [R0, R0+wr)):
+//   Y(R0:R0+wr, :) = nu*Y + eta * A_w Omega~^T          (k columns)
+//   T              =            A_w Psi~^T              (s columns, scratch)
+//   X              = nu*X + eta * Upsilon~(:, w) A_w
+//   Z              = nu*Z + eta * Phi~(:, w) T
+// Z uses the association Phi~_w (A_w Psi~^T): 2*wr*n*s + 2*s*s*wr flops per
+// window instead of the reference's (Phi~_w A_w) Psi~^T with
+// 2*s*wr*n + 2*s*s*n; both equal Phi~_w A_w Psi~^T.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "internal.h"
+
+namespace skema {
+
+bool tc_available(const skema_ctx* c);
+void tc_dense_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr, float* T);
+
+static int splitk_for(const skema_ctx* c, int64_t M, int64_t N, int64_t K) {
+  const int64_t tiles = ((M + 127) / 128) * ((N + 127) / 128);
+  int64_t sk = (2 * c->sm_count + tiles - 1) / tiles;
+  sk = std::min<int64_t>(sk, std::max<int64_t>(1, K / 256));
+  return (int)std::max<int64_t>(1, sk);
+}
+
+// The Gauss three-sketch body for one window. T is wr x s scratch.
+static void gauss_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr, float* T) {
+  const float eta = (float)c->p.sketch_eta, nu = (float)c->p.sketch_nu;
+  const Map& U = c->ups;
+  const Map& O = c->omg;
+  const Map& F = c->phi;
+  const Map& P = c->psi;
+  const float ybeta = y_rows_clean(c, R0, R0 + wr) ? 0.f : nu;
+  {  // Y rows: B(kk=j, col=r) = Omega~(r, j)
+    StageScope st(c, ST_OMEGA);
+    sgemm(c, wr, c->k, c->n, eta, Aw, Mat{O.f32, O.cs, O.rs}, ybeta,
+          MatOut{c->Y + R0 * c->k, c->k, 1});
+  }
+  y_rows_mark(c, R0, R0 + wr);
+  {  // T = A_w Psi~^T
+    StageScope st(c, ST_PSI);
+    sgemm(c, wr, c->s, c->n, 1.f, Aw, Mat{P.f32, P.cs, P.rs}, 0.f, MatOut{T, c->s, 1});
+  }
+  {  // X = nu X + eta Upsilon~(:, R0:R0+wr) A_w
+    StageScope st(c, ST_UPSILON);
+    sgemm(c, c->k, c->n, wr, eta, Mat{U.f32 + R0 * U.cs, U.rs, U.cs}, Aw, nu,
+          MatOut{c->X, c->n, 1});
+  }
+  {  // Z = nu Z + eta Phi~(:, R0:R0+wr) T
+    StageScope st(c, ST_PHI);
+    scale_block(c, MatOut{c->Z, c->s, 1}, c->s, c->s, nu);
+    sgemm(c, c->s, c->s, wr, eta, Mat{F.f32 + R0 * F.cs, F.rs, F.cs}, Mat{T, c->s, 1}, 1.f,
+          MatOut{c->Z, c->s, 1}, splitk_for(c, c->s, c->s, wr));
+  }
+}
+
+// SketchySPD, Gauss: Y(w,:) = nu*Y + eta * A_w Omega (Omega stored n x k).
+static void spd_gauss_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr) {
+  const float eta = (float)c->p.sketch_eta, nu = (float)c->p.sketch_nu;
+  const Map& O = c->omg;
+  const float ybeta = y_rows_clean(c, R0, R0 + wr) ? 0.f : nu;
+  sgemm(c, wr, c->k, c->n, eta, Aw, Mat{O.f32, O.cs, O.rs}, ybeta, MatOut{c->Y + R0 * c->k, c->k, 1});
+  y_rows_mark(c, R0, R0 + wr);
+}
+
+void spd_ssign_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr);
+
+void dense_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr, float* T) {
+  if (c->spd) {
+    if (c->p.dim_redux == SKEMA_MAP_GAUSS)
+      spd_gauss_window(c, Aw, R0, wr);
+    else
+      spd_ssign_window(c, Aw, R0, wr);
+    return;
+  }
+  if (c->p.dim_redux == SKEMA_MAP_SPARSE_SIGN) {
+    dense_ssign_window(c, Aw, R0, wr);
+    return;
+  }
+  if (c->p.precision != SKEMA_PREC_FP32) {
+    if (!tc_available(c)) fail(SKEMA_EUNSUPPORTED, "tensor-core sketch not available for this shape");
+    tc_dense_window(c, Aw, R0, wr, T);
+    return;
+  }
+  gauss_window(c, Aw, R0, wr, T);
+}
+
+size_t dense_scratch_bytes(const skema_ctx* c, int64_t wr) {
+  if (c->spd || c->p.dim_redux == SKEMA_MAP_SPARSE_SIGN) return 256;
+  return sizeof(float) * (size_t)(wr * c->s) + 256;
+}
+
+void dense_update(skema_ctx* c, Mat A, int64_t row0, int64_t nrows) {
+  const int64_t W = c->w;
+  float* T = (float*)workspace(c, dense_scratch_bytes(c, std::min(W, nrows)));
+  for (int64_t r = 0; r < nrows; r += W) {
+    const int64_t wr = std::min(W, nrows - r);
+    Mat Aw{A.p + r * A.rs, A.rs, A.cs};
+    dense_window(c, Aw, row0 + r, wr, T);
+  }
+}
+
+}  // namespace skema

@@ -1,0 +1,268 @@
+// gemm_f32.cu -- the plain FP32 contraction used by the FP32 form of the
+// sketch (the drop-in for KokkosBlas::gemm in Impl::mm,
+// src/Skema_Common.hpp:32-40) plus small strided elementwise kernels.
+//
+// SIMT GEMM: 128x128 output tile per 256-thread CTA, 8x8 outputs per thread,
+// K staged through double-buffered shared memory 8 deep. Operands are
+// addressed by (row stride, col stride) so that column-major A windows,
+// row-major maps and transposed views need no copies; the template picks the
+// coalesced load pattern from which stride is 1. Optional split-K over
+// grid.z with atomic accumulation for the small-output/large-K products.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "internal.h"
+
+namespace skema {
+
+namespace {
+
+constexpr int BM = 128, BN = 128, BK = 8, PAD = 4;
+
+template <bool A_M_CONTIG, bool B_N_CONTIG, bool ATOMIC>
+__global__ void __launch_bounds__(256)
+    sgemm_kernel(int64_t M, int64_t N, int64_t K, float alpha, const float* __restrict__ A,
+                 int64_t a_rs, int64_t a_cs, const float* __restrict__ B, int64_t b_rs,
+                 int64_t b_cs, float beta, float* __restrict__ C, int64_t c_rs, int64_t c_cs,
+                 int64_t kchunk) {
+  __shared__ __align__(16) float As[2][BK][BM + PAD];
+  __shared__ __align__(16) float Bs[2][BK][BN + PAD];
+  const int tid = threadIdx.x;
+  const int64_t m0 = (int64_t)blockIdx.x * BM;
+  const int64_t n0 = (int64_t)blockIdx.y * BN;
+  const int64_t kb = (int64_t)blockIdx.z * kchunk;
+  const int64_t ke = min(K, kb + kchunk);
+  if (kb >= ke) return;
+
+  // Load coordinates inside a tile.
+  int la_m[4], la_k[4], lb_n[4], lb_k[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    if (A_M_CONTIG) {
+      la_m[q] = tid & 127;
+      la_k[q] = (tid >> 7) + 2 * q;
+    } else {
+      la_k[q] = tid & 7;
+      la_m[q] = (tid >> 3) + 32 * q;
+    }
+    if (B_N_CONTIG) {
+      lb_n[q] = tid & 127;
+      lb_k[q] = (tid >> 7) + 2 * q;
+    } else {
+      lb_k[q] = tid & 7;
+      lb_n[q] = (tid >> 3) + 32 * q;
+    }
+  }
+  float ra[4], rb[4];
+  auto load_tile = [&](int64_t k0) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int64_t gm = m0 + la_m[q], gk = k0 + la_k[q];
+      ra[q] = (gm < M && gk < ke) ? __ldg(A + gm * a_rs + gk * a_cs) : 0.f;
+      const int64_t gn = n0 + lb_n[q], gk2 = k0 + lb_k[q];
+      rb[q] = (gn < N && gk2 < ke) ? __ldg(B + gk2 * b_rs + gn * b_cs) : 0.f;
+    }
+  };
+  auto store_tile = [&](int buf) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      As[buf][la_k[q]][la_m[q]] = ra[q];
+      Bs[buf][lb_k[q]][lb_n[q]] = rb[q];
+    }
+  };
+
+  const int tx = tid & 15, ty = tid >> 4;
+  float acc[8][8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[i][j] = 0.f;
+
+  load_tile(kb);
+  store_tile(0);
+  __syncthreads();
+  int buf = 0;
+  for (int64_t k0 = kb; k0 < ke; k0 += BK) {
+    const bool more = k0 + BK < ke;
+    if (more) load_tile(k0 + BK);
+#pragma unroll
+    for (int kk = 0; kk < BK; ++kk) {
+      const float4 a0 = *reinterpret_cast<const float4*>(&As[buf][kk][ty * 4]);
+      const float4 a1 = *reinterpret_cast<const float4*>(&As[buf][kk][64 + ty * 4]);
+      const float4 b0 = *reinterpret_cast<const float4*>(&Bs[buf][kk][tx * 4]);
+      const float4 b1 = *reinterpret_cast<const float4*>(&Bs[buf][kk][64 + tx * 4]);
+      const float a[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+      const float b[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+    }
+    if (more) {
+      store_tile(buf ^ 1);
+      __syncthreads();
+      buf ^= 1;
+    }
+  }
+
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const int64_t gm = m0 + (i < 4 ? ty * 4 + i : 64 + ty * 4 + (i - 4));
+    if (gm >= M) continue;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int64_t gn = n0 + (j < 4 ? tx * 4 + j : 64 + tx * 4 + (j - 4));
+      if (gn >= N) continue;
+      float* cp = C + gm * c_rs + gn * c_cs;
+      const float v = alpha * acc[i][j];
+      if (ATOMIC) {
+        atomicAdd(cp, v);
+      } else {
+        *cp = (beta == 0.f) ? v : fmaf(beta, *cp, v);
+      }
+    }
+  }
+}
+
+template <bool AM, bool BN_, bool AT>
+void launch_sgemm(skema_ctx* c, int64_t M, int64_t N, int64_t K, float alpha, Mat A, Mat B,
+                  float beta, MatOut C, int splitk) {
+  int64_t kchunk = (K + splitk - 1) / splitk;
+  kchunk = (kchunk + BK - 1) / BK * BK;
+  const int64_t gz = (K + kchunk - 1) / kchunk;
+  // M tiles on grid.x (2^31-1 limit); N in chunks of at most 65535 tiles.
+  const int64_t nchunk = (int64_t)65535 * BN;
+  for (int64_t nb = 0; nb < N; nb += nchunk) {
+    const int64_t nn = std::min(nchunk, N - nb);
+    dim3 grid((unsigned)((M + BM - 1) / BM), (unsigned)((nn + BN - 1) / BN), (unsigned)gz);
+    sgemm_kernel<AM, BN_, AT><<<grid, 256, 0, c->stream>>>(
+        M, nn, K, alpha, A.p, A.rs, A.cs, B.p + nb * B.cs, B.rs, B.cs, beta, C.p + nb * C.cs, C.rs,
+        C.cs, kchunk);
+    SKEMA_LAUNCHED(c);
+  }
+}
+
+__global__ void scale_kernel(float* __restrict__ C, int64_t rs, int64_t cs, int64_t M, int64_t N,
+                             float beta) {
+  const int64_t total = M * N;
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < total;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    int64_t i, j;
+    if (cs == 1) {
+      i = q / N;
+      j = q - i * N;
+    } else {
+      j = q / M;
+      i = q - j * M;
+    }
+    float* p = C + i * rs + j * cs;
+    *p = (beta == 0.f) ? 0.f : beta * *p;
+  }
+}
+
+__global__ void axpby_kernel(const float* __restrict__ S, int64_t srs, int64_t scs,
+                             float* __restrict__ D, int64_t drs, int64_t dcs, int64_t M,
+                             int64_t N, float alpha, float beta) {
+  const int64_t total = M * N;
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < total;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    int64_t i, j;
+    if (dcs == 1) {
+      i = q / N;
+      j = q - i * N;
+    } else {
+      j = q / M;
+      i = q - j * M;
+    }
+    float* d = D + i * drs + j * dcs;
+    const float v = alpha * S[i * srs + j * scs];
+    *d = (beta == 0.f) ? v : fmaf(beta, *d, v);
+  }
+}
+
+// Tiled transpose-capable copy through shared memory (32x32 tiles).
+__global__ void copy_kernel(const float* __restrict__ S, int64_t srs, int64_t scs,
+                            float* __restrict__ D, int64_t drs, int64_t dcs, int64_t M,
+                            int64_t N) {
+  __shared__ float t[32][33];
+  const int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
+  const int64_t ti = (M + 31) / 32, tj = (N + 31) / 32;
+  for (int64_t tile = blockIdx.x; tile < ti * tj; tile += gridDim.x) {
+  const int64_t i0 = (tile / tj) * 32, j0 = (tile % tj) * 32;
+  // read: make consecutive threads follow the source's unit stride
+  for (int r = ty; r < 32; r += 8) {
+    const int64_t i = (scs == 1) ? i0 + r : i0 + tx;
+    const int64_t j = (scs == 1) ? j0 + tx : j0 + r;
+    if (i < M && j < N) {
+      if (scs == 1)
+        t[r][tx] = S[i * srs + j * scs];
+      else
+        t[tx][r] = S[i * srs + j * scs];
+    }
+  }
+  __syncthreads();
+  for (int r = ty; r < 32; r += 8) {
+    const int64_t i = (dcs == 1) ? i0 + r : i0 + tx;
+    const int64_t j = (dcs == 1) ? j0 + tx : j0 + r;
+    if (i < M && j < N) {
+      if (dcs == 1)
+        D[i * drs + j * dcs] = t[r][tx];
+      else
+        D[i * drs + j * dcs] = t[tx][r];
+    }
+  }
+  __syncthreads();
+  }
+}
+
+int grid1d(const skema_ctx* c, int64_t total, int threads) {
+  const int64_t want = (total + threads - 1) / threads;
+  return (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)c->sm_count * 16));
+}
+
+}  // namespace
+
+void sgemm(skema_ctx* c, int64_t M, int64_t N, int64_t K, float alpha, Mat A, Mat B, float beta,
+           MatOut C, int splitk) {
+  if (M <= 0 || N <= 0) return;
+  if (K <= 0) {
+    if (splitk <= 1) scale_block(c, C, M, N, beta);
+    return;
+  }
+  const bool am = (A.rs == 1);
+  const bool bn = (B.cs == 1);
+  const bool at = splitk > 1;
+  if (am && bn && at) launch_sgemm<true, true, true>(c, M, N, K, alpha, A, B, beta, C, splitk);
+  else if (am && bn) launch_sgemm<true, true, false>(c, M, N, K, alpha, A, B, beta, C, 1);
+  else if (am && at) launch_sgemm<true, false, true>(c, M, N, K, alpha, A, B, beta, C, splitk);
+  else if (am) launch_sgemm<true, false, false>(c, M, N, K, alpha, A, B, beta, C, 1);
+  else if (bn && at) launch_sgemm<false, true, true>(c, M, N, K, alpha, A, B, beta, C, splitk);
+  else if (bn) launch_sgemm<false, true, false>(c, M, N, K, alpha, A, B, beta, C, 1);
+  else if (at) launch_sgemm<false, false, true>(c, M, N, K, alpha, A, B, beta, C, splitk);
+  else launch_sgemm<false, false, false>(c, M, N, K, alpha, A, B, beta, C, 1);
+}
+
+void scale_block(skema_ctx* c, MatOut C, int64_t M, int64_t N, float beta) {
+  if (M <= 0 || N <= 0 || beta == 1.f) return;
+  scale_kernel<<<grid1d(c, M * N, 256), 256, 0, c->stream>>>(C.p, C.rs, C.cs, M, N, beta);
+  SKEMA_LAUNCHED(c);
+}
+
+void axpby_block(skema_ctx* c, Mat src, MatOut dst, int64_t M, int64_t N, float alpha, float beta) {
+  if (M <= 0 || N <= 0) return;
+  axpby_kernel<<<grid1d(c, M * N, 256), 256, 0, c->stream>>>(src.p, src.rs, src.cs, dst.p, dst.rs,
+                                                              dst.cs, M, N, alpha, beta);
+  SKEMA_LAUNCHED(c);
+}
+
+void copy_block(skema_ctx* c, Mat src, MatOut dst, int64_t M, int64_t N) {
+  if (M <= 0 || N <= 0) return;
+  const int64_t tiles = ((M + 31) / 32) * ((N + 31) / 32);
+  const int grid = (int)std::min<int64_t>(tiles, (int64_t)c->sm_count * 32);
+  copy_kernel<<<grid, dim3(32, 8), 0, c->stream>>>(src.p, src.rs, src.cs, dst.p, dst.rs, dst.cs, M,
+                                                   N);
+  SKEMA_LAUNCHED(c);
+}
+
+}  // namespace skema

@@ -1,0 +1,194 @@
+// internal.h -- private declarations shared by the library's translation
+// units: the context, map storage and the launchers of every kernel.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "../../include/skema_c.h"
+
+namespace skema {
+
+// Thrown inside the library only; converted to a status at the C boundary.
+struct Error {
+  int status;
+  std::string msg;
+};
+
+[[noreturn]] void fail(int status, const std::string& msg);
+void cuda_check(cudaError_t e, const char* what);
+#define SKEMA_CUDA(call) ::skema::cuda_check((call), #call)
+// After a kernel launch: reports launch-configuration errors.
+#define SKEMA_LAUNCHED(ctx) \
+  do {                      \
+    ::skema::cuda_check(cudaGetLastError(), "kernel launch"); \
+    (ctx)->launches++;      \
+  } while (0)
+
+// A random map on the device.
+//
+// `nrow x ncol` is the stored shape of the reference's DimRedux ctor; the
+// map is `transposed` when that ctor got init_transposed=true
+// (src/Skema_SketchySVD.cpp:30-95). `lrows x lcols` is the logical operator
+// the sketch formulas use: Upsilon~ (k x m), Omega~ (k x n), Phi~ (s x m),
+// Psi~ (s x n); logical = stored^T when transposed.
+struct Map {
+  int kind = SKEMA_MAP_GAUSS;
+  int64_t nrow = 0, ncol = 0;
+  bool transposed = false;
+  int64_t lrows = 0, lcols = 0;
+  uint32_t seed = 0;
+  double maxval = 0.0;
+  int zeta = 0;
+  // Gauss: FP32 values; logical (r, c) at f32[r*rs + c*cs].
+  float* f32 = nullptr;
+  int64_t rs = 0, cs = 0;
+  // Gauss, tensor-core forms: logical rows in row-major BF16 / FP8 copies.
+  void* lowp = nullptr;
+  // SparseSign: stored rows, zeta packed entries each: column | sign << 31.
+  uint32_t* packed = nullptr;
+  // SparseSign maps that are row-sparse over the input rows (Upsilon, Phi of
+  // the three-sketch): (input row, map row, sign) triples sorted by input
+  // row, on the host and on the device.
+  std::vector<int64_t> inv_row;   // host, sorted input rows
+  int64_t* d_inv_row = nullptr;   // device copy of inv_row
+  uint32_t* d_inv_rs = nullptr;   // device: map row | sign << 31
+};
+
+struct Interval {
+  int64_t a, b;
+};
+
+enum Stage {
+  ST_OMEGA = 0,
+  ST_PSI,
+  ST_UPSILON,
+  ST_PHI,
+  ST_ENTRIES,
+  ST_WINDOW,
+  ST_FUSED,
+  ST_DAXPY,
+  ST_COUNT
+};
+extern const char* const kStageNames[ST_COUNT];
+
+struct PendingTimer {
+  int stage;
+  cudaEvent_t a, b;
+};
+
+}  // namespace skema
+
+struct skema_ctx {
+  skema_params p;
+  int64_t m = 0, n = 0, k = 0, s = 0, w = 1;
+  bool spd = false;     // SketchySPD: only Y = A Omega
+  int dev = 0;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  int64_t launches = 0;
+  skema::Map ups, omg, phi, psi;
+  // Sketches, FP32, row-major: X k x n, Y m x k, Z s x s.
+  float* X = nullptr;
+  float* Y = nullptr;
+  float* Z = nullptr;
+  // Rows of Y written since the last reset (merged, sorted intervals).
+  std::vector<skema::Interval> y_written;
+  // Workspace (grown on demand, owned).
+  void* ws = nullptr;
+  size_t ws_bytes = 0;
+  void* stage = nullptr;  // host-input staging
+  size_t stage_bytes = 0;
+  int sm_count = 148;
+  int cc_major = 0, cc_minor = 0;
+  // stage timers
+  bool timing = false;
+  std::vector<skema::PendingTimer> pending;
+  std::vector<cudaEvent_t> event_pool;
+  double stage_ms[skema::ST_COUNT] = {0};
+  int64_t stage_n[skema::ST_COUNT] = {0};
+};
+
+namespace skema {
+
+// Records CUDA events around the launches of one stage while timing is on.
+class StageScope {
+ public:
+  StageScope(skema_ctx* c, int stage);
+  ~StageScope();
+  StageScope(const StageScope&) = delete;
+  StageScope& operator=(const StageScope&) = delete;
+
+ private:
+  skema_ctx* c_;
+  int stage_;
+  cudaEvent_t a_ = nullptr;
+};
+
+void* workspace(skema_ctx* c, size_t bytes);
+void* staging(skema_ctx* c, size_t bytes);
+bool y_rows_clean(const skema_ctx* c, int64_t a, int64_t b);
+void y_rows_mark(skema_ctx* c, int64_t a, int64_t b);
+// Zero every Y row not written since the last reset.
+void y_materialize(skema_ctx* c);
+
+// ---- maps (maps.cu) ----
+void map_generate(skema_ctx* c, Map& mp, int precision);
+void map_free(Map& mp);
+void map_build_inverse(skema_ctx* c, Map& mp);
+
+// ---- FP32 SIMT GEMM (gemm_f32.cu) ----
+// C(i,j) = alpha * sum_kk A(i,kk) B(kk,j) + beta * C(i,j), every operand
+// addressed by (row stride, col stride). With splitk > 1 the K range is
+// split over grid.z and partial results are added atomically (requires the
+// caller to have applied beta beforehand; beta is ignored).
+struct Mat {
+  const float* p;
+  int64_t rs, cs;
+};
+struct MatOut {
+  float* p;
+  int64_t rs, cs;
+};
+void sgemm(skema_ctx* c, int64_t M, int64_t N, int64_t K, float alpha, Mat A,
+           Mat B, float beta, MatOut C, int splitk = 1);
+// C = beta * C over an M x N strided block.
+void scale_block(skema_ctx* c, MatOut C, int64_t M, int64_t N, float beta);
+// dst(i,j) = alpha * src(i,j) + beta * dst(i,j) over M x N (beta 0: no read).
+void axpby_block(skema_ctx* c, Mat src, MatOut dst, int64_t M, int64_t N,
+                 float alpha, float beta);
+// Copy a strided FP32 block into another strided block.
+void copy_block(skema_ctx* c, Mat src, MatOut dst, int64_t M, int64_t N);
+
+// ---- dense update (dense.cu) ----
+// One call of skema_linear_update_dense on device data.
+void dense_update(skema_ctx* c, Mat A, int64_t row0, int64_t nrows);
+// Per-window body shared with the RBF path: A_w holds rows [R0, R0+wr) of
+// the input; T is the scratch returned for dense_scratch_bytes(c, wr).
+void dense_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr, float* T);
+size_t dense_scratch_bytes(const skema_ctx* c, int64_t wr);
+
+// ---- sparse paths (sparse.cu) ----
+void csr_update(skema_ctx* c, const int64_t* rowptr, const int32_t* col,
+                const float* val, int64_t col_offset, int64_t row0,
+                int64_t nrows);
+void dense_ssign_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr);
+void spd_ssign_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr);
+
+// ---- RBF (rbf.cu) ----
+void rbf_update(skema_ctx* c, Mat P, int64_t npts, int64_t d, int64_t row0,
+                int64_t nrows);
+void rbf_fwd(skema_ctx* c, const float* pts, int64_t N, int64_t d,
+             double gamma, const float* omega, int64_t k, float* Y);
+void rbf_vjp(skema_ctx* c, const float* pts, int64_t N, int64_t d,
+             double gamma, const float* omega, int64_t k, const float* Ybar,
+             float* dpts, double* dgamma);
+
+// ---- FP64 approximation (approx.cu) ----
+void low_rank_approx(skema_ctx* c, double* U, double* S, double* V);
+
+}  // namespace skema

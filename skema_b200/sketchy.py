@@ -1,0 +1,561 @@
+"""Python host mirror of Skema's SketchySVD interface over the C ABI.
+
+Names and argument meanings follow the reference:
+
+* ``AlgParams`` -- the sketch fields of ``Skema::AlgParams``
+  (src/Skema_AlgParams.hpp:12-90) with the same defaults
+  (src/Skema_AlgParams.cpp:10-57) and the same command-line flags and
+  parsing rules (src/Skema_AlgParams.cpp:242-330, 335-600).
+* ``GaussDimRedux`` / ``SparseSignDimRedux`` -- the map types
+  (src/Skema_DimRedux.hpp:98-268), used as the DimReduxT selector.
+* ``SketchySVD`` -- ctor, ``linear_update``, ``low_rank_approx``
+  (src/Skema_SketchySVD.hpp:11-64); ``SketchySPD`` -- the one-sketch variant
+  (src/Skema_SketchySVD.hpp:67-108), update only.
+* ``sketchysvd(matrix, algParams)`` -- the driver entry
+  (src/Skema_SketchySVD.cpp:1244, 1408), returning (U, S, V).
+
+Inputs are numpy arrays / scipy CSR matrices (host memory, staged by the
+library) or CUDA torch tensors (device memory, used in place). Every call
+goes to the CUDA library; errors raise ``SkemaError``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass, field
+from typing import Any
+
+import numpy as np
+
+from . import _lib as L
+from ._lib import SkemaError
+
+__all__ = [
+    "AlgParams",
+    "GaussDimRedux",
+    "SparseSignDimRedux",
+    "SketchySVD",
+    "SketchySPD",
+    "sketchysvd",
+    "rbf_sketch_fwd",
+    "rbf_sketch_vjp",
+    "SkemaError",
+]
+
+INT_MAX = 2**31 - 1
+
+
+def _is_torch(x) -> bool:
+    return type(x).__module__.startswith("torch")
+
+
+def _error(msg: str):
+    # Skema::error (src/Skema_AlgParams.cpp:59-62)
+    raise RuntimeError(msg)
+
+
+def _find(args: list[str], flag: str) -> int:
+    if flag in args:
+        return args.index(flag)
+    if len(flag) > 2 and flag.startswith("--") and flag[2:] in args:
+        return args.index(flag[2:])
+    return -1
+
+
+def parse_bool(args, on, off, default):
+    """src/Skema_AlgParams.cpp:335-366."""
+    i = _find(args, on)
+    if i >= 0:
+        del args[i]
+        return True
+    i = _find(args, off)
+    if i >= 0:
+        del args[i]
+        return False
+    return default
+
+
+def parse_int(args, flag, default, lo=0, hi=100):
+    """src/Skema_AlgParams.cpp:433-474 (strtol prefix parse, 'inf' -> INT_MAX)."""
+    val = default
+    i = _find(args, flag)
+    if i >= 0:
+        if i + 1 >= len(args):
+            del args[i]
+            return val
+        s = args[i + 1]
+        if s in ("inf", "Inf"):
+            val = INT_MAX
+        else:
+            j = 0
+            t = s.strip()
+            if t[:1] in "+-":
+                j = 1
+            while j < len(t) and t[j].isdigit():
+                j += 1
+            if j == 0 or (j == 1 and t[:1] in "+-"):
+                _error(f"Unparseable input: {flag} {s}, must be an integer")
+            val = int(t[:j])
+        del args[i : i + 2]
+    if val < lo or val > hi:
+        _error(f"Bad input: {flag} {val},  must be in the range ({lo}, {hi})")
+    return val
+
+
+def parse_real(args, flag, default, lo=0.0, hi=1.0):
+    """src/Skema_AlgParams.cpp:476-513."""
+    val = default
+    i = _find(args, flag)
+    if i >= 0:
+        if i + 1 >= len(args):
+            del args[i]
+            return val
+        s = args[i + 1]
+        try:
+            val = float(s)
+        except ValueError:
+            _error(f"Unparseable input: {flag} {s}, must be a double")
+        del args[i : i + 2]
+    if val < lo or val > hi:
+        _error(f"Bad input: {flag} {val},  must be in the range ({lo}, {hi})")
+    return val
+
+
+def parse_enum(args, flag, default, names):
+    """src/Skema_AlgParams.cpp:368-412; returns the index into names."""
+    i = _find(args, flag)
+    if i >= 0:
+        if i + 1 >= len(args):
+            del args[i]
+            return default
+        v = args[i + 1]
+        del args[i : i + 2]
+        if v in names:
+            return names.index(v)
+        _error(f"Bad input: {flag} {v},  must be one of the values: {', '.join(names)}.")
+    return default
+
+
+def parse_string(args, flag, default):
+    i = _find(args, flag)
+    if i >= 0:
+        if i + 1 >= len(args):
+            del args[i]
+            return default
+        v = args[i + 1]
+        del args[i : i + 2]
+        return v
+    return default
+
+
+def parse_int_array(args, flag, default, lo=1, hi=INT_MAX):
+    """src/Skema_AlgParams.cpp:549-606: '[a,b,c]' with no spaces."""
+    i = _find(args, flag)
+    if i < 0:
+        return list(default)
+    if i + 1 >= len(args):
+        del args[i]
+        return list(default)
+    s = args[i + 1]
+    if not s.startswith("["):
+        _error(f"Unparseable input: {flag} {s}, must be of the form [int,...,int] with no spaces")
+    body = s[1:]
+    if body.endswith("]"):
+        body = body[:-1]
+    vals = []
+    for tok in body.split(","):
+        if tok == "":
+            continue
+        try:
+            v = int(tok)
+        except ValueError:
+            _error(f"Unparseable input: {flag} {tok}, must be of the form [int,...,int] with no spaces")
+        if v < lo or v > hi:
+            _error(f"Bad input: {flag} {tok},  must be in the range ({lo}, {hi})")
+        vals.append(v)
+    del args[i : i + 2]
+    return vals
+
+
+DIM_REDUX_NAMES = ["gauss", "sparse-sign"]      # src/Skema_Utils.hpp:74-80
+KERNEL_NAMES = ["none", "gaussrbf"]              # src/Skema_Utils.hpp:60-66
+SOLVER_NAMES = ["isvd", "sketch", "primme"]      # src/Skema_Utils.hpp:46-52
+PRECISION_NAMES = ["fp32", "bf16", "fp8"]
+
+
+@dataclass
+class AlgParams:
+    """Sketch fields of Skema::AlgParams with the reference defaults."""
+
+    solver: int = 0
+    inputfilename: str = ""
+    history_filename: str = ""
+    debug_filename: str = ""
+    issparse: bool = False
+    issymmetric: bool = False
+    matrix_m: int = 0
+    matrix_n: int = 0
+    matrix_nnz: int = 0
+    rank: int = 1
+    num_passes: int = 1
+    print_level: int = 0
+    debug: bool = False
+    window: int = 1
+    sketch_range: int = 1
+    sketch_core: int = 1
+    sketch_eta: float = 1.0
+    sketch_nu: float = 1.0
+    seeds: list = field(default_factory=lambda: [0, 1, 2, 3])
+    force_three_sketch: bool = False
+    sketch_compute_svals_iters: bool = False
+    dim_redux: int = L.MAP_GAUSS
+    kernel_func: int = L.KERNEL_NONE
+    kernel_gamma: float = 1.0
+    precision: int = L.PREC_FP32
+    device: int = 0
+
+    def parse(self, args: list[str]) -> None:
+        """Consume the sketch flags from args, as AlgParams::parse does."""
+        self.inputfilename = parse_string(args, "--input", "")
+        self.debug_filename = parse_string(args, "--debug-file", "")
+        self.history_filename = parse_string(args, "--history-file", "")
+        self.issparse = parse_bool(args, "--sparse", "--dense", False)
+        self.issymmetric = parse_bool(args, "--symmetric", "--asymmetric", False)
+        self.matrix_m = parse_int(args, "--m", self.matrix_m, 0, INT_MAX)
+        self.matrix_n = parse_int(args, "--n", self.matrix_n, 0, INT_MAX)
+        self.rank = parse_int(args, "--rank", self.rank, 1, INT_MAX)
+        self.num_passes = parse_int(args, "--num-passes", self.num_passes, 1, INT_MAX)
+        self.solver = parse_enum(args, "--solver", 0, SOLVER_NAMES)
+        self.print_level = parse_int(args, "--print-level", self.print_level, 0, 5)
+        self.debug = parse_bool(args, "--debug", "--debug-off", False)
+        self.window = parse_int(args, "--window", self.window, 1, INT_MAX)
+        self.dim_redux = parse_enum(args, "--model", L.MAP_GAUSS, DIM_REDUX_NAMES)
+        self.sketch_range = parse_int(args, "--range", self.sketch_range, 0, INT_MAX)
+        self.sketch_core = parse_int(args, "--core", self.sketch_core, 0, INT_MAX)
+        self.seeds = parse_int_array(args, "--seeds", self.seeds, 0, INT_MAX)
+        self.sketch_eta = parse_real(args, "--eta", 1.0, 0.0, math.inf)
+        self.sketch_nu = parse_real(args, "--nu", 1.0, 0.0, math.inf)
+        self.force_three_sketch = parse_bool(args, "--force-three-sketch", "--force-three-sketch-off", False)
+        self.sketch_compute_svals_iters = parse_bool(
+            args, "--sketch-compute-svals-iters", "--sketch-compute-svals-iters-off", False
+        )
+        self.kernel_func = parse_enum(args, "--kernel", L.KERNEL_NONE, KERNEL_NAMES)
+        self.kernel_gamma = parse_real(args, "--gamma", self.kernel_gamma, 0.0, math.inf)
+        self.precision = parse_enum(args, "--precision", L.PREC_FP32, PRECISION_NAMES)
+
+    def to_c(self) -> L.Params:
+        p = L.default_params()
+        p.matrix_m = int(self.matrix_m)
+        p.matrix_n = int(self.matrix_n)
+        p.rank = int(self.rank)
+        p.sketch_range = int(self.sketch_range)
+        p.sketch_core = int(self.sketch_core)
+        p.window = int(self.window)
+        p.sketch_eta = float(self.sketch_eta)
+        p.sketch_nu = float(self.sketch_nu)
+        seeds = list(self.seeds) + [0, 1, 2, 3][len(self.seeds):]
+        for i in range(4):
+            p.seeds[i] = int(seeds[i])
+        p.dim_redux = int(self.dim_redux)
+        p.issparse = int(bool(self.issparse))
+        p.issymmetric = int(bool(self.issymmetric))
+        p.force_three_sketch = int(bool(self.force_three_sketch))
+        p.kernel_func = int(self.kernel_func)
+        p.kernel_gamma = float(self.kernel_gamma)
+        p.precision = int(self.precision)
+        p.device = int(self.device)
+        return p
+
+
+class GaussDimRedux:
+    """DimReduxT selector: dense maps uniform on +-sqrt(2 ln(rows*cols))."""
+
+    kind = L.MAP_GAUSS
+
+
+class SparseSignDimRedux:
+    """DimReduxT selector: zeta = max(2, min(ncol, 8)) +-1 entries per stored row."""
+
+    kind = L.MAP_SPARSE_SIGN
+
+
+# ---------------------------------------------------------------- helpers --
+def _dense_arg(A):
+    """(pointer, ld, layout, mem, keepalive) for a 2-D float32 array/tensor."""
+    if _is_torch(A):
+        import torch
+
+        if A.dtype != torch.float32:
+            raise TypeError("dense input must be float32")
+        if A.dim() != 2:
+            raise ValueError("dense input must be 2-D")
+        if not A.is_cuda:
+            A = A.numpy()
+        else:
+            if A.stride(1) == 1 and (A.stride(0) >= A.shape[1] or A.shape[0] <= 1):
+                return A.data_ptr(), max(A.stride(0), A.shape[1], 1), L.ROW_MAJOR, L.MEM_DEVICE, A
+            if A.stride(0) == 1 and (A.stride(1) >= A.shape[0] or A.shape[1] <= 1):
+                return A.data_ptr(), max(A.stride(1), A.shape[0], 1), L.COL_MAJOR, L.MEM_DEVICE, A
+            A = A.contiguous()
+            return A.data_ptr(), A.shape[1], L.ROW_MAJOR, L.MEM_DEVICE, A
+    A = np.asarray(A)
+    if A.ndim != 2:
+        raise ValueError("dense input must be 2-D")
+    if A.dtype != np.float32:
+        A = A.astype(np.float32)
+    if A.flags.f_contiguous and not A.flags.c_contiguous:
+        return A.ctypes.data, max(A.shape[0], 1), L.COL_MAJOR, L.MEM_HOST, A
+    A = np.ascontiguousarray(A)
+    return A.ctypes.data, max(A.shape[1], 1), L.ROW_MAJOR, L.MEM_HOST, A
+
+
+def _csr_arg(A):
+    """(rowptr, col, val, nrows, ncols, mem, keepalive) for a CSR input."""
+    if isinstance(A, tuple):
+        rowptr, col, val = A[:3]
+        if _is_torch(rowptr) and rowptr.is_cuda:
+            import torch
+
+            assert rowptr.dtype == torch.int64 and col.dtype == torch.int32 and val.dtype == torch.float32
+            return rowptr.data_ptr(), col.data_ptr(), val.data_ptr(), rowptr.numel() - 1, None, L.MEM_DEVICE, A
+        rowptr = np.ascontiguousarray(rowptr, dtype=np.int64)
+        col = np.ascontiguousarray(col, dtype=np.int32)
+        val = np.ascontiguousarray(val, dtype=np.float32)
+        keep = (rowptr, col, val)
+        return rowptr.ctypes.data, col.ctypes.data, val.ctypes.data, len(rowptr) - 1, None, L.MEM_HOST, keep
+    # scipy.sparse
+    A = A.tocsr()
+    rowptr = np.ascontiguousarray(A.indptr, dtype=np.int64)
+    col = np.ascontiguousarray(A.indices, dtype=np.int32)
+    val = np.ascontiguousarray(A.data, dtype=np.float32)
+    keep = (rowptr, col, val)
+    return rowptr.ctypes.data, col.ctypes.data, val.ctypes.data, A.shape[0], A.shape[1], L.MEM_HOST, keep
+
+
+class _Context:
+    def __init__(self, alg: AlgParams, dim_redux=None):
+        if dim_redux is not None:
+            alg.dim_redux = dim_redux.kind
+        self.alg = alg
+        self.lib = L.load()
+        p = alg.to_c()
+        h = C.c_void_p()
+        st = self.lib.skema_create(C.byref(p), C.byref(h))
+        if st != L.OK:
+            msg = self.lib.skema_last_error(None)
+            raise SkemaError(st, msg.decode() if msg else "")
+        self.h = h
+        k, s, spd = C.c_int64(), C.c_int64(), C.c_int32()
+        self._check(self.lib.skema_get_dims(self.h, C.byref(k), C.byref(s), C.byref(spd)))
+        self.range, self.core, self.spd = k.value, s.value, bool(spd.value)
+        self.nrow, self.ncol, self.rank = alg.matrix_m, alg.matrix_n, alg.rank
+
+    def _check(self, st):
+        if st != L.OK:
+            msg = self.lib.skema_last_error(self.h)
+            raise SkemaError(st, msg.decode() if msg else "")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.skema_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # -- streaming --------------------------------------------------------
+    def reset(self):
+        self._check(self.lib.skema_reset(self.h))
+
+    def update_rows(self, A, row0: int = 0, nrows: int | None = None):
+        """Stream rows [row0, row0+nrows) (default: all rows of A)."""
+        if self.alg.kernel_func == L.KERNEL_GAUSSRBF:
+            ptr, ld, layout, mem, keep = _dense_arg(A)
+            npts, d = A.shape
+            nr = self.nrow - row0 if nrows is None else nrows
+            self._check(self.lib.skema_linear_update_rbf(self.h, ptr, ld, layout, npts, d, row0, nr, mem))
+        elif self.alg.issparse:
+            rp, col, val, nr_in, _, mem, keep = _csr_arg(A)
+            nr = nr_in if nrows is None else nrows
+            self._check(self.lib.skema_linear_update_csr(self.h, rp, col, val, row0, nr, mem))
+        else:
+            ptr, ld, layout, mem, keep = _dense_arg(A)
+            nr = A.shape[0] if nrows is None else nrows
+            self._check(self.lib.skema_linear_update_dense(self.h, ptr, ld, layout, row0, nr, mem))
+        if mem == L.MEM_HOST:
+            self.synchronize()
+        del keep
+
+    def linear_update(self, A):
+        """SketchySVD::linear_update: zero the sketches, then stream all rows."""
+        self.reset()
+        self.update_rows(A, 0, None)
+
+    def synchronize(self):
+        self._check(self.lib.skema_synchronize(self.h))
+
+    def launch_count(self) -> int:
+        return int(self.lib.skema_launch_count(self.h))
+
+    def timing_enable(self, on: bool = True):
+        self._check(self.lib.skema_timing_enable(self.h, 1 if on else 0))
+
+    def timing_get(self, stage: str):
+        """(milliseconds, launches) accumulated for one stage."""
+        ms, n = C.c_double(), C.c_int64()
+        self._check(self.lib.skema_timing_get(self.h, stage.encode(), C.byref(ms), C.byref(n)))
+        return ms.value, n.value
+
+    def set_stream(self, stream_handle: int | None):
+        """Launch on an external cudaStream_t (e.g. torch's current stream)."""
+        self._check(self.lib.skema_set_stream(self.h, stream_handle))
+
+    # -- sketches ---------------------------------------------------------
+    def _sketch_shape(self, which):
+        return {L.SKETCH_X: (self.range, self.ncol), L.SKETCH_Y: (self.nrow, self.range),
+                L.SKETCH_Z: (self.core, self.core)}[which]
+
+    def get_sketch(self, which, out=None):
+        shape = self._sketch_shape(which)
+        if out is None:
+            out = np.empty(shape, dtype=np.float32)
+        if _is_torch(out):
+            self._check(self.lib.skema_get_sketch(self.h, which, out.data_ptr(), shape[1], L.ROW_MAJOR, L.MEM_DEVICE))
+        else:
+            self._check(self.lib.skema_get_sketch(self.h, which, out.ctypes.data, shape[1], L.ROW_MAJOR, L.MEM_HOST))
+        return out
+
+    def set_sketch(self, which, buf):
+        shape = self._sketch_shape(which)
+        if _is_torch(buf):
+            self._check(self.lib.skema_set_sketch(self.h, which, buf.data_ptr(), shape[1], L.ROW_MAJOR, L.MEM_DEVICE))
+        else:
+            b = np.ascontiguousarray(buf, dtype=np.float32)
+            assert b.shape == shape
+            self._check(self.lib.skema_set_sketch(self.h, which, b.ctypes.data, shape[1], L.ROW_MAJOR, L.MEM_HOST))
+
+    # -- maps -------------------------------------------------------------
+    def map_info(self, which):
+        nr, nc, z, t = C.c_int64(), C.c_int64(), C.c_int32(), C.c_int32()
+        self._check(self.lib.skema_map_info(self.h, which, C.byref(nr), C.byref(nc), C.byref(z), C.byref(t)))
+        return nr.value, nc.value, z.value, bool(t.value)
+
+    def map_export(self, which):
+        """Gauss: (nrow x ncol float64 array, None); SparseSign: (values, indices)
+        with zeta entries per stored row."""
+        nr, nc, z, _ = self.map_info(which)
+        if z == 0:
+            vals = np.empty((nc, nr), dtype=np.float64)  # column-major storage
+            self._check(self.lib.skema_map_export(self.h, which, vals.ctypes.data, None))
+            return vals.T, None
+        vals = np.empty((nr, z), dtype=np.float64)
+        idx = np.empty((nr, z), dtype=np.int32)
+        self._check(self.lib.skema_map_export(self.h, which, vals.ctypes.data, idx.ctypes.data))
+        return vals, idx
+
+    def map_import(self, which, values, indices=None):
+        nr, nc, z, _ = self.map_info(which)
+        if z == 0:
+            v = np.asfortranarray(np.asarray(values, dtype=np.float64))
+            assert v.shape == (nr, nc)
+            self._check(self.lib.skema_map_import(self.h, which, v.ctypes.data, None))
+        else:
+            v = np.ascontiguousarray(values, dtype=np.float64).reshape(nr, z)
+            ix = np.ascontiguousarray(indices, dtype=np.int32).reshape(nr, z)
+            self._check(self.lib.skema_map_import(self.h, which, v.ctypes.data, ix.ctypes.data))
+
+
+class SketchySVD(_Context):
+    """SketchySVD<MatrixType, DimReduxT> (src/Skema_SketchySVD.hpp:11-64)."""
+
+    def get_sketches(self):
+        return (self.get_sketch(L.SKETCH_X), self.get_sketch(L.SKETCH_Y), self.get_sketch(L.SKETCH_Z))
+
+    def low_rank_approx(self, device_out=None):
+        """(U m x r, S r, V n x r), FP64. device_out: optional (U, S, V) CUDA
+        float64 tensors (column-major U, V) to fill in place."""
+        r = self.rank
+        if device_out is not None:
+            U, S, V = device_out
+            self._check(self.lib.skema_low_rank_approx(self.h, U.data_ptr(), S.data_ptr(), V.data_ptr(), L.MEM_DEVICE))
+            return U, S, V
+        U = np.empty((r, self.nrow), dtype=np.float64)
+        V = np.empty((r, self.ncol), dtype=np.float64)
+        S = np.empty(r, dtype=np.float64)
+        self._check(self.lib.skema_low_rank_approx(self.h, U.ctypes.data, S.ctypes.data, V.ctypes.data, L.MEM_HOST))
+        return U.T, S, V.T
+
+
+class SketchySPD(_Context):
+    """SketchySPD<MatrixType, DimReduxT> update (src/Skema_SketchySVD.hpp:67-108)."""
+
+    def get_sketches(self):
+        return self.get_sketch(L.SKETCH_Y)
+
+
+def sketchysvd(matrix, alg: AlgParams):
+    """Skema::sketchysvd (src/Skema_SketchySVD.cpp:1244-1405, 1408-1577),
+    three-sketch branch: returns (U, S, V)."""
+    with SketchySVD(alg) as sk:
+        if alg.kernel_func == L.KERNEL_GAUSSRBF:
+            sk.linear_update(matrix)
+        else:
+            sk.linear_update(matrix)
+        return sk.low_rank_approx()
+
+
+def _ctx_for_standalone(device: int = 0) -> _Context:
+    alg = AlgParams(matrix_m=1, matrix_n=1, rank=1, device=device)
+    return _Context(alg)
+
+
+def rbf_sketch_fwd(pts, gamma: float, omega, ctx: _Context | None = None):
+    """Y = K Omega^T for device tensors pts (N x d), omega (k x N)."""
+    import torch
+
+    own = ctx is None
+    ctx = ctx or _ctx_for_standalone(pts.device.index or 0)
+    try:
+        pts = pts.contiguous()
+        omega = omega.contiguous()
+        N, d = pts.shape
+        k = omega.shape[0]
+        Y = torch.empty((N, k), dtype=torch.float32, device=pts.device)
+        ctx._check(ctx.lib.skema_rbf_sketch_fwd(ctx.h, pts.data_ptr(), N, d, float(gamma), omega.data_ptr(), k, Y.data_ptr()))
+        ctx.synchronize()
+        return Y
+    finally:
+        if own:
+            ctx.close()
+
+
+def rbf_sketch_vjp(pts, gamma: float, omega, Ybar, ctx: _Context | None = None):
+    """(dL/dpts, dL/dgamma) of Y = K Omega^T given Ybar = dL/dY."""
+    import torch
+
+    own = ctx is None
+    ctx = ctx or _ctx_for_standalone(pts.device.index or 0)
+    try:
+        pts = pts.contiguous()
+        omega = omega.contiguous()
+        Ybar = Ybar.contiguous()
+        N, d = pts.shape
+        k = omega.shape[0]
+        dX = torch.empty_like(pts)
+        dg = torch.zeros(1, dtype=torch.float64, device=pts.device)
+        ctx._check(ctx.lib.skema_rbf_sketch_vjp(ctx.h, pts.data_ptr(), N, d, float(gamma), omega.data_ptr(), k,
+                                                Ybar.data_ptr(), dX.data_ptr(), dg.data_ptr()))
+        ctx.synchronize()
+        return dX, float(dg.item())
+    finally:
+        if own:
+            ctx.close()
