@@ -1,0 +1,519 @@
+"""Benchmark of the SketchySVD sketch update on B200 (one JSON line).
+
+Default workload (sparse-sign CSR): A is CSR 1,000,000 x 100,000 FP32 with
+~10 nonzeros per row at uniform random columns (duplicates merged), values
+N(0,1) plus a planted rank-20 component of scale 5 sampled on the pattern;
+SparseSign maps (zeta = 8), r = 20, k = 81, s = 163, windows of 10,000 rows.
+One step = skema_reset + the linear update over all rows (all windows), the
+inputs resident in HBM. Synthetic data, seeded.
+
+Other workloads (--workload): dense-fp32 / dense-bf16 / dense-fp8 (A
+200,000 x 20,000 FP32, r = 50, k = 201, s = 403, windows of 8,192 rows).
+
+Multi-GPU (torchrun, one rank per GPU): weak scaling by contiguous row
+blocks; each rank sketches its own block of the global matrix and the
+partial X and Z sketches are summed with an NCCL all-reduce (Y rows are
+disjoint and stay on their rank).
+
+--impl reference times the CPU oracle (the FP64 restatement of the
+reference's algorithm) on the host cores on a bounded sample per step.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
+TRAFFIC_PATH = os.path.join(ROOT, "profiles", "traffic.json")
+FALLBACK_PEAKS = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}
+
+WORKLOADS = {
+    "csr-sparse-sign": dict(m=1_000_000, n=100_000, nnz_row=10, planted=20, scale=5.0, rank=20,
+                            k=81, s=163, window=10_000, seed=2, kind=1),
+    "dense-fp32": dict(m=200_000, n=20_000, rank=50, k=201, s=403, window=8192, seed=3, kind=0, prec=0),
+    "dense-bf16": dict(m=200_000, n=20_000, rank=50, k=201, s=403, window=8192, seed=3, kind=0, prec=1),
+    "dense-fp8": dict(m=200_000, n=20_000, rank=50, k=201, s=403, window=8192, seed=3, kind=0, prec=2),
+}
+
+
+def load_peaks():
+    try:
+        with open(PEAKS_PATH) as f:
+            p = json.load(f)
+        return p, "measured"
+    except Exception:
+        return dict(FALLBACK_PEAKS), "fallback"
+
+
+# ------------------------------------------------------------- clocks ------
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.out = None
+
+    def __enter__(self):
+        try:
+            self.out = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=self.out, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.proc or not self.out:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        self.out.flush()
+        rows = []
+        with open(self.out.name) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.out.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------- synthetic ------
+def make_csr_torch(cfg, m_local, seed, device):
+    """Seeded CSR block on the device (torch RNG)."""
+    import torch
+
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    n, nr = cfg["n"], cfg["nnz_row"]
+    cols = torch.randint(0, n, (m_local, nr), generator=g, device=device)
+    cols, _ = cols.sort(dim=1)
+    keep = torch.ones_like(cols, dtype=torch.bool)
+    keep[:, 1:] = cols[:, 1:] != cols[:, :-1]
+    counts = keep.sum(1)
+    rowptr = torch.zeros(m_local + 1, dtype=torch.int64, device=device)
+    rowptr[1:] = torch.cumsum(counts, 0)
+    col = cols[keep].to(torch.int32)
+    rows = torch.repeat_interleave(torch.arange(m_local, device=device), counts)
+    p = cfg["planted"]
+    U = torch.randn(m_local, p, generator=g, device=device)
+    V = torch.randn(n, p, generator=g, device=device)
+    val = torch.randn(col.numel(), generator=g, device=device)
+    val += cfg["scale"] * (U[rows] * V[col.long()]).sum(1) / (p ** 0.5)
+    del U, V, rows, cols, keep, counts
+    return rowptr, col, val.float()
+
+
+def make_csr_numpy(cfg, m_local, seed):
+    rng = np.random.default_rng(seed)
+    n, nr = cfg["n"], cfg["nnz_row"]
+    cols = rng.integers(0, n, size=(m_local, nr))
+    cols.sort(axis=1)
+    keep = np.ones_like(cols, bool)
+    keep[:, 1:] = cols[:, 1:] != cols[:, :-1]
+    counts = keep.sum(1)
+    rowptr = np.zeros(m_local + 1, np.int64)
+    rowptr[1:] = np.cumsum(counts)
+    col = cols[keep].astype(np.int32)
+    p = cfg["planted"]
+    U = rng.standard_normal((m_local, p), dtype=np.float32)
+    V = rng.standard_normal((n, p), dtype=np.float32)
+    rows = np.repeat(np.arange(m_local), counts)
+    val = rng.standard_normal(col.size, dtype=np.float32) + cfg["scale"] * (U[rows] * V[col]).sum(1) / np.sqrt(p)
+    return rowptr, col, val.astype(np.float32)
+
+
+def make_dense_torch(cfg, m_local, seed, device):
+    """A = U_p diag(s) V_p^T + 1e-3 N(0,1), s_i = i^-1.5, p = 256 (FP32, column-major)."""
+    import torch
+
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    m, n, p = m_local, cfg["n"], 256
+    Ug = torch.randn(m, p, generator=g, device=device, dtype=torch.float64)
+    Vg = torch.randn(n, p, generator=g, device=device, dtype=torch.float64)
+    Uq = torch.linalg.qr(Ug)[0]
+    Vq = torch.linalg.qr(Vg)[0]
+    s = torch.arange(1, p + 1, device=device, dtype=torch.float64) ** -1.5
+    Af = torch.empty((n, m), dtype=torch.float32, device=device)  # A^T row-major = A column-major
+    blk = 2048
+    for j0 in range(0, n, blk):
+        j1 = min(n, j0 + blk)
+        Af[j0:j1] = ((Vq[j0:j1] * s) @ Uq.T).float()
+    del Ug, Vg, Uq, Vq
+    Af += 1e-3 * torch.randn(Af.shape, generator=g, device=device)
+    return Af.t()  # m x n view, column-major
+
+
+# ------------------------------------------------------------ our arm ------
+def run_gpu(args, cfg, peaks, peak_kind):
+    import torch
+    import torch.distributed as dist
+
+    import skema_b200 as sk
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    m_local = cfg["m"]
+    m_glob = m_local * world
+    a = sk.AlgParams(matrix_m=m_glob, matrix_n=cfg["n"], rank=cfg["rank"], sketch_range=cfg["k"],
+                     sketch_core=cfg["s"], window=cfg["window"], dim_redux=cfg["kind"], device=local)
+    sparse = args.workload.startswith("csr")
+    a.issparse = sparse
+    a.precision = cfg.get("prec", 0)
+    ctx = sk.SketchySVD(a)
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+    row0 = rank * m_local
+    if sparse:
+        rowptr, col, val = make_csr_torch(cfg, m_local, cfg["seed"] + rank, dev)
+        nnz = col.numel()
+        inp = (rowptr, col, val)
+    else:
+        A = make_dense_torch(cfg, m_local, cfg["seed"] + rank, dev)
+        nnz = m_local * cfg["n"]
+        inp = A
+    torch.cuda.synchronize()
+    k, s, n = cfg["k"], cfg["s"], cfg["n"]
+    Xbuf = torch.empty((k, n), dtype=torch.float32, device=dev) if world > 1 else None
+    Zbuf = torch.empty((s, s), dtype=torch.float32, device=dev) if world > 1 else None
+
+    def step():
+        ctx.reset()
+        ctx.update_rows(inp, row0, m_local)
+        if world > 1:
+            ctx.get_sketch(0, Xbuf)
+            ctx.get_sketch(2, Zbuf)
+            dist.all_reduce(Xbuf)
+            dist.all_reduce(Zbuf)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ctx.timing_enable(True)
+    l0 = ctx.launch_count()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    launches = ctx.launch_count() - l0
+    ms = e0.elapsed_time(e1) / args.steps
+    if sparse:
+        kstage = "update.omega"
+    else:
+        kstage = "update.fused" if a.precision else "update.omega"
+    kms, kcount = ctx.timing_get(kstage)
+    ctx.timing_enable(False)
+    ms_t = torch.tensor([ms], device=dev)
+    if world > 1:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms = float(ms_t.item())
+    rows_total = m_glob
+    value = rows_total / (ms / 1e3)
+
+    # dominant kernel roofline
+    if sparse:
+        zeta = 8
+        alg_bytes = (m_local + 1) * 8 + nnz * 8 + m_local * k * 4 + n * zeta * 4
+        achieved = alg_bytes / (kms / kcount / 1e3) / 1e9
+        roof = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": achieved / peaks["hbm_gbs"], "peak_source": peak_kind,
+                "kernel": "csr_ssign_y_kernel", "kernel_ms": kms / kcount,
+                "algorithmic_bytes": alg_bytes}
+    else:
+        flops = m_local * (2 * n * (2 * k + s) + 2 * s * s)
+        dms = kms / max(kcount, 1)
+        roof = {"bound": "tensor", "achieved": flops / (ms / 1e3) / 1e12,
+                "peak": peaks.get("bf16_tflops_sustained", 1400.0), "unit": "TFLOP/s",
+                "frac": flops / (ms / 1e3) / 1e12 / peaks.get("bf16_tflops_sustained", 1400.0),
+                "peak_source": peak_kind, "kernel": kstage, "kernel_ms": dms, "algorithmic_flops": flops}
+    traffic = None
+    try:
+        with open(TRAFFIC_PATH) as f:
+            traffic = json.load(f).get(args.workload)
+    except Exception:
+        pass
+    roof["traffic"] = traffic
+
+    # end to end through the public API with pinned host buffers
+    e2e = None
+    if rank == 0 and sparse and not args.no_e2e:
+        e2e = e2e_sparse(ctx, inp, m_local, row0, k, s, n, args)
+    if rank == 0 and not sparse and not args.no_e2e:
+        e2e = e2e_dense(ctx, inp, m_local, row0, k, s, n, args)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(args, cfg, budget_s=args.cpu_budget)
+
+    out = {
+        "metric": "sketched rows/s",
+        "value": value,
+        "unit": "rows/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": {0: "fp32", 1: "bf16", 2: "fp8"}[a.precision] if not sparse else "fp32",
+        "data": "synthetic (seeded; no dataset)",
+        "config": config_of(args, cfg, world, nnz),
+        "roofline": roof,
+        "cpu_baseline": cpu,
+        "e2e": e2e,
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+    }
+    ctx.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+def config_of(args, cfg, world, nnz):
+    c = {"workload": args.workload, "m_per_gpu": cfg["m"], "n": cfg["n"], "rank": cfg["rank"],
+         "range_k": cfg["k"], "core_s": cfg["s"], "window": cfg["window"],
+         "maps": "sparse-sign zeta=8" if cfg["kind"] == 1 else "gauss",
+         "parallelism": f"row-blocks x{world}" + (" + NCCL all-reduce of X,Z" if world > 1 else "")}
+    if args.workload.startswith("csr"):
+        c["nnz_per_gpu"] = int(nnz)
+        c["l2"] = "working set ~450 MB per step > 126 MB L2 (no flush needed)"
+    else:
+        c["l2"] = "A is 16 GB per step > 126 MB L2 (no flush needed)"
+    return c
+
+
+def e2e_sparse(ctx, inp, m_local, row0, k, s, n, args):
+    import torch
+
+    import skema_b200._lib as L
+
+    rowptr, col, val = inp
+    h_rp = rowptr.cpu().pin_memory()
+    h_col = col.cpu().pin_memory()
+    h_val = val.cpu().pin_memory()
+    hX = torch.empty((k, n), dtype=torch.float32).pin_memory()
+    hY = torch.empty((ctx.nrow, k), dtype=torch.float32).pin_memory()
+    hZ = torch.empty((s, s), dtype=torch.float32).pin_memory()
+    lib, h = ctx.lib, ctx.h
+
+    def one():
+        ctx._check(lib.skema_reset(h))
+        ctx._check(lib.skema_linear_update_csr(h, h_rp.data_ptr(), h_col.data_ptr(), h_val.data_ptr(), row0,
+                                               m_local, L.MEM_HOST))
+        ctx._check(lib.skema_get_sketch(h, 0, hX.data_ptr(), n, L.ROW_MAJOR, L.MEM_HOST))
+        ctx._check(lib.skema_get_sketch(h, 1, hY.data_ptr(), k, L.ROW_MAJOR, L.MEM_HOST))
+        ctx._check(lib.skema_get_sketch(h, 2, hZ.data_ptr(), s, L.ROW_MAJOR, L.MEM_HOST))
+
+    for _ in range(2):
+        one()
+    steps = max(3, min(args.steps, 10))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        one()
+    torch.cuda.synchronize()
+    dt = (time.perf_counter() - t0) / steps
+    h2d = h_rp.numel() * 8 + h_col.numel() * 4 + h_val.numel() * 4
+    d2h = (k * n + ctx.nrow * k + s * s) * 4
+    return {"value": m_local / dt, "unit": "rows/s", "h2d_bytes_per_step": int(h2d),
+            "d2h_bytes_per_step": int(d2h), "ms_per_step": dt * 1e3,
+            "path": "skema_linear_update_csr(mem=HOST) + skema_get_sketch(X,Y,Z, mem=HOST), pinned buffers",
+            "timer": "host wall clock around synchronous calls"}
+
+
+def e2e_dense(ctx, A, m_local, row0, k, s, n, args):
+    import torch
+
+    import skema_b200._lib as L
+
+    hA = A.t().contiguous().cpu().pin_memory()  # A^T row-major == A column-major (ld = m)
+    hX = torch.empty((k, n), dtype=torch.float32).pin_memory()
+    hY = torch.empty((ctx.nrow, k), dtype=torch.float32).pin_memory()
+    hZ = torch.empty((s, s), dtype=torch.float32).pin_memory()
+    lib, h = ctx.lib, ctx.h
+
+    def one():
+        ctx._check(lib.skema_reset(h))
+        ctx._check(lib.skema_linear_update_dense(h, hA.data_ptr(), m_local, L.COL_MAJOR, row0, m_local,
+                                                 L.MEM_HOST))
+        ctx._check(lib.skema_get_sketch(h, 0, hX.data_ptr(), n, L.ROW_MAJOR, L.MEM_HOST))
+        ctx._check(lib.skema_get_sketch(h, 1, hY.data_ptr(), k, L.ROW_MAJOR, L.MEM_HOST))
+        ctx._check(lib.skema_get_sketch(h, 2, hZ.data_ptr(), s, L.ROW_MAJOR, L.MEM_HOST))
+
+    one()
+    steps = 2
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        one()
+    torch.cuda.synchronize()
+    dt = (time.perf_counter() - t0) / steps
+    return {"value": m_local / dt, "unit": "rows/s", "h2d_bytes_per_step": int(m_local * n * 4),
+            "d2h_bytes_per_step": int((k * n + ctx.nrow * k + s * s) * 4), "ms_per_step": dt * 1e3,
+            "path": "skema_linear_update_dense(mem=HOST) + skema_get_sketch(X,Y,Z, mem=HOST), pinned buffers",
+            "timer": "host wall clock around synchronous calls"}
+
+
+# ------------------------------------------------------- CPU baseline ------
+def cpu_sample_sparse(cfg, budget_s, seed_rows=None):
+    """Oracle (FP64 CRS x SparseSign restatement, OpenMP) on windows of the
+    workload until budget_s elapses; returns (rows/s, rows, threads)."""
+    import scipy.sparse as sp
+
+    from oracle import sketchy_oracle as O
+
+    m, n, w = cfg["m"], cfg["n"], cfg["window"]
+    rows_max = seed_rows or m
+    rowptr, col, val = make_csr_numpy(cfg, rows_max, cfg["seed"])
+    A = sp.csr_matrix((val.astype(np.float64), col, rowptr), shape=(rows_max, n))
+    o = O.OracleSketch(m, n, cfg["rank"], w, kind=1, issparse=True, sketch_range=cfg["k"], sketch_core=cfg["s"])
+    t0 = time.perf_counter()
+    done = 0
+    while done < rows_max and time.perf_counter() - t0 < budget_s:
+        wr = min(w, rows_max - done)
+        o.update_rows(A, done, wr)
+        done += wr
+    dt = time.perf_counter() - t0
+    return done / dt, done, O.num_threads()
+
+
+def cpu_sample_dense(cfg, budget_s):
+    from oracle import sketchy_oracle as O
+
+    m, n, w = cfg["m"], cfg["n"], cfg["window"]
+    rng = np.random.default_rng(cfg["seed"])
+    A = rng.standard_normal((w, n))  # one window of the same shape, FP64
+    o = O.OracleSketch(m, n, cfg["rank"], w, kind=0, sketch_range=cfg["k"], sketch_core=cfg["s"])
+    t0 = time.perf_counter()
+    done = 0
+    while done == 0 or (done < 4 * w and time.perf_counter() - t0 < budget_s):
+        O.update_dense(o.maps, A, done % (m - w))  # x, y, z of one window
+        done += w
+    dt = time.perf_counter() - t0
+    return done / dt, done, O.num_threads()
+
+
+def cpu_baseline(args, cfg, budget_s):
+    if args.workload.startswith("csr"):
+        v, rows, thr = cpu_sample_sparse(cfg, budget_s)
+        sample = f"first {rows} rows ({rows // cfg['window']} windows) of the workload, FP64"
+    else:
+        v, rows, thr = cpu_sample_dense(cfg, budget_s)
+        sample = f"{rows} rows (whole windows of {cfg['window']}) of a same-shape FP64 matrix"
+    return {"value": v, "unit": "rows/s", "cores": thr, "kind": "port", "sample": sample,
+            "host_cpu": _cpu_model(), "nproc": os.cpu_count()}
+
+
+def _cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except Exception:
+        pass
+    return None
+
+
+def run_reference(args, cfg):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if rank != 0:
+        return
+    per_step = []
+    budget = max(1.0, min(10.0, 150.0 / max(1, args.steps + args.warmup)))
+    rows = 0
+    thr = 1
+    for i in range(args.warmup + args.steps):
+        if args.workload.startswith("csr"):
+            v, r, thr = cpu_sample_sparse(cfg, budget, seed_rows=min(cfg["m"], 200_000))
+        else:
+            v, r, thr = cpu_sample_dense(cfg, budget)
+        if i >= args.warmup:
+            per_step.append(v)
+            rows = r
+    v = statistics.median(per_step)
+    out = {
+        "metric": "sketched rows/s", "value": v, "unit": "rows/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": rows / v * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded; no dataset)",
+        "config": config_of(args, cfg, 1, 0), "impl": "reference",
+        "cpu_baseline": {"value": v, "unit": "rows/s", "cores": thr, "kind": "port",
+                         "sample": f"{rows} rows per step (bounded sample), FP64 oracle restatement",
+                         "host_cpu": _cpu_model(), "nproc": os.cpu_count()},
+        "e2e": {"value": v, "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="csr-sparse-sign", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-budget", type=float, default=12.0)
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    cfg = dict(WORKLOADS[args.workload])
+    if args.impl == "reference":
+        run_reference(args, cfg)
+        return
+    peaks, kind = load_peaks()
+    run_gpu(args, cfg, peaks, kind)
+
+
+if __name__ == "__main__":
+    main()

@@ -121,12 +121,19 @@ class Map:
         self.kind, self.nrow, self.ncol, self.seed = kind, nrow, ncol, seed
         self.transposed = transposed      # logical = stored^T
         self.init_transposed = ref_flag   # the reference ctor's flag
+        self._dense = None
         if kind == 0:
-            self.dense = gauss_map(seed, nrow, ncol)
+            self._dense = gauss_map(seed, nrow, ncol)
             self.idx = self.val = None
         else:
             self.idx, self.val = sparse_sign_map(seed, nrow, ncol)
-            self.dense = sparse_to_dense(self.idx, self.val, ncol)
+
+    @property
+    def dense(self) -> np.ndarray:
+        """Stored map as a dense FP64 matrix (built on first use)."""
+        if self._dense is None:
+            self._dense = sparse_to_dense(self.idx, self.val, self.ncol)
+        return self._dense
 
     @property
     def logical(self) -> np.ndarray:

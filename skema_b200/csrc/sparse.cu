@@ -40,7 +40,8 @@ template <bool Z8>
 __global__ void __launch_bounds__(256)
     csr_ssign_y_kernel(const int64_t* __restrict__ rowptr, const int32_t* __restrict__ col,
                        const float* __restrict__ val, int64_t col_offset, int64_t nrows,
-                       const uint32_t* __restrict__ omg, int zeta, int k, float* __restrict__ Y,
+                       const uint32_t* __restrict__ omg, int zeta, int k, int ncol,
+                       float* __restrict__ Y,
                        float alpha, float beta, int R) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -67,6 +68,7 @@ __global__ void __launch_bounds__(256)
         const int64_t e = base + u * 32 + lane;
         const bool ok = e < E;
         jj[u] = ok ? __ldcs(col + e) : -1;
+        if ((unsigned)jj[u] >= (unsigned)ncol) jj[u] = -1;  // columns outside [0, n) are ignored
         vv[u] = ok ? __ldcs(val + e) : 0.f;
         // largest l with srp[l] <= e (srp[rr] = E > e)
         int lo = 0, hi = rr;
@@ -153,12 +155,14 @@ __global__ void csr_ssign_entries_kernel(
     if (rsw >> 31) wgt = -wgt;
     const int64_t b = rowptr[li] - col_offset, en = rowptr[li + 1] - col_offset;
     if (is_u) {
-      for (int64_t q = b + lane; q < en; q += 32) atomicAdd(X + r * n + col[q], wgt * val[q]);
+      for (int64_t q = b + lane; q < en; q += 32)
+        if ((uint64_t)col[q] < (uint64_t)n) atomicAdd(X + r * n + col[q], wgt * val[q]);
     } else {
       const int64_t pairs = (en - b) * zeta_s;
       for (int64_t q = lane; q < pairs; q += 32) {
         const int64_t p = b + q / zeta_s;
         const int t = (int)(q % zeta_s);
+        if ((uint64_t)col[p] >= (uint64_t)n) continue;
         const uint32_t w = psi[(int64_t)col[p] * zeta_s + t];
         const float v = wgt * val[p];
         atomicAdd(Z + r * s + (w & 0x7fffffffu), (w >> 31) ? -v : v);
@@ -173,7 +177,7 @@ __global__ void csr_ssign_entries_kernel(
 // ---------------------------------------------------------------------------
 __global__ void csr_gauss_y_kernel(const int64_t* __restrict__ rowptr,
                                    const int32_t* __restrict__ col, const float* __restrict__ val,
-                                   int64_t col_offset, int64_t nrows,
+                                   int64_t col_offset, int64_t nrows, int64_t ncol,
                                    const float* __restrict__ mapT /* n x k rows */, int64_t k,
                                    float* __restrict__ Y, float alpha, float beta) {
   const int lane = threadIdx.x & 31;
@@ -185,6 +189,7 @@ __global__ void csr_gauss_y_kernel(const int64_t* __restrict__ rowptr,
       float a[4] = {0.f, 0.f, 0.f, 0.f};
       for (int64_t p = b; p < e; ++p) {
         const float v = val[p];
+        if ((uint64_t)col[p] >= (uint64_t)ncol) continue;
         const float* mrow = mapT + (int64_t)col[p] * k;
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
@@ -209,7 +214,7 @@ __global__ void csr_gauss_y_kernel(const int64_t* __restrict__ rowptr,
 __global__ void csr_gauss_scatter_kernel(const int64_t* __restrict__ rowptr,
                                          const int32_t* __restrict__ col,
                                          const float* __restrict__ val, int64_t col_offset,
-                                         int64_t nrows, const float* __restrict__ maprows,
+                                         int64_t nrows, int64_t ncol, const float* __restrict__ maprows,
                                          int64_t kk, float* __restrict__ out, int64_t ors,
                                          int64_t ocs, float alpha) {
   const int lane = threadIdx.x & 31;
@@ -221,6 +226,7 @@ __global__ void csr_gauss_scatter_kernel(const int64_t* __restrict__ rowptr,
     for (int64_t p = b; p < e; ++p) {
       const float v = alpha * val[p];
       const int64_t j = col[p];
+      if ((uint64_t)j >= (uint64_t)ncol) continue;
       for (int64_t r = lane; r < kk; r += 32) atomicAdd(out + r * ors + j * ocs, v * mrow[r]);
     }
   }
@@ -366,10 +372,10 @@ void launch_csr_ssign_y(skema_ctx* c, const int64_t* rowptr, const int32_t* col,
   const int grid = grid_cap(c, blocks_want, std::max(1, per_sm));
   if (O.zeta == 8)
     csr_ssign_y_kernel<true><<<grid, 32 * nw, smem, c->stream>>>(
-        rowptr, col, val, col_offset, nrows, O.packed, 8, k, Yrows, alpha, beta, R);
+        rowptr, col, val, col_offset, nrows, O.packed, 8, k, (int)c->n, Yrows, alpha, beta, R);
   else
     csr_ssign_y_kernel<false><<<grid, 32 * nw, smem, c->stream>>>(
-        rowptr, col, val, col_offset, nrows, O.packed, O.zeta, k, Yrows, alpha, beta, R);
+        rowptr, col, val, col_offset, nrows, O.packed, O.zeta, k, (int)c->n, Yrows, alpha, beta, R);
   SKEMA_LAUNCHED(c);
 }
 
@@ -422,21 +428,21 @@ void csr_update(skema_ctx* c, const int64_t* rowptr, const int32_t* col, const f
     const int64_t R0 = row0 + r;
     const float yb = y_rows_clean(c, R0, R0 + wr) ? 0.f : nu;
     csr_gauss_y_kernel<<<grid_cap(c, (wr + 7) / 8, 16), threads, 0, c->stream>>>(
-        rowptr + r, col, val, col_offset, wr, c->omg.f32, c->k, c->Y + R0 * c->k, eta, yb);
+        rowptr + r, col, val, col_offset, wr, c->n, c->omg.f32, c->k, c->Y + R0 * c->k, eta, yb);
     SKEMA_LAUNCHED(c);
     y_rows_mark(c, R0, R0 + wr);
     if (c->spd) continue;
     // X = nu X + eta (A_w^T Upsilon_stored(R0:R0+wr, :))^T
     scale_block(c, MatOut{c->X, c->n, 1}, c->k, c->n, nu);
     csr_gauss_scatter_kernel<<<grid_cap(c, (wr + 7) / 8, 16), threads, 0, c->stream>>>(
-        rowptr + r, col, val, col_offset, wr, c->ups.f32 + R0 * c->k, c->k, c->X, c->n, 1, eta);
+        rowptr + r, col, val, col_offset, wr, c->n, c->ups.f32 + R0 * c->k, c->k, c->X, c->n, 1, eta);
     SKEMA_LAUNCHED(c);
     // W^T = A_w^T Phi_stored(R0:R0+wr, :) in scratch (n x s), then
     // Z = nu Z + eta W Psi_stored.
     float* Wt = (float*)workspace(c, sizeof(float) * (size_t)(c->n * c->s));
     SKEMA_CUDA(cudaMemsetAsync(Wt, 0, sizeof(float) * (size_t)(c->n * c->s), c->stream));
     csr_gauss_scatter_kernel<<<grid_cap(c, (wr + 7) / 8, 16), threads, 0, c->stream>>>(
-        rowptr + r, col, val, col_offset, wr, c->phi.f32 + R0 * c->s, c->s, Wt, 1, c->s, 1.f);
+        rowptr + r, col, val, col_offset, wr, c->n, c->phi.f32 + R0 * c->s, c->s, Wt, 1, c->s, 1.f);
     SKEMA_LAUNCHED(c);
     scale_block(c, MatOut{c->Z, c->s, 1}, c->s, c->s, nu);
     const int64_t tiles = ((c->s + 127) / 128) * ((c->s + 127) / 128);

@@ -1,0 +1,312 @@
+"""GPU parity tests: the CUDA library through the C ABI against the oracle.
+
+Bars: map indices/signs and Gauss entries bit-exact; FP32 sketches X, Y, Z
+within 1e-5 relative Frobenius error of the FP64 oracle on the same inputs
+and maps; singular values of the fixed-rank approximation against the
+reference's own fixtures.
+"""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+from conftest import rel_fro
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-5  # FP32 sketch vs FP64 oracle, relative Frobenius
+
+
+@pytest.fixture(scope="module")
+def sk(lib_built):
+    import skema_b200
+
+    return skema_b200
+
+
+def dense_input(m, n, seed=0, noise=1e-4):
+    """U diag(s) V^T + noise with s_i = 10^(-0.1 i) (the small dense recipe)."""
+    rng = np.random.default_rng(seed)
+    p = min(m, n, 64)
+    U = np.linalg.qr(rng.normal(size=(m, p)))[0]
+    V = np.linalg.qr(rng.normal(size=(n, p)))[0]
+    s = 10.0 ** (-0.1 * np.arange(p))
+    return (U * s) @ V.T + noise * rng.normal(size=(m, n))
+
+
+def csr_input(m, n, nnz_row=10, seed=2, empty_every=0):
+    rng = np.random.default_rng(seed)
+    rows = np.repeat(np.arange(m), nnz_row)
+    cols = rng.integers(0, n, size=m * nnz_row)
+    vals = rng.normal(size=m * nnz_row)
+    A = sp.csr_matrix((vals, (rows, cols)), shape=(m, n))  # duplicates summed
+    A.sum_duplicates()
+    if empty_every:
+        A = A.tolil()
+        for i in range(0, m, empty_every):
+            A.rows[i] = []
+            A.data[i] = []
+        A = A.tocsr()
+    A.data = A.data.astype(np.float32).astype(np.float64)
+    return A
+
+
+def alg(sk, m, n, rank, window, kind, issparse=False, **kw):
+    a = sk.AlgParams(matrix_m=m, matrix_n=n, rank=rank, window=window, dim_redux=kind, issparse=issparse)
+    for key, v in kw.items():
+        setattr(a, key, v)
+    return a
+
+
+def oracle_for(oracle, a, spd=False, gamma=None):
+    return oracle.OracleSketch(a.matrix_m, a.matrix_n, a.rank, a.window, kind=a.dim_redux,
+                               issparse=a.issparse, sketch_range=a.sketch_range, sketch_core=a.sketch_core,
+                               eta=a.sketch_eta, nu=a.sketch_nu, seeds=tuple(a.seeds), spd=spd,
+                               kernel_gamma=gamma)
+
+
+def check_sketches(s, o):
+    X, Y, Z = s.get_sketches()
+    assert rel_fro(Y, o.Y) < TOL, rel_fro(Y, o.Y)
+    assert rel_fro(X, o.X) < TOL, rel_fro(X, o.X)
+    assert rel_fro(Z, o.Z) < TOL, rel_fro(Z, o.Z)
+
+
+# ------------------------------------------------------------------ maps ----
+@pytest.mark.parametrize("kind", [0, 1])
+@pytest.mark.parametrize("issparse", [False, True])
+def test_maps_bitexact(sk, oracle, kind, issparse):
+    a = alg(sk, 700, 300, 4, 50, kind, issparse)
+    o = oracle_for(oracle, a)
+    with sk.SketchySVD(a) as s:
+        for which, name in enumerate(["upsilon", "omega", "phi", "psi"]):
+            om = o.maps[name]
+            nr, nc, z, tr = s.map_info(which)
+            assert (nr, nc, tr) == (om.nrow, om.ncol, om.init_transposed)
+            vals, idx = s.map_export(which)
+            if kind == 0:
+                assert z == 0
+                assert np.array_equal(vals, om.dense.astype(np.float32).astype(np.float64))
+            else:
+                assert np.array_equal(idx, om.idx)
+                assert np.array_equal(vals, om.val)
+
+
+def test_map_import_roundtrip(sk, oracle):
+    a = alg(sk, 300, 200, 3, 50, 1, True)
+    with sk.SketchySVD(a) as s:
+        v, ix = s.map_export(1)
+        ix2 = np.sort((ix + 1) % ix.max(), axis=1)
+        s.map_import(1, -v, ix2)
+        v3, ix3 = s.map_export(1)
+        assert np.array_equal(ix3, ix2) and np.array_equal(v3, -v)
+        with pytest.raises(sk.SkemaError):
+            s.map_import(1, v * 0.5, ix)  # sparse-sign values must be +-1
+
+
+# ------------------------------------------------------------ dense FP32 ----
+@pytest.mark.parametrize("kind", [0, 1])
+@pytest.mark.parametrize("layout", ["C", "F"])
+def test_dense_fp32_parity(sk, oracle, kind, layout):
+    m, n = 2000, 1000
+    A = dense_input(m, n).astype(np.float32)
+    A = np.asfortranarray(A) if layout == "F" else np.ascontiguousarray(A)
+    a = alg(sk, m, n, 10, 100, kind)  # k = 41, s = 83 (config 1 shape)
+    o = oracle_for(oracle, a)
+    o.linear_update(A.astype(np.float64))
+    with sk.SketchySVD(a) as s:
+        assert (s.range, s.core) == (41, 83)
+        s.linear_update(A)
+        check_sketches(s, o)
+
+
+def test_dense_device_input_partial_window_eta_nu(sk, oracle):
+    import torch
+
+    m, n = 1234, 333
+    A = dense_input(m, n, seed=3).astype(np.float32)
+    a = alg(sk, m, n, 6, 200, 0, sketch_eta=0.75, sketch_nu=0.9)
+    o = oracle_for(oracle, a)
+    o.linear_update(A.astype(np.float64))
+    At = torch.from_numpy(A).cuda()
+    with sk.SketchySVD(a) as s:
+        s.linear_update(At)
+        check_sketches(s, o)
+        # column-major view of the same data
+        s.linear_update(At.t().contiguous().t())
+        check_sketches(s, o)
+
+
+def test_dense_streaming_blocks_equal_one_shot(sk, oracle):
+    m, n = 1200, 256
+    A = dense_input(m, n, seed=4).astype(np.float32)
+    a = alg(sk, m, n, 5, 100, 0)
+    with sk.SketchySVD(a) as s:
+        s.linear_update(A)
+        X1, Y1, Z1 = s.get_sketches()
+        s.reset()
+        s.update_rows(A[:500], 0)
+        s.update_rows(A[500:], 500)
+        s.update_rows(A[:0], 0)  # empty call is a no-op
+        X2, Y2, Z2 = s.get_sketches()
+    assert rel_fro(X2, X1) < 1e-6 and rel_fro(Y2, Y1) < 1e-6 and rel_fro(Z2, Z1) < 1e-6
+
+
+def test_single_shot_window_equals_m(sk, oracle):
+    m, n = 300, 120
+    A = dense_input(m, n, seed=6).astype(np.float32)
+    a = alg(sk, m, n, 4, m, 0)
+    o = oracle_for(oracle, a)
+    o.linear_update(A.astype(np.float64))
+    with sk.SketchySVD(a) as s:
+        s.linear_update(A)
+        check_sketches(s, o)
+
+
+# ------------------------------------------------------------------- CSR ----
+@pytest.mark.parametrize("kind", [1, 0])
+def test_csr_parity(sk, oracle, kind):
+    m, n = 20500, 5000
+    A = csr_input(m, n, empty_every=97)
+    a = alg(sk, m, n, 20, 1000, kind, issparse=True)  # k = 81, s = 163
+    o = oracle_for(oracle, a)
+    o.linear_update(A)
+    with sk.SketchySVD(a) as s:
+        s.linear_update(A)
+        check_sketches(s, o)
+
+
+def test_csr_device_input_and_eta_nu(sk, oracle):
+    import torch
+
+    m, n = 8000, 3000
+    A = csr_input(m, n, nnz_row=7, seed=9)
+    a = alg(sk, m, n, 8, 999, 1, issparse=True, sketch_eta=1.5, sketch_nu=0.5)
+    o = oracle_for(oracle, a)
+    o.linear_update(A)
+    rp = torch.from_numpy(A.indptr.astype(np.int64)).cuda()
+    cl = torch.from_numpy(A.indices.astype(np.int32)).cuda()
+    vl = torch.from_numpy(A.data.astype(np.float32)).cuda()
+    with sk.SketchySVD(a) as s:
+        s.linear_update((rp, cl, vl))
+        check_sketches(s, o)
+
+
+def test_csr_duplicate_columns_are_summed(sk, oracle):
+    m, n = 64, 40
+    rowptr = np.arange(0, 3 * m + 1, 3, dtype=np.int64)
+    col = np.tile(np.array([5, 5, 17], dtype=np.int32), m)
+    val = np.tile(np.array([1.0, 2.0, -1.0], dtype=np.float32), m)
+    a = alg(sk, m, n, 2, 16, 1, issparse=True)
+    merged = sp.csr_matrix((val.astype(np.float64), col, rowptr), shape=(m, n))
+    merged.sum_duplicates()
+    o = oracle_for(oracle, a)
+    o.linear_update(merged)
+    with sk.SketchySVD(a) as s:
+        s.linear_update((rowptr, col, val))
+        check_sketches(s, o)
+
+
+# ------------------------------------------------------------- SketchySPD ----
+@pytest.mark.parametrize("kind", [0, 1])
+@pytest.mark.parametrize("issparse", [False, True])
+def test_spd_update(sk, oracle, kind, issparse):
+    m = 900
+    B = dense_input(m, m, seed=7)
+    B = (B + B.T).astype(np.float32)
+    A = sp.csr_matrix(np.where(np.abs(B) > 2e-3, B, 0).astype(np.float64)) if issparse else B
+    a = alg(sk, m, m, 5, 128, kind, issparse=issparse, issymmetric=True)
+    o = oracle_for(oracle, a, spd=True)
+    o.linear_update(A if issparse else A.astype(np.float64))
+    with sk.SketchySPD(a) as s:
+        assert s.spd
+        s.linear_update(A)
+        Y = s.get_sketches()
+    assert rel_fro(Y, o.Y) < TOL
+
+
+# ------------------------------------------------------------------- RBF ----
+@pytest.mark.parametrize("kind", [0, 1])
+def test_rbf_update_parity(sk, oracle, kind):
+    N, d = 700, 5
+    P = oracle.mixture_points(N, d, seed=1)
+    gamma = oracle.median_gamma(P)
+    a = alg(sk, N, N, 6, 128, kind, kernel_func=1, kernel_gamma=gamma, force_three_sketch=True)
+    o = oracle_for(oracle, a, gamma=gamma)
+    o.linear_update(P.astype(np.float64))
+    with sk.SketchySVD(a) as s:
+        s.linear_update(P)
+        check_sketches(s, o)
+
+
+# -------------------------------------------------------- approximation ----
+@pytest.mark.parametrize("kind", [0, 1])
+def test_kat_rect(sk, kat, kind):
+    a = alg(sk, 32, 14, 10, 5, kind, sketch_range=12, sketch_core=25)
+    with sk.SketchySVD(a) as s:
+        s.linear_update(kat["rect_dense"].astype(np.float32))
+        U, S, V = s.low_rank_approx()
+    assert np.max(np.abs(S - kat["rect_svals"][:10])) / S[0] < 1e-5
+    assert np.allclose(U.T @ U, np.eye(10), atol=1e-8)
+    assert np.allclose(V.T @ V, np.eye(10), atol=1e-8)
+
+
+def test_kat_rect_csr(sk, kat):
+    A = sp.csr_matrix((kat["rect_csr_val"], kat["rect_csr_col"], kat["rect_csr_rowptr"]),
+                      shape=tuple(kat["rect_csr_shape"]))
+    for kind in (0, 1):
+        a = alg(sk, 32, 14, 10, 7, kind, issparse=True, sketch_range=12, sketch_core=25)
+        with sk.SketchySVD(a) as s:
+            s.linear_update(A)
+            _, S, _ = s.low_rank_approx()
+        assert np.max(np.abs(S - kat["rect_svals"][:10])) / S[0] < 1e-5
+
+
+def test_kat_symmetric(sk, kat):
+    a = alg(sk, 27, 27, 10, 4, 0, sketch_range=27, sketch_core=27)
+    with sk.SketchySVD(a) as s:
+        s.linear_update(kat["sym_dense"].astype(np.float32))
+        _, S, _ = s.low_rank_approx()
+    assert np.max(np.abs(S - kat["sym_svals"][:10])) / S[0] < 1e-5
+
+
+def test_kat_kernel(sk, kat):
+    a = alg(sk, 25, 25, 5, 6, 0, sketch_range=21, sketch_core=25, kernel_func=1, kernel_gamma=1.0,
+            force_three_sketch=True)
+    with sk.SketchySVD(a) as s:
+        s.linear_update(kat["kernel_points"].astype(np.float32))
+        _, S, _ = s.low_rank_approx()
+    assert np.max(np.abs(S - kat["kernel_svals"][:5])) / S[0] < 1e-5
+
+
+def test_low_rank_approx_vs_oracle(sk, oracle):
+    m, n = 2000, 1000
+    A = dense_input(m, n).astype(np.float32)
+    a = alg(sk, m, n, 10, 100, 0)
+    o = oracle_for(oracle, a)
+    with sk.SketchySVD(a) as s:
+        s.linear_update(A)
+        X, Y, Z = s.get_sketches()
+        U, S, V = s.low_rank_approx()
+    # the oracle's approximation from the GPU's own sketches isolates the solver
+    o.X, o.Y, o.Z = X.astype(np.float64), Y.astype(np.float64), Z.astype(np.float64)
+    Uo, So, Vo = o.low_rank_approx()
+    assert np.max(np.abs(S - So) / So[0]) < 1e-9
+    # singular vectors agree up to sign
+    assert np.allclose(np.abs(np.sum(U * Uo, axis=0)), 1.0, atol=1e-6)
+    assert np.allclose(np.abs(np.sum(V * Vo, axis=0)), 1.0, atol=1e-6)
+
+
+# ------------------------------------------------------------- errors ------
+def test_error_paths(sk):
+    a = alg(sk, 100, 50, 3, 10, 0)
+    with sk.SketchySVD(a) as s:
+        with pytest.raises(sk.SkemaError) as e:
+            s.update_rows(np.zeros((10, 50), np.float32), 95)  # rows past m
+        assert e.value.status == sk._lib.EINVAL
+        rp, cl, vl = np.array([0, 1], np.int64), np.array([0], np.int32), np.ones(1, np.float32)
+        st = s.lib.skema_linear_update_csr(s.h, rp.ctypes.data, cl.ctypes.data, vl.ctypes.data, 0, 1,
+                                           sk._lib.MEM_HOST)
+        assert st == sk._lib.ESTATE  # a dense context refuses a CSR update
+        Xs = np.arange(s.range * 50, dtype=np.float32).reshape(s.range, 50)
+        s.set_sketch(0, Xs)
+        assert np.array_equal(s.get_sketch(0), Xs)
