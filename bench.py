@@ -200,7 +200,9 @@ def run_gpu(args, cfg, peaks, peak_kind):
     a.issparse = sparse
     a.precision = cfg.get("prec", 0)
     ctx = sk.SketchySVD(a)
-    stream = torch.cuda.current_stream()
+    # one non-default stream for the library's launches and the timing events
+    stream = torch.cuda.Stream(device=dev)
+    torch.cuda.set_stream(stream)
     ctx.set_stream(stream.cuda_stream)
     row0 = rank * m_local
     if sparse:
@@ -230,25 +232,36 @@ def run_gpu(args, cfg, peaks, peak_kind):
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-    ctx.timing_enable(True)
-    l0 = ctx.launch_count()
+    if sparse:
+        kstage = "update.omega"
+    else:
+        kstage = "update.fused" if a.precision else "update.omega"
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
+    def load_for(seconds):
+        # untimed steps of the same work, so the clock samples bracket the
+        # timed steps under continuous load
+        t0 = time.perf_counter()
+        while time.perf_counter() - t0 < seconds:
+            for _ in range(8):
+                step()
+            torch.cuda.synchronize()
+
     with ClockSampler(local) as clk:
+        load_for(args.clock_lead)
+        l0 = ctx.launch_count()
+        ctx.timing_enable(True)
         torch.cuda.synchronize()
         e0.record(stream)
         for _ in range(args.steps):
             step()
         e1.record(stream)
         torch.cuda.synchronize()
-    launches = ctx.launch_count() - l0
+        launches = ctx.launch_count() - l0
+        kms, kcount = ctx.timing_get(kstage)
+        ctx.timing_enable(False)
+        load_for(args.clock_tail)
     ms = e0.elapsed_time(e1) / args.steps
-    if sparse:
-        kstage = "update.omega"
-    else:
-        kstage = "update.fused" if a.precision else "update.omega"
-    kms, kcount = ctx.timing_get(kstage)
-    ctx.timing_enable(False)
     ms_t = torch.tensor([ms], device=dev)
     if world > 1:
         dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
@@ -309,7 +322,7 @@ def run_gpu(args, cfg, peaks, peak_kind):
         "cpu_baseline": cpu,
         "e2e": e2e,
         "gpu_launches": launches,
-        "clocks": clk.summary(),
+        "clocks": dict(clk.summary(), window="samples span continuous load bracketing the timed steps"),
     }
     ctx.close()
     if world > 1:
@@ -505,6 +518,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=12.0)
+    ap.add_argument("--clock-lead", type=float, default=1.0, help="seconds of load before the timed steps")
+    ap.add_argument("--clock-tail", type=float, default=0.3, help="seconds of load after the timed steps")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     cfg = dict(WORKLOADS[args.workload])

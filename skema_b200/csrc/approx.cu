@@ -503,7 +503,7 @@ void low_rank_approx(skema_ctx* c, double* Uout, double* Sout, double* Vout) {
   int* st = (int*)bstat.p;
 
   // Q = Y (m x k, column-major, FP64); P = X^T (n x k, column-major)
-  f2d_kernel<<<g1(c, m * k), 256, 0, c->stream>>>(c->Y, k, 1, Q, 1, m, m, k);
+  f2d_kernel<<<g1(c, m * k), 256, 0, c->stream>>>(c->Y, 1, m, Q, 1, m, m, k);
   SKEMA_LAUNCHED(c);
   f2d_kernel<<<g1(c, n * k), 256, 0, c->stream>>>(c->X, 1, n, P, 1, n, n, k);
   SKEMA_LAUNCHED(c);

@@ -76,17 +76,20 @@ void y_rows_mark(skema_ctx* c, int64_t a, int64_t b) {
   v.swap(out);
 }
 
+// Y is column-major (m x k, ld = m): rows [a, b) are one strip per column.
+static void y_zero_rows(skema_ctx* c, int64_t a, int64_t b) {
+  if (a >= b) return;
+  SKEMA_CUDA(cudaMemset2DAsync(c->Y + a, sizeof(float) * (size_t)c->m, 0, sizeof(float) * (size_t)(b - a),
+                               (size_t)c->k, c->stream));
+}
+
 void y_materialize(skema_ctx* c) {
   int64_t at = 0;
   for (const Interval& iv : c->y_written) {
-    if (iv.a > at)
-      SKEMA_CUDA(cudaMemsetAsync(c->Y + at * c->k, 0, sizeof(float) * (size_t)((iv.a - at) * c->k),
-                                 c->stream));
+    if (iv.a > at) y_zero_rows(c, at, iv.a);
     at = std::max(at, iv.b);
   }
-  if (at < c->m)
-    SKEMA_CUDA(cudaMemsetAsync(c->Y + at * c->k, 0, sizeof(float) * (size_t)((c->m - at) * c->k),
-                               c->stream));
+  if (at < c->m) y_zero_rows(c, at, c->m);
   c->y_written.assign(1, Interval{0, c->m});
 }
 
@@ -515,6 +518,9 @@ static void sketch_shape(const skema_ctx* c, int32_t which, float** p, int64_t* 
   if (!*p) fail(SKEMA_ESTATE, "this context has no such sketch (SketchySPD keeps Y only)");
 }
 
+// X and Z are kept row-major, Y column-major (LayoutLeft, ld = m).
+static bool sketch_row_major(int32_t which) { return which != SKEMA_SKETCH_Y; }
+
 int skema_get_sketch(skema_ctx* c, int32_t which, float* buf, int64_t ld, int32_t layout,
                      int32_t mem) {
   return guarded(c, [&] {
@@ -523,17 +529,22 @@ int skema_get_sketch(skema_ctx* c, int32_t which, float* buf, int64_t ld, int32_
     sketch_shape(c, which, &src, &rows, &cols);
     check_dense_args(buf, ld, layout, rows, cols, mem);
     if (which == SKEMA_SKETCH_Y) y_materialize(c);
+    const bool irow = sketch_row_major(which);
+    const int64_t inner = irow ? cols : rows, outer = irow ? rows : cols;
+    const Mat sm = irow ? Mat{src, cols, 1} : Mat{src, 1, rows};
+    const bool want_row = layout == SKEMA_ROW_MAJOR;
     const cudaMemcpyKind kind = mem == SKEMA_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
-    if (layout == SKEMA_ROW_MAJOR) {
-      SKEMA_CUDA(cudaMemcpy2DAsync(buf, sizeof(float) * ld, src, sizeof(float) * cols,
-                                   sizeof(float) * cols, rows, kind, c->stream));
+    if (want_row == irow) {
+      SKEMA_CUDA(cudaMemcpy2DAsync(buf, sizeof(float) * ld, src, sizeof(float) * inner,
+                                   sizeof(float) * inner, outer, kind, c->stream));
     } else if (mem == SKEMA_MEM_DEVICE) {
-      copy_block(c, Mat{src, cols, 1}, MatOut{buf, 1, ld}, rows, cols);
+      copy_block(c, sm, want_row ? MatOut{buf, ld, 1} : MatOut{buf, 1, ld}, rows, cols);
     } else {
+      const int64_t tin = want_row ? cols : rows, tout = want_row ? rows : cols;
       float* tmp = (float*)staging(c, sizeof(float) * (size_t)(rows * cols));
-      copy_block(c, Mat{src, cols, 1}, MatOut{tmp, 1, rows}, rows, cols);
-      SKEMA_CUDA(cudaMemcpy2DAsync(buf, sizeof(float) * ld, tmp, sizeof(float) * rows,
-                                   sizeof(float) * rows, cols, cudaMemcpyDeviceToHost, c->stream));
+      copy_block(c, sm, want_row ? MatOut{tmp, cols, 1} : MatOut{tmp, 1, rows}, rows, cols);
+      SKEMA_CUDA(cudaMemcpy2DAsync(buf, sizeof(float) * ld, tmp, sizeof(float) * tin,
+                                   sizeof(float) * tin, tout, cudaMemcpyDeviceToHost, c->stream));
     }
     if (mem == SKEMA_MEM_HOST) SKEMA_CUDA(cudaStreamSynchronize(c->stream));
   });
@@ -546,17 +557,22 @@ int skema_set_sketch(skema_ctx* c, int32_t which, const float* buf, int64_t ld, 
     int64_t rows, cols;
     sketch_shape(c, which, &dst, &rows, &cols);
     check_dense_args(buf, ld, layout, rows, cols, mem);
+    const bool irow = sketch_row_major(which);
+    const int64_t inner = irow ? cols : rows, outer = irow ? rows : cols;
+    const MatOut dm = irow ? MatOut{dst, cols, 1} : MatOut{dst, 1, rows};
+    const bool have_row = layout == SKEMA_ROW_MAJOR;
     const cudaMemcpyKind kind = mem == SKEMA_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
-    if (layout == SKEMA_ROW_MAJOR) {
-      SKEMA_CUDA(cudaMemcpy2DAsync(dst, sizeof(float) * cols, buf, sizeof(float) * ld,
-                                   sizeof(float) * cols, rows, kind, c->stream));
+    if (have_row == irow) {
+      SKEMA_CUDA(cudaMemcpy2DAsync(dst, sizeof(float) * inner, buf, sizeof(float) * ld,
+                                   sizeof(float) * inner, outer, kind, c->stream));
     } else if (mem == SKEMA_MEM_DEVICE) {
-      copy_block(c, Mat{buf, 1, ld}, MatOut{dst, cols, 1}, rows, cols);
+      copy_block(c, have_row ? Mat{buf, ld, 1} : Mat{buf, 1, ld}, dm, rows, cols);
     } else {
+      const int64_t tin = have_row ? cols : rows, tout = have_row ? rows : cols;
       float* tmp = (float*)staging(c, sizeof(float) * (size_t)(rows * cols));
-      SKEMA_CUDA(cudaMemcpy2DAsync(tmp, sizeof(float) * rows, buf, sizeof(float) * ld,
-                                   sizeof(float) * rows, cols, cudaMemcpyHostToDevice, c->stream));
-      copy_block(c, Mat{tmp, 1, rows}, MatOut{dst, cols, 1}, rows, cols);
+      SKEMA_CUDA(cudaMemcpy2DAsync(tmp, sizeof(float) * tin, buf, sizeof(float) * ld,
+                                   sizeof(float) * tin, tout, cudaMemcpyHostToDevice, c->stream));
+      copy_block(c, have_row ? Mat{tmp, cols, 1} : Mat{tmp, 1, rows}, dm, rows, cols);
     }
     if (which == SKEMA_SKETCH_Y) {
       c->y_written.clear();

@@ -50,6 +50,10 @@ struct Map {
   void* lowp = nullptr;
   // SparseSign: stored rows, zeta packed entries each: column | sign << 31.
   uint32_t* packed = nullptr;
+  // Stored-transposed SparseSign with zeta == 8 and ncol <= 128: one 64-bit
+  // word per stored row, byte t = column | sign << 7 (the streaming Y
+  // kernel's map format).
+  uint64_t* packed8 = nullptr;
   // SparseSign maps that are row-sparse over the input rows (Upsilon, Phi of
   // the three-sketch): (input row, map row, sign) triples sorted by input
   // row, on the host and on the device.
@@ -92,7 +96,8 @@ struct skema_ctx {
   std::string err;
   int64_t launches = 0;
   skema::Map ups, omg, phi, psi;
-  // Sketches, FP32, row-major: X k x n, Y m x k, Z s x s.
+  // Sketches, FP32: X k x n and Z s x s row-major; Y m x k column-major
+  // (ld = m, the reference's LayoutLeft).
   float* X = nullptr;
   float* Y = nullptr;
   float* Z = nullptr;

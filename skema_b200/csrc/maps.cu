@@ -49,6 +49,21 @@ __global__ void sparse_sign_map_kernel(uint32_t* __restrict__ packed, int64_t nr
   }
 }
 
+// Byte form of a SparseSign map with zeta = 8 and at most 128 columns.
+__global__ void pack8_kernel(const uint32_t* __restrict__ packed, uint64_t* __restrict__ out,
+                             int64_t nrow) {
+  for (int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; row < nrow;
+       row += (int64_t)gridDim.x * blockDim.x) {
+    uint64_t w = 0;
+    for (int t = 0; t < 8; ++t) {
+      const uint32_t e = packed[row * 8 + t];
+      const uint64_t byte = (e & 0x7fu) | ((e >> 31) << 7);
+      w |= byte << (8 * t);
+    }
+    out[row] = w;
+  }
+}
+
 // Import path: logical FP32 layout from stored column-major doubles.
 __global__ void gauss_import_kernel(float* __restrict__ out, const double* __restrict__ stored,
                                     int64_t lrows, int64_t lcols, int64_t rs, int64_t cs,
@@ -66,6 +81,14 @@ __global__ void gauss_import_kernel(float* __restrict__ out, const double* __res
 static int grid_for(int64_t total, int threads, int sms) {
   const int64_t want = (total + threads - 1) / threads;
   return (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)sms * 32));
+}
+
+static void build_pack8(skema_ctx* c, Map& mp) {
+  if (mp.kind != SKEMA_MAP_SPARSE_SIGN || !mp.transposed) return;
+  if (mp.zeta != 8 || mp.ncol > 128) return;
+  if (!mp.packed8) SKEMA_CUDA(cudaMalloc(&mp.packed8, sizeof(uint64_t) * (size_t)mp.nrow));
+  pack8_kernel<<<grid_for(mp.nrow, 256, c->sm_count), 256, 0, c->stream>>>(mp.packed, mp.packed8, mp.nrow);
+  SKEMA_LAUNCHED(c);
 }
 
 static void gauss_layout(const skema_ctx* c, Map& mp) {
@@ -97,6 +120,7 @@ void map_generate(skema_ctx* c, Map& mp, int precision) {
     sparse_sign_map_kernel<<<grid_for(mp.nrow, threads, c->sm_count), threads, 0, c->stream>>>(
         mp.packed, mp.nrow, (uint32_t)mp.ncol, mp.zeta, mp.seed);
     SKEMA_LAUNCHED(c);
+    build_pack8(c, mp);
   }
 }
 
@@ -104,6 +128,8 @@ void map_free(Map& mp) {
   if (mp.f32) cudaFree(mp.f32);
   if (mp.lowp) cudaFree(mp.lowp);
   if (mp.packed) cudaFree(mp.packed);
+  if (mp.packed8) cudaFree(mp.packed8);
+  mp.packed8 = nullptr;
   if (mp.d_inv_row) cudaFree(mp.d_inv_row);
   if (mp.d_inv_rs) cudaFree(mp.d_inv_rs);
   mp.f32 = nullptr;
@@ -206,6 +232,7 @@ void map_import(skema_ctx* c, Map& mp, const double* values, const int32_t* indi
   }
   SKEMA_CUDA(cudaMemcpyAsync(mp.packed, h.data(), sizeof(uint32_t) * ne, cudaMemcpyHostToDevice,
                              c->stream));
+  build_pack8(c, mp);
   SKEMA_CUDA(cudaStreamSynchronize(c->stream));
   map_build_inverse(c, mp);
 }

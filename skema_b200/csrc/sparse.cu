@@ -8,10 +8,12 @@
 //   (src/Skema_DimRedux_SparseSign.cpp:53-111) after a serial col_subview
 //   (:125-155). Here all windows of a call are handled by two launches: a
 //   streaming kernel for Y (the HBM-bound part: every nonzero read once, every
-//   Y row written once) and a tiny kernel for the X/Z entries, whose window
+//   Y element written once) and a tiny kernel for the X/Z entries, whose window
 //   weights eta*nu^(W-1-w) reproduce the per-window axpy sequence.
 //   CSR x Gauss (src/Skema_SketchySVD.cpp:296-316), dense x SparseSign
 //   (:271-293) and the SketchySPD updates (:896-932) follow.
+//
+// Y is column-major (m x k, ld = m), the reference's LayoutLeft.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -28,106 +30,87 @@ int grid_cap(const skema_ctx* c, int64_t want, int per_sm) {
 }
 
 // ---------------------------------------------------------------------------
-// Y rows for a CSR window block times a stored-transposed SparseSign map.
-// One warp owns a tile of R consecutive rows; the tile's k-wide output rows
-// accumulate in shared memory (one shared atomic per (nonzero, map entry)),
-// then stream out once. Nonzeros are read with streaming loads, the map
-// (zeta words per input column) through the read-only path.
+// Y rows of a CSR block times a stored-transposed SparseSign map (n rows of
+// zeta entries over k columns).
+//
+// One thread per input row. Each warp owns 32 consecutive rows and a
+// bin-major accumulator acc[r * 32 + lane] in shared memory: lane l adds
+// +-a_ij into the k bins of its own row only, so the updates need no
+// atomics and every shared access of a warp hits 32 distinct banks. After
+// the rows are done, bin r of the 32 rows is one coalesced 128-byte store
+// into the column-major Y. Nonzeros go through the read-only path (the
+// warp's 32 rows are contiguous in col/val, so L1 serves the lanes' strided
+// walk); each lane keeps UNR nonzeros and their map words in flight. The
+// map is one 8-byte word per input column when zeta = 8 and k <= 128
+// (index in 7 bits, sign in the top bit of each byte), else zeta 32-bit
+// words (column | sign << 31).
 // ---------------------------------------------------------------------------
-constexpr int YUNR = 2;
+template <bool BYTE8>
+__device__ __forceinline__ void ssign_apply(float* __restrict__ my, const uint64_t* __restrict__ omg8,
+                                            const uint32_t* __restrict__ omg32, int zeta, int32_t j,
+                                            float a) {
+  if (BYTE8) {
+    const uint64_t w = __ldg(omg8 + j);
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+      const uint32_t byte = (uint32_t)(w >> (8 * t)) & 0xffu;
+      my[(byte & 0x7fu) * 32] += (byte & 0x80u) ? -a : a;
+    }
+  } else {
+    for (int t = 0; t < zeta; ++t) {
+      const uint32_t w = __ldg(omg32 + (int64_t)j * zeta + t);
+      my[(w & 0x7fffffffu) * 32] += (w >> 31) ? -a : a;
+    }
+  }
+}
 
-template <bool Z8>
-__global__ void __launch_bounds__(256)
+template <bool BYTE8, int UNR>
+__global__ void __launch_bounds__(128)
     csr_ssign_y_kernel(const int64_t* __restrict__ rowptr, const int32_t* __restrict__ col,
                        const float* __restrict__ val, int64_t col_offset, int64_t nrows,
-                       const uint32_t* __restrict__ omg, int zeta, int k, int ncol,
-                       float* __restrict__ Y,
-                       float alpha, float beta, int R) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int nw = blockDim.x >> 5;
-  int64_t* srp_all = reinterpret_cast<int64_t*>(smem_raw);
-  int64_t* srp = srp_all + warp * 32;
-  float* acc = reinterpret_cast<float*>(smem_raw + sizeof(int64_t) * 32 * nw) + (size_t)warp * R * k;
-  for (int q = lane; q < R * k; q += 32) acc[q] = 0.f;
-  __syncwarp();
-  const int64_t ntiles = (nrows + R - 1) / R;
+                       const uint64_t* __restrict__ omg8, const uint32_t* __restrict__ omg32,
+                       int zeta, int k, int ncol, float* __restrict__ Y, int64_t ldy, float alpha,
+                       float beta) {
+  extern __shared__ float acc_all[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  float* my = acc_all + (size_t)warp * k * 32 + lane;  // bins of this lane's row: my[r * 32]
+  for (int r = 0; r < k; ++r) my[r * 32] = 0.f;
+  const int64_t ntiles = (nrows + 31) / 32;
   for (int64_t tile = (int64_t)blockIdx.x * nw + warp; tile < ntiles;
        tile += (int64_t)gridDim.x * nw) {
-    const int64_t i0 = tile * R;
-    const int rr = (int)min((int64_t)R, nrows - i0);
-    if (lane <= rr) srp[lane] = __ldg(rowptr + i0 + lane) - col_offset;
-    __syncwarp();
-    const int64_t S = srp[0], E = srp[rr];
-    for (int64_t base = S; base < E; base += 32 * YUNR) {
-      int32_t jj[YUNR];
-      float vv[YUNR];
-      int rl[YUNR];
+    const int64_t i = tile * 32 + lane;
+    const bool live = i < nrows;
+    int64_t b = live ? __ldg(rowptr + i) - col_offset : 0;
+    int64_t e = __shfl_down_sync(0xffffffffu, b, 1);
+    if (lane == 31 || i + 1 >= nrows) e = live ? __ldg(rowptr + i + 1) - col_offset : 0;
+    int64_t p = b;
+    for (; p + UNR <= e; p += UNR) {
+      int32_t jj[UNR];
+      float aa[UNR];
 #pragma unroll
-      for (int u = 0; u < YUNR; ++u) {
-        const int64_t e = base + u * 32 + lane;
-        const bool ok = e < E;
-        jj[u] = ok ? __ldcs(col + e) : -1;
-        if ((unsigned)jj[u] >= (unsigned)ncol) jj[u] = -1;  // columns outside [0, n) are ignored
-        vv[u] = ok ? __ldcs(val + e) : 0.f;
-        // largest l with srp[l] <= e (srp[rr] = E > e)
-        int lo = 0, hi = rr;
-        while (hi - lo > 1) {
-          const int mid = (lo + hi) >> 1;
-          if (srp[mid] <= e) lo = mid; else hi = mid;
-        }
-        rl[u] = lo;
+      for (int u = 0; u < UNR; ++u) {
+        jj[u] = __ldg(col + p + u);
+        aa[u] = __ldg(val + p + u);
       }
-      if (Z8) {
-        uint4 w0[YUNR], w1[YUNR];
 #pragma unroll
-        for (int u = 0; u < YUNR; ++u) {
-          if (jj[u] >= 0) {
-            const uint4* op = reinterpret_cast<const uint4*>(omg + (int64_t)jj[u] * 8);
-            w0[u] = __ldg(op);
-            w1[u] = __ldg(op + 1);
-          }
-        }
-#pragma unroll
-        for (int u = 0; u < YUNR; ++u) {
-          if (jj[u] >= 0) {
-            float* a = acc + rl[u] * k;
-            const float v = vv[u];
-            const uint32_t w[8] = {w0[u].x, w0[u].y, w0[u].z, w0[u].w,
-                                   w1[u].x, w1[u].y, w1[u].z, w1[u].w};
-#pragma unroll
-            for (int t = 0; t < 8; ++t)
-              atomicAdd(a + (w[t] & 0x7fffffffu), (w[t] >> 31) ? -v : v);
-          }
-        }
-      } else {
-#pragma unroll
-        for (int u = 0; u < YUNR; ++u) {
-          if (jj[u] >= 0) {
-            float* a = acc + rl[u] * k;
-            const float v = vv[u];
-            for (int t = 0; t < zeta; ++t) {
-              const uint32_t w = __ldg(omg + (int64_t)jj[u] * zeta + t);
-              atomicAdd(a + (w & 0x7fffffffu), (w >> 31) ? -v : v);
-            }
-          }
-        }
-      }
+      for (int u = 0; u < UNR; ++u)
+        if ((unsigned)jj[u] < (unsigned)ncol) ssign_apply<BYTE8>(my, omg8, omg32, zeta, jj[u], aa[u]);
     }
-    __syncwarp();
-    for (int l = 0; l < rr; ++l) {
-      float* yrow = Y + (i0 + l) * (int64_t)k;
-      float* arow = acc + l * k;
-      for (int cc = lane; cc < k; cc += 32) {
-        const float a = arow[cc];
-        arow[cc] = 0.f;
+    for (; p < e; ++p) {
+      const int32_t j = __ldg(col + p);
+      if ((unsigned)j < (unsigned)ncol) ssign_apply<BYTE8>(my, omg8, omg32, zeta, j, __ldg(val + p));
+    }
+    if (live) {
+      float* yp = Y + i;
+      for (int r = 0; r < k; ++r) {
+        const float v = my[r * 32];
+        my[r * 32] = 0.f;
         if (beta == 0.f)
-          __stcs(yrow + cc, alpha * a);
+          __stcs(yp + r * ldy, alpha * v);
         else
-          yrow[cc] = fmaf(beta, yrow[cc], alpha * a);
+          yp[r * ldy] = fmaf(beta, yp[r * ldy], alpha * v);
       }
     }
-    __syncwarp();
   }
 }
 
@@ -179,7 +162,7 @@ __global__ void csr_gauss_y_kernel(const int64_t* __restrict__ rowptr,
                                    const int32_t* __restrict__ col, const float* __restrict__ val,
                                    int64_t col_offset, int64_t nrows, int64_t ncol,
                                    const float* __restrict__ mapT /* n x k rows */, int64_t k,
-                                   float* __restrict__ Y, float alpha, float beta) {
+                                   float* __restrict__ Y, int64_t ldy, float alpha, float beta) {
   const int lane = threadIdx.x & 31;
   const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -188,8 +171,8 @@ __global__ void csr_gauss_y_kernel(const int64_t* __restrict__ rowptr,
     for (int64_t c0 = 0; c0 < k; c0 += 128) {
       float a[4] = {0.f, 0.f, 0.f, 0.f};
       for (int64_t p = b; p < e; ++p) {
-        const float v = val[p];
         if ((uint64_t)col[p] >= (uint64_t)ncol) continue;
+        const float v = val[p];
         const float* mrow = mapT + (int64_t)col[p] * k;
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
@@ -201,7 +184,7 @@ __global__ void csr_gauss_y_kernel(const int64_t* __restrict__ rowptr,
       for (int u = 0; u < 4; ++u) {
         const int64_t cc = c0 + lane + 32 * u;
         if (cc < k) {
-          float* yp = Y + i * k + cc;
+          float* yp = Y + i + cc * ldy;
           *yp = (beta == 0.f) ? alpha * a[u] : fmaf(beta, *yp, alpha * a[u]);
         }
       }
@@ -214,9 +197,10 @@ __global__ void csr_gauss_y_kernel(const int64_t* __restrict__ rowptr,
 __global__ void csr_gauss_scatter_kernel(const int64_t* __restrict__ rowptr,
                                          const int32_t* __restrict__ col,
                                          const float* __restrict__ val, int64_t col_offset,
-                                         int64_t nrows, int64_t ncol, const float* __restrict__ maprows,
-                                         int64_t kk, float* __restrict__ out, int64_t ors,
-                                         int64_t ocs, float alpha) {
+                                         int64_t nrows, int64_t ncol,
+                                         const float* __restrict__ maprows, int64_t kk,
+                                         float* __restrict__ out, int64_t ors, int64_t ocs,
+                                         float alpha) {
   const int lane = threadIdx.x & 31;
   const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -236,35 +220,26 @@ __global__ void csr_gauss_scatter_kernel(const int64_t* __restrict__ rowptr,
 // Dense window x SparseSign (three-sketch, dense input, update(dense,
 // SparseSign) src/Skema_SketchySVD.cpp:271-293).
 // Y(R0+i, r) = beta*Y + alpha * sum_t sign_rt A_w(i, c_rt) for the k x n
-// row-sparse Omega~. Block: 32 rows x all r, staged in shared memory.
+// row-sparse Omega~: thread (row, map row), consecutive threads on
+// consecutive rows (coalesced gathers from a column-major window and
+// coalesced stores into the column-major Y).
 // ---------------------------------------------------------------------------
 __global__ void dense_ssign_y_kernel(const float* __restrict__ A, int64_t ars, int64_t acs,
                                      int64_t wr, const uint32_t* __restrict__ omg, int zeta,
-                                     int64_t k, float* __restrict__ Y, float alpha, float beta) {
-  extern __shared__ float st[];  // 32 x k
-  const int ti = threadIdx.x & 31, tr = threadIdx.x >> 5, nr = blockDim.x >> 5;
-  for (int64_t i0 = (int64_t)blockIdx.x * 32; i0 < wr; i0 += (int64_t)gridDim.x * 32) {
-    const int64_t i = i0 + ti;
-    for (int64_t r = tr; r < k; r += nr) {
-      float a = 0.f;
-      if (i < wr) {
-        for (int t = 0; t < zeta; ++t) {
-          const uint32_t w = __ldg(omg + r * zeta + t);
-          const float v = __ldg(A + i * ars + (int64_t)(w & 0x7fffffffu) * acs);
-          a += (w >> 31) ? -v : v;
-        }
-      }
-      st[ti * k + r] = a;
+                                     int64_t k, float* __restrict__ Y, int64_t ldy, float alpha,
+                                     float beta) {
+  const int64_t total = wr * k;
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < total;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = q / wr, i = q - r * wr;
+    float a = 0.f;
+    for (int t = 0; t < zeta; ++t) {
+      const uint32_t w = __ldg(omg + r * zeta + t);
+      const float v = __ldg(A + i * ars + (int64_t)(w & 0x7fffffffu) * acs);
+      a += (w >> 31) ? -v : v;
     }
-    __syncthreads();
-    const int64_t rows = min((int64_t)32, wr - i0);
-    for (int64_t q = threadIdx.x; q < rows * k; q += blockDim.x) {
-      const int64_t l = q / k, r = q - l * k;
-      float* yp = Y + (i0 + l) * k + r;
-      const float v = alpha * st[l * k + r];
-      *yp = (beta == 0.f) ? v : fmaf(beta, *yp, v);
-    }
-    __syncthreads();
+    float* yp = Y + i + r * ldy;
+    *yp = (beta == 0.f) ? alpha * a : fmaf(beta, *yp, alpha * a);
   }
 }
 
@@ -307,27 +282,28 @@ __global__ void dense_ssign_entries_kernel(const float* __restrict__ A, int64_t 
 
 // SketchySPD with a SparseSign Omega stored n x k (zeta per input column):
 // Y(R0+i, :) = beta*Y + alpha * sum_j A_w(i, j) Omega(j, :). One thread per
-// row, accumulating its k-row in shared memory (odd stride: no bank clash).
+// row with bin-major accumulators acc[r * blockDim + tid] (conflict free).
 __global__ void dense_colsparse_y_kernel(const float* __restrict__ A, int64_t ars, int64_t acs,
                                          int64_t wr, int64_t n, const uint32_t* __restrict__ omg,
-                                         int zeta, int64_t k, int64_t kp, float* __restrict__ Y,
+                                         int zeta, int64_t k, float* __restrict__ Y, int64_t ldy,
                                          float alpha, float beta) {
-  extern __shared__ float acc[];  // blockDim.x x kp
-  float* my = acc + (int64_t)threadIdx.x * kp;
-  for (int64_t i0 = (int64_t)blockIdx.x * blockDim.x; i0 < wr; i0 += (int64_t)gridDim.x * blockDim.x) {
+  extern __shared__ float acc[];
+  float* my = acc + threadIdx.x;
+  const int nt = blockDim.x;
+  for (int64_t i0 = (int64_t)blockIdx.x * nt; i0 < wr; i0 += (int64_t)gridDim.x * nt) {
     const int64_t i = i0 + threadIdx.x;
-    for (int64_t r = 0; r < k; ++r) my[r] = 0.f;
+    for (int64_t r = 0; r < k; ++r) my[r * nt] = 0.f;
     if (i < wr) {
       for (int64_t j = 0; j < n; ++j) {
         const float v = __ldg(A + i * ars + j * acs);
         for (int t = 0; t < zeta; ++t) {
           const uint32_t w = __ldg(omg + j * zeta + t);
-          my[w & 0x7fffffffu] += (w >> 31) ? -v : v;
+          my[(int64_t)(w & 0x7fffffffu) * nt] += (w >> 31) ? -v : v;
         }
       }
       for (int64_t r = 0; r < k; ++r) {
-        float* yp = Y + i * k + r;
-        *yp = (beta == 0.f) ? alpha * my[r] : fmaf(beta, *yp, alpha * my[r]);
+        float* yp = Y + i + r * ldy;
+        *yp = (beta == 0.f) ? alpha * my[r * nt] : fmaf(beta, *yp, alpha * my[r * nt]);
       }
     }
   }
@@ -340,46 +316,39 @@ std::pair<int64_t, int64_t> entry_range(const Map& mp, int64_t a, int64_t b) {
   return {lo - mp.inv_row.begin(), hi - mp.inv_row.begin()};
 }
 
-void launch_csr_ssign_y(skema_ctx* c, const int64_t* rowptr, const int32_t* col, const float* val,
-                        int64_t col_offset, int64_t nrows, const Map& O, float* Yrows, float alpha,
-                        float beta) {
+}  // namespace
+
+template <bool BYTE8, int UNR>
+void launch_csr_ssign_y_variant(skema_ctx* c, int warps_per_block, const int64_t* rowptr,
+                                const int32_t* col, const float* val, int64_t col_offset,
+                                int64_t nrows, const Map& O, float* Y, int64_t ldy, float alpha,
+                                float beta) {
   const int k = (int)c->k;
-  // rows per warp tile: ~6 KB of accumulators per warp, at most 31 rows
-  int R = (int)std::max<int64_t>(1, std::min<int64_t>(31, 6144 / (4 * (int64_t)k)));
-  int nw = 8;
-  size_t smem = sizeof(int64_t) * 32 * nw + sizeof(float) * (size_t)nw * R * k;
-  while (smem > 200 * 1024 && nw > 1) {
-    nw >>= 1;
-    smem = sizeof(int64_t) * 32 * nw + sizeof(float) * (size_t)nw * R * k;
-  }
-  if (smem > 200 * 1024) fail(SKEMA_EUNSUPPORTED, "sketch range too large for the sparse-sign kernel");
-  const int64_t ntiles = (nrows + R - 1) / R;
-  const int64_t blocks_want = (ntiles + nw - 1) / nw;
+  const size_t smem = sizeof(float) * 32 * (size_t)k * warps_per_block;
+  auto kern = csr_ssign_y_kernel<BYTE8, UNR>;
+  SKEMA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 1;
-  cudaFuncAttributes fa;
-  if (O.zeta == 8) {
-    SKEMA_CUDA(cudaFuncSetAttribute(csr_ssign_y_kernel<true>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    SKEMA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, csr_ssign_y_kernel<true>,
-                                                             32 * nw, smem));
-  } else {
-    SKEMA_CUDA(cudaFuncSetAttribute(csr_ssign_y_kernel<false>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    SKEMA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, csr_ssign_y_kernel<false>,
-                                                             32 * nw, smem));
-  }
-  (void)fa;
-  const int grid = grid_cap(c, blocks_want, std::max(1, per_sm));
-  if (O.zeta == 8)
-    csr_ssign_y_kernel<true><<<grid, 32 * nw, smem, c->stream>>>(
-        rowptr, col, val, col_offset, nrows, O.packed, 8, k, (int)c->n, Yrows, alpha, beta, R);
-  else
-    csr_ssign_y_kernel<false><<<grid, 32 * nw, smem, c->stream>>>(
-        rowptr, col, val, col_offset, nrows, O.packed, O.zeta, k, (int)c->n, Yrows, alpha, beta, R);
+  SKEMA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * warps_per_block, smem));
+  const int64_t tiles = (nrows + 31) / 32;
+  const int grid = grid_cap(c, (tiles + warps_per_block - 1) / warps_per_block, std::max(1, per_sm));
+  kern<<<grid, 32 * warps_per_block, smem, c->stream>>>(rowptr, col, val, col_offset, nrows, O.packed8,
+                                                        O.packed, O.zeta, k, (int)c->n, Y, ldy,
+                                                        alpha, beta);
   SKEMA_LAUNCHED(c);
 }
 
-}  // namespace
+static void launch_csr_ssign_y(skema_ctx* c, const int64_t* rowptr, const int32_t* col,
+                               const float* val, int64_t col_offset, int64_t nrows, const Map& O,
+                               float* Y, int64_t ldy, float alpha, float beta) {
+  int wpb = 4;
+  while (wpb > 1 && sizeof(float) * 32 * (size_t)c->k * wpb > 96 * 1024) wpb >>= 1;
+  if (sizeof(float) * 32 * (size_t)c->k * wpb > 200 * 1024)
+    fail(SKEMA_EUNSUPPORTED, "sketch range too large for the sparse-sign kernel");
+  if (O.packed8)
+    launch_csr_ssign_y_variant<true, 4>(c, wpb, rowptr, col, val, col_offset, nrows, O, Y, ldy, alpha, beta);
+  else
+    launch_csr_ssign_y_variant<false, 4>(c, wpb, rowptr, col, val, col_offset, nrows, O, Y, ldy, alpha, beta);
+}
 
 // ---------------------------------------------------------------------------
 void csr_update(skema_ctx* c, const int64_t* rowptr, const int32_t* col, const float* val,
@@ -389,12 +358,11 @@ void csr_update(skema_ctx* c, const int64_t* rowptr, const int32_t* col, const f
   const int64_t nwin = (nrows + W - 1) / W;
   const bool clean = y_rows_clean(c, row0, row0 + nrows);
   const float ybeta = clean ? 0.f : nu;
-  float* Yrows = c->Y + row0 * c->k;
 
   if (c->p.dim_redux == SKEMA_MAP_SPARSE_SIGN) {
     {
       StageScope st(c, ST_OMEGA);
-      launch_csr_ssign_y(c, rowptr, col, val, col_offset, nrows, c->omg, Yrows, eta, ybeta);
+      launch_csr_ssign_y(c, rowptr, col, val, col_offset, nrows, c->omg, c->Y + row0, c->m, eta, ybeta);
     }
     y_rows_mark(c, row0, row0 + nrows);
     if (c->spd) return;
@@ -409,9 +377,8 @@ void csr_update(skema_ctx* c, const int64_t* rowptr, const int32_t* col, const f
     const int64_t nue = ur.second - ur.first, npe = pr.second - pr.first;
     if (nue + npe > 0) {
       StageScope st(c, ST_ENTRIES);
-      const int threads = 256;
       const int grid = grid_cap(c, (nue + npe + 7) / 8, 8);
-      csr_ssign_entries_kernel<<<grid, threads, 0, c->stream>>>(
+      csr_ssign_entries_kernel<<<grid, 256, 0, c->stream>>>(
           rowptr, col, val, col_offset, row0, W, nwin, eta, nu, c->ups.d_inv_row + ur.first,
           c->ups.d_inv_rs + ur.first, nue, c->phi.d_inv_row + pr.first, c->phi.d_inv_rs + pr.first,
           npe, c->psi.packed, c->psi.zeta, c->X, c->n, c->Z, c->s);
@@ -427,18 +394,24 @@ void csr_update(skema_ctx* c, const int64_t* rowptr, const int32_t* col, const f
     const int64_t wr = std::min(W, nrows - r);
     const int64_t R0 = row0 + r;
     const float yb = y_rows_clean(c, R0, R0 + wr) ? 0.f : nu;
-    csr_gauss_y_kernel<<<grid_cap(c, (wr + 7) / 8, 16), threads, 0, c->stream>>>(
-        rowptr + r, col, val, col_offset, wr, c->n, c->omg.f32, c->k, c->Y + R0 * c->k, eta, yb);
-    SKEMA_LAUNCHED(c);
+    {
+      StageScope st(c, ST_OMEGA);
+      csr_gauss_y_kernel<<<grid_cap(c, (wr + 7) / 8, 16), threads, 0, c->stream>>>(
+          rowptr + r, col, val, col_offset, wr, c->n, c->omg.f32, c->k, c->Y + R0, c->m, eta, yb);
+      SKEMA_LAUNCHED(c);
+    }
     y_rows_mark(c, R0, R0 + wr);
     if (c->spd) continue;
-    // X = nu X + eta (A_w^T Upsilon_stored(R0:R0+wr, :))^T
-    scale_block(c, MatOut{c->X, c->n, 1}, c->k, c->n, nu);
-    csr_gauss_scatter_kernel<<<grid_cap(c, (wr + 7) / 8, 16), threads, 0, c->stream>>>(
-        rowptr + r, col, val, col_offset, wr, c->n, c->ups.f32 + R0 * c->k, c->k, c->X, c->n, 1, eta);
-    SKEMA_LAUNCHED(c);
+    {  // X = nu X + eta (A_w^T Upsilon_stored(R0:R0+wr, :))^T
+      StageScope st(c, ST_UPSILON);
+      scale_block(c, MatOut{c->X, c->n, 1}, c->k, c->n, nu);
+      csr_gauss_scatter_kernel<<<grid_cap(c, (wr + 7) / 8, 16), threads, 0, c->stream>>>(
+          rowptr + r, col, val, col_offset, wr, c->n, c->ups.f32 + R0 * c->k, c->k, c->X, c->n, 1, eta);
+      SKEMA_LAUNCHED(c);
+    }
     // W^T = A_w^T Phi_stored(R0:R0+wr, :) in scratch (n x s), then
     // Z = nu Z + eta W Psi_stored.
+    StageScope st(c, ST_PHI);
     float* Wt = (float*)workspace(c, sizeof(float) * (size_t)(c->n * c->s));
     SKEMA_CUDA(cudaMemsetAsync(Wt, 0, sizeof(float) * (size_t)(c->n * c->s), c->stream));
     csr_gauss_scatter_kernel<<<grid_cap(c, (wr + 7) / 8, 16), threads, 0, c->stream>>>(
@@ -455,13 +428,12 @@ void csr_update(skema_ctx* c, const int64_t* rowptr, const int32_t* col, const f
 void dense_ssign_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr) {
   const float eta = (float)c->p.sketch_eta, nu = (float)c->p.sketch_nu;
   const float ybeta = y_rows_clean(c, R0, R0 + wr) ? 0.f : nu;
-  const size_t smem = sizeof(float) * 32 * (size_t)c->k;
-  if (smem > 200 * 1024) fail(SKEMA_EUNSUPPORTED, "sketch range too large for the dense sparse-sign kernel");
-  SKEMA_CUDA(cudaFuncSetAttribute(dense_ssign_y_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)smem));
-  dense_ssign_y_kernel<<<grid_cap(c, (wr + 31) / 32, 4), 256, smem, c->stream>>>(
-      Aw.p, Aw.rs, Aw.cs, wr, c->omg.packed, c->omg.zeta, c->k, c->Y + R0 * c->k, eta, ybeta);
-  SKEMA_LAUNCHED(c);
+  {
+    StageScope st(c, ST_OMEGA);
+    dense_ssign_y_kernel<<<grid_cap(c, (wr * c->k + 255) / 256, 16), 256, 0, c->stream>>>(
+        Aw.p, Aw.rs, Aw.cs, wr, c->omg.packed, c->omg.zeta, c->k, c->Y + R0, c->m, eta, ybeta);
+    SKEMA_LAUNCHED(c);
+  }
   y_rows_mark(c, R0, R0 + wr);
   scale_block(c, MatOut{c->X, c->n, 1}, c->k, c->n, nu);
   scale_block(c, MatOut{c->Z, c->s, 1}, c->s, c->s, nu);
@@ -469,6 +441,7 @@ void dense_ssign_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr) {
   const auto pr = entry_range(c->phi, R0, R0 + wr);
   const int64_t nue = ur.second - ur.first, npe = pr.second - pr.first;
   if (nue + npe == 0) return;
+  StageScope st(c, ST_ENTRIES);
   dense_ssign_entries_kernel<<<grid_cap(c, (nue + npe + 7) / 8, 8), 256, 0, c->stream>>>(
       Aw.p, Aw.rs, Aw.cs, R0, eta, c->ups.d_inv_row + ur.first, c->ups.d_inv_rs + ur.first, nue,
       c->phi.d_inv_row + pr.first, c->phi.d_inv_rs + pr.first, npe, c->psi.packed, c->psi.zeta, c->X,
@@ -479,16 +452,15 @@ void dense_ssign_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr) {
 void spd_ssign_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr) {
   const float eta = (float)c->p.sketch_eta, nu = (float)c->p.sketch_nu;
   const float ybeta = y_rows_clean(c, R0, R0 + wr) ? 0.f : nu;
-  const int64_t kp = c->k | 1;
   int threads = 128;
-  while (threads > 32 && sizeof(float) * (size_t)(threads * kp) > 200 * 1024) threads >>= 1;
-  const size_t smem = sizeof(float) * (size_t)(threads * kp);
+  while (threads > 32 && sizeof(float) * (size_t)(threads * c->k) > 200 * 1024) threads >>= 1;
+  const size_t smem = sizeof(float) * (size_t)(threads * c->k);
   if (smem > 200 * 1024) fail(SKEMA_EUNSUPPORTED, "sketch range too large for the SPD sparse-sign kernel");
   SKEMA_CUDA(cudaFuncSetAttribute(dense_colsparse_y_kernel,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  StageScope st(c, ST_OMEGA);
   dense_colsparse_y_kernel<<<grid_cap(c, (wr + threads - 1) / threads, 4), threads, smem, c->stream>>>(
-      Aw.p, Aw.rs, Aw.cs, wr, c->n, c->omg.packed, c->omg.zeta, c->k, kp, c->Y + R0 * c->k, eta,
-      ybeta);
+      Aw.p, Aw.rs, Aw.cs, wr, c->n, c->omg.packed, c->omg.zeta, c->k, c->Y + R0, c->m, eta, ybeta);
   SKEMA_LAUNCHED(c);
   y_rows_mark(c, R0, R0 + wr);
 }
