@@ -192,6 +192,23 @@ int skema_rbf_sketch_vjp(skema_ctx* ctx, const float* pts, int64_t npts,
                          int64_t k, const float* Ybar, float* dpts,
                          double* dgamma);
 
+/* Allocation-free form of skema_rbf_sketch_fwd (no counterpart in the
+ * reference): same arguments and result, for callers that must not have a
+ * library allocate device memory -- a host framework that owns all device
+ * memory through its own pool or memory cap, or a latency-critical loop in
+ * which cudaMalloc's implicit device-wide synchronisation would stall other
+ * streams. Instead of the context workspace it uses one static 16 MiB
+ * scratch array compiled into the library (every GPU that loads the library
+ * holds it until the process exits), in kernel row blocks of
+ * floor(4194304 / npts) rows, and calls no cudaMalloc or cudaFree.
+ * Limit: npts <= 4194304, else SKEMA_EINVAL. The first call on a device
+ * looks up the array's device address (cudaGetSymbolAddress); make that
+ * first call before any stream capture. All calls share the array: calls
+ * that overlap on the GPU race and must be serialised by the caller. */
+int skema_rbf_sketch_fwd_noalloc(skema_ctx* ctx, const float* pts,
+                                 int64_t npts, int64_t d, double gamma,
+                                 const float* omega, int64_t k, float* Y);
+
 /* Wait for all work queued on ctx's stream. */
 int skema_synchronize(skema_ctx* ctx);
 

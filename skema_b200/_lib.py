@@ -83,6 +83,7 @@ SIGNATURES = {
     "skema_map_import": (C.c_int, [_P, _I32, _P, _P]),
     "skema_rbf_sketch_fwd": (C.c_int, [_P, _P, _I64, _I64, _D, _P, _I64, _P]),
     "skema_rbf_sketch_vjp": (C.c_int, [_P, _P, _I64, _I64, _D, _P, _I64, _P, _P, _P]),
+    "skema_rbf_sketch_fwd_noalloc": (C.c_int, [_P, _P, _I64, _I64, _D, _P, _I64, _P]),
     "skema_synchronize": (C.c_int, [_P]),
     "skema_set_stream": (C.c_int, [_P, _P]),
     "skema_launch_count": (_I64, [_P]),

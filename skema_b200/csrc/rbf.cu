@@ -169,6 +169,11 @@ int64_t rows_per_block(int64_t N, int64_t cap_rows) {
 
 }  // namespace
 
+void rbf_window_block(skema_ctx* c, Mat P, int64_t N, int64_t d, float gamma, int64_t R0,
+                      int64_t wr, float* out, int64_t ldo) {
+  launch_tile(c, 0, P, N, d, gamma, R0, wr, out, ldo, nullptr, nullptr, nullptr);
+}
+
 void rbf_update(skema_ctx* c, Mat P, int64_t npts, int64_t d, int64_t row0, int64_t nrows) {
   const int64_t W = c->w;
   const int64_t N = npts;
