@@ -27,6 +27,19 @@ void cuda_check(cudaError_t e, const char* what) {
   }
 }
 
+void check_device_error(skema_ctx* c) {
+  if (!c->dev_err_armed || !c->dev_err) return;
+  int h = 0;
+  SKEMA_CUDA(cudaMemcpyAsync(&h, c->dev_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  SKEMA_CUDA(cudaStreamSynchronize(c->stream));
+  c->dev_err_armed = false;
+  if (h != 0) {
+    SKEMA_CUDA(cudaMemsetAsync(c->dev_err, 0, sizeof(int), c->stream));
+    SKEMA_CUDA(cudaStreamSynchronize(c->stream));
+    fail(SKEMA_ETIMEOUT, "a tensor-core kernel gave up waiting on its pipeline; the sketches are invalid");
+  }
+}
+
 void* workspace(skema_ctx* c, size_t bytes) {
   if (bytes <= c->ws_bytes) return c->ws;
   if (c->ws) {
@@ -158,8 +171,11 @@ static void free_all(skema_ctx* c) {
   if (c->Z) cudaFree(c->Z);
   if (c->ws) cudaFree(c->ws);
   if (c->stage) cudaFree(c->stage);
+  if (c->op16) cudaFree(c->op16);
+  if (c->dev_err) cudaFree(c->dev_err);
   c->X = c->Y = c->Z = nullptr;
-  c->ws = c->stage = nullptr;
+  c->ws = c->stage = c->op16 = nullptr;
+  c->dev_err = nullptr;
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   c->own_stream = nullptr;
 }
@@ -318,7 +334,10 @@ int skema_create(const skema_params* p, skema_ctx** out) {
         map_build_inverse(c, c->ups);
         map_build_inverse(c, c->phi);
       }
+      tc_prepare_maps(c);
     }
+    SKEMA_CUDA(cudaMalloc(&c->dev_err, sizeof(int)));
+    SKEMA_CUDA(cudaMemsetAsync(c->dev_err, 0, sizeof(int), c->stream));
     if (!c->spd) {
       SKEMA_CUDA(cudaMalloc(&c->X, sizeof(float) * (size_t)(c->k * c->n)));
       SKEMA_CUDA(cudaMalloc(&c->Z, sizeof(float) * (size_t)(c->s * c->s)));
@@ -484,6 +503,7 @@ int skema_low_rank_approx(skema_ctx* c, double* U, double* S, double* V, int32_t
     if (c->s < c->k) fail(SKEMA_EINVAL, "core must be >= range");
     const int64_t r = c->p.rank;
     if (r > c->k) fail(SKEMA_EINVAL, "rank must not exceed range");
+    check_device_error(c);
     if (mem == SKEMA_MEM_DEVICE) {
       low_rank_approx(c, U, S, V);
       return;
@@ -528,6 +548,7 @@ int skema_get_sketch(skema_ctx* c, int32_t which, float* buf, int64_t ld, int32_
     int64_t rows, cols;
     sketch_shape(c, which, &src, &rows, &cols);
     check_dense_args(buf, ld, layout, rows, cols, mem);
+    check_device_error(c);
     if (which == SKEMA_SKETCH_Y) y_materialize(c);
     const bool irow = sketch_row_major(which);
     const int64_t inner = irow ? cols : rows, outer = irow ? rows : cols;
@@ -629,6 +650,7 @@ int skema_map_import(skema_ctx* c, int32_t which, const double* values, const in
   return guarded(c, [&] {
     Map* mp = map_of(c, which);
     map_import(c, *mp, values, indices);
+    tc_prepare_maps(c);
   });
 }
 
@@ -654,12 +676,16 @@ int skema_rbf_sketch_vjp(skema_ctx* c, const float* pts, int64_t npts, int64_t d
 }
 
 int skema_synchronize(skema_ctx* c) {
-  return guarded(c, [&] { SKEMA_CUDA(cudaStreamSynchronize(c->stream)); });
+  return guarded(c, [&] {
+    SKEMA_CUDA(cudaStreamSynchronize(c->stream));
+    check_device_error(c);
+  });
 }
 
 int skema_set_stream(skema_ctx* c, void* stream) {
   return guarded(c, [&] {
     SKEMA_CUDA(cudaStreamSynchronize(c->stream));
+    check_device_error(c);
     c->stream = stream ? (cudaStream_t)stream : c->own_stream;
   });
 }

@@ -19,9 +19,6 @@
 
 namespace skema {
 
-bool tc_available(const skema_ctx* c);
-void tc_dense_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr, float* T);
-
 static int splitk_for(const skema_ctx* c, int64_t M, int64_t N, int64_t K) {
   const int64_t tiles = ((M + 127) / 128) * ((N + 127) / 128);
   int64_t sk = (2 * c->sm_count + tiles - 1) / tiles;
@@ -83,7 +80,7 @@ void dense_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr, float* T) {
     return;
   }
   if (c->p.precision != SKEMA_PREC_FP32) {
-    if (!tc_available(c)) fail(SKEMA_EUNSUPPORTED, "tensor-core sketch not available for this shape");
+    if (!tc_available(c)) fail(SKEMA_EUNSUPPORTED, "this precision is not available for this sketch");
     tc_dense_window(c, Aw, R0, wr, T);
     return;
   }
@@ -92,6 +89,7 @@ void dense_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr, float* T) {
 
 size_t dense_scratch_bytes(const skema_ctx* c, int64_t wr) {
   if (c->spd || c->p.dim_redux == SKEMA_MAP_SPARSE_SIGN) return 256;
+  if (tc_available(c)) return tc_scratch_bytes(c, wr);
   return sizeof(float) * (size_t)(wr * c->s) + 256;
 }
 

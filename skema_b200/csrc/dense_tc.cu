@@ -1,18 +1,340 @@
-// dense_tc.cu -- tensor-core (tcgen05) forms of the dense Gauss sketch.
+// dense_tc.cu -- the BF16 tensor-core form of the dense Gauss sketch
+// (update(dense, Gauss), src/Skema_SketchySVD.cpp:256-268).
+//
+// Per window A_w (rows [R0, R0+wr)), FP32 accumulation throughout:
+//   A16          = bf16(A_w)                    column-major, ld wp = pad8(wr)
+//   [Y_w | T]    = A16 [Omega~; Psi~]^T         M = wr, N = k + s, K = n
+//                  (Y_w -> Y with eta / nu, T -> BF16 scratch, column-major)
+//   X^T          = nu X^T + eta A16^T Upsilon~_w^T   M = n, N = k, K = wr
+//   Z^T          = nu Z^T + eta T^T Phi~_w^T         M = s, N = s, K = wr
+// Each product is oriented so that its output's contiguous dimension runs
+// along the tile rows (TMEM lanes): Y and T are column-major, X and Z
+// row-major, so X^T and Z^T are the products that store coalesced.
+// The maps are kept as BF16 row-major copies (Upsilon~ k x m, Phi~ s x m,
+// and Omega~ / Psi~ stacked into one (k+s) x n operand); every BF16 row
+// stride is padded to a multiple of 8 elements (16 bytes) for TMA.
+//
+// Split-K: with one 128-row CTA per SM a product with few tiles leaves SMs
+// idle (157 X tiles on 148 SMs is two waves, the second nearly empty), so K
+// is split when that shortens the critical path; the split partial sums are
+// added with FP32 atomics into outputs scaled by nu beforehand.
+#include <cuda.h>
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <mutex>
 
 #include "internal.h"
+#include "tc_gemm.cuh"
 
 namespace skema {
 
-bool tc_available(const skema_ctx* c) {
-  (void)c;
-  return false;
+namespace {
+
+constexpr int kNT = 208;  // N tile of every product (k = 201, s = 403 pad to 208 / 416)
+
+int64_t pad8(int64_t x) { return (x + 7) / 8 * 8; }
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  if (!fn) fail(SKEMA_ENOKERNEL, "cuTensorMapEncodeTiled is not available from the driver");
+  return fn;
 }
 
-void tc_dense_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr, float* T) {
-  (void)c, (void)Aw, (void)R0, (void)wr, (void)T;
-  fail(SKEMA_EUNSUPPORTED, "tensor-core sketch not built");
+// 2-D BF16 tensor map: dim0 contiguous (extent d0), dim1 with byte stride
+// st1, box {b0, b1}, 128-byte swizzle, out-of-range elements read as zero.
+CUtensorMap tmap_bf16(const void* base, uint64_t d0, uint64_t d1, uint64_t st1, uint32_t b0, uint32_t b1) {
+  if (reinterpret_cast<uintptr_t>(base) % 16) fail(SKEMA_EINVAL, "TMA base address not 16-byte aligned");
+  if (st1 % 16) fail(SKEMA_EINVAL, "TMA row stride not a multiple of 16 bytes");
+  CUtensorMap tm;
+  cuuint64_t dims[2] = {d0, d1};
+  cuuint64_t strides[1] = {st1};
+  cuuint32_t box[2] = {b0, b1};
+  cuuint32_t es[2] = {1, 1};
+  const CUresult r = encode_fn()(&tm, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims,
+                                 strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                 CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) fail(SKEMA_EINVAL, "cuTensorMapEncodeTiled rejected a tensor map");
+  return tm;
+}
+
+// Column-major FP32 block (srs == 1, 16-byte aligned columns) -> BF16
+// column-major, eight rows per thread: one read and one write pass.
+__global__ void to_bf16_cm_vec_kernel(const float* __restrict__ S, int64_t scs, int64_t rows, int64_t cols,
+                                      __nv_bfloat16* __restrict__ D, int64_t ld) {
+  const int64_t r8 = (rows + 7) / 8;
+  const int64_t total = r8 * cols;
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < total;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t j = q / r8, i = (q - j * r8) * 8;
+    const float* sp = S + i + j * scs;
+    float v[8];
+    if (i + 8 <= rows) {
+      const float4 a = __ldcs(reinterpret_cast<const float4*>(sp));
+      const float4 b = __ldcs(reinterpret_cast<const float4*>(sp + 4));
+      v[0] = a.x, v[1] = a.y, v[2] = a.z, v[3] = a.w, v[4] = b.x, v[5] = b.y, v[6] = b.z, v[7] = b.w;
+    } else {
+      for (int t = 0; t < 8; ++t) v[t] = (i + t < rows) ? sp[t] : 0.f;
+    }
+    __nv_bfloat162 h[4];
+#pragma unroll
+    for (int t = 0; t < 4; ++t) h[t] = __floats2bfloat162_rn(v[2 * t], v[2 * t + 1]);
+    *reinterpret_cast<uint4*>(D + i + j * ld) = *reinterpret_cast<const uint4*>(h);
+  }
+}
+
+// Any strided FP32 block -> BF16 with D(i, j) at D[i * drs + j * dcs], by
+// 32 x 32 tiles through shared memory so that both the read (along the
+// source's unit stride) and the write (along the destination's) coalesce.
+__global__ void to_bf16_tiled_kernel(const float* __restrict__ S, int64_t srs, int64_t scs, int64_t rows,
+                                     int64_t cols, __nv_bfloat16* __restrict__ D, int64_t drs, int64_t dcs) {
+  __shared__ float tile[32][33];
+  const int64_t ti = (rows + 31) / 32, tj = (cols + 31) / 32;
+  const bool s_rowfast = srs <= scs;  // source unit stride along i
+  const bool d_rowfast = drs <= dcs;
+  for (int64_t t = blockIdx.x; t < ti * tj; t += gridDim.x) {
+    const int64_t i0 = (t % ti) * 32, j0 = (t / ti) * 32;
+    for (int q = threadIdx.y; q < 32; q += blockDim.y) {
+      const int64_t i = s_rowfast ? i0 + threadIdx.x : i0 + q;
+      const int64_t j = s_rowfast ? j0 + q : j0 + threadIdx.x;
+      const float v = (i < rows && j < cols) ? S[i * srs + j * scs] : 0.f;
+      if (s_rowfast)
+        tile[threadIdx.x][q] = v;
+      else
+        tile[q][threadIdx.x] = v;
+    }
+    __syncthreads();
+    for (int q = threadIdx.y; q < 32; q += blockDim.y) {
+      const int64_t i = d_rowfast ? i0 + threadIdx.x : i0 + q;
+      const int64_t j = d_rowfast ? j0 + q : j0 + threadIdx.x;
+      const float v = d_rowfast ? tile[threadIdx.x][q] : tile[q][threadIdx.x];
+      if (i < rows && j < cols) D[i * drs + j * dcs] = __float2bfloat16(v);
+    }
+    __syncthreads();
+  }
+}
+
+void to_bf16(skema_ctx* c, Mat src, int64_t rows, int64_t cols, __nv_bfloat16* D, int64_t drs, int64_t dcs) {
+  if (rows <= 0 || cols <= 0) return;
+  const bool vec = src.rs == 1 && drs == 1 && src.cs % 4 == 0 && dcs % 8 == 0 &&
+                   reinterpret_cast<uintptr_t>(src.p) % 16 == 0 && reinterpret_cast<uintptr_t>(D) % 16 == 0;
+  if (vec) {
+    const int64_t work = ((rows + 7) / 8) * cols;
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((work + 255) / 256, (int64_t)c->sm_count * 16));
+    to_bf16_cm_vec_kernel<<<grid, 256, 0, c->stream>>>(src.p, src.cs, rows, cols, D, dcs);
+  } else {
+    const int64_t tiles = ((rows + 31) / 32) * ((cols + 31) / 32);
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(tiles, (int64_t)c->sm_count * 16));
+    to_bf16_tiled_kernel<<<grid, dim3(32, 8), 0, c->stream>>>(src.p, src.rs, src.cs, rows, cols, D, drs, dcs);
+  }
+  SKEMA_LAUNCHED(c);
+}
+
+// BF16 column-major (ld) <- FP32 column-major (ld), rows x cols.
+__global__ void f32_to_bf16_cm_kernel(const float* __restrict__ S, __nv_bfloat16* __restrict__ D, int64_t rows,
+                                      int64_t cols, int64_t ld) {
+  const int64_t total = rows * cols;
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < total;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t j = q / rows, i = q - j * rows;
+    D[i + j * ld] = __float2bfloat16(S[i + j * ld]);
+  }
+}
+
+struct Plan {
+  int ks;
+  int64_t kchunk;
+};
+
+// Split of K that minimises the estimated critical path in k-steps: waves of
+// one CTA per SM times the k-steps of one split, plus a fixed cost per tile
+// for the pipeline fill and the epilogue.
+Plan plan_split(const skema_ctx* c, int64_t tiles, int64_t K, int max_ks) {
+  const int64_t ksteps = (K + tc::BK - 1) / tc::BK;
+  int best = 1;
+  double best_cost = 1e300;
+  for (int ks = 1; ks <= max_ks; ++ks) {
+    if (ks > 1 && ksteps / ks < 8) break;  // at least 8 k-steps per split
+    const int64_t waves = (tiles * ks + c->sm_count - 1) / c->sm_count;
+    const double cost = (double)waves * ((double)ksteps / ks + 6.0);
+    if (cost < best_cost * 0.97) {
+      best_cost = cost;
+      best = ks;
+    }
+  }
+  const int64_t kchunk = (ksteps + best - 1) / best * tc::BK;
+  const int ks = (int)((K + kchunk - 1) / kchunk);
+  return Plan{ks, kchunk};
+}
+
+template <bool A_MN>
+void launch_gemm(skema_ctx* c, const CUtensorMap& ta, const CUtensorMap& tb, int64_t M, int64_t N, int64_t K,
+                 Plan pl, int m_fast, const tc::OutSpec& o) {
+  constexpr int S = 4;
+  constexpr uint32_t STAGE = ((tc::BM * tc::BK * 2 + kNT * tc::BK * 2 + 1023) / 1024) * 1024;
+  const size_t smem = (size_t)S * STAGE + 1024 + 256;
+  auto kern = tc::gemm_bf16_kernel<kNT, S, A_MN>;
+  SKEMA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  tc::Grid3 g;
+  g.mtiles = (int)((M + tc::BM - 1) / tc::BM);
+  g.ntiles = (int)((N + kNT - 1) / kNT);
+  g.ksplit = pl.ks;
+  g.m_fast = m_fast;
+  const int64_t grid = (int64_t)g.mtiles * g.ntiles * g.ksplit;
+  if (grid <= 0 || K <= 0) return;
+  if (grid > 0x7fffffff) fail(SKEMA_EINVAL, "tensor-core grid too large");
+  kern<<<(unsigned)grid, tc::kThreads, smem, c->stream>>>(ta, tb, K, pl.kchunk, g, o, c->dev_err);
+  SKEMA_LAUNCHED(c);
+  c->dev_err_armed = true;
+}
+
+tc::OutSpec out_spec() {
+  tc::OutSpec o;
+  o.p0 = nullptr, o.p1 = nullptr, o.p1f = nullptr;
+  o.rs0 = o.cs0 = o.rs1 = o.cs1 = 0;
+  o.alpha0 = 1.f, o.beta0 = 0.f, o.alpha1 = 1.f, o.beta1 = 0.f;
+  o.rows = 0, o.split = 0, o.ncols = 0;
+  o.atomic0 = 0, o.atomic1 = 0;
+  return o;
+}
+
+}  // namespace
+
+bool tc_available(const skema_ctx* c) {
+  return c->p.precision == SKEMA_PREC_BF16 && c->ups.lowp && c->phi.lowp && c->op16;
+}
+
+// BF16 copies of the Gauss maps for the tensor-core form (dense and kernel
+// inputs); called after the maps are generated and after each map import.
+void tc_prepare_maps(skema_ctx* c) {
+  if (c->p.precision != SKEMA_PREC_BF16 || c->spd || c->p.issparse || c->p.dim_redux != SKEMA_MAP_GAUSS)
+    return;
+  const int64_t mp = pad8(c->m), np = pad8(c->n);
+  if (!c->ups.lowp) {
+    SKEMA_CUDA(cudaMalloc(&c->ups.lowp, sizeof(__nv_bfloat16) * (size_t)(c->k * mp)));
+    SKEMA_CUDA(cudaMalloc(&c->phi.lowp, sizeof(__nv_bfloat16) * (size_t)(c->s * mp)));
+    SKEMA_CUDA(cudaMalloc(&c->op16, sizeof(__nv_bfloat16) * (size_t)((c->k + c->s) * np)));
+  }
+  c->ld_maps16 = mp;
+  c->ld_op16 = np;
+  auto conv = [&](const Map& M, void* dst, int64_t ld) {
+    to_bf16(c, Mat{M.f32, M.rs, M.cs}, M.lrows, M.lcols, static_cast<__nv_bfloat16*>(dst), ld, 1);
+  };
+  conv(c->ups, c->ups.lowp, mp);
+  conv(c->phi, c->phi.lowp, mp);
+  conv(c->omg, c->op16, np);
+  conv(c->psi, static_cast<__nv_bfloat16*>(c->op16) + c->k * np, np);
+}
+
+size_t tc_scratch_bytes(const skema_ctx* c, int64_t wr) {
+  const int64_t wp = pad8(wr);
+  size_t b = sizeof(__nv_bfloat16) * (size_t)(wp * c->n) + 256;         // A16
+  b += sizeof(__nv_bfloat16) * (size_t)(wp * c->s) + 256;               // T16
+  b += sizeof(float) * (size_t)(wp * c->s) + 256;                       // T32 (split-K)
+  b += sizeof(__nv_bfloat16) * (size_t)((c->k + c->s) * wp) + 512;      // map slices (unaligned R0)
+  return b;
+}
+
+void tc_dense_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr, void* scratch) {
+  const float eta = (float)c->p.sketch_eta, nu = (float)c->p.sketch_nu;
+  const int64_t k = c->k, s = c->s, n = c->n, m = c->m;
+  const int64_t wp = pad8(wr);
+  char* sp = static_cast<char*>(scratch);
+  auto take = [&](size_t bytes) {
+    char* p = sp;
+    sp += (bytes + 255) / 256 * 256;
+    return p;
+  };
+  __nv_bfloat16* A16 = reinterpret_cast<__nv_bfloat16*>(take(sizeof(__nv_bfloat16) * (size_t)(wp * n)));
+  __nv_bfloat16* T16 = reinterpret_cast<__nv_bfloat16*>(take(sizeof(__nv_bfloat16) * (size_t)(wp * s)));
+  float* T32 = reinterpret_cast<float*>(take(sizeof(float) * (size_t)(wp * s)));
+  const float ybeta = y_rows_clean(c, R0, R0 + wr) ? 0.f : nu;
+
+  {  // A16 = bf16(A_w)
+    StageScope st(c, ST_WINDOW);
+    to_bf16(c, Aw, wr, n, A16, 1, wp);
+  }
+  // Upsilon~ / Phi~ columns of this window: in place when R0 keeps the
+  // 16-byte alignment TMA needs, else converted into an aligned slice.
+  const __nv_bfloat16* U16 = static_cast<const __nv_bfloat16*>(c->ups.lowp) + R0;
+  const __nv_bfloat16* F16 = static_cast<const __nv_bfloat16*>(c->phi.lowp) + R0;
+  int64_t ldm = c->ld_maps16;
+  if (R0 % 8 != 0) {
+    __nv_bfloat16* us = reinterpret_cast<__nv_bfloat16*>(take(sizeof(__nv_bfloat16) * (size_t)(k * wp)));
+    __nv_bfloat16* fs = reinterpret_cast<__nv_bfloat16*>(take(sizeof(__nv_bfloat16) * (size_t)(s * wp)));
+    to_bf16(c, Mat{c->ups.f32 + R0 * c->ups.cs, c->ups.rs, c->ups.cs}, k, wr, us, wp, 1);
+    to_bf16(c, Mat{c->phi.f32 + R0 * c->phi.cs, c->phi.rs, c->phi.cs}, s, wr, fs, wp, 1);
+    U16 = us;
+    F16 = fs;
+    ldm = wp;
+  }
+  const uint64_t wp2 = (uint64_t)wp * 2;
+  {  // [Y_w | T] = A16 [Omega~; Psi~]^T
+    StageScope st(c, ST_FUSED);
+    const CUtensorMap ta = tmap_bf16(A16, (uint64_t)wr, (uint64_t)n, wp2, 64, 64);
+    const CUtensorMap tb = tmap_bf16(c->op16, (uint64_t)n, (uint64_t)(k + s), (uint64_t)c->ld_op16 * 2, 64, kNT);
+    const int64_t tiles = ((wr + 127) / 128) * ((k + s + kNT - 1) / kNT);
+    const Plan pl = plan_split(c, tiles, n, 8);
+    tc::OutSpec o = out_spec();
+    o.p0 = c->Y + R0, o.rs0 = 1, o.cs0 = m, o.alpha0 = eta, o.beta0 = ybeta;
+    o.rows = wr, o.split = k, o.ncols = k + s;
+    if (pl.ks == 1) {
+      o.p1 = T16, o.rs1 = 1, o.cs1 = wp;
+    } else {
+      scale_block(c, MatOut{c->Y + R0, 1, m}, wr, k, ybeta);
+      SKEMA_CUDA(cudaMemsetAsync(T32, 0, sizeof(float) * (size_t)(wp * s), c->stream));
+      o.atomic0 = 1, o.beta0 = 0.f;
+      o.p1f = T32, o.rs1 = 1, o.cs1 = wp, o.atomic1 = 1;
+    }
+    launch_gemm<true>(c, ta, tb, wr, k + s, n, pl, 0, o);
+    if (pl.ks > 1) {
+      const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((wr * s + 255) / 256, c->sm_count * 16));
+      f32_to_bf16_cm_kernel<<<grid, 256, 0, c->stream>>>(T32, T16, wr, s, wp);
+      SKEMA_LAUNCHED(c);
+    }
+  }
+  y_rows_mark(c, R0, R0 + wr);
+  {  // X^T = nu X^T + eta A16^T Upsilon~_w^T
+    StageScope st(c, ST_UPSILON);
+    const CUtensorMap ta = tmap_bf16(A16, (uint64_t)wr, (uint64_t)n, wp2, 64, 128);
+    const CUtensorMap tb = tmap_bf16(U16, (uint64_t)wr, (uint64_t)k, (uint64_t)ldm * 2, 64, kNT);
+    const int64_t tiles = ((n + 127) / 128) * ((k + kNT - 1) / kNT);
+    const Plan pl = plan_split(c, tiles, wr, 8);
+    tc::OutSpec o = out_spec();
+    o.p0 = c->X, o.rs0 = 1, o.cs0 = n, o.alpha0 = eta, o.beta0 = nu;
+    o.rows = n, o.split = k, o.ncols = k;
+    if (pl.ks > 1) {
+      scale_block(c, MatOut{c->X, n, 1}, k, n, nu);
+      o.atomic0 = 1, o.beta0 = 0.f;
+    }
+    launch_gemm<false>(c, ta, tb, n, k, wr, pl, 1, o);
+  }
+  {  // Z^T = nu Z^T + eta T^T Phi~_w^T
+    StageScope st(c, ST_PHI);
+    const CUtensorMap ta = tmap_bf16(T16, (uint64_t)wr, (uint64_t)s, wp2, 64, 128);
+    const CUtensorMap tb = tmap_bf16(F16, (uint64_t)wr, (uint64_t)s, (uint64_t)ldm * 2, 64, kNT);
+    const int64_t tiles = ((s + 127) / 128) * ((s + kNT - 1) / kNT);
+    const Plan pl = plan_split(c, tiles, wr, 32);
+    tc::OutSpec o = out_spec();
+    o.p0 = c->Z, o.rs0 = 1, o.cs0 = s, o.alpha0 = eta, o.beta0 = nu;
+    o.rows = s, o.split = s, o.ncols = s;
+    if (pl.ks > 1) {
+      scale_block(c, MatOut{c->Z, s, 1}, s, s, nu);
+      o.atomic0 = 1, o.beta0 = 0.f;
+    }
+    launch_gemm<false>(c, ta, tb, s, s, wr, pl, 0, o);
+  }
 }
 
 }  // namespace skema

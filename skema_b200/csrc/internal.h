@@ -110,6 +110,15 @@ struct skema_ctx {
   size_t stage_bytes = 0;
   int sm_count = 148;
   int cc_major = 0, cc_minor = 0;
+  // BF16 tensor-core form: Omega~ and Psi~ stacked as one (k+s) x n
+  // row-major operand (ld_op16), Upsilon~ / Phi~ copies in Map::lowp with
+  // ld_maps16; padded row strides are multiples of 8 elements.
+  void* op16 = nullptr;
+  int64_t ld_op16 = 0, ld_maps16 = 0;
+  // Device status word of the bounded waits in the tensor-core kernels
+  // (non-zero: a wait timed out); checked at the next synchronising call.
+  int* dev_err = nullptr;
+  bool dev_err_armed = false;
   // stage timers
   bool timing = false;
   std::vector<skema::PendingTimer> pending;
@@ -176,6 +185,15 @@ void dense_update(skema_ctx* c, Mat A, int64_t row0, int64_t nrows);
 // the input; T is the scratch returned for dense_scratch_bytes(c, wr).
 void dense_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr, float* T);
 size_t dense_scratch_bytes(const skema_ctx* c, int64_t wr);
+
+// ---- BF16 tensor-core form (dense_tc.cu) ----
+bool tc_available(const skema_ctx* c);
+void tc_prepare_maps(skema_ctx* c);
+size_t tc_scratch_bytes(const skema_ctx* c, int64_t wr);
+void tc_dense_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr, void* scratch);
+// Reads the tensor-core status word (synchronises the stream) and fails with
+// SKEMA_ETIMEOUT if a kernel gave up on a wait since the last check.
+void check_device_error(skema_ctx* c);
 
 // ---- sparse paths (sparse.cu) ----
 void csr_update(skema_ctx* c, const int64_t* rowptr, const int32_t* col,

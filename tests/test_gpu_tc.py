@@ -1,0 +1,129 @@
+"""GPU parity tests of the BF16 tensor-core form of the dense Gauss sketch.
+
+The input window and the maps are rounded to BF16 (8-bit significand,
+unit roundoff 2^-9) and every product accumulates in FP32, so the sketches
+are compared with the FP64 oracle on the same inputs and maps at a relative
+Frobenius tolerance of 6e-3: about three times the error of one rounding of
+each operand of a sum of random-signed terms. Z sees two roundings (T is
+kept in BF16 between its two products) and gets 1e-2.
+
+Shapes cover: windows whose first row is and is not a multiple of 8 (the
+Upsilon / Phi window slices are TMA operands in place or copied), row- and
+column-major host input, device input, split-K (the rank-50 shape: k = 201,
+s = 403, 24 output tiles per product) with eta / nu and two update calls,
+and the Gauss RBF kernel input.
+"""
+import numpy as np
+import pytest
+
+from conftest import rel_fro
+from test_gpu_sketch import alg, dense_input, oracle_for
+
+pytestmark = pytest.mark.gpu
+
+TOL_XY = 6e-3
+TOL_Z = 1e-2
+
+
+@pytest.fixture(scope="module")
+def sk(lib_built):
+    import skema_b200
+
+    return skema_b200
+
+
+def bf16(a, sk):
+    a.precision = sk._lib.PREC_BF16
+    return a
+
+
+def check(s, o, tag=""):
+    X, Y, Z = s.get_sketches()
+    ex, ey, ez = rel_fro(X, o.X), rel_fro(Y, o.Y), rel_fro(Z, o.Z)
+    assert np.isfinite(X).all() and np.isfinite(Y).all() and np.isfinite(Z).all(), tag
+    assert ey < TOL_XY, (tag, "Y", ey)
+    assert ex < TOL_XY, (tag, "X", ex)
+    assert ez < TOL_Z, (tag, "Z", ez)
+    return ex, ey, ez
+
+
+@pytest.mark.parametrize("layout", ["C", "F"])
+def test_dense_bf16_parity(sk, oracle, layout):
+    m, n = 2000, 1000
+    A = dense_input(m, n).astype(np.float32)
+    A = np.asfortranarray(A) if layout == "F" else np.ascontiguousarray(A)
+    a = bf16(alg(sk, m, n, 10, 100, 0), sk)  # windows start at 100, 200, ...: both alignments
+    o = oracle_for(oracle, a)
+    o.linear_update(A.astype(np.float64))
+    with sk.SketchySVD(a) as s:
+        s.linear_update(A)
+        check(s, o, layout)
+
+
+def test_dense_bf16_split_k_eta_nu_two_calls(sk, oracle):
+    import torch
+
+    m, n = 4096, 3000
+    A = dense_input(m, n, seed=11).astype(np.float32)
+    a = bf16(alg(sk, m, n, 50, 2048, 0, sketch_eta=1.25, sketch_nu=0.8), sk)
+    o = oracle_for(oracle, a)
+    o.linear_update(A.astype(np.float64))
+    At = torch.from_numpy(A).cuda()
+    with sk.SketchySVD(a) as s:
+        assert (s.range, s.core) == (201, 403)
+        s.update_rows(At[:2048], 0)
+        s.update_rows(At[2048:], 2048)
+        check(s, o, "split-k")
+
+
+def test_dense_bf16_ragged_window(sk, oracle):
+    m, n = 777, 333
+    A = dense_input(m, n, seed=5).astype(np.float32)
+    a = bf16(alg(sk, m, n, 7, 129, 0, sketch_nu=0.5), sk)  # 129-row windows, last one 3 rows
+    o = oracle_for(oracle, a)
+    o.linear_update(A.astype(np.float64))
+    with sk.SketchySVD(a) as s:
+        s.linear_update(A)
+        check(s, o, "ragged")
+
+
+def test_rbf_bf16_parity(sk, oracle):
+    N, d = 700, 5
+    P = oracle.mixture_points(N, d, seed=1)
+    gamma = oracle.median_gamma(P)
+    a = bf16(alg(sk, N, N, 6, 128, 0, kernel_func=1, kernel_gamma=gamma, force_three_sketch=True), sk)
+    o = oracle_for(oracle, a, gamma=gamma)
+    o.linear_update(P.astype(np.float64))
+    with sk.SketchySVD(a) as s:
+        s.linear_update(P)
+        check(s, o, "rbf")
+
+
+def test_bf16_low_rank_approx(sk, oracle):
+    m, n = 2000, 1000
+    A = dense_input(m, n).astype(np.float32)
+    a32 = alg(sk, m, n, 10, 256, 0)
+    with sk.SketchySVD(a32) as s:
+        s.linear_update(A)
+        _, S32, _ = s.low_rank_approx()
+    with sk.SketchySVD(bf16(alg(sk, m, n, 10, 256, 0), sk)) as s:
+        s.linear_update(A)
+        U, S, V = s.low_rank_approx()
+    assert np.max(np.abs(S - S32)) / S32[0] < 1e-2
+    assert np.allclose(U.T @ U, np.eye(10), atol=1e-8)
+    assert np.allclose(V.T @ V, np.eye(10), atol=1e-8)
+
+
+def test_bf16_map_import_refreshes_copies(sk, oracle):
+    m, n = 512, 256
+    A = dense_input(m, n, seed=8).astype(np.float32)
+    a = bf16(alg(sk, m, n, 4, 128, 0), sk)
+    with sk.SketchySVD(a) as s:
+        v, ix = s.map_export(1)  # Omega~
+        s.map_import(1, -v, ix)
+        s.linear_update(A)
+        Y = s.get_sketch(1)
+    with sk.SketchySVD(bf16(alg(sk, m, n, 4, 128, 0), sk)) as s:
+        s.linear_update(A)
+        Y0 = s.get_sketch(1)
+    assert rel_fro(Y, -Y0) < 1e-6
