@@ -540,9 +540,13 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=12.0)
     ap.add_argument("--clock-lead", type=float, default=1.0, help="seconds of load before the timed steps")
     ap.add_argument("--clock-tail", type=float, default=0.3, help="seconds of load after the timed steps")
+    ap.add_argument("--rows", type=int, default=0,
+                    help="rows per GPU instead of the workload's (small cases for profiling)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     cfg = dict(WORKLOADS[args.workload])
+    if args.rows > 0:
+        cfg["m"] = args.rows
     if args.impl == "reference":
         run_reference(args, cfg)
         return

@@ -2,7 +2,7 @@
 // (update(dense, Gauss), src/Skema_SketchySVD.cpp:256-268).
 //
 // Per window A_w (rows [R0, R0+wr)), FP32 accumulation throughout:
-//   A16          = bf16(A_w)                    column-major, ld wp = pad8(wr)
+//   A16          = bf16(A_w)                    row-blocked (64-row blocks)
 //   [Y_w | T]    = A16 [Omega~; Psi~]^T         M = wr, N = k + s, K = n
 //                  (Y_w -> Y with eta / nu, T -> BF16 scratch, column-major)
 //   X^T          = nu X^T + eta A16^T Upsilon~_w^T   M = n, N = k, K = wr
@@ -69,15 +69,54 @@ CUtensorMap tmap_bf16(const void* base, uint64_t d0, uint64_t d1, uint64_t st1, 
   return tm;
 }
 
-// Column-major FP32 block (srs == 1, 16-byte aligned columns) -> BF16
-// column-major, eight rows per thread: one read and one write pass.
-__global__ void to_bf16_cm_vec_kernel(const float* __restrict__ S, int64_t scs, int64_t rows, int64_t cols,
-                                      __nv_bfloat16* __restrict__ D, int64_t ld) {
-  const int64_t r8 = (rows + 7) / 8;
-  const int64_t total = r8 * cols;
+// 2-D FP32 tensor map, 128-byte swizzle (box inner extent 32), OOB zero.
+CUtensorMap tmap_f32(const void* base, uint64_t d0, uint64_t d1, uint64_t st1, uint32_t b0, uint32_t b1) {
+  if (reinterpret_cast<uintptr_t>(base) % 16) fail(SKEMA_EINVAL, "TMA base address not 16-byte aligned");
+  if (st1 % 16) fail(SKEMA_EINVAL, "TMA row stride not a multiple of 16 bytes");
+  CUtensorMap tm;
+  cuuint64_t dims[2] = {d0, d1};
+  cuuint64_t strides[1] = {st1};
+  cuuint32_t box[2] = {b0, b1};
+  cuuint32_t es[2] = {1, 1};
+  const CUresult r = encode_fn()(&tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void*>(base), dims,
+                                 strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                 CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) fail(SKEMA_EINVAL, "cuTensorMapEncodeTiled rejected an FP32 tensor map");
+  return tm;
+}
+
+// 3-D BF16 tensor map of the row-blocked window: {64, d1, d2} with the
+// 64-element lines contiguous, byte strides 128 (dim1) and d1 * 128 (dim2),
+// box {64, b1, 1}.
+CUtensorMap tmap_bf16_blocked(const void* base, uint64_t d1, uint64_t d2, uint32_t b1) {
+  if (reinterpret_cast<uintptr_t>(base) % 16) fail(SKEMA_EINVAL, "TMA base address not 16-byte aligned");
+  CUtensorMap tm;
+  cuuint64_t dims[3] = {64, d1, d2};
+  cuuint64_t strides[2] = {128, d1 * 128};
+  cuuint32_t box[3] = {64, b1, 1};
+  cuuint32_t es[3] = {1, 1, 1};
+  const CUresult r = encode_fn()(&tm, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<void*>(base), dims,
+                                 strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                 CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) fail(SKEMA_EINVAL, "cuTensorMapEncodeTiled rejected a blocked tensor map");
+  return tm;
+}
+
+// The window in BF16, row-blocked: element (i, j) of a rows x cols block at
+// D[((i / 64) * cols + j) * 64 + i % 64], i.e. for each 64-row block the
+// columns one after another, each a 128-byte line of 64 rows. Rows past
+// `rows` in the last block are written as zeros. A TMA box of 64 rows x
+// 64 or 128 columns is then one contiguous 8 or 16 KB run, read MN-major by
+// the [Y|T] product and K-major by the X product.
+__global__ void to_bf16_blocked_vec_kernel(const float* __restrict__ S, int64_t scs, int64_t rows,
+                                           int64_t cols, __nv_bfloat16* __restrict__ D, int64_t nrb) {
+  const int64_t g8 = nrb * 8;  // 8-row groups, padding included
+  const int64_t total = g8 * cols;
   for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < total;
        q += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t j = q / r8, i = (q - j * r8) * 8;
+    const int64_t j = q / g8, i = (q - j * g8) * 8;
     const float* sp = S + i + j * scs;
     float v[8];
     if (i + 8 <= rows) {
@@ -90,8 +129,59 @@ __global__ void to_bf16_cm_vec_kernel(const float* __restrict__ S, int64_t scs, 
     __nv_bfloat162 h[4];
 #pragma unroll
     for (int t = 0; t < 4; ++t) h[t] = __floats2bfloat162_rn(v[2 * t], v[2 * t + 1]);
-    *reinterpret_cast<uint4*>(D + i + j * ld) = *reinterpret_cast<const uint4*>(h);
+    *reinterpret_cast<uint4*>(D + ((i >> 6) * cols + j) * 64 + (i & 63)) = *reinterpret_cast<const uint4*>(h);
   }
+}
+
+// The same layout from any strided FP32 block, 64 x 32 tiles through shared
+// memory (reads along the source's unit stride, writes 128-byte lines).
+__global__ void to_bf16_blocked_tiled_kernel(const float* __restrict__ S, int64_t srs, int64_t scs, int64_t rows,
+                                             int64_t cols, __nv_bfloat16* __restrict__ D, int64_t nrb) {
+  __shared__ float tile[64][33];
+  const int64_t tj = (cols + 31) / 32;
+  const bool s_rowfast = srs <= scs;
+  for (int64_t t = blockIdx.x; t < nrb * tj; t += gridDim.x) {
+    const int64_t rb = t / tj, j0 = (t - rb * tj) * 32;
+    if (s_rowfast) {
+      for (int q = threadIdx.y; q < 32; q += blockDim.y)
+        for (int h = 0; h < 2; ++h) {
+          const int r = threadIdx.x + 32 * h;
+          const int64_t i = rb * 64 + r, j = j0 + q;
+          tile[r][q] = (i < rows && j < cols) ? S[i * srs + j * scs] : 0.f;
+        }
+    } else {
+      for (int r = threadIdx.y; r < 64; r += blockDim.y) {
+        const int64_t i = rb * 64 + r, j = j0 + threadIdx.x;
+        tile[r][threadIdx.x] = (i < rows && j < cols) ? S[i * srs + j * scs] : 0.f;
+      }
+    }
+    __syncthreads();
+    for (int q = threadIdx.y; q < 32; q += blockDim.y) {
+      const int64_t j = j0 + q;
+      if (j < cols) {
+        const int r = 2 * threadIdx.x;
+        *reinterpret_cast<__nv_bfloat162*>(D + (rb * cols + j) * 64 + r) =
+            __floats2bfloat162_rn(tile[r][q], tile[r + 1][q]);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+void to_bf16_blocked(skema_ctx* c, Mat src, int64_t rows, int64_t cols, __nv_bfloat16* D) {
+  const int64_t nrb = (rows + 63) / 64;
+  if (nrb <= 0 || cols <= 0) return;
+  const bool vec = src.rs == 1 && src.cs % 4 == 0 && reinterpret_cast<uintptr_t>(src.p) % 16 == 0;
+  if (vec) {
+    const int64_t work = nrb * 8 * cols;
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((work + 255) / 256, (int64_t)c->sm_count * 16));
+    to_bf16_blocked_vec_kernel<<<grid, 256, 0, c->stream>>>(src.p, src.cs, rows, cols, D, nrb);
+  } else {
+    const int64_t tiles = nrb * ((cols + 31) / 32);
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(tiles, (int64_t)c->sm_count * 16));
+    to_bf16_blocked_tiled_kernel<<<grid, dim3(32, 8), 0, c->stream>>>(src.p, src.rs, src.cs, rows, cols, D, nrb);
+  }
+  SKEMA_LAUNCHED(c);
 }
 
 // Any strided FP32 block -> BF16 with D(i, j) at D[i * drs + j * dcs], by
@@ -127,17 +217,9 @@ __global__ void to_bf16_tiled_kernel(const float* __restrict__ S, int64_t srs, i
 
 void to_bf16(skema_ctx* c, Mat src, int64_t rows, int64_t cols, __nv_bfloat16* D, int64_t drs, int64_t dcs) {
   if (rows <= 0 || cols <= 0) return;
-  const bool vec = src.rs == 1 && drs == 1 && src.cs % 4 == 0 && dcs % 8 == 0 &&
-                   reinterpret_cast<uintptr_t>(src.p) % 16 == 0 && reinterpret_cast<uintptr_t>(D) % 16 == 0;
-  if (vec) {
-    const int64_t work = ((rows + 7) / 8) * cols;
-    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((work + 255) / 256, (int64_t)c->sm_count * 16));
-    to_bf16_cm_vec_kernel<<<grid, 256, 0, c->stream>>>(src.p, src.cs, rows, cols, D, dcs);
-  } else {
-    const int64_t tiles = ((rows + 31) / 32) * ((cols + 31) / 32);
-    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(tiles, (int64_t)c->sm_count * 16));
-    to_bf16_tiled_kernel<<<grid, dim3(32, 8), 0, c->stream>>>(src.p, src.rs, src.cs, rows, cols, D, drs, dcs);
-  }
+  const int64_t tiles = ((rows + 31) / 32) * ((cols + 31) / 32);
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(tiles, (int64_t)c->sm_count * 16));
+  to_bf16_tiled_kernel<<<grid, dim3(32, 8), 0, c->stream>>>(src.p, src.rs, src.cs, rows, cols, D, drs, dcs);
   SKEMA_LAUNCHED(c);
 }
 
@@ -178,23 +260,60 @@ Plan plan_split(const skema_ctx* c, int64_t tiles, int64_t K, int max_ks) {
   return Plan{ks, kchunk};
 }
 
-template <bool A_MN>
+// Split for a product bound by HBM rather than by the tensor pipe: enough
+// units (about eight rounds over the SMs) that the last round is a small
+// fraction of the whole, with at least 8 k-steps per unit.
+Plan plan_split_stream(const skema_ctx* c, int64_t tiles, int64_t K, int max_ks) {
+  const int64_t ksteps = (K + tc::BK - 1) / tc::BK;
+  int64_t ks = (8 * (int64_t)c->sm_count + tiles - 1) / tiles;
+  ks = std::max<int64_t>(1, std::min<int64_t>({ks, (int64_t)max_ks, ksteps / 8}));
+  const int64_t kchunk = (ksteps + ks - 1) / ks * tc::BK;
+  return Plan{(int)((K + kchunk - 1) / kchunk), kchunk};
+}
+
+// Persistent launch: min(units, SMs) CTAs of one per SM (the 5-stage ring
+// takes 211 KB of shared memory).
+template <int AMODE>
 void launch_gemm(skema_ctx* c, const CUtensorMap& ta, const CUtensorMap& tb, int64_t M, int64_t N, int64_t K,
                  Plan pl, int m_fast, const tc::OutSpec& o) {
-  constexpr int S = 4;
+  constexpr int S = 5;
   constexpr uint32_t STAGE = ((tc::BM * tc::BK * 2 + kNT * tc::BK * 2 + 1023) / 1024) * 1024;
   const size_t smem = (size_t)S * STAGE + 1024 + 256;
-  auto kern = tc::gemm_bf16_kernel<kNT, S, A_MN>;
+  auto kern = tc::gemm_bf16_kernel<kNT, S, AMODE>;
   SKEMA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   tc::Grid3 g;
   g.mtiles = (int)((M + tc::BM - 1) / tc::BM);
   g.ntiles = (int)((N + kNT - 1) / kNT);
   g.ksplit = pl.ks;
   g.m_fast = m_fast;
-  const int64_t grid = (int64_t)g.mtiles * g.ntiles * g.ksplit;
-  if (grid <= 0 || K <= 0) return;
-  if (grid > 0x7fffffff) fail(SKEMA_EINVAL, "tensor-core grid too large");
-  kern<<<(unsigned)grid, tc::kThreads, smem, c->stream>>>(ta, tb, K, pl.kchunk, g, o, c->dev_err);
+  const int64_t units = (int64_t)g.mtiles * g.ntiles * g.ksplit;
+  if (units <= 0 || K <= 0) return;
+  if (units > 0x7fffffff) fail(SKEMA_EINVAL, "tensor-core grid too large");
+  const int grid = (int)std::min<int64_t>(units, c->sm_count);
+  kern<<<grid, tc::kThreads, smem, c->stream>>>(ta, tb, K, pl.kchunk, g, o, c->dev_err);
+  SKEMA_LAUNCHED(c);
+  c->dev_err_armed = true;
+}
+
+// X^T product straight from the FP32 window (converts it and writes A16).
+template <bool AROW>
+void launch_gemm_a32(skema_ctx* c, const CUtensorMap& ta32, const CUtensorMap& tb, const CUtensorMap& ta16,
+                     int64_t M, int64_t N, int64_t K, Plan pl, const tc::OutSpec& o) {
+  constexpr int S1 = 3, S2 = 3;
+  constexpr uint32_t STAGE = ((tc::BM * tc::BK * 2 + kNT * tc::BK * 2 + 1023) / 1024) * 1024;
+  const size_t smem = (size_t)S1 * tc::BM * tc::BK * 4 + (size_t)S2 * STAGE + 1024 + 256;
+  auto kern = tc::gemm_a32_kernel<kNT, S1, S2, AROW>;
+  SKEMA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  tc::Grid3 g;
+  g.mtiles = (int)((M + tc::BM - 1) / tc::BM);
+  g.ntiles = (int)((N + kNT - 1) / kNT);
+  g.ksplit = pl.ks;
+  g.m_fast = 1;
+  const int64_t units = (int64_t)g.mtiles * g.ntiles * g.ksplit;
+  if (units <= 0 || K <= 0) return;
+  if (units > 0x7fffffff) fail(SKEMA_EINVAL, "tensor-core grid too large");
+  const int grid = (int)std::min<int64_t>(units, c->sm_count);
+  kern<<<grid, tc::kThreadsA32, smem, c->stream>>>(ta32, tb, ta16, K, pl.kchunk, g, o, c->dev_err);
   SKEMA_LAUNCHED(c);
   c->dev_err_armed = true;
 }
@@ -239,7 +358,8 @@ void tc_prepare_maps(skema_ctx* c) {
 
 size_t tc_scratch_bytes(const skema_ctx* c, int64_t wr) {
   const int64_t wp = pad8(wr);
-  size_t b = sizeof(__nv_bfloat16) * (size_t)(wp * c->n) + 256;         // A16
+  const int64_t w64 = (wr + 63) / 64 * 64;
+  size_t b = sizeof(__nv_bfloat16) * (size_t)(w64 * c->n) + 256;        // A16 (row-blocked)
   b += sizeof(__nv_bfloat16) * (size_t)(wp * c->s) + 256;               // T16
   b += sizeof(float) * (size_t)(wp * c->s) + 256;                       // T32 (split-K)
   b += sizeof(__nv_bfloat16) * (size_t)((c->k + c->s) * wp) + 512;      // map slices (unaligned R0)
@@ -256,14 +376,20 @@ void tc_dense_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr, void* scratch
     sp += (bytes + 255) / 256 * 256;
     return p;
   };
-  __nv_bfloat16* A16 = reinterpret_cast<__nv_bfloat16*>(take(sizeof(__nv_bfloat16) * (size_t)(wp * n)));
+  const int64_t nrb = (wr + 63) / 64;
+  __nv_bfloat16* A16 = reinterpret_cast<__nv_bfloat16*>(take(sizeof(__nv_bfloat16) * (size_t)(nrb * 64 * n)));
   __nv_bfloat16* T16 = reinterpret_cast<__nv_bfloat16*>(take(sizeof(__nv_bfloat16) * (size_t)(wp * s)));
   float* T32 = reinterpret_cast<float*>(take(sizeof(float) * (size_t)(wp * s)));
   const float ybeta = y_rows_clean(c, R0, R0 + wr) ? 0.f : nu;
 
-  {  // A16 = bf16(A_w)
+  // The X^T product reads the FP32 window itself (and writes A16) when TMA
+  // can address it: 16-byte aligned base and stride.
+  const bool al = reinterpret_cast<uintptr_t>(Aw.p) % 16 == 0;
+  const bool a32_cm = al && Aw.rs == 1 && Aw.cs % 4 == 0;
+  const bool a32_rm = al && Aw.cs == 1 && Aw.rs % 4 == 0;
+  if (!a32_cm && !a32_rm) {  // A16 = bf16(A_w), row-blocked, zero rows up to a multiple of 64
     StageScope st(c, ST_WINDOW);
-    to_bf16(c, Aw, wr, n, A16, 1, wp);
+    to_bf16_blocked(c, Aw, wr, n, A16);
   }
   // Upsilon~ / Phi~ columns of this window: in place when R0 keeps the
   // 16-byte alignment TMA needs, else converted into an aligned slice.
@@ -280,9 +406,32 @@ void tc_dense_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr, void* scratch
     ldm = wp;
   }
   const uint64_t wp2 = (uint64_t)wp * 2;
+  {  // X^T = nu X^T + eta A_w^T Upsilon~_w^T
+    StageScope st(c, ST_UPSILON);
+    const CUtensorMap tb = tmap_bf16(U16, (uint64_t)wr, (uint64_t)k, (uint64_t)ldm * 2, 64, kNT);
+    const int64_t tiles = ((n + 127) / 128) * ((k + kNT - 1) / kNT);
+    const Plan pl = (a32_cm || a32_rm) ? plan_split_stream(c, tiles, wr, 8) : plan_split(c, tiles, wr, 8);
+    tc::OutSpec o = out_spec();
+    o.p0 = c->X, o.rs0 = 1, o.cs0 = n, o.alpha0 = eta, o.beta0 = nu;
+    o.rows = n, o.split = k, o.ncols = k;
+    if (pl.ks > 1) {
+      scale_block(c, MatOut{c->X, n, 1}, k, n, nu);
+      o.atomic0 = 1, o.beta0 = 0.f;
+    }
+    const CUtensorMap ta16 = tmap_bf16_blocked(A16, (uint64_t)n, (uint64_t)nrb, 128);
+    if (a32_cm) {
+      const CUtensorMap ta32 = tmap_f32(Aw.p, (uint64_t)wr, (uint64_t)n, (uint64_t)Aw.cs * 4, 32, 128);
+      launch_gemm_a32<false>(c, ta32, tb, ta16, n, k, wr, pl, o);
+    } else if (a32_rm) {
+      const CUtensorMap ta32 = tmap_f32(Aw.p, (uint64_t)n, (uint64_t)wr, (uint64_t)Aw.rs * 4, 32, 64);
+      launch_gemm_a32<true>(c, ta32, tb, ta16, n, k, wr, pl, o);
+    } else {
+      launch_gemm<tc::A_KMAJ_BLK>(c, ta16, tb, n, k, wr, pl, 1, o);
+    }
+  }
   {  // [Y_w | T] = A16 [Omega~; Psi~]^T
     StageScope st(c, ST_FUSED);
-    const CUtensorMap ta = tmap_bf16(A16, (uint64_t)wr, (uint64_t)n, wp2, 64, 64);
+    const CUtensorMap ta = tmap_bf16_blocked(A16, (uint64_t)n, (uint64_t)nrb, 64);
     const CUtensorMap tb = tmap_bf16(c->op16, (uint64_t)n, (uint64_t)(k + s), (uint64_t)c->ld_op16 * 2, 64, kNT);
     const int64_t tiles = ((wr + 127) / 128) * ((k + s + kNT - 1) / kNT);
     const Plan pl = plan_split(c, tiles, n, 8);
@@ -297,7 +446,7 @@ void tc_dense_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr, void* scratch
       o.atomic0 = 1, o.beta0 = 0.f;
       o.p1f = T32, o.rs1 = 1, o.cs1 = wp, o.atomic1 = 1;
     }
-    launch_gemm<true>(c, ta, tb, wr, k + s, n, pl, 0, o);
+    launch_gemm<tc::A_MN_BLK>(c, ta, tb, wr, k + s, n, pl, 0, o);
     if (pl.ks > 1) {
       const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((wr * s + 255) / 256, c->sm_count * 16));
       f32_to_bf16_cm_kernel<<<grid, 256, 0, c->stream>>>(T32, T16, wr, s, wp);
@@ -305,21 +454,6 @@ void tc_dense_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr, void* scratch
     }
   }
   y_rows_mark(c, R0, R0 + wr);
-  {  // X^T = nu X^T + eta A16^T Upsilon~_w^T
-    StageScope st(c, ST_UPSILON);
-    const CUtensorMap ta = tmap_bf16(A16, (uint64_t)wr, (uint64_t)n, wp2, 64, 128);
-    const CUtensorMap tb = tmap_bf16(U16, (uint64_t)wr, (uint64_t)k, (uint64_t)ldm * 2, 64, kNT);
-    const int64_t tiles = ((n + 127) / 128) * ((k + kNT - 1) / kNT);
-    const Plan pl = plan_split(c, tiles, wr, 8);
-    tc::OutSpec o = out_spec();
-    o.p0 = c->X, o.rs0 = 1, o.cs0 = n, o.alpha0 = eta, o.beta0 = nu;
-    o.rows = n, o.split = k, o.ncols = k;
-    if (pl.ks > 1) {
-      scale_block(c, MatOut{c->X, n, 1}, k, n, nu);
-      o.atomic0 = 1, o.beta0 = 0.f;
-    }
-    launch_gemm<false>(c, ta, tb, n, k, wr, pl, 1, o);
-  }
   {  // Z^T = nu Z^T + eta T^T Phi~_w^T
     StageScope st(c, ST_PHI);
     const CUtensorMap ta = tmap_bf16(T16, (uint64_t)wr, (uint64_t)s, wp2, 64, 128);
@@ -333,7 +467,7 @@ void tc_dense_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr, void* scratch
       scale_block(c, MatOut{c->Z, s, 1}, s, s, nu);
       o.atomic0 = 1, o.beta0 = 0.f;
     }
-    launch_gemm<false>(c, ta, tb, s, s, wr, pl, 0, o);
+    launch_gemm<tc::A_KMAJ>(c, ta, tb, s, s, wr, pl, 0, o);
   }
 }
 

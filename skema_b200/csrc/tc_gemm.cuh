@@ -1,23 +1,27 @@
-// tc_gemm.cuh -- a BF16 x BF16 -> FP32 tensor-core GEMM for sm_100a
-// (tcgen05.mma with the accumulator in TMEM, operands staged by TMA), used by
-// the BF16 form of the dense sketch.
+// tc_gemm.cuh -- a persistent BF16 x BF16 -> FP32 tensor-core GEMM for
+// sm_100a (tcgen05.mma with accumulators in TMEM, operands staged by TMA),
+// used by the BF16 form of the dense sketch.
 //
-// One CTA computes a 128 x NT output tile (NT <= 256, multiple of 16) over
-// K in steps of 64, with an S-stage shared-memory ring:
-//   warp 4 (one lane)  TMA producer: waits for a free stage, posts the bytes
-//                      it expects and issues the operand loads;
-//   warp 5 (one lane)  MMA issuer: waits for a full stage, issues four
-//                      tcgen05.mma (K = 16 each) and commits the stage back;
+// Work unit: a 128 x NT output tile (NT <= 256, multiple of 16) over one
+// split of K. The grid is at most one CTA per SM; CTA b takes units b,
+// b + gridDim.x, ... Roles (192 threads):
+//   warp 4 (one lane)  TMA producer: runs ahead over all units of the CTA,
+//                      filling an S-stage shared-memory ring (one 64-wide
+//                      K step of A and B per stage);
+//   warp 5 (one lane)  MMA issuer: four tcgen05.mma (K = 16) per stage into
+//                      one of two TMEM accumulators, alternating per unit;
 //                      warp 5 also allocates and frees the TMEM columns;
-//   warps 0-3          epilogue: wait for the accumulator, read TMEM lanes
-//                      32w..32w+31 with tcgen05.ld and write the outputs.
+//   warps 0-3          epilogue: read the finished accumulator with
+//                      tcgen05.ld (warp w owns TMEM lanes 32w..32w+31), hand
+//                      it back to the MMA issuer, then store.
+// With two accumulators the epilogue of one unit overlaps the main loop of
+// the next.
+//
 // Output tile rows run along TMEM lanes, so consecutive lanes of a warp own
 // consecutive output rows: callers orient each product so that the output's
 // contiguous dimension is the row dimension (coalesced epilogue stores).
-// Operands are 128-byte-swizzled (TMA SWIZZLE_128B). A is K-major (rows of
-// 64 K-elements = 128 B, 8-row groups 1024 B apart) or MN-major (lines of 64
-// M-elements per K index, K-groups of 8 lines 1024 B apart, the two 64-row
-// halves of the tile 8 KB apart); B is K-major.
+// Operands are 128-byte-swizzled (TMA SWIZZLE_128B). A comes from one of
+// three tensor-map shapes (AMode); B is K-major (rows of 64 K-elements).
 //
 // Every wait is bounded by a timer; on time-out the waiting thread sets
 // *err, all roles stop issuing, every thread meets the final barrier, TMEM
@@ -35,6 +39,20 @@ constexpr int BM = 128;      // tile rows (TMEM lanes)
 constexpr int BK = 64;       // K per stage (one 128-byte swizzle row of BF16)
 constexpr int kThreads = 192;
 constexpr unsigned long long kWaitNs = 2000000000ull;  // 2 s per wait
+
+// Where the A tile of a K step comes from.
+enum AMode : int {
+  // 2-D map {K, rows}, K innermost: one box {64, 128} at (k, m0).
+  A_KMAJ = 0,
+  // Row-blocked 3-D map {64, rows, K/64} (64 K-elements of a row contiguous,
+  // then the rows, then the 64-blocks of K): one box {64, 128, 1} at
+  // (0, m0, k/64) -- a contiguous 16 KB run.
+  A_KMAJ_BLK = 1,
+  // Row-blocked 3-D map {64, K, M/64} (64 M-elements contiguous, then K,
+  // then the 64-blocks of M), read MN-major: two boxes {64, 64, 1} at
+  // (0, k, m0/64) and (0, k, m0/64 + 1) -- two contiguous 8 KB runs.
+  A_MN_BLK = 2,
+};
 
 struct OutSpec {
   // columns [0, split) of the tile row space go to p0, [split, ncols) to p1
@@ -63,6 +81,9 @@ __device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count) {
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(bytes)
                : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* b) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(b)) : "memory");
 }
 __device__ __forceinline__ bool mbar_try(uint64_t* b, uint32_t parity) {
   uint32_t ok;
@@ -93,6 +114,29 @@ __device__ __forceinline__ void tma_load_2d(const CUtensorMap* tm, uint64_t* bar
           smem_u32(dst)),
       "l"(tm), "r"(smem_u32(bar)), "r"(c0), "r"(c1)
       : "memory");
+}
+__device__ __forceinline__ void tma_load_3d(const CUtensorMap* tm, uint64_t* bar, void* dst, int c0, int c1,
+                                            int c2) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];" ::"r"(
+          smem_u32(dst)),
+      "l"(tm), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2)
+      : "memory");
+}
+__device__ __forceinline__ void tma_store_3d(const CUtensorMap* tm, const void* src, int c0, int c1, int c2) {
+  asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%2, %3, %4}], [%1];" ::"l"(tm),
+               "r"(smem_u32(src)), "r"(c0), "r"(c1), "r"(c2)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read_all() {
+  asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+// Orders this thread's generic-proxy shared-memory writes before later
+// async-proxy reads (tensor-core operands, TMA stores).
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 __device__ __forceinline__ void tc_fence_before() {
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -143,31 +187,12 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-// Tile scheduling: tile t -> (mt, nt, ks). M fastest when m_fast, else N.
+// Work units: unit t -> (mt, nt, ks). M fastest when m_fast, else N.
 struct Grid3 {
   int mtiles, ntiles, ksplit;
   int m_fast;
 };
-
-template <int NT, int S, bool A_MN>
-__global__ void __launch_bounds__(kThreads, 1)
-    gemm_bf16_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
-                     int64_t K, int64_t kchunk, Grid3 g, OutSpec o, int* err) {
-  constexpr uint32_t A_BYTES = BM * BK * 2;  // 16 KB
-  constexpr uint32_t B_BYTES = NT * BK * 2;
-  constexpr uint32_t STAGE = ((A_BYTES + B_BYTES + 1023) / 1024) * 1024;
-  constexpr uint32_t TCOLS = NT <= 32 ? 32 : NT <= 64 ? 64 : NT <= 128 ? 128 : 256;
-  extern __shared__ __align__(1024) unsigned char smem_raw[];
-  unsigned char* smem = reinterpret_cast<unsigned char*>(
-      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
-  uint64_t* full = reinterpret_cast<uint64_t*>(smem + S * STAGE);
-  uint64_t* empty = full + S;
-  uint64_t* accf = empty + S;
-  uint32_t* tbase = reinterpret_cast<uint32_t*>(accf + 1);
-
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  int t = blockIdx.x;
-  int mt, nt, ks;
+__device__ __forceinline__ void decode_unit(const Grid3& g, int t, int& mt, int& nt, int& ks) {
   if (g.m_fast) {
     mt = t % g.mtiles;
     t /= g.mtiles;
@@ -179,21 +204,93 @@ __global__ void __launch_bounds__(kThreads, 1)
     mt = t % g.mtiles;
     ks = t / g.mtiles;
   }
-  const int64_t k0 = (int64_t)ks * kchunk;
-  const int64_t k1 = min(K, k0 + kchunk);
-  const int KT = (int)((k1 - k0 + BK - 1) / BK);
+}
+
+// Stores one finished 128 x NT accumulator (warps 0-3, warp w on TMEM lanes
+// 32w..32w+31): waits for it, reads it 16 columns at a time, hands it back
+// to the MMA issuer after the last read, and writes the columns per OutSpec.
+// False when the wait failed (the warp then stops).
+template <int NT, uint32_t TCOLS>
+__device__ __forceinline__ bool epilogue_unit(const OutSpec& o, uint32_t tmem, uint32_t acc, uint32_t aph,
+                                              uint64_t* tfull, uint64_t* tempty, int mt, int nt, int warp,
+                                              int lane, int* err) {
+  // tcgen05.ld is warp-collective: the whole warp reads TMEM or none of it
+  if (!__all_sync(0xffffffffu, mbar_wait(tfull + acc, aph, err))) return false;
+  tc_fence_after();
+  const int64_t row = (int64_t)mt * BM + warp * 32 + lane;
+  const uint32_t taddr = tmem + acc * TCOLS + ((uint32_t)(warp * 32) << 16);
+  for (int c0 = 0; c0 < NT; c0 += 16) {
+    float v[16];
+    tmem_ld16(taddr + c0, v);
+    if (c0 + 16 >= NT) {
+      // last read of this accumulator: hand it back before storing
+      tc_fence_before();
+      mbar_arrive(tempty + acc);
+    }
+    if (row >= o.rows) continue;
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+      const int64_t col = (int64_t)nt * NT + c0 + i;
+      if (col >= o.ncols) continue;
+      if (col < o.split) {
+        float* p = o.p0 + row * o.rs0 + col * o.cs0;
+        if (o.atomic0)
+          atomicAdd(p, o.alpha0 * v[i]);
+        else
+          *p = (o.beta0 == 0.f) ? o.alpha0 * v[i] : fmaf(o.beta0, *p, o.alpha0 * v[i]);
+      } else {
+        const int64_t cc = col - o.split;
+        if (o.p1) {
+          o.p1[row * o.rs1 + cc * o.cs1] = __float2bfloat16(o.alpha1 * v[i]);
+        } else if (o.p1f) {
+          float* p = o.p1f + row * o.rs1 + cc * o.cs1;
+          if (o.atomic1)
+            atomicAdd(p, o.alpha1 * v[i]);
+          else
+            *p = (o.beta1 == 0.f) ? o.alpha1 * v[i] : fmaf(o.beta1, *p, o.alpha1 * v[i]);
+        }
+      }
+    }
+  }
+  return true;
+}
+
+template <int NT, int S, int AMODE>
+__global__ void __launch_bounds__(kThreads, 1)
+    gemm_bf16_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                     int64_t K, int64_t kchunk, Grid3 g, OutSpec o, int* err) {
+  constexpr uint32_t A_BYTES = BM * BK * 2;  // 16 KB
+  constexpr uint32_t B_BYTES = NT * BK * 2;
+  constexpr uint32_t STAGE = ((A_BYTES + B_BYTES + 1023) / 1024) * 1024;
+  constexpr uint32_t TCOLS = NT <= 32 ? 32 : NT <= 64 ? 64 : NT <= 128 ? 128 : 256;
+  static_assert(NT % 16 == 0 && NT <= 256, "N tile");
+  static_assert(2 * TCOLS <= 512, "two accumulators must fit TMEM");
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char* smem = reinterpret_cast<unsigned char*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + S * STAGE);
+  uint64_t* empty = full + S;
+  uint64_t* tfull = empty + S;   // [2] accumulator ready (MMA -> epilogue)
+  uint64_t* tempty = tfull + 2;  // [2] accumulator drained (epilogue -> MMA)
+  uint32_t* tbase = reinterpret_cast<uint32_t*>(tempty + 2);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int total = g.mtiles * g.ntiles * g.ksplit;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < S; ++s) {
       mbar_init(full + s, 1);
       mbar_init(empty + s, 1);
     }
-    mbar_init(accf, 1);
+    for (int a = 0; a < 2; ++a) {
+      mbar_init(tfull + a, 1);
+      mbar_init(tempty + a, 4 * 32);
+    }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 5) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tbase)),
-                 "r"(TCOLS)
+                 "r"(2 * TCOLS)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
@@ -202,87 +299,80 @@ __global__ void __launch_bounds__(kThreads, 1)
   tc_fence_after();
   const uint32_t tmem = *tbase;
 
-  if (warp == 4 && lane == 0 && KT > 0) {
+  if (warp == 4 && lane == 0) {
     // ---------------- TMA producer ----------------
-    for (int kt = 0; kt < KT; ++kt) {
-      const int s = kt % S;
-      const uint32_t ph = (kt / S) & 1;
-      if (!mbar_wait(empty + s, ph ^ 1, err)) break;
-      unsigned char* sa = smem + s * STAGE;
-      unsigned char* sb = sa + A_BYTES;
-      mbar_expect_tx(full + s, A_BYTES + B_BYTES);
-      const int kc = (int)(k0 + (int64_t)kt * BK);
-      if (A_MN) {
-        tma_load_2d(&tmA, full + s, sa, mt * BM, kc);
-        tma_load_2d(&tmA, full + s, sa + 8192, mt * BM + 64, kc);
-      } else {
-        tma_load_2d(&tmA, full + s, sa, kc, mt * BM);
-      }
-      tma_load_2d(&tmB, full + s, sb, kc, nt * NT);
-    }
-  } else if (warp == 5 && lane == 0 && KT > 0) {
-    // ---------------- MMA issuer ----------------
-    constexpr uint32_t idesc = idesc_bf16(NT, A_MN, false);
+    uint32_t it = 0;
     bool ok = true;
-    for (int kt = 0; kt < KT; ++kt) {
-      const int s = kt % S;
-      const uint32_t ph = (kt / S) & 1;
-      if (!mbar_wait(full + s, ph, err)) {
-        ok = false;
-        break;
+    for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
+      int mt, nt, ks;
+      decode_unit(g, t, mt, nt, ks);
+      const int64_t k0 = (int64_t)ks * kchunk;
+      const int KT = (int)((min(K, k0 + kchunk) - k0 + BK - 1) / BK);
+      for (int kt = 0; kt < KT; ++kt, ++it) {
+        const int s = it % S;
+        const uint32_t ph = (it / S) & 1;
+        if (!mbar_wait(empty + s, ph ^ 1, err)) {
+          ok = false;
+          break;
+        }
+        unsigned char* sa = smem + s * STAGE;
+        unsigned char* sb = sa + A_BYTES;
+        mbar_expect_tx(full + s, A_BYTES + B_BYTES);
+        const int kc = (int)(k0 + (int64_t)kt * BK);
+        if (AMODE == A_KMAJ) {
+          tma_load_2d(&tmA, full + s, sa, kc, mt * BM);
+        } else if (AMODE == A_KMAJ_BLK) {
+          tma_load_3d(&tmA, full + s, sa, 0, mt * BM, kc / BK);
+        } else {
+          tma_load_3d(&tmA, full + s, sa, 0, kc, 2 * mt);
+          tma_load_3d(&tmA, full + s, sa + 8192, 0, kc, 2 * mt + 1);
+        }
+        tma_load_2d(&tmB, full + s, sb, kc, nt * NT);
       }
-      tc_fence_after();
-      const uint32_t sa = smem_u32(smem + s * STAGE);
-      const uint32_t sb = sa + A_BYTES;
-#pragma unroll
-      for (int kk = 0; kk < BK / 16; ++kk) {
-        const uint64_t ad = A_MN ? sdesc(sa + kk * 2048, 8192, 1024) : sdesc(sa + kk * 32, 16, 1024);
-        const uint64_t bd = sdesc(sb + kk * 32, 16, 1024);
-        umma(tmem, ad, bd, idesc, (kt > 0 || kk > 0) ? 1u : 0u);
-      }
-      umma_commit(empty + s);
     }
-    if (ok) umma_commit(accf);
+  } else if (warp == 5 && lane == 0) {
+    // ---------------- MMA issuer ----------------
+    constexpr uint32_t idesc = idesc_bf16(NT, AMODE == A_MN_BLK, false);
+    uint32_t it = 0, tcount = 0;
+    bool ok = true;
+    for (int t = blockIdx.x; t < total && ok; t += gridDim.x, ++tcount) {
+      int mt, nt, ks;
+      decode_unit(g, t, mt, nt, ks);
+      const int64_t k0 = (int64_t)ks * kchunk;
+      const int KT = (int)((min(K, k0 + kchunk) - k0 + BK - 1) / BK);
+      const uint32_t acc = tcount & 1, aph = (tcount >> 1) & 1;
+      if (!mbar_wait(tempty + acc, aph ^ 1, err)) break;
+      tc_fence_after();
+      const uint32_t d = tmem + acc * TCOLS;
+      for (int kt = 0; kt < KT; ++kt, ++it) {
+        const int s = it % S;
+        const uint32_t ph = (it / S) & 1;
+        if (!mbar_wait(full + s, ph, err)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t sa = smem_u32(smem + s * STAGE);
+        const uint32_t sb = sa + A_BYTES;
+#pragma unroll
+        for (int kk = 0; kk < BK / 16; ++kk) {
+          const uint64_t ad =
+              AMODE == A_MN_BLK ? sdesc(sa + kk * 2048, 8192, 1024) : sdesc(sa + kk * 32, 16, 1024);
+          const uint64_t bd = sdesc(sb + kk * 32, 16, 1024);
+          umma(d, ad, bd, idesc, (kt > 0 || kk > 0) ? 1u : 0u);
+        }
+        umma_commit(empty + s);
+      }
+      if (ok) umma_commit(tfull + acc);
+    }
   } else if (warp < 4) {
     // ---------------- epilogue ----------------
-    // tcgen05.ld is warp-collective: the whole warp reads TMEM or none of it
-    const bool have = __all_sync(0xffffffffu, KT > 0 && mbar_wait(accf, 0, err));
-    if (have) tc_fence_after();
-    const int64_t row = (int64_t)mt * BM + warp * 32 + lane;
-    const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16);
-    for (int c0 = 0; c0 < NT; c0 += 16) {
-      float v[16];
-      if (have) {
-        tmem_ld16(taddr + c0, v);
-      } else {
-#pragma unroll
-        for (int i = 0; i < 16; ++i) v[i] = 0.f;
-      }
-      if (!have || row >= o.rows) continue;
-#pragma unroll
-      for (int i = 0; i < 16; ++i) {
-        const int64_t col = (int64_t)nt * NT + c0 + i;
-        if (col >= o.ncols) continue;
-        if (col < o.split) {
-          float* p = o.p0 + row * o.rs0 + col * o.cs0;
-          if (o.atomic0)
-            atomicAdd(p, o.alpha0 * v[i]);
-          else
-            *p = (o.beta0 == 0.f) ? o.alpha0 * v[i] : fmaf(o.beta0, *p, o.alpha0 * v[i]);
-        } else {
-          const int64_t cc = col - o.split;
-          if (o.p1) {
-            __nv_bfloat16* p = o.p1 + row * o.rs1 + cc * o.cs1;
-            *p = __float2bfloat16(o.alpha1 * v[i]);
-          } else if (o.p1f) {
-            float* p = o.p1f + row * o.rs1 + cc * o.cs1;
-            if (o.atomic1)
-              atomicAdd(p, o.alpha1 * v[i]);
-            else
-              *p = (o.beta1 == 0.f) ? o.alpha1 * v[i] : fmaf(o.beta1, *p, o.alpha1 * v[i]);
-          }
-        }
-      }
+    uint32_t tcount = 0;
+    for (int t = blockIdx.x; t < total; t += gridDim.x, ++tcount) {
+      int mt, nt, ks;
+      decode_unit(g, t, mt, nt, ks);
+      const uint32_t acc = tcount & 1, aph = (tcount >> 1) & 1;
+      if (!epilogue_unit<NT, TCOLS>(o, tmem, acc, aph, tfull, tempty, mt, nt, warp, lane, err)) break;
     }
   }
   if ((warp == 4 || warp == 5) && lane == 0 && *(volatile int*)err) {
@@ -297,7 +387,238 @@ __global__ void __launch_bounds__(kThreads, 1)
   if (warp == 5) {
     __syncwarp();
     tc_fence_after();
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TCOLS) : "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * TCOLS) : "memory");
+  }
+}
+
+// ---------------------------------------------------------------------------
+// The same GEMM with A read as FP32 and rounded to BF16 inside the kernel,
+// for X^T = A_w^T Upsilon~_w^T straight from the FP32 window: M runs over
+// the window's columns, K over its rows. Each K step's A tile (64 window
+// rows x 128 columns) arrives by TMA as FP32; four converter warps round it
+// into the 128-byte-swizzled K-major BF16 operand, and one converter thread
+// stores that operand with TMA into the row-blocked BF16 copy of the window
+// (A16, A_MN_BLK / A_KMAJ_BLK shape) that the [Y|T] product reads next. So
+// every element of the window is read from HBM once as FP32 and written
+// once as BF16, and no separate conversion pass runs.
+//   AROW = false: column-major window (rows contiguous); the FP32 tile is
+//                 two 128-byte-swizzled boxes {32 rows, 128 columns}.
+//   AROW = true:  row-major window (columns contiguous); four boxes
+//                 {32 columns, 64 rows}.
+// Threads: warps 0-3 epilogue, warp 4 TMA producer, warp 5 MMA issuer,
+// warps 6-9 converters. Rings: S1 FP32 stages (producer -> converters) and
+// S2 BF16 stages (A from the converters, B by TMA -> MMA); a BF16 stage is
+// free again when the MMAs that read it are done and the TMA store of its
+// A tile has read it.
+constexpr int kThreadsA32 = 320;
+
+template <int NT, int S1, int S2, bool AROW>
+__global__ void __launch_bounds__(kThreadsA32, 1)
+    gemm_a32_kernel(const __grid_constant__ CUtensorMap tmA32, const __grid_constant__ CUtensorMap tmB,
+                    const __grid_constant__ CUtensorMap tmA16, int64_t K, int64_t kchunk, Grid3 g, OutSpec o,
+                    int* err) {
+  constexpr uint32_t A32_BYTES = BM * BK * 4;  // 32 KB
+  constexpr uint32_t A_BYTES = BM * BK * 2;    // 16 KB
+  constexpr uint32_t B_BYTES = NT * BK * 2;
+  constexpr uint32_t STAGE = ((A_BYTES + B_BYTES + 1023) / 1024) * 1024;
+  constexpr uint32_t TCOLS = NT <= 32 ? 32 : NT <= 64 ? 64 : NT <= 128 ? 128 : 256;
+  static_assert(NT % 16 == 0 && NT <= 256, "N tile");
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char* smem = reinterpret_cast<unsigned char*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+  unsigned char* st32 = smem;                    // S1 x A32_BYTES
+  unsigned char* stbf = smem + S1 * A32_BYTES;   // S2 x STAGE
+  uint64_t* f32full = reinterpret_cast<uint64_t*>(stbf + S2 * STAGE);
+  uint64_t* f32empty = f32full + S1;
+  uint64_t* full = f32empty + S1;
+  uint64_t* empty = full + S2;
+  uint64_t* tfull = empty + S2;
+  uint64_t* tempty = tfull + 2;
+  uint32_t* tbase = reinterpret_cast<uint32_t*>(tempty + 2);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int total = g.mtiles * g.ntiles * g.ksplit;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < S1; ++s) {
+      mbar_init(f32full + s, 1);
+      mbar_init(f32empty + s, 128);
+    }
+    for (int s = 0; s < S2; ++s) {
+      mbar_init(full + s, 1 + 128);  // producer (B bytes) + converters (A tile)
+      mbar_init(empty + s, 2);       // MMA commit + A-tile store drained
+    }
+    for (int a = 0; a < 2; ++a) {
+      mbar_init(tfull + a, 1);
+      mbar_init(tempty + a, 4 * 32);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 5) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tbase)),
+                 "r"(2 * TCOLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tbase;
+
+  if (warp == 4 && lane == 0) {
+    // ---------------- TMA producer ----------------
+    uint32_t it = 0;
+    bool ok = true;
+    for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
+      int mt, nt, ks;
+      decode_unit(g, t, mt, nt, ks);
+      const int64_t k0 = (int64_t)ks * kchunk;
+      const int KT = (int)((min(K, k0 + kchunk) - k0 + BK - 1) / BK);
+      for (int kt = 0; kt < KT; ++kt, ++it) {
+        const int s1 = it % S1, s2 = it % S2;
+        const uint32_t ph1 = (it / S1) & 1, ph2 = (it / S2) & 1;
+        const int kc = (int)(k0 + (int64_t)kt * BK);
+        if (!mbar_wait(f32empty + s1, ph1 ^ 1, err)) {
+          ok = false;
+          break;
+        }
+        unsigned char* a32 = st32 + s1 * A32_BYTES;
+        mbar_expect_tx(f32full + s1, A32_BYTES);
+        if (!AROW) {
+          tma_load_2d(&tmA32, f32full + s1, a32, kc, mt * BM);
+          tma_load_2d(&tmA32, f32full + s1, a32 + 16384, kc + 32, mt * BM);
+        } else {
+#pragma unroll
+          for (int q = 0; q < 4; ++q) tma_load_2d(&tmA32, f32full + s1, a32 + q * 8192, mt * BM + 32 * q, kc);
+        }
+        if (!mbar_wait(empty + s2, ph2 ^ 1, err)) {
+          ok = false;
+          break;
+        }
+        mbar_expect_tx(full + s2, B_BYTES);
+        tma_load_2d(&tmB, full + s2, stbf + s2 * STAGE + A_BYTES, kc, nt * NT);
+      }
+    }
+  } else if (warp == 5 && lane == 0) {
+    // ---------------- MMA issuer ----------------
+    constexpr uint32_t idesc = idesc_bf16(NT, false, false);
+    uint32_t it = 0, tcount = 0;
+    bool ok = true;
+    for (int t = blockIdx.x; t < total && ok; t += gridDim.x, ++tcount) {
+      int mt, nt, ks;
+      decode_unit(g, t, mt, nt, ks);
+      const int64_t k0 = (int64_t)ks * kchunk;
+      const int KT = (int)((min(K, k0 + kchunk) - k0 + BK - 1) / BK);
+      const uint32_t acc = tcount & 1, aph = (tcount >> 1) & 1;
+      if (!mbar_wait(tempty + acc, aph ^ 1, err)) break;
+      tc_fence_after();
+      const uint32_t d = tmem + acc * TCOLS;
+      for (int kt = 0; kt < KT; ++kt, ++it) {
+        const int s2 = it % S2;
+        const uint32_t ph2 = (it / S2) & 1;
+        if (!mbar_wait(full + s2, ph2, err)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t sa = smem_u32(stbf + s2 * STAGE);
+        const uint32_t sb = sa + A_BYTES;
+#pragma unroll
+        for (int kk = 0; kk < BK / 16; ++kk)
+          umma(d, sdesc(sa + kk * 32, 16, 1024), sdesc(sb + kk * 32, 16, 1024), idesc, (kt > 0 || kk > 0) ? 1u : 0u);
+        umma_commit(empty + s2);
+      }
+      if (ok) umma_commit(tfull + acc);
+    }
+  } else if (warp >= 6) {
+    // ---------------- converters ----------------
+    const int ct = threadIdx.x - 6 * 32;  // A-tile line (window column) of this thread
+    uint32_t it = 0;
+    bool ok = true;
+    for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
+      int mt, nt, ks;
+      decode_unit(g, t, mt, nt, ks);
+      const int64_t k0 = (int64_t)ks * kchunk;
+      const int KT = (int)((min(K, k0 + kchunk) - k0 + BK - 1) / BK);
+      for (int kt = 0; kt < KT; ++kt, ++it) {
+        const int s1 = it % S1, s2 = it % S2;
+        const uint32_t ph1 = (it / S1) & 1, ph2 = (it / S2) & 1;
+        if (!mbar_wait(f32full + s1, ph1, err) || !mbar_wait(empty + s2, ph2 ^ 1, err)) {
+          ok = false;
+          break;
+        }
+        const unsigned char* a32 = st32 + s1 * A32_BYTES;
+        unsigned char* dst = stbf + s2 * STAGE + ct * 128;
+        const int sw = ct & 7;
+        if (!AROW) {
+          // line ct of each FP32 box holds rows 32h..32h+31 of column ct
+#pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            const unsigned char* src = a32 + (q >> 2) * 16384 + ct * 128;
+            const int c = 2 * (q & 3);
+            const float4 x = *reinterpret_cast<const float4*>(src + ((c ^ sw) << 4));
+            const float4 y = *reinterpret_cast<const float4*>(src + (((c + 1) ^ sw) << 4));
+            __nv_bfloat162 h[4] = {__floats2bfloat162_rn(x.x, x.y), __floats2bfloat162_rn(x.z, x.w),
+                                   __floats2bfloat162_rn(y.x, y.y), __floats2bfloat162_rn(y.z, y.w)};
+            *reinterpret_cast<uint4*>(dst + ((q ^ sw) << 4)) = *reinterpret_cast<const uint4*>(h);
+          }
+        } else {
+          // column ct lives in box ct / 32 at element ct % 32 of every line
+          const unsigned char* box = a32 + (ct >> 5) * 8192;
+          const int jj = ct & 31;
+#pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            float f[8];
+#pragma unroll
+            for (int e = 0; e < 8; ++e) {
+              const int i = 8 * q + e;
+              f[e] = *reinterpret_cast<const float*>(box + i * 128 + ((((jj >> 2) ^ (i & 7))) << 4) + (jj & 3) * 4);
+            }
+            __nv_bfloat162 h[4] = {__floats2bfloat162_rn(f[0], f[1]), __floats2bfloat162_rn(f[2], f[3]),
+                                   __floats2bfloat162_rn(f[4], f[5]), __floats2bfloat162_rn(f[6], f[7])};
+            *reinterpret_cast<uint4*>(dst + ((q ^ sw) << 4)) = *reinterpret_cast<const uint4*>(h);
+          }
+        }
+        fence_proxy_async();
+        mbar_arrive(f32empty + s1);
+        mbar_arrive(full + s2);
+        if (ct == 0) {
+          // all 128 lines written (and the B tile landed): store the BF16
+          // tile, wait until TMA has read it, then release the stage
+          if (!mbar_wait(full + s2, ph2, err)) {
+            ok = false;
+            break;
+          }
+          fence_proxy_async();
+          const int kc = (int)(k0 + (int64_t)kt * BK);
+          tma_store_3d(&tmA16, stbf + s2 * STAGE, 0, mt * BM, kc / BK);
+          bulk_commit();
+          bulk_wait_read_all();
+          mbar_arrive(empty + s2);
+        }
+      }
+    }
+    if (ct == 0) bulk_wait_all();
+  } else if (warp < 4) {
+    // ---------------- epilogue ----------------
+    uint32_t tcount = 0;
+    for (int t = blockIdx.x; t < total; t += gridDim.x, ++tcount) {
+      int mt, nt, ks;
+      decode_unit(g, t, mt, nt, ks);
+      const uint32_t acc = tcount & 1, aph = (tcount >> 1) & 1;
+      if (!epilogue_unit<NT, TCOLS>(o, tmem, acc, aph, tfull, tempty, mt, nt, warp, lane, err)) break;
+    }
+  }
+  if ((warp == 4 || warp == 5 || threadIdx.x == 6 * 32) && lane == 0 && *(volatile int*)err) {
+    const unsigned long long t0 = now_ns();
+    while (now_ns() - t0 < 20000000ull) __nanosleep(1000);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 5) {
+    __syncwarp();
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * TCOLS) : "memory");
   }
 }
 

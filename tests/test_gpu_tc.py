@@ -76,15 +76,38 @@ def test_dense_bf16_split_k_eta_nu_two_calls(sk, oracle):
         check(s, o, "split-k")
 
 
-def test_dense_bf16_ragged_window(sk, oracle):
-    m, n = 777, 333
+@pytest.mark.parametrize("layout", ["C", "F"])
+@pytest.mark.parametrize("n", [333, 336])
+def test_dense_bf16_ragged_window(sk, oracle, layout, n):
+    # 129-row windows, the last one 3 rows. Strides that are not a multiple
+    # of 4 elements (n = 333 row-major, 129 / 3 column-major) take the
+    # separate conversion pass; the others are read as FP32 by the X^T product.
+    m = 777
     A = dense_input(m, n, seed=5).astype(np.float32)
-    a = bf16(alg(sk, m, n, 7, 129, 0, sketch_nu=0.5), sk)  # 129-row windows, last one 3 rows
+    A = np.asfortranarray(A) if layout == "F" else np.ascontiguousarray(A)
+    a = bf16(alg(sk, m, n, 7, 129, 0, sketch_nu=0.5), sk)
     o = oracle_for(oracle, a)
     o.linear_update(A.astype(np.float64))
     with sk.SketchySVD(a) as s:
         s.linear_update(A)
         check(s, o, "ragged")
+
+
+def test_dense_bf16_device_column_major_offsets(sk, oracle):
+    # a column-major device matrix (ld = m): windows start at rows 0, 96, 192
+    # (16-byte aligned: FP32 read by TMA) and the last window is ragged
+    import torch
+
+    m, n = 252, 512
+    A = dense_input(m, n, seed=12).astype(np.float32)
+    a = bf16(alg(sk, m, n, 5, 96, 0, sketch_eta=0.5), sk)
+    o = oracle_for(oracle, a)
+    o.linear_update(A.astype(np.float64))
+    At = torch.from_numpy(np.asfortranarray(A)).cuda().t().contiguous().t()
+    assert At.stride() == (1, m)
+    with sk.SketchySVD(a) as s:
+        s.linear_update(At)
+        check(s, o, "device-F")
 
 
 def test_rbf_bf16_parity(sk, oracle):
