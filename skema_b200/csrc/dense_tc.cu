@@ -28,14 +28,11 @@
 
 #include "internal.h"
 #include "tc_gemm.cuh"
+#include "tma.h"
 
 namespace skema {
 
 namespace {
-
-constexpr int kNT = 208;  // N tile of every product (k = 201, s = 403 pad to 208 / 416)
-
-int64_t pad8(int64_t x) { return (x + 7) / 8 * 8; }
 
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
@@ -51,9 +48,10 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   return fn;
 }
 
-// 2-D BF16 tensor map: dim0 contiguous (extent d0), dim1 with byte stride
-// st1, box {b0, b1}, 128-byte swizzle, out-of-range elements read as zero.
-CUtensorMap tmap_bf16(const void* base, uint64_t d0, uint64_t d1, uint64_t st1, uint32_t b0, uint32_t b1) {
+}  // namespace
+
+CUtensorMap tmap_2d(CUtensorMapDataType dtype, const void* base, uint64_t d0, uint64_t d1, uint64_t st1,
+                    uint32_t b0, uint32_t b1, CUtensorMapSwizzle swizzle) {
   if (reinterpret_cast<uintptr_t>(base) % 16) fail(SKEMA_EINVAL, "TMA base address not 16-byte aligned");
   if (st1 % 16) fail(SKEMA_EINVAL, "TMA row stride not a multiple of 16 bytes");
   CUtensorMap tm;
@@ -61,47 +59,52 @@ CUtensorMap tmap_bf16(const void* base, uint64_t d0, uint64_t d1, uint64_t st1, 
   cuuint64_t strides[1] = {st1};
   cuuint32_t box[2] = {b0, b1};
   cuuint32_t es[2] = {1, 1};
-  const CUresult r = encode_fn()(&tm, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims,
-                                 strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                                 CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+  const CUresult r = encode_fn()(&tm, dtype, 2, const_cast<void*>(base), dims, strides, box, es,
+                                 CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (r != CUDA_SUCCESS) fail(SKEMA_EINVAL, "cuTensorMapEncodeTiled rejected a tensor map");
+  if (r != CUDA_SUCCESS) fail(SKEMA_EINVAL, "cuTensorMapEncodeTiled rejected a 2-D tensor map");
   return tm;
 }
 
-// 2-D FP32 tensor map, 128-byte swizzle (box inner extent 32), OOB zero.
-CUtensorMap tmap_f32(const void* base, uint64_t d0, uint64_t d1, uint64_t st1, uint32_t b0, uint32_t b1) {
+CUtensorMap tmap_3d(CUtensorMapDataType dtype, const void* base, uint64_t d0, uint64_t d1, uint64_t d2,
+                    uint64_t st1, uint64_t st2, uint32_t b0, uint32_t b1, uint32_t b2,
+                    CUtensorMapSwizzle swizzle) {
   if (reinterpret_cast<uintptr_t>(base) % 16) fail(SKEMA_EINVAL, "TMA base address not 16-byte aligned");
-  if (st1 % 16) fail(SKEMA_EINVAL, "TMA row stride not a multiple of 16 bytes");
+  if (st1 % 16 || st2 % 16) fail(SKEMA_EINVAL, "TMA stride not a multiple of 16 bytes");
   CUtensorMap tm;
-  cuuint64_t dims[2] = {d0, d1};
-  cuuint64_t strides[1] = {st1};
-  cuuint32_t box[2] = {b0, b1};
-  cuuint32_t es[2] = {1, 1};
-  const CUresult r = encode_fn()(&tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void*>(base), dims,
-                                 strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                                 CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (r != CUDA_SUCCESS) fail(SKEMA_EINVAL, "cuTensorMapEncodeTiled rejected an FP32 tensor map");
-  return tm;
-}
-
-// 3-D BF16 tensor map of the row-blocked window: {64, d1, d2} with the
-// 64-element lines contiguous, byte strides 128 (dim1) and d1 * 128 (dim2),
-// box {64, b1, 1}.
-CUtensorMap tmap_bf16_blocked(const void* base, uint64_t d1, uint64_t d2, uint32_t b1) {
-  if (reinterpret_cast<uintptr_t>(base) % 16) fail(SKEMA_EINVAL, "TMA base address not 16-byte aligned");
-  CUtensorMap tm;
-  cuuint64_t dims[3] = {64, d1, d2};
-  cuuint64_t strides[2] = {128, d1 * 128};
-  cuuint32_t box[3] = {64, b1, 1};
+  cuuint64_t dims[3] = {d0, d1, d2};
+  cuuint64_t strides[2] = {st1, st2};
+  cuuint32_t box[3] = {b0, b1, b2};
   cuuint32_t es[3] = {1, 1, 1};
-  const CUresult r = encode_fn()(&tm, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<void*>(base), dims,
-                                 strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                                 CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+  const CUresult r = encode_fn()(&tm, dtype, 3, const_cast<void*>(base), dims, strides, box, es,
+                                 CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (r != CUDA_SUCCESS) fail(SKEMA_EINVAL, "cuTensorMapEncodeTiled rejected a blocked tensor map");
+  if (r != CUDA_SUCCESS) fail(SKEMA_EINVAL, "cuTensorMapEncodeTiled rejected a 3-D tensor map");
   return tm;
+}
+
+namespace {
+
+constexpr int kNT = 208;  // N tile of every product (k = 201, s = 403 pad to 208 / 416)
+
+int64_t pad8(int64_t x) { return (x + 7) / 8 * 8; }
+
+// 2-D BF16 map, 128-byte swizzle.
+CUtensorMap tmap_bf16(const void* base, uint64_t d0, uint64_t d1, uint64_t st1, uint32_t b0, uint32_t b1) {
+  return tmap_2d(CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, base, d0, d1, st1, b0, b1, CU_TENSOR_MAP_SWIZZLE_128B);
+}
+
+// 2-D FP32 map, 128-byte swizzle (box inner extent 32).
+CUtensorMap tmap_f32(const void* base, uint64_t d0, uint64_t d1, uint64_t st1, uint32_t b0, uint32_t b1) {
+  return tmap_2d(CU_TENSOR_MAP_DATA_TYPE_FLOAT32, base, d0, d1, st1, b0, b1, CU_TENSOR_MAP_SWIZZLE_128B);
+}
+
+// 3-D BF16 map of the row-blocked window: {64, d1, d2} with the 64-element
+// lines contiguous, byte strides 128 (dim1) and d1 * 128 (dim2), box
+// {64, b1, 1}.
+CUtensorMap tmap_bf16_blocked(const void* base, uint64_t d1, uint64_t d2, uint32_t b1) {
+  return tmap_3d(CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, base, 64, d1, d2, 128, d1 * 128, 64, b1, 1,
+                 CU_TENSOR_MAP_SWIZZLE_128B);
 }
 
 // The window in BF16, row-blocked: element (i, j) of a rows x cols block at

@@ -191,6 +191,28 @@ def test_csr_device_input_and_eta_nu(sk, oracle):
         check_sketches(s, o)
 
 
+@pytest.mark.parametrize("m", [1000, 1001])
+def test_csr_blocks_dirty_rows_and_offsets(sk, oracle, m):
+    # Both forms of the Y kernel: the TMA write-out (clean rows, first row a
+    # multiple of 4, m a multiple of 4) and the per-lane write-out (any other
+    # start row, odd m, rows updated a second time with the nu term).
+    n = 700
+    A = csr_input(m, n, nnz_row=9, seed=13)
+    a = alg(sk, m, n, 5, 100, 1, issparse=True, sketch_eta=0.75, sketch_nu=0.9)
+    o = oracle_for(oracle, a)
+    o.reset()
+    # (500, 3): a 3-row TMA tile clipped at row 503, whose rows must stay
+    # untouched until the (503, ...) call writes them
+    calls = [(0, 500), (500, 3), (503, m - 503), (0, 500), (200, 300)]
+    for r0, nr in calls:
+        o.update_rows(A, r0, nr)
+    with sk.SketchySVD(a) as s:
+        s.reset()
+        for r0, nr in calls:
+            s.update_rows(A[r0:r0 + nr], r0)
+        check_sketches(s, o)
+
+
 def test_csr_duplicate_columns_are_summed(sk, oracle):
     m, n = 64, 40
     rowptr = np.arange(0, 3 * m + 1, 3, dtype=np.int64)
