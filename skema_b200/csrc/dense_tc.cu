@@ -27,8 +27,7 @@
 #include <mutex>
 
 #include "internal.h"
-#include "tc_gemm.cuh"
-#include "tma.h"
+#include "tc_host.h"
 
 namespace skema {
 
@@ -83,16 +82,49 @@ CUtensorMap tmap_3d(CUtensorMapDataType dtype, const void* base, uint64_t d0, ui
   return tm;
 }
 
-namespace {
-
-constexpr int kNT = 208;  // N tile of every product (k = 201, s = 403 pad to 208 / 416)
-
-int64_t pad8(int64_t x) { return (x + 7) / 8 * 8; }
-
-// 2-D BF16 map, 128-byte swizzle.
 CUtensorMap tmap_bf16(const void* base, uint64_t d0, uint64_t d1, uint64_t st1, uint32_t b0, uint32_t b1) {
   return tmap_2d(CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, base, d0, d1, st1, b0, b1, CU_TENSOR_MAP_SWIZZLE_128B);
 }
+
+Plan plan_split(const skema_ctx* c, int64_t tiles, int64_t K, int max_ks) {
+  const int64_t ksteps = (K + tc::BK - 1) / tc::BK;
+  int best = 1;
+  double best_cost = 1e300;
+  for (int ks = 1; ks <= max_ks; ++ks) {
+    if (ks > 1 && ksteps / ks < 8) break;  // at least 8 k-steps per split
+    const int64_t waves = (tiles * ks + c->sm_count - 1) / c->sm_count;
+    const double cost = (double)waves * ((double)ksteps / ks + 6.0);
+    if (cost < best_cost * 0.97) {
+      best_cost = cost;
+      best = ks;
+    }
+  }
+  const int64_t kchunk = (ksteps + best - 1) / best * tc::BK;
+  const int ks = (int)((K + kchunk - 1) / kchunk);
+  return Plan{ks, kchunk};
+}
+
+Plan plan_split_stream(const skema_ctx* c, int64_t tiles, int64_t K, int max_ks) {
+  const int64_t ksteps = (K + tc::BK - 1) / tc::BK;
+  int64_t ks = (8 * (int64_t)c->sm_count + tiles - 1) / tiles;
+  ks = std::max<int64_t>(1, std::min<int64_t>({ks, (int64_t)max_ks, ksteps / 8}));
+  const int64_t kchunk = (ksteps + ks - 1) / ks * tc::BK;
+  return Plan{(int)((K + kchunk - 1) / kchunk), kchunk};
+}
+
+tc::OutSpec out_spec() {
+  tc::OutSpec o;
+  o.p0 = nullptr, o.p1 = nullptr, o.p1f = nullptr;
+  o.rs0 = o.cs0 = o.rs1 = o.cs1 = 0;
+  o.alpha0 = 1.f, o.beta0 = 0.f, o.alpha1 = 1.f, o.beta1 = 0.f;
+  o.rows = 0, o.split = 0, o.ncols = 0;
+  o.atomic0 = 0, o.atomic1 = 0;
+  return o;
+}
+
+namespace {
+
+constexpr int kNT = 208;  // N tile of every product (k = 201, s = 403 pad to 208 / 416)
 
 // 2-D FP32 map, 128-byte swizzle (box inner extent 32).
 CUtensorMap tmap_f32(const void* base, uint64_t d0, uint64_t d1, uint64_t st1, uint32_t b0, uint32_t b1) {
@@ -106,7 +138,6 @@ CUtensorMap tmap_bf16_blocked(const void* base, uint64_t d1, uint64_t d2, uint32
   return tmap_3d(CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, base, 64, d1, d2, 128, d1 * 128, 64, b1, 1,
                  CU_TENSOR_MAP_SWIZZLE_128B);
 }
-
 // The window in BF16, row-blocked: element (i, j) of a rows x cols block at
 // D[((i / 64) * cols + j) * 64 + i % 64], i.e. for each 64-row block the
 // columns one after another, each a 128-byte line of 64 rows. Rows past
@@ -218,6 +249,8 @@ __global__ void to_bf16_tiled_kernel(const float* __restrict__ S, int64_t srs, i
   }
 }
 
+}  // namespace
+
 void to_bf16(skema_ctx* c, Mat src, int64_t rows, int64_t cols, __nv_bfloat16* D, int64_t drs, int64_t dcs) {
   if (rows <= 0 || cols <= 0) return;
   const int64_t tiles = ((rows + 31) / 32) * ((cols + 31) / 32);
@@ -225,6 +258,8 @@ void to_bf16(skema_ctx* c, Mat src, int64_t rows, int64_t cols, __nv_bfloat16* D
   to_bf16_tiled_kernel<<<grid, dim3(32, 8), 0, c->stream>>>(src.p, src.rs, src.cs, rows, cols, D, drs, dcs);
   SKEMA_LAUNCHED(c);
 }
+
+namespace {
 
 // BF16 column-major (ld) <- FP32 column-major (ld), rows x cols.
 __global__ void f32_to_bf16_cm_kernel(const float* __restrict__ S, __nv_bfloat16* __restrict__ D, int64_t rows,
@@ -235,43 +270,6 @@ __global__ void f32_to_bf16_cm_kernel(const float* __restrict__ S, __nv_bfloat16
     const int64_t j = q / rows, i = q - j * rows;
     D[i + j * ld] = __float2bfloat16(S[i + j * ld]);
   }
-}
-
-struct Plan {
-  int ks;
-  int64_t kchunk;
-};
-
-// Split of K that minimises the estimated critical path in k-steps: waves of
-// one CTA per SM times the k-steps of one split, plus a fixed cost per tile
-// for the pipeline fill and the epilogue.
-Plan plan_split(const skema_ctx* c, int64_t tiles, int64_t K, int max_ks) {
-  const int64_t ksteps = (K + tc::BK - 1) / tc::BK;
-  int best = 1;
-  double best_cost = 1e300;
-  for (int ks = 1; ks <= max_ks; ++ks) {
-    if (ks > 1 && ksteps / ks < 8) break;  // at least 8 k-steps per split
-    const int64_t waves = (tiles * ks + c->sm_count - 1) / c->sm_count;
-    const double cost = (double)waves * ((double)ksteps / ks + 6.0);
-    if (cost < best_cost * 0.97) {
-      best_cost = cost;
-      best = ks;
-    }
-  }
-  const int64_t kchunk = (ksteps + best - 1) / best * tc::BK;
-  const int ks = (int)((K + kchunk - 1) / kchunk);
-  return Plan{ks, kchunk};
-}
-
-// Split for a product bound by HBM rather than by the tensor pipe: enough
-// units (about eight rounds over the SMs) that the last round is a small
-// fraction of the whole, with at least 8 k-steps per unit.
-Plan plan_split_stream(const skema_ctx* c, int64_t tiles, int64_t K, int max_ks) {
-  const int64_t ksteps = (K + tc::BK - 1) / tc::BK;
-  int64_t ks = (8 * (int64_t)c->sm_count + tiles - 1) / tiles;
-  ks = std::max<int64_t>(1, std::min<int64_t>({ks, (int64_t)max_ks, ksteps / 8}));
-  const int64_t kchunk = (ksteps + ks - 1) / ks * tc::BK;
-  return Plan{(int)((K + kchunk - 1) / kchunk), kchunk};
 }
 
 // Persistent launch: min(units, SMs) CTAs of one per SM (the 5-stage ring
@@ -321,17 +319,53 @@ void launch_gemm_a32(skema_ctx* c, const CUtensorMap& ta32, const CUtensorMap& t
   c->dev_err_armed = true;
 }
 
-tc::OutSpec out_spec() {
-  tc::OutSpec o;
-  o.p0 = nullptr, o.p1 = nullptr, o.p1f = nullptr;
-  o.rs0 = o.cs0 = o.rs1 = o.cs1 = 0;
-  o.alpha0 = 1.f, o.beta0 = 0.f, o.alpha1 = 1.f, o.beta1 = 0.f;
-  o.rows = 0, o.split = 0, o.ncols = 0;
-  o.atomic0 = 0, o.atomic1 = 0;
-  return o;
+}  // namespace
+
+void t32_to_t16(skema_ctx* c, const float* T32, __nv_bfloat16* T16, int64_t rows, int64_t cols, int64_t ld) {
+  if (rows <= 0 || cols <= 0) return;
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((rows * cols + 255) / 256, c->sm_count * 16));
+  f32_to_bf16_cm_kernel<<<grid, 256, 0, c->stream>>>(T32, T16, rows, cols, ld);
+  SKEMA_LAUNCHED(c);
 }
 
-}  // namespace
+size_t tc_slice_bytes(const skema_ctx* c, int64_t wr) {
+  return sizeof(__nv_bfloat16) * (size_t)((c->k + c->s) * pad8(wr)) + 512;
+}
+
+TcSlices tc_window_slices(skema_ctx* c, int64_t R0, int64_t wr, char** sp) {
+  TcSlices sl{static_cast<const __nv_bfloat16*>(c->ups.lowp) + R0,
+              static_cast<const __nv_bfloat16*>(c->phi.lowp) + R0, c->ld_maps16};
+  if (R0 % 8 == 0) return sl;
+  const int64_t wp = pad8(wr);
+  auto take = [&](size_t bytes) {
+    char* p = *sp;
+    *sp += (bytes + 255) / 256 * 256;
+    return reinterpret_cast<__nv_bfloat16*>(p);
+  };
+  __nv_bfloat16* us = take(sizeof(__nv_bfloat16) * (size_t)(c->k * wp));
+  __nv_bfloat16* fs = take(sizeof(__nv_bfloat16) * (size_t)(c->s * wp));
+  to_bf16(c, Mat{c->ups.f32 + R0 * c->ups.cs, c->ups.rs, c->ups.cs}, c->k, wr, us, wp, 1);
+  to_bf16(c, Mat{c->phi.f32 + R0 * c->phi.cs, c->phi.rs, c->phi.cs}, c->s, wr, fs, wp, 1);
+  return TcSlices{us, fs, wp};
+}
+
+void tc_z_update(skema_ctx* c, const __nv_bfloat16* T16, int64_t wp, const TcSlices& sl, int64_t wr) {
+  const float eta = (float)c->p.sketch_eta, nu = (float)c->p.sketch_nu;
+  const int64_t s = c->s;
+  StageScope st(c, ST_PHI);
+  const CUtensorMap ta = tmap_bf16(T16, (uint64_t)wr, (uint64_t)s, (uint64_t)wp * 2, 64, 128);
+  const CUtensorMap tb = tmap_bf16(sl.F16, (uint64_t)wr, (uint64_t)s, (uint64_t)sl.ldm * 2, 64, kNT);
+  const int64_t tiles = ((s + 127) / 128) * ((s + kNT - 1) / kNT);
+  const Plan pl = plan_split(c, tiles, wr, 32);
+  tc::OutSpec o = out_spec();
+  o.p0 = c->Z, o.rs0 = 1, o.cs0 = s, o.alpha0 = eta, o.beta0 = nu;
+  o.rows = s, o.split = s, o.ncols = s;
+  if (pl.ks > 1) {
+    scale_block(c, MatOut{c->Z, s, 1}, s, s, nu);
+    o.atomic0 = 1, o.beta0 = 0.f;
+  }
+  launch_gemm<tc::A_KMAJ>(c, ta, tb, s, s, wr, pl, 0, o);
+}
 
 bool tc_available(const skema_ctx* c) {
   return c->p.precision == SKEMA_PREC_BF16 && c->ups.lowp && c->phi.lowp && c->op16;
@@ -365,7 +399,7 @@ size_t tc_scratch_bytes(const skema_ctx* c, int64_t wr) {
   size_t b = sizeof(__nv_bfloat16) * (size_t)(w64 * c->n) + 256;        // A16 (row-blocked)
   b += sizeof(__nv_bfloat16) * (size_t)(wp * c->s) + 256;               // T16
   b += sizeof(float) * (size_t)(wp * c->s) + 256;                       // T32 (split-K)
-  b += sizeof(__nv_bfloat16) * (size_t)((c->k + c->s) * wp) + 512;      // map slices (unaligned R0)
+  b += tc_slice_bytes(c, wr);                                           // map slices (unaligned R0)
   return b;
 }
 
@@ -394,24 +428,10 @@ void tc_dense_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr, void* scratch
     StageScope st(c, ST_WINDOW);
     to_bf16_blocked(c, Aw, wr, n, A16);
   }
-  // Upsilon~ / Phi~ columns of this window: in place when R0 keeps the
-  // 16-byte alignment TMA needs, else converted into an aligned slice.
-  const __nv_bfloat16* U16 = static_cast<const __nv_bfloat16*>(c->ups.lowp) + R0;
-  const __nv_bfloat16* F16 = static_cast<const __nv_bfloat16*>(c->phi.lowp) + R0;
-  int64_t ldm = c->ld_maps16;
-  if (R0 % 8 != 0) {
-    __nv_bfloat16* us = reinterpret_cast<__nv_bfloat16*>(take(sizeof(__nv_bfloat16) * (size_t)(k * wp)));
-    __nv_bfloat16* fs = reinterpret_cast<__nv_bfloat16*>(take(sizeof(__nv_bfloat16) * (size_t)(s * wp)));
-    to_bf16(c, Mat{c->ups.f32 + R0 * c->ups.cs, c->ups.rs, c->ups.cs}, k, wr, us, wp, 1);
-    to_bf16(c, Mat{c->phi.f32 + R0 * c->phi.cs, c->phi.rs, c->phi.cs}, s, wr, fs, wp, 1);
-    U16 = us;
-    F16 = fs;
-    ldm = wp;
-  }
-  const uint64_t wp2 = (uint64_t)wp * 2;
+  const TcSlices sl = tc_window_slices(c, R0, wr, &sp);
   {  // X^T = nu X^T + eta A_w^T Upsilon~_w^T
     StageScope st(c, ST_UPSILON);
-    const CUtensorMap tb = tmap_bf16(U16, (uint64_t)wr, (uint64_t)k, (uint64_t)ldm * 2, 64, kNT);
+    const CUtensorMap tb = tmap_bf16(sl.U16, (uint64_t)wr, (uint64_t)k, (uint64_t)sl.ldm * 2, 64, kNT);
     const int64_t tiles = ((n + 127) / 128) * ((k + kNT - 1) / kNT);
     const Plan pl = (a32_cm || a32_rm) ? plan_split_stream(c, tiles, wr, 8) : plan_split(c, tiles, wr, 8);
     tc::OutSpec o = out_spec();
@@ -450,28 +470,10 @@ void tc_dense_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr, void* scratch
       o.p1f = T32, o.rs1 = 1, o.cs1 = wp, o.atomic1 = 1;
     }
     launch_gemm<tc::A_MN_BLK>(c, ta, tb, wr, k + s, n, pl, 0, o);
-    if (pl.ks > 1) {
-      const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((wr * s + 255) / 256, c->sm_count * 16));
-      f32_to_bf16_cm_kernel<<<grid, 256, 0, c->stream>>>(T32, T16, wr, s, wp);
-      SKEMA_LAUNCHED(c);
-    }
+    if (pl.ks > 1) t32_to_t16(c, T32, T16, wr, s, wp);
   }
   y_rows_mark(c, R0, R0 + wr);
-  {  // Z^T = nu Z^T + eta T^T Phi~_w^T
-    StageScope st(c, ST_PHI);
-    const CUtensorMap ta = tmap_bf16(T16, (uint64_t)wr, (uint64_t)s, wp2, 64, 128);
-    const CUtensorMap tb = tmap_bf16(F16, (uint64_t)wr, (uint64_t)s, (uint64_t)ldm * 2, 64, kNT);
-    const int64_t tiles = ((s + 127) / 128) * ((s + kNT - 1) / kNT);
-    const Plan pl = plan_split(c, tiles, wr, 32);
-    tc::OutSpec o = out_spec();
-    o.p0 = c->Z, o.rs0 = 1, o.cs0 = s, o.alpha0 = eta, o.beta0 = nu;
-    o.rows = s, o.split = s, o.ncols = s;
-    if (pl.ks > 1) {
-      scale_block(c, MatOut{c->Z, s, 1}, s, s, nu);
-      o.atomic0 = 1, o.beta0 = 0.f;
-    }
-    launch_gemm<tc::A_KMAJ>(c, ta, tb, s, s, wr, pl, 0, o);
-  }
+  tc_z_update(c, T16, wp, sl, wr);
 }
 
 }  // namespace skema

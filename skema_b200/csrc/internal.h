@@ -202,6 +202,10 @@ void csr_update(skema_ctx* c, const int64_t* rowptr, const int32_t* col,
 void dense_ssign_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr);
 void spd_ssign_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr);
 
+// ---- RBF, BF16 tensor-core form without a stored kernel (rbf_tc.cu) ----
+bool rbf_tc_supported(const skema_ctx* c, int64_t d);
+void rbf_tc_update(skema_ctx* c, Mat P, int64_t npts, int64_t d, int64_t row0, int64_t nrows);
+
 // ---- RBF (rbf.cu) ----
 void rbf_update(skema_ctx* c, Mat P, int64_t npts, int64_t d, int64_t row0,
                 int64_t nrows);

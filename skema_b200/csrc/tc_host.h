@@ -1,0 +1,49 @@
+// tc_host.h -- host-side pieces shared by the tensor-core forms of the
+// sketch (dense windows in dense_tc.cu, Gauss-RBF windows in rbf_tc.cu).
+#pragma once
+#include <cuda_bf16.h>
+
+#include "internal.h"
+#include "tc_gemm.cuh"
+#include "tma.h"
+
+namespace skema {
+
+inline int64_t pad8(int64_t x) { return (x + 7) / 8 * 8; }
+
+// A split of K into ks ranges of kchunk (a multiple of 64).
+struct Plan {
+  int ks;
+  int64_t kchunk;
+};
+// Split that minimises waves x (k-steps per split + fill) for a product
+// bound by the tensor pipe, one CTA per SM.
+Plan plan_split(const skema_ctx* c, int64_t tiles, int64_t K, int max_ks);
+// Split for an HBM-bound product: about eight rounds of units over the SMs.
+Plan plan_split_stream(const skema_ctx* c, int64_t tiles, int64_t K, int max_ks);
+
+tc::OutSpec out_spec();
+
+CUtensorMap tmap_bf16(const void* base, uint64_t d0, uint64_t d1, uint64_t st1, uint32_t b0, uint32_t b1);
+
+// FP32 strided block -> BF16 with D(i, j) at D[i * drs + j * dcs].
+void to_bf16(skema_ctx* c, Mat src, int64_t rows, int64_t cols, __nv_bfloat16* D, int64_t drs, int64_t dcs);
+// BF16 column-major (ld) <- FP32 column-major (ld), rows x cols.
+void t32_to_t16(skema_ctx* c, const float* T32, __nv_bfloat16* T16, int64_t rows, int64_t cols, int64_t ld);
+
+// The window's columns of the BF16 Upsilon~ / Phi~ copies as TMA operands:
+// in place when R0 is a multiple of 8 (16-byte aligned), else converted
+// into scratch taken from *sp (k x wp and s x wp, 256-byte aligned).
+struct TcSlices {
+  const __nv_bfloat16* U16;
+  const __nv_bfloat16* F16;
+  int64_t ldm;
+};
+TcSlices tc_window_slices(skema_ctx* c, int64_t R0, int64_t wr, char** sp);
+size_t tc_slice_bytes(const skema_ctx* c, int64_t wr);
+
+// Z = nu Z + eta Phi~_w T for the window's T (BF16, wr x s column-major,
+// ld wp), as Z^T = T^T Phi~_w^T on the tensor cores.
+void tc_z_update(skema_ctx* c, const __nv_bfloat16* T16, int64_t wp, const TcSlices& sl, int64_t wr);
+
+}  // namespace skema

@@ -1,0 +1,307 @@
+// tc_rbf.cuh -- the Gauss-RBF kernel sketch without materialising K:
+// O = P V with P(q, j) = exp(-gamma ||x_q - x_j||^2) generated tile by
+// tile on the tensor cores (sm_100a tcgen05, TMEM accumulators, TMA).
+//
+// For one unit (128 "query" points q, one chunk of output columns, one
+// range of 64-point "key" blocks j):
+//   Gram     S = Q K_b^T            tcgen05, M = 128, N = 64, K = d (BF16)
+//   kernel   P = exp2(2 g' S + c_q + c_j), with c_p = -g' ||x_p||^2 and
+//            g' = gamma * log2(e), clamped at 1 (d^2 >= 0), 1 on the
+//            diagonal point q == point j (the reference's window rule),
+//            written as BF16 into 128-byte-swizzled shared memory
+//   sketch   O += P V_b             tcgen05, M = 128, N = NC1 (+ NC2), K = 64
+// where V_b holds the output columns' map entries for the 64 key points,
+// K-major (one row per output column). Gram tiles of the next block are
+// computed while the kernel warps exponentiate the current one, and the
+// sketch product of a block runs while the next block is exponentiated.
+//
+//   row pass (Y / T of a window):  q = window rows, j = all points,
+//                                  V = [Omega~; Psi~] (output = k + s columns)
+//   column pass (X of a window):   q = all points, j = window rows,
+//                                  V = Upsilon~ restricted to the window
+//
+// Roles (192 threads): warps 0-3 kernel-tile warps and epilogue (warp w owns
+// TMEM lanes 32w..32w+31, i.e. query rows), warp 4 TMA producer, warp 5 MMA
+// issuer and TMEM owner. Every wait is bounded (see tc_gemm.cuh).
+#pragma once
+#include "tc_gemm.cuh"
+
+namespace skema {
+namespace tc {
+
+constexpr int RBF_BQ = 128;  // query rows per unit (TMEM lanes)
+constexpr int RBF_BJ = 64;   // key points per block
+constexpr int RBF_S = 2;     // key/value stages
+constexpr uint32_t RBF_SCOL = 448;  // TMEM column of the Gram tile (O uses [0, 448))
+
+// 2^x by the PTX ex2.approx instruction (relative error about 2^-22, far
+// below the BF16 rounding of the result); 2^-inf = 0.
+__device__ __forceinline__ float ex2_approx(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+struct RbfArgs {
+  int64_t nq;          // valid query rows (rows >= nq are ignored)
+  int64_t qbase;       // point index of query row 0
+  int64_t kbase;       // point index of key column 0 (diagonal test)
+  int64_t nblocks;     // key blocks in total (64 points each)
+  int64_t bchunk;      // key blocks per split
+  int qtiles, nchunks, ksplit;
+  int chunk_cols;      // output columns per chunk (NC1 + NC2)
+  const float* cq;     // c_p of the query points, indexed by query row
+  const float* ckey;   // c_p of the key points, indexed by key column, padded with -inf
+  float two_g;         // 2 * gamma * log2(e)
+};
+
+template <int NC1, int NC2, int DK>
+__global__ void __launch_bounds__(kThreads, 1)
+    rbf_sketch_kernel(const __grid_constant__ CUtensorMap tmQ, const __grid_constant__ CUtensorMap tmK,
+                      const __grid_constant__ CUtensorMap tmV1, const __grid_constant__ CUtensorMap tmV2,
+                      RbfArgs a, OutSpec o, int* err) {
+  constexpr int NC = NC1 + NC2;
+  static_assert(NC1 % 16 == 0 && NC1 <= 256 && NC2 % 16 == 0 && NC2 <= 256, "chunk tiles");
+  static_assert(NC <= (int)RBF_SCOL, "O and the Gram tile share TMEM");
+  constexpr uint32_t Q_BYTES = DK * RBF_BQ * 128;      // DK sub-tiles of 64 d-values
+  constexpr uint32_t K_BYTES = DK * RBF_BJ * 128;
+  constexpr uint32_t V_BYTES = NC * 128;               // NC rows of 64 key values
+  constexpr uint32_t STAGE = ((K_BYTES + V_BYTES + 256 + 1023) / 1024) * 1024;  // + c_key of the block
+  constexpr uint32_t P_BYTES = RBF_BQ * 128;           // 128 rows of 64 BF16
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char* smem = reinterpret_cast<unsigned char*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+  unsigned char* qs = smem;
+  unsigned char* st = qs + Q_BYTES;
+  unsigned char* ps = st + RBF_S * STAGE;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(ps + 2 * P_BYTES);
+  uint64_t* qfull = bar + 0;
+  uint64_t* qempty = bar + 1;
+  uint64_t* full = bar + 2;              // [RBF_S]
+  uint64_t* empty = full + RBF_S;        // [RBF_S]
+  uint64_t* sfull = empty + RBF_S;
+  uint64_t* sfree = sfull + 1;
+  uint64_t* pfull = sfree + 1;           // [2]
+  uint64_t* pfree = pfull + 2;           // [2]
+  uint64_t* ofull = pfree + 2;
+  uint64_t* ofree = ofull + 1;
+  uint32_t* tbase = reinterpret_cast<uint32_t*>(ofree + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int total = a.qtiles * a.nchunks * a.ksplit;
+
+  if (threadIdx.x == 0) {
+    mbar_init(qfull, 1);
+    mbar_init(qempty, 1);
+    for (int s = 0; s < RBF_S; ++s) {
+      mbar_init(full + s, 1);
+      mbar_init(empty + s, 1);
+    }
+    mbar_init(sfull, 1);
+    mbar_init(sfree, 128);
+    for (int p = 0; p < 2; ++p) {
+      mbar_init(pfull + p, 128);
+      mbar_init(pfree + p, 1);
+    }
+    mbar_init(ofull, 1);
+    mbar_init(ofree, 128);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 5) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tbase)),
+                 "r"(512)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tbase;
+
+  // unit t -> (query tile, chunk, key split), chunk fastest
+  auto decode = [&](int t, int& qt, int& ch, int& ks, int64_t& b0, int64_t& b1) {
+    ch = t % a.nchunks;
+    t /= a.nchunks;
+    qt = t % a.qtiles;
+    ks = t / a.qtiles;
+    b0 = (int64_t)ks * a.bchunk;
+    b1 = min(a.nblocks, b0 + a.bchunk);
+  };
+
+  if (warp == 4 && lane == 0) {
+    // ---------------- TMA producer ----------------
+    uint32_t it = 0, un = 0;
+    bool ok = true;
+    for (int t = blockIdx.x; t < total && ok; t += gridDim.x, ++un) {
+      int qt, ch, ks;
+      int64_t b0, b1;
+      decode(t, qt, ch, ks, b0, b1);
+      if (!mbar_wait(qempty, (un & 1) ^ 1, err)) break;
+      mbar_expect_tx(qfull, Q_BYTES);
+#pragma unroll
+      for (int dk = 0; dk < DK; ++dk)
+        tma_load_2d(&tmQ, qfull, qs + dk * RBF_BQ * 128, 64 * dk, (int)(a.qbase + (int64_t)qt * RBF_BQ));
+      for (int64_t b = b0; b < b1; ++b, ++it) {
+        const int s = it % RBF_S;
+        const uint32_t ph = (it / RBF_S) & 1;
+        if (!mbar_wait(empty + s, ph ^ 1, err)) {
+          ok = false;
+          break;
+        }
+        unsigned char* sk = st + s * STAGE;
+        mbar_expect_tx(full + s, K_BYTES + V_BYTES + 256);
+#pragma unroll
+        for (int dk = 0; dk < DK; ++dk)
+          tma_load_2d(&tmK, full + s, sk + dk * RBF_BJ * 128, 64 * dk, (int)(a.kbase + b * RBF_BJ));
+        tma_load_2d(&tmV1, full + s, sk + K_BYTES, (int)(b * RBF_BJ), ch * NC);
+        if (NC2 > 0) tma_load_2d(&tmV2, full + s, sk + K_BYTES + NC1 * 128, (int)(b * RBF_BJ), ch * NC + NC1);
+        // the 64 key constants of the block (256 bytes)
+        asm volatile(
+            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], 256, [%2];" ::"r"(
+                smem_u32(sk + K_BYTES + V_BYTES)),
+            "l"(a.ckey + b * RBF_BJ), "r"(smem_u32(full + s))
+            : "memory");
+      }
+    }
+  } else if (warp == 5 && lane == 0) {
+    // ---------------- MMA issuer ----------------
+    constexpr uint32_t id_g = idesc_bf16(RBF_BJ, false, false);
+    constexpr uint32_t id_1 = idesc_bf16(NC1, false, false);
+    constexpr uint32_t id_2 = idesc_bf16(NC2 > 0 ? NC2 : 16, false, false);
+    const uint32_t tS = tmem + RBF_SCOL;
+    uint32_t it = 0, un = 0, g = 0, pc = 0;
+    bool ok = true;
+    // O += P_b V_b for the block whose P is in buffer pc % 2 and whose V is in stage s
+    auto sketch = [&](int s, bool first) -> bool {
+      const uint32_t pb = pc & 1;
+      if (!mbar_wait(pfull + pb, (pc >> 1) & 1, err)) return false;
+      tc_fence_after();
+      const uint32_t pa = smem_u32(ps + pb * P_BYTES);
+      const uint32_t vb = smem_u32(st + s * STAGE + K_BYTES);
+#pragma unroll
+      for (int kk = 0; kk < RBF_BJ / 16; ++kk) {
+        const uint32_t acc = (!first || kk > 0) ? 1u : 0u;
+        umma(tmem, sdesc(pa + kk * 32, 16, 1024), sdesc(vb + kk * 32, 16, 1024), id_1, acc);
+        if (NC2 > 0)
+          umma(tmem + NC1, sdesc(pa + kk * 32, 16, 1024), sdesc(vb + NC1 * 128 + kk * 32, 16, 1024), id_2, acc);
+      }
+      umma_commit(empty + s);
+      umma_commit(pfree + pb);
+      ++pc;
+      return true;
+    };
+    for (int t = blockIdx.x; t < total && ok; t += gridDim.x, ++un) {
+      int qt, ch, ks;
+      int64_t b0, b1;
+      decode(t, qt, ch, ks, b0, b1);
+      if (!mbar_wait(qfull, un & 1, err)) break;
+      int prev_s = -1;
+      bool first = true;
+      for (int64_t b = b0; b < b1; ++b, ++it) {
+        const int s = it % RBF_S;
+        const uint32_t ph = (it / RBF_S) & 1;
+        if (!mbar_wait(full + s, ph, err) || !mbar_wait(sfree, (g & 1) ^ 1, err)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t qa = smem_u32(qs), kb = smem_u32(st + s * STAGE);
+#pragma unroll
+        for (int dk = 0; dk < DK; ++dk)
+#pragma unroll
+          for (int kk = 0; kk < 4; ++kk)
+            umma(tS, sdesc(qa + dk * RBF_BQ * 128 + kk * 32, 16, 1024),
+                 sdesc(kb + dk * RBF_BJ * 128 + kk * 32, 16, 1024), id_g, (dk > 0 || kk > 0) ? 1u : 0u);
+        umma_commit(sfull);
+        ++g;
+        if (b + 1 == b1) umma_commit(qempty);
+        if (prev_s >= 0) {
+          if (first && !mbar_wait(ofree, (un & 1) ^ 1, err)) {
+            ok = false;
+            break;
+          }
+          if (!sketch(prev_s, first)) {
+            ok = false;
+            break;
+          }
+          first = false;
+        }
+        prev_s = s;
+      }
+      if (!ok) break;
+      if (prev_s >= 0) {
+        if (first && !mbar_wait(ofree, (un & 1) ^ 1, err)) break;
+        if (!sketch(prev_s, first)) break;
+      }
+      umma_commit(ofull);
+    }
+  } else if (warp < 4) {
+    // ---------------- kernel tiles + epilogue ----------------
+    const uint32_t lane_off = (uint32_t)(warp * 32) << 16;
+    uint32_t it = 0, un = 0, g = 0, pc = 0;
+    for (int t = blockIdx.x; t < total; t += gridDim.x, ++un) {
+      int qt, ch, ks;
+      int64_t b0, b1;
+      decode(t, qt, ch, ks, b0, b1);
+      const int64_t qrow = (int64_t)qt * RBF_BQ + warp * 32 + lane;  // query row of this thread
+      const float cq = qrow < a.nq ? a.cq[qrow] : 0.f;
+      const int64_t gq = a.qbase + qrow;                              // its point index
+      bool ok = true;
+      for (int64_t b = b0; b < b1; ++b, ++it, ++g, ++pc) {
+        if (!__all_sync(0xffffffffu, mbar_wait(sfull, g & 1, err))) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        float sv[64];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) tmem_ld16(tmem + RBF_SCOL + lane_off + 16 * c, sv + 16 * c);
+        tc_fence_before();
+        mbar_arrive(sfree);
+        const uint32_t pb = pc & 1;
+        if (!__all_sync(0xffffffffu, mbar_wait(pfree + pb, ((pc >> 1) & 1) ^ 1, err))) {
+          ok = false;
+          break;
+        }
+        const float* ck = reinterpret_cast<const float*>(st + (it % RBF_S) * STAGE + K_BYTES + V_BYTES);
+        const int64_t dcol = gq - (a.kbase + b * RBF_BJ);  // diagonal column in this block, if any
+        const bool diag = __any_sync(0xffffffffu, dcol >= 0 && dcol < RBF_BJ);
+        unsigned char* prow = ps + pb * P_BYTES + (warp * 32 + lane) * 128;
+        const int sw = lane & 7;  // (row & 7) with row = 32 * warp + lane
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          float e[8];
+#pragma unroll
+          for (int u = 0; u < 8; ++u) {
+            const int col = 8 * q + u;
+            const float x = fminf(fmaf(a.two_g, sv[col], cq + ck[col]), 0.f);
+            e[u] = ex2_approx(x);
+            if (diag && col == dcol) e[u] = 1.f;
+          }
+          __nv_bfloat162 h[4] = {__floats2bfloat162_rn(e[0], e[1]), __floats2bfloat162_rn(e[2], e[3]),
+                                 __floats2bfloat162_rn(e[4], e[5]), __floats2bfloat162_rn(e[6], e[7])};
+          *reinterpret_cast<uint4*>(prow + ((q ^ sw) << 4)) = *reinterpret_cast<const uint4*>(h);
+        }
+        fence_proxy_async();
+        mbar_arrive(pfull + pb);
+      }
+      if (!ok) break;
+      // epilogue: O (128 x NC) of this unit, output columns ch * NC + c
+      if (!epilogue_unit<NC, 0>(o, tmem, 0, un & 1, ofull, ofree, qt, ch, warp, lane, err)) break;
+    }
+  }
+  if ((warp == 4 || warp == 5) && lane == 0 && *(volatile int*)err) {
+    const unsigned long long t0 = now_ns();
+    while (now_ns() - t0 < 20000000ull) __nanosleep(1000);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 5) {
+    __syncwarp();
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512) : "memory");
+  }
+}
+
+}  // namespace tc
+}  // namespace skema

@@ -122,6 +122,25 @@ def test_rbf_bf16_parity(sk, oracle):
         check(s, o, "rbf")
 
 
+@pytest.mark.parametrize("N,d,rank,window,eta,nu", [
+    (3000, 64, 20, 1024, 1.0, 1.0),     # one d-subtile; k + s = 244, one output chunk
+    (2600, 100, 20, 999, 0.75, 0.9),    # two d-subtiles, unaligned windows (map slices copied)
+    (2048, 32, 70, 512, 1.0, 1.0),      # k = 281, s = 563: three row-pass chunks, wide X chunk
+])
+def test_rbf_bf16_tensor_core_parity(sk, oracle, N, d, rank, window, eta, nu):
+    # the kernel is never stored: both passes regenerate its tiles from the
+    # BF16 points (Gram on the tensor cores, exp in registers)
+    P = oracle.mixture_points(N, d, seed=3)
+    gamma = oracle.median_gamma(P)
+    a = bf16(alg(sk, N, N, rank, window, 0, kernel_func=1, kernel_gamma=gamma, force_three_sketch=True,
+                 sketch_eta=eta, sketch_nu=nu), sk)
+    o = oracle_for(oracle, a, gamma=gamma)
+    o.linear_update(P.astype(np.float64))
+    with sk.SketchySVD(a) as s:
+        s.linear_update(P)
+        check(s, o, f"rbf-tc N={N} d={d}")
+
+
 def test_bf16_low_rank_approx(sk, oracle):
     m, n = 2000, 1000
     A = dense_input(m, n).astype(np.float32)
