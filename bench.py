@@ -8,7 +8,10 @@ One step = skema_reset + the linear update over all rows (all windows), the
 inputs resident in HBM. Synthetic data, seeded.
 
 Other workloads (--workload): dense-fp32 / dense-bf16 / dense-fp8 (A
-200,000 x 20,000 FP32, r = 50, k = 201, s = 403, windows of 8,192 rows).
+200,000 x 20,000 FP32, r = 50, k = 201, s = 403, windows of 8,192 rows);
+rbf-bf16 / rbf-fp32 (Gauss-RBF kernel of 100,000 points in 128 dimensions,
+r = 64, k = 257, s = 515, windows of 4,096 rows; one step sketches all
+100,000 kernel rows, the kernel's rows split over the ranks).
 
 Multi-GPU (torchrun, one rank per GPU): weak scaling by contiguous row
 blocks; each rank sketches its own block of the global matrix and the
@@ -47,6 +50,13 @@ WORKLOADS = {
     "dense-fp32": dict(m=200_000, n=20_000, rank=50, k=201, s=403, window=8192, seed=3, kind=0, prec=0),
     "dense-bf16": dict(m=200_000, n=20_000, rank=50, k=201, s=403, window=8192, seed=3, kind=0, prec=1),
     "dense-fp8": dict(m=200_000, n=20_000, rank=50, k=201, s=403, window=8192, seed=3, kind=0, prec=2),
+    # Gauss-RBF kernel input: 100,000 points in 128 dimensions; K (100,000^2)
+    # is regenerated tile by tile inside the sketch kernels (BF16 form) or
+    # materialised one 4,096-row window at a time (FP32 form)
+    "rbf-bf16": dict(m=100_000, n=100_000, d=128, rank=64, k=257, s=515, window=4096, seed=4, kind=0, prec=1,
+                     rbf=True),
+    "rbf-fp32": dict(m=100_000, n=100_000, d=128, rank=64, k=257, s=515, window=4096, seed=4, kind=0, prec=0,
+                     rbf=True),
 }
 
 
@@ -178,6 +188,25 @@ def make_dense_torch(cfg, m_local, seed, device):
     return Af.t()  # m x n view, column-major
 
 
+def make_points_torch(cfg, n_pts, seed, device):
+    """8-component Gaussian mixture in d dimensions: means ~ N(0, 4I), unit
+    covariance, equal weights (FP32, row-major n_pts x d); and gamma =
+    1 / (2 * median squared pairwise distance of a 1,000-point subsample)."""
+    import torch
+
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    d = cfg["d"]
+    means = 2.0 * torch.randn(8, d, generator=g, device=device)
+    lab = torch.randint(0, 8, (n_pts,), generator=g, device=device)
+    P = means[lab] + torch.randn(n_pts, d, generator=g, device=device)
+    sub = P[torch.randperm(n_pts, generator=g, device=device)[:1000]].double()
+    d2 = torch.cdist(sub, sub).pow(2)
+    iu = torch.triu_indices(1000, 1000, 1, device=device)
+    gamma = 1.0 / (2.0 * float(d2[iu[0], iu[1]].median()))
+    return P.contiguous(), gamma
+
+
 # ------------------------------------------------------------ our arm ------
 def run_gpu(args, cfg, peaks, peak_kind):
     import torch
@@ -194,20 +223,37 @@ def run_gpu(args, cfg, peaks, peak_kind):
         import datetime
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    m_local = cfg["m"]
-    m_glob = m_local * world
-    a = sk.AlgParams(matrix_m=m_glob, matrix_n=cfg["n"], rank=cfg["rank"], sketch_range=cfg["k"],
-                     sketch_core=cfg["s"], window=cfg["window"], dim_redux=cfg["kind"], device=local)
+    rbf = bool(cfg.get("rbf"))
+    if rbf:
+        # the kernel's rows are sharded over the ranks (every rank holds all
+        # points): total work fixed as the rank count grows
+        m_glob = cfg["m"]
+        per = (m_glob + world - 1) // world
+        row0 = rank * per
+        m_local = max(0, min(per, m_glob - row0))
+        P, gamma = make_points_torch(cfg, m_glob, cfg["seed"], dev)
+        cfg["gamma"] = gamma
+    else:
+        m_local = cfg["m"]
+        m_glob = m_local * world
+        row0 = rank * m_local
+    a = sk.AlgParams(matrix_m=m_glob, matrix_n=m_glob if rbf else cfg["n"], rank=cfg["rank"],
+                     sketch_range=cfg["k"], sketch_core=cfg["s"], window=cfg["window"], dim_redux=cfg["kind"],
+                     device=local)
     sparse = args.workload.startswith("csr")
     a.issparse = sparse
     a.precision = cfg.get("prec", 0)
+    if rbf:
+        a.kernel_func, a.kernel_gamma, a.force_three_sketch = 1, gamma, True
     ctx = sk.SketchySVD(a)
     # one non-default stream for the library's launches and the timing events
     stream = torch.cuda.Stream(device=dev)
     torch.cuda.set_stream(stream)
     ctx.set_stream(stream.cuda_stream)
-    row0 = rank * m_local
-    if sparse:
+    if rbf:
+        nnz = 0
+        inp = P
+    elif sparse:
         rowptr, col, val = make_csr_torch(cfg, m_local, cfg["seed"] + rank, dev)
         nnz = col.numel()
         inp = (rowptr, col, val)
@@ -280,6 +326,8 @@ def run_gpu(args, cfg, peaks, peak_kind):
     except Exception:
         traffic_tab = {}
     step_flops = m_local * (2 * n * (2 * k + s) + 2 * s * s)
+    if rbf:
+        step_flops += m_local * 2 * n * cfg["d"]  # the Gram tile of each kernel entry, once
     hbm_peak = peaks["hbm_gbs"]
     tc_peak = peaks.get("bf16_tflops_sustained", 1400.0)
 
@@ -305,6 +353,18 @@ def run_gpu(args, cfg, peaks, peak_kind):
         # rowptr + (col, val) per nonzero + Y rows written + the byte-packed map
         alg_bytes = (m_local + 1) * 8 + nnz * 8 + m_local * k * 4 + n * zeta
         roof = hbm_roof("csr_ssign_y_kernel", "update.omega", alg_bytes)
+    elif rbf and a.precision:
+        # row pass: Gram + [Y|T] sketch per kernel entry; column pass: Gram + X
+        d = cfg["d"]
+        rp = tc_roof("rbf_sketch_kernel row pass", "update.fused", 2 * m_local * n * (d + k + s), tc_peak, peak_kind)
+        cp = tc_roof("rbf_sketch_kernel column pass", "update.upsilon", 2 * m_local * n * (d + k), tc_peak,
+                     peak_kind)
+        first, second = (rp, cp) if stage_raw["update.fused"][0] >= stage_raw["update.upsilon"][0] else (cp, rp)
+        roof = dict(first)
+        roof["other_kernel"] = second
+    elif rbf:
+        roof = tc_roof("sgemm_kernel (T = K_w Psi~^T, FP32 SIMT)", "update.psi", 2 * m_local * n * s, 74.4,
+                       "nominal FP32 SIMT (148 SMs x 128 FMA/clk x 2 x 1.965 GHz)", bound="fp32-simt")
     elif a.precision:
         # the two large kernels per window: [Y|T] on the tensor pipe and the X^T
         # product that streams the FP32 window (4 B read + 2 B BF16 copy written
@@ -327,7 +387,9 @@ def run_gpu(args, cfg, peaks, peak_kind):
     e2e = None
     if rank == 0 and sparse and not args.no_e2e:
         e2e = e2e_sparse(ctx, inp, m_local, row0, k, s, n, args)
-    if rank == 0 and not sparse and not args.no_e2e:
+    elif rank == 0 and rbf and not args.no_e2e:
+        e2e = e2e_rbf(ctx, inp, m_local, row0, k, s, n, args)
+    elif rank == 0 and not sparse and not args.no_e2e:
         e2e = e2e_dense(ctx, inp, m_local, row0, k, s, n, args)
 
     cpu = None
@@ -343,7 +405,7 @@ def run_gpu(args, cfg, peaks, peak_kind):
         "warmup": args.warmup,
         "ms_per_step": ms,
         "higher_is_better": True,
-        "scaling": "weak",
+        "scaling": "strong" if rbf else "weak",
         "vs_baseline": None,
         "dtype": {0: "fp32", 1: "bf16", 2: "fp8"}[a.precision] if not sparse else "fp32",
         "data": "synthetic (seeded; no dataset)",
@@ -370,6 +432,14 @@ def config_of(args, cfg, world, nnz):
     if args.workload.startswith("csr"):
         c["nnz_per_gpu"] = int(nnz)
         c["l2"] = "working set ~450 MB per step > 126 MB L2 (no flush needed)"
+    elif cfg.get("rbf"):
+        c["m_per_gpu"] = (cfg["m"] + world - 1) // world
+        c.update({"points": cfg["m"], "d": cfg["d"], "gamma": cfg.get("gamma"),
+                  "kernel": "gauss-rbf, 8-component mixture, gamma = 1/(2 median sq. distance of 1,000 points)",
+                  "parallelism": f"kernel row-blocks x{world}" + (" + NCCL all-reduce of X,Z" if world > 1 else ""),
+                  "l2": "maps 0.6 GB (BF16) and Y 0.1 GB per step > 126 MB L2 (no flush needed)"})
+        c["kernel_stored"] = "never (tiles regenerated in the sketch kernels)" if cfg.get("prec") else \
+            "one window at a time (FP32)"
     else:
         c["l2"] = "A is 16 GB per step > 126 MB L2 (no flush needed)"
     return c
@@ -411,6 +481,39 @@ def e2e_sparse(ctx, inp, m_local, row0, k, s, n, args):
     return {"value": m_local / dt, "unit": "rows/s", "h2d_bytes_per_step": int(h2d),
             "d2h_bytes_per_step": int(d2h), "ms_per_step": dt * 1e3,
             "path": "skema_linear_update_csr(mem=HOST) + skema_get_sketch(X,Y,Z, mem=HOST), pinned buffers",
+            "timer": "host wall clock around synchronous calls"}
+
+
+def e2e_rbf(ctx, P, m_local, row0, k, s, n, args):
+    import torch
+
+    import skema_b200._lib as L
+
+    hP = P.cpu().pin_memory()  # n x d row-major points
+    d = hP.shape[1]
+    hX = torch.empty((k, n), dtype=torch.float32).pin_memory()
+    hY = torch.empty((ctx.nrow, k), dtype=torch.float32).pin_memory()
+    hZ = torch.empty((s, s), dtype=torch.float32).pin_memory()
+    lib, h = ctx.lib, ctx.h
+
+    def one():
+        ctx._check(lib.skema_reset(h))
+        ctx._check(lib.skema_linear_update_rbf(h, hP.data_ptr(), d, L.ROW_MAJOR, n, d, row0, m_local, L.MEM_HOST))
+        ctx._check(lib.skema_get_sketch(h, 0, hX.data_ptr(), n, L.ROW_MAJOR, L.MEM_HOST))
+        ctx._check(lib.skema_get_sketch(h, 1, hY.data_ptr(), k, L.ROW_MAJOR, L.MEM_HOST))
+        ctx._check(lib.skema_get_sketch(h, 2, hZ.data_ptr(), s, L.ROW_MAJOR, L.MEM_HOST))
+
+    one()
+    steps = 2
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        one()
+    torch.cuda.synchronize()
+    dt = (time.perf_counter() - t0) / steps
+    return {"value": m_local / dt, "unit": "rows/s", "h2d_bytes_per_step": int(n * d * 4),
+            "d2h_bytes_per_step": int((k * n + ctx.nrow * k + s * s) * 4), "ms_per_step": dt * 1e3,
+            "path": "skema_linear_update_rbf(mem=HOST) + skema_get_sketch(X,Y,Z, mem=HOST), pinned buffers",
             "timer": "host wall clock around synchronous calls"}
 
 
@@ -486,8 +589,31 @@ def cpu_sample_dense(cfg, budget_s):
     return done / dt, done, O.num_threads()
 
 
+def cpu_sample_rbf(cfg, budget_s):
+    """Oracle (FP64 kernel window + dense sketch restatement) on 1,024-row
+    windows of a same-recipe point set until budget_s elapses."""
+    from oracle import sketchy_oracle as O
+
+    N, d, w = cfg["m"], cfg["d"], 1024
+    X = O.mixture_points(N, d, seed=cfg["seed"])
+    gamma = O.median_gamma(X)
+    o = O.OracleSketch(N, N, cfg["rank"], w, kind=0, sketch_range=cfg["k"], sketch_core=cfg["s"],
+                       kernel_gamma=gamma)
+    t0 = time.perf_counter()
+    done = 0
+    while done == 0 or (done < 4 * w and time.perf_counter() - t0 < budget_s):
+        Kw = O.rbf_window(X, gamma, done, w)
+        O.update_dense(o.maps, Kw, done)
+        done += w
+    dt = time.perf_counter() - t0
+    return done / dt, done, O.num_threads()
+
+
 def cpu_baseline(args, cfg, budget_s):
-    if args.workload.startswith("csr"):
+    if cfg.get("rbf"):
+        v, rows, thr = cpu_sample_rbf(cfg, budget_s)
+        sample = f"{rows} kernel rows (windows of 1024) of a same-recipe point set, FP64"
+    elif args.workload.startswith("csr"):
         v, rows, thr = cpu_sample_sparse(cfg, budget_s)
         sample = f"first {rows} rows ({rows // cfg['window']} windows) of the workload, FP64"
     else:
@@ -517,7 +643,9 @@ def run_reference(args, cfg):
     rows = 0
     thr = 1
     for i in range(args.warmup + args.steps):
-        if args.workload.startswith("csr"):
+        if cfg.get("rbf"):
+            v, r, thr = cpu_sample_rbf(cfg, budget)
+        elif args.workload.startswith("csr"):
             v, r, thr = cpu_sample_sparse(cfg, budget, seed_rows=min(cfg["m"], 200_000))
         else:
             v, r, thr = cpu_sample_dense(cfg, budget)
@@ -529,6 +657,7 @@ def run_reference(args, cfg):
         "metric": "sketched rows/s", "value": v, "unit": "rows/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": rows / v * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded; no dataset)",
+        **({"scaling": "strong"} if cfg.get("rbf") else {}),
         "config": config_of(args, cfg, 1, 0), "impl": "reference",
         "cpu_baseline": {"value": v, "unit": "rows/s", "cores": thr, "kind": "port",
                          "sample": f"{rows} rows per step (bounded sample), FP64 oracle restatement",

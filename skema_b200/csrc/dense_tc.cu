@@ -119,6 +119,7 @@ tc::OutSpec out_spec() {
   o.alpha0 = 1.f, o.beta0 = 0.f, o.alpha1 = 1.f, o.beta1 = 0.f;
   o.rows = 0, o.split = 0, o.ncols = 0;
   o.atomic0 = 0, o.atomic1 = 0;
+  o.row_log2w = 0.f, o.row_wlen = 1, o.row_nwin = 1;
   return o;
 }
 
@@ -349,22 +350,22 @@ TcSlices tc_window_slices(skema_ctx* c, int64_t R0, int64_t wr, char** sp) {
   return TcSlices{us, fs, wp};
 }
 
-void tc_z_update(skema_ctx* c, const __nv_bfloat16* T16, int64_t wp, const TcSlices& sl, int64_t wr) {
-  const float eta = (float)c->p.sketch_eta, nu = (float)c->p.sketch_nu;
+void tc_z_update(skema_ctx* c, const __nv_bfloat16* T16, int64_t ldT, const TcSlices& sl, int64_t K, float beta) {
+  const float eta = (float)c->p.sketch_eta;
   const int64_t s = c->s;
   StageScope st(c, ST_PHI);
-  const CUtensorMap ta = tmap_bf16(T16, (uint64_t)wr, (uint64_t)s, (uint64_t)wp * 2, 64, 128);
-  const CUtensorMap tb = tmap_bf16(sl.F16, (uint64_t)wr, (uint64_t)s, (uint64_t)sl.ldm * 2, 64, kNT);
+  const CUtensorMap ta = tmap_bf16(T16, (uint64_t)K, (uint64_t)s, (uint64_t)ldT * 2, 64, 128);
+  const CUtensorMap tb = tmap_bf16(sl.F16, (uint64_t)K, (uint64_t)s, (uint64_t)sl.ldm * 2, 64, kNT);
   const int64_t tiles = ((s + 127) / 128) * ((s + kNT - 1) / kNT);
-  const Plan pl = plan_split(c, tiles, wr, 32);
+  const Plan pl = plan_split(c, tiles, K, 32);
   tc::OutSpec o = out_spec();
-  o.p0 = c->Z, o.rs0 = 1, o.cs0 = s, o.alpha0 = eta, o.beta0 = nu;
+  o.p0 = c->Z, o.rs0 = 1, o.cs0 = s, o.alpha0 = eta, o.beta0 = beta;
   o.rows = s, o.split = s, o.ncols = s;
   if (pl.ks > 1) {
-    scale_block(c, MatOut{c->Z, s, 1}, s, s, nu);
+    scale_block(c, MatOut{c->Z, s, 1}, s, s, beta);
     o.atomic0 = 1, o.beta0 = 0.f;
   }
-  launch_gemm<tc::A_KMAJ>(c, ta, tb, s, s, wr, pl, 0, o);
+  launch_gemm<tc::A_KMAJ>(c, ta, tb, s, s, K, pl, 0, o);
 }
 
 bool tc_available(const skema_ctx* c) {
@@ -473,7 +474,7 @@ void tc_dense_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr, void* scratch
     if (pl.ks > 1) t32_to_t16(c, T32, T16, wr, s, wp);
   }
   y_rows_mark(c, R0, R0 + wr);
-  tc_z_update(c, T16, wp, sl, wr);
+  tc_z_update(c, T16, wp, sl, wr, nu);
 }
 
 }  // namespace skema

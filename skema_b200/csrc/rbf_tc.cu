@@ -2,11 +2,14 @@
 // (SketchySVD over the kernel matrix K(i, j) = exp(-gamma ||x_i - x_j||^2),
 // the window of src/Skema_Window.hpp:90-107 and the kernel of
 // src/Skema_Kernel.cpp:6-81, diagonal forced to 1 as at :62-68). K is never
-// stored: each window is sketched by two passes of rbf_sketch_kernel
-// (tc_rbf.cuh) that regenerate its tiles from the points:
-//   row pass     [Y_w | T] = K_w [Omega~; Psi~]^T   query = window rows
-//   column pass  X^T = nu X^T + eta K_w^T Upsilon~_w^T   query = all points
-// then Z^T = nu Z^T + eta T^T Phi~_w^T on the dense tensor-core GEMM.
+// stored: the kernel rows of a call are sketched by two passes of
+// rbf_sketch_kernel (tc_rbf.cuh) that regenerate its tiles from the points:
+//   row pass     [Y | T] = K(rows, :) [Omega~; Psi~]^T   query = the rows
+//   column pass  X^T = nu^G X^T + eta sum_w nu^(G-1-w) K_w^T Upsilon~_w^T
+//                                                        query = all points
+// then Z^T = nu^G Z^T + eta T^T Phi~^T on the dense tensor-core GEMM, with
+// window w's T rows weighted by nu^(G-1-w) (one group of G windows per
+// call when nu > 0, see rbf_tc_update).
 // Distances come from the Gram expansion ||x_i||^2 + ||x_j||^2 - 2 x_i.x_j
 // of the BF16-rounded points (FP32 accumulation), clamped at 0; the point
 // norms are those of the same rounded points, so a point's distance to
@@ -53,20 +56,29 @@ __global__ void rbf_prep_kernel(const float* __restrict__ P, int64_t prs, int64_
   }
 }
 
-// c of the window's rows [R0, R0 + wr), -inf up to npad.
-__global__ void rbf_window_c_kernel(const float* __restrict__ cval, int64_t R0, int64_t wr,
-                                    float* __restrict__ out, int64_t npad) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < npad; i += (int64_t)gridDim.x * blockDim.x)
-    out[i] = i < wr ? cval[R0 + i] : -INFINITY;
+// Key constants of the column pass: c of rows [R0, R0 + nr) plus the
+// log2 window weight (G - 1 - i / W) * log2w of row i (windows of W rows, G
+// of them), -inf from nr up to npad.
+__global__ void rbf_key_c_kernel(const float* __restrict__ cval, int64_t R0, int64_t nr, int64_t W, int64_t G,
+                                 float log2w, float* __restrict__ out, int64_t npad) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < npad; i += (int64_t)gridDim.x * blockDim.x) {
+    float v = -INFINITY;
+    if (i < nr) {
+      v = cval[R0 + i];
+      const int64_t e = G - 1 - i / W;
+      if (log2w != 0.f && e > 0) v += (float)e * log2w;
+    }
+    out[i] = v;
+  }
 }
 
-template <int NC1, int NC2, int DK>
+template <int NC1, int NC2, int DK, int S>
 void launch_rbf(skema_ctx* c, const CUtensorMap& tq, const CUtensorMap& tk, const CUtensorMap& tv1,
                 const CUtensorMap& tv2, const tc::RbfArgs& a, const tc::OutSpec& o) {
   constexpr uint32_t Q_BYTES = DK * tc::RBF_BQ * 128;
   constexpr uint32_t STAGE = ((DK * tc::RBF_BJ * 128 + (NC1 + NC2) * 128 + 256 + 1023) / 1024) * 1024;
-  const size_t smem = Q_BYTES + (size_t)tc::RBF_S * STAGE + 2 * tc::RBF_BQ * 128 + 1024 + 256;
-  auto kern = tc::rbf_sketch_kernel<NC1, NC2, DK>;
+  const size_t smem = Q_BYTES + (size_t)S * STAGE + 2 * tc::RBF_BQ * 128 + 1024 + 256;
+  auto kern = tc::rbf_sketch_kernel<NC1, NC2, DK, S>;
   SKEMA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int64_t units = (int64_t)a.qtiles * a.nchunks * a.ksplit;
   if (units <= 0 || a.nblocks <= 0) return;
@@ -77,17 +89,18 @@ void launch_rbf(skema_ctx* c, const CUtensorMap& tq, const CUtensorMap& tk, cons
   c->dev_err_armed = true;
 }
 
-// Output-column chunks of one pass: (NC1, NC2) = (256, 144) or (256, 16).
+// Output-column chunks of one pass: (NC1, NC2) = (256, 144) with two key /
+// value stages, or (256, 16) with three.
 template <int DK>
 void run_pass(skema_ctx* c, bool narrow, const CUtensorMap& tq, const CUtensorMap& tk, const void* V, int64_t vcols,
               int64_t vrows, int64_t vld, const tc::RbfArgs& a, const tc::OutSpec& o) {
   const CUtensorMap tv1 = tmap_bf16(V, (uint64_t)vcols, (uint64_t)vrows, (uint64_t)vld * 2, 64, 256);
   if (narrow) {
     const CUtensorMap tv2 = tmap_bf16(V, (uint64_t)vcols, (uint64_t)vrows, (uint64_t)vld * 2, 64, 16);
-    launch_rbf<256, 16, DK>(c, tq, tk, tv1, tv2, a, o);
+    launch_rbf<256, 16, DK, 3>(c, tq, tk, tv1, tv2, a, o);
   } else {
     const CUtensorMap tv2 = tmap_bf16(V, (uint64_t)vcols, (uint64_t)vrows, (uint64_t)vld * 2, 64, 144);
-    launch_rbf<256, 144, DK>(c, tq, tk, tv1, tv2, a, o);
+    launch_rbf<256, 144, DK, 2>(c, tq, tk, tv1, tv2, a, o);
   }
 }
 
@@ -97,6 +110,12 @@ bool rbf_tc_supported(const skema_ctx* c, int64_t d) {
   return tc_available(c) && d >= 1 && d <= 128 && c->k <= 448 && c->n == c->m;
 }
 
+// All windows of the call in one row pass, one column pass and one Z
+// product when nu > 0: the per-window sequence X = nu X + eta x_w (likewise
+// Z) over G windows equals X = nu^G X + eta sum_w nu^(G-1-w) x_w, so window
+// w's kernel rows carry the weight nu^(G-1-w) -- in the key constants of the
+// column pass and in the T rows that feed Z -- while its Y rows get eta
+// alone. Other nu take one window at a time (G = 1).
 void rbf_tc_update(skema_ctx* c, Mat P, int64_t N, int64_t d, int64_t row0, int64_t nrows) {
   const float eta = (float)c->p.sketch_eta, nu = (float)c->p.sketch_nu;
   const float gl = (float)c->p.kernel_gamma * kLog2e;
@@ -104,22 +123,26 @@ void rbf_tc_update(skema_ctx* c, Mat P, int64_t N, int64_t d, int64_t row0, int6
   const int DK = d <= 64 ? 1 : 2;
   const int64_t dp = 64 * DK;
   const int64_t npad = (N + tc::RBF_BJ - 1) / tc::RBF_BJ * tc::RBF_BJ;
-  const int64_t wmax = std::min(W, nrows);
-  const int64_t wp = pad8(wmax);
-  const int64_t wpad = (wmax + tc::RBF_BJ - 1) / tc::RBF_BJ * tc::RBF_BJ;
+  const int64_t nwin = (nrows + W - 1) / W;
+  const bool fold = nu > 0.f;
+  const float log2nu = (fold && nu != 1.f) ? std::log2(nu) : 0.f;
+  const int64_t gwin = fold ? nwin : 1;            // windows per group
+  const int64_t gmax = std::min(nrows, gwin * W);  // rows per group
+  const int64_t gp = pad8(gmax);
+  const int64_t gpad = (gmax + tc::RBF_BJ - 1) / tc::RBF_BJ * tc::RBF_BJ;
   auto rup = [](size_t b) { return (b + 255) / 256 * 256; };
   const size_t b_x16 = rup(sizeof(__nv_bfloat16) * (size_t)(N * dp));
   const size_t b_c = rup(sizeof(float) * (size_t)npad);
-  const size_t b_cw = rup(sizeof(float) * (size_t)wpad);
-  const size_t b_t16 = rup(sizeof(__nv_bfloat16) * (size_t)(wp * s));
-  const size_t b_t32 = rup(sizeof(float) * (size_t)(wp * s));
-  char* ws = static_cast<char*>(workspace(c, b_x16 + b_c + b_cw + b_t16 + b_t32 + tc_slice_bytes(c, wmax)));
+  const size_t b_ck = rup(sizeof(float) * (size_t)gpad);
+  const size_t b_t16 = rup(sizeof(__nv_bfloat16) * (size_t)(gp * s));
+  const size_t b_t32 = rup(sizeof(float) * (size_t)(gp * s));
+  char* ws = static_cast<char*>(workspace(c, b_x16 + b_c + b_ck + b_t16 + b_t32 + tc_slice_bytes(c, gmax)));
   __nv_bfloat16* X16 = reinterpret_cast<__nv_bfloat16*>(ws);
   float* cval = reinterpret_cast<float*>(ws + b_x16);
-  float* cwin = reinterpret_cast<float*>(ws + b_x16 + b_c);
-  __nv_bfloat16* T16 = reinterpret_cast<__nv_bfloat16*>(ws + b_x16 + b_c + b_cw);
-  float* T32 = reinterpret_cast<float*>(ws + b_x16 + b_c + b_cw + b_t16);
-  char* slice_sp = ws + b_x16 + b_c + b_cw + b_t16 + b_t32;
+  float* ckey = reinterpret_cast<float*>(ws + b_x16 + b_c);
+  __nv_bfloat16* T16 = reinterpret_cast<__nv_bfloat16*>(ws + b_x16 + b_c + b_ck);
+  float* T32 = reinterpret_cast<float*>(ws + b_x16 + b_c + b_ck + b_t16);
+  char* slice_sp = ws + b_x16 + b_c + b_ck + b_t16 + b_t32;
 
   {
     StageScope st(c, ST_WINDOW);
@@ -130,67 +153,79 @@ void rbf_tc_update(skema_ctx* c, Mat P, int64_t N, int64_t d, int64_t row0, int6
   const CUtensorMap tq = tmap_bf16(X16, (uint64_t)dp, (uint64_t)N, (uint64_t)dp * 2, 64, tc::RBF_BQ);
   const CUtensorMap tk = tmap_bf16(X16, (uint64_t)dp, (uint64_t)N, (uint64_t)dp * 2, 64, tc::RBF_BJ);
 
-  for (int64_t r = 0; r < nrows; r += W) {
-    const int64_t wr = std::min(W, nrows - r);
-    const int64_t R0 = row0 + r;
-    const float ybeta = y_rows_clean(c, R0, R0 + wr) ? 0.f : nu;
+  for (int64_t g0 = 0; g0 < nwin; g0 += gwin) {
+    const int64_t R0 = row0 + g0 * W;
+    const int64_t nr = std::min(gwin * W, nrows - g0 * W);  // rows of this group
+    const int64_t G = (nr + W - 1) / W;                      // windows of this group
+    const int64_t ldT = pad8(nr);
+    const float nuG = fold ? std::pow(nu, (float)G) : nu;    // G = 1 when not folded
+    if (!y_rows_clean(c, R0, R0 + nr)) y_materialize(c);    // rows written before get the nu term
+    const float ybeta = y_rows_clean(c, R0, R0 + nr) ? 0.f : nu;
     char* sp = slice_sp;
-    const TcSlices sl = tc_window_slices(c, R0, wr, &sp);
-    {  // row pass: [Y_w | T] = K_w [Omega~; Psi~]^T
+    const TcSlices sl = tc_window_slices(c, R0, nr, &sp);
+    {  // row pass: [Y | T] = K(rows, :) [Omega~; Psi~]^T, T rows weighted per window
       StageScope st(c, ST_FUSED);
       tc::RbfArgs a;
-      a.nq = wr, a.qbase = R0, a.kbase = 0;
+      a.nq = nr, a.qbase = R0, a.kbase = 0;
       a.nblocks = npad / tc::RBF_BJ;
-      a.qtiles = (int)((wr + tc::RBF_BQ - 1) / tc::RBF_BQ);
-      a.chunk_cols = 400;
-      a.nchunks = (int)((k + s + 399) / 400);
+      a.qtiles = (int)((nr + tc::RBF_BQ - 1) / tc::RBF_BQ);
+      a.chunk_cols = 272;
+      a.nchunks = (int)((k + s + 271) / 272);
       const Plan pl = plan_split(c, (int64_t)a.qtiles * a.nchunks, npad, 16);
       a.bchunk = pl.kchunk / tc::RBF_BJ;
       a.ksplit = (int)((a.nblocks + a.bchunk - 1) / a.bchunk);
       a.cq = cval + R0, a.ckey = cval, a.two_g = 2.f * gl;
+      a.klog2w = 0.f, a.kwlen = W, a.knwin = 1;
       tc::OutSpec o = out_spec();
       o.p0 = c->Y + R0, o.rs0 = 1, o.cs0 = m, o.alpha0 = eta, o.beta0 = ybeta;
-      o.rows = wr, o.split = k, o.ncols = k + s;
+      o.rows = nr, o.split = k, o.ncols = k + s;
+      o.row_log2w = log2nu, o.row_wlen = W, o.row_nwin = G;
       if (a.ksplit == 1) {
-        o.p1 = T16, o.rs1 = 1, o.cs1 = wp;
+        o.p1 = T16, o.rs1 = 1, o.cs1 = ldT;
       } else {
-        scale_block(c, MatOut{c->Y + R0, 1, m}, wr, k, ybeta);
-        SKEMA_CUDA(cudaMemsetAsync(T32, 0, sizeof(float) * (size_t)(wp * s), c->stream));
+        scale_block(c, MatOut{c->Y + R0, 1, m}, nr, k, ybeta);
+        SKEMA_CUDA(cudaMemsetAsync(T32, 0, sizeof(float) * (size_t)(ldT * s), c->stream));
         o.atomic0 = 1, o.beta0 = 0.f;
-        o.p1f = T32, o.rs1 = 1, o.cs1 = wp, o.atomic1 = 1;
+        o.p1f = T32, o.rs1 = 1, o.cs1 = ldT, o.atomic1 = 1;
       }
       if (DK == 1)
-        run_pass<1>(c, false, tq, tk, c->op16, N, k + s, c->ld_op16, a, o);
+        run_pass<1>(c, true, tq, tk, c->op16, N, k + s, c->ld_op16, a, o);
       else
-        run_pass<2>(c, false, tq, tk, c->op16, N, k + s, c->ld_op16, a, o);
-      if (a.ksplit > 1) t32_to_t16(c, T32, T16, wr, s, wp);
+        run_pass<2>(c, true, tq, tk, c->op16, N, k + s, c->ld_op16, a, o);
+      if (a.ksplit > 1) t32_to_t16(c, T32, T16, nr, s, ldT);
     }
-    y_rows_mark(c, R0, R0 + wr);
-    {  // column pass: X^T = nu X^T + eta K_w^T Upsilon~_w^T
+    y_rows_mark(c, R0, R0 + nr);
+    {  // column pass: X^T = nu^G X^T + eta sum_w nu^(G-1-w) K_w^T Upsilon~_w^T
       StageScope st(c, ST_UPSILON);
-      const int64_t wpad_w = (wr + tc::RBF_BJ - 1) / tc::RBF_BJ * tc::RBF_BJ;
-      rbf_window_c_kernel<<<(int)std::max<int64_t>(1, (wpad_w + 255) / 256), 256, 0, c->stream>>>(cval, R0, wr, cwin,
-                                                                                                  wpad_w);
+      const int64_t kpad = (nr + tc::RBF_BJ - 1) / tc::RBF_BJ * tc::RBF_BJ;
+      rbf_key_c_kernel<<<(int)std::max<int64_t>(1, std::min<int64_t>((kpad + 255) / 256, c->sm_count * 8)), 256, 0,
+                         c->stream>>>(cval, R0, nr, W, G, log2nu, ckey, kpad);
       SKEMA_LAUNCHED(c);
       const bool narrow = k <= 272;
       tc::RbfArgs a;
       a.nq = N, a.qbase = 0, a.kbase = R0;
-      a.nblocks = wpad_w / tc::RBF_BJ;
-      a.bchunk = a.nblocks;
-      a.ksplit = 1;
+      a.nblocks = kpad / tc::RBF_BJ;
       a.qtiles = (int)((N + tc::RBF_BQ - 1) / tc::RBF_BQ);
       a.chunk_cols = narrow ? 272 : 400;
       a.nchunks = (int)((k + a.chunk_cols - 1) / a.chunk_cols);
-      a.cq = cval, a.ckey = cwin, a.two_g = 2.f * gl;
+      const Plan pl = plan_split(c, (int64_t)a.qtiles * a.nchunks, kpad, 8);
+      a.bchunk = pl.kchunk / tc::RBF_BJ;
+      a.ksplit = (int)((a.nblocks + a.bchunk - 1) / a.bchunk);
+      a.cq = cval, a.ckey = ckey, a.two_g = 2.f * gl;
+      a.klog2w = log2nu, a.kwlen = W, a.knwin = G;
       tc::OutSpec o = out_spec();
-      o.p0 = c->X, o.rs0 = 1, o.cs0 = c->n, o.alpha0 = eta, o.beta0 = nu;
+      o.p0 = c->X, o.rs0 = 1, o.cs0 = c->n, o.alpha0 = eta, o.beta0 = nuG;
       o.rows = N, o.split = k, o.ncols = k;
+      if (a.ksplit > 1) {
+        scale_block(c, MatOut{c->X, c->n, 1}, k, c->n, nuG);
+        o.atomic0 = 1, o.beta0 = 0.f;
+      }
       if (DK == 1)
-        run_pass<1>(c, narrow, tq, tk, sl.U16, wr, k, sl.ldm, a, o);
+        run_pass<1>(c, narrow, tq, tk, sl.U16, nr, k, sl.ldm, a, o);
       else
-        run_pass<2>(c, narrow, tq, tk, sl.U16, wr, k, sl.ldm, a, o);
+        run_pass<2>(c, narrow, tq, tk, sl.U16, nr, k, sl.ldm, a, o);
     }
-    tc_z_update(c, T16, wp, sl, wr);
+    tc_z_update(c, T16, ldT, sl, nr, nuG);
   }
 }
 

@@ -65,6 +65,11 @@ struct OutSpec {
   int64_t split, ncols;   // valid output columns
   int atomic0;            // 1: atomicAdd alpha0*acc into p0 (split-K)
   int atomic1;            // 1: atomicAdd alpha1*acc into p1f (split-K)
+  // Window weights of the second part: row r (of windows of row_wlen rows,
+  // row_nwin of them) is scaled by 2^((row_nwin - 1 - r / row_wlen) *
+  // row_log2w); row_log2w = 0 leaves it unweighted.
+  float row_log2w;
+  int64_t row_wlen, row_nwin;
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -175,16 +180,36 @@ __device__ __forceinline__ void umma_commit(uint64_t* bar) {
                    smem_u32(bar))
                : "memory");
 }
+// 16 consecutive TMEM columns of this thread's lane; the load and its wait
+// are one asm statement so no use of the registers can precede the wait.
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
   uint32_t r[16];
   asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n\t"
+      "tcgen05.wait::ld.sync.aligned;"
       : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
         "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-      : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      : "r"(taddr)
+      : "memory");
 #pragma unroll
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+// 32 consecutive columns as two loads in flight and one wait.
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%32];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, "
+      "[%33];\n\t"
+      "tcgen05.wait::ld.sync.aligned;"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr), "r"(taddr + 16)
+      : "memory");
+#pragma unroll
+  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
 // Work units: unit t -> (mt, nt, ks). M fastest when m_fast, else N.
@@ -219,17 +244,28 @@ __device__ __forceinline__ bool epilogue_unit(const OutSpec& o, uint32_t tmem, u
   tc_fence_after();
   const int64_t row = (int64_t)mt * BM + warp * 32 + lane;
   const uint32_t taddr = tmem + acc * TCOLS + ((uint32_t)(warp * 32) << 16);
-  for (int c0 = 0; c0 < NT; c0 += 16) {
-    float v[16];
-    tmem_ld16(taddr + c0, v);
-    if (c0 + 16 >= NT) {
+  float alpha1 = o.alpha1;
+  if (o.row_log2w != 0.f && row < o.rows) {
+    const int64_t e = o.row_nwin - 1 - row / o.row_wlen;
+    if (e > 0) alpha1 *= exp2f((float)e * o.row_log2w);
+  }
+  for (int c0 = 0; c0 < NT; c0 += 32) {
+    // 32 columns per TMEM round trip (16 for an odd last chunk)
+    const int w = (c0 + 32 <= NT) ? 32 : 16;
+    float v[32];
+    if (w == 32)
+      tmem_ld32(taddr + c0, v);
+    else
+      tmem_ld16(taddr + c0, v);
+    if (c0 + w >= NT) {
       // last read of this accumulator: hand it back before storing
       tc_fence_before();
       mbar_arrive(tempty + acc);
     }
     if (row >= o.rows) continue;
 #pragma unroll
-    for (int i = 0; i < 16; ++i) {
+    for (int i = 0; i < 32; ++i) {
+      if (i >= w) break;
       const int64_t col = (int64_t)nt * NT + c0 + i;
       if (col >= o.ncols) continue;
       if (col < o.split) {
@@ -241,13 +277,13 @@ __device__ __forceinline__ bool epilogue_unit(const OutSpec& o, uint32_t tmem, u
       } else {
         const int64_t cc = col - o.split;
         if (o.p1) {
-          o.p1[row * o.rs1 + cc * o.cs1] = __float2bfloat16(o.alpha1 * v[i]);
+          o.p1[row * o.rs1 + cc * o.cs1] = __float2bfloat16(alpha1 * v[i]);
         } else if (o.p1f) {
           float* p = o.p1f + row * o.rs1 + cc * o.cs1;
           if (o.atomic1)
-            atomicAdd(p, o.alpha1 * v[i]);
+            atomicAdd(p, alpha1 * v[i]);
           else
-            *p = (o.beta1 == 0.f) ? o.alpha1 * v[i] : fmaf(o.beta1, *p, o.alpha1 * v[i]);
+            *p = (o.beta1 == 0.f) ? alpha1 * v[i] : fmaf(o.beta1, *p, alpha1 * v[i]);
         }
       }
     }

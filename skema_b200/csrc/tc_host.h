@@ -42,8 +42,9 @@ struct TcSlices {
 TcSlices tc_window_slices(skema_ctx* c, int64_t R0, int64_t wr, char** sp);
 size_t tc_slice_bytes(const skema_ctx* c, int64_t wr);
 
-// Z = nu Z + eta Phi~_w T for the window's T (BF16, wr x s column-major,
-// ld wp), as Z^T = T^T Phi~_w^T on the tensor cores.
-void tc_z_update(skema_ctx* c, const __nv_bfloat16* T16, int64_t wp, const TcSlices& sl, int64_t wr);
+// Z = beta Z + eta Phi~(:, rows) T for T (BF16, K x s column-major, ld
+// ldT) over K rows whose Phi~ columns are sl.F16, as Z^T = T^T Phi~^T on
+// the tensor cores.
+void tc_z_update(skema_ctx* c, const __nv_bfloat16* T16, int64_t ldT, const TcSlices& sl, int64_t K, float beta);
 
 }  // namespace skema

@@ -31,7 +31,6 @@ namespace tc {
 
 constexpr int RBF_BQ = 128;  // query rows per unit (TMEM lanes)
 constexpr int RBF_BJ = 64;   // key points per block
-constexpr int RBF_S = 2;     // key/value stages
 constexpr uint32_t RBF_SCOL = 448;  // TMEM column of the Gram tile (O uses [0, 448))
 
 // 2^x by the PTX ex2.approx instruction (relative error about 2^-22, far
@@ -53,9 +52,14 @@ struct RbfArgs {
   const float* cq;     // c_p of the query points, indexed by query row
   const float* ckey;   // c_p of the key points, indexed by key column, padded with -inf
   float two_g;         // 2 * gamma * log2(e)
+  // Window weights folded into ckey (key column j of window j / kwlen, of
+  // knwin, carries + (knwin - 1 - j / kwlen) * klog2w); the forced diagonal
+  // entry is that weight instead of 1. klog2w = 0: unweighted.
+  float klog2w;
+  int64_t kwlen, knwin;
 };
 
-template <int NC1, int NC2, int DK>
+template <int NC1, int NC2, int DK, int RBF_S>
 __global__ void __launch_bounds__(kThreads, 1)
     rbf_sketch_kernel(const __grid_constant__ CUtensorMap tmQ, const __grid_constant__ CUtensorMap tmK,
                       const __grid_constant__ CUtensorMap tmV1, const __grid_constant__ CUtensorMap tmV2,
@@ -254,8 +258,8 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         tc_fence_after();
         float sv[64];
-#pragma unroll
-        for (int c = 0; c < 4; ++c) tmem_ld16(tmem + RBF_SCOL + lane_off + 16 * c, sv + 16 * c);
+        tmem_ld32(tmem + RBF_SCOL + lane_off, sv);
+        tmem_ld32(tmem + RBF_SCOL + lane_off + 32, sv + 32);
         tc_fence_before();
         mbar_arrive(sfree);
         const uint32_t pb = pc & 1;
@@ -266,17 +270,25 @@ __global__ void __launch_bounds__(kThreads, 1)
         const float* ck = reinterpret_cast<const float*>(st + (it % RBF_S) * STAGE + K_BYTES + V_BYTES);
         const int64_t dcol = gq - (a.kbase + b * RBF_BJ);  // diagonal column in this block, if any
         const bool diag = __any_sync(0xffffffffu, dcol >= 0 && dcol < RBF_BJ);
+        float dval = 1.f;
+        if (diag && a.klog2w != 0.f && dcol >= 0 && dcol < RBF_BJ) {
+          const int64_t e = a.knwin - 1 - (b * RBF_BJ + dcol) / a.kwlen;
+          if (e > 0) dval = exp2f((float)e * a.klog2w);
+        }
         unsigned char* prow = ps + pb * P_BYTES + (warp * 32 + lane) * 128;
         const int sw = lane & 7;  // (row & 7) with row = 32 * warp + lane
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
           float e[8];
+          const float4 k0 = reinterpret_cast<const float4*>(ck)[2 * q];
+          const float4 k1 = reinterpret_cast<const float4*>(ck)[2 * q + 1];
+          const float kc[8] = {k0.x, k0.y, k0.z, k0.w, k1.x, k1.y, k1.z, k1.w};
 #pragma unroll
           for (int u = 0; u < 8; ++u) {
             const int col = 8 * q + u;
-            const float x = fminf(fmaf(a.two_g, sv[col], cq + ck[col]), 0.f);
+            const float x = fminf(fmaf(a.two_g, sv[col], cq + kc[u]), 0.f);
             e[u] = ex2_approx(x);
-            if (diag && col == dcol) e[u] = 1.f;
+            if (diag && col == dcol) e[u] = dval;
           }
           __nv_bfloat162 h[4] = {__floats2bfloat162_rn(e[0], e[1]), __floats2bfloat162_rn(e[2], e[3]),
                                  __floats2bfloat162_rn(e[4], e[5]), __floats2bfloat162_rn(e[6], e[7])};

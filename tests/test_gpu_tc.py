@@ -141,6 +141,28 @@ def test_rbf_bf16_tensor_core_parity(sk, oracle, N, d, rank, window, eta, nu):
         check(s, o, f"rbf-tc N={N} d={d}")
 
 
+@pytest.mark.parametrize("nu", [0.8, -0.5])
+def test_rbf_bf16_blocks_and_dirty_rows(sk, oracle, nu):
+    # several calls over row blocks, one of them repeated (its Y rows get the
+    # nu term); nu > 0 folds each call's windows into one pass with weights,
+    # nu <= 0 takes them one window at a time
+    N, d = 2000, 48
+    P = oracle.mixture_points(N, d, seed=7)
+    gamma = oracle.median_gamma(P)
+    a = bf16(alg(sk, N, N, 10, 300, 0, kernel_func=1, kernel_gamma=gamma, force_three_sketch=True,
+                 sketch_eta=1.1, sketch_nu=nu), sk)
+    o = oracle_for(oracle, a, gamma=gamma)
+    o.reset()
+    calls = [(0, 1000), (1000, 1000), (400, 600)]
+    for r0, nr in calls:
+        o.update_rows(P.astype(np.float64), r0, nr)
+    with sk.SketchySVD(a) as s:
+        s.reset()
+        for r0, nr in calls:
+            s.update_rows(P, r0, nr)
+        check(s, o, f"rbf blocks nu={nu}")
+
+
 def test_bf16_low_rank_approx(sk, oracle):
     m, n = 2000, 1000
     A = dense_input(m, n).astype(np.float32)
