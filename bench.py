@@ -224,13 +224,13 @@ def run_gpu(args, cfg, peaks, peak_kind):
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     rbf = bool(cfg.get("rbf"))
+    from skema_b200.distributed import reduce_partial_sketches, shard_rows
+
     if rbf:
         # the kernel's rows are sharded over the ranks (every rank holds all
         # points): total work fixed as the rank count grows
         m_glob = cfg["m"]
-        per = (m_glob + world - 1) // world
-        row0 = rank * per
-        m_local = max(0, min(per, m_glob - row0))
+        row0, m_local = shard_rows(m_glob, world, rank, cfg["window"])
         P, gamma = make_points_torch(cfg, m_glob, cfg["seed"], dev)
         cfg["gamma"] = gamma
     else:
@@ -272,8 +272,7 @@ def run_gpu(args, cfg, peaks, peak_kind):
         if world > 1:
             ctx.get_sketch(0, Xbuf)
             ctx.get_sketch(2, Zbuf)
-            dist.all_reduce(Xbuf)
-            dist.all_reduce(Zbuf)
+            reduce_partial_sketches(Xbuf, Zbuf, m_glob, cfg["window"], float(a.sketch_nu))
 
     for _ in range(args.warmup):
         step()
