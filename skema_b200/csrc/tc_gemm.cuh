@@ -58,6 +58,8 @@ struct OutSpec {
   // columns [0, split) of the tile row space go to p0, [split, ncols) to p1
   float* p0;
   __nv_bfloat16* p1;      // BF16 output for the second part (or nullptr)
+  __nv_bfloat16* p1lo;    // with p1: the BF16 rounding of (value - p1), so p1 + p1lo
+                          // carries about 16 significant bits (or nullptr)
   float* p1f;             // FP32 output for the second part (or nullptr)
   int64_t rs0, cs0, rs1, cs1;
   float alpha0, beta0, alpha1, beta1;
@@ -277,7 +279,10 @@ __device__ __forceinline__ bool epilogue_unit(const OutSpec& o, uint32_t tmem, u
       } else {
         const int64_t cc = col - o.split;
         if (o.p1) {
-          o.p1[row * o.rs1 + cc * o.cs1] = __float2bfloat16(alpha1 * v[i]);
+          const float x = alpha1 * v[i];
+          const __nv_bfloat16 hi = __float2bfloat16(x);
+          o.p1[row * o.rs1 + cc * o.cs1] = hi;
+          if (o.p1lo) o.p1lo[row * o.rs1 + cc * o.cs1] = __float2bfloat16(x - __bfloat162float(hi));
         } else if (o.p1f) {
           float* p = o.p1f + row * o.rs1 + cc * o.cs1;
           if (o.atomic1)
