@@ -351,7 +351,7 @@ def run_gpu(args, cfg, peaks, peak_kind):
         zeta = 8
         # rowptr + (col, val) per nonzero + Y rows written + the byte-packed map
         alg_bytes = (m_local + 1) * 8 + nnz * 8 + m_local * k * 4 + n * zeta
-        roof = hbm_roof("csr_ssign_y_kernel", "update.omega", alg_bytes)
+        roof = hbm_roof("csr_ssign_y16_kernel", "update.omega", alg_bytes)
     elif rbf and a.precision:
         # row pass: Gram + [Y|T] sketch per kernel entry; column pass: Gram + X
         d = cfg["d"]

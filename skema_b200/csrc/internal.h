@@ -50,10 +50,11 @@ struct Map {
   void* lowp = nullptr;
   // SparseSign: stored rows, zeta packed entries each: column | sign << 31.
   uint32_t* packed = nullptr;
-  // Stored-transposed SparseSign with zeta == 8 and ncol <= 128: one 64-bit
-  // word per stored row, byte t = column | sign << 7 (the streaming Y
-  // kernel's map format).
-  uint64_t* packed8 = nullptr;
+  // Stored-transposed SparseSign with zeta == 8 and ncol <= 128, as eight
+  // 16-bit entries per stored row (16 bytes): (column * 128) | sign << 15,
+  // the byte offset of the column's bin in a warp's bin-major accumulator
+  // (the streaming Y kernel's map format).
+  void* packed16 = nullptr;
   // SparseSign maps that are row-sparse over the input rows (Upsilon, Phi of
   // the three-sketch): (input row, map row, sign) triples sorted by input
   // row, on the host and on the device.

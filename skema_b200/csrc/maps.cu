@@ -49,18 +49,21 @@ __global__ void sparse_sign_map_kernel(uint32_t* __restrict__ packed, int64_t nr
   }
 }
 
-// Byte form of a SparseSign map with zeta = 8 and at most 128 columns.
-__global__ void pack8_kernel(const uint32_t* __restrict__ packed, uint64_t* __restrict__ out,
-                             int64_t nrow) {
+// Offset form of a SparseSign map with zeta = 8 and at most 128 columns:
+// eight 16-bit entries per stored row, entry t
+// = (column * 128) | sign << 15, i.e. the byte offset of bin `column` in a
+// warp's bin-major accumulator (32 floats per bin) with the sign on top.
+__global__ void pack16_kernel(const uint32_t* __restrict__ packed, uint4* __restrict__ out, int64_t nrow) {
   for (int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; row < nrow;
        row += (int64_t)gridDim.x * blockDim.x) {
-    uint64_t w = 0;
-    for (int t = 0; t < 8; ++t) {
-      const uint32_t e = packed[row * 8 + t];
-      const uint64_t byte = (e & 0x7fu) | ((e >> 31) << 7);
-      w |= byte << (8 * t);
+    uint32_t w[4];
+    for (int q = 0; q < 4; ++q) {
+      const uint32_t e0 = packed[row * 8 + 2 * q], e1 = packed[row * 8 + 2 * q + 1];
+      const uint32_t h0 = ((e0 & 0x7fu) << 7) | ((e0 >> 31) << 15);
+      const uint32_t h1 = ((e1 & 0x7fu) << 7) | ((e1 >> 31) << 15);
+      w[q] = h0 | (h1 << 16);
     }
-    out[row] = w;
+    out[row] = make_uint4(w[0], w[1], w[2], w[3]);
   }
 }
 
@@ -83,11 +86,12 @@ static int grid_for(int64_t total, int threads, int sms) {
   return (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)sms * 32));
 }
 
-static void build_pack8(skema_ctx* c, Map& mp) {
+static void build_pack16(skema_ctx* c, Map& mp) {
   if (mp.kind != SKEMA_MAP_SPARSE_SIGN || !mp.transposed) return;
   if (mp.zeta != 8 || mp.ncol > 128) return;
-  if (!mp.packed8) SKEMA_CUDA(cudaMalloc(&mp.packed8, sizeof(uint64_t) * (size_t)mp.nrow));
-  pack8_kernel<<<grid_for(mp.nrow, 256, c->sm_count), 256, 0, c->stream>>>(mp.packed, mp.packed8, mp.nrow);
+  if (!mp.packed16) SKEMA_CUDA(cudaMalloc(&mp.packed16, sizeof(uint4) * (size_t)mp.nrow));
+  pack16_kernel<<<grid_for(mp.nrow, 256, c->sm_count), 256, 0, c->stream>>>(
+      mp.packed, reinterpret_cast<uint4*>(mp.packed16), mp.nrow);
   SKEMA_LAUNCHED(c);
 }
 
@@ -120,7 +124,7 @@ void map_generate(skema_ctx* c, Map& mp, int precision) {
     sparse_sign_map_kernel<<<grid_for(mp.nrow, threads, c->sm_count), threads, 0, c->stream>>>(
         mp.packed, mp.nrow, (uint32_t)mp.ncol, mp.zeta, mp.seed);
     SKEMA_LAUNCHED(c);
-    build_pack8(c, mp);
+    build_pack16(c, mp);
   }
 }
 
@@ -128,8 +132,8 @@ void map_free(Map& mp) {
   if (mp.f32) cudaFree(mp.f32);
   if (mp.lowp) cudaFree(mp.lowp);
   if (mp.packed) cudaFree(mp.packed);
-  if (mp.packed8) cudaFree(mp.packed8);
-  mp.packed8 = nullptr;
+  if (mp.packed16) cudaFree(mp.packed16);
+  mp.packed16 = nullptr;
   if (mp.d_inv_row) cudaFree(mp.d_inv_row);
   if (mp.d_inv_rs) cudaFree(mp.d_inv_rs);
   mp.f32 = nullptr;
@@ -232,7 +236,7 @@ void map_import(skema_ctx* c, Map& mp, const double* values, const int32_t* indi
   }
   SKEMA_CUDA(cudaMemcpyAsync(mp.packed, h.data(), sizeof(uint32_t) * ne, cudaMemcpyHostToDevice,
                              c->stream));
-  build_pack8(c, mp);
+  build_pack16(c, mp);
   SKEMA_CUDA(cudaStreamSynchronize(c->stream));
   map_build_inverse(c, mp);
 }

@@ -40,35 +40,23 @@ int grid_cap(const skema_ctx* c, int64_t want, int per_sm) {
 // the rows are done, bin r of the 32 rows is one coalesced 128-byte store
 // into the column-major Y. Nonzeros go through the read-only path (the
 // warp's 32 rows are contiguous in col/val, so L1 serves the lanes' strided
-// walk); each lane keeps UNR nonzeros and their map words in flight. The
-// map is one 8-byte word per input column when zeta = 8 and k <= 128
-// (index in 7 bits, sign in the top bit of each byte), else zeta 32-bit
-// words (column | sign << 31).
+// walk). This general form reads zeta 32-bit map words per input column
+// (column | sign << 31); csr_ssign_y16_kernel below is the form for zeta = 8
+// and k <= 128.
 // ---------------------------------------------------------------------------
-template <bool BYTE8>
-__device__ __forceinline__ void ssign_apply(float* __restrict__ my, const uint64_t* __restrict__ omg8,
-                                            const uint32_t* __restrict__ omg32, int zeta, int32_t j,
-                                            float a) {
-  if (BYTE8) {
-    const uint64_t w = __ldg(omg8 + j);
-#pragma unroll
-    for (int t = 0; t < 8; ++t) {
-      const uint32_t byte = (uint32_t)(w >> (8 * t)) & 0xffu;
-      my[(byte & 0x7fu) * 32] += (byte & 0x80u) ? -a : a;
-    }
-  } else {
-    for (int t = 0; t < zeta; ++t) {
-      const uint32_t w = __ldg(omg32 + (int64_t)j * zeta + t);
-      my[(w & 0x7fffffffu) * 32] += (w >> 31) ? -a : a;
-    }
+__device__ __forceinline__ void ssign_apply(float* __restrict__ my, const uint32_t* __restrict__ omg32, int zeta,
+                                            int32_t j, float a) {
+  for (int t = 0; t < zeta; ++t) {
+    const uint32_t w = __ldg(omg32 + (int64_t)j * zeta + t);
+    my[(w & 0x7fffffffu) * 32] += (w >> 31) ? -a : a;
   }
 }
 
-template <bool BYTE8, int UNR>
+template <int UNR>
 __global__ void __launch_bounds__(128)
     csr_ssign_y_kernel(const int64_t* __restrict__ rowptr, const int32_t* __restrict__ col,
                        const float* __restrict__ val, int64_t col_offset, int64_t nrows,
-                       const uint64_t* __restrict__ omg8, const uint32_t* __restrict__ omg32,
+                       const uint32_t* __restrict__ omg32,
                        int zeta, int k, int ncol, float* __restrict__ Y, int64_t ldy, float alpha,
                        float beta) {
   extern __shared__ float acc_all[];
@@ -94,11 +82,11 @@ __global__ void __launch_bounds__(128)
       }
 #pragma unroll
       for (int u = 0; u < UNR; ++u)
-        if ((unsigned)jj[u] < (unsigned)ncol) ssign_apply<BYTE8>(my, omg8, omg32, zeta, jj[u], aa[u]);
+        if ((unsigned)jj[u] < (unsigned)ncol) ssign_apply(my, omg32, zeta, jj[u], aa[u]);
     }
     for (; p < e; ++p) {
       const int32_t j = __ldg(col + p);
-      if ((unsigned)j < (unsigned)ncol) ssign_apply<BYTE8>(my, omg8, omg32, zeta, j, __ldg(val + p));
+      if ((unsigned)j < (unsigned)ncol) ssign_apply(my, omg32, zeta, j, __ldg(val + p));
     }
     if (live) {
       float* yp = Y + i;
@@ -111,6 +99,90 @@ __global__ void __launch_bounds__(128)
           yp[r * ldy] = fmaf(beta, yp[r * ldy], alpha * v);
       }
     }
+  }
+}
+
+// The same Y rows with fewer instructions per bin update, for the map's
+// 16-bit offset form (zeta = 8, k <= 128): each entry already is the byte
+// offset of its bin in the warp's accumulator with the sign in bit 15, so an
+// update is one extract, one add, one sign flip on the value's bits and the
+// shared read-modify-write. alpha is folded into the nonzeros as they are
+// loaded; each lane loads up to U nonzeros of its row and their map rows
+// before applying any. The write-out walks a pointer down the column-major Y
+// and the bins are cleared afterwards with 16-byte stores.
+// The launch keeps about 128 KB of bins per SM and gives the rest of the
+// unified L1 / shared memory to L1: each lane walks its own row in col/val,
+// so a warp keeps ~20 lines live between its steps, and with the largest
+// shared-memory carve-out those lines were evicted and fetched again
+// (0.163 ms at 20 warps/SM vs 0.129 ms at 12 warps/SM with a 55 % carve-out
+// for the 1e6 x 1e5, 1e7-nonzero case).
+__device__ __forceinline__ void bin_add(uint32_t addr, float v) {
+  float x;
+  asm volatile("ld.shared.f32 %0, [%1];" : "=f"(x) : "r"(addr));
+  asm volatile("st.shared.f32 [%0], %1;" ::"r"(addr), "f"(x + v) : "memory");
+}
+
+template <int U>
+__global__ void __launch_bounds__(128)
+    csr_ssign_y16_kernel(const int64_t* __restrict__ rowptr, const int32_t* __restrict__ col,
+                         const float* __restrict__ val, int64_t col_offset, int64_t nrows,
+                         const uint4* __restrict__ omg16, int k, int ncol, float* __restrict__ Y, int64_t ldy,
+                         float alpha, float beta) {
+  extern __shared__ __align__(16) float acc_all[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  float* bins = acc_all + (size_t)warp * k * 32;
+  const uint32_t base = (uint32_t)__cvta_generic_to_shared(bins + lane);
+  float4* bins4 = reinterpret_cast<float4*>(bins);
+  const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+  for (int q = lane; q < k * 8; q += 32) bins4[q] = z4;
+  __syncwarp();
+  const int64_t ntiles = (nrows + 31) / 32;
+  for (int64_t tile = (int64_t)blockIdx.x * nw + warp; tile < ntiles; tile += (int64_t)gridDim.x * nw) {
+    const int64_t i = tile * 32 + lane;
+    const bool live = i < nrows;
+    int64_t b = live ? __ldg(rowptr + i) - col_offset : 0;
+    int64_t e = __shfl_down_sync(0xffffffffu, b, 1);
+    if (lane == 31 || i + 1 >= nrows) e = live ? __ldg(rowptr + i + 1) - col_offset : 0;
+    for (int64_t p = b; p < e; p += U) {
+      int32_t jj[U];
+      uint32_t ab[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        jj[u] = -1;
+        ab[u] = 0u;
+        if (p + u < e) {
+          jj[u] = __ldcs(col + p + u);
+          ab[u] = __float_as_uint(__ldcs(val + p + u) * alpha);
+        }
+      }
+      uint4 ww[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u)
+        ww[u] = ((unsigned)jj[u] < (unsigned)ncol) ? __ldg(omg16 + jj[u]) : make_uint4(0u, 0u, 0u, 0u);
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        if ((unsigned)jj[u] >= (unsigned)ncol) continue;
+        const uint32_t w[4] = {ww[u].x, ww[u].y, ww[u].z, ww[u].w};
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          bin_add(base + (w[q] & 0x7fffu), __uint_as_float(ab[u] ^ ((w[q] << 16) & 0x80000000u)));
+          bin_add(base + ((w[q] >> 16) & 0x7fffu), __uint_as_float(ab[u] ^ (w[q] & 0x80000000u)));
+        }
+      }
+    }
+    if (live) {
+      float* yp = Y + i;
+      if (beta == 0.f) {
+#pragma unroll 9
+        for (int r = 0; r < k; ++r, yp += ldy) __stcs(yp, bins[r * 32 + lane]);
+      } else {
+#pragma unroll 9
+        for (int r = 0; r < k; ++r, yp += ldy) *yp = fmaf(beta, *yp, bins[r * 32 + lane]);
+      }
+    }
+    __syncwarp();
+    for (int q = lane; q < k * 8; q += 32) bins4[q] = z4;
+    __syncwarp();
   }
 }
 
@@ -318,22 +390,44 @@ std::pair<int64_t, int64_t> entry_range(const Map& mp, int64_t a, int64_t b) {
 
 }  // namespace
 
-template <bool BYTE8, int UNR>
+template <int UNR>
 void launch_csr_ssign_y_variant(skema_ctx* c, int warps_per_block, const int64_t* rowptr,
                                 const int32_t* col, const float* val, int64_t col_offset,
                                 int64_t nrows, const Map& O, float* Y, int64_t ldy, float alpha,
                                 float beta) {
   const int k = (int)c->k;
   const size_t smem = sizeof(float) * 32 * (size_t)k * warps_per_block;
-  auto kern = csr_ssign_y_kernel<BYTE8, UNR>;
+  auto kern = csr_ssign_y_kernel<UNR>;
   SKEMA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 1;
   SKEMA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * warps_per_block, smem));
   const int64_t tiles = (nrows + 31) / 32;
   const int grid = grid_cap(c, (tiles + warps_per_block - 1) / warps_per_block, std::max(1, per_sm));
-  kern<<<grid, 32 * warps_per_block, smem, c->stream>>>(rowptr, col, val, col_offset, nrows, O.packed8,
-                                                        O.packed, O.zeta, k, (int)c->n, Y, ldy,
-                                                        alpha, beta);
+  kern<<<grid, 32 * warps_per_block, smem, c->stream>>>(rowptr, col, val, col_offset, nrows, O.packed, O.zeta,
+                                                        k, (int)c->n, Y, ldy, alpha, beta);
+  SKEMA_LAUNCHED(c);
+}
+
+template <int U>
+static void launch_csr_ssign_y16(skema_ctx* c, int wpb, const int64_t* rowptr, const int32_t* col, const float* val,
+                                 int64_t col_offset, int64_t nrows, const Map& O, float* Y, int64_t ldy, float alpha,
+                                 float beta) {
+  const int k = (int)c->k;
+  const size_t smem = sizeof(float) * 32 * (size_t)k * wpb;
+  auto kern = csr_ssign_y16_kernel<U>;
+  SKEMA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  // ~128 KB of bins per SM; the carve-out leaves the rest of the unified
+  // L1 / shared memory to L1
+  int smem_sm = 0;
+  SKEMA_CUDA(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, c->dev));
+  const int per_sm = (int)std::max<size_t>(1, (size_t)(128 * 1024) / smem);
+  const int carve = (int)std::min<size_t>(100, (per_sm * (smem + 1024) * 100 + smem_sm - 1) / std::max(1, smem_sm) + 2);
+  SKEMA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, carve));
+  const int64_t tiles = (nrows + 31) / 32;
+  const int grid = grid_cap(c, (tiles + wpb - 1) / wpb, per_sm);
+  kern<<<grid, 32 * wpb, smem, c->stream>>>(rowptr, col, val, col_offset, nrows,
+                                            static_cast<const uint4*>(O.packed16), k, (int)c->n, Y, ldy, alpha,
+                                            beta);
   SKEMA_LAUNCHED(c);
 }
 
@@ -344,10 +438,10 @@ static void launch_csr_ssign_y(skema_ctx* c, const int64_t* rowptr, const int32_
   while (wpb > 1 && sizeof(float) * 32 * (size_t)c->k * wpb > 96 * 1024) wpb >>= 1;
   if (sizeof(float) * 32 * (size_t)c->k * wpb > 200 * 1024)
     fail(SKEMA_EUNSUPPORTED, "sketch range too large for the sparse-sign kernel");
-  if (O.packed8)
-    launch_csr_ssign_y_variant<true, 4>(c, wpb, rowptr, col, val, col_offset, nrows, O, Y, ldy, alpha, beta);
+  if (O.packed16)
+    launch_csr_ssign_y16<6>(c, wpb, rowptr, col, val, col_offset, nrows, O, Y, ldy, alpha, beta);
   else
-    launch_csr_ssign_y_variant<false, 4>(c, wpb, rowptr, col, val, col_offset, nrows, O, Y, ldy, alpha, beta);
+    launch_csr_ssign_y_variant<4>(c, wpb, rowptr, col, val, col_offset, nrows, O, Y, ldy, alpha, beta);
 }
 
 // ---------------------------------------------------------------------------
