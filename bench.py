@@ -57,6 +57,9 @@ WORKLOADS = {
                      rbf=True),
     "rbf-fp32": dict(m=100_000, n=100_000, d=128, rank=64, k=257, s=515, window=4096, seed=4, kind=0, prec=0,
                      rbf=True),
+    # the kernel-sketch forward / adjoint pair: 50,000 points in 64 dimensions
+    # (same mixture recipe), Omega k = 129; one step = forward + VJP
+    "rbf-vjp": dict(m=50_000, n=50_000, d=64, rank=32, k=129, s=259, window=50_000, seed=1, kind=0, vjp=True),
 }
 
 
@@ -208,6 +211,108 @@ def make_points_torch(cfg, n_pts, seed, device):
 
 
 # ------------------------------------------------------------ our arm ------
+def run_vjp(args, cfg, peaks, peak_kind):
+    """Forward Y = K Omega^T and the VJP w.r.t. gamma and the points through
+    the C ABI on device buffers; the cotangent is fixed (2 Y of the first
+    forward, i.e. L = ||Y||_F^2). Ranks under torchrun run replicas."""
+    import torch
+    import torch.distributed as dist
+
+    import skema_b200._lib as L
+    from skema_b200.sketchy import _ctx_for_standalone
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    N, d, k = cfg["m"], cfg["d"], cfg["k"]
+    P, gamma = make_points_torch(cfg, N, cfg["seed"], dev)
+    g = torch.Generator(device=dev)
+    g.manual_seed(5)
+    Om = (2.0 * torch.rand(k, N, generator=g, device=dev) - 1.0).contiguous()
+    Y = torch.empty((N, k), dtype=torch.float32, device=dev)
+    dX = torch.empty_like(P)
+    dg = torch.zeros(1, dtype=torch.float64, device=dev)
+    ctx = _ctx_for_standalone(local)
+    stream = torch.cuda.Stream(device=dev)
+    torch.cuda.set_stream(stream)
+    ctx.set_stream(stream.cuda_stream)
+    lib, h = ctx.lib, ctx.h
+    ctx._check(lib.skema_rbf_sketch_fwd(h, P.data_ptr(), N, d, gamma, Om.data_ptr(), k, Y.data_ptr()))
+    Ybar = (2.0 * Y).contiguous()
+    torch.cuda.synchronize()
+
+    def step():
+        ctx._check(lib.skema_rbf_sketch_fwd(h, P.data_ptr(), N, d, gamma, Om.data_ptr(), k, Y.data_ptr()))
+        ctx._check(lib.skema_rbf_sketch_vjp(h, P.data_ptr(), N, d, gamma, Om.data_ptr(), k, Ybar.data_ptr(),
+                                            dX.data_ptr(), dg.data_ptr()))
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        t0 = time.perf_counter()
+        while time.perf_counter() - t0 < args.clock_lead:
+            step()
+            torch.cuda.synchronize()
+        l0 = ctx.launch_count()
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        launches = ctx.launch_count() - l0
+        t0 = time.perf_counter()
+        while time.perf_counter() - t0 < args.clock_tail:
+            step()
+            torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    ms_t = torch.tensor([ms], device=dev)
+    if world > 1:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms = float(ms_t.item())
+    # forward 2N^2(d + k) (Gram tiles + the sketch), VJP 2N^2(k + 2d) (M = Ybar Omega,
+    # E X and E^T X) plus recomputed Gram tiles 2N^2 d
+    flops = 2.0 * N * N * (d + k) + 2.0 * N * N * (k + 3 * d)
+    roof = {"bound": "fp32-simt", "achieved": flops / (ms / 1e3) / 1e12, "peak": 74.4, "unit": "TFLOP/s",
+            "frac": flops / (ms / 1e3) / 1e12 / 74.4,
+            "peak_source": "nominal FP32 SIMT (148 SMs x 128 FMA/clk x 2 x 1.965 GHz)",
+            "kernel": "sgemm_kernel + rbf_tile_kernel (forward and adjoint)", "kernel_ms": ms,
+            "algorithmic_flops_per_step": flops, "traffic": None}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        v, ns, thr = cpu_sample_vjp(cfg)
+        cpu = {"value": v, "unit": "rows/s", "cores": thr, "kind": "port",
+               "sample": f"forward + VJP of a {ns}-point problem (same d, k) in FP64, scaled by (N/{ns})^2",
+               "host_cpu": _cpu_model(), "nproc": os.cpu_count()}
+    out = {
+        "metric": "sketched rows/s", "value": world * N / (ms / 1e3), "unit": "rows/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic (seeded; no dataset)",
+        "config": dict(config_of(args, cfg, world, 0), gamma=gamma),
+        "roofline": roof, "cpu_baseline": cpu,
+        "e2e": {"value": world * N / (ms / 1e3), "unit": "rows/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0, "note": "device-buffer entry points; same as value"},
+        "gpu_launches": launches,
+        "clocks": dict(clk.summary(), window="samples span continuous load bracketing the timed steps"),
+    }
+    ctx.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
 def run_gpu(args, cfg, peaks, peak_kind):
     import torch
     import torch.distributed as dist
@@ -446,6 +551,11 @@ def run_gpu(args, cfg, peaks, peak_kind):
 
 
 def config_of(args, cfg, world, nnz):
+    if cfg.get("vjp"):
+        return {"workload": args.workload, "points": cfg["m"], "d": cfg["d"], "k": cfg["k"],
+                "step": "skema_rbf_sketch_fwd + skema_rbf_sketch_vjp, device buffers",
+                "cotangent": "fixed 2 Y (L = ||Y||_F^2)", "parallelism": f"replicas x{world}",
+                "l2": "K tiles (2.5e9 entries) recomputed per step, never stored; E blocks stream > 126 MB L2"}
     c = {"workload": args.workload, "m_per_gpu": cfg["m"], "n": cfg["n"], "rank": cfg["rank"],
          "range_k": cfg["k"], "core_s": cfg["s"], "window": cfg["window"],
          "maps": "sparse-sign zeta=8" if cfg["kind"] == 1 else "gauss",
@@ -630,6 +740,23 @@ def cpu_sample_rbf(cfg, budget_s):
     return done / dt, done, O.num_threads()
 
 
+def cpu_sample_vjp(cfg, ns=1000):
+    """Oracle FP64 forward + VJP of an ns-point problem with the workload's d
+    and k; every term costs N^2 (d or k), so the full-size time is the
+    sample's times (N / ns)^2. Returns (rows/s, ns, threads)."""
+    from oracle import sketchy_oracle as O
+
+    N, d, k = cfg["m"], cfg["d"], cfg["k"]
+    Xs = O.mixture_points(ns, d, seed=cfg["seed"])
+    gs = O.median_gamma(Xs)
+    Os = np.random.default_rng(5).uniform(-1, 1, size=(k, ns))
+    t0 = time.perf_counter()
+    Ys = O.rbf_fwd64(Xs, gs, Os)
+    O.rbf_vjp64(Xs, gs, Os, 2.0 * Ys)
+    ts = time.perf_counter() - t0
+    return N / (ts * (N / ns) ** 2), ns, O.num_threads()
+
+
 def cpu_baseline(args, cfg, budget_s):
     if cfg.get("rbf"):
         v, rows, thr = cpu_sample_rbf(cfg, budget_s)
@@ -664,7 +791,10 @@ def run_reference(args, cfg):
     rows = 0
     thr = 1
     for i in range(args.warmup + args.steps):
-        if cfg.get("rbf"):
+        if cfg.get("vjp"):
+            v, ns, thr = cpu_sample_vjp(cfg)
+            r = cfg["m"]
+        elif cfg.get("rbf"):
             v, r, thr = cpu_sample_rbf(cfg, budget)
         elif args.workload.startswith("csr"):
             v, r, thr = cpu_sample_sparse(cfg, budget, seed_rows=min(cfg["m"], 200_000))
@@ -713,6 +843,9 @@ def main():
         run_reference(args, cfg)
         return
     peaks, kind = load_peaks()
+    if cfg.get("vjp"):
+        run_vjp(args, cfg, peaks, kind)
+        return
     run_gpu(args, cfg, peaks, kind)
 
 
