@@ -60,6 +60,8 @@ WORKLOADS = {
     # the kernel-sketch forward / adjoint pair: 50,000 points in 64 dimensions
     # (same mixture recipe), Omega k = 129; one step = forward + VJP
     "rbf-vjp": dict(m=50_000, n=50_000, d=64, rank=32, k=129, s=259, window=50_000, seed=1, kind=0, vjp=True),
+    "rbf-vjp-bf16": dict(m=50_000, n=50_000, d=64, rank=32, k=129, s=259, window=50_000, seed=1, kind=0, vjp=True,
+                         prec=1),
 }
 
 
@@ -238,7 +240,8 @@ def run_vjp(args, cfg, peaks, peak_kind):
     Y = torch.empty((N, k), dtype=torch.float32, device=dev)
     dX = torch.empty_like(P)
     dg = torch.zeros(1, dtype=torch.float64, device=dev)
-    ctx = _ctx_for_standalone(local)
+    prec = cfg.get("prec", 0)
+    ctx = _ctx_for_standalone(local, prec)
     stream = torch.cuda.Stream(device=dev)
     torch.cuda.set_stream(stream)
     ctx.set_stream(stream.cuda_stream)
@@ -283,11 +286,41 @@ def run_vjp(args, cfg, peaks, peak_kind):
     # forward 2N^2(d + k) (Gram tiles + the sketch), VJP 2N^2(k + 2d) (M = Ybar Omega,
     # E X and E^T X) plus recomputed Gram tiles 2N^2 d
     flops = 2.0 * N * N * (d + k) + 2.0 * N * N * (k + 3 * d)
-    roof = {"bound": "fp32-simt", "achieved": flops / (ms / 1e3) / 1e12, "peak": 74.4, "unit": "TFLOP/s",
-            "frac": flops / (ms / 1e3) / 1e12 / 74.4,
-            "peak_source": "nominal FP32 SIMT (148 SMs x 128 FMA/clk x 2 x 1.965 GHz)",
-            "kernel": "sgemm_kernel + rbf_tile_kernel (forward and adjoint)", "kernel_ms": ms,
-            "algorithmic_flops_per_step": flops, "traffic": None}
+    if prec == 1:
+        # tensor-core form: the forward is one rbf_sketch_kernel launch, the
+        # adjoint two rbf_vjp_kernel passes, each with its own Gram tiles
+        # (2 N^2 (d + k + d) per pass: S, M and E X); the roofline is taken
+        # over the whole step against the sustained BF16 peak
+        flops = 2.0 * N * N * (d + k) + 2 * 2.0 * N * N * (2 * d + k)
+        pk = peaks["bf16_tflops_sustained"]
+        roof = {"bound": "tensor", "achieved": flops / (ms / 1e3) / 1e12, "peak": pk, "unit": "TFLOP/s",
+                "frac": flops / (ms / 1e3) / 1e12 / pk,
+                "peak_source": f"bf16_tflops_sustained ({peak_kind})",
+                "kernel": "rbf_sketch_kernel (forward) + 2 x rbf_vjp_kernel (adjoint)", "kernel_ms": ms,
+                "algorithmic_flops_per_step": flops, "traffic": None}
+    else:
+        roof = {"bound": "fp32-simt", "achieved": flops / (ms / 1e3) / 1e12, "peak": 74.4, "unit": "TFLOP/s",
+                "frac": flops / (ms / 1e3) / 1e12 / 74.4,
+                "peak_source": "nominal FP32 SIMT (148 SMs x 128 FMA/clk x 2 x 1.965 GHz)",
+                "kernel": "sgemm_kernel + rbf_tile_kernel (forward and adjoint)", "kernel_ms": ms,
+                "algorithmic_flops_per_step": flops, "traffic": None}
+    acc = None
+    if prec == 1 and not args.no_accuracy:
+        # the same forward / adjoint through an FP32 context, as the yardstick
+        ref = _ctx_for_standalone(local, 0)
+        ref.set_stream(stream.cuda_stream)
+        Y32 = torch.empty_like(Y)
+        dX32 = torch.empty_like(dX)
+        dg32 = torch.zeros(1, dtype=torch.float64, device=dev)
+        ref._check(lib.skema_rbf_sketch_fwd(ref.h, P.data_ptr(), N, d, gamma, Om.data_ptr(), k, Y32.data_ptr()))
+        ref._check(lib.skema_rbf_sketch_vjp(ref.h, P.data_ptr(), N, d, gamma, Om.data_ptr(), k, Ybar.data_ptr(),
+                                            dX32.data_ptr(), dg32.data_ptr()))
+        torch.cuda.synchronize()
+        rel = lambda a, b: float((a.double() - b.double()).norm() / b.double().norm())
+        acc = {"against": "the FP32 form on the same inputs",
+               "Y_rel_fro": rel(Y, Y32), "dX_rel_fro": rel(dX, dX32),
+               "dgamma_rel": float(abs(dg.item() - dg32.item()) / abs(dg32.item()))}
+        ref.close()
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         v, ns, thr = cpu_sample_vjp(cfg)
@@ -297,7 +330,8 @@ def run_vjp(args, cfg, peaks, peak_kind):
     out = {
         "metric": "sketched rows/s", "value": world * N / (ms / 1e3), "unit": "rows/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic (seeded; no dataset)",
+        "scaling": "weak", "vs_baseline": None, "dtype": "bf16" if prec == 1 else "fp32",
+        "data": "synthetic (seeded; no dataset)",
         "config": dict(config_of(args, cfg, world, 0), gamma=gamma),
         "roofline": roof, "cpu_baseline": cpu,
         "e2e": {"value": world * N / (ms / 1e3), "unit": "rows/s", "h2d_bytes_per_step": 0,
@@ -305,6 +339,8 @@ def run_vjp(args, cfg, peaks, peak_kind):
         "gpu_launches": launches,
         "clocks": dict(clk.summary(), window="samples span continuous load bracketing the timed steps"),
     }
+    if acc is not None:
+        out["accuracy"] = acc
     ctx.close()
     if world > 1:
         dist.barrier()
@@ -554,6 +590,7 @@ def config_of(args, cfg, world, nnz):
     if cfg.get("vjp"):
         return {"workload": args.workload, "points": cfg["m"], "d": cfg["d"], "k": cfg["k"],
                 "step": "skema_rbf_sketch_fwd + skema_rbf_sketch_vjp, device buffers",
+                "precision": "bf16 tensor-core form" if cfg.get("prec") == 1 else "fp32",
                 "cotangent": "fixed 2 Y (L = ||Y||_F^2)", "parallelism": f"replicas x{world}",
                 "l2": "K tiles (2.5e9 entries) recomputed per step, never stored; E blocks stream > 126 MB L2"}
     c = {"workload": args.workload, "m_per_gpu": cfg["m"], "n": cfg["n"], "rank": cfg["rank"],

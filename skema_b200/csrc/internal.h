@@ -206,6 +206,12 @@ void spd_ssign_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr);
 // ---- RBF, BF16 tensor-core form without a stored kernel (rbf_tc.cu) ----
 bool rbf_tc_supported(const skema_ctx* c, int64_t d);
 void rbf_tc_update(skema_ctx* c, Mat P, int64_t npts, int64_t d, int64_t row0, int64_t nrows);
+// The standalone forward / adjoint pair in the same form (d <= 64, k <= 192).
+bool rbf_pair_tc_supported(const skema_ctx* c, int64_t d, int64_t k, double gamma);
+void rbf_fwd_tc(skema_ctx* c, const float* pts, int64_t N, int64_t d, double gamma, const float* omega, int64_t k,
+                float* Y);
+void rbf_vjp_tc(skema_ctx* c, const float* pts, int64_t N, int64_t d, double gamma, const float* omega, int64_t k,
+                const float* Ybar, float* dpts, double* dgamma);
 
 // ---- RBF (rbf.cu) ----
 void rbf_update(skema_ctx* c, Mat P, int64_t npts, int64_t d, int64_t row0,

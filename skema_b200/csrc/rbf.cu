@@ -201,6 +201,10 @@ void rbf_update(skema_ctx* c, Mat P, int64_t npts, int64_t d, int64_t row0, int6
 
 void rbf_fwd(skema_ctx* c, const float* pts, int64_t N, int64_t d, double gamma,
              const float* omega, int64_t k, float* Y) {
+  if (rbf_pair_tc_supported(c, d, k, gamma)) {
+    rbf_fwd_tc(c, pts, N, d, gamma, omega, k, Y);
+    return;
+  }
   const Mat P{pts, d, 1};
   const int64_t wb = rows_per_block(N, N);
   float* Kw = (float*)workspace(c, sizeof(float) * (size_t)(wb * N));
@@ -214,6 +218,10 @@ void rbf_fwd(skema_ctx* c, const float* pts, int64_t N, int64_t d, double gamma,
 
 void rbf_vjp(skema_ctx* c, const float* pts, int64_t N, int64_t d, double gamma,
              const float* omega, int64_t k, const float* Ybar, float* dpts, double* dgamma) {
+  if (rbf_pair_tc_supported(c, d, k, gamma)) {
+    rbf_vjp_tc(c, pts, N, d, gamma, omega, k, Ybar, dpts, dgamma);
+    return;
+  }
   const Mat P{pts, d, 1};
   const int64_t wb = rows_per_block(N, N);
   const size_t eb = (sizeof(float) * (size_t)(wb * N) + 255) / 256 * 256;

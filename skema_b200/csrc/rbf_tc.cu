@@ -234,4 +234,167 @@ void rbf_tc_update(skema_ctx* c, Mat P, int64_t N, int64_t d, int64_t row0, int6
   }
 }
 
+// ---------------------------------------------------------------------------
+// The standalone forward / adjoint pair (skema_rbf_sketch_fwd / _vjp) in the
+// BF16 form: Y = K Omega^T by rbf_sketch_kernel (queries and keys all
+// points, V = Omega), the adjoint by two passes of rbf_vjp_kernel.
+namespace {
+
+// E X + E^T X and the row / column sums of E -> dL/dx (FP32 points, d
+// columns, S with leading dimension d).
+__global__ void rbf_pair_dx_kernel(const float* __restrict__ P, int64_t N, int64_t d, float gamma,
+                                   const float* __restrict__ rsum, const float* __restrict__ csum,
+                                   const float* __restrict__ S, float* __restrict__ dX) {
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < N * d; q += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = q / d;
+    dX[q] = -2.f * gamma * ((rsum[i] + csum[i]) * P[q] - S[q]);
+  }
+}
+
+struct PairPrep {
+  __nv_bfloat16* X16;
+  float* cval;
+  int64_t npad;
+};
+
+// Points -> BF16 rows (d padded to 64) and their constants; scratch from *sp.
+PairPrep pair_prep(skema_ctx* c, const float* pts, int64_t N, int64_t d, float gl, char** sp) {
+  auto take = [&](size_t b) {
+    char* p = *sp;
+    *sp += (b + 255) / 256 * 256;
+    return p;
+  };
+  PairPrep pp;
+  pp.npad = (N + tc::RBF_BJ - 1) / tc::RBF_BJ * tc::RBF_BJ;
+  pp.X16 = reinterpret_cast<__nv_bfloat16*>(take(sizeof(__nv_bfloat16) * (size_t)(N * 64)));
+  pp.cval = reinterpret_cast<float*>(take(sizeof(float) * (size_t)pp.npad));
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((pp.npad * 32 + 255) / 256, c->sm_count * 16));
+  rbf_prep_kernel<<<grid, 256, 0, c->stream>>>(pts, d, 1, N, d, 64, gl, pp.X16, pp.cval, pp.npad);
+  SKEMA_LAUNCHED(c);
+  return pp;
+}
+
+size_t pair_prep_bytes(int64_t N) {
+  const int64_t npad = (N + 63) / 64 * 64;
+  return sizeof(__nv_bfloat16) * (size_t)(N * 64) + sizeof(float) * (size_t)npad + 512;
+}
+
+template <int KK>
+void launch_vjp(skema_ctx* c, const CUtensorMap& tqx, const CUtensorMap& tkx, const CUtensorMap& tqa,
+                const CUtensorMap& tkb, const CUtensorMap& txt, const tc::RbfVjpArgs& a) {
+  constexpr uint32_t STAGE = ((64 * 128 + KK * 64 * 128 + 64 * 128 + 256 + 1023) / 1024) * 1024;
+  const size_t smem = 128 * 128 + KK * 128 * 128 + 3 * (size_t)STAGE + 2 * 128 * 128 + 1024 + 256;
+  auto kern = tc::rbf_vjp_kernel<1, KK>;
+  SKEMA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int64_t units = (int64_t)a.qtiles * a.ksplit;
+  const int grid = (int)std::min<int64_t>(units, c->sm_count);
+  kern<<<grid, tc::kThreads, smem, c->stream>>>(tqx, tkx, tqa, tkb, txt, a, c->dev_err);
+  SKEMA_LAUNCHED(c);
+  c->dev_err_armed = true;
+}
+
+}  // namespace
+
+bool rbf_pair_tc_supported(const skema_ctx* c, int64_t d, int64_t k, double gamma) {
+  return c->p.precision == SKEMA_PREC_BF16 && tc_available(c) && d >= 1 && d <= 64 && k >= 1 && k <= 192 &&
+         gamma > 0.0;
+}
+
+void rbf_fwd_tc(skema_ctx* c, const float* pts, int64_t N, int64_t d, double gamma, const float* omega, int64_t k,
+                float* Y) {
+  const float gl = (float)gamma * kLog2e;
+  const int64_t ldN = pad8(N);
+  char* ws = static_cast<char*>(workspace(c, pair_prep_bytes(N) + sizeof(__nv_bfloat16) * (size_t)(k * ldN) + 256));
+  char* sp = ws;
+  const PairPrep pp = pair_prep(c, pts, N, d, gl, &sp);
+  __nv_bfloat16* Om16 = reinterpret_cast<__nv_bfloat16*>(sp);  // k x N row-major, ld pad8(N)
+  to_bf16(c, Mat{omega, N, 1}, k, N, Om16, ldN, 1);
+  const CUtensorMap tq = tmap_bf16(pp.X16, 64, (uint64_t)N, 128, 64, tc::RBF_BQ);
+  const CUtensorMap tk = tmap_bf16(pp.X16, 64, (uint64_t)N, 128, 64, tc::RBF_BJ);
+  tc::RbfArgs a;
+  a.nq = N, a.qbase = 0, a.kbase = 0;
+  a.nblocks = pp.npad / tc::RBF_BJ;
+  a.qtiles = (int)((N + tc::RBF_BQ - 1) / tc::RBF_BQ);
+  const bool small = k <= 144;
+  a.chunk_cols = small ? 144 : k <= 272 ? 272 : 400;
+  a.nchunks = (int)((k + a.chunk_cols - 1) / a.chunk_cols);
+  const Plan pl = plan_split(c, (int64_t)a.qtiles * a.nchunks, pp.npad, 16);
+  a.bchunk = pl.kchunk / tc::RBF_BJ;
+  a.ksplit = (int)((a.nblocks + a.bchunk - 1) / a.bchunk);
+  a.cq = pp.cval, a.ckey = pp.cval, a.two_g = 2.f * gl;
+  a.klog2w = 0.f, a.kwlen = 1, a.knwin = 1;
+  tc::OutSpec o = out_spec();
+  o.p0 = Y, o.rs0 = k, o.cs0 = 1, o.alpha0 = 1.f, o.beta0 = 0.f;
+  o.rows = N, o.split = k, o.ncols = k;
+  if (a.ksplit > 1) {
+    SKEMA_CUDA(cudaMemsetAsync(Y, 0, sizeof(float) * (size_t)(N * k), c->stream));
+    o.atomic0 = 1;
+  }
+  const CUtensorMap tv1 = tmap_bf16(Om16, (uint64_t)N, (uint64_t)k, (uint64_t)ldN * 2, 64, small ? 128 : 256);
+  if (small) {
+    const CUtensorMap tv2 = tmap_bf16(Om16, (uint64_t)N, (uint64_t)k, (uint64_t)ldN * 2, 64, 16);
+    launch_rbf<128, 16, 1, 3>(c, tq, tk, tv1, tv2, a, o);
+  } else {
+    run_pass<1>(c, k <= 272, tq, tk, Om16, N, k, ldN, a, o);
+  }
+}
+
+void rbf_vjp_tc(skema_ctx* c, const float* pts, int64_t N, int64_t d, double gamma, const float* omega, int64_t k,
+                const float* Ybar, float* dpts, double* dgamma) {
+  const float gl = (float)gamma * kLog2e;
+  const int KK = (int)((k + 63) / 64);
+  const int64_t kp = 64 * KK, ldN = pad8(N);
+  auto rup = [](size_t b) { return (b + 255) / 256 * 256; };
+  const size_t b_xt = rup(sizeof(__nv_bfloat16) * (size_t)(64 * ldN));
+  const size_t b_a = rup(sizeof(__nv_bfloat16) * (size_t)(N * kp));
+  const size_t b_s = rup(sizeof(float) * (size_t)(N * d));
+  const size_t b_v = rup(sizeof(float) * (size_t)N);
+  char* ws = static_cast<char*>(workspace(c, pair_prep_bytes(N) + b_xt + 2 * b_a + b_s + 2 * b_v));
+  char* sp = ws;
+  const PairPrep pp = pair_prep(c, pts, N, d, gl, &sp);
+  __nv_bfloat16* XT16 = reinterpret_cast<__nv_bfloat16*>(sp);  // 64 x N: features as rows
+  __nv_bfloat16* Yb16 = reinterpret_cast<__nv_bfloat16*>(sp + b_xt);        // N x kp
+  __nv_bfloat16* OmT16 = reinterpret_cast<__nv_bfloat16*>(sp + b_xt + b_a);  // N x kp
+  float* S = reinterpret_cast<float*>(sp + b_xt + 2 * b_a);
+  float* rs = reinterpret_cast<float*>(sp + b_xt + 2 * b_a + b_s);
+  float* cs = reinterpret_cast<float*>(sp + b_xt + 2 * b_a + b_s + b_v);
+  // zero padding (features >= d, columns >= k) and the accumulators
+  SKEMA_CUDA(cudaMemsetAsync(XT16, 0, b_xt + 2 * b_a + b_s + 2 * b_v, c->stream));
+  SKEMA_CUDA(cudaMemsetAsync(dgamma, 0, sizeof(double), c->stream));
+  to_bf16(c, Mat{pts, d, 1}, N, d, XT16, 1, ldN);
+  to_bf16(c, Mat{Ybar, k, 1}, N, k, Yb16, kp, 1);
+  to_bf16(c, Mat{omega, 1, N}, N, k, OmT16, kp, 1);
+  const CUtensorMap tqx = tmap_bf16(pp.X16, 64, (uint64_t)N, 128, 64, tc::RBF_BQ);
+  const CUtensorMap tkx = tmap_bf16(pp.X16, 64, (uint64_t)N, 128, 64, tc::RBF_BJ);
+  const CUtensorMap txt = tmap_bf16(XT16, (uint64_t)N, 64, (uint64_t)ldN * 2, 64, 64);
+  const CUtensorMap tyq = tmap_bf16(Yb16, (uint64_t)kp, (uint64_t)N, (uint64_t)kp * 2, 64, tc::RBF_BQ);
+  const CUtensorMap tyk = tmap_bf16(Yb16, (uint64_t)kp, (uint64_t)N, (uint64_t)kp * 2, 64, tc::RBF_BJ);
+  const CUtensorMap toq = tmap_bf16(OmT16, (uint64_t)kp, (uint64_t)N, (uint64_t)kp * 2, 64, tc::RBF_BQ);
+  const CUtensorMap tok = tmap_bf16(OmT16, (uint64_t)kp, (uint64_t)N, (uint64_t)kp * 2, 64, tc::RBF_BJ);
+  tc::RbfVjpArgs a;
+  a.N = N;
+  a.nblocks = pp.npad / tc::RBF_BJ;
+  a.qtiles = (int)((N + tc::RBF_BQ - 1) / tc::RBF_BQ);
+  const Plan pl = plan_split(c, a.qtiles, pp.npad, 8);
+  a.bchunk = pl.kchunk / tc::RBF_BJ;
+  a.ksplit = (int)((a.nblocks + a.bchunk - 1) / a.bchunk);
+  a.cval = pp.cval, a.two_g = 2.f * gl, a.inv_g = 1.f / gl;
+  a.S = S, a.d = d;
+  for (int pass = 0; pass < 2; ++pass) {
+    a.rsum = pass == 0 ? rs : cs;
+    a.dgamma = pass == 0 ? dgamma : nullptr;
+    const CUtensorMap& tqa = pass == 0 ? tyq : toq;
+    const CUtensorMap& tkb = pass == 0 ? tok : tyk;
+    if (KK == 1)
+      launch_vjp<1>(c, tqx, tkx, tqa, tkb, txt, a);
+    else if (KK == 2)
+      launch_vjp<2>(c, tqx, tkx, tqa, tkb, txt, a);
+    else
+      launch_vjp<3>(c, tqx, tkx, tqa, tkb, txt, a);
+  }
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((N * d + 255) / 256, c->sm_count * 16));
+  rbf_pair_dx_kernel<<<grid, 256, 0, c->stream>>>(pts, N, d, (float)gamma, rs, cs, S, dpts);
+  SKEMA_LAUNCHED(c);
+}
+
 }  // namespace skema

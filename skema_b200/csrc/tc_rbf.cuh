@@ -315,5 +315,317 @@ __global__ void __launch_bounds__(kThreads, 1)
   }
 }
 
+// ---------------------------------------------------------------------------
+// Adjoint of Y = K Omega^T (the kernel-sketch VJP) with K regenerated tile by
+// tile. Given Ybar = dL/dY, with M = Ybar Omega and E = M o K (E_ii = 0:
+// the diagonal entry of K is fixed at 1 and has no gradient),
+//   dL/dgamma = -sum_ij E_ij d_ij^2,
+//   dL/dx_i   = -2 gamma [ (rowsum(E)_i + colsum(E)_i) x_i - (E X)_i - (E^T X)_i ].
+// One pass of this kernel, for a unit of 128 query points q and a range of
+// 64-point key blocks j:
+//   S = X_q X_j^T   and   M = A_q B_j^T        tcgen05, N = 64, into TMEM
+//   E = M o exp2(2 g' S + c_q + c_j)           four warps, in registers;
+//                                              row sums of E and the dgamma
+//                                              terms accumulate per thread
+//   O += E X_j                                 tcgen05, N = padded d
+// then O, the row sums and the dgamma terms go out with FP32 / FP64
+// atomics. The first pass (A = Ybar, B = Omega^T) gives E X, rowsum(E) and
+// dgamma; the second (A = Omega^T, B = Ybar) sees E^T and gives E^T X and
+// colsum(E). K, M and E are never stored.
+struct RbfVjpArgs {
+  int64_t N;          // points
+  int64_t nblocks;    // 64-point key blocks (N padded)
+  int64_t bchunk;     // key blocks per split
+  int qtiles, ksplit;
+  const float* cval;  // c_p = -g' ||bf16(x_p)||^2, -inf past N
+  float two_g;        // 2 g'
+  float inv_g;        // 1 / g'  (d^2 = -(2 g' S + c_q + c_j) / g')
+  float* S;           // N x d, += E X
+  int64_t d;
+  float* rsum;        // N, += row sums of E
+  double* dgamma;     // += -sum E d^2 (first pass), or nullptr
+};
+
+template <int DK, int KK>
+__global__ void __launch_bounds__(kThreads, 1)
+    rbf_vjp_kernel(const __grid_constant__ CUtensorMap tmQx, const __grid_constant__ CUtensorMap tmKx,
+                   const __grid_constant__ CUtensorMap tmQa, const __grid_constant__ CUtensorMap tmKb,
+                   const __grid_constant__ CUtensorMap tmXt, RbfVjpArgs a, int* err) {
+  constexpr int NS = 3;                     // key stages
+  constexpr int DP = 64 * DK;               // padded features = output columns
+  constexpr uint32_t QX = DK * RBF_BQ * 128;
+  constexpr uint32_t QA = KK * RBF_BQ * 128;
+  constexpr uint32_t KX = DK * RBF_BJ * 128;
+  constexpr uint32_t KB = KK * RBF_BJ * 128;
+  constexpr uint32_t XT = DP * 128;         // DP rows of 64 keys
+  constexpr uint32_t STAGE = ((KX + KB + XT + 256 + 1023) / 1024) * 1024;
+  constexpr uint32_t P_BYTES = RBF_BQ * 128;
+  constexpr uint32_t TS = 128, TM = 192;    // TMEM columns of S and M; O at 0
+  static_assert(DK == 1, "one 64-row box of X^T per key block");
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char* smem = reinterpret_cast<unsigned char*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+  unsigned char* qx = smem;
+  unsigned char* qa = qx + QX;
+  unsigned char* st = qa + QA;
+  unsigned char* ps = st + NS * STAGE;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(ps + 2 * P_BYTES);
+  uint64_t* qfull = bar + 0;
+  uint64_t* qempty = bar + 1;
+  uint64_t* full = bar + 2;
+  uint64_t* empty = full + NS;
+  uint64_t* sfull = empty + NS;
+  uint64_t* sfree = sfull + 1;
+  uint64_t* pfull = sfree + 1;
+  uint64_t* pfree = pfull + 2;
+  uint64_t* ofull = pfree + 2;
+  uint64_t* ofree = ofull + 1;
+  uint32_t* tbase = reinterpret_cast<uint32_t*>(ofree + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int total = a.qtiles * a.ksplit;
+  if (threadIdx.x == 0) {
+    mbar_init(qfull, 1);
+    mbar_init(qempty, 1);
+    for (int s = 0; s < NS; ++s) {
+      mbar_init(full + s, 1);
+      mbar_init(empty + s, 1);
+    }
+    mbar_init(sfull, 1);
+    mbar_init(sfree, 128);
+    for (int p = 0; p < 2; ++p) {
+      mbar_init(pfull + p, 128);
+      mbar_init(pfree + p, 1);
+    }
+    mbar_init(ofull, 1);
+    mbar_init(ofree, 128);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 5) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tbase)),
+                 "r"(256)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tbase;
+  auto decode = [&](int t, int& qt, int64_t& b0, int64_t& b1) {
+    qt = t % a.qtiles;
+    b0 = (int64_t)(t / a.qtiles) * a.bchunk;
+    b1 = min(a.nblocks, b0 + a.bchunk);
+  };
+
+  if (warp == 4 && lane == 0) {
+    // ---------------- TMA producer ----------------
+    uint32_t it = 0, un = 0;
+    bool ok = true;
+    for (int t = blockIdx.x; t < total && ok; t += gridDim.x, ++un) {
+      int qt;
+      int64_t b0, b1;
+      decode(t, qt, b0, b1);
+      if (!mbar_wait(qempty, (un & 1) ^ 1, err)) break;
+      mbar_expect_tx(qfull, QX + QA);
+#pragma unroll
+      for (int f = 0; f < DK; ++f) tma_load_2d(&tmQx, qfull, qx + f * RBF_BQ * 128, 64 * f, qt * RBF_BQ);
+#pragma unroll
+      for (int f = 0; f < KK; ++f) tma_load_2d(&tmQa, qfull, qa + f * RBF_BQ * 128, 64 * f, qt * RBF_BQ);
+      for (int64_t b = b0; b < b1; ++b, ++it) {
+        const int s = it % NS;
+        const uint32_t ph = (it / NS) & 1;
+        if (!mbar_wait(empty + s, ph ^ 1, err)) {
+          ok = false;
+          break;
+        }
+        unsigned char* sk = st + s * STAGE;
+        mbar_expect_tx(full + s, KX + KB + XT + 256);
+        const int kb = (int)(b * RBF_BJ);
+#pragma unroll
+        for (int f = 0; f < DK; ++f) tma_load_2d(&tmKx, full + s, sk + f * RBF_BJ * 128, 64 * f, kb);
+#pragma unroll
+        for (int f = 0; f < KK; ++f) tma_load_2d(&tmKb, full + s, sk + KX + f * RBF_BJ * 128, 64 * f, kb);
+        tma_load_2d(&tmXt, full + s, sk + KX + KB, kb, 0);
+        asm volatile(
+            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], 256, [%2];" ::"r"(
+                smem_u32(sk + KX + KB + XT)),
+            "l"(a.cval + b * RBF_BJ), "r"(smem_u32(full + s))
+            : "memory");
+      }
+    }
+  } else if (warp == 5 && lane == 0) {
+    // ---------------- MMA issuer ----------------
+    constexpr uint32_t id64 = idesc_bf16(RBF_BJ, false, false);
+    constexpr uint32_t idD = idesc_bf16(DP, false, false);
+    uint32_t it = 0, un = 0, g = 0, pc = 0;
+    bool ok = true;
+    auto out_mma = [&](int s, bool first) -> bool {
+      const uint32_t pb = pc & 1;
+      if (!mbar_wait(pfull + pb, (pc >> 1) & 1, err)) return false;
+      tc_fence_after();
+      const uint32_t pa = smem_u32(ps + pb * P_BYTES);
+      const uint32_t xb = smem_u32(st + s * STAGE + KX + KB);
+#pragma unroll
+      for (int kk = 0; kk < RBF_BJ / 16; ++kk)
+        umma(tmem, sdesc(pa + kk * 32, 16, 1024), sdesc(xb + kk * 32, 16, 1024), idD, (!first || kk > 0) ? 1u : 0u);
+      umma_commit(empty + s);
+      umma_commit(pfree + pb);
+      ++pc;
+      return true;
+    };
+    for (int t = blockIdx.x; t < total && ok; t += gridDim.x, ++un) {
+      int qt;
+      int64_t b0, b1;
+      decode(t, qt, b0, b1);
+      if (!mbar_wait(qfull, un & 1, err)) break;
+      int prev_s = -1;
+      bool first = true;
+      for (int64_t b = b0; b < b1; ++b, ++it) {
+        const int s = it % NS;
+        const uint32_t ph = (it / NS) & 1;
+        if (!mbar_wait(full + s, ph, err) || !mbar_wait(sfree, (g & 1) ^ 1, err)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t qxa = smem_u32(qx), qaa = smem_u32(qa), kb = smem_u32(st + s * STAGE);
+#pragma unroll
+        for (int f = 0; f < DK; ++f)
+#pragma unroll
+          for (int kk = 0; kk < 4; ++kk)
+            umma(tmem + TS, sdesc(qxa + f * RBF_BQ * 128 + kk * 32, 16, 1024),
+                 sdesc(kb + f * RBF_BJ * 128 + kk * 32, 16, 1024), id64, (f > 0 || kk > 0) ? 1u : 0u);
+#pragma unroll
+        for (int f = 0; f < KK; ++f)
+#pragma unroll
+          for (int kk = 0; kk < 4; ++kk)
+            umma(tmem + TM, sdesc(qaa + f * RBF_BQ * 128 + kk * 32, 16, 1024),
+                 sdesc(kb + KX + f * RBF_BJ * 128 + kk * 32, 16, 1024), id64, (f > 0 || kk > 0) ? 1u : 0u);
+        umma_commit(sfull);
+        ++g;
+        if (b + 1 == b1) umma_commit(qempty);
+        if (prev_s >= 0) {
+          if (first && !mbar_wait(ofree, (un & 1) ^ 1, err)) {
+            ok = false;
+            break;
+          }
+          if (!out_mma(prev_s, first)) {
+            ok = false;
+            break;
+          }
+          first = false;
+        }
+        prev_s = s;
+      }
+      if (!ok) break;
+      if (prev_s >= 0) {
+        if (first && !mbar_wait(ofree, (un & 1) ^ 1, err)) break;
+        if (!out_mma(prev_s, first)) break;
+      }
+      umma_commit(ofull);
+    }
+  } else if (warp < 4) {
+    // ---------------- E tiles, row sums, dgamma, epilogue ----------------
+    const uint32_t lane_off = (uint32_t)(warp * 32) << 16;
+    uint32_t it = 0, un = 0, g = 0, pc = 0;
+    for (int t = blockIdx.x; t < total; t += gridDim.x, ++un) {
+      int qt;
+      int64_t b0, b1;
+      decode(t, qt, b0, b1);
+      const int64_t gq = (int64_t)qt * RBF_BQ + warp * 32 + lane;  // query point of this thread
+      const bool live = gq < a.N;
+      const float cq = live ? a.cval[gq] : 0.f;
+      float rs_acc = 0.f, dg_acc = 0.f;
+      bool ok = true;
+      for (int64_t b = b0; b < b1; ++b, ++it, ++g, ++pc) {
+        if (!__all_sync(0xffffffffu, mbar_wait(sfull, g & 1, err))) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t pb = pc & 1;
+        if (!__all_sync(0xffffffffu, mbar_wait(pfree + pb, ((pc >> 1) & 1) ^ 1, err))) {
+          ok = false;
+          break;
+        }
+        const float* ck = reinterpret_cast<const float*>(st + (it % NS) * STAGE + KX + KB + XT);
+        const int64_t dcol = gq - b * RBF_BJ;  // diagonal column of this block, if any
+        unsigned char* prow = ps + pb * P_BYTES + (warp * 32 + lane) * 128;
+        const int sw = lane & 7;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          float sv[32], mv[32];
+          tmem_ld32(tmem + TS + lane_off + 32 * h, sv);
+          tmem_ld32(tmem + TM + lane_off + 32 * h, mv);
+          if (h == 1) {
+            tc_fence_before();
+            mbar_arrive(sfree);
+          }
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const float4 k0 = reinterpret_cast<const float4*>(ck)[8 * h + 2 * q];
+            const float4 k1 = reinterpret_cast<const float4*>(ck)[8 * h + 2 * q + 1];
+            const float kc[8] = {k0.x, k0.y, k0.z, k0.w, k1.x, k1.y, k1.z, k1.w};
+            float e[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+              const int cl = 8 * q + u, col = 32 * h + cl;
+              // clamped to [-256, 0]: 2^x is 0 below -126 either way, and
+              // the padding keys (c = -inf, M = 0) give 0 * x = 0, not NaN
+              const float x = fmaxf(fminf(fmaf(a.two_g, sv[cl], cq + kc[u]), 0.f), -256.f);
+              float ev = mv[cl] * ex2_approx(x);
+              if (col == dcol) ev = 0.f;
+              rs_acc += ev;
+              dg_acc = fmaf(ev, x, dg_acc);
+              e[u] = ev;
+            }
+            __nv_bfloat162 hh[4] = {__floats2bfloat162_rn(e[0], e[1]), __floats2bfloat162_rn(e[2], e[3]),
+                                    __floats2bfloat162_rn(e[4], e[5]), __floats2bfloat162_rn(e[6], e[7])};
+            *reinterpret_cast<uint4*>(prow + (((4 * h + q) ^ sw) << 4)) = *reinterpret_cast<const uint4*>(hh);
+          }
+        }
+        fence_proxy_async();
+        mbar_arrive(pfull + pb);
+      }
+      if (!ok) break;
+      // epilogue: O = (E X)_q for this unit's key range
+      if (!__all_sync(0xffffffffu, mbar_wait(ofull, un & 1, err))) break;
+      tc_fence_after();
+#pragma unroll
+      for (int c0 = 0; c0 < DP; c0 += 32) {
+        float v[32];
+        tmem_ld32(tmem + lane_off + c0, v);
+        if (c0 + 32 >= DP) {
+          tc_fence_before();
+          mbar_arrive(ofree);
+        }
+        if (live) {
+#pragma unroll
+          for (int i = 0; i < 32; ++i)
+            if (c0 + i < a.d) atomicAdd(a.S + gq * a.d + c0 + i, v[i]);
+        }
+      }
+      if (live) atomicAdd(a.rsum + gq, rs_acc);
+      if (a.dgamma) {
+#pragma unroll
+        for (int o = 16; o; o >>= 1) dg_acc += __shfl_xor_sync(0xffffffffu, dg_acc, o);
+        // -sum E d^2 = sum E x / g' with x = -g' d^2
+        if (lane == 0) atomicAdd(a.dgamma, (double)dg_acc * (double)a.inv_g);
+      }
+    }
+  }
+  if ((warp == 4 || warp == 5) && lane == 0 && *(volatile int*)err) {
+    const unsigned long long t0 = now_ns();
+    while (now_ns() - t0 < 20000000ull) __nanosleep(1000);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 5) {
+    __syncwarp();
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256) : "memory");
+  }
+}
+
 }  // namespace tc
 }  // namespace skema

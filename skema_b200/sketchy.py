@@ -513,17 +513,20 @@ def sketchysvd(matrix, alg: AlgParams):
         return sk.low_rank_approx()
 
 
-def _ctx_for_standalone(device: int = 0) -> _Context:
-    alg = AlgParams(matrix_m=1, matrix_n=1, rank=1, device=device)
+def _ctx_for_standalone(device: int = 0, precision: int = L.PREC_FP32) -> _Context:
+    alg = AlgParams(matrix_m=1, matrix_n=1, rank=1, device=device, precision=precision)
     return _Context(alg)
 
 
-def rbf_sketch_fwd(pts, gamma: float, omega, ctx: _Context | None = None):
-    """Y = K Omega^T for device tensors pts (N x d), omega (k x N)."""
+def rbf_sketch_fwd(pts, gamma: float, omega, ctx: _Context | None = None, precision: int = L.PREC_FP32):
+    """Y = K Omega^T for device tensors pts (N x d), omega (k x N).
+    precision (used when no ctx is given): PREC_BF16 takes the tensor-core
+    form for d <= 64 and k <= 192 (kernel tiles from BF16 points, FP32
+    accumulation), PREC_FP32 the FP32 form."""
     import torch
 
     own = ctx is None
-    ctx = ctx or _ctx_for_standalone(pts.device.index or 0)
+    ctx = ctx or _ctx_for_standalone(pts.device.index or 0, precision)
     try:
         pts = pts.contiguous()
         omega = omega.contiguous()
@@ -538,12 +541,13 @@ def rbf_sketch_fwd(pts, gamma: float, omega, ctx: _Context | None = None):
             ctx.close()
 
 
-def rbf_sketch_vjp(pts, gamma: float, omega, Ybar, ctx: _Context | None = None):
-    """(dL/dpts, dL/dgamma) of Y = K Omega^T given Ybar = dL/dY."""
+def rbf_sketch_vjp(pts, gamma: float, omega, Ybar, ctx: _Context | None = None, precision: int = L.PREC_FP32):
+    """(dL/dpts, dL/dgamma) of Y = K Omega^T given Ybar = dL/dY; precision
+    as for rbf_sketch_fwd."""
     import torch
 
     own = ctx is None
-    ctx = ctx or _ctx_for_standalone(pts.device.index or 0)
+    ctx = ctx or _ctx_for_standalone(pts.device.index or 0, precision)
     try:
         pts = pts.contiguous()
         omega = omega.contiguous()

@@ -72,3 +72,61 @@ def test_rbf_vjp_vs_finite_differences(setup, oracle):
         E[i, f] = hh
         fd = (L(X64 + E, g) - L(X64 - E, g)) / (2 * hh)
         assert abs(dX[i, f] - fd) <= 1e-4 * np.abs(dX).max() + 1e-4 * abs(fd)
+
+
+# BF16 tensor-core form of the pair (BF16 context, d <= 64, k <= 192): kernel
+# tiles from BF16-rounded points via the Gram expansion, M = Ybar Omega and
+# E X from BF16 operands, FP32 accumulation. Bars against the FP64 oracle
+# (relative Frobenius / absolute relative): Y 1e-2, dL/dX 3e-2, dL/dgamma 2e-2.
+BF16_CASES = [
+    (500, 6, 17, 1),     # one 64-column slice of Ybar / Omega
+    (700, 64, 129, 2),   # the benchmark's d and k on a small N; three slices
+    (777, 33, 192, 3),   # k at the limit, ragged N and d
+    (130, 1, 64, 4),     # d = 1, k one full slice
+    (64, 8, 5, 5),       # a single key block
+]
+
+
+@pytest.mark.parametrize("N,d,k,seed", BF16_CASES)
+def test_rbf_pair_bf16_against_fp64(lib_built, oracle, N, d, k, seed):
+    import torch
+
+    import skema_b200 as sk
+    from skema_b200 import _lib as L
+
+    X = oracle.mixture_points(N, d, seed=seed)
+    g = oracle.median_gamma(X)
+    rng = np.random.default_rng(seed)
+    Om = rng.uniform(-1, 1, size=(k, N)).astype(np.float32)
+    Yb = rng.normal(size=(N, k)).astype(np.float32)
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    Y = sk.rbf_sketch_fwd(dev(X), g, dev(Om), precision=L.PREC_BF16).cpu().numpy()
+    dX, dg = sk.rbf_sketch_vjp(dev(X), g, dev(Om), dev(Yb), precision=L.PREC_BF16)
+    dX = dX.cpu().numpy()
+    X64, Om64 = X.astype(np.float64), Om.astype(np.float64)
+    Y64 = oracle.rbf_fwd64(X64, g, Om64)
+    dX64, dg64 = oracle.rbf_vjp64(X64, g, Om64, Yb.astype(np.float64))
+    ey = np.linalg.norm(Y - Y64) / np.linalg.norm(Y64)
+    ex = np.linalg.norm(dX - dX64) / np.linalg.norm(dX64)
+    eg = abs(dg - dg64) / abs(dg64)
+    print(f"bf16 pair N={N} d={d} k={k}: Y {ey:.2e} dX {ex:.2e} dgamma {eg:.2e}")
+    assert np.isfinite(Y).all() and np.isfinite(dX).all() and np.isfinite(dg)
+    assert ey < 1e-2 and ex < 3e-2 and eg < 2e-2, (ey, ex, eg)
+
+
+@pytest.mark.parametrize("d,k", [(65, 17), (6, 193)])
+def test_rbf_pair_bf16_context_outside_the_tensor_core_shapes(lib_built, oracle, d, k):
+    """Shapes past d = 64 or k = 192 take the FP32 form in a BF16 context."""
+    import torch
+
+    import skema_b200 as sk
+    from skema_b200 import _lib as L
+
+    N = 300
+    X = oracle.mixture_points(N, d, seed=7)
+    g = oracle.median_gamma(X)
+    Om = np.random.default_rng(7).uniform(-1, 1, size=(k, N)).astype(np.float32)
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    Y = sk.rbf_sketch_fwd(dev(X), g, dev(Om), precision=L.PREC_BF16).cpu().numpy()
+    Y64 = oracle.rbf_fwd64(X.astype(np.float64), g, Om.astype(np.float64))
+    assert np.linalg.norm(Y - Y64) / np.linalg.norm(Y64) < 1e-5
