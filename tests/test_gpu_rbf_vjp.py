@@ -76,8 +76,12 @@ def test_rbf_vjp_vs_finite_differences(setup, oracle):
 
 # BF16 tensor-core form of the pair (BF16 context, d <= 64, k <= 192): kernel
 # tiles from BF16-rounded points via the Gram expansion, M = Ybar Omega and
-# E X from BF16 operands, FP32 accumulation. Bars against the FP64 oracle
-# (relative Frobenius / absolute relative): Y 1e-2, dL/dX 3e-2, dL/dgamma 2e-2.
+# E X from BF16 operands, FP32 accumulation. Bars against the FP64 oracle:
+# Y and dL/dX 1e-2 and 3e-2 relative (Frobenius). dL/dgamma = -sum E d^2 is
+# a sum of terms of both signs whose total can be far smaller than the
+# terms (condition sum|E d^2| / |dL/dgamma| reaches 2e4 on the 64-point
+# case), so its bar is normwise: |error| <= 2e-3 sum|E d^2| against FP64,
+# and <= 1e-4 sum|E d^2| against the same sum from BF16-rounded operands.
 BF16_CASES = [
     (500, 6, 17, 1),     # one 64-column slice of Ybar / Omega
     (700, 64, 129, 2),   # the benchmark's d and k on a small N; three slices
@@ -108,10 +112,20 @@ def test_rbf_pair_bf16_against_fp64(lib_built, oracle, N, d, k, seed):
     dX64, dg64 = oracle.rbf_vjp64(X64, g, Om64, Yb.astype(np.float64))
     ey = np.linalg.norm(Y - Y64) / np.linalg.norm(Y64)
     ex = np.linalg.norm(dX - dX64) / np.linalg.norm(dX64)
-    eg = abs(dg - dg64) / abs(dg64)
-    print(f"bf16 pair N={N} d={d} k={k}: Y {ey:.2e} dX {ex:.2e} dgamma {eg:.2e}")
+    # the dgamma sum from BF16-rounded points and Ybar / Omega, FP64 arithmetic
+    bf = lambda a: torch.from_numpy(np.asarray(a, np.float32)).bfloat16().double().numpy()
+    Xb = bf(X)
+    n2 = (Xb ** 2).sum(1)
+    D2b = np.maximum(n2[:, None] + n2[None, :] - 2.0 * Xb @ Xb.T, 0.0)
+    Eb = (bf(Yb) @ bf(Om)) * np.exp(-g * D2b)
+    np.fill_diagonal(Eb, 0.0)
+    dgb = -(Eb * D2b).sum()
+    scale = np.abs(Eb * D2b).sum()
+    eg, egb = abs(dg - dg64) / scale, abs(dg - dgb) / scale
+    print(f"bf16 pair N={N} d={d} k={k}: Y {ey:.2e} dX {ex:.2e} dgamma {eg:.2e} (vs BF16 operands {egb:.2e})")
     assert np.isfinite(Y).all() and np.isfinite(dX).all() and np.isfinite(dg)
-    assert ey < 1e-2 and ex < 3e-2 and eg < 2e-2, (ey, ex, eg)
+    assert ey < 1e-2 and ex < 3e-2, (ey, ex)
+    assert eg < 2e-3 and egb < 1e-4, (eg, egb)
 
 
 @pytest.mark.parametrize("d,k", [(65, 17), (6, 193)])
