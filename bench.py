@@ -548,6 +548,13 @@ def run_gpu(args, cfg, peaks, peak_kind):
         a32 = dataclasses.replace(a, precision=0)
         with sk.SketchySVD(a32) as c32:
             c32.set_stream(stream.cuda_stream)
+            if a.precision == 2:
+                # the FP8 form holds its maps on the scaled E4M3 grid: the
+                # yardstick takes the same maps
+                from skema_b200 import _lib as L
+
+                for which in (L.UPSILON, L.OMEGA, L.PHI, L.PSI):
+                    c32.map_import(which, ctx.map_export(which)[0])
             c32.reset()
             c32.update_rows(inp, row0, m_local)
             _, S32, _ = c32.low_rank_approx()

@@ -172,9 +172,12 @@ static void free_all(skema_ctx* c) {
   if (c->ws) cudaFree(c->ws);
   if (c->stage) cudaFree(c->stage);
   if (c->op16) cudaFree(c->op16);
+  if (c->op8) cudaFree(c->op8);
+  if (c->fp8_win) cudaFree(c->fp8_win);
   if (c->dev_err) cudaFree(c->dev_err);
   c->X = c->Y = c->Z = nullptr;
-  c->ws = c->stage = c->op16 = nullptr;
+  c->ws = c->stage = c->op16 = c->op8 = nullptr;
+  c->fp8_win = nullptr;
   c->dev_err = nullptr;
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   c->own_stream = nullptr;

@@ -20,10 +20,12 @@
 // added with FP32 atomics into outputs scaled by nu beforehand.
 #include <cuda.h>
 #include <cuda_bf16.h>
+#include <cuda_fp8.h>
 #include <cuda_runtime.h>
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <cstring>
 #include <mutex>
 
 #include "internal.h"
@@ -120,6 +122,7 @@ tc::OutSpec out_spec() {
   o.rows = 0, o.split = 0, o.ncols = 0;
   o.atomic0 = 0, o.atomic1 = 0;
   o.row_log2w = 0.f, o.row_wlen = 1, o.row_nwin = 1;
+  o.scale = nullptr;
   return o;
 }
 
@@ -304,7 +307,7 @@ void launch_gemm(skema_ctx* c, const CUtensorMap& ta, const CUtensorMap& tb, int
 // X^T product straight from the FP32 window (converts it and writes A16).
 template <bool AROW>
 void launch_gemm_a32(skema_ctx* c, const CUtensorMap& ta32, const CUtensorMap& tb, const CUtensorMap& ta16,
-                     int64_t M, int64_t N, int64_t K, Plan pl, const tc::OutSpec& o) {
+                     int64_t M, int64_t N, int64_t K, Plan pl, const tc::OutSpec& o, uint32_t* amax) {
   constexpr int S1 = 3, S2 = 3;
   constexpr uint32_t STAGE = ((tc::BM * tc::BK * 2 + kNT * tc::BK * 2 + 1023) / 1024) * 1024;
   const size_t smem = (size_t)S1 * tc::BM * tc::BK * 4 + (size_t)S2 * STAGE + 1024 + 256;
@@ -319,7 +322,146 @@ void launch_gemm_a32(skema_ctx* c, const CUtensorMap& ta32, const CUtensorMap& t
   if (units <= 0 || K <= 0) return;
   if (units > 0x7fffffff) fail(SKEMA_EINVAL, "tensor-core grid too large");
   const int grid = (int)std::min<int64_t>(units, c->sm_count);
-  kern<<<grid, tc::kThreadsA32, smem, c->stream>>>(ta32, tb, ta16, K, pl.kchunk, g, o, c->dev_err);
+  kern<<<grid, tc::kThreadsA32, smem, c->stream>>>(ta32, tb, ta16, K, pl.kchunk, g, o, amax, c->dev_err);
+  SKEMA_LAUNCHED(c);
+  c->dev_err_armed = true;
+}
+
+// ---- FP8 form -------------------------------------------------------------
+// E4M3: largest finite value 448. Scales are powers of two, so scaling is
+// exact and only the rounding to the E4M3 grid loses information.
+constexpr float kE4M3Max = 448.f;
+
+__host__ __device__ inline float pow2_scale_for(float amax) {
+  // largest power of two s with amax * s <= 448 (1 when amax is 0 or not finite)
+  if (!(amax > 0.f) || !(amax < 3.0e38f)) return 1.f;
+  const float r = kE4M3Max / amax;
+  int e;
+#ifdef __CUDA_ARCH__
+  e = (int)((__float_as_uint(r) >> 23) & 0xffu) - 127;
+#else
+  uint32_t bits;
+  memcpy(&bits, &r, 4);
+  e = (int)((bits >> 23) & 0xffu) - 127;
+#endif
+  e = e < -126 ? -126 : (e > 127 ? 127 : e);
+  return ldexpf(1.f, e);
+}
+
+__device__ __forceinline__ uint8_t to_e4m3(float x) {
+  return (uint8_t)__nv_cvt_float_to_fp8(x, __NV_SATFINITE, __NV_E4M3);
+}
+__device__ __forceinline__ float from_e4m3(uint8_t b) {
+  const __half_raw h = __nv_cvt_fp8_to_halfraw((__nv_fp8_storage_t)b, __NV_E4M3);
+  return __half2float(__half(h));
+}
+
+// Map values onto the scaled E4M3 grid, in place: v -> e4m3(v * sm) / sm.
+__global__ void fp8_round_map_kernel(float* __restrict__ v, int64_t count, float sm) {
+  const float inv = 1.f / sm;  // sm is a power of two: exact
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < count; q += (int64_t)gridDim.x * blockDim.x)
+    v[q] = from_e4m3(to_e4m3(v[q] * sm)) * inv;
+}
+
+// Logical map rows [0, rows) -> E4M3(sm * map) at D[(r0 + r) * ld + j].
+__global__ void fp8_op_kernel(const float* __restrict__ f, int64_t rs, int64_t cs, int64_t rows, int64_t cols,
+                              float sm, uint8_t* __restrict__ D, int64_t ld) {
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < rows * cols;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = q / cols, j = q - r * cols;
+    D[r * ld + j] = to_e4m3(f[r * rs + j * cs] * sm);
+  }
+}
+
+// max |a| over the row-blocked BF16 window (padding rows are zeros), into
+// *amax as float bits.
+__global__ void amax_a16_kernel(const __nv_bfloat16* __restrict__ A16, int64_t count, uint32_t* amax) {
+  float mx = 0.f;
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < count; q += (int64_t)gridDim.x * blockDim.x)
+    mx = fmaxf(mx, fabsf(__bfloat162float(A16[q])));
+  const uint32_t wm = __reduce_max_sync(0xffffffffu, __float_as_uint(mx));
+  if ((threadIdx.x & 31) == 0) atomicMax(amax, wm);
+}
+
+// Row-blocked BF16 window (64-row blocks, a 128-byte line of 64 rows per
+// column) -> E4M3(scale_A a) row-major with row stride ld8 bytes, by 64 x 64
+// tiles through shared memory; scale_A from the window's amax (win[0]).
+// Block 0 also writes the [Y | T] product scale 1 / (scale_A scale_map)
+// into win[1].
+__global__ void __launch_bounds__(256)
+    a16_to_a8_kernel(const __nv_bfloat16* __restrict__ A16, int64_t rows, int64_t cols, uint8_t* __restrict__ A8,
+                     int64_t ld8, uint32_t* win, float smap) {
+  __shared__ uint32_t tile[64][17];  // [row][4-column group], padded
+  const float sa = pow2_scale_for(__uint_as_float(win[0]));
+  if (blockIdx.x == 0 && threadIdx.x == 0) win[1] = __float_as_uint(1.f / (sa * smap));
+  const int64_t nrb = (rows + 63) / 64, ncb = (cols + 63) / 64;
+  for (int64_t t = blockIdx.x; t < nrb * ncb; t += gridDim.x) {
+    const int64_t rb = t / ncb, j0 = (t - rb * ncb) * 64;
+    // read: column j0 + c of block rb is 64 BF16 rows (a 128-byte line);
+    // thread (c, g) converts rows 4g..4g+3 of column c
+    for (int q = threadIdx.x; q < 64 * 16; q += 256) {
+      const int c = q >> 4, g = q & 15;
+      uint32_t packed = 0;
+      if (j0 + c < cols) {
+        const uint2 w = *reinterpret_cast<const uint2*>(A16 + (rb * cols + j0 + c) * 64 + 4 * g);
+        const __nv_bfloat162 p0 = *reinterpret_cast<const __nv_bfloat162*>(&w.x);
+        const __nv_bfloat162 p1 = *reinterpret_cast<const __nv_bfloat162*>(&w.y);
+        const float v[4] = {__low2float(p0), __high2float(p0), __low2float(p1), __high2float(p1)};
+#pragma unroll
+        for (int e = 0; e < 4; ++e) packed |= (uint32_t)to_e4m3(v[e] * sa) << (8 * e);
+      }
+      // bytes of rows 4g..4g+3 in column c: scatter into the row-major tile
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        uint8_t* row = reinterpret_cast<uint8_t*>(&tile[4 * g + e][0]);
+        row[c] = (uint8_t)(packed >> (8 * e));
+      }
+    }
+    __syncthreads();
+    // write: row r of the tile is 64 bytes, 16 words
+    for (int q = threadIdx.x; q < 64 * 16; q += 256) {
+      const int r = q >> 4, w = q & 15;
+      const int64_t i = rb * 64 + r, j = j0 + 4 * w;
+      if (i < rows && j < cols) {
+        if (j + 4 <= cols) {
+          *reinterpret_cast<uint32_t*>(A8 + i * ld8 + j) = tile[r][w];
+        } else {
+          for (int e = 0; e < 4 && j + e < cols; ++e) A8[i * ld8 + j + e] = (uint8_t)(tile[r][w] >> (8 * e));
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+CUtensorMap tmap_u8(const void* base, uint64_t d0, uint64_t d1, uint64_t st1, uint32_t b0, uint32_t b1) {
+  return tmap_2d(CU_TENSOR_MAP_DATA_TYPE_UINT8, base, d0, d1, st1, b0, b1, CU_TENSOR_MAP_SWIZZLE_128B);
+}
+
+// [Y | T] in FP8: K split in multiples of the kernel's 128-element stage.
+Plan plan_fp8(Plan pl, int64_t K) {
+  pl.kchunk = (pl.kchunk + 127) / 128 * 128;
+  pl.ks = (int)((K + pl.kchunk - 1) / pl.kchunk);
+  return pl;
+}
+
+void launch_gemm_fp8(skema_ctx* c, const CUtensorMap& ta, const CUtensorMap& tb, int64_t M, int64_t N, int64_t K,
+                     Plan pl, const tc::OutSpec& o) {
+  constexpr int S = 5;
+  constexpr uint32_t STAGE = ((tc::BM * 128 + kNT * 128 + 1023) / 1024) * 1024;
+  const size_t smem = (size_t)S * STAGE + 1024 + 256;
+  auto kern = tc::gemm_fp8_kernel<kNT, S>;
+  SKEMA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  tc::Grid3 g;
+  g.mtiles = (int)((M + tc::BM - 1) / tc::BM);
+  g.ntiles = (int)((N + kNT - 1) / kNT);
+  g.m_fast = 0;
+  g.ksplit = pl.ks;
+  const int64_t units = (int64_t)g.mtiles * g.ntiles * g.ksplit;
+  if (units <= 0 || K <= 0) return;
+  if (units > 0x7fffffff) fail(SKEMA_EINVAL, "tensor-core grid too large");
+  const int grid = (int)std::min<int64_t>(units, c->sm_count);
+  kern<<<grid, tc::kThreads, smem, c->stream>>>(ta, tb, K, pl.kchunk, g, o, c->dev_err);
   SKEMA_LAUNCHED(c);
   c->dev_err_armed = true;
 }
@@ -374,14 +516,47 @@ void tc_z_update(skema_ctx* c, const __nv_bfloat16* T16, int64_t ldT, const TcSl
 }
 
 bool tc_available(const skema_ctx* c) {
-  return c->p.precision == SKEMA_PREC_BF16 && c->ups.lowp && c->phi.lowp && c->op16;
+  if (c->p.precision == SKEMA_PREC_FP8 && !(c->op8 && c->fp8_win)) return false;
+  return (c->p.precision == SKEMA_PREC_BF16 || c->p.precision == SKEMA_PREC_FP8) && c->ups.lowp && c->phi.lowp &&
+         c->op16;
 }
 
 // BF16 copies of the Gauss maps for the tensor-core form (dense and kernel
 // inputs); called after the maps are generated and after each map import.
 void tc_prepare_maps(skema_ctx* c) {
-  if (c->p.precision != SKEMA_PREC_BF16 || c->spd || c->p.issparse || c->p.dim_redux != SKEMA_MAP_GAUSS)
+  const bool fp8 = c->p.precision == SKEMA_PREC_FP8;
+  if ((c->p.precision != SKEMA_PREC_BF16 && !fp8) || c->spd || c->p.issparse || c->p.dim_redux != SKEMA_MAP_GAUSS)
     return;
+  if (fp8) {
+    // one power-of-two scale for all four maps (the largest maxval bounds
+    // them all), and the maps themselves moved onto that E4M3 grid, so that
+    // the FP8, BF16 and FP32 uses of a map see the same values
+    double mx = 0.0;
+    for (const Map* M : {&c->ups, &c->omg, &c->phi, &c->psi}) mx = std::max(mx, M->maxval);
+    c->fp8_map_scale = pow2_scale_for((float)mx);
+    for (Map* M : {&c->ups, &c->omg, &c->phi, &c->psi}) {
+      const int64_t cnt = M->lrows * M->lcols;
+      const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((cnt + 255) / 256, c->sm_count * 16));
+      fp8_round_map_kernel<<<grid, 256, 0, c->stream>>>(M->f32, cnt, c->fp8_map_scale);
+      SKEMA_LAUNCHED(c);
+    }
+    const int64_t n8 = (c->n + 15) / 16 * 16;
+    if (!c->op8) {
+      SKEMA_CUDA(cudaMalloc(&c->op8, (size_t)((c->k + c->s) * n8)));
+      SKEMA_CUDA(cudaMalloc(&c->fp8_win, 2 * sizeof(uint32_t)));
+    }
+    c->ld_op8 = n8;
+    SKEMA_CUDA(cudaMemsetAsync(c->op8, 0, (size_t)((c->k + c->s) * n8), c->stream));
+    auto conv8 = [&](const Map& M, int64_t r0) {
+      const int64_t cnt = M.lrows * M.lcols;
+      const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((cnt + 255) / 256, c->sm_count * 16));
+      fp8_op_kernel<<<grid, 256, 0, c->stream>>>(M.f32, M.rs, M.cs, M.lrows, M.lcols, c->fp8_map_scale,
+                                                 static_cast<uint8_t*>(c->op8) + r0 * n8, n8);
+      SKEMA_LAUNCHED(c);
+    };
+    conv8(c->omg, 0);
+    conv8(c->psi, c->k);
+  }
   const int64_t mp = pad8(c->m), np = pad8(c->n);
   if (!c->ups.lowp) {
     SKEMA_CUDA(cudaMalloc(&c->ups.lowp, sizeof(__nv_bfloat16) * (size_t)(c->k * mp)));
@@ -406,6 +581,7 @@ size_t tc_scratch_bytes(const skema_ctx* c, int64_t wr) {
   b += sizeof(__nv_bfloat16) * (size_t)(wp * c->s) + 256;               // T16
   b += sizeof(float) * (size_t)(wp * c->s) + 256;                       // T32 (split-K)
   b += tc_slice_bytes(c, wr);                                           // map slices (unaligned R0)
+  if (c->p.precision == SKEMA_PREC_FP8) b += (size_t)(wr * ((c->n + 15) / 16 * 16)) + 256;  // A8
   return b;
 }
 
@@ -424,6 +600,14 @@ void tc_dense_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr, void* scratch
   __nv_bfloat16* T16 = reinterpret_cast<__nv_bfloat16*>(take(sizeof(__nv_bfloat16) * (size_t)(wp * s)));
   float* T32 = reinterpret_cast<float*>(take(sizeof(float) * (size_t)(wp * s)));
   const float ybeta = y_rows_clean(c, R0, R0 + wr) ? 0.f : nu;
+  // FP8 form: the window's amax comes out of the X^T product (or a pass over
+  // A16), its power-of-two scale is applied while A16 is rounded to E4M3,
+  // and the [Y | T] product runs E4M3 x E4M3 with the scales undone in its
+  // epilogue. X^T and Z stay on the BF16 path.
+  const bool fp8 = c->p.precision == SKEMA_PREC_FP8;
+  const int64_t ld8 = (n + 15) / 16 * 16;
+  uint8_t* A8 = fp8 ? reinterpret_cast<uint8_t*>(take((size_t)(wr * ld8))) : nullptr;
+  if (fp8) SKEMA_CUDA(cudaMemsetAsync(c->fp8_win, 0, 2 * sizeof(uint32_t), c->stream));
 
   // The X^T product reads the FP32 window itself (and writes A16) when TMA
   // can address it: 16-byte aligned base and stride.
@@ -433,6 +617,12 @@ void tc_dense_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr, void* scratch
   if (!a32_cm && !a32_rm) {  // A16 = bf16(A_w), row-blocked, zero rows up to a multiple of 64
     StageScope st(c, ST_WINDOW);
     to_bf16_blocked(c, Aw, wr, n, A16);
+    if (fp8) {
+      const int64_t cnt = nrb * 64 * n;
+      const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((cnt + 255) / 256, c->sm_count * 8));
+      amax_a16_kernel<<<grid, 256, 0, c->stream>>>(A16, cnt, c->fp8_win);
+      SKEMA_LAUNCHED(c);
+    }
   }
   const TcSlices sl = tc_window_slices(c, R0, wr, &sp);
   {  // X^T = nu X^T + eta A_w^T Upsilon~_w^T
@@ -450,20 +640,26 @@ void tc_dense_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr, void* scratch
     const CUtensorMap ta16 = tmap_bf16_blocked(A16, (uint64_t)n, (uint64_t)nrb, 128);
     if (a32_cm) {
       const CUtensorMap ta32 = tmap_f32(Aw.p, (uint64_t)wr, (uint64_t)n, (uint64_t)Aw.cs * 4, 32, 128);
-      launch_gemm_a32<false>(c, ta32, tb, ta16, n, k, wr, pl, o);
+      launch_gemm_a32<false>(c, ta32, tb, ta16, n, k, wr, pl, o, fp8 ? c->fp8_win : nullptr);
     } else if (a32_rm) {
       const CUtensorMap ta32 = tmap_f32(Aw.p, (uint64_t)n, (uint64_t)wr, (uint64_t)Aw.rs * 4, 32, 64);
-      launch_gemm_a32<true>(c, ta32, tb, ta16, n, k, wr, pl, o);
+      launch_gemm_a32<true>(c, ta32, tb, ta16, n, k, wr, pl, o, fp8 ? c->fp8_win : nullptr);
     } else {
       launch_gemm<tc::A_KMAJ_BLK>(c, ta16, tb, n, k, wr, pl, 1, o);
     }
   }
-  {  // [Y_w | T] = A16 [Omega~; Psi~]^T
+  if (fp8) {  // A8 = e4m3(scale_A A16), row-major
+    StageScope st(c, ST_WINDOW);
+    const int64_t tiles = nrb * ((n + 63) / 64);
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(tiles, c->sm_count * 8));
+    a16_to_a8_kernel<<<grid, 256, 0, c->stream>>>(A16, wr, n, A8, ld8, c->fp8_win, c->fp8_map_scale);
+    SKEMA_LAUNCHED(c);
+  }
+  {  // [Y_w | T] = A16 [Omega~; Psi~]^T  (FP8 form: A8 op8^T, scaled back)
     StageScope st(c, ST_FUSED);
-    const CUtensorMap ta = tmap_bf16_blocked(A16, (uint64_t)n, (uint64_t)nrb, 64);
-    const CUtensorMap tb = tmap_bf16(c->op16, (uint64_t)n, (uint64_t)(k + s), (uint64_t)c->ld_op16 * 2, 64, kNT);
     const int64_t tiles = ((wr + 127) / 128) * ((k + s + kNT - 1) / kNT);
-    const Plan pl = plan_split(c, tiles, n, 8);
+    Plan pl = plan_split(c, tiles, n, 8);
+    if (fp8) pl = plan_fp8(pl, n);
     tc::OutSpec o = out_spec();
     o.p0 = c->Y + R0, o.rs0 = 1, o.cs0 = m, o.alpha0 = eta, o.beta0 = ybeta;
     o.rows = wr, o.split = k, o.ncols = k + s;
@@ -475,7 +671,17 @@ void tc_dense_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr, void* scratch
       o.atomic0 = 1, o.beta0 = 0.f;
       o.p1f = T32, o.rs1 = 1, o.cs1 = wp, o.atomic1 = 1;
     }
-    launch_gemm<tc::A_MN_BLK>(c, ta, tb, wr, k + s, n, pl, 0, o);
+    if (fp8) {
+      o.scale = reinterpret_cast<const float*>(c->fp8_win + 1);
+      const CUtensorMap ta = tmap_u8(A8, (uint64_t)n, (uint64_t)wr, (uint64_t)ld8, 128, 128);
+      const CUtensorMap tb = tmap_u8(c->op8, (uint64_t)n, (uint64_t)(k + s), (uint64_t)c->ld_op8, 128, kNT);
+      launch_gemm_fp8(c, ta, tb, wr, k + s, n, pl, o);
+    } else {
+      const CUtensorMap ta = tmap_bf16_blocked(A16, (uint64_t)n, (uint64_t)nrb, 64);
+      const CUtensorMap tb =
+          tmap_bf16(c->op16, (uint64_t)n, (uint64_t)(k + s), (uint64_t)c->ld_op16 * 2, 64, kNT);
+      launch_gemm<tc::A_MN_BLK>(c, ta, tb, wr, k + s, n, pl, 0, o);
+    }
     if (pl.ks > 1) t32_to_t16(c, T32, T16, nullptr, wr, s, wp);
   }
   y_rows_mark(c, R0, R0 + wr);

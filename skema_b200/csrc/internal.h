@@ -116,6 +116,16 @@ struct skema_ctx {
   // ld_maps16; padded row strides are multiples of 8 elements.
   void* op16 = nullptr;
   int64_t ld_op16 = 0, ld_maps16 = 0;
+  // FP8 form: the Gauss maps are held on the E4M3 grid scaled by
+  // fp8_map_scale (a power of two, so every map value is exact in FP8, BF16
+  // and FP32 alike); op8 is E4M3(fp8_map_scale [Omega~; Psi~]), (k+s) x n
+  // row-major with ld_op8 (a multiple of 16 bytes). fp8_win holds, on the
+  // device, the amax bits of the current window's A and the product scale
+  // 1 / (scale_A * fp8_map_scale) of its [Y | T] GEMM.
+  void* op8 = nullptr;
+  int64_t ld_op8 = 0;
+  float fp8_map_scale = 1.f;
+  uint32_t* fp8_win = nullptr;
   // Device status word of the bounded waits in the tensor-core kernels
   // (non-zero: a wait timed out); checked at the next synchronising call.
   int* dev_err = nullptr;

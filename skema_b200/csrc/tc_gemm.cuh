@@ -72,6 +72,9 @@ struct OutSpec {
   // row_log2w); row_log2w = 0 leaves it unweighted.
   float row_log2w;
   int64_t row_wlen, row_nwin;
+  // When set, alpha0 and alpha1 are multiplied by *scale (a device value
+  // written by an earlier launch: the FP8 form's 1 / (scale_A scale_map)).
+  const float* scale;
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -171,6 +174,21 @@ __host__ __device__ constexpr uint32_t idesc_bf16(int n, bool a_mn_major, bool b
          | ((uint32_t)(n >> 3) << 17)     // N / 8
          | ((uint32_t)(BM >> 4) << 24);   // M / 16
 }
+// Instruction descriptor: E4M3 x E4M3 -> F32 (kind::f8f6f4), both operands
+// K-major, M = 128, N = n.
+__host__ __device__ constexpr uint32_t idesc_e4m3(int n) {
+  return (1u << 4)                        // D: F32
+         | (0u << 7)                      // A: E4M3
+         | (0u << 10)                     // B: E4M3
+         | ((uint32_t)(n >> 3) << 17)     // N / 8
+         | ((uint32_t)(BM >> 4) << 24);   // M / 16
+}
+__device__ __forceinline__ void umma_f8(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n tcgen05.mma.cta_group::1.kind::f8f6f4 [%0], %1, %2, %3, p;\n}\n" ::"r"(d),
+      "l"(a), "l"(b), "r"(idesc), "r"(acc)
+      : "memory");
+}
 __device__ __forceinline__ void umma(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
   asm volatile(
       "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(d),
@@ -246,7 +264,12 @@ __device__ __forceinline__ bool epilogue_unit(const OutSpec& o, uint32_t tmem, u
   tc_fence_after();
   const int64_t row = (int64_t)mt * BM + warp * 32 + lane;
   const uint32_t taddr = tmem + acc * TCOLS + ((uint32_t)(warp * 32) << 16);
-  float alpha1 = o.alpha1;
+  float alpha0 = o.alpha0, alpha1 = o.alpha1;
+  if (o.scale) {
+    const float sc = *o.scale;
+    alpha0 *= sc;
+    alpha1 *= sc;
+  }
   if (o.row_log2w != 0.f && row < o.rows) {
     const int64_t e = o.row_nwin - 1 - row / o.row_wlen;
     if (e > 0) alpha1 *= exp2f((float)e * o.row_log2w);
@@ -273,9 +296,9 @@ __device__ __forceinline__ bool epilogue_unit(const OutSpec& o, uint32_t tmem, u
       if (col < o.split) {
         float* p = o.p0 + row * o.rs0 + col * o.cs0;
         if (o.atomic0)
-          atomicAdd(p, o.alpha0 * v[i]);
+          atomicAdd(p, alpha0 * v[i]);
         else
-          *p = (o.beta0 == 0.f) ? o.alpha0 * v[i] : fmaf(o.beta0, *p, o.alpha0 * v[i]);
+          *p = (o.beta0 == 0.f) ? alpha0 * v[i] : fmaf(o.beta0, *p, alpha0 * v[i]);
       } else {
         const int64_t cc = col - o.split;
         if (o.p1) {
@@ -433,6 +456,130 @@ __global__ void __launch_bounds__(kThreads, 1)
 }
 
 // ---------------------------------------------------------------------------
+// The FP8 form of the same GEMM: E4M3 x E4M3 -> FP32 (tcgen05 kind::f8f6f4),
+// both operands K-major from 2-D maps, 128 K-elements (one 128-byte swizzle
+// row of bytes) per stage and four MMAs of K = 32 per stage. The operand
+// scales are folded into the epilogue through OutSpec::scale.
+template <int NT, int S>
+__global__ void __launch_bounds__(kThreads, 1)
+    gemm_fp8_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, int64_t K,
+                    int64_t kchunk, Grid3 g, OutSpec o, int* err) {
+  constexpr int BK8 = 128;
+  constexpr uint32_t A_BYTES = BM * BK8;  // 16 KB
+  constexpr uint32_t B_BYTES = NT * BK8;
+  constexpr uint32_t STAGE = ((A_BYTES + B_BYTES + 1023) / 1024) * 1024;
+  constexpr uint32_t TCOLS = NT <= 32 ? 32 : NT <= 64 ? 64 : NT <= 128 ? 128 : 256;
+  static_assert(NT % 16 == 0 && NT <= 256, "N tile");
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char* smem = reinterpret_cast<unsigned char*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + S * STAGE);
+  uint64_t* empty = full + S;
+  uint64_t* tfull = empty + S;
+  uint64_t* tempty = tfull + 2;
+  uint32_t* tbase = reinterpret_cast<uint32_t*>(tempty + 2);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int total = g.mtiles * g.ntiles * g.ksplit;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < S; ++s) {
+      mbar_init(full + s, 1);
+      mbar_init(empty + s, 1);
+    }
+    for (int a = 0; a < 2; ++a) {
+      mbar_init(tfull + a, 1);
+      mbar_init(tempty + a, 4 * 32);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 5) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tbase)),
+                 "r"(2 * TCOLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tbase;
+
+  if (warp == 4 && lane == 0) {
+    uint32_t it = 0;
+    bool ok = true;
+    for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
+      int mt, nt, ks;
+      decode_unit(g, t, mt, nt, ks);
+      const int64_t k0 = (int64_t)ks * kchunk;
+      const int KT = (int)((min(K, k0 + kchunk) - k0 + BK8 - 1) / BK8);
+      for (int kt = 0; kt < KT; ++kt, ++it) {
+        const int s = it % S;
+        const uint32_t ph = (it / S) & 1;
+        if (!mbar_wait(empty + s, ph ^ 1, err)) {
+          ok = false;
+          break;
+        }
+        unsigned char* sa = smem + s * STAGE;
+        mbar_expect_tx(full + s, A_BYTES + B_BYTES);
+        const int kc = (int)(k0 + (int64_t)kt * BK8);
+        tma_load_2d(&tmA, full + s, sa, kc, mt * BM);
+        tma_load_2d(&tmB, full + s, sa + A_BYTES, kc, nt * NT);
+      }
+    }
+  } else if (warp == 5 && lane == 0) {
+    constexpr uint32_t idesc = idesc_e4m3(NT);
+    uint32_t it = 0, tcount = 0;
+    bool ok = true;
+    for (int t = blockIdx.x; t < total && ok; t += gridDim.x, ++tcount) {
+      int mt, nt, ks;
+      decode_unit(g, t, mt, nt, ks);
+      const int64_t k0 = (int64_t)ks * kchunk;
+      const int KT = (int)((min(K, k0 + kchunk) - k0 + BK8 - 1) / BK8);
+      const uint32_t acc = tcount & 1, aph = (tcount >> 1) & 1;
+      if (!mbar_wait(tempty + acc, aph ^ 1, err)) break;
+      tc_fence_after();
+      const uint32_t d = tmem + acc * TCOLS;
+      for (int kt = 0; kt < KT; ++kt, ++it) {
+        const int s = it % S;
+        const uint32_t ph = (it / S) & 1;
+        if (!mbar_wait(full + s, ph, err)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t sa = smem_u32(smem + s * STAGE);
+        const uint32_t sb = sa + A_BYTES;
+#pragma unroll
+        for (int kk = 0; kk < BK8 / 32; ++kk)
+          umma_f8(d, sdesc(sa + kk * 32, 16, 1024), sdesc(sb + kk * 32, 16, 1024), idesc,
+                  (kt > 0 || kk > 0) ? 1u : 0u);
+        umma_commit(empty + s);
+      }
+      if (ok) umma_commit(tfull + acc);
+    }
+  } else if (warp < 4) {
+    uint32_t tcount = 0;
+    for (int t = blockIdx.x; t < total; t += gridDim.x, ++tcount) {
+      int mt, nt, ks;
+      decode_unit(g, t, mt, nt, ks);
+      const uint32_t acc = tcount & 1, aph = (tcount >> 1) & 1;
+      if (!epilogue_unit<NT, TCOLS>(o, tmem, acc, aph, tfull, tempty, mt, nt, warp, lane, err)) break;
+    }
+  }
+  if ((warp == 4 || warp == 5) && lane == 0 && *(volatile int*)err) {
+    const unsigned long long t0 = now_ns();
+    while (now_ns() - t0 < 20000000ull) __nanosleep(1000);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 5) {
+    __syncwarp();
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * TCOLS) : "memory");
+  }
+}
+
+// ---------------------------------------------------------------------------
 // The same GEMM with A read as FP32 and rounded to BF16 inside the kernel,
 // for X^T = A_w^T Upsilon~_w^T straight from the FP32 window: M runs over
 // the window's columns, K over its rows. Each K step's A tile (64 window
@@ -457,7 +604,7 @@ template <int NT, int S1, int S2, bool AROW>
 __global__ void __launch_bounds__(kThreadsA32, 1)
     gemm_a32_kernel(const __grid_constant__ CUtensorMap tmA32, const __grid_constant__ CUtensorMap tmB,
                     const __grid_constant__ CUtensorMap tmA16, int64_t K, int64_t kchunk, Grid3 g, OutSpec o,
-                    int* err) {
+                    uint32_t* amax, int* err) {
   constexpr uint32_t A32_BYTES = BM * BK * 4;  // 32 KB
   constexpr uint32_t A_BYTES = BM * BK * 2;    // 16 KB
   constexpr uint32_t B_BYTES = NT * BK * 2;
@@ -584,13 +731,16 @@ __global__ void __launch_bounds__(kThreadsA32, 1)
       for (int kt = 0; kt < KT; ++kt, ++it) {
         const int s1 = it % S1, s2 = it % S2;
         const uint32_t ph1 = (it / S1) & 1, ph2 = (it / S2) & 1;
-        if (!mbar_wait(f32full + s1, ph1, err) || !mbar_wait(empty + s2, ph2 ^ 1, err)) {
+        // warp-uniform: the amax reduction below is warp-collective
+        const bool got = mbar_wait(f32full + s1, ph1, err) && mbar_wait(empty + s2, ph2 ^ 1, err);
+        if (!__all_sync(0xffffffffu, got)) {
           ok = false;
           break;
         }
         const unsigned char* a32 = st32 + s1 * A32_BYTES;
         unsigned char* dst = stbf + s2 * STAGE + ct * 128;
         const int sw = ct & 7;
+        float mx = 0.f;  // max |a| over this thread's 64 values (FP8 form's window scale)
         if (!AROW) {
           // line ct of each FP32 box holds rows 32h..32h+31 of column ct
 #pragma unroll
@@ -599,6 +749,9 @@ __global__ void __launch_bounds__(kThreadsA32, 1)
             const int c = 2 * (q & 3);
             const float4 x = *reinterpret_cast<const float4*>(src + ((c ^ sw) << 4));
             const float4 y = *reinterpret_cast<const float4*>(src + (((c + 1) ^ sw) << 4));
+            if (amax)
+              mx = fmaxf(mx, fmaxf(fmaxf(fmaxf(fabsf(x.x), fabsf(x.y)), fmaxf(fabsf(x.z), fabsf(x.w))),
+                                   fmaxf(fmaxf(fabsf(y.x), fabsf(y.y)), fmaxf(fabsf(y.z), fabsf(y.w)))));
             __nv_bfloat162 h[4] = {__floats2bfloat162_rn(x.x, x.y), __floats2bfloat162_rn(x.z, x.w),
                                    __floats2bfloat162_rn(y.x, y.y), __floats2bfloat162_rn(y.z, y.w)};
             *reinterpret_cast<uint4*>(dst + ((q ^ sw) << 4)) = *reinterpret_cast<const uint4*>(h);
@@ -614,11 +767,18 @@ __global__ void __launch_bounds__(kThreadsA32, 1)
             for (int e = 0; e < 8; ++e) {
               const int i = 8 * q + e;
               f[e] = *reinterpret_cast<const float*>(box + i * 128 + ((((jj >> 2) ^ (i & 7))) << 4) + (jj & 3) * 4);
+              if (amax) mx = fmaxf(mx, fabsf(f[e]));
             }
             __nv_bfloat162 h[4] = {__floats2bfloat162_rn(f[0], f[1]), __floats2bfloat162_rn(f[2], f[3]),
                                    __floats2bfloat162_rn(f[4], f[5]), __floats2bfloat162_rn(f[6], f[7])};
             *reinterpret_cast<uint4*>(dst + ((q ^ sw) << 4)) = *reinterpret_cast<const uint4*>(h);
           }
+        }
+        if (amax) {
+          // |a| as bits: for non-negative floats the integer order is the
+          // float order, so the window's amax is one integer atomicMax
+          const uint32_t wm = __reduce_max_sync(0xffffffffu, __float_as_uint(mx));
+          if ((ct & 31) == 0) atomicMax(amax, wm);
         }
         fence_proxy_async();
         mbar_arrive(f32empty + s1);
@@ -628,14 +788,18 @@ __global__ void __launch_bounds__(kThreadsA32, 1)
           // tile, wait until TMA has read it, then release the stage
           if (!mbar_wait(full + s2, ph2, err)) {
             ok = false;
-            break;
+          } else {
+            fence_proxy_async();
+            const int kc = (int)(k0 + (int64_t)kt * BK);
+            tma_store_3d(&tmA16, stbf + s2 * STAGE, 0, mt * BM, kc / BK);
+            bulk_commit();
+            bulk_wait_read_all();
+            mbar_arrive(empty + s2);
           }
-          fence_proxy_async();
-          const int kc = (int)(k0 + (int64_t)kt * BK);
-          tma_store_3d(&tmA16, stbf + s2 * STAGE, 0, mt * BM, kc / BK);
-          bulk_commit();
-          bulk_wait_read_all();
-          mbar_arrive(empty + s2);
+        }
+        if (!__all_sync(0xffffffffu, ok)) {
+          ok = false;
+          break;
         }
       }
     }

@@ -191,3 +191,124 @@ def test_bf16_map_import_refreshes_copies(sk, oracle):
         s.linear_update(A)
         Y0 = s.get_sketch(1)
     assert rel_fro(Y, -Y0) < 1e-6
+
+
+# ---------------------------------------------------------------- FP8 form --
+# The FP8 context holds its Gauss maps on the E4M3 grid scaled by one power of
+# two (2^floor(log2(448 / max maxval))), so the oracle takes the same maps:
+# the FP64 oracle maps rounded to FP32, scaled, rounded to E4M3 (round to
+# nearest even) and scaled back -- the map test checks that bit for bit. The
+# window is scaled by a power of two from its amax and rounded to E4M3 for
+# the [Y | T] product; X^T stays on the BF16 path. Bars (relative Frobenius
+# against the FP64 oracle with the same maps): X 6e-3 (BF16), Y and Z 4e-2
+# (one E4M3 rounding of every window entry: relative spacing 2^-3, so up to
+# 2^-4 per entry and about 2.5e-2 in the mean square).
+TOL_X8 = 6e-3
+TOL_YZ8 = 4e-2
+
+
+def fp8(a, sk):
+    a.precision = sk._lib.PREC_FP8
+    return a
+
+
+def e4m3_grid(maps):
+    """The FP8 context's version of the oracle maps (dict name -> Map)."""
+    import math
+
+    import torch
+
+    mx = max(math.sqrt(2.0 * math.log(mp.nrow * mp.ncol)) for mp in maps.values())
+    r = np.float32(448.0) / np.float32(mx)
+    e = int((np.frombuffer(np.float32(r).tobytes(), np.uint32)[0] >> 23) & 0xFF) - 127
+    sm = 2.0 ** e
+    for mp in maps.values():
+        f32 = torch.from_numpy(np.asarray(mp.dense)).float()
+        q = (f32 * sm).to(torch.float8_e4m3fn).float() / sm
+        mp._dense = q.double().numpy()
+    return sm
+
+
+def test_fp8_maps_on_the_e4m3_grid(sk, oracle):
+    m, n = 600, 300
+    a = fp8(alg(sk, m, n, 5, 100, 0), sk)
+    o = oracle_for(oracle, a)
+    e4m3_grid(o.maps)
+    with sk.SketchySVD(a) as s:
+        for which, name in ((sk._lib.UPSILON, "upsilon"), (sk._lib.OMEGA, "omega"), (sk._lib.PHI, "phi"),
+                            (sk._lib.PSI, "psi")):
+            got = s.map_export(which)[0]
+            assert np.array_equal(got, o.maps[name].dense), name
+
+
+def check8(s, o, tag=""):
+    X, Y, Z = s.get_sketches()
+    ex, ey, ez = rel_fro(X, o.X), rel_fro(Y, o.Y), rel_fro(Z, o.Z)
+    print(f"fp8 {tag}: X {ex:.2e} Y {ey:.2e} Z {ez:.2e}")
+    assert np.isfinite(X).all() and np.isfinite(Y).all() and np.isfinite(Z).all(), tag
+    assert ex < TOL_X8, (tag, "X", ex)
+    assert ey < TOL_YZ8, (tag, "Y", ey)
+    assert ez < TOL_YZ8, (tag, "Z", ez)
+
+
+@pytest.mark.parametrize("layout", ["C", "F"])
+def test_dense_fp8_parity(sk, oracle, layout):
+    m, n = 2000, 1000
+    A = dense_input(m, n).astype(np.float32)
+    A = np.asfortranarray(A) if layout == "F" else np.ascontiguousarray(A)
+    a = fp8(alg(sk, m, n, 10, 100, 0), sk)
+    o = oracle_for(oracle, a)
+    e4m3_grid(o.maps)
+    o.linear_update(A.astype(np.float64))
+    with sk.SketchySVD(a) as s:
+        s.linear_update(A)
+        check8(s, o, layout)
+
+
+def test_dense_fp8_split_k_eta_nu_two_calls(sk, oracle):
+    import torch
+
+    m, n = 4096, 3000
+    A = dense_input(m, n, seed=11).astype(np.float32)
+    a = fp8(alg(sk, m, n, 50, 2048, 0, sketch_eta=1.25, sketch_nu=0.8), sk)
+    o = oracle_for(oracle, a)
+    e4m3_grid(o.maps)
+    o.linear_update(A.astype(np.float64))
+    At = torch.from_numpy(A).cuda()
+    with sk.SketchySVD(a) as s:
+        s.update_rows(At[:2048], 0)
+        s.update_rows(At[2048:], 2048)
+        check8(s, o, "split-k")
+
+
+@pytest.mark.parametrize("n", [333, 336])
+def test_dense_fp8_ragged_window(sk, oracle, n):
+    # n = 333 row-major: the separate BF16 conversion and its amax pass
+    m = 777
+    A = np.ascontiguousarray(dense_input(m, n, seed=5).astype(np.float32))
+    a = fp8(alg(sk, m, n, 7, 129, 0, sketch_nu=0.5), sk)
+    o = oracle_for(oracle, a)
+    e4m3_grid(o.maps)
+    o.linear_update(A.astype(np.float64))
+    with sk.SketchySVD(a) as s:
+        s.linear_update(A)
+        check8(s, o, f"ragged n={n}")
+
+
+def test_dense_fp8_window_scale_tracks_amax(sk, oracle):
+    # two windows whose magnitudes differ by 2^20: each gets its own scale,
+    # so the small one keeps its relative accuracy
+    m, n = 256, 512
+    A = dense_input(m, n, seed=9).astype(np.float32)
+    A[128:] *= 2.0 ** -20
+    a = fp8(alg(sk, m, n, 5, 128, 0), sk)
+    o = oracle_for(oracle, a)
+    e4m3_grid(o.maps)
+    o.linear_update(A.astype(np.float64))
+    with sk.SketchySVD(a) as s:
+        s.linear_update(A)
+        Y = s.get_sketch(sk._lib.SKETCH_Y)
+    for r0 in (0, 128):
+        e = rel_fro(Y[r0:r0 + 128], o.Y[r0:r0 + 128])
+        print(f"fp8 window at {r0}: Y {e:.2e}")
+        assert e < TOL_YZ8, (r0, e)
