@@ -509,7 +509,14 @@ def run_gpu(args, cfg, peaks, peak_kind):
         # the two large kernels per window: [Y|T] on the tensor pipe and the X^T
         # product that streams the FP32 window (4 B read + 2 B BF16 copy written
         # per element); the one with more measured time is the roofline kernel
-        yt = tc_roof("gemm_bf16_kernel", "update.fused", 2 * m_local * n * (k + s), tc_peak, peak_kind)
+        if a.precision == 2:
+            # E4M3 [Y|T]; no FP8 peak is measured: the dense FP8 rate is twice
+            # the BF16 rate on this part, so the denominator is 2x the measured
+            # sustained BF16 figure
+            yt = tc_roof("gemm_fp8_kernel", "update.fused", 2 * m_local * n * (k + s), 2 * tc_peak,
+                         f"2 x bf16_tflops_sustained ({peak_kind}); FP8 peak not measured")
+        else:
+            yt = tc_roof("gemm_bf16_kernel", "update.fused", 2 * m_local * n * (k + s), tc_peak, peak_kind)
         xa = hbm_roof("gemm_a32_kernel", "update.upsilon", m_local * n * 6)
         xa["achieved_tflops"] = 2 * m_local * n * k * args.steps / (stage_raw["update.upsilon"][0] / 1e3) / 1e12
         first, second = (yt, xa) if stage_raw["update.fused"][0] >= stage_raw["update.upsilon"][0] else (xa, yt)

@@ -723,6 +723,7 @@ __global__ void __launch_bounds__(kThreadsA32, 1)
     const int ct = threadIdx.x - 6 * 32;  // A-tile line (window column) of this thread
     uint32_t it = 0;
     bool ok = true;
+    float mx = 0.f;  // max |a| over every value this thread converts (FP8 form's window scale)
     for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
       int mt, nt, ks;
       decode_unit(g, t, mt, nt, ks);
@@ -740,7 +741,6 @@ __global__ void __launch_bounds__(kThreadsA32, 1)
         const unsigned char* a32 = st32 + s1 * A32_BYTES;
         unsigned char* dst = stbf + s2 * STAGE + ct * 128;
         const int sw = ct & 7;
-        float mx = 0.f;  // max |a| over this thread's 64 values (FP8 form's window scale)
         if (!AROW) {
           // line ct of each FP32 box holds rows 32h..32h+31 of column ct
 #pragma unroll
@@ -774,12 +774,6 @@ __global__ void __launch_bounds__(kThreadsA32, 1)
             *reinterpret_cast<uint4*>(dst + ((q ^ sw) << 4)) = *reinterpret_cast<const uint4*>(h);
           }
         }
-        if (amax) {
-          // |a| as bits: for non-negative floats the integer order is the
-          // float order, so the window's amax is one integer atomicMax
-          const uint32_t wm = __reduce_max_sync(0xffffffffu, __float_as_uint(mx));
-          if ((ct & 31) == 0) atomicMax(amax, wm);
-        }
         fence_proxy_async();
         mbar_arrive(f32empty + s1);
         mbar_arrive(full + s2);
@@ -804,6 +798,12 @@ __global__ void __launch_bounds__(kThreadsA32, 1)
       }
     }
     if (ct == 0) bulk_wait_all();
+    if (amax) {
+      // |a| as bits: for non-negative floats the integer order is the float
+      // order, so the window's amax is one integer atomicMax per warp
+      const uint32_t wm = __reduce_max_sync(0xffffffffu, __float_as_uint(mx));
+      if ((ct & 31) == 0) atomicMax(amax, wm);
+    }
   } else if (warp < 4) {
     // ---------------- epilogue ----------------
     uint32_t tcount = 0;
