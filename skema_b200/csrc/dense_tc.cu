@@ -384,49 +384,58 @@ __global__ void amax_a16_kernel(const __nv_bfloat16* __restrict__ A16, int64_t c
 }
 
 // Row-blocked BF16 window (64-row blocks, a 128-byte line of 64 rows per
-// column) -> E4M3(scale_A a) row-major with row stride ld8 bytes, by 64 x 64
-// tiles through shared memory; scale_A from the window's amax (win[0]).
-// Block 0 also writes the [Y | T] product scale 1 / (scale_A scale_map)
-// into win[1].
+// column) -> E4M3(scale_A a) row-major with row stride ld8 bytes, by tiles
+// of 64 rows x 128 columns through shared memory: each thread loads four
+// 16-byte pieces (8 rows of one column) before converting any, the tile is
+// transposed in shared memory as bytes, and each row leaves as 16-byte
+// stores. scale_A comes from the window's amax (win[0]); block 0 also writes
+// the [Y | T] product scale 1 / (scale_A scale_map) into win[1].
 __global__ void __launch_bounds__(256)
     a16_to_a8_kernel(const __nv_bfloat16* __restrict__ A16, int64_t rows, int64_t cols, uint8_t* __restrict__ A8,
                      int64_t ld8, uint32_t* win, float smap) {
-  __shared__ uint32_t tile[64][17];  // [row][4-column group], padded
+  constexpr int TC = 128, RS = TC + 16;  // tile columns; shared row stride in bytes (16-byte aligned rows)
+  __shared__ __align__(16) uint8_t tile[64 * RS];
   const float sa = pow2_scale_for(__uint_as_float(win[0]));
   if (blockIdx.x == 0 && threadIdx.x == 0) win[1] = __float_as_uint(1.f / (sa * smap));
-  const int64_t nrb = (rows + 63) / 64, ncb = (cols + 63) / 64;
+  const int64_t nrb = (rows + 63) / 64, ncb = (cols + TC - 1) / TC;
   for (int64_t t = blockIdx.x; t < nrb * ncb; t += gridDim.x) {
-    const int64_t rb = t / ncb, j0 = (t - rb * ncb) * 64;
-    // read: column j0 + c of block rb is 64 BF16 rows (a 128-byte line);
-    // thread (c, g) converts rows 4g..4g+3 of column c
-    for (int q = threadIdx.x; q < 64 * 16; q += 256) {
-      const int c = q >> 4, g = q & 15;
-      uint32_t packed = 0;
-      if (j0 + c < cols) {
-        const uint2 w = *reinterpret_cast<const uint2*>(A16 + (rb * cols + j0 + c) * 64 + 4 * g);
-        const __nv_bfloat162 p0 = *reinterpret_cast<const __nv_bfloat162*>(&w.x);
-        const __nv_bfloat162 p1 = *reinterpret_cast<const __nv_bfloat162*>(&w.y);
-        const float v[4] = {__low2float(p0), __high2float(p0), __low2float(p1), __high2float(p1)};
+    const int64_t rb = t / ncb, j0 = (t - rb * ncb) * TC;
+    // piece q = (column c, row group g): 8 consecutive rows (16 bytes) of a
+    // column line; eight consecutive threads cover one 128-byte line
+    uint4 w[4];
 #pragma unroll
-        for (int e = 0; e < 4; ++e) packed |= (uint32_t)to_e4m3(v[e] * sa) << (8 * e);
-      }
-      // bytes of rows 4g..4g+3 in column c: scatter into the row-major tile
+    for (int u = 0; u < 4; ++u) {
+      const int q = threadIdx.x + 256 * u, c = q >> 3, g = q & 7;
+      w[u] = make_uint4(0u, 0u, 0u, 0u);
+      if (j0 + c < cols) w[u] = *reinterpret_cast<const uint4*>(A16 + (rb * cols + j0 + c) * 64 + 8 * g);
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int q = threadIdx.x + 256 * u, c = q >> 3, g = q & 7;
+      const uint32_t h[4] = {w[u].x, w[u].y, w[u].z, w[u].w};
 #pragma unroll
       for (int e = 0; e < 4; ++e) {
-        uint8_t* row = reinterpret_cast<uint8_t*>(&tile[4 * g + e][0]);
-        row[c] = (uint8_t)(packed >> (8 * e));
+        const __nv_bfloat162 p = *reinterpret_cast<const __nv_bfloat162*>(&h[e]);
+        tile[(8 * g + 2 * e) * RS + c] = to_e4m3(__low2float(p) * sa);
+        tile[(8 * g + 2 * e + 1) * RS + c] = to_e4m3(__high2float(p) * sa);
       }
     }
     __syncthreads();
-    // write: row r of the tile is 64 bytes, 16 words
-    for (int q = threadIdx.x; q < 64 * 16; q += 256) {
-      const int r = q >> 4, w = q & 15;
-      const int64_t i = rb * 64 + r, j = j0 + 4 * w;
+    // row r of the tile: TC bytes as TC / 16 pieces of 16 bytes
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      const int q = threadIdx.x + 256 * u, r = q >> 3, pc = q & 7;
+      const int64_t i = rb * 64 + r, j = j0 + 16 * pc;
       if (i < rows && j < cols) {
-        if (j + 4 <= cols) {
-          *reinterpret_cast<uint32_t*>(A8 + i * ld8 + j) = tile[r][w];
+        const uint4 v = *reinterpret_cast<const uint4*>(tile + r * RS + 16 * pc);
+        uint8_t* dst = A8 + i * ld8 + j;
+        if (j + 16 <= cols) {
+          *reinterpret_cast<uint4*>(dst) = v;
         } else {
-          for (int e = 0; e < 4 && j + e < cols; ++e) A8[i * ld8 + j + e] = (uint8_t)(tile[r][w] >> (8 * e));
+          const uint32_t vw[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+          for (int e = 0; e < 16; ++e)
+            if (j + e < cols) dst[e] = (uint8_t)(vw[e >> 2] >> (8 * (e & 3)));
         }
       }
     }
@@ -650,8 +659,8 @@ void tc_dense_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr, void* scratch
   }
   if (fp8) {  // A8 = e4m3(scale_A A16), row-major
     StageScope st(c, ST_WINDOW);
-    const int64_t tiles = nrb * ((n + 63) / 64);
-    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(tiles, c->sm_count * 8));
+    const int64_t tiles = nrb * ((n + 127) / 128);
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(tiles, c->sm_count * 16));
     a16_to_a8_kernel<<<grid, 256, 0, c->stream>>>(A16, wr, n, A8, ld8, c->fp8_win, c->fp8_map_scale);
     SKEMA_LAUNCHED(c);
   }
