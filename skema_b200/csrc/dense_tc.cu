@@ -385,40 +385,48 @@ __global__ void amax_a16_kernel(const __nv_bfloat16* __restrict__ A16, int64_t c
 
 // Row-blocked BF16 window (64-row blocks, a 128-byte line of 64 rows per
 // column) -> E4M3(scale_A a) row-major with row stride ld8 bytes, by tiles
-// of 64 rows x 128 columns through shared memory: each thread loads four
-// 16-byte pieces (8 rows of one column) before converting any, the tile is
-// transposed in shared memory as bytes, and each row leaves as 16-byte
-// stores. scale_A comes from the window's amax (win[0]); block 0 also writes
-// the [Y | T] product scale 1 / (scale_A scale_map) into win[1].
+// of 64 rows x 128 columns through shared memory. A thread takes 4 x 4
+// blocks (4 rows of 4 columns: four 8-byte loads, sixteen lanes covering one
+// column line), converts them and stores each block row as one 32-bit word
+// of the row-major tile; rows then leave as 16-byte stores. scale_A comes
+// from the window's amax (win[0]); block 0 also writes the [Y | T] product
+// scale 1 / (scale_A scale_map) into win[1].
 __global__ void __launch_bounds__(256)
     a16_to_a8_kernel(const __nv_bfloat16* __restrict__ A16, int64_t rows, int64_t cols, uint8_t* __restrict__ A8,
                      int64_t ld8, uint32_t* win, float smap) {
-  constexpr int TC = 128, RS = TC + 16;  // tile columns; shared row stride in bytes (16-byte aligned rows)
+  constexpr int TC = 128, RS = TC + 16;  // tile columns; shared row stride in bytes
   __shared__ __align__(16) uint8_t tile[64 * RS];
   const float sa = pow2_scale_for(__uint_as_float(win[0]));
   if (blockIdx.x == 0 && threadIdx.x == 0) win[1] = __float_as_uint(1.f / (sa * smap));
   const int64_t nrb = (rows + 63) / 64, ncb = (cols + TC - 1) / TC;
   for (int64_t t = blockIdx.x; t < nrb * ncb; t += gridDim.x) {
     const int64_t rb = t / ncb, j0 = (t - rb * ncb) * TC;
-    // piece q = (column c, row group g): 8 consecutive rows (16 bytes) of a
-    // column line; eight consecutive threads cover one 128-byte line
-    uint4 w[4];
+    uint2 w[2][4];
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const int q = threadIdx.x + 256 * u, c = q >> 3, g = q & 7;
-      w[u] = make_uint4(0u, 0u, 0u, 0u);
-      if (j0 + c < cols) w[u] = *reinterpret_cast<const uint4*>(A16 + (rb * cols + j0 + c) * 64 + 8 * g);
+    for (int v = 0; v < 2; ++v) {
+      const int b = threadIdx.x + 256 * v, g = b & 15, cq = b >> 4;  // rows 4g.., columns 4cq..
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int64_t col = j0 + 4 * cq + j;
+        w[v][j] = make_uint2(0u, 0u);
+        if (col < cols) w[v][j] = *reinterpret_cast<const uint2*>(A16 + (rb * cols + col) * 64 + 4 * g);
+      }
     }
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const int q = threadIdx.x + 256 * u, c = q >> 3, g = q & 7;
-      const uint32_t h[4] = {w[u].x, w[u].y, w[u].z, w[u].w};
+    for (int v = 0; v < 2; ++v) {
+      const int b = threadIdx.x + 256 * v, g = b & 15, cq = b >> 4;
+      uint32_t row[4] = {0u, 0u, 0u, 0u};
 #pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        const __nv_bfloat162 p = *reinterpret_cast<const __nv_bfloat162*>(&h[e]);
-        tile[(8 * g + 2 * e) * RS + c] = to_e4m3(__low2float(p) * sa);
-        tile[(8 * g + 2 * e + 1) * RS + c] = to_e4m3(__high2float(p) * sa);
+      for (int j = 0; j < 4; ++j) {
+        const __nv_bfloat162 lo = *reinterpret_cast<const __nv_bfloat162*>(&w[v][j].x);  // rows 4g, 4g+1
+        const __nv_bfloat162 hi = *reinterpret_cast<const __nv_bfloat162*>(&w[v][j].y);  // rows 4g+2, 4g+3
+        row[0] |= (uint32_t)to_e4m3(__low2float(lo) * sa) << (8 * j);
+        row[1] |= (uint32_t)to_e4m3(__high2float(lo) * sa) << (8 * j);
+        row[2] |= (uint32_t)to_e4m3(__low2float(hi) * sa) << (8 * j);
+        row[3] |= (uint32_t)to_e4m3(__high2float(hi) * sa) << (8 * j);
       }
+#pragma unroll
+      for (int e = 0; e < 4; ++e) *reinterpret_cast<uint32_t*>(tile + (4 * g + e) * RS + 4 * cq) = row[e];
     }
     __syncthreads();
     // row r of the tile: TC bytes as TC / 16 pieces of 16 bytes

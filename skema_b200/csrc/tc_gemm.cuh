@@ -732,9 +732,7 @@ __global__ void __launch_bounds__(kThreadsA32, 1)
       for (int kt = 0; kt < KT; ++kt, ++it) {
         const int s1 = it % S1, s2 = it % S2;
         const uint32_t ph1 = (it / S1) & 1, ph2 = (it / S2) & 1;
-        // warp-uniform: the amax reduction below is warp-collective
-        const bool got = mbar_wait(f32full + s1, ph1, err) && mbar_wait(empty + s2, ph2 ^ 1, err);
-        if (!__all_sync(0xffffffffu, got)) {
+        if (!mbar_wait(f32full + s1, ph1, err) || !mbar_wait(empty + s2, ph2 ^ 1, err)) {
           ok = false;
           break;
         }
@@ -782,25 +780,23 @@ __global__ void __launch_bounds__(kThreadsA32, 1)
           // tile, wait until TMA has read it, then release the stage
           if (!mbar_wait(full + s2, ph2, err)) {
             ok = false;
-          } else {
-            fence_proxy_async();
-            const int kc = (int)(k0 + (int64_t)kt * BK);
-            tma_store_3d(&tmA16, stbf + s2 * STAGE, 0, mt * BM, kc / BK);
-            bulk_commit();
-            bulk_wait_read_all();
-            mbar_arrive(empty + s2);
+            break;
           }
-        }
-        if (!__all_sync(0xffffffffu, ok)) {
-          ok = false;
-          break;
+          fence_proxy_async();
+          const int kc = (int)(k0 + (int64_t)kt * BK);
+          tma_store_3d(&tmA16, stbf + s2 * STAGE, 0, mt * BM, kc / BK);
+          bulk_commit();
+          bulk_wait_read_all();
+          mbar_arrive(empty + s2);
         }
       }
     }
     if (ct == 0) bulk_wait_all();
     if (amax) {
       // |a| as bits: for non-negative floats the integer order is the float
-      // order, so the window's amax is one integer atomicMax per warp
+      // order, so the window's amax is one integer atomicMax per warp. Every
+      // lane leaves the loop above (the waits are bounded), so the whole
+      // warp meets here.
       const uint32_t wm = __reduce_max_sync(0xffffffffu, __float_as_uint(mx));
       if ((ct & 31) == 0) atomicMax(amax, wm);
     }
