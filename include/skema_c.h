@@ -154,6 +154,33 @@ int skema_linear_update_rbf(skema_ctx* ctx, const float* pts, int64_t ld,
 int skema_low_rank_approx(skema_ctx* ctx, double* U, double* S, double* V,
                           int32_t mem);
 
+/* Residual norms of a fixed-rank approximation: SketchySVD::compute_residuals
+ * (src/Skema_SketchySVD.cpp:719-727) with Skema::residuals and
+ * map_A_by_window (src/Skema_Residuals.hpp:58-110, 160-217):
+ *   rnorm_j = || [ (A^T U - V S)(:, j) ; (A V - U S)(:, j) ] ||_2,  j < rank.
+ * A is streamed a second time, in the same forms as the sketch update:
+ *   skema_residuals_begin(ctx, U, S, V, mem)   U (m x rank), S (rank),
+ *       V (n x rank), column-major, as returned by skema_low_rank_approx
+ *   skema_residuals_update_dense / _csr / _rbf(...)   arguments exactly as
+ *       skema_linear_update_dense / _csr / _rbf; rows in any order, each row
+ *       once; the sketches are not touched
+ *   skema_residuals_finish(ctx, rnorms, mem)   rank doubles; closes the pass.
+ * SketchySPD contexts take the one-sided form ||(A V - V S)(:, j)||_2
+ * (src/Skema_Residuals.hpp:112-158); U may then be NULL. FP64 arithmetic.
+ * An update or finish without an open pass fails with SKEMA_ESTATE. */
+int skema_residuals_begin(skema_ctx* ctx, const double* U, const double* S,
+                          const double* V, int32_t mem);
+int skema_residuals_update_dense(skema_ctx* ctx, const float* A, int64_t ld,
+                                 int32_t layout, int64_t row0, int64_t nrows,
+                                 int32_t mem);
+int skema_residuals_update_csr(skema_ctx* ctx, const int64_t* rowptr,
+                               const int32_t* col, const float* val,
+                               int64_t row0, int64_t nrows, int32_t mem);
+int skema_residuals_update_rbf(skema_ctx* ctx, const float* pts, int64_t ld,
+                               int32_t layout, int64_t npts, int64_t d,
+                               int64_t row0, int64_t nrows, int32_t mem);
+int skema_residuals_finish(skema_ctx* ctx, double* rnorms, int32_t mem);
+
 /* Copy one sketch out of / into the context (the reference only exposes them
  * through its debug dumps, src/Skema_SketchySVD.cpp:192-206, 235-245).
  * X is k x n, Y is m x k, Z is s x s; `layout` is the layout of buf. */

@@ -295,6 +295,29 @@ class OracleSketch:
         return (Q @ Uc)[:, :r], S[:r], (P @ Vt.T)[:, :r]
 
 
+def residuals(A, U, S, V, window=None):
+    """Residual norms of src/Skema_Residuals.hpp:160-217 (two-sided, with
+    map_A_by_window :58-110): per column j,
+    ||[(A^T U - V S)(:, j); (A V - U S)(:, j)]||_2, A^T U accumulated window
+    by window as the reference does. A: dense (m x n) FP64 array or scipy CSR.
+    U None: the SketchySPD form ||(A V - V S)(:, j)||_2 (:112-158)."""
+    m = A.shape[0]
+    w = m if window is None else window
+    S = np.asarray(S, dtype=np.float64)
+    AV = np.zeros((m, V.shape[1]))
+    AtU = np.zeros((A.shape[1], V.shape[1])) if U is not None else None
+    for r0 in range(0, m, w):
+        Aw = A[r0:r0 + w]
+        AV[r0:r0 + w] = Aw @ V
+        if U is not None:
+            AtU += Aw.T @ U[r0:r0 + w]
+    if U is None:
+        return np.linalg.norm(AV - V * S, axis=0)
+    d1 = AtU - V * S
+    d2 = AV - U * S
+    return np.sqrt((d1 ** 2).sum(0) + (d2 ** 2).sum(0))
+
+
 def _dgels(A, B):
     """LAPACK dgels on a square A (the reference's linalg::ls)."""
     from scipy.linalg import lapack

@@ -76,6 +76,11 @@ SIGNATURES = {
     "skema_linear_update_csr": (C.c_int, [_P, _P, _P, _P, _I64, _I64, _I32]),
     "skema_linear_update_rbf": (C.c_int, [_P, _P, _I64, _I32, _I64, _I64, _I64, _I64, _I32]),
     "skema_low_rank_approx": (C.c_int, [_P, _P, _P, _P, _I32]),
+    "skema_residuals_begin": (C.c_int, [_P, _P, _P, _P, _I32]),
+    "skema_residuals_update_dense": (C.c_int, [_P, _P, _I64, _I32, _I64, _I64, _I32]),
+    "skema_residuals_update_csr": (C.c_int, [_P, _P, _P, _P, _I64, _I64, _I32]),
+    "skema_residuals_update_rbf": (C.c_int, [_P, _P, _I64, _I32, _I64, _I64, _I64, _I64, _I32]),
+    "skema_residuals_finish": (C.c_int, [_P, _P, _I32]),
     "skema_get_sketch": (C.c_int, [_P, _I32, _P, _I64, _I32, _I32]),
     "skema_set_sketch": (C.c_int, [_P, _I32, _P, _I64, _I32, _I32]),
     "skema_map_info": (C.c_int, [_P, _I32, C.POINTER(_I64), C.POINTER(_I64), C.POINTER(_I32), C.POINTER(_I32)]),

@@ -475,6 +475,12 @@ void apply_map(skema_ctx* c, const Map& mp, const double* Qm, int64_t cols, int6
 
 }  // namespace
 
+void dgemm_f32_f64(skema_ctx* c, int64_t M, int64_t N, int64_t K, double alpha, const float* A, int64_t ars,
+                   int64_t acs, const double* B, int64_t brs, int64_t bcs, double beta, double* C, int64_t crs,
+                   int64_t ccs) {
+  dgemm<float, double>(c, M, N, K, alpha, A, ars, acs, B, brs, bcs, beta, C, crs, ccs);
+}
+
 void low_rank_approx(skema_ctx* c, double* Uout, double* Sout, double* Vout) {
   const int64_t m = c->m, n = c->n, k = c->k, s = c->s, r = c->p.rank;
   y_materialize(c);

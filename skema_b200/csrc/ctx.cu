@@ -172,6 +172,7 @@ static void free_all(skema_ctx* c) {
   if (c->ws) cudaFree(c->ws);
   if (c->stage) cudaFree(c->stage);
   if (c->op16) cudaFree(c->op16);
+  residual_free(c);
   if (c->op8) cudaFree(c->op8);
   if (c->fp8_win) cudaFree(c->fp8_win);
   if (c->dev_err) cudaFree(c->dev_err);
@@ -520,6 +521,83 @@ int skema_low_rank_approx(skema_ctx* c, double* U, double* S, double* V, int32_t
     if (U) SKEMA_CUDA(cudaMemcpyAsync(U, dU, ub, cudaMemcpyDeviceToHost, c->stream));
     if (V) SKEMA_CUDA(cudaMemcpyAsync(V, dV, vb, cudaMemcpyDeviceToHost, c->stream));
     if (S) SKEMA_CUDA(cudaMemcpyAsync(S, dS, sizeof(double) * (size_t)r, cudaMemcpyDeviceToHost, c->stream));
+    SKEMA_CUDA(cudaStreamSynchronize(c->stream));
+  });
+}
+
+// ---- residual pass ----------------------------------------------------------
+int skema_residuals_begin(skema_ctx* c, const double* U, const double* S, const double* V, int32_t mem) {
+  return guarded(c, [&] {
+    if (mem != SKEMA_MEM_DEVICE && mem != SKEMA_MEM_HOST) fail(SKEMA_EINVAL, "bad mem kind");
+    if (!S || !V || (!c->spd && !U)) fail(SKEMA_EINVAL, "null U, S or V");
+    const int64_t r = c->p.rank;
+    if (mem == SKEMA_MEM_DEVICE) {
+      residual_begin(c, U, S, V);
+      return;
+    }
+    const size_t ub = c->spd ? 0 : sizeof(double) * (size_t)(c->m * r);
+    const size_t vb = sizeof(double) * (size_t)(c->n * r), sb = sizeof(double) * (size_t)r;
+    const size_t up = (ub + 255) / 256 * 256, vp = (vb + 255) / 256 * 256;
+    char* buf = (char*)staging(c, up + vp + sb + 256);
+    double* dU = (double*)buf;
+    double* dV = (double*)(buf + up);
+    double* dS = (double*)(buf + up + vp);
+    if (!c->spd) SKEMA_CUDA(cudaMemcpyAsync(dU, U, ub, cudaMemcpyHostToDevice, c->stream));
+    SKEMA_CUDA(cudaMemcpyAsync(dV, V, vb, cudaMemcpyHostToDevice, c->stream));
+    SKEMA_CUDA(cudaMemcpyAsync(dS, S, sb, cudaMemcpyHostToDevice, c->stream));
+    residual_begin(c, dU, dS, dV);
+    // the staging buffer is reused by the next host-input call
+    SKEMA_CUDA(cudaStreamSynchronize(c->stream));
+  });
+}
+
+namespace {
+// Routes the update entry points to the residual pass for one call.
+struct ResidualRoute {
+  skema_ctx* c;
+  explicit ResidualRoute(skema_ctx* cc) : c(cc) { c->residual_pass = true; }
+  ~ResidualRoute() { c->residual_pass = false; }
+};
+int no_pass(skema_ctx* c) {
+  return guarded(c, [&] { fail(SKEMA_ESTATE, "no residual pass open: call skema_residuals_begin first"); });
+}
+}  // namespace
+
+int skema_residuals_update_dense(skema_ctx* c, const float* A, int64_t ld, int32_t layout, int64_t row0,
+                                 int64_t nrows, int32_t mem) {
+  if (!c || !c->res_ready) return c ? no_pass(c) : SKEMA_EINVAL;
+  ResidualRoute route(c);
+  return skema_linear_update_dense(c, A, ld, layout, row0, nrows, mem);
+}
+
+int skema_residuals_update_csr(skema_ctx* c, const int64_t* rowptr, const int32_t* col, const float* val,
+                               int64_t row0, int64_t nrows, int32_t mem) {
+  if (!c || !c->res_ready) return c ? no_pass(c) : SKEMA_EINVAL;
+  ResidualRoute route(c);
+  return skema_linear_update_csr(c, rowptr, col, val, row0, nrows, mem);
+}
+
+int skema_residuals_update_rbf(skema_ctx* c, const float* pts, int64_t ld, int32_t layout, int64_t npts, int64_t d,
+                               int64_t row0, int64_t nrows, int32_t mem) {
+  if (!c || !c->res_ready) return c ? no_pass(c) : SKEMA_EINVAL;
+  ResidualRoute route(c);
+  return skema_linear_update_rbf(c, pts, ld, layout, npts, d, row0, nrows, mem);
+}
+
+int skema_residuals_finish(skema_ctx* c, double* rnorms, int32_t mem) {
+  return guarded(c, [&] {
+    if (mem != SKEMA_MEM_DEVICE && mem != SKEMA_MEM_HOST) fail(SKEMA_EINVAL, "bad mem kind");
+    if (!rnorms) fail(SKEMA_EINVAL, "null rnorms");
+    if (!c->res_ready) fail(SKEMA_ESTATE, "no residual pass open: call skema_residuals_begin first");
+    check_device_error(c);
+    const int64_t r = c->p.rank;
+    if (mem == SKEMA_MEM_DEVICE) {
+      residual_finish(c, rnorms);
+      return;
+    }
+    double* d = (double*)staging(c, sizeof(double) * (size_t)r + 256);
+    residual_finish(c, d);
+    SKEMA_CUDA(cudaMemcpyAsync(rnorms, d, sizeof(double) * (size_t)r, cudaMemcpyDeviceToHost, c->stream));
     SKEMA_CUDA(cudaStreamSynchronize(c->stream));
   });
 }

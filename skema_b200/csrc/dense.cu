@@ -94,6 +94,10 @@ size_t dense_scratch_bytes(const skema_ctx* c, int64_t wr) {
 }
 
 void dense_update(skema_ctx* c, Mat A, int64_t row0, int64_t nrows) {
+  if (c->residual_pass) {
+    residual_dense(c, A, row0, nrows);
+    return;
+  }
   const int64_t W = c->w;
   float* T = (float*)workspace(c, dense_scratch_bytes(c, std::min(W, nrows)));
   for (int64_t r = 0; r < nrows; r += W) {

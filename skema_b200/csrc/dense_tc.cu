@@ -311,7 +311,7 @@ void launch_gemm_a32(skema_ctx* c, const CUtensorMap& ta32, const CUtensorMap& t
   constexpr int S1 = 3, S2 = 3;
   constexpr uint32_t STAGE = ((tc::BM * tc::BK * 2 + kNT * tc::BK * 2 + 1023) / 1024) * 1024;
   const size_t smem = (size_t)S1 * tc::BM * tc::BK * 4 + (size_t)S2 * STAGE + 1024 + 256;
-  auto kern = tc::gemm_a32_kernel<kNT, S1, S2, AROW>;
+  auto kern = amax ? tc::gemm_a32_kernel<kNT, S1, S2, AROW, true> : tc::gemm_a32_kernel<kNT, S1, S2, AROW, false>;
   SKEMA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   tc::Grid3 g;
   g.mtiles = (int)((M + tc::BM - 1) / tc::BM);

@@ -126,6 +126,18 @@ struct skema_ctx {
   int64_t ld_op8 = 0;
   float fp8_map_scale = 1.f;
   uint32_t* fp8_win = nullptr;
+  // Residual pass (skema_residuals_*): the approximation's U and V as
+  // row-major FP64 copies (m x r, n x r), S, the accumulated A^T U (n x r,
+  // row-major) and the per-column sums of squares of A V - U S. While
+  // residual_pass is set, the update entry points feed the residual pass
+  // instead of the sketches.
+  double* res_U = nullptr;
+  double* res_V = nullptr;
+  double* res_S = nullptr;
+  double* res_AtU = nullptr;
+  double* res_sq = nullptr;
+  bool res_ready = false;
+  bool residual_pass = false;
   // Device status word of the bounded waits in the tensor-core kernels
   // (non-zero: a wait timed out); checked at the next synchronising call.
   int* dev_err = nullptr;
@@ -234,5 +246,20 @@ void rbf_vjp(skema_ctx* c, const float* pts, int64_t N, int64_t d,
 
 // ---- FP64 approximation (approx.cu) ----
 void low_rank_approx(skema_ctx* c, double* U, double* S, double* V);
+// C = alpha A B + beta C in FP64 (A FP32, exact in FP64), strided operands.
+void dgemm_f32_f64(skema_ctx* c, int64_t M, int64_t N, int64_t K, double alpha, const float* A, int64_t ars,
+                   int64_t acs, const double* B, int64_t brs, int64_t bcs, double beta, double* C, int64_t crs,
+                   int64_t ccs);
+
+// ---- residual norms (residuals.cu) ----
+// U (m x r), S (r), V (n x r) column-major, device pointers.
+void residual_begin(skema_ctx* c, const double* U, const double* S, const double* V);
+void residual_dense(skema_ctx* c, Mat A, int64_t row0, int64_t nrows);
+void residual_csr(skema_ctx* c, const int64_t* rowptr, const int32_t* col, const float* val, int64_t col_offset,
+                  int64_t row0, int64_t nrows);
+void residual_rbf(skema_ctx* c, Mat P, int64_t npts, int64_t d, int64_t row0, int64_t nrows);
+// rnorms (r doubles, device pointer).
+void residual_finish(skema_ctx* c, double* rnorms);
+void residual_free(skema_ctx* c);
 
 }  // namespace skema

@@ -175,6 +175,10 @@ void rbf_window_block(skema_ctx* c, Mat P, int64_t N, int64_t d, float gamma, in
 }
 
 void rbf_update(skema_ctx* c, Mat P, int64_t npts, int64_t d, int64_t row0, int64_t nrows) {
+  if (c->residual_pass) {
+    residual_rbf(c, P, npts, d, row0, nrows);
+    return;
+  }
   if (!c->spd && c->p.precision == SKEMA_PREC_BF16 && rbf_tc_supported(c, d)) {
     // tensor-core form: kernel tiles regenerated inside the sketch kernels
     rbf_tc_update(c, P, npts, d, row0, nrows);

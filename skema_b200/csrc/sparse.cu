@@ -447,6 +447,10 @@ static void launch_csr_ssign_y(skema_ctx* c, const int64_t* rowptr, const int32_
 // ---------------------------------------------------------------------------
 void csr_update(skema_ctx* c, const int64_t* rowptr, const int32_t* col, const float* val,
                 int64_t col_offset, int64_t row0, int64_t nrows) {
+  if (c->residual_pass) {
+    residual_csr(c, rowptr, col, val, col_offset, row0, nrows);
+    return;
+  }
   const float eta = (float)c->p.sketch_eta, nu = (float)c->p.sketch_nu;
   const int64_t W = c->w;
   const int64_t nwin = (nrows + W - 1) / W;

@@ -600,7 +600,7 @@ __global__ void __launch_bounds__(kThreads, 1)
 // A tile has read it.
 constexpr int kThreadsA32 = 320;
 
-template <int NT, int S1, int S2, bool AROW>
+template <int NT, int S1, int S2, bool AROW, bool AMAX>
 __global__ void __launch_bounds__(kThreadsA32, 1)
     gemm_a32_kernel(const __grid_constant__ CUtensorMap tmA32, const __grid_constant__ CUtensorMap tmB,
                     const __grid_constant__ CUtensorMap tmA16, int64_t K, int64_t kchunk, Grid3 g, OutSpec o,
@@ -747,7 +747,7 @@ __global__ void __launch_bounds__(kThreadsA32, 1)
             const int c = 2 * (q & 3);
             const float4 x = *reinterpret_cast<const float4*>(src + ((c ^ sw) << 4));
             const float4 y = *reinterpret_cast<const float4*>(src + (((c + 1) ^ sw) << 4));
-            if (amax)
+            if (AMAX)
               mx = fmaxf(mx, fmaxf(fmaxf(fmaxf(fabsf(x.x), fabsf(x.y)), fmaxf(fabsf(x.z), fabsf(x.w))),
                                    fmaxf(fmaxf(fabsf(y.x), fabsf(y.y)), fmaxf(fabsf(y.z), fabsf(y.w)))));
             __nv_bfloat162 h[4] = {__floats2bfloat162_rn(x.x, x.y), __floats2bfloat162_rn(x.z, x.w),
@@ -765,7 +765,7 @@ __global__ void __launch_bounds__(kThreadsA32, 1)
             for (int e = 0; e < 8; ++e) {
               const int i = 8 * q + e;
               f[e] = *reinterpret_cast<const float*>(box + i * 128 + ((((jj >> 2) ^ (i & 7))) << 4) + (jj & 3) * 4);
-              if (amax) mx = fmaxf(mx, fabsf(f[e]));
+              if (AMAX) mx = fmaxf(mx, fabsf(f[e]));
             }
             __nv_bfloat162 h[4] = {__floats2bfloat162_rn(f[0], f[1]), __floats2bfloat162_rn(f[2], f[3]),
                                    __floats2bfloat162_rn(f[4], f[5]), __floats2bfloat162_rn(f[6], f[7])};
@@ -792,7 +792,7 @@ __global__ void __launch_bounds__(kThreadsA32, 1)
       }
     }
     if (ct == 0) bulk_wait_all();
-    if (amax) {
+    if (AMAX) {
       // |a| as bits: for non-negative floats the integer order is the float
       // order, so the window's amax is one integer atomicMax per warp. Every
       // lane leaves the loop above (the waits are bounded), so the whole

@@ -378,22 +378,81 @@ class _Context:
 
     def update_rows(self, A, row0: int = 0, nrows: int | None = None):
         """Stream rows [row0, row0+nrows) (default: all rows of A)."""
+        self._stream(A, row0, nrows, "skema_linear_update")
+
+    def _stream(self, A, row0, nrows, prefix):
         if self.alg.kernel_func == L.KERNEL_GAUSSRBF:
             ptr, ld, layout, mem, keep = _dense_arg(A)
             npts, d = A.shape
             nr = self.nrow - row0 if nrows is None else nrows
-            self._check(self.lib.skema_linear_update_rbf(self.h, ptr, ld, layout, npts, d, row0, nr, mem))
+            self._check(getattr(self.lib, prefix + "_rbf")(self.h, ptr, ld, layout, npts, d, row0, nr, mem))
         elif self.alg.issparse:
             rp, col, val, nr_in, _, mem, keep = _csr_arg(A)
             nr = nr_in if nrows is None else nrows
-            self._check(self.lib.skema_linear_update_csr(self.h, rp, col, val, row0, nr, mem))
+            self._check(getattr(self.lib, prefix + "_csr")(self.h, rp, col, val, row0, nr, mem))
         else:
             ptr, ld, layout, mem, keep = _dense_arg(A)
             nr = A.shape[0] if nrows is None else nrows
-            self._check(self.lib.skema_linear_update_dense(self.h, ptr, ld, layout, row0, nr, mem))
+            self._check(getattr(self.lib, prefix + "_dense")(self.h, ptr, ld, layout, row0, nr, mem))
         if mem == L.MEM_HOST:
             self.synchronize()
         del keep
+
+    # -- residuals --------------------------------------------------------
+    def residuals(self, A, U, S, V, row_blocks=None):
+        """Skema::residuals (src/Skema_Residuals.hpp:160-217): per-column
+        ||[A^T U - V S; A V - U S]||_2 (SketchySPD: ||A V - V S||_2) for host
+        FP64 U (m x r), S (r), V (n x r); A streamed again like the update.
+        row_blocks: optional list of (row0, A_block) pairs instead of A."""
+        Uc = None if U is None else np.asfortranarray(np.asarray(U, dtype=np.float64))
+        Sc = np.ascontiguousarray(np.asarray(S, dtype=np.float64))
+        Vc = np.asfortranarray(np.asarray(V, dtype=np.float64))
+        self._check(self.lib.skema_residuals_begin(self.h, None if Uc is None else Uc.ctypes.data, Sc.ctypes.data,
+                                                   Vc.ctypes.data, L.MEM_HOST))
+        for row0, blk in (row_blocks if row_blocks is not None else [(0, A)]):
+            self._stream(blk, row0, None, "skema_residuals_update")
+        out = np.empty(self.rank, dtype=np.float64)
+        self._check(self.lib.skema_residuals_finish(self.h, out.ctypes.data, L.MEM_HOST))
+        return out
+
+    def compute_residuals(self, A):
+        """SketchySVD::compute_residuals (src/Skema_SketchySVD.cpp:719-727):
+        residual norms of the last low_rank_approx, kept as self.rnrms."""
+        if getattr(self, "uvecs", None) is None:
+            raise SkemaError(L.ESTATE, "compute_residuals needs a low_rank_approx first")
+        self.rnrms = self.residuals(A, self.uvecs, self.svals, self.vvecs)
+        return self.rnrms
+
+    def save_history(self, path=None):
+        """SketchySVD::save_history (src/Skema_SketchySVD.cpp:730-755): a JSON
+        object with "timings", "traces", "svals" and "rnrms", written with a
+        4-space indent to `path`, or returned as a string when path is None.
+        Timings hold this build's stage timers (milliseconds, when timing is
+        on) under the reference's keys; traces stay empty (no per-window
+        singular-value traces are taken)."""
+        import json
+
+        upd = {}
+        for key, stage in (("upsilon", "update.upsilon"), ("omega", "update.omega"), ("phi", "update.phi"),
+                           ("psi", "update.psi"), ("window", "update.window"), ("daxpy", "update.daxpy")):
+            try:
+                upd[key] = self.timing_get(stage)[0] / 1e3
+            except SkemaError:
+                upd[key] = 0.0
+        timings = {"init": {k: 0.0 for k in ("upsilon", "omega", "phi", "psi")}, "update": upd,
+                   "approx": {k: 0.0 for k in ("phi", "psi", "dgeqrf", "dgemm", "dgels", "dgesvd")}}
+        r = self.rank
+        sv = getattr(self, "svals", None)
+        rn = getattr(self, "rnrms", None)
+        hist = {"timings": timings, "traces": {},
+                "svals": [float(x) for x in (sv if sv is not None else np.zeros(r))],
+                "rnrms": [float(x) for x in (rn if rn is not None else np.zeros(r))]}
+        text = json.dumps(hist, indent=4)
+        if path is None:
+            return text
+        with open(path, "w") as f:
+            f.write(text + "\n")
+        return text
 
     def linear_update(self, A):
         """SketchySVD::linear_update: zero the sketches, then stream all rows."""
@@ -492,6 +551,7 @@ class SketchySVD(_Context):
         V = np.empty((r, self.ncol), dtype=np.float64)
         S = np.empty(r, dtype=np.float64)
         self._check(self.lib.skema_low_rank_approx(self.h, U.ctypes.data, S.ctypes.data, V.ctypes.data, L.MEM_HOST))
+        self.uvecs, self.svals, self.vvecs = U.T, S, V.T
         return U.T, S, V.T
 
 
@@ -506,11 +566,12 @@ def sketchysvd(matrix, alg: AlgParams):
     """Skema::sketchysvd (src/Skema_SketchySVD.cpp:1244-1405, 1408-1577),
     three-sketch branch: returns (U, S, V)."""
     with SketchySVD(alg) as sk:
-        if alg.kernel_func == L.KERNEL_GAUSSRBF:
-            sk.linear_update(matrix)
-        else:
-            sk.linear_update(matrix)
-        return sk.low_rank_approx()
+        sk.linear_update(matrix)
+        U, S, V = sk.low_rank_approx()
+        sk.compute_residuals(matrix)
+        if getattr(alg, "history_filename", ""):
+            sk.save_history(alg.history_filename)
+        return U, S, V
 
 
 def _ctx_for_standalone(device: int = 0, precision: int = L.PREC_FP32) -> _Context:

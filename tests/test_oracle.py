@@ -150,3 +150,30 @@ def test_oracle_vjp_matches_finite_differences(oracle):
     hx = 1e-3
     fdx = (L(X + hx * V, g) - L(X - hx * V, g)) / (2 * hx)
     assert abs(fdx - (dX * V).sum()) / abs(fdx) < 1e-5
+
+
+def test_residuals_restatement_pins():
+    """Skema::residuals (src/Skema_Residuals.hpp:58-217) restated: exact
+    singular triplets give zero, the windowed A^T U sum equals the one-shot
+    product, CSR equals dense, and the SPD form is ||A V - V S||."""
+    import scipy.sparse as sp
+
+    from oracle import sketchy_oracle as O
+
+    rng = np.random.default_rng(3)
+    A = rng.normal(size=(90, 40))
+    U, S, Vt = np.linalg.svd(A, full_matrices=False)
+    r = 6
+    assert np.max(O.residuals(A, U[:, :r], S[:r], Vt[:r].T, window=7)) < 1e-12 * S[0]
+    Up = np.linalg.qr(rng.normal(size=(90, r)))[0]
+    Vp = np.linalg.qr(rng.normal(size=(40, r)))[0]
+    Sp = np.sort(rng.uniform(1, 2, size=r))[::-1]
+    one = O.residuals(A, Up, Sp, Vp)
+    win = O.residuals(A, Up, Sp, Vp, window=16)
+    assert np.allclose(one, win, rtol=1e-13)
+    direct = np.sqrt(((A.T @ Up - Vp * Sp) ** 2).sum(0) + ((A @ Vp - Up * Sp) ** 2).sum(0))
+    assert np.allclose(one, direct, rtol=1e-13)
+    Asp = sp.random(90, 40, density=0.1, random_state=1, format="csr")
+    assert np.allclose(O.residuals(Asp, Up, Sp, Vp, window=32), O.residuals(Asp.toarray(), Up, Sp, Vp), rtol=1e-13)
+    B = A[:40] @ A[:40].T
+    assert np.allclose(O.residuals(B, None, Sp, Vp), np.linalg.norm(B @ Vp - Vp * Sp, axis=0), rtol=1e-13)
