@@ -570,6 +570,29 @@ def run_gpu(args, cfg, peaks, peak_kind):
                "max_rel_err_sigma_i": float(np.max(d / S32)), "max_err_over_sigma_1": float(np.max(d) / S32[0]),
                "sigma_1": float(S32[0]), "sigma_r": float(S32[-1])}
 
+    # the residual pass (compute_residuals, the second stream of A behind
+    # Skema::sketchysvd): FP64 on the device, timed once after the bench
+    # steps, rank 0 at N = 1, with the U, S, V of this step's approximation
+    respass = None
+    if rank == 0 and world == 1 and not args.no_residuals and not (rbf and a.precision):
+        step()
+        U, S, V = ctx.low_rank_approx()
+        r0e = torch.cuda.Event(enable_timing=True)
+        r1e = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        r0e.record(stream)
+        rn = ctx.residuals(None, U, S, V, row_blocks=[(row0, inp)])
+        r1e.record(stream)
+        torch.cuda.synchronize()
+        rms = r0e.elapsed_time(r1e)
+        r = cfg["rank"]
+        # FP64 work: A V and A^T U, 2 m n r flops each (dense input); the
+        # CSR form does 4 r flops per nonzero
+        fl = (4.0 * nnz * r) if sparse else (4.0 * m_local * (n if not rbf else m_glob) * r)
+        respass = {"ms": rms, "fp64_tflops": fl / (rms / 1e3) / 1e12,
+                   "rnorm_over_sigma1_max": float(np.max(rn) / S[0]),
+                   "includes": "H2D of U, S, V (host FP64) + the FP64 products + D2H of the norms"}
+
     out = {
         "metric": "sketched rows/s",
         "value": value,
@@ -592,6 +615,8 @@ def run_gpu(args, cfg, peaks, peak_kind):
     }
     if acc is not None:
         out["accuracy"] = acc
+    if respass is not None:
+        out["residual_pass"] = respass
     ctx.close()
     if world > 1:
         dist.barrier()
@@ -878,6 +903,7 @@ def main():
     ap.add_argument("--workload", default="csr-sparse-sign", choices=sorted(WORKLOADS))
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-residuals", action="store_true", help="skip the residual-pass timing")
     ap.add_argument("--no-accuracy", action="store_true",
                     help="skip the reduced-precision forms' singular-value check against the FP32 path")
     ap.add_argument("--cpu-budget", type=float, default=12.0)
