@@ -430,8 +430,6 @@ class _Context:
         Timings hold this build's stage timers (milliseconds, when timing is
         on) under the reference's keys; traces stay empty (no per-window
         singular-value traces are taken)."""
-        import json
-
         upd = {}
         for key, stage in (("upsilon", "update.upsilon"), ("omega", "update.omega"), ("phi", "update.phi"),
                            ("psi", "update.psi"), ("window", "update.window"), ("daxpy", "update.daxpy")):
@@ -439,20 +437,10 @@ class _Context:
                 upd[key] = self.timing_get(stage)[0] / 1e3
             except SkemaError:
                 upd[key] = 0.0
-        timings = {"init": {k: 0.0 for k in ("upsilon", "omega", "phi", "psi")}, "update": upd,
-                   "approx": {k: 0.0 for k in ("phi", "psi", "dgeqrf", "dgemm", "dgels", "dgesvd")}}
         r = self.rank
         sv = getattr(self, "svals", None)
         rn = getattr(self, "rnrms", None)
-        hist = {"timings": timings, "traces": {},
-                "svals": [float(x) for x in (sv if sv is not None else np.zeros(r))],
-                "rnrms": [float(x) for x in (rn if rn is not None else np.zeros(r))]}
-        text = json.dumps(hist, indent=4)
-        if path is None:
-            return text
-        with open(path, "w") as f:
-            f.write(text + "\n")
-        return text
+        return write_history(path, np.zeros(r) if sv is None else sv, np.zeros(r) if rn is None else rn, upd)
 
     def linear_update(self, A):
         """SketchySVD::linear_update: zero the sketches, then stream all rows."""
@@ -560,6 +548,28 @@ class SketchySPD(_Context):
 
     def get_sketches(self):
         return self.get_sketch(L.SKETCH_Y)
+
+
+def write_history(path, svals, rnrms, update_seconds=None):
+    """The JSON of SketchySVD::save_history (src/Skema_SketchySVD.cpp:730-755):
+    {"timings": {init, update, approx}, "traces": {}, "svals": [...],
+    "rnrms": [...]} with a 4-space indent, the reference's timing keys
+    (src/Skema_SketchySVD.cpp:101-116; update times in seconds where
+    given, else 0). Written to `path` (with a newline) unless path is None;
+    the text is returned."""
+    import json
+
+    upd = {k: 0.0 for k in ("upsilon", "omega", "phi", "psi", "window", "daxpy")}
+    upd.update(update_seconds or {})
+    timings = {"init": {k: 0.0 for k in ("upsilon", "omega", "phi", "psi")}, "update": upd,
+               "approx": {k: 0.0 for k in ("phi", "psi", "dgeqrf", "dgemm", "dgels", "dgesvd")}}
+    hist = {"timings": timings, "traces": {}, "svals": [float(x) for x in svals],
+            "rnrms": [float(x) for x in rnrms]}
+    text = json.dumps(hist, indent=4)
+    if path is not None:
+        with open(path, "w") as f:
+            f.write(text + "\n")
+    return text
 
 
 def sketchysvd(matrix, alg: AlgParams):
