@@ -724,6 +724,7 @@ __global__ void __launch_bounds__(kThreadsA32, 1)
     uint32_t it = 0;
     bool ok = true;
     float mx = 0.f;  // max |a| over every value this thread converts (FP8 form's window scale)
+    int pend = -1;   // (thread 0) BF16 stage whose A-tile store is still being read
     for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
       int mt, nt, ks;
       decode_unit(g, t, mt, nt, ks);
@@ -777,7 +778,9 @@ __global__ void __launch_bounds__(kThreadsA32, 1)
         mbar_arrive(full + s2);
         if (ct == 0) {
           // all 128 lines written (and the B tile landed): store the BF16
-          // tile, wait until TMA has read it, then release the stage
+          // tile. The stage is released once TMA has read it; that is waited
+          // for one stage later (the store before this one must be read by
+          // now), so this thread never stalls on its own fresh store.
           if (!mbar_wait(full + s2, ph2, err)) {
             ok = false;
             break;
@@ -786,12 +789,18 @@ __global__ void __launch_bounds__(kThreadsA32, 1)
           const int kc = (int)(k0 + (int64_t)kt * BK);
           tma_store_3d(&tmA16, stbf + s2 * STAGE, 0, mt * BM, kc / BK);
           bulk_commit();
-          bulk_wait_read_all();
-          mbar_arrive(empty + s2);
+          if (pend >= 0) {
+            asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+            mbar_arrive(empty + pend);
+          }
+          pend = s2;
         }
       }
     }
-    if (ct == 0) bulk_wait_all();
+    if (ct == 0) {
+      bulk_wait_all();
+      if (pend >= 0) mbar_arrive(empty + pend);
+    }
     if (AMAX) {
       // |a| as bits: for non-negative floats the integer order is the float
       // order, so the window's amax is one integer atomicMax per warp. Every
