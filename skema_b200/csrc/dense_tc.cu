@@ -106,12 +106,10 @@ Plan plan_split(const skema_ctx* c, int64_t tiles, int64_t K, int max_ks) {
   return Plan{ks, kchunk};
 }
 
-Plan plan_split_stream(const skema_ctx* c, int64_t tiles, int64_t K, int max_ks) {
-  const int64_t ksteps = (K + tc::BK - 1) / tc::BK;
-  int64_t ks = (8 * (int64_t)c->sm_count + tiles - 1) / tiles;
-  ks = std::max<int64_t>(1, std::min<int64_t>({ks, (int64_t)max_ks, ksteps / 8}));
-  const int64_t kchunk = (ksteps + ks - 1) / ks * tc::BK;
-  return Plan{(int)((K + kchunk - 1) / kchunk), kchunk};
+Plan plan_streamk(const skema_ctx* c, int ctas) {
+  Plan p{1, 0};
+  p.streamk = std::max(1, std::min(ctas, c->sm_count));
+  return p;
 }
 
 tc::OutSpec out_spec() {
@@ -282,6 +280,24 @@ __global__ void f32_to_bf16_cm_kernel(const float* __restrict__ S, __nv_bfloat16
 
 // Persistent launch: min(units, SMs) CTAs of one per SM (the 5-stage ring
 // takes 211 KB of shared memory).
+// Tiles, K-steps and schedule of one launch; *grid gets the CTA count.
+tc::Grid3 grid_of(const skema_ctx* c, int64_t M, int64_t N, int64_t K, int nt, int bk, const Plan& pl, int m_fast,
+                  int* grid) {
+  tc::Grid3 g;
+  g.mtiles = (int)((M + tc::BM - 1) / tc::BM);
+  g.ntiles = (int)((N + nt - 1) / nt);
+  g.ksplit = pl.ks;
+  g.m_fast = m_fast;
+  g.ksteps = (K + bk - 1) / bk;
+  g.kcsteps = pl.kchunk > 0 ? (int)(pl.kchunk / bk) : (int)g.ksteps;
+  g.streamk = pl.streamk > 0 ? 1 : 0;
+  const int64_t units = (int64_t)g.mtiles * g.ntiles * (g.streamk ? g.ksteps : g.ksplit);
+  if (units > 0x7fffffff) fail(SKEMA_EINVAL, "tensor-core grid too large");
+  *grid = (int)std::min<int64_t>(units, g.streamk ? pl.streamk : c->sm_count);
+  if (M <= 0 || N <= 0 || K <= 0) *grid = 0;
+  return g;
+}
+
 template <int AMODE>
 void launch_gemm(skema_ctx* c, const CUtensorMap& ta, const CUtensorMap& tb, int64_t M, int64_t N, int64_t K,
                  Plan pl, int m_fast, const tc::OutSpec& o) {
@@ -290,16 +306,10 @@ void launch_gemm(skema_ctx* c, const CUtensorMap& ta, const CUtensorMap& tb, int
   const size_t smem = (size_t)S * STAGE + 1024 + 256;
   auto kern = tc::gemm_bf16_kernel<kNT, S, AMODE>;
   SKEMA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  tc::Grid3 g;
-  g.mtiles = (int)((M + tc::BM - 1) / tc::BM);
-  g.ntiles = (int)((N + kNT - 1) / kNT);
-  g.ksplit = pl.ks;
-  g.m_fast = m_fast;
-  const int64_t units = (int64_t)g.mtiles * g.ntiles * g.ksplit;
-  if (units <= 0 || K <= 0) return;
-  if (units > 0x7fffffff) fail(SKEMA_EINVAL, "tensor-core grid too large");
-  const int grid = (int)std::min<int64_t>(units, c->sm_count);
-  kern<<<grid, tc::kThreads, smem, c->stream>>>(ta, tb, K, pl.kchunk, g, o, c->dev_err);
+  int grid = 0;
+  const tc::Grid3 g = grid_of(c, M, N, K, kNT, tc::BK, pl, m_fast, &grid);
+  if (grid <= 0) return;
+  kern<<<grid, tc::kThreads, smem, c->stream>>>(ta, tb, g, o, c->dev_err);
   SKEMA_LAUNCHED(c);
   c->dev_err_armed = true;
 }
@@ -313,16 +323,10 @@ void launch_gemm_a32(skema_ctx* c, const CUtensorMap& ta32, const CUtensorMap& t
   const size_t smem = (size_t)S1 * tc::BM * tc::BK * 4 + (size_t)S2 * STAGE + 1024 + 256;
   auto kern = amax ? tc::gemm_a32_kernel<kNT, S1, S2, AROW, true> : tc::gemm_a32_kernel<kNT, S1, S2, AROW, false>;
   SKEMA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  tc::Grid3 g;
-  g.mtiles = (int)((M + tc::BM - 1) / tc::BM);
-  g.ntiles = (int)((N + kNT - 1) / kNT);
-  g.ksplit = pl.ks;
-  g.m_fast = 1;
-  const int64_t units = (int64_t)g.mtiles * g.ntiles * g.ksplit;
-  if (units <= 0 || K <= 0) return;
-  if (units > 0x7fffffff) fail(SKEMA_EINVAL, "tensor-core grid too large");
-  const int grid = (int)std::min<int64_t>(units, c->sm_count);
-  kern<<<grid, tc::kThreadsA32, smem, c->stream>>>(ta32, tb, ta16, K, pl.kchunk, g, o, amax, c->dev_err);
+  int grid = 0;
+  const tc::Grid3 g = grid_of(c, M, N, K, kNT, tc::BK, pl, 1, &grid);
+  if (grid <= 0) return;
+  kern<<<grid, tc::kThreadsA32, smem, c->stream>>>(ta32, tb, ta16, g, o, amax, c->dev_err);
   SKEMA_LAUNCHED(c);
   c->dev_err_armed = true;
 }
@@ -469,16 +473,10 @@ void launch_gemm_fp8(skema_ctx* c, const CUtensorMap& ta, const CUtensorMap& tb,
   const size_t smem = (size_t)S * STAGE + 1024 + 256;
   auto kern = tc::gemm_fp8_kernel<kNT, S>;
   SKEMA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  tc::Grid3 g;
-  g.mtiles = (int)((M + tc::BM - 1) / tc::BM);
-  g.ntiles = (int)((N + kNT - 1) / kNT);
-  g.m_fast = 0;
-  g.ksplit = pl.ks;
-  const int64_t units = (int64_t)g.mtiles * g.ntiles * g.ksplit;
-  if (units <= 0 || K <= 0) return;
-  if (units > 0x7fffffff) fail(SKEMA_EINVAL, "tensor-core grid too large");
-  const int grid = (int)std::min<int64_t>(units, c->sm_count);
-  kern<<<grid, tc::kThreads, smem, c->stream>>>(ta, tb, K, pl.kchunk, g, o, c->dev_err);
+  int grid = 0;
+  const tc::Grid3 g = grid_of(c, M, N, K, kNT, 128, pl, 0, &grid);
+  if (grid <= 0) return;
+  kern<<<grid, tc::kThreads, smem, c->stream>>>(ta, tb, g, o, c->dev_err);
   SKEMA_LAUNCHED(c);
   c->dev_err_armed = true;
 }
@@ -520,12 +518,14 @@ void tc_z_update(skema_ctx* c, const __nv_bfloat16* T16, int64_t ldT, const TcSl
   StageScope st(c, ST_PHI);
   const CUtensorMap ta = tmap_bf16(T16, (uint64_t)K, (uint64_t)s, (uint64_t)ldT * 2, 64, 128);
   const CUtensorMap tb = tmap_bf16(sl.F16, (uint64_t)K, (uint64_t)s, (uint64_t)sl.ldm * 2, 64, kNT);
-  const int64_t tiles = ((s + 127) / 128) * ((s + kNT - 1) / kNT);
-  const Plan pl = plan_split(c, tiles, K, 32);
+  // Z^T has few tiles (8 at s = 403) and a long K: stream-K over 64 CTAs
+  // gives every tile about eight partial sums (a K split over all SMs gave
+  // 32, and their atomics dominated the product)
+  const Plan pl = plan_streamk(c, 64);
   tc::OutSpec o = out_spec();
   o.p0 = c->Z, o.rs0 = 1, o.cs0 = s, o.alpha0 = eta, o.beta0 = beta;
   o.rows = s, o.split = s, o.ncols = s;
-  if (pl.ks > 1) {
+  if (pl.split()) {
     scale_block(c, MatOut{c->Z, s, 1}, s, s, beta);
     o.atomic0 = 1, o.beta0 = 0.f;
   }
@@ -645,12 +645,14 @@ void tc_dense_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr, void* scratch
   {  // X^T = nu X^T + eta A_w^T Upsilon~_w^T
     StageScope st(c, ST_UPSILON);
     const CUtensorMap tb = tmap_bf16(sl.U16, (uint64_t)wr, (uint64_t)k, (uint64_t)sl.ldm * 2, 64, kNT);
-    const int64_t tiles = ((n + 127) / 128) * ((k + kNT - 1) / kNT);
-    const Plan pl = (a32_cm || a32_rm) ? plan_split_stream(c, tiles, wr, 8) : plan_split(c, tiles, wr, 8);
+    // stream-K over all SMs: each X^T tile gets one or two partial sums (a
+    // K split into eight ranges gave eight, and their atomics bounded the
+    // product)
+    const Plan pl = plan_streamk(c, c->sm_count);
     tc::OutSpec o = out_spec();
     o.p0 = c->X, o.rs0 = 1, o.cs0 = n, o.alpha0 = eta, o.beta0 = nu;
     o.rows = n, o.split = k, o.ncols = k;
-    if (pl.ks > 1) {
+    if (pl.split()) {
       scale_block(c, MatOut{c->X, n, 1}, k, n, nu);
       o.atomic0 = 1, o.beta0 = 0.f;
     }
@@ -680,7 +682,7 @@ void tc_dense_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr, void* scratch
     tc::OutSpec o = out_spec();
     o.p0 = c->Y + R0, o.rs0 = 1, o.cs0 = m, o.alpha0 = eta, o.beta0 = ybeta;
     o.rows = wr, o.split = k, o.ncols = k + s;
-    if (pl.ks == 1) {
+    if (!pl.split()) {
       o.p1 = T16, o.rs1 = 1, o.cs1 = wp;
     } else {
       scale_block(c, MatOut{c->Y + R0, 1, m}, wr, k, ybeta);
@@ -699,7 +701,7 @@ void tc_dense_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr, void* scratch
           tmap_bf16(c->op16, (uint64_t)n, (uint64_t)(k + s), (uint64_t)c->ld_op16 * 2, 64, kNT);
       launch_gemm<tc::A_MN_BLK>(c, ta, tb, wr, k + s, n, pl, 0, o);
     }
-    if (pl.ks > 1) t32_to_t16(c, T32, T16, nullptr, wr, s, wp);
+    if (pl.split()) t32_to_t16(c, T32, T16, nullptr, wr, s, wp);
   }
   y_rows_mark(c, R0, R0 + wr);
   tc_z_update(c, T16, wp, sl, wr, nu);

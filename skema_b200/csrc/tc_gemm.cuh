@@ -233,9 +233,19 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
 }
 
 // Work units: unit t -> (mt, nt, ks). M fastest when m_fast, else N.
+// Work of a launch: mtiles x ntiles output tiles of ksteps K-steps each.
+// Split mode (streamk = 0): unit t = (mt, nt, ks) covers K-steps
+// [ks kcsteps, (ks + 1) kcsteps); CTA b takes units b, b + gridDim.x, ...
+// Stream-K mode (streamk = 1): the tiles' K-steps in tile order are cut into
+// gridDim.x equal runs and CTA b takes run b, so a tile is shared by at most
+// a few CTAs and gets that many partial sums (added atomically), whatever
+// the tile count is against the SM count.
 struct Grid3 {
   int mtiles, ntiles, ksplit;
   int m_fast;
+  int64_t ksteps;
+  int kcsteps;
+  int streamk;
 };
 __device__ __forceinline__ void decode_unit(const Grid3& g, int t, int& mt, int& nt, int& ks) {
   if (g.m_fast) {
@@ -249,6 +259,36 @@ __device__ __forceinline__ void decode_unit(const Grid3& g, int t, int& mt, int&
     mt = t % g.mtiles;
     ks = t / g.mtiles;
   }
+}
+
+// A CTA's next segment of work: tile (mt, nt) and its K-steps [kt0, kt1).
+struct Sched {
+  int64_t pos, end;  // stream-K: this CTA's run of K-steps
+  int t;             // split mode: next unit
+};
+__device__ __forceinline__ void sched_init(const Grid3& g, Sched& s) {
+  const int64_t T = (int64_t)g.mtiles * g.ntiles * g.ksteps;
+  s.pos = T * blockIdx.x / gridDim.x;
+  s.end = T * (blockIdx.x + 1) / gridDim.x;
+  s.t = blockIdx.x;
+}
+__device__ __forceinline__ bool next_seg(const Grid3& g, Sched& s, int& mt, int& nt, int& kt0, int& kt1) {
+  int ks;
+  if (g.streamk) {
+    if (s.pos >= s.end) return false;
+    const int64_t tile = s.pos / g.ksteps;
+    kt0 = (int)(s.pos - tile * g.ksteps);
+    kt1 = (int)min(g.ksteps, (int64_t)kt0 + (s.end - s.pos));
+    s.pos += kt1 - kt0;
+    decode_unit(g, (int)tile, mt, nt, ks);
+    return true;
+  }
+  if (s.t >= g.mtiles * g.ntiles * g.ksplit) return false;
+  decode_unit(g, s.t, mt, nt, ks);
+  kt0 = ks * g.kcsteps;
+  kt1 = (int)min(g.ksteps, (int64_t)kt0 + g.kcsteps);
+  s.t += gridDim.x;
+  return true;
 }
 
 // Stores one finished 128 x NT accumulator (warps 0-3, warp w on TMEM lanes
@@ -322,7 +362,7 @@ __device__ __forceinline__ bool epilogue_unit(const OutSpec& o, uint32_t tmem, u
 template <int NT, int S, int AMODE>
 __global__ void __launch_bounds__(kThreads, 1)
     gemm_bf16_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
-                     int64_t K, int64_t kchunk, Grid3 g, OutSpec o, int* err) {
+                     Grid3 g, OutSpec o, int* err) {
   constexpr uint32_t A_BYTES = BM * BK * 2;  // 16 KB
   constexpr uint32_t B_BYTES = NT * BK * 2;
   constexpr uint32_t STAGE = ((A_BYTES + B_BYTES + 1023) / 1024) * 1024;
@@ -339,7 +379,6 @@ __global__ void __launch_bounds__(kThreads, 1)
   uint32_t* tbase = reinterpret_cast<uint32_t*>(tempty + 2);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int total = g.mtiles * g.ntiles * g.ksplit;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < S; ++s) {
@@ -367,11 +406,11 @@ __global__ void __launch_bounds__(kThreads, 1)
     // ---------------- TMA producer ----------------
     uint32_t it = 0;
     bool ok = true;
-    for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
-      int mt, nt, ks;
-      decode_unit(g, t, mt, nt, ks);
-      const int64_t k0 = (int64_t)ks * kchunk;
-      const int KT = (int)((min(K, k0 + kchunk) - k0 + BK - 1) / BK);
+    Sched sc;
+    sched_init(g, sc);
+    int mt, nt, kt0, kt1;
+    while (ok && next_seg(g, sc, mt, nt, kt0, kt1)) {
+      const int KT = kt1 - kt0;
       for (int kt = 0; kt < KT; ++kt, ++it) {
         const int s = it % S;
         const uint32_t ph = (it / S) & 1;
@@ -382,7 +421,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         unsigned char* sa = smem + s * STAGE;
         unsigned char* sb = sa + A_BYTES;
         mbar_expect_tx(full + s, A_BYTES + B_BYTES);
-        const int kc = (int)(k0 + (int64_t)kt * BK);
+        const int kc = (kt0 + kt) * BK;
         if (AMODE == A_KMAJ) {
           tma_load_2d(&tmA, full + s, sa, kc, mt * BM);
         } else if (AMODE == A_KMAJ_BLK) {
@@ -399,11 +438,11 @@ __global__ void __launch_bounds__(kThreads, 1)
     constexpr uint32_t idesc = idesc_bf16(NT, AMODE == A_MN_BLK, false);
     uint32_t it = 0, tcount = 0;
     bool ok = true;
-    for (int t = blockIdx.x; t < total && ok; t += gridDim.x, ++tcount) {
-      int mt, nt, ks;
-      decode_unit(g, t, mt, nt, ks);
-      const int64_t k0 = (int64_t)ks * kchunk;
-      const int KT = (int)((min(K, k0 + kchunk) - k0 + BK - 1) / BK);
+    Sched sc;
+    sched_init(g, sc);
+    int mt, nt, kt0, kt1;
+    while (ok && next_seg(g, sc, mt, nt, kt0, kt1)) {
+      const int KT = kt1 - kt0;
       const uint32_t acc = tcount & 1, aph = (tcount >> 1) & 1;
       if (!mbar_wait(tempty + acc, aph ^ 1, err)) break;
       tc_fence_after();
@@ -428,13 +467,15 @@ __global__ void __launch_bounds__(kThreads, 1)
         umma_commit(empty + s);
       }
       if (ok) umma_commit(tfull + acc);
+      ++tcount;
     }
   } else if (warp < 4) {
     // ---------------- epilogue ----------------
     uint32_t tcount = 0;
-    for (int t = blockIdx.x; t < total; t += gridDim.x, ++tcount) {
-      int mt, nt, ks;
-      decode_unit(g, t, mt, nt, ks);
+    Sched sc;
+    sched_init(g, sc);
+    int mt, nt, kt0, kt1;
+    for (; next_seg(g, sc, mt, nt, kt0, kt1); ++tcount) {
       const uint32_t acc = tcount & 1, aph = (tcount >> 1) & 1;
       if (!epilogue_unit<NT, TCOLS>(o, tmem, acc, aph, tfull, tempty, mt, nt, warp, lane, err)) break;
     }
@@ -462,8 +503,8 @@ __global__ void __launch_bounds__(kThreads, 1)
 // scales are folded into the epilogue through OutSpec::scale.
 template <int NT, int S>
 __global__ void __launch_bounds__(kThreads, 1)
-    gemm_fp8_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, int64_t K,
-                    int64_t kchunk, Grid3 g, OutSpec o, int* err) {
+    gemm_fp8_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, Grid3 g,
+                    OutSpec o, int* err) {
   constexpr int BK8 = 128;
   constexpr uint32_t A_BYTES = BM * BK8;  // 16 KB
   constexpr uint32_t B_BYTES = NT * BK8;
@@ -480,7 +521,6 @@ __global__ void __launch_bounds__(kThreads, 1)
   uint32_t* tbase = reinterpret_cast<uint32_t*>(tempty + 2);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int total = g.mtiles * g.ntiles * g.ksplit;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < S; ++s) {
@@ -507,11 +547,11 @@ __global__ void __launch_bounds__(kThreads, 1)
   if (warp == 4 && lane == 0) {
     uint32_t it = 0;
     bool ok = true;
-    for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
-      int mt, nt, ks;
-      decode_unit(g, t, mt, nt, ks);
-      const int64_t k0 = (int64_t)ks * kchunk;
-      const int KT = (int)((min(K, k0 + kchunk) - k0 + BK8 - 1) / BK8);
+    Sched sc;
+    sched_init(g, sc);
+    int mt, nt, kt0, kt1;
+    while (ok && next_seg(g, sc, mt, nt, kt0, kt1)) {
+      const int KT = kt1 - kt0;
       for (int kt = 0; kt < KT; ++kt, ++it) {
         const int s = it % S;
         const uint32_t ph = (it / S) & 1;
@@ -521,7 +561,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         unsigned char* sa = smem + s * STAGE;
         mbar_expect_tx(full + s, A_BYTES + B_BYTES);
-        const int kc = (int)(k0 + (int64_t)kt * BK8);
+        const int kc = (kt0 + kt) * BK8;
         tma_load_2d(&tmA, full + s, sa, kc, mt * BM);
         tma_load_2d(&tmB, full + s, sa + A_BYTES, kc, nt * NT);
       }
@@ -530,11 +570,11 @@ __global__ void __launch_bounds__(kThreads, 1)
     constexpr uint32_t idesc = idesc_e4m3(NT);
     uint32_t it = 0, tcount = 0;
     bool ok = true;
-    for (int t = blockIdx.x; t < total && ok; t += gridDim.x, ++tcount) {
-      int mt, nt, ks;
-      decode_unit(g, t, mt, nt, ks);
-      const int64_t k0 = (int64_t)ks * kchunk;
-      const int KT = (int)((min(K, k0 + kchunk) - k0 + BK8 - 1) / BK8);
+    Sched sc;
+    sched_init(g, sc);
+    int mt, nt, kt0, kt1;
+    while (ok && next_seg(g, sc, mt, nt, kt0, kt1)) {
+      const int KT = kt1 - kt0;
       const uint32_t acc = tcount & 1, aph = (tcount >> 1) & 1;
       if (!mbar_wait(tempty + acc, aph ^ 1, err)) break;
       tc_fence_after();
@@ -556,12 +596,14 @@ __global__ void __launch_bounds__(kThreads, 1)
         umma_commit(empty + s);
       }
       if (ok) umma_commit(tfull + acc);
+      ++tcount;
     }
   } else if (warp < 4) {
     uint32_t tcount = 0;
-    for (int t = blockIdx.x; t < total; t += gridDim.x, ++tcount) {
-      int mt, nt, ks;
-      decode_unit(g, t, mt, nt, ks);
+    Sched sc;
+    sched_init(g, sc);
+    int mt, nt, kt0, kt1;
+    for (; next_seg(g, sc, mt, nt, kt0, kt1); ++tcount) {
       const uint32_t acc = tcount & 1, aph = (tcount >> 1) & 1;
       if (!epilogue_unit<NT, TCOLS>(o, tmem, acc, aph, tfull, tempty, mt, nt, warp, lane, err)) break;
     }
@@ -603,8 +645,7 @@ constexpr int kThreadsA32 = 320;
 template <int NT, int S1, int S2, bool AROW, bool AMAX>
 __global__ void __launch_bounds__(kThreadsA32, 1)
     gemm_a32_kernel(const __grid_constant__ CUtensorMap tmA32, const __grid_constant__ CUtensorMap tmB,
-                    const __grid_constant__ CUtensorMap tmA16, int64_t K, int64_t kchunk, Grid3 g, OutSpec o,
-                    uint32_t* amax, int* err) {
+                    const __grid_constant__ CUtensorMap tmA16, Grid3 g, OutSpec o, uint32_t* amax, int* err) {
   constexpr uint32_t A32_BYTES = BM * BK * 4;  // 32 KB
   constexpr uint32_t A_BYTES = BM * BK * 2;    // 16 KB
   constexpr uint32_t B_BYTES = NT * BK * 2;
@@ -625,7 +666,6 @@ __global__ void __launch_bounds__(kThreadsA32, 1)
   uint32_t* tbase = reinterpret_cast<uint32_t*>(tempty + 2);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int total = g.mtiles * g.ntiles * g.ksplit;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < S1; ++s) {
@@ -657,15 +697,15 @@ __global__ void __launch_bounds__(kThreadsA32, 1)
     // ---------------- TMA producer ----------------
     uint32_t it = 0;
     bool ok = true;
-    for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
-      int mt, nt, ks;
-      decode_unit(g, t, mt, nt, ks);
-      const int64_t k0 = (int64_t)ks * kchunk;
-      const int KT = (int)((min(K, k0 + kchunk) - k0 + BK - 1) / BK);
+    Sched sc;
+    sched_init(g, sc);
+    int mt, nt, kt0, kt1;
+    while (ok && next_seg(g, sc, mt, nt, kt0, kt1)) {
+      const int KT = kt1 - kt0;
       for (int kt = 0; kt < KT; ++kt, ++it) {
         const int s1 = it % S1, s2 = it % S2;
         const uint32_t ph1 = (it / S1) & 1, ph2 = (it / S2) & 1;
-        const int kc = (int)(k0 + (int64_t)kt * BK);
+        const int kc = (kt0 + kt) * BK;
         if (!mbar_wait(f32empty + s1, ph1 ^ 1, err)) {
           ok = false;
           break;
@@ -692,11 +732,11 @@ __global__ void __launch_bounds__(kThreadsA32, 1)
     constexpr uint32_t idesc = idesc_bf16(NT, false, false);
     uint32_t it = 0, tcount = 0;
     bool ok = true;
-    for (int t = blockIdx.x; t < total && ok; t += gridDim.x, ++tcount) {
-      int mt, nt, ks;
-      decode_unit(g, t, mt, nt, ks);
-      const int64_t k0 = (int64_t)ks * kchunk;
-      const int KT = (int)((min(K, k0 + kchunk) - k0 + BK - 1) / BK);
+    Sched sc;
+    sched_init(g, sc);
+    int mt, nt, kt0, kt1;
+    while (ok && next_seg(g, sc, mt, nt, kt0, kt1)) {
+      const int KT = kt1 - kt0;
       const uint32_t acc = tcount & 1, aph = (tcount >> 1) & 1;
       if (!mbar_wait(tempty + acc, aph ^ 1, err)) break;
       tc_fence_after();
@@ -717,6 +757,7 @@ __global__ void __launch_bounds__(kThreadsA32, 1)
         umma_commit(empty + s2);
       }
       if (ok) umma_commit(tfull + acc);
+      ++tcount;
     }
   } else if (warp >= 6) {
     // ---------------- converters ----------------
@@ -725,11 +766,11 @@ __global__ void __launch_bounds__(kThreadsA32, 1)
     bool ok = true;
     float mx = 0.f;  // max |a| over every value this thread converts (FP8 form's window scale)
     int pend = -1;   // (thread 0) BF16 stage whose A-tile store is still being read
-    for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
-      int mt, nt, ks;
-      decode_unit(g, t, mt, nt, ks);
-      const int64_t k0 = (int64_t)ks * kchunk;
-      const int KT = (int)((min(K, k0 + kchunk) - k0 + BK - 1) / BK);
+    Sched sc;
+    sched_init(g, sc);
+    int mt, nt, kt0, kt1;
+    while (ok && next_seg(g, sc, mt, nt, kt0, kt1)) {
+      const int KT = kt1 - kt0;
       for (int kt = 0; kt < KT; ++kt, ++it) {
         const int s1 = it % S1, s2 = it % S2;
         const uint32_t ph1 = (it / S1) & 1, ph2 = (it / S2) & 1;
@@ -786,7 +827,7 @@ __global__ void __launch_bounds__(kThreadsA32, 1)
             break;
           }
           fence_proxy_async();
-          const int kc = (int)(k0 + (int64_t)kt * BK);
+          const int kc = (kt0 + kt) * BK;
           tma_store_3d(&tmA16, stbf + s2 * STAGE, 0, mt * BM, kc / BK);
           bulk_commit();
           if (pend >= 0) {
@@ -812,9 +853,10 @@ __global__ void __launch_bounds__(kThreadsA32, 1)
   } else if (warp < 4) {
     // ---------------- epilogue ----------------
     uint32_t tcount = 0;
-    for (int t = blockIdx.x; t < total; t += gridDim.x, ++tcount) {
-      int mt, nt, ks;
-      decode_unit(g, t, mt, nt, ks);
+    Sched sc;
+    sched_init(g, sc);
+    int mt, nt, kt0, kt1;
+    for (; next_seg(g, sc, mt, nt, kt0, kt1); ++tcount) {
       const uint32_t acc = tcount & 1, aph = (tcount >> 1) & 1;
       if (!epilogue_unit<NT, TCOLS>(o, tmem, acc, aph, tfull, tempty, mt, nt, warp, lane, err)) break;
     }

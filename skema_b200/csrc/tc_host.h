@@ -11,16 +11,21 @@ namespace skema {
 
 inline int64_t pad8(int64_t x) { return (x + 7) / 8 * 8; }
 
-// A split of K into ks ranges of kchunk (a multiple of 64).
+// A split of K into ks ranges of kchunk (a multiple of the kernel's K
+// step), or, with streamk > 0, a stream-K schedule over streamk CTAs (each
+// takes an equal run of the tiles' K-steps). Either split adds partial sums
+// atomically into outputs scaled beforehand.
 struct Plan {
   int ks;
   int64_t kchunk;
+  int streamk = 0;
+  bool split() const { return ks > 1 || streamk > 0; }
 };
+// Stream-K over `ctas` CTAs (at most one per SM).
+Plan plan_streamk(const skema_ctx* c, int ctas);
 // Split that minimises waves x (k-steps per split + fill) for a product
 // bound by the tensor pipe, one CTA per SM.
 Plan plan_split(const skema_ctx* c, int64_t tiles, int64_t K, int max_ks);
-// Split for an HBM-bound product: about eight rounds of units over the SMs.
-Plan plan_split_stream(const skema_ctx* c, int64_t tiles, int64_t K, int max_ks);
 
 tc::OutSpec out_spec();
 
