@@ -98,6 +98,11 @@ void dense_update(skema_ctx* c, Mat A, int64_t row0, int64_t nrows) {
     residual_dense(c, A, row0, nrows);
     return;
   }
+  if (!c->spd && c->p.dim_redux == SKEMA_MAP_GAUSS && c->p.precision != SKEMA_PREC_FP32) {
+    if (!tc_available(c)) fail(SKEMA_EUNSUPPORTED, "this precision is not available for this sketch");
+    tc_dense_update(c, A, row0, nrows);
+    return;
+  }
   const int64_t W = c->w;
   float* T = (float*)workspace(c, dense_scratch_bytes(c, std::min(W, nrows)));
   for (int64_t r = 0; r < nrows; r += W) {

@@ -25,6 +25,7 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <mutex>
 
@@ -265,16 +266,16 @@ namespace {
 
 // BF16 column-major (ld) <- FP32 column-major (ld), rows x cols, and the
 // BF16 rounding of the remainder into L (when given).
-__global__ void f32_to_bf16_cm_kernel(const float* __restrict__ S, __nv_bfloat16* __restrict__ D,
-                                      __nv_bfloat16* __restrict__ L, int64_t rows, int64_t cols, int64_t ld) {
+__global__ void f32_to_bf16_cm_kernel(const float* __restrict__ S, int64_t lds, __nv_bfloat16* __restrict__ D,
+                                      __nv_bfloat16* __restrict__ L, int64_t ldd, int64_t rows, int64_t cols) {
   const int64_t total = rows * cols;
   for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < total;
        q += (int64_t)gridDim.x * blockDim.x) {
     const int64_t j = q / rows, i = q - j * rows;
-    const float x = S[i + j * ld];
+    const float x = S[i + j * lds];
     const __nv_bfloat16 hi = __float2bfloat16(x);
-    D[i + j * ld] = hi;
-    if (L) L[i + j * ld] = __float2bfloat16(x - __bfloat162float(hi));
+    D[i + j * ldd] = hi;
+    if (L) L[i + j * ldd] = __float2bfloat16(x - __bfloat162float(hi));
   }
 }
 
@@ -483,11 +484,11 @@ void launch_gemm_fp8(skema_ctx* c, const CUtensorMap& ta, const CUtensorMap& tb,
 
 }  // namespace
 
-void t32_to_t16(skema_ctx* c, const float* T32, __nv_bfloat16* T16, __nv_bfloat16* T16lo, int64_t rows,
-                int64_t cols, int64_t ld) {
+void t32_to_t16(skema_ctx* c, const float* T32, int64_t ld32, __nv_bfloat16* T16, __nv_bfloat16* T16lo, int64_t ld16,
+                int64_t rows, int64_t cols) {
   if (rows <= 0 || cols <= 0) return;
   const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((rows * cols + 255) / 256, c->sm_count * 16));
-  f32_to_bf16_cm_kernel<<<grid, 256, 0, c->stream>>>(T32, T16, T16lo, rows, cols, ld);
+  f32_to_bf16_cm_kernel<<<grid, 256, 0, c->stream>>>(T32, ld32, T16, T16lo, ld16, rows, cols);
   SKEMA_LAUNCHED(c);
 }
 
@@ -602,7 +603,7 @@ size_t tc_scratch_bytes(const skema_ctx* c, int64_t wr) {
   return b;
 }
 
-void tc_dense_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr, void* scratch) {
+void tc_dense_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr, void* scratch, const ZDefer* zd) {
   const float eta = (float)c->p.sketch_eta, nu = (float)c->p.sketch_nu;
   const int64_t k = c->k, s = c->s, n = c->n, m = c->m;
   const int64_t wp = pad8(wr);
@@ -682,8 +683,13 @@ void tc_dense_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr, void* scratch
     tc::OutSpec o = out_spec();
     o.p0 = c->Y + R0, o.rs0 = 1, o.cs0 = m, o.alpha0 = eta, o.beta0 = ybeta;
     o.rows = wr, o.split = k, o.ncols = k + s;
+    // T goes to this window's scratch, or (Z deferred) to its rows of the
+    // group's T, weighted nu^(G-1-w) for window w of the group
+    __nv_bfloat16* Tdst = zd ? zd->T16 + (R0 - zd->row0) : T16;
+    const int64_t ldTd = zd ? zd->ldT : wp;
+    if (zd) o.row_log2w = zd->log2nu, o.row_wlen = wr + 1, o.row_nwin = zd->windows - zd->w;
     if (!pl.split()) {
-      o.p1 = T16, o.rs1 = 1, o.cs1 = wp;
+      o.p1 = Tdst, o.rs1 = 1, o.cs1 = ldTd;
     } else {
       scale_block(c, MatOut{c->Y + R0, 1, m}, wr, k, ybeta);
       SKEMA_CUDA(cudaMemsetAsync(T32, 0, sizeof(float) * (size_t)(wp * s), c->stream));
@@ -701,10 +707,54 @@ void tc_dense_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr, void* scratch
           tmap_bf16(c->op16, (uint64_t)n, (uint64_t)(k + s), (uint64_t)c->ld_op16 * 2, 64, kNT);
       launch_gemm<tc::A_MN_BLK>(c, ta, tb, wr, k + s, n, pl, 0, o);
     }
-    if (pl.split()) t32_to_t16(c, T32, T16, nullptr, wr, s, wp);
+    if (pl.split()) t32_to_t16(c, T32, wp, Tdst, nullptr, ldTd, wr, s);
   }
   y_rows_mark(c, R0, R0 + wr);
-  tc_z_update(c, T16, wp, sl, wr, nu);
+  if (!zd) tc_z_update(c, T16, wp, sl, wr, nu);
+}
+
+// The windows of one call with Z deferred: X^T and [Y | T] per window, T of
+// every window into one buffer, then one Z^T product over all the rows of a
+// group of windows -- Z = nu^G Z + eta sum_w nu^(G-1-w) Phi~_w T_w, the
+// per-window recurrence (src/Skema_SketchySVD.cpp:187-189) summed. A Z^T
+// product over K = 8,192 rows per window was atomics-bound; over the call's
+// rows its partial sums are few next to its work. Groups are capped at
+// 512 MB of BF16 T; nu <= 0 (no log2 weight) keeps Z per window.
+void tc_dense_update(skema_ctx* c, Mat A, int64_t row0, int64_t nrows) {
+  const int64_t W = c->w, s = c->s;
+  const float nu = (float)c->p.sketch_nu;
+  const int64_t wmax = std::min(W, nrows);
+  const size_t win_bytes = tc_scratch_bytes(c, wmax);
+  if (!(nu > 0.f)) {
+    void* ws = workspace(c, win_bytes);
+    for (int64_t r = 0; r < nrows; r += W)
+      tc_dense_window(c, Mat{A.p + r * A.rs, A.rs, A.cs}, row0 + r, std::min(W, nrows - r), ws, nullptr);
+    return;
+  }
+  const int64_t cap_rows = std::max<int64_t>(1, ((int64_t)512 << 20) / (2 * s) / W) * W;
+  const int64_t grows = std::min(nrows, cap_rows);
+  const int64_t ldT = pad8(grows);
+  const size_t t_bytes = (sizeof(__nv_bfloat16) * (size_t)(ldT * s) + 255) / 256 * 256;
+  char* ws = static_cast<char*>(workspace(c, win_bytes + t_bytes + tc_slice_bytes(c, grows) + 256));
+  void* win_scratch = ws;
+  ZDefer zd;
+  zd.T16 = reinterpret_cast<__nv_bfloat16*>(ws + (win_bytes + 255) / 256 * 256);
+  zd.ldT = ldT;
+  zd.log2nu = nu == 1.f ? 0.f : std::log2(nu);
+  char* slice_sp = reinterpret_cast<char*>(zd.T16) + t_bytes;
+  for (int64_t g0 = 0; g0 < nrows; g0 += grows) {
+    const int64_t gr = std::min(grows, nrows - g0);
+    zd.row0 = row0 + g0;
+    zd.windows = (gr + W - 1) / W;
+    for (int64_t w = 0; w < zd.windows; ++w) {
+      zd.w = w;
+      const int64_t r = g0 + w * W;
+      tc_dense_window(c, Mat{A.p + r * A.rs, A.rs, A.cs}, row0 + r, std::min(W, nrows - r), win_scratch, &zd);
+    }
+    char* sp = slice_sp;
+    const TcSlices sl = tc_window_slices(c, zd.row0, gr, &sp);
+    tc_z_update(c, zd.T16, ldT, sl, gr, std::pow(nu, (float)zd.windows));
+  }
 }
 
 }  // namespace skema

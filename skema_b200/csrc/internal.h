@@ -1,6 +1,7 @@
 // internal.h -- private declarations shared by the library's translation
 // units: the context, map storage and the launchers of every kernel.
 #pragma once
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -213,7 +214,16 @@ size_t dense_scratch_bytes(const skema_ctx* c, int64_t wr);
 bool tc_available(const skema_ctx* c);
 void tc_prepare_maps(skema_ctx* c);
 size_t tc_scratch_bytes(const skema_ctx* c, int64_t wr);
-void tc_dense_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr, void* scratch);
+// Z deferred to the end of a group of windows: T of window w (of `windows`)
+// goes to rows [R0 - row0, ...) of T16 (ld ldT), weighted nu^(windows-1-w).
+struct ZDefer {
+  __nv_bfloat16* T16;
+  int64_t ldT, row0, windows, w;
+  float log2nu;
+};
+void tc_dense_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr, void* scratch, const ZDefer* zd = nullptr);
+// All windows of one dense call in the tensor-core forms (Z per group of windows).
+void tc_dense_update(skema_ctx* c, Mat A, int64_t row0, int64_t nrows);
 // Reads the tensor-core status word (synchronises the stream) and fails with
 // SKEMA_ETIMEOUT if a kernel gave up on a wait since the last check.
 void check_device_error(skema_ctx* c);

@@ -193,7 +193,7 @@ void rbf_tc_update(skema_ctx* c, Mat P, int64_t N, int64_t d, int64_t row0, int6
         run_pass<1>(c, true, tq, tk, c->op16, N, k + s, c->ld_op16, a, o);
       else
         run_pass<2>(c, true, tq, tk, c->op16, N, k + s, c->ld_op16, a, o);
-      if (a.ksplit > 1) t32_to_t16(c, T32, T16, T16lo, nr, s, ldT);
+      if (a.ksplit > 1) t32_to_t16(c, T32, ldT, T16, T16lo, ldT, nr, s);
     }
     y_rows_mark(c, R0, R0 + nr);
     {  // column pass: X^T = nu^G X^T + eta sum_w nu^(G-1-w) K_w^T Upsilon~_w^T

@@ -33,10 +33,10 @@ CUtensorMap tmap_bf16(const void* base, uint64_t d0, uint64_t d1, uint64_t st1, 
 
 // FP32 strided block -> BF16 with D(i, j) at D[i * drs + j * dcs].
 void to_bf16(skema_ctx* c, Mat src, int64_t rows, int64_t cols, __nv_bfloat16* D, int64_t drs, int64_t dcs);
-// BF16 column-major (ld) <- FP32 column-major (ld), rows x cols; T16lo
-// (when given) receives the BF16 rounding of the remainder.
-void t32_to_t16(skema_ctx* c, const float* T32, __nv_bfloat16* T16, __nv_bfloat16* T16lo, int64_t rows,
-                int64_t cols, int64_t ld);
+// BF16 column-major (ld16) <- FP32 column-major (ld32), rows x cols; T16lo
+// (when given, ld16) receives the BF16 rounding of the remainder.
+void t32_to_t16(skema_ctx* c, const float* T32, int64_t ld32, __nv_bfloat16* T16, __nv_bfloat16* T16lo, int64_t ld16,
+                int64_t rows, int64_t cols);
 
 // The window's columns of the BF16 Upsilon~ / Phi~ copies as TMA operands:
 // in place when R0 is a multiple of 8 (16-byte aligned), else converted

@@ -312,3 +312,25 @@ def test_dense_fp8_window_scale_tracks_amax(sk, oracle):
         e = rel_fro(Y[r0:r0 + 128], o.Y[r0:r0 + 128])
         print(f"fp8 window at {r0}: Y {e:.2e}")
         assert e < TOL_YZ8, (r0, e)
+
+
+@pytest.mark.parametrize("prec", ["bf16", "fp8"])
+def test_dense_tc_many_windows_one_call_nu(sk, oracle, prec):
+    # a device input of six windows (the last ragged) in one call: Z is formed
+    # once for the call from the windows' T weighted nu^(G-1-w)
+    import torch
+
+    m, n = 2900, 700
+    A = dense_input(m, n, seed=21).astype(np.float32)
+    a = alg(sk, m, n, 8, 500, 0, sketch_eta=1.25, sketch_nu=0.8)
+    a = bf16(a, sk) if prec == "bf16" else fp8(a, sk)
+    o = oracle_for(oracle, a)
+    if prec == "fp8":
+        e4m3_grid(o.maps)
+    o.linear_update(A.astype(np.float64))
+    with sk.SketchySVD(a) as s:
+        s.linear_update(torch.from_numpy(A).cuda())
+        if prec == "bf16":
+            check(s, o, "six windows")
+        else:
+            check8(s, o, "six windows")
