@@ -122,6 +122,7 @@ tc::OutSpec out_spec() {
   o.atomic0 = 0, o.atomic1 = 0;
   o.row_log2w = 0.f, o.row_wlen = 1, o.row_nwin = 1;
   o.scale = nullptr;
+  o.scale_wlen = 1;
   return o;
 }
 
@@ -394,15 +395,15 @@ __global__ void amax_a16_kernel(const __nv_bfloat16* __restrict__ A16, int64_t c
 // blocks (4 rows of 4 columns: four 8-byte loads, sixteen lanes covering one
 // column line), converts them and stores each block row as one 32-bit word
 // of the row-major tile; rows then leave as 16-byte stores. scale_A comes
-// from the window's amax (win[0]); block 0 also writes the [Y | T] product
-// scale 1 / (scale_A scale_map) into win[1].
+// from the window's amax (*amax); block 0 also writes the [Y | T] product
+// scale 1 / (scale_A scale_map) into *scale_out.
 __global__ void __launch_bounds__(256)
     a16_to_a8_kernel(const __nv_bfloat16* __restrict__ A16, int64_t rows, int64_t cols, uint8_t* __restrict__ A8,
-                     int64_t ld8, uint32_t* win, float smap) {
+                     int64_t ld8, const uint32_t* amax, float* scale_out, float smap) {
   constexpr int TC = 128, RS = TC + 16;  // tile columns; shared row stride in bytes
   __shared__ __align__(16) uint8_t tile[64 * RS];
-  const float sa = pow2_scale_for(__uint_as_float(win[0]));
-  if (blockIdx.x == 0 && threadIdx.x == 0) win[1] = __float_as_uint(1.f / (sa * smap));
+  const float sa = pow2_scale_for(__uint_as_float(*amax));
+  if (blockIdx.x == 0 && threadIdx.x == 0) *scale_out = 1.f / (sa * smap);
   const int64_t nrb = (rows + 63) / 64, ncb = (cols + TC - 1) / TC;
   for (int64_t t = blockIdx.x; t < nrb * ncb; t += gridDim.x) {
     const int64_t rb = t / ncb, j0 = (t - rb * ncb) * TC;
@@ -603,9 +604,123 @@ size_t tc_scratch_bytes(const skema_ctx* c, int64_t wr) {
   return b;
 }
 
-void tc_dense_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr, void* scratch, const ZDefer* zd) {
+namespace {
+
+// X^T = nu X^T + eta A_w^T Upsilon~_w^T for one window, leaving bf16(A_w)
+// row-blocked in A16 (zero rows up to a multiple of 64). The product reads
+// the FP32 window itself (and writes A16) when TMA can address it (16-byte
+// aligned base and stride); otherwise a conversion pass writes A16 first.
+// amax (FP8 form) receives max |a| of the window. Returns the window's
+// Upsilon~ / Phi~ slices (copies taken from *sp when R0 is unaligned).
+TcSlices xt_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr, __nv_bfloat16* A16, uint32_t* amax, char** sp) {
+  const float eta = (float)c->p.sketch_eta, nu = (float)c->p.sketch_nu;
+  const int64_t k = c->k, n = c->n;
+  const int64_t nrb = (wr + 63) / 64;
+  const bool al = reinterpret_cast<uintptr_t>(Aw.p) % 16 == 0;
+  const bool a32_cm = al && Aw.rs == 1 && Aw.cs % 4 == 0;
+  const bool a32_rm = al && Aw.cs == 1 && Aw.rs % 4 == 0;
+  if (!a32_cm && !a32_rm) {
+    StageScope st(c, ST_WINDOW);
+    to_bf16_blocked(c, Aw, wr, n, A16);
+    if (amax) {
+      const int64_t cnt = nrb * 64 * n;
+      const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((cnt + 255) / 256, c->sm_count * 8));
+      amax_a16_kernel<<<grid, 256, 0, c->stream>>>(A16, cnt, amax);
+      SKEMA_LAUNCHED(c);
+    }
+  }
+  const TcSlices sl = tc_window_slices(c, R0, wr, sp);
+  StageScope st(c, ST_UPSILON);
+  const CUtensorMap tb = tmap_bf16(sl.U16, (uint64_t)wr, (uint64_t)k, (uint64_t)sl.ldm * 2, 64, kNT);
+  // stream-K over all SMs: each X^T tile gets one or two partial sums (a K
+  // split into eight ranges gave eight, and their atomics bounded the product)
+  const Plan pl = plan_streamk(c, c->sm_count);
+  tc::OutSpec o = out_spec();
+  o.p0 = c->X, o.rs0 = 1, o.cs0 = n, o.alpha0 = eta, o.beta0 = nu;
+  o.rows = n, o.split = k, o.ncols = k;
+  if (pl.split()) {
+    scale_block(c, MatOut{c->X, n, 1}, k, n, nu);
+    o.atomic0 = 1, o.beta0 = 0.f;
+  }
+  const CUtensorMap ta16 = tmap_bf16_blocked(A16, (uint64_t)n, (uint64_t)nrb, 128);
+  if (a32_cm) {
+    const CUtensorMap ta32 = tmap_f32(Aw.p, (uint64_t)wr, (uint64_t)n, (uint64_t)Aw.cs * 4, 32, 128);
+    launch_gemm_a32<false>(c, ta32, tb, ta16, n, k, wr, pl, o, amax);
+  } else if (a32_rm) {
+    const CUtensorMap ta32 = tmap_f32(Aw.p, (uint64_t)n, (uint64_t)wr, (uint64_t)Aw.rs * 4, 32, 64);
+    launch_gemm_a32<true>(c, ta32, tb, ta16, n, k, wr, pl, o, amax);
+  } else {
+    launch_gemm<tc::A_KMAJ_BLK>(c, ta16, tb, n, k, wr, pl, 1, o);
+  }
+  return sl;
+}
+
+// A8 = e4m3(scale_A A16) row-major for rows rows, from the window's amax.
+void to_a8(skema_ctx* c, const __nv_bfloat16* A16, int64_t rows, uint8_t* A8, int64_t ld8, const uint32_t* amax,
+           float* scale_out) {
+  StageScope st(c, ST_WINDOW);
+  const int64_t tiles = ((rows + 63) / 64) * ((c->n + 127) / 128);
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(tiles, c->sm_count * 16));
+  a16_to_a8_kernel<<<grid, 256, 0, c->stream>>>(A16, rows, c->n, A8, ld8, amax, scale_out, c->fp8_map_scale);
+  SKEMA_LAUNCHED(c);
+}
+
+// Rows to process as one [Y | T] product: the M extent gr, with T going to
+// Tdst (ld ldTd), rows weighted nu^(G-1-row/wlen); FP8 scales per wlen rows.
+struct YtSpec {
+  int64_t R0, gr;
+  const __nv_bfloat16* A16;   // row-blocked BF16 (BF16 form)
+  const uint8_t* A8;          // row-major E4M3, ld8 (FP8 form)
+  int64_t ld8;
+  const float* scales;        // FP8: per-window product scales
+  __nv_bfloat16* Tdst;
+  int64_t ldTd;
+  float log2w;
+  int64_t wlen, nwin;
+  float* T32;                 // split-K scratch (ldTd rows per column)
+};
+
+void yt_product(skema_ctx* c, const YtSpec& y) {
   const float eta = (float)c->p.sketch_eta, nu = (float)c->p.sketch_nu;
   const int64_t k = c->k, s = c->s, n = c->n, m = c->m;
+  const bool fp8 = c->p.precision == SKEMA_PREC_FP8;
+  const float ybeta = y_rows_clean(c, y.R0, y.R0 + y.gr) ? 0.f : nu;
+  StageScope st(c, ST_FUSED);
+  const int64_t tiles = ((y.gr + 127) / 128) * ((k + s + kNT - 1) / kNT);
+  Plan pl = plan_split(c, tiles, n, 8);
+  if (fp8) pl = plan_fp8(pl, n);
+  tc::OutSpec o = out_spec();
+  o.p0 = c->Y + y.R0, o.rs0 = 1, o.cs0 = m, o.alpha0 = eta, o.beta0 = ybeta;
+  o.rows = y.gr, o.split = k, o.ncols = k + s;
+  o.row_log2w = y.log2w, o.row_wlen = y.wlen, o.row_nwin = y.nwin;
+  if (!pl.split()) {
+    o.p1 = y.Tdst, o.rs1 = 1, o.cs1 = y.ldTd;
+  } else {
+    scale_block(c, MatOut{c->Y + y.R0, 1, m}, y.gr, k, ybeta);
+    SKEMA_CUDA(cudaMemsetAsync(y.T32, 0, sizeof(float) * (size_t)(y.ldTd * s), c->stream));
+    o.atomic0 = 1, o.beta0 = 0.f;
+    o.p1f = y.T32, o.rs1 = 1, o.cs1 = y.ldTd, o.atomic1 = 1;
+  }
+  if (fp8) {
+    o.scale = y.scales, o.scale_wlen = y.wlen;
+    const CUtensorMap ta = tmap_u8(y.A8, (uint64_t)n, (uint64_t)y.gr, (uint64_t)y.ld8, 128, 128);
+    const CUtensorMap tb = tmap_u8(c->op8, (uint64_t)n, (uint64_t)(k + s), (uint64_t)c->ld_op8, 128, kNT);
+    launch_gemm_fp8(c, ta, tb, y.gr, k + s, n, pl, o);
+  } else {
+    const CUtensorMap ta = tmap_bf16_blocked(y.A16, (uint64_t)n, (uint64_t)((y.gr + 63) / 64), 64);
+    const CUtensorMap tb = tmap_bf16(c->op16, (uint64_t)n, (uint64_t)(k + s), (uint64_t)c->ld_op16 * 2, 64, kNT);
+    launch_gemm<tc::A_MN_BLK>(c, ta, tb, y.gr, k + s, n, pl, 0, o);
+  }
+  if (pl.split()) t32_to_t16(c, y.T32, y.ldTd, y.Tdst, nullptr, y.ldTd, y.gr, s);
+}
+
+}  // namespace
+
+// One window: X^T, [Y | T] and Z. Used for the windows of host-staged calls
+// and for the kernel windows of the FP32 RBF path.
+void tc_dense_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr, void* scratch) {
+  const float nu = (float)c->p.sketch_nu;
+  const int64_t s = c->s, n = c->n;
   const int64_t wp = pad8(wr);
   char* sp = static_cast<char*>(scratch);
   auto take = [&](size_t bytes) {
@@ -617,7 +732,6 @@ void tc_dense_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr, void* scratch
   __nv_bfloat16* A16 = reinterpret_cast<__nv_bfloat16*>(take(sizeof(__nv_bfloat16) * (size_t)(nrb * 64 * n)));
   __nv_bfloat16* T16 = reinterpret_cast<__nv_bfloat16*>(take(sizeof(__nv_bfloat16) * (size_t)(wp * s)));
   float* T32 = reinterpret_cast<float*>(take(sizeof(float) * (size_t)(wp * s)));
-  const float ybeta = y_rows_clean(c, R0, R0 + wr) ? 0.f : nu;
   // FP8 form: the window's amax comes out of the X^T product (or a pass over
   // A16), its power-of-two scale is applied while A16 is rounded to E4M3,
   // and the [Y | T] product runs E4M3 x E4M3 with the scales undone in its
@@ -626,134 +740,86 @@ void tc_dense_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr, void* scratch
   const int64_t ld8 = (n + 15) / 16 * 16;
   uint8_t* A8 = fp8 ? reinterpret_cast<uint8_t*>(take((size_t)(wr * ld8))) : nullptr;
   if (fp8) SKEMA_CUDA(cudaMemsetAsync(c->fp8_win, 0, 2 * sizeof(uint32_t), c->stream));
-
-  // The X^T product reads the FP32 window itself (and writes A16) when TMA
-  // can address it: 16-byte aligned base and stride.
-  const bool al = reinterpret_cast<uintptr_t>(Aw.p) % 16 == 0;
-  const bool a32_cm = al && Aw.rs == 1 && Aw.cs % 4 == 0;
-  const bool a32_rm = al && Aw.cs == 1 && Aw.rs % 4 == 0;
-  if (!a32_cm && !a32_rm) {  // A16 = bf16(A_w), row-blocked, zero rows up to a multiple of 64
-    StageScope st(c, ST_WINDOW);
-    to_bf16_blocked(c, Aw, wr, n, A16);
-    if (fp8) {
-      const int64_t cnt = nrb * 64 * n;
-      const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((cnt + 255) / 256, c->sm_count * 8));
-      amax_a16_kernel<<<grid, 256, 0, c->stream>>>(A16, cnt, c->fp8_win);
-      SKEMA_LAUNCHED(c);
-    }
-  }
-  const TcSlices sl = tc_window_slices(c, R0, wr, &sp);
-  {  // X^T = nu X^T + eta A_w^T Upsilon~_w^T
-    StageScope st(c, ST_UPSILON);
-    const CUtensorMap tb = tmap_bf16(sl.U16, (uint64_t)wr, (uint64_t)k, (uint64_t)sl.ldm * 2, 64, kNT);
-    // stream-K over all SMs: each X^T tile gets one or two partial sums (a
-    // K split into eight ranges gave eight, and their atomics bounded the
-    // product)
-    const Plan pl = plan_streamk(c, c->sm_count);
-    tc::OutSpec o = out_spec();
-    o.p0 = c->X, o.rs0 = 1, o.cs0 = n, o.alpha0 = eta, o.beta0 = nu;
-    o.rows = n, o.split = k, o.ncols = k;
-    if (pl.split()) {
-      scale_block(c, MatOut{c->X, n, 1}, k, n, nu);
-      o.atomic0 = 1, o.beta0 = 0.f;
-    }
-    const CUtensorMap ta16 = tmap_bf16_blocked(A16, (uint64_t)n, (uint64_t)nrb, 128);
-    if (a32_cm) {
-      const CUtensorMap ta32 = tmap_f32(Aw.p, (uint64_t)wr, (uint64_t)n, (uint64_t)Aw.cs * 4, 32, 128);
-      launch_gemm_a32<false>(c, ta32, tb, ta16, n, k, wr, pl, o, fp8 ? c->fp8_win : nullptr);
-    } else if (a32_rm) {
-      const CUtensorMap ta32 = tmap_f32(Aw.p, (uint64_t)n, (uint64_t)wr, (uint64_t)Aw.rs * 4, 32, 64);
-      launch_gemm_a32<true>(c, ta32, tb, ta16, n, k, wr, pl, o, fp8 ? c->fp8_win : nullptr);
-    } else {
-      launch_gemm<tc::A_KMAJ_BLK>(c, ta16, tb, n, k, wr, pl, 1, o);
-    }
-  }
-  if (fp8) {  // A8 = e4m3(scale_A A16), row-major
-    StageScope st(c, ST_WINDOW);
-    const int64_t tiles = nrb * ((n + 127) / 128);
-    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(tiles, c->sm_count * 16));
-    a16_to_a8_kernel<<<grid, 256, 0, c->stream>>>(A16, wr, n, A8, ld8, c->fp8_win, c->fp8_map_scale);
-    SKEMA_LAUNCHED(c);
-  }
-  {  // [Y_w | T] = A16 [Omega~; Psi~]^T  (FP8 form: A8 op8^T, scaled back)
-    StageScope st(c, ST_FUSED);
-    const int64_t tiles = ((wr + 127) / 128) * ((k + s + kNT - 1) / kNT);
-    Plan pl = plan_split(c, tiles, n, 8);
-    if (fp8) pl = plan_fp8(pl, n);
-    tc::OutSpec o = out_spec();
-    o.p0 = c->Y + R0, o.rs0 = 1, o.cs0 = m, o.alpha0 = eta, o.beta0 = ybeta;
-    o.rows = wr, o.split = k, o.ncols = k + s;
-    // T goes to this window's scratch, or (Z deferred) to its rows of the
-    // group's T, weighted nu^(G-1-w) for window w of the group
-    __nv_bfloat16* Tdst = zd ? zd->T16 + (R0 - zd->row0) : T16;
-    const int64_t ldTd = zd ? zd->ldT : wp;
-    if (zd) o.row_log2w = zd->log2nu, o.row_wlen = wr + 1, o.row_nwin = zd->windows - zd->w;
-    if (!pl.split()) {
-      o.p1 = Tdst, o.rs1 = 1, o.cs1 = ldTd;
-    } else {
-      scale_block(c, MatOut{c->Y + R0, 1, m}, wr, k, ybeta);
-      SKEMA_CUDA(cudaMemsetAsync(T32, 0, sizeof(float) * (size_t)(wp * s), c->stream));
-      o.atomic0 = 1, o.beta0 = 0.f;
-      o.p1f = T32, o.rs1 = 1, o.cs1 = wp, o.atomic1 = 1;
-    }
-    if (fp8) {
-      o.scale = reinterpret_cast<const float*>(c->fp8_win + 1);
-      const CUtensorMap ta = tmap_u8(A8, (uint64_t)n, (uint64_t)wr, (uint64_t)ld8, 128, 128);
-      const CUtensorMap tb = tmap_u8(c->op8, (uint64_t)n, (uint64_t)(k + s), (uint64_t)c->ld_op8, 128, kNT);
-      launch_gemm_fp8(c, ta, tb, wr, k + s, n, pl, o);
-    } else {
-      const CUtensorMap ta = tmap_bf16_blocked(A16, (uint64_t)n, (uint64_t)nrb, 64);
-      const CUtensorMap tb =
-          tmap_bf16(c->op16, (uint64_t)n, (uint64_t)(k + s), (uint64_t)c->ld_op16 * 2, 64, kNT);
-      launch_gemm<tc::A_MN_BLK>(c, ta, tb, wr, k + s, n, pl, 0, o);
-    }
-    if (pl.split()) t32_to_t16(c, T32, wp, Tdst, nullptr, ldTd, wr, s);
-  }
+  const TcSlices sl = xt_window(c, Aw, R0, wr, A16, fp8 ? c->fp8_win : nullptr, &sp);
+  float* scale = fp8 ? reinterpret_cast<float*>(c->fp8_win + 1) : nullptr;
+  if (fp8) to_a8(c, A16, wr, A8, ld8, c->fp8_win, scale);
+  YtSpec y{};
+  y.R0 = R0, y.gr = wr, y.A16 = A16, y.A8 = A8, y.ld8 = ld8, y.scales = scale, y.T32 = T32;
+  y.Tdst = T16, y.ldTd = wp, y.log2w = 0.f, y.wlen = wr, y.nwin = 1;
+  yt_product(c, y);
   y_rows_mark(c, R0, R0 + wr);
-  if (!zd) tc_z_update(c, T16, wp, sl, wr, nu);
+  tc_z_update(c, T16, wp, sl, wr, nu);
 }
 
-// The windows of one call with Z deferred: X^T and [Y | T] per window, T of
-// every window into one buffer, then one Z^T product over all the rows of a
-// group of windows -- Z = nu^G Z + eta sum_w nu^(G-1-w) Phi~_w T_w, the
-// per-window recurrence (src/Skema_SketchySVD.cpp:187-189) summed. A Z^T
-// product over K = 8,192 rows per window was atomics-bound; over the call's
-// rows its partial sums are few next to its work. Groups are capped at
-// 512 MB of BF16 T; nu <= 0 (no log2 weight) keeps Z per window.
+// The windows of one call. X^T runs per window (the recurrence X = nu X +
+// eta x_w); [Y | T] and Z run once per group of windows: Y rows are
+// disjoint, so a window's Y rows need only its own product, and Z = nu^G Z
+// + eta sum_w nu^(G-1-w) Phi~_w T_w is the per-window recurrence
+// (src/Skema_SketchySVD.cpp:187-189) summed, with window w's T rows
+// weighted nu^(G-1-w) in the [Y | T] epilogue. One [Y | T] product over
+// tens of thousands of rows needs no K split (its tile count fills the SMs
+// many times over), and one Z^T product over the group avoids a product per
+// window that was bound by its split-K atomics. The group's BF16 (or E4M3)
+// window copies and T are kept: groups are capped at 2 GB of A16 and 512 MB
+// of T. Windows that do not start on 64-row blocks, or nu <= 0, take one
+// window at a time.
 void tc_dense_update(skema_ctx* c, Mat A, int64_t row0, int64_t nrows) {
-  const int64_t W = c->w, s = c->s;
+  const int64_t W = c->w, s = c->s, n = c->n;
   const float nu = (float)c->p.sketch_nu;
-  const int64_t wmax = std::min(W, nrows);
-  const size_t win_bytes = tc_scratch_bytes(c, wmax);
-  if (!(nu > 0.f)) {
-    void* ws = workspace(c, win_bytes);
+  const bool fp8 = c->p.precision == SKEMA_PREC_FP8;
+  if (!(nu > 0.f) || W % 64 != 0 || nrows <= W) {
+    void* ws = workspace(c, tc_scratch_bytes(c, std::min(W, nrows)));
     for (int64_t r = 0; r < nrows; r += W)
-      tc_dense_window(c, Mat{A.p + r * A.rs, A.rs, A.cs}, row0 + r, std::min(W, nrows - r), ws, nullptr);
+      tc_dense_window(c, Mat{A.p + r * A.rs, A.rs, A.cs}, row0 + r, std::min(W, nrows - r), ws);
     return;
   }
-  const int64_t cap_rows = std::max<int64_t>(1, ((int64_t)512 << 20) / (2 * s) / W) * W;
-  const int64_t grows = std::min(nrows, cap_rows);
-  const int64_t ldT = pad8(grows);
-  const size_t t_bytes = (sizeof(__nv_bfloat16) * (size_t)(ldT * s) + 255) / 256 * 256;
-  char* ws = static_cast<char*>(workspace(c, win_bytes + t_bytes + tc_slice_bytes(c, grows) + 256));
-  void* win_scratch = ws;
-  ZDefer zd;
-  zd.T16 = reinterpret_cast<__nv_bfloat16*>(ws + (win_bytes + 255) / 256 * 256);
-  zd.ldT = ldT;
-  zd.log2nu = nu == 1.f ? 0.f : std::log2(nu);
-  char* slice_sp = reinterpret_cast<char*>(zd.T16) + t_bytes;
-  for (int64_t g0 = 0; g0 < nrows; g0 += grows) {
-    const int64_t gr = std::min(grows, nrows - g0);
-    zd.row0 = row0 + g0;
-    zd.windows = (gr + W - 1) / W;
-    for (int64_t w = 0; w < zd.windows; ++w) {
-      zd.w = w;
-      const int64_t r = g0 + w * W;
-      tc_dense_window(c, Mat{A.p + r * A.rs, A.rs, A.cs}, row0 + r, std::min(W, nrows - r), win_scratch, &zd);
+  const int64_t cap_a = ((int64_t)2 << 30) / (2 * n), cap_t = ((int64_t)512 << 20) / (2 * s);
+  const int64_t grows = std::min(nrows, std::max<int64_t>(1, std::min(cap_a, cap_t) / W) * W);
+  const int64_t gwin_max = (grows + W - 1) / W;
+  const int64_t ldT = pad8(grows), ld8 = (n + 15) / 16 * 16;
+  auto rup = [](size_t b) { return (b + 255) / 256 * 256; };
+  const size_t b_a16 = rup(sizeof(__nv_bfloat16) * (size_t)(((grows + 63) / 64) * 64 * n));
+  const size_t b_a8 = fp8 ? rup((size_t)(grows * ld8)) : 0;
+  const size_t b_t16 = rup(sizeof(__nv_bfloat16) * (size_t)(ldT * s));
+  const size_t b_t32 = rup(sizeof(float) * (size_t)(ldT * s));
+  const size_t b_sl = rup(tc_slice_bytes(c, grows)) + rup(tc_slice_bytes(c, W));
+  char* ws = static_cast<char*>(workspace(c, b_a16 + b_a8 + b_t16 + b_t32 + b_sl));
+  __nv_bfloat16* A16 = reinterpret_cast<__nv_bfloat16*>(ws);
+  uint8_t* A8 = reinterpret_cast<uint8_t*>(ws + b_a16);
+  __nv_bfloat16* T16 = reinterpret_cast<__nv_bfloat16*>(ws + b_a16 + b_a8);
+  float* T32 = reinterpret_cast<float*>(ws + b_a16 + b_a8 + b_t16);
+  char* slice_sp = ws + b_a16 + b_a8 + b_t16 + b_t32;
+  uint32_t* amax = nullptr;
+  float* scales = nullptr;
+  if (fp8) {
+    if (c->fp8_win_cap < gwin_max) {
+      if (c->fp8_win) cudaFree(c->fp8_win);
+      SKEMA_CUDA(cudaMalloc(&c->fp8_win, sizeof(uint32_t) * (size_t)(2 * gwin_max)));
+      c->fp8_win_cap = gwin_max;
     }
+    amax = c->fp8_win;
+    scales = reinterpret_cast<float*>(c->fp8_win + gwin_max);
+  }
+  const float log2nu = nu == 1.f ? 0.f : std::log2(nu);
+  for (int64_t g0 = 0; g0 < nrows; g0 += grows) {
+    const int64_t gr = std::min(grows, nrows - g0), G = (gr + W - 1) / W, R0 = row0 + g0;
+    if (!y_rows_clean(c, R0, R0 + gr)) y_materialize(c);
+    if (fp8) SKEMA_CUDA(cudaMemsetAsync(amax, 0, sizeof(uint32_t) * (size_t)(2 * gwin_max), c->stream));
+    for (int64_t w = 0; w < G; ++w) {
+      const int64_t r = g0 + w * W, wr = std::min(W, nrows - r);
+      __nv_bfloat16* A16w = A16 + (w * W / 64) * 64 * n;
+      char* sp = slice_sp + rup(tc_slice_bytes(c, grows));
+      xt_window(c, Mat{A.p + r * A.rs, A.rs, A.cs}, row0 + r, wr, A16w, fp8 ? amax + w : nullptr, &sp);
+      if (fp8) to_a8(c, A16w, wr, A8 + w * W * ld8, ld8, amax + w, scales + w);
+    }
+    YtSpec y{};
+    y.R0 = R0, y.gr = gr, y.A16 = A16, y.A8 = A8, y.ld8 = ld8, y.scales = scales, y.T32 = T32;
+    y.Tdst = T16, y.ldTd = ldT, y.log2w = log2nu, y.wlen = W, y.nwin = G;
+    yt_product(c, y);
+    y_rows_mark(c, R0, R0 + gr);
     char* sp = slice_sp;
-    const TcSlices sl = tc_window_slices(c, zd.row0, gr, &sp);
-    tc_z_update(c, zd.T16, ldT, sl, gr, std::pow(nu, (float)zd.windows));
+    const TcSlices sl = tc_window_slices(c, R0, gr, &sp);
+    tc_z_update(c, T16, ldT, sl, gr, std::pow(nu, (float)G));
   }
 }
 

@@ -127,6 +127,7 @@ struct skema_ctx {
   int64_t ld_op8 = 0;
   float fp8_map_scale = 1.f;
   uint32_t* fp8_win = nullptr;
+  int64_t fp8_win_cap = 1;  // windows fp8_win has room for (amax and scale each)
   // Residual pass (skema_residuals_*): the approximation's U and V as
   // row-major FP64 copies (m x r, n x r), S, the accumulated A^T U (n x r,
   // row-major) and the per-column sums of squares of A V - U S. While
@@ -214,15 +215,9 @@ size_t dense_scratch_bytes(const skema_ctx* c, int64_t wr);
 bool tc_available(const skema_ctx* c);
 void tc_prepare_maps(skema_ctx* c);
 size_t tc_scratch_bytes(const skema_ctx* c, int64_t wr);
-// Z deferred to the end of a group of windows: T of window w (of `windows`)
-// goes to rows [R0 - row0, ...) of T16 (ld ldT), weighted nu^(windows-1-w).
-struct ZDefer {
-  __nv_bfloat16* T16;
-  int64_t ldT, row0, windows, w;
-  float log2nu;
-};
-void tc_dense_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr, void* scratch, const ZDefer* zd = nullptr);
-// All windows of one dense call in the tensor-core forms (Z per group of windows).
+void tc_dense_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr, void* scratch);
+// All windows of one dense call in the tensor-core forms ([Y | T] and Z per
+// group of windows).
 void tc_dense_update(skema_ctx* c, Mat A, int64_t row0, int64_t nrows);
 // Reads the tensor-core status word (synchronises the stream) and fails with
 // SKEMA_ETIMEOUT if a kernel gave up on a wait since the last check.

@@ -72,9 +72,11 @@ struct OutSpec {
   // row_log2w); row_log2w = 0 leaves it unweighted.
   float row_log2w;
   int64_t row_wlen, row_nwin;
-  // When set, alpha0 and alpha1 are multiplied by *scale (a device value
-  // written by an earlier launch: the FP8 form's 1 / (scale_A scale_map)).
+  // When set, alpha0 and alpha1 of row r are multiplied by
+  // scale[r / scale_wlen] (device values written by an earlier launch: the
+  // FP8 form's 1 / (scale_A scale_map) of each window).
   const float* scale;
+  int64_t scale_wlen;
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -305,8 +307,8 @@ __device__ __forceinline__ bool epilogue_unit(const OutSpec& o, uint32_t tmem, u
   const int64_t row = (int64_t)mt * BM + warp * 32 + lane;
   const uint32_t taddr = tmem + acc * TCOLS + ((uint32_t)(warp * 32) << 16);
   float alpha0 = o.alpha0, alpha1 = o.alpha1;
-  if (o.scale) {
-    const float sc = *o.scale;
+  if (o.scale && row < o.rows) {
+    const float sc = o.scale[row / o.scale_wlen];
     alpha0 *= sc;
     alpha1 *= sc;
   }

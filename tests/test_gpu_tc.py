@@ -315,14 +315,17 @@ def test_dense_fp8_window_scale_tracks_amax(sk, oracle):
 
 
 @pytest.mark.parametrize("prec", ["bf16", "fp8"])
-def test_dense_tc_many_windows_one_call_nu(sk, oracle, prec):
-    # a device input of six windows (the last ragged) in one call: Z is formed
-    # once for the call from the windows' T weighted nu^(G-1-w)
+@pytest.mark.parametrize("window", [500, 512])
+def test_dense_tc_many_windows_one_call_nu(sk, oracle, prec, window):
+    # a device input of six windows (the last ragged) in one call. Windows of
+    # 512 rows (64-row blocks) form one group: X^T per window, one [Y | T]
+    # product and one Z^T product for the group, T weighted nu^(G-1-w);
+    # windows of 500 rows take the per-window path
     import torch
 
     m, n = 2900, 700
     A = dense_input(m, n, seed=21).astype(np.float32)
-    a = alg(sk, m, n, 8, 500, 0, sketch_eta=1.25, sketch_nu=0.8)
+    a = alg(sk, m, n, 8, window, 0, sketch_eta=1.25, sketch_nu=0.8)
     a = bf16(a, sk) if prec == "bf16" else fp8(a, sk)
     o = oracle_for(oracle, a)
     if prec == "fp8":
