@@ -96,7 +96,9 @@ Plan plan_split(const skema_ctx* c, int64_t tiles, int64_t K, int max_ks) {
   for (int ks = 1; ks <= max_ks; ++ks) {
     if (ks > 1 && ksteps / ks < 8) break;  // at least 8 k-steps per split
     const int64_t waves = (tiles * ks + c->sm_count - 1) / c->sm_count;
-    const double cost = (double)waves * ((double)ksteps / ks + 6.0);
+    // a split adds atomic partial sums to every output element; their cost
+    // shows as about 12 k-steps per wave
+    const double cost = (double)waves * ((double)ksteps / ks + 6.0 + (ks > 1 ? 12.0 : 0.0));
     if (cost < best_cost * 0.97) {
       best_cost = cost;
       best = ks;
