@@ -56,6 +56,12 @@ enum { SKEMA_PREC_FP32 = 0, SKEMA_PREC_BF16 = 1, SKEMA_PREC_FP8 = 2 };
 enum { SKEMA_UPSILON = 0, SKEMA_OMEGA = 1, SKEMA_PHI = 2, SKEMA_PSI = 3 };
 enum { SKEMA_COL_MAJOR = 0, SKEMA_ROW_MAJOR = 1 };
 enum { SKEMA_MEM_DEVICE = 0, SKEMA_MEM_HOST = 1 };
+/* SketchySPD fixed-rank approximation (src/Skema_SketchySVD.cpp:935-1151):
+ * NYSTROM (default) is the stable fixed-rank Nystrom approximation that the
+ * reference's comments describe; REFERENCE_STEPS repeats the reference's
+ * steps as they run (E from the unshifted Y, eigenvalues less ||Y||_2, and
+ * the SparseSign shift multiplying instead of adding), for parity runs. */
+enum { SKEMA_SPD_NYSTROM = 0, SKEMA_SPD_REFERENCE_STEPS = 1 };
 /* Which sketch, for skema_get_sketch / skema_set_sketch. */
 enum { SKEMA_SKETCH_X = 0, SKEMA_SKETCH_Y = 1, SKEMA_SKETCH_Z = 2 };
 
@@ -81,6 +87,7 @@ typedef struct {
   double kernel_gamma;
   int32_t precision;          /* SKEMA_PREC_* (new)                           */
   int32_t device;             /* CUDA device ordinal                          */
+  int32_t spd_approx;         /* SKEMA_SPD_* (new): SketchySPD approximation  */
 } skema_params;
 
 typedef struct skema_ctx skema_ctx;
@@ -150,7 +157,13 @@ int skema_linear_update_rbf(skema_ctx* ctx, const float* pts, int64_t ld,
  * CholeskyQR2 in place of dgeqrf/dorgqr, triangular solves in place of the
  * dgels calls on T1/T2, and a one-sided Jacobi SVD in place of dgesvd.
  * Outputs: U (m x rank), S (rank), V (n x rank), column-major. Singular
- * vectors equal LAPACK's up to sign. Any output pointer may be NULL. */
+ * vectors equal LAPACK's up to sign. Any output pointer may be NULL.
+ * SketchySPD contexts: SketchySPD::low_rank_approx
+ * (src/Skema_SketchySVD.cpp:935-1151) per params.spd_approx, returning the
+ * eigenvectors in U (m x rank) and eigenvalues in S; V is not used. A
+ * Cholesky factor that does not exist fails with SKEMA_ENOTPD (the
+ * reference exits there). The sketch Y is left unchanged (the reference
+ * overwrites it with E). */
 int skema_low_rank_approx(skema_ctx* ctx, double* U, double* S, double* V,
                           int32_t mem);
 

@@ -287,6 +287,45 @@ class OracleSketch:
         assert C.shape == (k, k)
         return Q, C, P
 
+    def spd_low_rank_approx(self, nystrom=False):
+        """(U, S) of SketchySPD::low_rank_approx (src/Skema_SketchySVD.cpp:
+        935-1151), FP64, from the Y sketch and the stored Omega (n x k).
+        nystrom=False follows the reference's steps as they run:
+          nu = ||Y||_2; eta = eps * ||Y||_2 (the reference takes this second
+          norm of a buffer dgesvd has already overwritten, :964-965, so its
+          value depends on the LAPACK build; it enters only at the level of
+          eps); Y_eta = Y + eta Omega (Gauss axpy), or for SparseSign each
+          stored entry of Omega multiplies its Y entry by eta * sign
+          (SparseSignDimRedux::axpy, src/Skema_DimRedux_SparseSign.cpp:
+          113-123, `*=`); B = Omega^T Y_eta; R^T R = (B + B^T) / 2 (dpotrf
+          'U'); E = Y R^{-1} from the unshifted Y (:1094-1103); U S V^T =
+          svd(E); S_j <- max(0, S_j^2 - nu) (:1145-1147).
+        nystrom=True is the fixed-rank Nystrom approximation the reference's
+        comments describe (Tropp, Yurtsever, Udell and Cevher, 2017): the
+        shift eta = eps ||Y||_2 is added as Y_eta = Y + eta Omega for both
+        map kinds, E = Y_eta R^{-1}, and S_j <- max(0, S_j^2 - eta)."""
+        import scipy.linalg as sla
+
+        Y = np.asarray(self.Y, dtype=np.float64)
+        om = self.maps["omega"]
+        Om = np.asarray(om.dense, dtype=np.float64)
+        nu = np.linalg.svd(Y, compute_uv=False)[0]
+        eta = np.finfo(np.float64).eps * nu
+        Ye = Y.copy()
+        if not nystrom and om.kind == 1:
+            for i in range(om.nrow):
+                for cidx, v in zip(om.idx[i], om.val[i]):
+                    Ye[i, cidx] *= eta * v
+        else:
+            Ye += eta * Om
+        B = Om.T @ Ye
+        R = sla.cholesky(0.5 * (B + B.T), lower=False)
+        E = sla.solve_triangular(R, (Ye if nystrom else Y).T, trans="T", lower=False).T
+        U, S, _ = np.linalg.svd(E, full_matrices=False)
+        r = self.rank
+        sub = eta if nystrom else nu
+        return U[:, :r], np.maximum(0.0, S[:r] ** 2 - sub)
+
     def low_rank_approx(self):
         """(U, S, V) of src/Skema_SketchySVD.cpp:569-664 (dgesvd)."""
         Q, C, P = self.initial_approx()

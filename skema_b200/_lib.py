@@ -21,6 +21,7 @@ STATUS_NAMES = {
 MAP_GAUSS, MAP_SPARSE_SIGN = 0, 1
 KERNEL_NONE, KERNEL_GAUSSRBF = 0, 1
 PREC_FP32, PREC_BF16, PREC_FP8 = 0, 1, 2
+SPD_NYSTROM, SPD_REFERENCE_STEPS = 0, 1
 UPSILON, OMEGA, PHI, PSI = 0, 1, 2, 3
 COL_MAJOR, ROW_MAJOR = 0, 1
 MEM_DEVICE, MEM_HOST = 0, 1
@@ -56,6 +57,7 @@ class Params(C.Structure):
         ("kernel_gamma", C.c_double),
         ("precision", C.c_int32),
         ("device", C.c_int32),
+        ("spd_approx", C.c_int32),
     ]
 
 

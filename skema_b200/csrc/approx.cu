@@ -22,6 +22,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <limits>
 #include <vector>
 
 #include "internal.h"
@@ -473,7 +474,150 @@ void apply_map(skema_ctx* c, const Map& mp, const double* Qm, int64_t cols, int6
   }
 }
 
+// ---- SketchySPD pieces -----------------------------------------------------
+// Stored SparseSign rows (zeta entries: column | sign << 31) -> dense n x k
+// (column-major, ld n, zeroed beforehand); duplicate entries add up.
+__global__ void ssign_dense_kernel(const uint32_t* __restrict__ packed, int zeta, int64_t n, double* __restrict__ D) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    for (int t = 0; t < zeta; ++t) {
+      const uint32_t w = packed[i * zeta + t];
+      D[i + (int64_t)(w & 0x7fffffffu) * n] += (w >> 31) ? -1.0 : 1.0;
+    }
+}
+// SparseSignDimRedux::axpy as the reference runs it (`*=`): each stored entry
+// multiplies its Y entry by eta * sign, a duplicate entry twice.
+__global__ void ssign_scale_kernel(const uint32_t* __restrict__ packed, int zeta, int64_t n, double* __restrict__ Y,
+                                   int64_t ldy, double eta) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    for (int t = 0; t < zeta; ++t) {
+      const uint32_t w = packed[i * zeta + t];
+      Y[i + (int64_t)(w & 0x7fffffffu) * ldy] *= eta * ((w >> 31) ? -1.0 : 1.0);
+    }
+}
+__global__ void daxpy_kernel(double* __restrict__ Y, const double* __restrict__ X, int64_t cnt, double a) {
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < cnt; q += (int64_t)gridDim.x * blockDim.x)
+    Y[q] += a * X[q];
+}
+// C = (B + B^T) / 2, column-major k x k.
+__global__ void symmetrize_kernel(const double* __restrict__ B, double* __restrict__ C, int64_t k) {
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < k * k; q += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = q % k, j = q / k;
+    C[q] = 0.5 * (B[i + j * k] + B[j + i * k]);
+  }
+}
+// out_j = max(0, S_j^2 - sub): squared singular values of E less the shift.
+__global__ void spd_eig_kernel(const double* __restrict__ S, double* __restrict__ out, int64_t r, double sub) {
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < r; j += (int64_t)gridDim.x * blockDim.x)
+    out[j] = fmax(0.0, S[j] * S[j] - sub);
+}
+
 }  // namespace
+
+// SketchySPD::low_rank_approx (src/Skema_SketchySVD.cpp:935-1151) in FP64 on
+// the device, with Omega the stored n x k map and Y the m x k sketch (m = n):
+//   nu = ||Y||_2 (from the largest eigenvalue of Y^T Y), eta = eps nu
+//   Y_eta = Y + eta Omega   (REFERENCE_STEPS with SparseSign: each stored map
+//                            entry multiplies its Y entry by eta * sign)
+//   B = Omega^T Y_eta, R^T R = (B + B^T) / 2 (upper Cholesky, as dpotrf 'U')
+//   E = Y_eta R^{-1}        (REFERENCE_STEPS: the unshifted Y, :1094-1103)
+//   U S V^T = svd(E)        (CholeskyQR2 of E, then a Jacobi SVD of its R)
+//   U <- U(:, 1:r), S_j <- max(0, S_j^2 - eta)   (REFERENCE_STEPS: - nu)
+// The reference takes eta from the norm of a buffer dgesvd has already
+// overwritten (:964-965), a value that depends on the LAPACK build; here eta
+// is eps ||Y||_2, the value its comment states. It enters at the level of eps.
+void spd_low_rank_approx(skema_ctx* c, double* Uout, double* Sout) {
+  const int64_t m = c->m, n = c->n, k = c->k, r = c->p.rank;
+  const bool ref_steps = c->p.spd_approx == SKEMA_SPD_REFERENCE_STEPS;
+  const Map& O = c->omg;
+  y_materialize(c);
+  DevBuf bY(sizeof(double) * (size_t)(m * k));
+  DevBuf bYe(sizeof(double) * (size_t)(m * k));
+  DevBuf bO(sizeof(double) * (size_t)(n * k));
+  DevBuf bW(sizeof(double) * cholqr_work_doubles(m, k));
+  DevBuf bsmall(sizeof(double) * (size_t)(8 * k * k + 4 * k + 64));
+  DevBuf bstat(sizeof(int) * 4);
+  double* Yd = bY.d();
+  double* Ye = bYe.d();
+  double* Od = bO.d();
+  double* W = bW.d();
+  double* G = bsmall.d();       // k x k
+  double* R = G + k * k;        // k x k
+  double* Rinv = R + k * k;     // k x k
+  double* Cw = Rinv + k * k;    // k x k
+  double* Vc = Cw + k * k;      // k x k
+  double* Uc = Vc + k * k;      // k x k
+  double* Vt = Uc + k * k;      // k x k
+  double* RE = Vt + k * k;      // k x k
+  double* Sv = RE + k * k;      // k
+  double* sig = Sv + k;         // k
+  int* st = (int*)bstat.p;
+
+  f2d_kernel<<<g1(c, m * k), 256, 0, c->stream>>>(c->Y, 1, m, Yd, 1, m, m, k);
+  SKEMA_LAUNCHED(c);
+  if (O.kind == SKEMA_MAP_GAUSS) {
+    // stored (i, j) = logical (j, i)
+    f2d_kernel<<<g1(c, n * k), 256, 0, c->stream>>>(O.f32, O.cs, O.rs, Od, 1, n, n, k);
+  } else {
+    SKEMA_CUDA(cudaMemsetAsync(Od, 0, sizeof(double) * (size_t)(n * k), c->stream));
+    ssign_dense_kernel<<<g1(c, n), 256, 0, c->stream>>>(O.packed, O.zeta, n, Od);
+  }
+  SKEMA_LAUNCHED(c);
+
+  // nu = ||Y||_2 = sqrt(lambda_max(Y^T Y))
+  dgemm<double, double>(c, k, k, m, 1.0, Yd, m, 1, Yd, 1, m, 0.0, G, 1, k);
+  jacobi_svd_kernel<<<1, 1024, 0, c->stream>>>(G, Vc, k, 60, 1e-15, st + 1);
+  SKEMA_LAUNCHED(c);
+  svd_finish_kernel<<<1, 256, 0, c->stream>>>(G, Vc, k, Uc, Vt, Sv, sig);
+  SKEMA_LAUNCHED(c);
+  double lmax = 0.0;
+  SKEMA_CUDA(cudaMemcpyAsync(&lmax, Sv, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  SKEMA_CUDA(cudaStreamSynchronize(c->stream));
+  const double nu = std::sqrt(std::max(lmax, 0.0));
+  const double eta = std::numeric_limits<double>::epsilon() * nu;
+
+  // Y_eta
+  SKEMA_CUDA(cudaMemcpyAsync(Ye, Yd, sizeof(double) * (size_t)(m * k), cudaMemcpyDeviceToDevice, c->stream));
+  if (ref_steps && O.kind == SKEMA_MAP_SPARSE_SIGN) {
+    ssign_scale_kernel<<<g1(c, n), 256, 0, c->stream>>>(O.packed, O.zeta, n, Ye, m, eta);
+  } else {
+    daxpy_kernel<<<g1(c, m * k), 256, 0, c->stream>>>(Ye, Od, m * k, eta);
+  }
+  SKEMA_LAUNCHED(c);
+  // B = Omega^T Y_eta; R^T R = (B + B^T) / 2
+  dgemm<double, double>(c, k, k, n, 1.0, Od, n, 1, Ye, 1, m, 0.0, Cw, 1, k);
+  symmetrize_kernel<<<g1(c, k * k), 256, 0, c->stream>>>(Cw, G, k);
+  SKEMA_LAUNCHED(c);
+  cholesky_kernel<<<1, 1024, 0, c->stream>>>(G, k, st);
+  SKEMA_LAUNCHED(c);
+  int bad = 0;
+  SKEMA_CUDA(cudaMemcpyAsync(&bad, st, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  SKEMA_CUDA(cudaStreamSynchronize(c->stream));
+  if (bad != 0) fail(SKEMA_ENOTPD, "SketchySPD: (B + B^T) / 2 is not positive definite (dpotrf would fail)");
+  lower_to_upper_kernel<<<g1(c, k * k), 256, 0, c->stream>>>(G, R, k);
+  SKEMA_LAUNCHED(c);
+  identity_kernel<<<g1(c, k * k), 256, 0, c->stream>>>(Rinv, k);
+  SKEMA_LAUNCHED(c);
+  trsm_upper_kernel<<<(int)((k * 32 + 255) / 256), 256, 0, c->stream>>>(R, k, Rinv, k, k);
+  SKEMA_LAUNCHED(c);
+  // E = (Y_eta or Y) R^{-1}, into Yd's buffer when it is no longer needed
+  double* E = ref_steps ? Ye : Yd;
+  const double* src = ref_steps ? Yd : Ye;
+  dgemm<double, double>(c, m, k, k, 1.0, src, 1, m, Rinv, 1, k, 0.0, E, 1, m, false);
+  // svd(E) = Q svd(R_E)
+  cholqr(c, E, m, k, RE, W, st);
+  SKEMA_CUDA(cudaMemcpyAsync(Cw, RE, sizeof(double) * (size_t)(k * k), cudaMemcpyDeviceToDevice, c->stream));
+  jacobi_svd_kernel<<<1, 1024, 0, c->stream>>>(Cw, Vc, k, 60, 1e-15, st + 1);
+  SKEMA_LAUNCHED(c);
+  svd_finish_kernel<<<1, 256, 0, c->stream>>>(Cw, Vc, k, Uc, Vt, Sv, sig);
+  SKEMA_LAUNCHED(c);
+  if (Uout) dgemm<double, double>(c, m, r, k, 1.0, E, 1, m, Uc, 1, k, 0.0, Uout, 1, m, false);
+  if (Sout) {
+    spd_eig_kernel<<<1, 256, 0, c->stream>>>(Sv, Sout, r, ref_steps ? nu : eta);
+    SKEMA_LAUNCHED(c);
+  }
+  // the DevBufs are released at return: wait for the work that reads them
+  SKEMA_CUDA(cudaStreamSynchronize(c->stream));
+}
 
 void dgemm_f32_f64(skema_ctx* c, int64_t M, int64_t N, int64_t K, double alpha, const float* A, int64_t ars,
                    int64_t acs, const double* B, int64_t brs, int64_t bcs, double beta, double* C, int64_t crs,

@@ -275,6 +275,7 @@ int skema_params_init(skema_params* p) {
   p->kernel_gamma = 1.0;
   p->precision = SKEMA_PREC_FP32;
   p->device = 0;
+  p->spd_approx = SKEMA_SPD_NYSTROM;
   return SKEMA_OK;
 }
 
@@ -501,8 +502,29 @@ int skema_linear_update_rbf(skema_ctx* c, const float* pts, int64_t ld, int32_t 
 
 int skema_low_rank_approx(skema_ctx* c, double* U, double* S, double* V, int32_t mem) {
   return guarded(c, [&] {
-    if (c->spd) fail(SKEMA_EUNSUPPORTED, "the SketchySPD fixed-rank approximation is not provided");
     if (mem != SKEMA_MEM_DEVICE && mem != SKEMA_MEM_HOST) fail(SKEMA_EINVAL, "bad mem kind");
+    if (c->spd) {
+      if (c->p.spd_approx != SKEMA_SPD_NYSTROM && c->p.spd_approx != SKEMA_SPD_REFERENCE_STEPS)
+        fail(SKEMA_EINVAL, "spd_approx must be SKEMA_SPD_NYSTROM or SKEMA_SPD_REFERENCE_STEPS");
+      if (c->m != c->n) fail(SKEMA_EINVAL, "SketchySPD needs a square matrix");
+      if (c->k > c->m) fail(SKEMA_EINVAL, "range must not exceed the matrix size");
+      if (c->p.rank > c->k) fail(SKEMA_EINVAL, "rank must not exceed range");
+      check_device_error(c);
+      const int64_t r = c->p.rank;
+      if (mem == SKEMA_MEM_DEVICE) {
+        spd_low_rank_approx(c, U, S);
+        return;
+      }
+      const size_t ub = sizeof(double) * (size_t)(c->m * r);
+      char* buf = (char*)staging(c, ub + sizeof(double) * (size_t)r + 512);
+      double* dU = (double*)buf;
+      double* dS = (double*)(buf + (ub + 255) / 256 * 256);
+      spd_low_rank_approx(c, U ? dU : nullptr, S ? dS : nullptr);
+      if (U) SKEMA_CUDA(cudaMemcpyAsync(U, dU, ub, cudaMemcpyDeviceToHost, c->stream));
+      if (S) SKEMA_CUDA(cudaMemcpyAsync(S, dS, sizeof(double) * (size_t)r, cudaMemcpyDeviceToHost, c->stream));
+      SKEMA_CUDA(cudaStreamSynchronize(c->stream));
+      return;
+    }
     if (c->k > c->n || c->k > c->m) fail(SKEMA_EINVAL, "range must not exceed min(m, n)");
     if (c->s < c->k) fail(SKEMA_EINVAL, "core must be >= range");
     const int64_t r = c->p.rank;

@@ -251,6 +251,8 @@ void rbf_vjp(skema_ctx* c, const float* pts, int64_t N, int64_t d,
 
 // ---- FP64 approximation (approx.cu) ----
 void low_rank_approx(skema_ctx* c, double* U, double* S, double* V);
+// SketchySPD: U (m x rank, column-major) and S (rank), device pointers (either may be NULL).
+void spd_low_rank_approx(skema_ctx* c, double* U, double* S);
 // C = alpha A B + beta C in FP64 (A FP32, exact in FP64), strided operands.
 void dgemm_f32_f64(skema_ctx* c, int64_t M, int64_t N, int64_t K, double alpha, const float* A, int64_t ars,
                    int64_t acs, const double* B, int64_t brs, int64_t bcs, double beta, double* C, int64_t crs,

@@ -181,6 +181,7 @@ DIM_REDUX_NAMES = ["gauss", "sparse-sign"]      # src/Skema_Utils.hpp:74-80
 KERNEL_NAMES = ["none", "gaussrbf"]              # src/Skema_Utils.hpp:60-66
 SOLVER_NAMES = ["isvd", "sketch", "primme"]      # src/Skema_Utils.hpp:46-52
 PRECISION_NAMES = ["fp32", "bf16", "fp8"]
+SPD_APPROX_NAMES = ["nystrom", "reference-steps"]
 
 
 @dataclass
@@ -213,6 +214,7 @@ class AlgParams:
     kernel_gamma: float = 1.0
     precision: int = L.PREC_FP32
     device: int = 0
+    spd_approx: int = L.SPD_NYSTROM
 
     def parse(self, args: list[str]) -> None:
         """Consume the sketch flags from args, as AlgParams::parse does."""
@@ -242,6 +244,7 @@ class AlgParams:
         self.kernel_func = parse_enum(args, "--kernel", L.KERNEL_NONE, KERNEL_NAMES)
         self.kernel_gamma = parse_real(args, "--gamma", self.kernel_gamma, 0.0, math.inf)
         self.precision = parse_enum(args, "--precision", L.PREC_FP32, PRECISION_NAMES)
+        self.spd_approx = parse_enum(args, "--spd-approx", L.SPD_NYSTROM, SPD_APPROX_NAMES)
 
     def to_c(self) -> L.Params:
         p = L.default_params()
@@ -264,6 +267,7 @@ class AlgParams:
         p.kernel_gamma = float(self.kernel_gamma)
         p.precision = int(self.precision)
         p.device = int(self.device)
+        p.spd_approx = int(self.spd_approx)
         return p
 
 
@@ -544,10 +548,34 @@ class SketchySVD(_Context):
 
 
 class SketchySPD(_Context):
-    """SketchySPD<MatrixType, DimReduxT> update (src/Skema_SketchySVD.hpp:67-108)."""
+    """SketchySPD<MatrixType, DimReduxT> (src/Skema_SketchySVD.hpp:67-108)."""
 
     def get_sketches(self):
         return self.get_sketch(L.SKETCH_Y)
+
+    def low_rank_approx(self, device_out=None):
+        """SketchySPD::low_rank_approx (src/Skema_SketchySVD.cpp:935-1151):
+        (U m x r eigenvectors, S r eigenvalues), FP64, as chosen by
+        AlgParams.spd_approx. device_out: optional (U, S) CUDA float64
+        tensors (column-major U) to fill in place."""
+        r = self.rank
+        if device_out is not None:
+            U, S = device_out
+            self._check(self.lib.skema_low_rank_approx(self.h, U.data_ptr(), S.data_ptr(), None, L.MEM_DEVICE))
+            return U, S
+        U = np.empty((r, self.nrow), dtype=np.float64)
+        S = np.empty(r, dtype=np.float64)
+        self._check(self.lib.skema_low_rank_approx(self.h, U.ctypes.data, S.ctypes.data, None, L.MEM_HOST))
+        self.uvecs, self.svals, self.vvecs = U.T, S, None
+        return U.T, S
+
+    def compute_residuals(self, A):
+        """SketchySPD::compute_residuals (src/Skema_SketchySVD.cpp:1206-1213):
+        ||(A U - U S)(:, j)||_2 for the last low_rank_approx."""
+        if getattr(self, "uvecs", None) is None:
+            raise SkemaError(L.ESTATE, "compute_residuals needs a low_rank_approx first")
+        self.rnrms = self.residuals(A, None, self.svals, self.uvecs)
+        return self.rnrms
 
 
 def write_history(path, svals, rnrms, update_seconds=None):
@@ -573,11 +601,18 @@ def write_history(path, svals, rnrms, update_seconds=None):
 
 
 def sketchysvd(matrix, alg: AlgParams):
-    """Skema::sketchysvd (src/Skema_SketchySVD.cpp:1244-1405, 1408-1577),
-    three-sketch branch: returns (U, S, V)."""
-    with SketchySVD(alg) as sk:
+    """Skema::sketchysvd (src/Skema_SketchySVD.cpp:1244-1405, 1408-1577):
+    update, fixed-rank approximation, residuals and (with history_filename)
+    the history file. Returns (U, S, V); the SketchySPD branch (issymmetric
+    without force_three_sketch) returns (U, S, None), S the eigenvalues."""
+    spd = bool(alg.issymmetric) and not bool(alg.force_three_sketch)
+    with (SketchySPD if spd else SketchySVD)(alg) as sk:
         sk.linear_update(matrix)
-        U, S, V = sk.low_rank_approx()
+        if spd:
+            U, S = sk.low_rank_approx()
+            V = None
+        else:
+            U, S, V = sk.low_rank_approx()
         sk.compute_residuals(matrix)
         if getattr(alg, "history_filename", ""):
             sk.save_history(alg.history_filename)

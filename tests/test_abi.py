@@ -114,3 +114,14 @@ def test_algparams_parse_errors():
         AlgParams().parse(["--seeds", "1,2"])
     with pytest.raises(RuntimeError):
         AlgParams().parse(["--window", "abc"])
+
+
+def test_spd_approx_flag():
+    from skema_b200 import _lib as L
+    from skema_b200.sketchy import AlgParams
+
+    a = AlgParams()
+    assert a.spd_approx == L.SPD_NYSTROM and L.default_params().spd_approx == L.SPD_NYSTROM
+    args = ["--spd-approx", "reference-steps"]
+    a.parse(args)
+    assert a.spd_approx == L.SPD_REFERENCE_STEPS and a.to_c().spd_approx == L.SPD_REFERENCE_STEPS

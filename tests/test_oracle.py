@@ -4,6 +4,8 @@ Pins: the Random123 known-answer vectors of Philox4x32-10 (the generator
 both the oracle and the library use), and the reference's own fixtures
 (test/data/*_svals.txt) reproduced end to end by the oracle's SketchySVD.
 """
+import os
+
 import numpy as np
 import pytest
 import scipy.sparse as sp
@@ -177,3 +179,33 @@ def test_residuals_restatement_pins():
     assert np.allclose(O.residuals(Asp, Up, Sp, Vp, window=32), O.residuals(Asp.toarray(), Up, Sp, Vp), rtol=1e-13)
     B = A[:40] @ A[:40].T
     assert np.allclose(O.residuals(B, None, Sp, Vp), np.linalg.norm(B @ Vp - Vp * Sp, axis=0), rtol=1e-13)
+
+
+def test_spd_approx_restatement_pins():
+    """SketchySPD::low_rank_approx (src/Skema_SketchySVD.cpp:935-1151)
+    restated. The Nystrom form recovers the reference's kernel fixture
+    (25 points, gamma = 1) exactly with a full-range sketch and to ~1e-6 with
+    k = 21; the reference's own steps subtract ||Y||_2 from the squared
+    singular values, which leaves nothing of this spectrum, and its
+    SparseSign shift (`*=` in SparseSignDimRedux::axpy) leaves (B + B^T) / 2
+    indefinite here."""
+    from oracle import sketchy_oracle as O
+
+    d = np.load(os.path.join(os.path.dirname(__file__), "golden", "kat_fixtures.npz"))
+    X = d["kernel_points"].astype(np.float64)
+    sv = d["kernel_svals"]
+    N = X.shape[0]
+    for k, tol in ((25, 1e-12), (21, 2e-6)):
+        for kind in (0, 1):
+            o = O.OracleSketch(N, N, 5, N, kind=kind, sketch_range=k, spd=True, kernel_gamma=1.0)
+            o.linear_update(X)
+            U, S = o.spd_low_rank_approx(nystrom=True)
+            assert np.max(np.abs(S - sv[:5]) / sv[:5]) < tol, (k, kind, S)
+            assert np.allclose(U.T @ U, np.eye(5), atol=1e-10)
+    o = O.OracleSketch(N, N, 5, N, kind=0, sketch_range=25, spd=True, kernel_gamma=1.0)
+    o.linear_update(X)
+    assert np.all(o.spd_low_rank_approx(nystrom=False)[1] == 0.0)
+    o = O.OracleSketch(N, N, 5, N, kind=1, sketch_range=25, spd=True, kernel_gamma=1.0)
+    o.linear_update(X)
+    with pytest.raises(np.linalg.LinAlgError):
+        o.spd_low_rank_approx(nystrom=False)
