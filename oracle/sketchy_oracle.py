@@ -303,14 +303,17 @@ class OracleSketch:
         nystrom=True is the fixed-rank Nystrom approximation the reference's
         comments describe (Tropp, Yurtsever, Udell and Cevher, 2017): the
         shift eta = eps ||Y||_2 is added as Y_eta = Y + eta Omega for both
-        map kinds, E = Y_eta R^{-1}, and S_j <- max(0, S_j^2 - eta)."""
+        map kinds, E = Y_eta R^{-1}, and S_j <- max(0, S_j^2 - eta). Its eps
+        is the FP32 machine epsilon, the precision the library holds Y in
+        (the reference holds Y in FP64 and uses the FP64 epsilon); the
+        reference's steps keep the FP64 epsilon."""
         import scipy.linalg as sla
 
         Y = np.asarray(self.Y, dtype=np.float64)
         om = self.maps["omega"]
         Om = np.asarray(om.dense, dtype=np.float64)
         nu = np.linalg.svd(Y, compute_uv=False)[0]
-        eta = np.finfo(np.float64).eps * nu
+        eta = float(np.finfo(np.float32 if nystrom else np.float64).eps) * nu
         Ye = Y.copy()
         if not nystrom and om.kind == 1:
             for i in range(om.nrow):

@@ -515,7 +515,7 @@ __global__ void spd_eig_kernel(const double* __restrict__ S, double* __restrict_
 
 // SketchySPD::low_rank_approx (src/Skema_SketchySVD.cpp:935-1151) in FP64 on
 // the device, with Omega the stored n x k map and Y the m x k sketch (m = n):
-//   nu = ||Y||_2 (from the largest eigenvalue of Y^T Y), eta = eps nu
+//   nu = ||Y||_2 (from the largest eigenvalue of Y^T Y), eta = eps nu (below)
 //   Y_eta = Y + eta Omega   (REFERENCE_STEPS with SparseSign: each stored map
 //                            entry multiplies its Y entry by eta * sign)
 //   B = Omega^T Y_eta, R^T R = (B + B^T) / 2 (upper Cholesky, as dpotrf 'U')
@@ -523,8 +523,11 @@ __global__ void spd_eig_kernel(const double* __restrict__ S, double* __restrict_
 //   U S V^T = svd(E)        (CholeskyQR2 of E, then a Jacobi SVD of its R)
 //   U <- U(:, 1:r), S_j <- max(0, S_j^2 - eta)   (REFERENCE_STEPS: - nu)
 // The reference takes eta from the norm of a buffer dgesvd has already
-// overwritten (:964-965), a value that depends on the LAPACK build; here eta
-// is eps ||Y||_2, the value its comment states. It enters at the level of eps.
+// overwritten (:964-965), a value that depends on the LAPACK build; its
+// steps here use eps ||Y||_2, the value its comment states, which enters at
+// the level of eps. The Nystrom form shifts by the FP32 epsilon times
+// ||Y||_2, because Y is held in FP32: a shift below the rounding of Y leaves
+// B indefinite for spectra that decay to zero.
 void spd_low_rank_approx(skema_ctx* c, double* Uout, double* Sout) {
   const int64_t m = c->m, n = c->n, k = c->k, r = c->p.rank;
   const bool ref_steps = c->p.spd_approx == SKEMA_SPD_REFERENCE_STEPS;
@@ -573,7 +576,10 @@ void spd_low_rank_approx(skema_ctx* c, double* Uout, double* Sout) {
   SKEMA_CUDA(cudaMemcpyAsync(&lmax, Sv, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   SKEMA_CUDA(cudaStreamSynchronize(c->stream));
   const double nu = std::sqrt(std::max(lmax, 0.0));
-  const double eta = std::numeric_limits<double>::epsilon() * nu;
+  // the Nystrom shift covers the rounding of Y, which is held in FP32 here
+  // (the reference holds Y in FP64 and shifts by the FP64 epsilon)
+  const double eta =
+      (ref_steps ? std::numeric_limits<double>::epsilon() : (double)std::numeric_limits<float>::epsilon()) * nu;
 
   // Y_eta
   SKEMA_CUDA(cudaMemcpyAsync(Ye, Yd, sizeof(double) * (size_t)(m * k), cudaMemcpyDeviceToDevice, c->stream));
