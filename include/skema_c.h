@@ -109,7 +109,7 @@ int skema_create(const skema_params* p, skema_ctx** out);
 int skema_destroy(skema_ctx* ctx);
 
 /* Message of the last failed call on ctx ("" if none). A NULL ctx returns the
- * message of the last failed skema_create on this thread. */
+ * message of the last failed skema_create or file call on this thread. */
 const char* skema_last_error(const skema_ctx* ctx);
 
 /* Resolved sketch sizes (range k, core s) and whether the context runs the
@@ -248,6 +248,39 @@ int skema_rbf_sketch_vjp(skema_ctx* ctx, const float* pts, int64_t npts,
 int skema_rbf_sketch_fwd_noalloc(skema_ctx* ctx, const float* pts,
                                  int64_t npts, int64_t d, double gamma,
                                  const float* omega, int64_t k, float* Y);
+
+/* ---- matrix files ----------------------------------------------------- */
+/* Skema::read_matrix / write_matrix (src/Skema_IO.hpp:10-40,
+ * src/Skema_IO.cpp:8-104), chosen by the file extension. Arrays returned by
+ * the readers are allocated with malloc and released by the *_free calls.
+ *   .mtx dense: MatrixMarket "matrix array" (column-major values);
+ *   .mtx CRS:   MatrixMarket "matrix coordinate" (1-based; symmetric and
+ *               skew-symmetric files expanded; pattern entries 1), as
+ *               KokkosKernels' read_kokkos_crst_matrix reads it;
+ *   .bin CRS:   int32 nrows, int64 nnz, uint64 row_map[nrows+1],
+ *               int32 entries[nnz], float64 values[nnz]; ncol = nrows
+ *               unless a column index is larger. A dense .bin is rejected
+ *               (SKEMA_EUNSUPPORTED), as in the reference.
+ * CRS rows come back sorted by column with duplicate entries summed. Errors
+ * are reported by skema_last_error(NULL). The values are FP64, as the
+ * reference reads them; the update entry points take FP32. */
+typedef struct {
+  int64_t nrow, ncol, nnz;
+  int64_t* rowptr; /* nrow + 1 entries, rowptr[0] = 0 */
+  int32_t* col;
+  double* val;
+} skema_crs;
+typedef struct {
+  int64_t nrow, ncol;
+  double* data; /* column-major, nrow * ncol */
+} skema_dense;
+int skema_read_crs(const char* path, skema_crs* out);
+void skema_crs_free(skema_crs* a);
+int skema_read_dense(const char* path, skema_dense* out);
+void skema_dense_free(skema_dense* a);
+/* write_mtx / write_bin for CRS (src/Skema_IO.cpp:88-104): a .mtx file is
+ * written as "coordinate real general" with 17 significant digits. */
+int skema_write_crs(const char* path, const skema_crs* a);
 
 /* Wait for all work queued on ctx's stream. */
 int skema_synchronize(skema_ctx* ctx);

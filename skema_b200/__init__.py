@@ -9,7 +9,9 @@ from .sketchy import (
     SparseSignDimRedux,
     rbf_sketch_fwd,
     rbf_sketch_vjp,
+    read_matrix,
     sketchysvd,
+    write_matrix,
 )
 
 __all__ = [
@@ -19,6 +21,8 @@ __all__ = [
     "SketchySVD",
     "SketchySPD",
     "sketchysvd",
+    "read_matrix",
+    "write_matrix",
     "rbf_sketch_fwd",
     "rbf_sketch_vjp",
     "SkemaError",

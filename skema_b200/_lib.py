@@ -61,6 +61,19 @@ class Params(C.Structure):
     ]
 
 
+class Crs(C.Structure):
+    """``skema_crs``: a CRS matrix returned by skema_read_crs."""
+
+    _fields_ = [("nrow", C.c_int64), ("ncol", C.c_int64), ("nnz", C.c_int64),
+                ("rowptr", C.POINTER(C.c_int64)), ("col", C.POINTER(C.c_int32)), ("val", C.POINTER(C.c_double))]
+
+
+class Dense(C.Structure):
+    """``skema_dense``: a column-major matrix returned by skema_read_dense."""
+
+    _fields_ = [("nrow", C.c_int64), ("ncol", C.c_int64), ("data", C.POINTER(C.c_double))]
+
+
 _P = C.c_void_p
 _I64 = C.c_int64
 _I32 = C.c_int32
@@ -96,6 +109,11 @@ SIGNATURES = {
     "skema_launch_count": (_I64, [_P]),
     "skema_timing_enable": (C.c_int, [_P, _I32]),
     "skema_timing_get": (C.c_int, [_P, C.c_char_p, C.POINTER(C.c_double), C.POINTER(_I64)]),
+    "skema_read_crs": (C.c_int, [C.c_char_p, C.POINTER(Crs)]),
+    "skema_crs_free": (None, [C.POINTER(Crs)]),
+    "skema_read_dense": (C.c_int, [C.c_char_p, C.POINTER(Dense)]),
+    "skema_dense_free": (None, [C.POINTER(Dense)]),
+    "skema_write_crs": (C.c_int, [C.c_char_p, C.POINTER(Crs)]),
 }
 
 _lib = None

@@ -14,6 +14,10 @@ namespace skema {
 
 static thread_local std::string g_create_error;
 
+// The message skema_last_error(NULL) returns: failures of skema_create and
+// of the file calls, which have no context.
+void set_thread_error(const std::string& msg) { g_create_error = msg; }
+
 void fail(int status, const std::string& msg) { throw Error{status, msg}; }
 
 void cuda_check(cudaError_t e, const char* what) {

@@ -578,6 +578,65 @@ class SketchySPD(_Context):
         return self.rnrms
 
 
+def read_matrix(path, sparse: bool | None = None):
+    """Skema::read_matrix (src/Skema_IO.hpp:13-21) through the library's
+    readers: a .bin file or (sparse=True) a MatrixMarket coordinate file
+    gives a scipy CSR matrix (FP64, rows sorted, duplicates summed); a
+    MatrixMarket array file gives a dense FP64 numpy array. sparse=None
+    decides from the file (.bin, or a .mtx whose banner says coordinate)."""
+    import scipy.sparse as sp
+
+    lib = L.load()
+    p = str(path)
+    if sparse is None:
+        if p.lower().endswith(".mtx"):
+            with open(p, "rb") as f:
+                sparse = b"coordinate" in f.readline().lower()
+        else:
+            sparse = True
+    if sparse:
+        a = L.Crs()
+        st = lib.skema_read_crs(p.encode(), C.byref(a))
+        if st != L.OK:
+            raise SkemaError(st, lib.skema_last_error(None).decode())
+        try:
+            nr, nc, nnz = a.nrow, a.ncol, a.nnz
+            rp = np.ctypeslib.as_array(a.rowptr, shape=(nr + 1,)).copy()
+            col = np.ctypeslib.as_array(a.col, shape=(nnz,)).copy() if nnz else np.zeros(0, np.int32)
+            val = np.ctypeslib.as_array(a.val, shape=(nnz,)).copy() if nnz else np.zeros(0)
+        finally:
+            lib.skema_crs_free(C.byref(a))
+        return sp.csr_matrix((val, col, rp), shape=(nr, nc))
+    d = L.Dense()
+    st = lib.skema_read_dense(p.encode(), C.byref(d))
+    if st != L.OK:
+        raise SkemaError(st, lib.skema_last_error(None).decode())
+    try:
+        out = np.ctypeslib.as_array(d.data, shape=(d.ncol * d.nrow,)).reshape(d.ncol, d.nrow).T.copy() \
+            if d.nrow * d.ncol else np.zeros((d.nrow, d.ncol))
+    finally:
+        lib.skema_dense_free(C.byref(d))
+    return out
+
+
+def write_matrix(A, path):
+    """Skema::write_matrix for CRS input (src/Skema_IO.cpp:88-104): a scipy
+    sparse matrix to .mtx (coordinate real general) or .bin."""
+    import scipy.sparse as sp
+
+    lib = L.load()
+    A = sp.csr_matrix(A)
+    A.sort_indices()
+    rp = np.ascontiguousarray(A.indptr, dtype=np.int64)
+    col = np.ascontiguousarray(A.indices, dtype=np.int32)
+    val = np.ascontiguousarray(A.data, dtype=np.float64)
+    a = L.Crs(A.shape[0], A.shape[1], A.nnz, rp.ctypes.data_as(C.POINTER(C.c_int64)),
+              col.ctypes.data_as(C.POINTER(C.c_int32)), val.ctypes.data_as(C.POINTER(C.c_double)))
+    st = lib.skema_write_crs(str(path).encode(), C.byref(a))
+    if st != L.OK:
+        raise SkemaError(st, lib.skema_last_error(None).decode())
+
+
 def write_history(path, svals, rnrms, update_seconds=None):
     """The JSON of SketchySVD::save_history (src/Skema_SketchySVD.cpp:730-755):
     {"timings": {init, update, approx}, "traces": {}, "svals": [...],
