@@ -270,6 +270,19 @@ class OracleSketch:
         self.reset()
         self.update_rows(A, 0, self.m)
 
+    def linear_update_traced(self, A):
+        """linear_update with sketch_compute_svals_iters
+        (src/Skema_SketchySVD.cpp:164-216): the top-rank singular values of
+        the fixed-rank approximation after every window, keyed "0", "1", ...
+        The approximation here leaves Y intact (the reference's QR overwrites
+        it, App. A Q6, which this restatement does not repeat)."""
+        self.reset()
+        traces = {}
+        for w, r0 in enumerate(range(0, self.m, self.window)):
+            self.update_rows(A, r0, min(self.window, self.m - r0))
+            traces[str(w)] = {"svals": [float(x) for x in self.low_rank_approx()[1]]}
+        return traces
+
     # --------------------------------------------------------- approx ----
     def initial_approx(self):
         """(Q, C, P) of src/Skema_SketchySVD.cpp:338-566."""

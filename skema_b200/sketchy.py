@@ -336,6 +336,15 @@ def _csr_arg(A):
     return rowptr.ctypes.data, col.ctypes.data, val.ctypes.data, A.shape[0], A.shape[1], L.MEM_HOST, keep
 
 
+def _row_block(A, r0, w):
+    """Rows [r0, r0 + w) of a dense (numpy / torch) or CSR (scipy or
+    (rowptr, col, val)) input, as the block the update entry points take."""
+    if isinstance(A, tuple):
+        rowptr, col, val = A[:3]
+        return (rowptr[r0:r0 + w + 1], col, val)  # absolute offsets into col / val
+    return A[r0:r0 + w]
+
+
 class _Context:
     def __init__(self, alg: AlgParams, dim_redux=None):
         if dim_redux is not None:
@@ -444,12 +453,30 @@ class _Context:
         r = self.rank
         sv = getattr(self, "svals", None)
         rn = getattr(self, "rnrms", None)
-        return write_history(path, np.zeros(r) if sv is None else sv, np.zeros(r) if rn is None else rn, upd)
+        return write_history(path, np.zeros(r) if sv is None else sv, np.zeros(r) if rn is None else rn, upd,
+                             getattr(self, "traces", None))
 
     def linear_update(self, A):
-        """SketchySVD::linear_update: zero the sketches, then stream all rows."""
+        """SketchySVD::linear_update: zero the sketches, then stream all rows.
+        With AlgParams.sketch_compute_svals_iters (and more than one window)
+        the rows go one window at a time and the top-rank singular values
+        after each window are kept as self.traces[str(w)]["svals"]
+        (src/Skema_SketchySVD.cpp:164-216); the approximation here does not
+        overwrite Y, so the later windows see the true sketch."""
         self.reset()
-        self.update_rows(A, 0, None)
+        self.traces = {}
+        W = int(self.alg.window)
+        if not getattr(self.alg, "sketch_compute_svals_iters", False) or W >= self.nrow or self.spd:
+            self.update_rows(A, 0, None)
+            return
+        for w, r0 in enumerate(range(0, self.nrow, W)):
+            wr = min(W, self.nrow - r0)
+            if self.alg.kernel_func == L.KERNEL_GAUSSRBF:
+                self.update_rows(A, r0, wr)
+            else:
+                self.update_rows(_row_block(A, r0, wr), r0, wr)
+            S = self.low_rank_approx()[1]
+            self.traces[str(w)] = {"svals": [float(x) for x in S]}
 
     def synchronize(self):
         self._check(self.lib.skema_synchronize(self.h))
@@ -637,7 +664,7 @@ def write_matrix(A, path):
         raise SkemaError(st, lib.skema_last_error(None).decode())
 
 
-def write_history(path, svals, rnrms, update_seconds=None):
+def write_history(path, svals, rnrms, update_seconds=None, traces=None):
     """The JSON of SketchySVD::save_history (src/Skema_SketchySVD.cpp:730-755):
     {"timings": {init, update, approx}, "traces": {}, "svals": [...],
     "rnrms": [...]} with a 4-space indent, the reference's timing keys
@@ -650,7 +677,7 @@ def write_history(path, svals, rnrms, update_seconds=None):
     upd.update(update_seconds or {})
     timings = {"init": {k: 0.0 for k in ("upsilon", "omega", "phi", "psi")}, "update": upd,
                "approx": {k: 0.0 for k in ("phi", "psi", "dgeqrf", "dgemm", "dgels", "dgesvd")}}
-    hist = {"timings": timings, "traces": {}, "svals": [float(x) for x in svals],
+    hist = {"timings": timings, "traces": dict(traces or {}), "svals": [float(x) for x in svals],
             "rnrms": [float(x) for x in rnrms]}
     text = json.dumps(hist, indent=4)
     if path is not None:
