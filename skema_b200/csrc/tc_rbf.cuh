@@ -72,6 +72,12 @@ __global__ void __launch_bounds__(kThreads, 1)
   constexpr uint32_t V_BYTES = NC * 128;               // NC rows of 64 key values
   constexpr uint32_t STAGE = ((K_BYTES + V_BYTES + 256 + 1023) / 1024) * 1024;  // + c_key of the block
   constexpr uint32_t P_BYTES = RBF_BQ * 128;           // 128 rows of 64 BF16
+  // With a chunk of at most 384 columns, P (128 x 64 BF16 = 32 TMEM columns)
+  // is double-buffered in TMEM at columns 384 and 416 and the sketch MMA
+  // reads it from there, which leaves shared memory to the V operand alone;
+  // wider chunks keep P in shared memory.
+  constexpr bool PT = NC <= 384;
+  constexpr uint32_t P_TCOL = 384;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* smem = reinterpret_cast<unsigned char*>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
@@ -181,13 +187,19 @@ __global__ void __launch_bounds__(kThreads, 1)
       if (!mbar_wait(pfull + pb, (pc >> 1) & 1, err)) return false;
       tc_fence_after();
       const uint32_t pa = smem_u32(ps + pb * P_BYTES);
+      const uint32_t pt = tmem + P_TCOL + pb * 32;
       const uint32_t vb = smem_u32(st + s * STAGE + K_BYTES);
 #pragma unroll
       for (int kk = 0; kk < RBF_BJ / 16; ++kk) {
         const uint32_t acc = (!first || kk > 0) ? 1u : 0u;
-        umma(tmem, sdesc(pa + kk * 32, 16, 1024), sdesc(vb + kk * 32, 16, 1024), id_1, acc);
-        if (NC2 > 0)
-          umma(tmem + NC1, sdesc(pa + kk * 32, 16, 1024), sdesc(vb + NC1 * 128 + kk * 32, 16, 1024), id_2, acc);
+        if (PT) {
+          umma_ts(tmem, pt + kk * 8, sdesc(vb + kk * 32, 16, 1024), id_1, acc);
+          if (NC2 > 0) umma_ts(tmem + NC1, pt + kk * 8, sdesc(vb + NC1 * 128 + kk * 32, 16, 1024), id_2, acc);
+        } else {
+          umma(tmem, sdesc(pa + kk * 32, 16, 1024), sdesc(vb + kk * 32, 16, 1024), id_1, acc);
+          if (NC2 > 0)
+            umma(tmem + NC1, sdesc(pa + kk * 32, 16, 1024), sdesc(vb + NC1 * 128 + kk * 32, 16, 1024), id_2, acc);
+        }
       }
       umma_commit(empty + s);
       umma_commit(pfree + pb);
@@ -267,6 +279,7 @@ __global__ void __launch_bounds__(kThreads, 1)
           ok = false;
           break;
         }
+        if (PT) tc_fence_after();  // the MMA that read this P buffer has completed
         const float* ck = reinterpret_cast<const float*>(st + (it % RBF_S) * STAGE + K_BYTES + V_BYTES);
         const int64_t dcol = gq - (a.kbase + b * RBF_BJ);  // diagonal column in this block, if any
         const bool diag = __any_sync(0xffffffffu, dcol >= 0 && dcol < RBF_BJ);
@@ -277,6 +290,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         unsigned char* prow = ps + pb * P_BYTES + (warp * 32 + lane) * 128;
         const int sw = lane & 7;  // (row & 7) with row = 32 * warp + lane
+        uint32_t pw[32];          // P row as BF16 pairs (TMEM form)
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
           float e[8];
@@ -292,9 +306,19 @@ __global__ void __launch_bounds__(kThreads, 1)
           }
           __nv_bfloat162 h[4] = {__floats2bfloat162_rn(e[0], e[1]), __floats2bfloat162_rn(e[2], e[3]),
                                  __floats2bfloat162_rn(e[4], e[5]), __floats2bfloat162_rn(e[6], e[7])};
-          *reinterpret_cast<uint4*>(prow + ((q ^ sw) << 4)) = *reinterpret_cast<const uint4*>(h);
+          if (PT) {
+#pragma unroll
+            for (int u = 0; u < 4; ++u) pw[4 * q + u] = *reinterpret_cast<const uint32_t*>(&h[u]);
+          } else {
+            *reinterpret_cast<uint4*>(prow + ((q ^ sw) << 4)) = *reinterpret_cast<const uint4*>(h);
+          }
         }
-        fence_proxy_async();
+        if (PT) {
+          tmem_st32(tmem + P_TCOL + pb * 32 + lane_off, pw);
+          tc_fence_before();
+        } else {
+          fence_proxy_async();
+        }
         mbar_arrive(pfull + pb);
       }
       if (!ok) break;
