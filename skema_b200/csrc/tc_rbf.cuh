@@ -78,6 +78,12 @@ __global__ void __launch_bounds__(kThreads, 1)
   // wider chunks keep P in shared memory.
   constexpr bool PT = NC <= 384;
   constexpr uint32_t P_TCOL = 384;
+  // Q (128 x 64 DK BF16 = 32 DK columns) goes to TMEM at columns NC.. as well
+  // when it fits below P: the Gram MMA then reads only K from shared memory.
+  // The kernel-tile warps copy it there at the start of each unit and free
+  // its shared-memory copy at once.
+  constexpr bool QT = PT && NC + 32 * DK <= (int)P_TCOL;
+  constexpr uint32_t Q_TCOL = NC;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* smem = reinterpret_cast<unsigned char*>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
@@ -95,14 +101,16 @@ __global__ void __launch_bounds__(kThreads, 1)
   uint64_t* pfree = pfull + 2;           // [2]
   uint64_t* ofull = pfree + 2;
   uint64_t* ofree = ofull + 1;
-  uint32_t* tbase = reinterpret_cast<uint32_t*>(ofree + 1);
+  uint64_t* qtm = ofree + 1;             // Q copied into TMEM (QT)
+  uint32_t* tbase = reinterpret_cast<uint32_t*>(qtm + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int total = a.qtiles * a.nchunks * a.ksplit;
 
   if (threadIdx.x == 0) {
     mbar_init(qfull, 1);
-    mbar_init(qempty, 1);
+    mbar_init(qempty, QT ? 128 : 1);
+    mbar_init(qtm, 128);
     for (int s = 0; s < RBF_S; ++s) {
       mbar_init(full + s, 1);
       mbar_init(empty + s, 1);
@@ -210,7 +218,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       int qt, ch, ks;
       int64_t b0, b1;
       decode(t, qt, ch, ks, b0, b1);
-      if (!mbar_wait(qfull, un & 1, err)) break;
+      if (!mbar_wait(QT ? qtm : qfull, un & 1, err)) break;
       int prev_s = -1;
       bool first = true;
       for (int64_t b = b0; b < b1; ++b, ++it) {
@@ -225,12 +233,16 @@ __global__ void __launch_bounds__(kThreads, 1)
 #pragma unroll
         for (int dk = 0; dk < DK; ++dk)
 #pragma unroll
-          for (int kk = 0; kk < 4; ++kk)
-            umma(tS, sdesc(qa + dk * RBF_BQ * 128 + kk * 32, 16, 1024),
-                 sdesc(kb + dk * RBF_BJ * 128 + kk * 32, 16, 1024), id_g, (dk > 0 || kk > 0) ? 1u : 0u);
+          for (int kk = 0; kk < 4; ++kk) {
+            const uint64_t bd = sdesc(kb + dk * RBF_BJ * 128 + kk * 32, 16, 1024);
+            if (QT)
+              umma_ts(tS, tmem + Q_TCOL + dk * 32 + kk * 8, bd, id_g, (dk > 0 || kk > 0) ? 1u : 0u);
+            else
+              umma(tS, sdesc(qa + dk * RBF_BQ * 128 + kk * 32, 16, 1024), bd, id_g, (dk > 0 || kk > 0) ? 1u : 0u);
+          }
         umma_commit(sfull);
         ++g;
-        if (b + 1 == b1) umma_commit(qempty);
+        if (!QT && b + 1 == b1) umma_commit(qempty);
         if (prev_s >= 0) {
           if (first && !mbar_wait(ofree, (un & 1) ^ 1, err)) {
             ok = false;
@@ -261,6 +273,28 @@ __global__ void __launch_bounds__(kThreads, 1)
       decode(t, qt, ch, ks, b0, b1);
       const int64_t qrow = (int64_t)qt * RBF_BQ + warp * 32 + lane;  // query row of this thread
       const float cq = qrow < a.nq ? a.cq[qrow] : 0.f;
+      if (QT) {
+        // this thread's Q row into TMEM (the Gram MMAs of the previous unit
+        // have completed: their S tiles were all read), then free the
+        // shared-memory copy for the next unit's load
+        if (!__all_sync(0xffffffffu, mbar_wait(qfull, un & 1, err))) break;
+        const int row = warp * 32 + lane;
+#pragma unroll
+        for (int dk = 0; dk < DK; ++dk) {
+          uint32_t qw[32];
+          const unsigned char* qrowp = qs + dk * RBF_BQ * 128 + row * 128;
+#pragma unroll
+          for (int c = 0; c < 8; ++c) {
+            const uint4 v = *reinterpret_cast<const uint4*>(qrowp + ((c ^ (row & 7)) << 4));
+            qw[4 * c] = v.x, qw[4 * c + 1] = v.y, qw[4 * c + 2] = v.z, qw[4 * c + 3] = v.w;
+          }
+          tmem_st32(tmem + Q_TCOL + dk * 32 + lane_off, qw);
+        }
+        tc_fence_before();
+        mbar_arrive(qtm);
+        fence_proxy_async();
+        mbar_arrive(qempty);
+      }
       const int64_t gq = a.qbase + qrow;                              // its point index
       bool ok = true;
       for (int64_t b = b0; b < b1; ++b, ++it, ++g, ++pc) {
