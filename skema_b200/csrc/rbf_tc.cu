@@ -78,14 +78,13 @@ void launch_rbf(skema_ctx* c, const CUtensorMap& tq, const CUtensorMap& tk, cons
   constexpr uint32_t Q_BYTES = DK * tc::RBF_BQ * 128;
   constexpr uint32_t STAGE = ((DK * tc::RBF_BJ * 128 + (NC1 + NC2) * 128 + 256 + 1023) / 1024) * 1024;
   const size_t smem = Q_BYTES + (size_t)S * STAGE + 2 * tc::RBF_BQ * 128 + 1024 + 256;
-  constexpr int EW = NC1 + NC2 <= 320 ? 2 : 1;  // kernel-tile warpgroups
-  auto kern = tc::rbf_sketch_kernel<NC1, NC2, DK, S, EW>;
+  auto kern = tc::rbf_sketch_kernel<NC1, NC2, DK, S>;
   SKEMA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int64_t units = (int64_t)a.qtiles * a.nchunks * a.ksplit;
   if (units <= 0 || a.nblocks <= 0) return;
   if (units > 0x7fffffff) fail(SKEMA_EINVAL, "kernel-sketch grid too large");
   const int grid = (int)std::min<int64_t>(units, c->sm_count);
-  kern<<<grid, tc::rbf_threads<EW>(), smem, c->stream>>>(tq, tk, tv1, tv2, a, o, c->dev_err);
+  kern<<<grid, tc::kThreads, smem, c->stream>>>(tq, tk, tv1, tv2, a, o, c->dev_err);
   SKEMA_LAUNCHED(c);
   c->dev_err_armed = true;
 }

@@ -59,67 +59,65 @@ struct RbfArgs {
   int64_t kwlen, knwin;
 };
 
-// EW = 2 (chunks of at most 320 columns): two kernel-tile warpgroups,
-// warps 0-3 and 6-9, take the key blocks in turn (block it of the CTA's
-// sequence goes to group it % 2), each with its own Gram tile S_g (TMEM
-// columns 384 + 64 g) and P buffer P_g (TMEM columns 320 + 32 g, read there
-// by the sketch MMA as its A operand). One group's exponentials overlap the
-// other's TMEM round trips, which bound a single group. Group 0 also runs the
-// epilogue. EW = 1 (wider chunks): one group, one Gram tile at column 448
-// and P double-buffered in shared memory.
-template <int EW>
-constexpr int rbf_threads() {
-  return EW == 2 ? 320 : 192;
-}
-
-template <int NC1, int NC2, int DK, int RBF_S, int EW>
-__global__ void __launch_bounds__(rbf_threads<EW>(), 1)
+template <int NC1, int NC2, int DK, int RBF_S>
+__global__ void __launch_bounds__(kThreads, 1)
     rbf_sketch_kernel(const __grid_constant__ CUtensorMap tmQ, const __grid_constant__ CUtensorMap tmK,
                       const __grid_constant__ CUtensorMap tmV1, const __grid_constant__ CUtensorMap tmV2,
                       RbfArgs a, OutSpec o, int* err) {
   constexpr int NC = NC1 + NC2;
   static_assert(NC1 % 16 == 0 && NC1 <= 256 && NC2 % 16 == 0 && NC2 <= 256, "chunk tiles");
-  static_assert(EW == 1 || EW == 2, "one or two kernel-tile warpgroups");
-  static_assert(EW == 1 ? NC <= (int)RBF_SCOL : NC <= 320, "O, P and the Gram tiles share TMEM");
+  static_assert(NC <= (int)RBF_SCOL, "O and the Gram tile share TMEM");
   constexpr uint32_t Q_BYTES = DK * RBF_BQ * 128;      // DK sub-tiles of 64 d-values
   constexpr uint32_t K_BYTES = DK * RBF_BJ * 128;
   constexpr uint32_t V_BYTES = NC * 128;               // NC rows of 64 key values
   constexpr uint32_t STAGE = ((K_BYTES + V_BYTES + 256 + 1023) / 1024) * 1024;  // + c_key of the block
   constexpr uint32_t P_BYTES = RBF_BQ * 128;           // 128 rows of 64 BF16
-  constexpr bool PT = EW == 2;                         // P in TMEM
-  constexpr uint32_t P_TCOL = 320, S_TCOL = EW == 2 ? 384 : RBF_SCOL;
+  // With a chunk of at most 384 columns, P (128 x 64 BF16 = 32 TMEM columns)
+  // is double-buffered in TMEM at columns 384 and 416 and the sketch MMA
+  // reads it from there, which leaves shared memory to the V operand alone;
+  // wider chunks keep P in shared memory.
+  constexpr bool PT = NC <= 384;
+  constexpr uint32_t P_TCOL = 384;
+  // Q (128 x 64 DK BF16 = 32 DK columns) goes to TMEM at columns NC.. as well
+  // when it fits below P: the Gram MMA then reads only K from shared memory.
+  // The kernel-tile warps copy it there at the start of each unit and free
+  // its shared-memory copy at once.
+  constexpr bool QT = PT && NC + 32 * DK <= (int)P_TCOL;
+  constexpr uint32_t Q_TCOL = NC;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* smem = reinterpret_cast<unsigned char*>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
   unsigned char* qs = smem;
   unsigned char* st = qs + Q_BYTES;
   unsigned char* ps = st + RBF_S * STAGE;
-  uint64_t* bar = reinterpret_cast<uint64_t*>(ps + (PT ? 0 : 2 * P_BYTES));
+  uint64_t* bar = reinterpret_cast<uint64_t*>(ps + 2 * P_BYTES);
   uint64_t* qfull = bar + 0;
   uint64_t* qempty = bar + 1;
   uint64_t* full = bar + 2;              // [RBF_S]
   uint64_t* empty = full + RBF_S;        // [RBF_S]
-  uint64_t* sfull = empty + RBF_S;       // [2] Gram tile ready (per S buffer)
-  uint64_t* sfree = sfull + 2;           // [2] Gram tile read
-  uint64_t* pfull = sfree + 2;           // [2]
+  uint64_t* sfull = empty + RBF_S;
+  uint64_t* sfree = sfull + 1;
+  uint64_t* pfull = sfree + 1;           // [2]
   uint64_t* pfree = pfull + 2;           // [2]
   uint64_t* ofull = pfree + 2;
   uint64_t* ofree = ofull + 1;
-  uint32_t* tbase = reinterpret_cast<uint32_t*>(ofree + 1);
+  uint64_t* qtm = ofree + 1;             // Q copied into TMEM (QT)
+  uint32_t* tbase = reinterpret_cast<uint32_t*>(qtm + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int total = a.qtiles * a.nchunks * a.ksplit;
 
   if (threadIdx.x == 0) {
     mbar_init(qfull, 1);
-    mbar_init(qempty, 1);
+    mbar_init(qempty, QT ? 128 : 1);
+    mbar_init(qtm, 128);
     for (int s = 0; s < RBF_S; ++s) {
       mbar_init(full + s, 1);
       mbar_init(empty + s, 1);
     }
+    mbar_init(sfull, 1);
+    mbar_init(sfree, 128);
     for (int p = 0; p < 2; ++p) {
-      mbar_init(sfull + p, 1);
-      mbar_init(sfree + p, 128);
       mbar_init(pfull + p, 128);
       mbar_init(pfree + p, 1);
     }
@@ -147,9 +145,6 @@ __global__ void __launch_bounds__(rbf_threads<EW>(), 1)
     b0 = (int64_t)ks * a.bchunk;
     b1 = min(a.nblocks, b0 + a.bchunk);
   };
-  // S buffer and its use count for block number it of this CTA
-  auto sbuf = [&](uint32_t it) -> uint32_t { return EW == 2 ? (it & 1) : 0u; };
-  auto suse = [&](uint32_t it) -> uint32_t { return EW == 2 ? (it >> 1) : it; };
 
   if (warp == 4 && lane == 0) {
     // ---------------- TMA producer ----------------
@@ -191,7 +186,8 @@ __global__ void __launch_bounds__(rbf_threads<EW>(), 1)
     constexpr uint32_t id_g = idesc_bf16(RBF_BJ, false, false);
     constexpr uint32_t id_1 = idesc_bf16(NC1, false, false);
     constexpr uint32_t id_2 = idesc_bf16(NC2 > 0 ? NC2 : 16, false, false);
-    uint32_t it = 0, un = 0, pc = 0;
+    const uint32_t tS = tmem + RBF_SCOL;
+    uint32_t it = 0, un = 0, g = 0, pc = 0;
     bool ok = true;
     // O += P_b V_b for the block whose P is in buffer pc % 2 and whose V is in stage s
     auto sketch = [&](int s, bool first) -> bool {
@@ -222,28 +218,31 @@ __global__ void __launch_bounds__(rbf_threads<EW>(), 1)
       int qt, ch, ks;
       int64_t b0, b1;
       decode(t, qt, ch, ks, b0, b1);
-      if (!mbar_wait(qfull, un & 1, err)) break;
+      if (!mbar_wait(QT ? qtm : qfull, un & 1, err)) break;
       int prev_s = -1;
       bool first = true;
       for (int64_t b = b0; b < b1; ++b, ++it) {
         const int s = it % RBF_S;
         const uint32_t ph = (it / RBF_S) & 1;
-        const uint32_t sb = sbuf(it);
-        if (!mbar_wait(full + s, ph, err) || !mbar_wait(sfree + sb, (suse(it) & 1) ^ 1, err)) {
+        if (!mbar_wait(full + s, ph, err) || !mbar_wait(sfree, (g & 1) ^ 1, err)) {
           ok = false;
           break;
         }
         tc_fence_after();
         const uint32_t qa = smem_u32(qs), kb = smem_u32(st + s * STAGE);
-        const uint32_t tS = tmem + S_TCOL + sb * 64;
 #pragma unroll
         for (int dk = 0; dk < DK; ++dk)
 #pragma unroll
-          for (int kk = 0; kk < 4; ++kk)
-            umma(tS, sdesc(qa + dk * RBF_BQ * 128 + kk * 32, 16, 1024),
-                 sdesc(kb + dk * RBF_BJ * 128 + kk * 32, 16, 1024), id_g, (dk > 0 || kk > 0) ? 1u : 0u);
-        umma_commit(sfull + sb);
-        if (b + 1 == b1) umma_commit(qempty);
+          for (int kk = 0; kk < 4; ++kk) {
+            const uint64_t bd = sdesc(kb + dk * RBF_BJ * 128 + kk * 32, 16, 1024);
+            if (QT)
+              umma_ts(tS, tmem + Q_TCOL + dk * 32 + kk * 8, bd, id_g, (dk > 0 || kk > 0) ? 1u : 0u);
+            else
+              umma(tS, sdesc(qa + dk * RBF_BQ * 128 + kk * 32, 16, 1024), bd, id_g, (dk > 0 || kk > 0) ? 1u : 0u);
+          }
+        umma_commit(sfull);
+        ++g;
+        if (!QT && b + 1 == b1) umma_commit(qempty);
         if (prev_s >= 0) {
           if (first && !mbar_wait(ofree, (un & 1) ^ 1, err)) {
             ok = false;
@@ -264,35 +263,53 @@ __global__ void __launch_bounds__(rbf_threads<EW>(), 1)
       }
       umma_commit(ofull);
     }
-  } else if (warp < 4 || (EW == 2 && warp >= 6)) {
-    // ---------------- kernel tiles (+ epilogue: group 0) ----------------
-    const int grp = warp < 4 ? 0 : 1;
-    const int wq = warp & 3;                       // TMEM lane quarter of this warp
-    const uint32_t lane_off = (uint32_t)(wq * 32) << 16;
-    uint32_t it = 0, un = 0;
+  } else if (warp < 4) {
+    // ---------------- kernel tiles + epilogue ----------------
+    const uint32_t lane_off = (uint32_t)(warp * 32) << 16;
+    uint32_t it = 0, un = 0, g = 0, pc = 0;
     for (int t = blockIdx.x; t < total; t += gridDim.x, ++un) {
       int qt, ch, ks;
       int64_t b0, b1;
       decode(t, qt, ch, ks, b0, b1);
-      const int64_t qrow = (int64_t)qt * RBF_BQ + wq * 32 + lane;  // query row of this thread
+      const int64_t qrow = (int64_t)qt * RBF_BQ + warp * 32 + lane;  // query row of this thread
       const float cq = qrow < a.nq ? a.cq[qrow] : 0.f;
-      const int64_t gq = a.qbase + qrow;                            // its point index
+      if (QT) {
+        // this thread's Q row into TMEM (the Gram MMAs of the previous unit
+        // have completed: their S tiles were all read), then free the
+        // shared-memory copy for the next unit's load
+        if (!__all_sync(0xffffffffu, mbar_wait(qfull, un & 1, err))) break;
+        const int row = warp * 32 + lane;
+#pragma unroll
+        for (int dk = 0; dk < DK; ++dk) {
+          uint32_t qw[32];
+          const unsigned char* qrowp = qs + dk * RBF_BQ * 128 + row * 128;
+#pragma unroll
+          for (int c = 0; c < 8; ++c) {
+            const uint4 v = *reinterpret_cast<const uint4*>(qrowp + ((c ^ (row & 7)) << 4));
+            qw[4 * c] = v.x, qw[4 * c + 1] = v.y, qw[4 * c + 2] = v.z, qw[4 * c + 3] = v.w;
+          }
+          tmem_st32(tmem + Q_TCOL + dk * 32 + lane_off, qw);
+        }
+        tc_fence_before();
+        mbar_arrive(qtm);
+        fence_proxy_async();
+        mbar_arrive(qempty);
+      }
+      const int64_t gq = a.qbase + qrow;                              // its point index
       bool ok = true;
-      for (int64_t b = b0; b < b1; ++b, ++it) {
-        if (EW == 2 && (int)(it & 1) != grp) continue;  // the other group's block
-        const uint32_t sb = sbuf(it);
-        if (!__all_sync(0xffffffffu, mbar_wait(sfull + sb, suse(it) & 1, err))) {
+      for (int64_t b = b0; b < b1; ++b, ++it, ++g, ++pc) {
+        if (!__all_sync(0xffffffffu, mbar_wait(sfull, g & 1, err))) {
           ok = false;
           break;
         }
         tc_fence_after();
         float sv[64];
-        tmem_ld32(tmem + S_TCOL + sb * 64 + lane_off, sv);
-        tmem_ld32(tmem + S_TCOL + sb * 64 + lane_off + 32, sv + 32);
+        tmem_ld32(tmem + RBF_SCOL + lane_off, sv);
+        tmem_ld32(tmem + RBF_SCOL + lane_off + 32, sv + 32);
         tc_fence_before();
-        mbar_arrive(sfree + sb);
-        const uint32_t pb = it & 1;  // the P buffer of block it (the MMA's pc == it)
-        if (!__all_sync(0xffffffffu, mbar_wait(pfree + pb, ((it >> 1) & 1) ^ 1, err))) {
+        mbar_arrive(sfree);
+        const uint32_t pb = pc & 1;
+        if (!__all_sync(0xffffffffu, mbar_wait(pfree + pb, ((pc >> 1) & 1) ^ 1, err))) {
           ok = false;
           break;
         }
@@ -305,8 +322,8 @@ __global__ void __launch_bounds__(rbf_threads<EW>(), 1)
           const int64_t e = a.knwin - 1 - (b * RBF_BJ + dcol) / a.kwlen;
           if (e > 0) dval = exp2f((float)e * a.klog2w);
         }
-        unsigned char* prow = ps + pb * P_BYTES + (wq * 32 + lane) * 128;
-        const int sw = lane & 7;  // (row & 7) with row = 32 * wq + lane
+        unsigned char* prow = ps + pb * P_BYTES + (warp * 32 + lane) * 128;
+        const int sw = lane & 7;  // (row & 7) with row = 32 * warp + lane
         uint32_t pw[32];          // P row as BF16 pairs (TMEM form)
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
@@ -340,7 +357,7 @@ __global__ void __launch_bounds__(rbf_threads<EW>(), 1)
       }
       if (!ok) break;
       // epilogue: O (128 x NC) of this unit, output columns ch * NC + c
-      if (grp == 0 && !epilogue_unit<NC, 0>(o, tmem, 0, un & 1, ofull, ofree, qt, ch, wq, lane, err)) break;
+      if (!epilogue_unit<NC, 0>(o, tmem, 0, un & 1, ofull, ofree, qt, ch, warp, lane, err)) break;
     }
   }
   if ((warp == 4 || warp == 5) && lane == 0 && *(volatile int*)err) {
