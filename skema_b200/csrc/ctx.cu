@@ -110,6 +110,13 @@ void y_materialize(skema_ctx* c) {
   c->y_written.assign(1, Interval{0, c->m});
 }
 
+void xz_materialize(skema_ctx* c, cudaStream_t stream) {
+  if (!c->xz_pending) return;
+  if (c->X) SKEMA_CUDA(cudaMemsetAsync(c->X, 0, sizeof(float) * (size_t)(c->k * c->n), stream));
+  if (c->Z) SKEMA_CUDA(cudaMemsetAsync(c->Z, 0, sizeof(float) * (size_t)(c->s * c->s), stream));
+  c->xz_pending = false;
+}
+
 const char* const kStageNames[ST_COUNT] = {"update.omega",   "update.psi",    "update.upsilon",
                                             "update.phi",     "update.entries", "update.window",
                                             "update.fused",   "update.daxpy"};
@@ -125,10 +132,12 @@ static cudaEvent_t pool_event(skema_ctx* c) {
   return e;
 }
 
-StageScope::StageScope(skema_ctx* c, int stage) : c_(c), stage_(stage) {
+StageScope::StageScope(skema_ctx* c, int stage) : StageScope(c, stage, c->stream) {}
+
+StageScope::StageScope(skema_ctx* c, int stage, cudaStream_t stream) : c_(c), stage_(stage), stream_(stream) {
   if (!c_->timing) return;
   a_ = pool_event(c_);
-  SKEMA_CUDA(cudaEventRecord(a_, c_->stream));
+  SKEMA_CUDA(cudaEventRecord(a_, stream_));
 }
 
 StageScope::~StageScope() {
@@ -140,7 +149,7 @@ StageScope::~StageScope() {
   } else if (cudaEventCreate(&b) != cudaSuccess) {
     return;
   }
-  if (cudaEventRecord(b, c_->stream) != cudaSuccess) return;
+  if (cudaEventRecord(b, stream_) != cudaSuccess) return;
   c_->pending.push_back(PendingTimer{stage_, a_, b});
 }
 
@@ -186,6 +195,11 @@ static void free_all(skema_ctx* c) {
   c->dev_err = nullptr;
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   c->own_stream = nullptr;
+  if (c->side) cudaStreamDestroy(c->side);
+  if (c->fork_ev) cudaEventDestroy(c->fork_ev);
+  if (c->join_ev) cudaEventDestroy(c->join_ev);
+  c->side = nullptr;
+  c->fork_ev = c->join_ev = nullptr;
 }
 
 // Runs f, converting library errors into a status and remembering the message.
@@ -194,6 +208,7 @@ static int guarded(skema_ctx* c, F&& f) {
   if (!c) return SKEMA_EINVAL;
   try {
     SKEMA_CUDA(cudaSetDevice(c->dev));
+    if (!c->xz_defer) xz_materialize(c, c->stream);
     f();
     c->err.clear();
     return SKEMA_OK;
@@ -331,6 +346,9 @@ int skema_create(const skema_params* p, skema_ctx** out) {
     if (prop.major != 10) fail(SKEMA_ENOKERNEL, "this build carries sm_100a code only");
     SKEMA_CUDA(cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking));
     c->stream = c->own_stream;
+    SKEMA_CUDA(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
+    SKEMA_CUDA(cudaEventCreateWithFlags(&c->fork_ev, cudaEventDisableTiming));
+    SKEMA_CUDA(cudaEventCreateWithFlags(&c->join_ev, cudaEventDisableTiming));
     plan_maps(c);
     if (c->spd) {
       map_generate(c, c->omg, p->precision);
@@ -395,11 +413,11 @@ int skema_get_dims(const skema_ctx* c, int64_t* range, int64_t* core, int32_t* s
 
 int skema_reset(skema_ctx* c) {
   return guarded(c, [&] {
-    if (c->X) SKEMA_CUDA(cudaMemsetAsync(c->X, 0, sizeof(float) * (size_t)(c->k * c->n), c->stream));
-    if (c->Z) SKEMA_CUDA(cudaMemsetAsync(c->Z, 0, sizeof(float) * (size_t)(c->s * c->s), c->stream));
-    // Y is zeroed lazily: the update kernels treat rows not written since the
-    // reset as zero (write-only), and y_materialize() clears the rest before
-    // Y is read back or factorised.
+    // X and Z are zeroed by the next call (xz_materialize), Y lazily: the
+    // update kernels treat rows not written since the reset as zero
+    // (write-only), and y_materialize() clears the rest before Y is read
+    // back or factorised.
+    c->xz_pending = c->X || c->Z;
     c->y_written.clear();
   });
 }
@@ -442,6 +460,12 @@ int skema_linear_update_dense(skema_ctx* c, const float* A, int64_t ld, int32_t 
 
 int skema_linear_update_csr(skema_ctx* c, const int64_t* rowptr, const int32_t* col,
                             const float* val, int64_t row0, int64_t nrows, int32_t mem) {
+  if (!c) return SKEMA_EINVAL;
+  struct Defer {  // csr_update zeroes a pending X / Z itself
+    skema_ctx* c;
+    ~Defer() { c->xz_defer = false; }
+  } defer{c};
+  c->xz_defer = true;
   return guarded(c, [&] {
     if (!c->p.issparse) fail(SKEMA_ESTATE, "context was created for a dense input");
     if (row0 < 0 || nrows < 0 || row0 + nrows > c->m) fail(SKEMA_EINVAL, "row range outside A");

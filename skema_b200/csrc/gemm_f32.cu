@@ -243,9 +243,9 @@ void sgemm(skema_ctx* c, int64_t M, int64_t N, int64_t K, float alpha, Mat A, Ma
   else launch_sgemm<false, false, false>(c, M, N, K, alpha, A, B, beta, C, 1);
 }
 
-void scale_block(skema_ctx* c, MatOut C, int64_t M, int64_t N, float beta) {
+void scale_block(skema_ctx* c, MatOut C, int64_t M, int64_t N, float beta, cudaStream_t stream) {
   if (M <= 0 || N <= 0 || beta == 1.f) return;
-  scale_kernel<<<grid1d(c, M * N, 256), 256, 0, c->stream>>>(C.p, C.rs, C.cs, M, N, beta);
+  scale_kernel<<<grid1d(c, M * N, 256), 256, 0, stream ? stream : c->stream>>>(C.p, C.rs, C.cs, M, N, beta);
   SKEMA_LAUNCHED(c);
 }
 

@@ -95,6 +95,10 @@ struct skema_ctx {
   int dev = 0;
   cudaStream_t own_stream = nullptr;
   cudaStream_t stream = nullptr;
+  // Side stream for work that runs beside a kernel on `stream` within one
+  // call (forked from and joined back to `stream` before the call returns).
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
   std::string err;
   int64_t launches = 0;
   skema::Map ups, omg, phi, psi;
@@ -105,6 +109,11 @@ struct skema_ctx {
   float* Z = nullptr;
   // Rows of Y written since the last reset (merged, sorted intervals).
   std::vector<skema::Interval> y_written;
+  // X and Z are zeroed lazily after a reset: every entry point zeroes them
+  // on `stream` first (xz_materialize), except the CSR update, which zeroes
+  // them on the side stream beside its Y kernel when it touches them.
+  bool xz_pending = false;
+  bool xz_defer = false;
   // Workspace (grown on demand, owned).
   void* ws = nullptr;
   size_t ws_bytes = 0;
@@ -158,6 +167,7 @@ namespace skema {
 class StageScope {
  public:
   StageScope(skema_ctx* c, int stage);
+  StageScope(skema_ctx* c, int stage, cudaStream_t stream);
   ~StageScope();
   StageScope(const StageScope&) = delete;
   StageScope& operator=(const StageScope&) = delete;
@@ -165,6 +175,7 @@ class StageScope {
  private:
   skema_ctx* c_;
   int stage_;
+  cudaStream_t stream_;
   cudaEvent_t a_ = nullptr;
 };
 
@@ -174,6 +185,8 @@ bool y_rows_clean(const skema_ctx* c, int64_t a, int64_t b);
 void y_rows_mark(skema_ctx* c, int64_t a, int64_t b);
 // Zero every Y row not written since the last reset.
 void y_materialize(skema_ctx* c);
+// Zero X and Z on `stream` if a reset left them pending.
+void xz_materialize(skema_ctx* c, cudaStream_t stream);
 
 // ---- maps (maps.cu) ----
 void map_generate(skema_ctx* c, Map& mp, int precision);
@@ -196,7 +209,7 @@ struct MatOut {
 void sgemm(skema_ctx* c, int64_t M, int64_t N, int64_t K, float alpha, Mat A,
            Mat B, float beta, MatOut C, int splitk = 1);
 // C = beta * C over an M x N strided block.
-void scale_block(skema_ctx* c, MatOut C, int64_t M, int64_t N, float beta);
+void scale_block(skema_ctx* c, MatOut C, int64_t M, int64_t N, float beta, cudaStream_t stream = nullptr);
 // dst(i,j) = alpha * src(i,j) + beta * dst(i,j) over M x N (beta 0: no read).
 void axpby_block(skema_ctx* c, Mat src, MatOut dst, int64_t M, int64_t N,
                  float alpha, float beta);

@@ -51,19 +51,32 @@ __global__ void sparse_sign_map_kernel(uint32_t* __restrict__ packed, int64_t nr
 
 // Offset form of a SparseSign map with zeta = 8 and at most 128 columns:
 // eight 16-bit entries per stored row, entry t
-// = (column * 128) | sign << 15, i.e. the byte offset of bin `column` in a
-// warp's bin-major accumulator (32 floats per bin) with the sign on top.
+// = (column * 128) | sign << 15 | dup, i.e. the byte offset of bin `column`
+// in a warp's bin-major accumulator (32 floats per bin) with the sign on top.
+// The entries are stably sorted by column (generated rows already are), and
+// bit 0 (dup) marks an entry whose column equals the previous entry's: the
+// sketch kernel then adds it to the previous entry's sum rather than to a
+// value it loaded before that sum was stored. Stable order keeps the
+// additions into each bin in entry order.
 __global__ void pack16_kernel(const uint32_t* __restrict__ packed, uint4* __restrict__ out, int64_t nrow) {
   for (int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; row < nrow;
        row += (int64_t)gridDim.x * blockDim.x) {
-    uint32_t w[4];
-    for (int q = 0; q < 4; ++q) {
-      const uint32_t e0 = packed[row * 8 + 2 * q], e1 = packed[row * 8 + 2 * q + 1];
-      const uint32_t h0 = ((e0 & 0x7fu) << 7) | ((e0 >> 31) << 15);
-      const uint32_t h1 = ((e1 & 0x7fu) << 7) | ((e1 >> 31) << 15);
-      w[q] = h0 | (h1 << 16);
+    uint32_t h[8];
+    for (int t = 0; t < 8; ++t) {
+      const uint32_t e = packed[row * 8 + t];
+      h[t] = ((e & 0x7fu) << 7) | ((e >> 31) << 15);
     }
-    out[row] = make_uint4(w[0], w[1], w[2], w[3]);
+    for (int t = 1; t < 8; ++t) {  // stable insertion sort on the column bits
+      const uint32_t v = h[t];
+      int u = t - 1;
+      while (u >= 0 && (h[u] & 0x3f80u) > (v & 0x3f80u)) {
+        h[u + 1] = h[u];
+        --u;
+      }
+      h[u + 1] = v;
+    }
+    for (int t = 1; t < 8; ++t) h[t] |= (h[t] & 0x3f80u) == (h[t - 1] & 0x3f80u) ? 1u : 0u;
+    out[row] = make_uint4(h[0] | (h[1] << 16), h[2] | (h[3] << 16), h[4] | (h[5] << 16), h[6] | (h[7] << 16));
   }
 }
 

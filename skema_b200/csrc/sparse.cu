@@ -102,24 +102,46 @@ __global__ void __launch_bounds__(128)
   }
 }
 
-// The same Y rows with fewer instructions per bin update, for the map's
-// 16-bit offset form (zeta = 8, k <= 128): each entry already is the byte
-// offset of its bin in the warp's accumulator with the sign in bit 15, so an
-// update is one extract, one add, one sign flip on the value's bits and the
-// shared read-modify-write. alpha is folded into the nonzeros as they are
-// loaded; each lane loads up to U nonzeros of its row and their map rows
-// before applying any. The write-out walks a pointer down the column-major Y
-// and the bins are cleared afterwards with 16-byte stores.
+// The same Y rows for the map's 16-bit offset form (zeta = 8, k <= 128):
+// each entry is the byte offset of its bin in the warp's accumulator, the
+// sign in bit 15 and a same-bin-as-previous flag in bit 0 (pack16_kernel).
+// Per nonzero the eight bin loads are issued together, then the eight stores
+// in entry order; a flagged entry adds to the previous entry's sum instead of
+// its own (stale) load, so every bin still sees its additions in entry order
+// and Y is bit-identical to one read-modify-write per entry.
+// The work is pipelined across each warp's tiles: the next tile's row range
+// is loaded when a tile starts and its first U nonzeros with the current
+// tile's last batch, so their latency overlaps the apply and the write-out.
+// Map rows are gathered through L2 only (.cg): 1e7 random 16-byte gathers
+// would otherwise evict the col/val lines that the lanes' row walks reuse
+// from L1. The write-out moves four bins per 16-byte access (lane -> bin
+// r0 + lane / 8, rows 4 (lane % 8) .. + 3) and clears them in the same pass.
 // The launch keeps about 128 KB of bins per SM and gives the rest of the
-// unified L1 / shared memory to L1: each lane walks its own row in col/val,
-// so a warp keeps ~20 lines live between its steps, and with the largest
-// shared-memory carve-out those lines were evicted and fetched again
-// (0.163 ms at 20 warps/SM vs 0.129 ms at 12 warps/SM with a 55 % carve-out
-// for the 1e6 x 1e5, 1e7-nonzero case).
-__device__ __forceinline__ void bin_add(uint32_t addr, float v) {
+// unified L1 / shared memory to L1, which the row walks need (measured on the
+// 1e6 x 1e5, 1e7-nonzero case: 48 KB less L1 cost 8 %, 96 KB less 34 %).
+__device__ __forceinline__ float bin_ld(uint32_t addr) {
   float x;
-  asm volatile("ld.shared.f32 %0, [%1];" : "=f"(x) : "r"(addr));
-  asm volatile("st.shared.f32 [%0], %1;" ::"r"(addr), "f"(x + v) : "memory");
+  asm volatile("ld.shared.f32 %0, [%1];" : "=f"(x) : "r"(addr) : "memory");
+  return x;
+}
+__device__ __forceinline__ void bin_st(uint32_t addr, float v) {
+  asm volatile("st.shared.f32 [%0], %1;" ::"r"(addr), "f"(v) : "memory");
+}
+
+__device__ __forceinline__ void ssign_apply8(uint32_t base, uint4 wv, float a) {
+  const uint32_t abits = __float_as_uint(a);
+  const uint32_t e[8] = {wv.x & 0xffffu, wv.x >> 16, wv.y & 0xffffu, wv.y >> 16,
+                         wv.z & 0xffffu, wv.z >> 16, wv.w & 0xffffu, wv.w >> 16};
+  float v[8];
+#pragma unroll
+  for (int t = 0; t < 8; ++t) v[t] = bin_ld(base + (e[t] & 0x7f80u));
+  float prev = 0.f;
+#pragma unroll
+  for (int t = 0; t < 8; ++t) {
+    const float nv = ((e[t] & 1u) ? prev : v[t]) + __uint_as_float(abits ^ ((e[t] << 16) & 0x80000000u));
+    bin_st(base + (e[t] & 0x7f80u), nv);
+    prev = nv;
+  }
 }
 
 template <int U>
@@ -137,52 +159,80 @@ __global__ void __launch_bounds__(128)
   for (int q = lane; q < k * 8; q += 32) bins4[q] = z4;
   __syncwarp();
   const int64_t ntiles = (nrows + 31) / 32;
-  for (int64_t tile = (int64_t)blockIdx.x * nw + warp; tile < ntiles; tile += (int64_t)gridDim.x * nw) {
-    const int64_t i = tile * 32 + lane;
-    const bool live = i < nrows;
-    int64_t b = live ? __ldg(rowptr + i) - col_offset : 0;
-    int64_t e = __shfl_down_sync(0xffffffffu, b, 1);
-    if (lane == 31 || i + 1 >= nrows) e = live ? __ldg(rowptr + i + 1) - col_offset : 0;
-    for (int64_t p = b; p < e; p += U) {
-      int32_t jj[U];
-      uint32_t ab[U];
+  const int64_t tstride = (int64_t)gridDim.x * nw;
+  const bool vec = (reinterpret_cast<uintptr_t>(Y) & 15) == 0 && ldy % 4 == 0;
+  int64_t tile = (int64_t)blockIdx.x * nw + warp;
+  auto row_range = [&](int64_t t, int64_t& b, int64_t& e) {
+    const int64_t i = t * 32 + lane;
+    b = 0, e = 0;
+    if (t < ntiles && i < nrows) b = __ldg(rowptr + i) - col_offset, e = __ldg(rowptr + i + 1) - col_offset;
+  };
+  auto load_batch = [&](int64_t q0, int64_t q1, int32_t* jj, float* aa) {
 #pragma unroll
-      for (int u = 0; u < U; ++u) {
-        jj[u] = -1;
-        ab[u] = 0u;
-        if (p + u < e) {
-          jj[u] = __ldcs(col + p + u);
-          ab[u] = __float_as_uint(__ldcs(val + p + u) * alpha);
-        }
-      }
+    for (int u = 0; u < U; ++u) {
+      jj[u] = -1, aa[u] = 0.f;
+      if (q0 + u < q1) jj[u] = __ldcs(col + q0 + u), aa[u] = __ldcs(val + q0 + u);
+    }
+  };
+  int64_t b, e;
+  row_range(tile, b, e);
+  int32_t jj[U];
+  float aa[U];
+  load_batch(b, e, jj, aa);
+  for (; tile < ntiles; tile += tstride) {
+    int64_t nb, ne;
+    row_range(tile + tstride, nb, ne);
+    for (int64_t p = b;; p += U) {
       uint4 ww[U];
 #pragma unroll
       for (int u = 0; u < U; ++u)
-        ww[u] = ((unsigned)jj[u] < (unsigned)ncol) ? __ldg(omg16 + jj[u]) : make_uint4(0u, 0u, 0u, 0u);
+        ww[u] = (unsigned)jj[u] < (unsigned)ncol ? __ldcg(omg16 + jj[u]) : make_uint4(0u, 0u, 0u, 0u);
+      // the next batch: the rest of this row, else the next tile's first
+      const bool more = p + U < e;
+      int32_t j2[U];
+      float a2[U];
+      load_batch(more ? p + U : nb, more ? e : ne, j2, a2);
 #pragma unroll
-      for (int u = 0; u < U; ++u) {
-        if ((unsigned)jj[u] >= (unsigned)ncol) continue;
-        const uint32_t w[4] = {ww[u].x, ww[u].y, ww[u].z, ww[u].w};
+      for (int u = 0; u < U; ++u)
+        if ((unsigned)jj[u] < (unsigned)ncol) ssign_apply8(base, ww[u], aa[u] * alpha);
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          bin_add(base + (w[q] & 0x7fffu), __uint_as_float(ab[u] ^ ((w[q] << 16) & 0x80000000u)));
-          bin_add(base + ((w[q] >> 16) & 0x7fffu), __uint_as_float(ab[u] ^ (w[q] & 0x80000000u)));
+      for (int u = 0; u < U; ++u) jj[u] = j2[u], aa[u] = a2[u];
+      if (!more) break;
+    }
+    __syncwarp();
+    const int64_t r0 = tile * 32;
+    if (vec && r0 + 32 <= nrows) {
+      const int sub = lane >> 3, q4 = lane & 7;
+      float* yp = Y + r0 + 4 * q4 + (int64_t)sub * ldy;
+      for (int r = sub; r < k; r += 4, yp += 4 * ldy) {
+        float4* bp = bins4 + r * 8 + q4;
+        float4 v = *bp;
+        *bp = z4;
+        float4* y4 = reinterpret_cast<float4*>(yp);
+        if (beta == 0.f) {
+          __stcs(y4, v);
+        } else {
+          const float4 o = *y4;
+          v.x = fmaf(beta, o.x, v.x), v.y = fmaf(beta, o.y, v.y), v.z = fmaf(beta, o.z, v.z),
+          v.w = fmaf(beta, o.w, v.w);
+          *y4 = v;
         }
       }
-    }
-    if (live) {
-      float* yp = Y + i;
-      if (beta == 0.f) {
-#pragma unroll 9
-        for (int r = 0; r < k; ++r, yp += ldy) __stcs(yp, bins[r * 32 + lane]);
-      } else {
-#pragma unroll 9
-        for (int r = 0; r < k; ++r, yp += ldy) *yp = fmaf(beta, *yp, bins[r * 32 + lane]);
+    } else {
+      const int64_t i = r0 + lane;
+      if (i < nrows) {
+        float* yp = Y + i;
+        if (beta == 0.f) {
+          for (int r = 0; r < k; ++r, yp += ldy) __stcs(yp, bins[r * 32 + lane]);
+        } else {
+          for (int r = 0; r < k; ++r, yp += ldy) *yp = fmaf(beta, *yp, bins[r * 32 + lane]);
+        }
       }
+      __syncwarp();
+      for (int q = lane; q < k * 8; q += 32) bins4[q] = z4;
     }
     __syncwarp();
-    for (int q = lane; q < k * 8; q += 32) bins4[q] = z4;
-    __syncwarp();
+    b = nb, e = ne;
   }
 }
 
@@ -439,7 +489,7 @@ static void launch_csr_ssign_y(skema_ctx* c, const int64_t* rowptr, const int32_
   if (sizeof(float) * 32 * (size_t)c->k * wpb > 200 * 1024)
     fail(SKEMA_EUNSUPPORTED, "sketch range too large for the sparse-sign kernel");
   if (O.packed16)
-    launch_csr_ssign_y16<6>(c, wpb, rowptr, col, val, col_offset, nrows, O, Y, ldy, alpha, beta);
+    launch_csr_ssign_y16<4>(c, wpb, rowptr, col, val, col_offset, nrows, O, Y, ldy, alpha, beta);
   else
     launch_csr_ssign_y_variant<4>(c, wpb, rowptr, col, val, col_offset, nrows, O, Y, ldy, alpha, beta);
 }
@@ -458,33 +508,49 @@ void csr_update(skema_ctx* c, const int64_t* rowptr, const int32_t* col, const f
   const float ybeta = clean ? 0.f : nu;
 
   if (c->p.dim_redux == SKEMA_MAP_SPARSE_SIGN) {
+    // X / Z (zeroing after a reset, the nu scaling and the Upsilon / Phi
+    // entries) touch neither Y nor anything the Y kernel reads: they run on
+    // the side stream, forked before the Y launch and joined after it,
+    // beside the Y kernel.
+    const auto ur = entry_range(c->ups, row0, row0 + nrows);
+    const auto pr = entry_range(c->phi, row0, row0 + nrows);
+    const int64_t nue = c->spd ? 0 : ur.second - ur.first, npe = c->spd ? 0 : pr.second - pr.first;
+    const bool side = c->xz_pending || (!c->spd && (nu != 1.f || nue + npe > 0));
+    if (side) SKEMA_CUDA(cudaEventRecord(c->fork_ev, c->stream));
     {
       StageScope st(c, ST_OMEGA);
       launch_csr_ssign_y(c, rowptr, col, val, col_offset, nrows, c->omg, c->Y + row0, c->m, eta, ybeta);
     }
     y_rows_mark(c, row0, row0 + nrows);
-    if (c->spd) return;
-    if (nu != 1.f) {
-      StageScope st(c, ST_DAXPY);
-      const float sc = (float)std::pow((double)nu, (double)nwin);
-      scale_block(c, MatOut{c->X, c->n, 1}, c->k, c->n, sc);
-      scale_block(c, MatOut{c->Z, c->s, 1}, c->s, c->s, sc);
+    if (!side) return;
+    SKEMA_CUDA(cudaStreamWaitEvent(c->side, c->fork_ev, 0));
+    xz_materialize(c, c->side);
+    if (c->spd) {
+      SKEMA_CUDA(cudaEventRecord(c->join_ev, c->side));
+      SKEMA_CUDA(cudaStreamWaitEvent(c->stream, c->join_ev, 0));
+      return;
     }
-    const auto ur = entry_range(c->ups, row0, row0 + nrows);
-    const auto pr = entry_range(c->phi, row0, row0 + nrows);
-    const int64_t nue = ur.second - ur.first, npe = pr.second - pr.first;
+    if (nu != 1.f) {
+      StageScope st(c, ST_DAXPY, c->side);
+      const float sc = (float)std::pow((double)nu, (double)nwin);
+      scale_block(c, MatOut{c->X, c->n, 1}, c->k, c->n, sc, c->side);
+      scale_block(c, MatOut{c->Z, c->s, 1}, c->s, c->s, sc, c->side);
+    }
     if (nue + npe > 0) {
-      StageScope st(c, ST_ENTRIES);
+      StageScope st(c, ST_ENTRIES, c->side);
       const int grid = grid_cap(c, (nue + npe + 7) / 8, 8);
-      csr_ssign_entries_kernel<<<grid, 256, 0, c->stream>>>(
+      csr_ssign_entries_kernel<<<grid, 256, 0, c->side>>>(
           rowptr, col, val, col_offset, row0, W, nwin, eta, nu, c->ups.d_inv_row + ur.first,
           c->ups.d_inv_rs + ur.first, nue, c->phi.d_inv_row + pr.first, c->phi.d_inv_rs + pr.first,
           npe, c->psi.packed, c->psi.zeta, c->X, c->n, c->Z, c->s);
       SKEMA_LAUNCHED(c);
     }
+    SKEMA_CUDA(cudaEventRecord(c->join_ev, c->side));
+    SKEMA_CUDA(cudaStreamWaitEvent(c->stream, c->join_ev, 0));
     return;
   }
 
+  xz_materialize(c, c->stream);
   // Gauss maps, all stored transposed (src/Skema_SketchySVD.cpp:296-316):
   // stored rows contiguous, logical (r, j) at f32[r + j*lrows].
   const int threads = 256;

@@ -193,15 +193,15 @@ def test_csr_device_input_and_eta_nu(sk, oracle):
 
 @pytest.mark.parametrize("m", [1000, 1001])
 def test_csr_blocks_dirty_rows_and_offsets(sk, oracle, m):
-    # Both forms of the Y kernel: the TMA write-out (clean rows, first row a
-    # multiple of 4, m a multiple of 4) and the per-lane write-out (any other
-    # start row, odd m, rows updated a second time with the nu term).
+    # Both write-outs of the Y kernel: 16-byte (full 32-row tiles, first row
+    # and m multiples of 4) and per-lane (any other start row, odd m, a
+    # clipped tile), on clean rows and on rows updated again with the nu term.
     n = 700
     A = csr_input(m, n, nnz_row=9, seed=13)
     a = alg(sk, m, n, 5, 100, 1, issparse=True, sketch_eta=0.75, sketch_nu=0.9)
     o = oracle_for(oracle, a)
     o.reset()
-    # (500, 3): a 3-row TMA tile clipped at row 503, whose rows must stay
+    # (500, 3): a 3-row tile clipped at row 503, whose rows must stay
     # untouched until the (503, ...) call writes them
     calls = [(0, 500), (500, 3), (503, m - 503), (0, 500), (200, 300)]
     for r0, nr in calls:
@@ -227,6 +227,52 @@ def test_csr_duplicate_columns_are_summed(sk, oracle):
     with sk.SketchySVD(a) as s:
         s.linear_update((rowptr, col, val))
         check_sketches(s, o)
+
+
+@pytest.mark.parametrize("issparse", [True, False])
+def test_reset_then_read_or_update(sk, oracle, issparse):
+    # A reset leaves X and Z to be zeroed by the next call: a read-back sees
+    # zeros, and an update after the reset equals one on a fresh context
+    # (the CSR update zeroes them on its side stream beside the Y kernel).
+    m, n = 2000, 600
+    A = csr_input(m, n, nnz_row=8, seed=4) if issparse else dense_input(m, n, seed=4)
+    a = alg(sk, m, n, 6, 500, 1, issparse=issparse, sketch_nu=0.8)
+    o = oracle_for(oracle, a)
+    o.linear_update(A)
+    with sk.SketchySVD(a) as s:
+        s.update_rows(A, 0, None)
+        s.update_rows(A, 0, None)
+        s.reset()
+        for sketch in s.get_sketches():
+            assert not np.any(sketch)
+        s.update_rows(A, 0, None)
+        s.reset()
+        s.update_rows(A, 0, None)
+        check_sketches(s, o)
+
+
+def test_csr_imported_map_unsorted_duplicate_bins(sk):
+    # The zeta = 8, k <= 128 kernel takes the map in a 16-bit offset form
+    # sorted by bin with repeated bins flagged; an imported map may list its
+    # rows unsorted with repeats anywhere.
+    m, n = 3000, 900
+    A = csr_input(m, n, nnz_row=11, seed=21)
+    a = alg(sk, m, n, 20, m, 1, issparse=True)  # k = 81, zeta = 8
+    rng = np.random.default_rng(5)
+    with sk.SketchySVD(a) as s:
+        _, ix = s.map_export(1)
+        assert ix.shape == (n, 8)
+        ix2 = rng.integers(0, 81, size=ix.shape).astype(np.int32)
+        ix2[::3, 1] = ix2[::3, 0]  # adjacent repeat
+        ix2[::5, 7] = ix2[::5, 2]  # repeat far apart
+        ix2[::7, 3:6] = ix2[::7, 6:7]  # four of one bin
+        v2 = np.where(rng.random(ix.shape) < 0.5, -1.0, 1.0)
+        s.map_import(1, v2, ix2)
+        s.linear_update(A)
+        Y = s.get_sketches()[1]
+    OmT = np.zeros((n, 81))
+    np.add.at(OmT, (np.repeat(np.arange(n), 8), ix2.ravel()), v2.ravel())
+    assert rel_fro(Y, A @ OmT) < 1e-6
 
 
 # ------------------------------------------------------------- SketchySPD ----
