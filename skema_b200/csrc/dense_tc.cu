@@ -393,17 +393,20 @@ __global__ void amax_a16_kernel(const __nv_bfloat16* __restrict__ A16, int64_t c
 
 // Row-blocked BF16 window (64-row blocks, a 128-byte line of 64 rows per
 // column) -> E4M3(scale_A a) row-major with row stride ld8 bytes, by tiles
-// of 64 rows x 128 columns through shared memory. A thread takes 4 x 4
-// blocks (4 rows of 4 columns: four 8-byte loads, sixteen lanes covering one
-// column line), converts them and stores each block row as one 32-bit word
-// of the row-major tile; rows then leave as 16-byte stores. scale_A comes
-// from the window's amax (*amax); block 0 also writes the [Y | T] product
-// scale 1 / (scale_A scale_map) into *scale_out.
+// of 64 rows x 128 columns through shared memory. A thread takes two 4 x 4
+// blocks (4 rows of 4 columns: four 8-byte loads), converts them and stores
+// each block row as one 32-bit word of the row-major tile; rows then leave
+// as 16-byte global stores. Within a warp the lanes cover 8 row quads x 4
+// column quads: the loads are 64-byte runs of 4 column lines, and with a
+// tile row stride of 33 words both the word stores and the row read-out
+// hit 32 distinct banks. scale_A comes from the window's amax (*amax);
+// block 0 also writes the [Y | T] product scale 1 / (scale_A scale_map)
+// into *scale_out.
 __global__ void __launch_bounds__(256)
     a16_to_a8_kernel(const __nv_bfloat16* __restrict__ A16, int64_t rows, int64_t cols, uint8_t* __restrict__ A8,
                      int64_t ld8, const uint32_t* amax, float* scale_out, float smap) {
-  constexpr int TC = 128, RS = TC + 16;  // tile columns; shared row stride in bytes
-  __shared__ __align__(16) uint8_t tile[64 * RS];
+  constexpr int TC = 128, W = TC / 4 + 1;  // tile columns; shared row stride in 32-bit words
+  __shared__ uint32_t tile[64 * W];
   const float sa = pow2_scale_for(__uint_as_float(*amax));
   if (blockIdx.x == 0 && threadIdx.x == 0) *scale_out = 1.f / (sa * smap);
   const int64_t nrb = (rows + 63) / 64, ncb = (cols + TC - 1) / TC;
@@ -412,7 +415,9 @@ __global__ void __launch_bounds__(256)
     uint2 w[2][4];
 #pragma unroll
     for (int v = 0; v < 2; ++v) {
-      const int b = threadIdx.x + 256 * v, g = b & 15, cq = b >> 4;  // rows 4g.., columns 4cq..
+      // rows 4g .. 4g+3 and columns 4cq .. 4cq+3 of the tile
+      const int b = threadIdx.x + 256 * v;
+      const int g = (b & 7) | (((b >> 5) & 1) << 3), cq = ((b >> 3) & 3) | ((b >> 6) << 2);
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
         const int64_t col = j0 + 4 * cq + j;
@@ -422,7 +427,8 @@ __global__ void __launch_bounds__(256)
     }
 #pragma unroll
     for (int v = 0; v < 2; ++v) {
-      const int b = threadIdx.x + 256 * v, g = b & 15, cq = b >> 4;
+      const int b = threadIdx.x + 256 * v;
+      const int g = (b & 7) | (((b >> 5) & 1) << 3), cq = ((b >> 3) & 3) | ((b >> 6) << 2);
       uint32_t row[4] = {0u, 0u, 0u, 0u};
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
@@ -434,7 +440,7 @@ __global__ void __launch_bounds__(256)
         row[3] |= (uint32_t)to_e4m3(__high2float(hi) * sa) << (8 * j);
       }
 #pragma unroll
-      for (int e = 0; e < 4; ++e) *reinterpret_cast<uint32_t*>(tile + (4 * g + e) * RS + 4 * cq) = row[e];
+      for (int e = 0; e < 4; ++e) tile[(4 * g + e) * W + cq] = row[e];
     }
     __syncthreads();
     // row r of the tile: TC bytes as TC / 16 pieces of 16 bytes
@@ -443,7 +449,8 @@ __global__ void __launch_bounds__(256)
       const int q = threadIdx.x + 256 * u, r = q >> 3, pc = q & 7;
       const int64_t i = rb * 64 + r, j = j0 + 16 * pc;
       if (i < rows && j < cols) {
-        const uint4 v = *reinterpret_cast<const uint4*>(tile + r * RS + 16 * pc);
+        const uint32_t* src = tile + r * W + 4 * pc;
+        const uint4 v = make_uint4(src[0], src[1], src[2], src[3]);
         uint8_t* dst = A8 + i * ld8 + j;
         if (j + 16 <= cols) {
           *reinterpret_cast<uint4*>(dst) = v;
