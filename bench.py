@@ -404,6 +404,8 @@ def run_gpu(args, cfg, peaks, peak_kind):
         inp = A
     torch.cuda.synchronize()
     k, s, n = cfg["k"], cfg["s"], cfg["n"]
+    if rbf:
+        n = m_glob  # the kernel matrix is points x points (--rows shrinks both)
     Xbuf = torch.empty((k, n), dtype=torch.float32, device=dev) if world > 1 else None
     Zbuf = torch.empty((s, s), dtype=torch.float32, device=dev) if world > 1 else None
 
@@ -641,7 +643,8 @@ def config_of(args, cfg, world, nnz):
                 "precision": "bf16 tensor-core form" if cfg.get("prec") == 1 else "fp32",
                 "cotangent": "fixed 2 Y (L = ||Y||_F^2)", "parallelism": f"replicas x{world}",
                 "l2": "K tiles (2.5e9 entries) recomputed per step, never stored; E blocks stream > 126 MB L2"}
-    c = {"workload": args.workload, "m_per_gpu": cfg["m"], "n": cfg["n"], "rank": cfg["rank"],
+    c = {"workload": args.workload, "m_per_gpu": cfg["m"], "n": cfg["m"] if cfg.get("rbf") else cfg["n"],
+         "rank": cfg["rank"],
          "range_k": cfg["k"], "core_s": cfg["s"], "window": cfg["window"],
          "maps": "sparse-sign zeta=8" if cfg["kind"] == 1 else "gauss",
          "parallelism": f"row-blocks x{world}" + (" + NCCL all-reduce of X,Z" if world > 1 else "")}
