@@ -117,7 +117,9 @@ const char* skema_last_error(const skema_ctx* ctx);
 int skema_get_dims(const skema_ctx* ctx, int64_t* range, int64_t* core, int32_t* spd);
 
 /* Zero X, Y, Z: the start of SketchySVD::linear_update
- * (src/Skema_SketchySVD.cpp:131-133). */
+ * (src/Skema_SketchySVD.cpp:131-133). The zeroing is deferred: the next
+ * call on ctx performs it first (a CSR update does it beside its Y kernel),
+ * so every later call sees zero sketches. */
 int skema_reset(skema_ctx* ctx);
 
 /* SketchySVD<matrix_type,*>::linear_update + update
