@@ -385,7 +385,8 @@ __global__ void __launch_bounds__(kThreads, 1)
 //   E = M o exp2(2 g' S + c_q + c_j)           four warps, in registers;
 //                                              row sums of E and the dgamma
 //                                              terms accumulate per thread
-//   O += E X_j                                 tcgen05, N = padded d
+//   O += E X_j                                 tcgen05, N = padded d, E read
+//                                              from TMEM (two 32-column buffers)
 // then O, the row sums and the dgamma terms go out with FP32 / FP64
 // atomics. The first pass (A = Ybar, B = Omega^T) gives E X, rowsum(E) and
 // dgamma; the second (A = Omega^T, B = Ybar) sees E^T and gives E^T X and
@@ -419,6 +420,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   constexpr uint32_t STAGE = ((KX + KB + XT + 256 + 1023) / 1024) * 1024;
   constexpr uint32_t P_BYTES = RBF_BQ * 128;
   constexpr uint32_t TS = 128, TM = 192;    // TMEM columns of S and M; O at 0
+  constexpr uint32_t TE = 64;               // E buffers (BF16 pairs) at 64 and 96
   static_assert(DK == 1, "one 64-row box of X^T per key block");
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* smem = reinterpret_cast<unsigned char*>(
@@ -521,11 +523,11 @@ __global__ void __launch_bounds__(kThreads, 1)
       const uint32_t pb = pc & 1;
       if (!mbar_wait(pfull + pb, (pc >> 1) & 1, err)) return false;
       tc_fence_after();
-      const uint32_t pa = smem_u32(ps + pb * P_BYTES);
+      const uint32_t ea = tmem + TE + pb * 32;
       const uint32_t xb = smem_u32(st + s * STAGE + KX + KB);
 #pragma unroll
       for (int kk = 0; kk < RBF_BJ / 16; ++kk)
-        umma(tmem, sdesc(pa + kk * 32, 16, 1024), sdesc(xb + kk * 32, 16, 1024), idD, (!first || kk > 0) ? 1u : 0u);
+        umma_ts(tmem, ea + kk * 8, sdesc(xb + kk * 32, 16, 1024), idD, (!first || kk > 0) ? 1u : 0u);
       umma_commit(empty + s);
       umma_commit(pfree + pb);
       ++pc;
@@ -606,10 +608,10 @@ __global__ void __launch_bounds__(kThreads, 1)
           ok = false;
           break;
         }
+        tc_fence_after();  // the MMA that read this E buffer has completed
         const float* ck = reinterpret_cast<const float*>(st + (it % NS) * STAGE + KX + KB + XT);
         const int64_t dcol = gq - b * RBF_BJ;  // diagonal column of this block, if any
-        unsigned char* prow = ps + pb * P_BYTES + (warp * 32 + lane) * 128;
-        const int sw = lane & 7;
+        uint32_t ew[32];                       // the E row as BF16 pairs (TMEM form)
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
           float sv[32], mv[32];
@@ -639,10 +641,12 @@ __global__ void __launch_bounds__(kThreads, 1)
             }
             __nv_bfloat162 hh[4] = {__floats2bfloat162_rn(e[0], e[1]), __floats2bfloat162_rn(e[2], e[3]),
                                     __floats2bfloat162_rn(e[4], e[5]), __floats2bfloat162_rn(e[6], e[7])};
-            *reinterpret_cast<uint4*>(prow + (((4 * h + q) ^ sw) << 4)) = *reinterpret_cast<const uint4*>(hh);
+#pragma unroll
+            for (int u = 0; u < 4; ++u) ew[16 * h + 4 * q + u] = *reinterpret_cast<const uint32_t*>(&hh[u]);
           }
         }
-        fence_proxy_async();
+        tmem_st32(tmem + TE + pb * 32 + lane_off, ew);
+        tc_fence_before();
         mbar_arrive(pfull + pb);
       }
       if (!ok) break;
