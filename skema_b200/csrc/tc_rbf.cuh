@@ -421,6 +421,11 @@ __global__ void __launch_bounds__(kThreads, 1)
   constexpr uint32_t P_BYTES = RBF_BQ * 128;
   constexpr uint32_t TS = 128, TM = 192;    // TMEM columns of S and M; O at 0
   constexpr uint32_t TE = 64;               // E buffers (BF16 pairs) at 64 and 96
+  // The unit's query rows (X_q: 32 DK columns, A_q: 32 KK columns) are
+  // copied into TMEM at its start by the E warps, so the S and M MMAs read
+  // only the key-side operands from shared memory.
+  constexpr uint32_t TQX = 256, TQA = TQX + 32 * DK;
+  static_assert(TQA + 32 * KK <= 512, "query rows must fit TMEM");
   static_assert(DK == 1, "one 64-row box of X^T per key block");
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* smem = reinterpret_cast<unsigned char*>(
@@ -440,13 +445,15 @@ __global__ void __launch_bounds__(kThreads, 1)
   uint64_t* pfree = pfull + 2;
   uint64_t* ofull = pfree + 2;
   uint64_t* ofree = ofull + 1;
-  uint32_t* tbase = reinterpret_cast<uint32_t*>(ofree + 1);
+  uint64_t* qtm = ofree + 1;  // query rows copied into TMEM
+  uint32_t* tbase = reinterpret_cast<uint32_t*>(qtm + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int total = a.qtiles * a.ksplit;
   if (threadIdx.x == 0) {
     mbar_init(qfull, 1);
-    mbar_init(qempty, 1);
+    mbar_init(qempty, 128);
+    mbar_init(qtm, 128);
     for (int s = 0; s < NS; ++s) {
       mbar_init(full + s, 1);
       mbar_init(empty + s, 1);
@@ -463,7 +470,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   }
   if (warp == 5) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tbase)),
-                 "r"(256)
+                 "r"(512)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
@@ -537,7 +544,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       int qt;
       int64_t b0, b1;
       decode(t, qt, b0, b1);
-      if (!mbar_wait(qfull, un & 1, err)) break;
+      if (!mbar_wait(qtm, un & 1, err)) break;
       int prev_s = -1;
       bool first = true;
       for (int64_t b = b0; b < b1; ++b, ++it) {
@@ -548,22 +555,21 @@ __global__ void __launch_bounds__(kThreads, 1)
           break;
         }
         tc_fence_after();
-        const uint32_t qxa = smem_u32(qx), qaa = smem_u32(qa), kb = smem_u32(st + s * STAGE);
+        const uint32_t kb = smem_u32(st + s * STAGE);
 #pragma unroll
         for (int f = 0; f < DK; ++f)
 #pragma unroll
           for (int kk = 0; kk < 4; ++kk)
-            umma(tmem + TS, sdesc(qxa + f * RBF_BQ * 128 + kk * 32, 16, 1024),
-                 sdesc(kb + f * RBF_BJ * 128 + kk * 32, 16, 1024), id64, (f > 0 || kk > 0) ? 1u : 0u);
+            umma_ts(tmem + TS, tmem + TQX + f * 32 + kk * 8, sdesc(kb + f * RBF_BJ * 128 + kk * 32, 16, 1024), id64,
+                    (f > 0 || kk > 0) ? 1u : 0u);
 #pragma unroll
         for (int f = 0; f < KK; ++f)
 #pragma unroll
           for (int kk = 0; kk < 4; ++kk)
-            umma(tmem + TM, sdesc(qaa + f * RBF_BQ * 128 + kk * 32, 16, 1024),
-                 sdesc(kb + KX + f * RBF_BJ * 128 + kk * 32, 16, 1024), id64, (f > 0 || kk > 0) ? 1u : 0u);
+            umma_ts(tmem + TM, tmem + TQA + f * 32 + kk * 8, sdesc(kb + KX + f * RBF_BJ * 128 + kk * 32, 16, 1024),
+                    id64, (f > 0 || kk > 0) ? 1u : 0u);
         umma_commit(sfull);
         ++g;
-        if (b + 1 == b1) umma_commit(qempty);
         if (prev_s >= 0) {
           if (first && !mbar_wait(ofree, (un & 1) ^ 1, err)) {
             ok = false;
@@ -596,6 +602,28 @@ __global__ void __launch_bounds__(kThreads, 1)
       const bool live = gq < a.N;
       const float cq = live ? a.cval[gq] : 0.f;
       float rs_acc = 0.f, dg_acc = 0.f;
+      {
+        // this thread's X_q and A_q rows into TMEM (the S and M MMAs of the
+        // previous unit have completed: their tiles were all read), then
+        // free the shared-memory copies for the next unit's loads
+        if (!__all_sync(0xffffffffu, mbar_wait(qfull, un & 1, err))) break;
+        const int row = warp * 32 + lane;
+#pragma unroll
+        for (int f = 0; f < DK + KK; ++f) {
+          uint32_t qw[32];
+          const unsigned char* qrowp = (f < DK ? qx + f * RBF_BQ * 128 : qa + (f - DK) * RBF_BQ * 128) + row * 128;
+#pragma unroll
+          for (int c = 0; c < 8; ++c) {
+            const uint4 v = *reinterpret_cast<const uint4*>(qrowp + ((c ^ (row & 7)) << 4));
+            qw[4 * c] = v.x, qw[4 * c + 1] = v.y, qw[4 * c + 2] = v.z, qw[4 * c + 3] = v.w;
+          }
+          tmem_st32(tmem + TQX + f * 32 + lane_off, qw);
+        }
+        tc_fence_before();
+        mbar_arrive(qtm);
+        fence_proxy_async();
+        mbar_arrive(qempty);
+      }
       bool ok = true;
       for (int64_t b = b0; b < b1; ++b, ++it, ++g, ++pc) {
         if (!__all_sync(0xffffffffu, mbar_wait(sfull, g & 1, err))) {
@@ -685,7 +713,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   if (warp == 5) {
     __syncwarp();
     tc_fence_after();
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256) : "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512) : "memory");
   }
 }
 
