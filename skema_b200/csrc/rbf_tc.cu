@@ -283,7 +283,7 @@ template <int KK>
 void launch_vjp(skema_ctx* c, const CUtensorMap& tqx, const CUtensorMap& tkx, const CUtensorMap& tqa,
                 const CUtensorMap& tkb, const CUtensorMap& txt, const tc::RbfVjpArgs& a) {
   constexpr uint32_t STAGE = ((64 * 128 + KK * 64 * 128 + 64 * 128 + 256 + 1023) / 1024) * 1024;
-  const size_t smem = 128 * 128 + KK * 128 * 128 + 3 * (size_t)STAGE + 2 * 128 * 128 + 1024 + 256;
+  const size_t smem = 128 * 128 + KK * 128 * 128 + 3 * (size_t)STAGE + 1024 + 256;
   auto kern = tc::rbf_vjp_kernel<1, KK>;
   SKEMA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int64_t units = (int64_t)a.qtiles * a.ksplit;

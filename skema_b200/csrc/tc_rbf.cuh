@@ -418,7 +418,6 @@ __global__ void __launch_bounds__(kThreads, 1)
   constexpr uint32_t KB = KK * RBF_BJ * 128;
   constexpr uint32_t XT = DP * 128;         // DP rows of 64 keys
   constexpr uint32_t STAGE = ((KX + KB + XT + 256 + 1023) / 1024) * 1024;
-  constexpr uint32_t P_BYTES = RBF_BQ * 128;
   constexpr uint32_t TS = 128, TM = 192;    // TMEM columns of S and M; O at 0
   constexpr uint32_t TE = 64;               // E buffers (BF16 pairs) at 64 and 96
   // The unit's query rows (X_q: 32 DK columns, A_q: 32 KK columns) are
@@ -433,8 +432,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   unsigned char* qx = smem;
   unsigned char* qa = qx + QX;
   unsigned char* st = qa + QA;
-  unsigned char* ps = st + NS * STAGE;
-  uint64_t* bar = reinterpret_cast<uint64_t*>(ps + 2 * P_BYTES);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(st + NS * STAGE);
   uint64_t* qfull = bar + 0;
   uint64_t* qempty = bar + 1;
   uint64_t* full = bar + 2;
