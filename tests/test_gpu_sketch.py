@@ -251,6 +251,34 @@ def test_reset_then_read_or_update(sk, oracle, issparse):
         check_sketches(s, o)
 
 
+def test_csr_update_on_caller_stream(sk, oracle):
+    # The CSR update forks its X / Z work onto a side stream and joins it
+    # back before returning; on a caller's stream the sketches read back in
+    # that stream's order must be complete.
+    import torch
+
+    m, n = 6000, 2000
+    A = csr_input(m, n, nnz_row=9, seed=17)
+    a = alg(sk, m, n, 8, 1500, 1, issparse=True, sketch_nu=0.7)
+    o = oracle_for(oracle, a)
+    o.linear_update(A)
+    rp = torch.from_numpy(A.indptr.astype(np.int64)).cuda()
+    cl = torch.from_numpy(A.indices.astype(np.int32)).cuda()
+    vl = torch.from_numpy(A.data.astype(np.float32)).cuda()
+    st = torch.cuda.Stream()
+    with sk.SketchySVD(a) as s, torch.cuda.stream(st):
+        s.set_stream(st.cuda_stream)
+        for _ in range(3):
+            s.reset()
+            s.update_rows((rp, cl, vl), 0, m)
+        X = torch.empty((s.range, n), dtype=torch.float32, device="cuda")
+        s.get_sketch(0, X)
+        Xh = X.cpu().numpy()
+        s.set_stream(None)
+        check_sketches(s, o)
+    assert rel_fro(Xh, o.X) < TOL
+
+
 def test_csr_imported_map_unsorted_duplicate_bins(sk):
     # The zeta = 8, k <= 128 kernel takes the map in a 16-bit offset form
     # sorted by bin with repeated bins flagged; an imported map may list its
