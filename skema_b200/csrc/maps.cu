@@ -49,7 +49,7 @@ __global__ void sparse_sign_map_kernel(uint32_t* __restrict__ packed, int64_t nr
   }
 }
 
-// Offset form of a SparseSign map with zeta = 8 and at most 128 columns:
+// Offset form of a SparseSign map with zeta = 8 and at most 256 columns:
 // eight 16-bit entries per stored row, entry t
 // = (column * 128) | sign << 15 | dup, i.e. the byte offset of bin `column`
 // in a warp's bin-major accumulator (32 floats per bin) with the sign on top.
@@ -64,18 +64,18 @@ __global__ void pack16_kernel(const uint32_t* __restrict__ packed, uint4* __rest
     uint32_t h[8];
     for (int t = 0; t < 8; ++t) {
       const uint32_t e = packed[row * 8 + t];
-      h[t] = ((e & 0x7fu) << 7) | ((e >> 31) << 15);
+      h[t] = ((e & 0xffu) << 7) | ((e >> 31) << 15);
     }
     for (int t = 1; t < 8; ++t) {  // stable insertion sort on the column bits
       const uint32_t v = h[t];
       int u = t - 1;
-      while (u >= 0 && (h[u] & 0x3f80u) > (v & 0x3f80u)) {
+      while (u >= 0 && (h[u] & 0x7f80u) > (v & 0x7f80u)) {
         h[u + 1] = h[u];
         --u;
       }
       h[u + 1] = v;
     }
-    for (int t = 1; t < 8; ++t) h[t] |= (h[t] & 0x3f80u) == (h[t - 1] & 0x3f80u) ? 1u : 0u;
+    for (int t = 1; t < 8; ++t) h[t] |= (h[t] & 0x7f80u) == (h[t - 1] & 0x7f80u) ? 1u : 0u;
     out[row] = make_uint4(h[0] | (h[1] << 16), h[2] | (h[3] << 16), h[4] | (h[5] << 16), h[6] | (h[7] << 16));
   }
 }
@@ -101,7 +101,7 @@ static int grid_for(int64_t total, int threads, int sms) {
 
 static void build_pack16(skema_ctx* c, Map& mp) {
   if (mp.kind != SKEMA_MAP_SPARSE_SIGN || !mp.transposed) return;
-  if (mp.zeta != 8 || mp.ncol > 128) return;
+  if (mp.zeta != 8 || mp.ncol > 256) return;
   if (!mp.packed16) SKEMA_CUDA(cudaMalloc(&mp.packed16, sizeof(uint4) * (size_t)mp.nrow));
   pack16_kernel<<<grid_for(mp.nrow, 256, c->sm_count), 256, 0, c->stream>>>(
       mp.packed, reinterpret_cast<uint4*>(mp.packed16), mp.nrow);

@@ -42,7 +42,7 @@ int grid_cap(const skema_ctx* c, int64_t want, int per_sm) {
 // warp's 32 rows are contiguous in col/val, so L1 serves the lanes' strided
 // walk). This general form reads zeta 32-bit map words per input column
 // (column | sign << 31); csr_ssign_y16_kernel below is the form for zeta = 8
-// and k <= 128.
+// and k <= 256.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void ssign_apply(float* __restrict__ my, const uint32_t* __restrict__ omg32, int zeta,
                                             int32_t j, float a) {
@@ -102,7 +102,7 @@ __global__ void __launch_bounds__(128)
   }
 }
 
-// The same Y rows for the map's 16-bit offset form (zeta = 8, k <= 128):
+// The same Y rows for the map's 16-bit offset form (zeta = 8, k <= 256):
 // each entry is the byte offset of its bin in the warp's accumulator, the
 // sign in bit 15 and a same-bin-as-previous flag in bit 0 (pack16_kernel).
 // Per nonzero the eight bin loads are issued together, then the eight stores
@@ -463,6 +463,16 @@ static void launch_csr_ssign_y16(skema_ctx* c, int wpb, const int64_t* rowptr, c
                                  int64_t col_offset, int64_t nrows, const Map& O, float* Y, int64_t ldy, float alpha,
                                  float beta) {
   const int k = (int)c->k;
+  // warps per block: the most warps within about 128 KB of bins per SM,
+  // in the fewest blocks (k = 81: 4 x 3 = 12 warps; k = 161: 2 x 3 = 6)
+  {
+    const size_t per_warp = sizeof(float) * 32 * (size_t)k;
+    int best = 0;
+    for (int w = 4; w >= 1; w >>= 1) {
+      const int warps = w * (int)((size_t)(128 * 1024) / (per_warp * w));
+      if (warps > best) best = warps, wpb = w;
+    }
+  }
   const size_t smem = sizeof(float) * 32 * (size_t)k * wpb;
   auto kern = csr_ssign_y16_kernel<U>;
   SKEMA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

@@ -251,6 +251,20 @@ def test_reset_then_read_or_update(sk, oracle, issparse):
         check_sketches(s, o)
 
 
+@pytest.mark.parametrize("rank", [32, 40, 63])
+def test_csr_sparse_sign_wide_range(sk, oracle, rank):
+    # k = 4 r + 1 = 129, 161, 253: the 16-bit offset form with bins above 127
+    m, n = 5000, 1500
+    A = csr_input(m, n, nnz_row=9, seed=rank, empty_every=41)
+    a = alg(sk, m, n, rank, 1200, 1, issparse=True, sketch_nu=0.9)
+    o = oracle_for(oracle, a)
+    o.linear_update(A)
+    with sk.SketchySVD(a) as s:
+        assert s.range == 4 * rank + 1
+        s.linear_update(A)
+        check_sketches(s, o)
+
+
 def test_csr_update_on_caller_stream(sk, oracle):
     # The CSR update forks its X / Z work onto a side stream and joins it
     # back before returning; on a caller's stream the sketches read back in
