@@ -235,14 +235,19 @@ int skema_rbf_sketch_vjp(skema_ctx* ctx, const float* pts, int64_t npts,
                          double* dgamma);
 
 /* Allocation-free form of skema_rbf_sketch_fwd (no counterpart in the
- * reference): same arguments and result, for callers that must not have a
- * library allocate device memory -- a host framework that owns all device
+ * reference): same arguments, for callers that must not have a library
+ * allocate device memory -- a host framework that owns all device
  * memory through its own pool or memory cap, or a latency-critical loop in
  * which cudaMalloc's implicit device-wide synchronisation would stall other
  * streams. Instead of the context workspace it uses one static 16 MiB
  * scratch array compiled into the library (every GPU that loads the library
  * holds it until the process exits), in kernel row blocks of
- * floor(4194304 / npts) rows, and calls no cudaMalloc or cudaFree.
+ * floor(4194304 / npts) rows, and calls no cudaMalloc or cudaFree. It
+ * always computes in FP32 (kernel rows by explicit differences, then an FP32
+ * product), whatever the context's precision: its result is what
+ * skema_rbf_sketch_fwd returns in an FP32 context, while in a BF16 context
+ * skema_rbf_sketch_fwd takes the tensor-core form (d <= 64, k <= 192), whose
+ * result differs from the FP32 one by the BF16 rounding (about 3e-3).
  * Limit: npts <= 4194304, else SKEMA_EINVAL. The first call on a device
  * looks up the array's device address (cudaGetSymbolAddress); make that
  * first call before any stream capture. All calls share the array: calls
@@ -290,6 +295,23 @@ int skema_synchronize(skema_ctx* ctx);
 /* Use an external CUDA stream (cudaStream_t passed as void*; NULL restores
  * the context's own stream). */
 int skema_set_stream(skema_ctx* ctx, void* stream);
+
+/* Limit of every bounded device-side wait of the tensor-core kernels, in
+ * nanoseconds (ns <= 0 restores the default of 2 s). A kernel whose wait runs
+ * out sets the context's status word, lets the copies and tensor-core
+ * operations it has in flight land for 20 ms, frees its tensor memory and
+ * returns; the next synchronising call on ctx then fails with
+ * SKEMA_ETIMEOUT and clears the word, and the sketches are invalid until the
+ * next skema_reset. No reference counterpart: the reference has no device
+ * waits. Synchronises ctx's stream. */
+int skema_set_wait_limit(skema_ctx* ctx, int64_t ns);
+
+/* Cap, in bytes, on the device workspace and staging buffers ctx may hold
+ * (0: no cap, the default). A call that would grow them beyond the cap
+ * fails with SKEMA_ENOMEM before allocating; buffers already held are kept.
+ * The maps and sketches allocated by skema_create are not counted. No
+ * reference counterpart. */
+int skema_set_workspace_limit(skema_ctx* ctx, int64_t bytes);
 
 /* Number of this library's kernels launched on ctx so far (for accounting). */
 int64_t skema_launch_count(const skema_ctx* ctx);

@@ -106,6 +106,8 @@ SIGNATURES = {
     "skema_rbf_sketch_fwd_noalloc": (C.c_int, [_P, _P, _I64, _I64, _D, _P, _I64, _P]),
     "skema_synchronize": (C.c_int, [_P]),
     "skema_set_stream": (C.c_int, [_P, _P]),
+    "skema_set_wait_limit": (C.c_int, [_P, _I64]),
+    "skema_set_workspace_limit": (C.c_int, [_P, _I64]),
     "skema_launch_count": (_I64, [_P]),
     "skema_timing_enable": (C.c_int, [_P, _I32]),
     "skema_timing_get": (C.c_int, [_P, C.c_char_p, C.POINTER(C.c_double), C.POINTER(_I64)]),

@@ -22,6 +22,7 @@ void fail(int status, const std::string& msg) { throw Error{status, msg}; }
 
 void cuda_check(cudaError_t e, const char* what) {
   if (e != cudaSuccess) {
+    (void)cudaGetLastError();  // a failed call (e.g. cudaMalloc) must not fail the next launch check
     const int st = (e == cudaErrorMemoryAllocation) ? SKEMA_ENOMEM
                    : (e == cudaErrorNoDevice || e == cudaErrorNoKernelImageForDevice ||
                       e == cudaErrorInsufficientDriver)
@@ -29,6 +30,14 @@ void cuda_check(cudaError_t e, const char* what) {
                        : SKEMA_ECUDA;
     fail(st, std::string(what) + ": " + cudaGetErrorString(e));
   }
+}
+
+// Writes the limit of every bounded device wait (ns; <= 0: the 2 s default)
+// into the context's status block, ordered on the context stream.
+static void set_wait_limit(skema_ctx* c, int64_t ns) {
+  const unsigned long long v = ns > 0 ? (unsigned long long)ns : tc_default_wait_ns();
+  SKEMA_CUDA(cudaMemcpyAsync(c->dev_err + 2, &v, sizeof(v), cudaMemcpyHostToDevice, c->stream));
+  SKEMA_CUDA(cudaStreamSynchronize(c->stream));
 }
 
 void check_device_error(skema_ctx* c) {
@@ -44,8 +53,20 @@ void check_device_error(skema_ctx* c) {
   }
 }
 
+// Fails with SKEMA_ENOMEM when growing a context buffer from `have` to
+// `want` bytes would take the context's workspace and staging above the limit
+// set by skema_set_workspace_limit.
+static void check_ws_limit(const skema_ctx* c, size_t have, size_t want) {
+  if (c->ws_limit == 0) return;
+  const size_t total = c->ws_bytes + c->stage_bytes - have + want;
+  if (total > c->ws_limit)
+    fail(SKEMA_ENOMEM, "workspace of " + std::to_string(total) + " bytes needed, above the limit of " +
+                           std::to_string(c->ws_limit) + " bytes set by skema_set_workspace_limit");
+}
+
 void* workspace(skema_ctx* c, size_t bytes) {
   if (bytes <= c->ws_bytes) return c->ws;
+  check_ws_limit(c, c->ws_bytes, std::max<size_t>(bytes, 1 << 20));
   if (c->ws) {
     SKEMA_CUDA(cudaStreamSynchronize(c->stream));
     SKEMA_CUDA(cudaFree(c->ws));
@@ -60,6 +81,7 @@ void* workspace(skema_ctx* c, size_t bytes) {
 
 void* staging(skema_ctx* c, size_t bytes) {
   if (bytes <= c->stage_bytes) return c->stage;
+  check_ws_limit(c, c->stage_bytes, std::max<size_t>(bytes, 1 << 20));
   if (c->stage) {
     SKEMA_CUDA(cudaStreamSynchronize(c->stream));
     SKEMA_CUDA(cudaFree(c->stage));
@@ -108,6 +130,21 @@ void y_materialize(skema_ctx* c) {
   }
   if (at < c->m) y_zero_rows(c, at, c->m);
   c->y_written.assign(1, Interval{0, c->m});
+}
+
+float y_beta(skema_ctx* c, int64_t a, int64_t b, float nu) {
+  if (y_rows_clean(c, a, b)) return 0.f;
+  // Rows of [a, b) not written since the reset still hold whatever Y held
+  // before it: zero them, so that beta = nu scales zeros there.
+  int64_t at = a;
+  for (const Interval& iv : c->y_written) {
+    if (iv.b <= a || iv.a >= b) continue;
+    if (iv.a > at) y_zero_rows(c, at, iv.a);
+    at = std::max(at, iv.b);
+  }
+  if (at < b) y_zero_rows(c, at, b);
+  y_rows_mark(c, a, b);
+  return nu;
 }
 
 void xz_materialize(skema_ctx* c, cudaStream_t stream) {
@@ -363,8 +400,10 @@ int skema_create(const skema_params* p, skema_ctx** out) {
       }
       tc_prepare_maps(c);
     }
-    SKEMA_CUDA(cudaMalloc(&c->dev_err, sizeof(int)));
-    SKEMA_CUDA(cudaMemsetAsync(c->dev_err, 0, sizeof(int), c->stream));
+    // device status block: int status at [0], the wait limit (ns) at [2..3]
+    SKEMA_CUDA(cudaMalloc(&c->dev_err, 4 * sizeof(int)));
+    SKEMA_CUDA(cudaMemsetAsync(c->dev_err, 0, 4 * sizeof(int), c->stream));
+    set_wait_limit(c, 0);
     if (!c->spd) {
       SKEMA_CUDA(cudaMalloc(&c->X, sizeof(float) * (size_t)(c->k * c->n)));
       SKEMA_CUDA(cudaMalloc(&c->Z, sizeof(float) * (size_t)(c->s * c->s)));
@@ -818,6 +857,21 @@ int skema_set_stream(skema_ctx* c, void* stream) {
     SKEMA_CUDA(cudaStreamSynchronize(c->stream));
     check_device_error(c);
     c->stream = stream ? (cudaStream_t)stream : c->own_stream;
+  });
+}
+
+int skema_set_wait_limit(skema_ctx* c, int64_t ns) {
+  return guarded(c, [&] {
+    SKEMA_CUDA(cudaStreamSynchronize(c->stream));
+    check_device_error(c);
+    set_wait_limit(c, ns);
+  });
+}
+
+int skema_set_workspace_limit(skema_ctx* c, int64_t bytes) {
+  return guarded(c, [&] {
+    if (bytes < 0) fail(SKEMA_EINVAL, "workspace limit must be >= 0");
+    c->ws_limit = (size_t)bytes;
   });
 }
 

@@ -33,7 +33,7 @@ static void gauss_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr, float* T)
   const Map& O = c->omg;
   const Map& F = c->phi;
   const Map& P = c->psi;
-  const float ybeta = y_rows_clean(c, R0, R0 + wr) ? 0.f : nu;
+  const float ybeta = y_beta(c, R0, R0 + wr, nu);
   {  // Y rows: B(kk=j, col=r) = Omega~(r, j)
     StageScope st(c, ST_OMEGA);
     sgemm(c, wr, c->k, c->n, eta, Aw, Mat{O.f32, O.cs, O.rs}, ybeta, MatOut{c->Y + R0, 1, c->m});
@@ -60,7 +60,7 @@ static void gauss_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr, float* T)
 static void spd_gauss_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr) {
   const float eta = (float)c->p.sketch_eta, nu = (float)c->p.sketch_nu;
   const Map& O = c->omg;
-  const float ybeta = y_rows_clean(c, R0, R0 + wr) ? 0.f : nu;
+  const float ybeta = y_beta(c, R0, R0 + wr, nu);
   sgemm(c, wr, c->k, c->n, eta, Aw, Mat{O.f32, O.cs, O.rs}, ybeta, MatOut{c->Y + R0, 1, c->m});
   y_rows_mark(c, R0, R0 + wr);
 }

@@ -543,6 +543,8 @@ void tc_z_update(skema_ctx* c, const __nv_bfloat16* T16, int64_t ldT, const TcSl
   launch_gemm<tc::A_KMAJ>(c, ta, tb, s, s, K, pl, 0, o);
 }
 
+unsigned long long tc_default_wait_ns() { return tc::kWaitNs; }
+
 bool tc_available(const skema_ctx* c) {
   if (c->p.precision == SKEMA_PREC_FP8 && !(c->op8 && c->fp8_win)) return false;
   return (c->p.precision == SKEMA_PREC_BF16 || c->p.precision == SKEMA_PREC_FP8) && c->ups.lowp && c->phi.lowp &&
@@ -693,7 +695,7 @@ void yt_product(skema_ctx* c, const YtSpec& y) {
   const float eta = (float)c->p.sketch_eta, nu = (float)c->p.sketch_nu;
   const int64_t k = c->k, s = c->s, n = c->n, m = c->m;
   const bool fp8 = c->p.precision == SKEMA_PREC_FP8;
-  const float ybeta = y_rows_clean(c, y.R0, y.R0 + y.gr) ? 0.f : nu;
+  const float ybeta = y_beta(c, y.R0, y.R0 + y.gr, nu);
   StageScope st(c, ST_FUSED);
   const int64_t tiles = ((y.gr + 127) / 128) * ((k + s + kNT - 1) / kNT);
   Plan pl = plan_split(c, tiles, n, 8);
@@ -812,7 +814,6 @@ void tc_dense_update(skema_ctx* c, Mat A, int64_t row0, int64_t nrows) {
   const float log2nu = nu == 1.f ? 0.f : std::log2(nu);
   for (int64_t g0 = 0; g0 < nrows; g0 += grows) {
     const int64_t gr = std::min(grows, nrows - g0), G = (gr + W - 1) / W, R0 = row0 + g0;
-    if (!y_rows_clean(c, R0, R0 + gr)) y_materialize(c);
     if (fp8) SKEMA_CUDA(cudaMemsetAsync(amax, 0, sizeof(uint32_t) * (size_t)(2 * gwin_max), c->stream));
     for (int64_t w = 0; w < G; ++w) {
       const int64_t r = g0 + w * W, wr = std::min(W, nrows - r);

@@ -119,6 +119,7 @@ struct skema_ctx {
   size_t ws_bytes = 0;
   void* stage = nullptr;  // host-input staging
   size_t stage_bytes = 0;
+  size_t ws_limit = 0;    // cap on ws_bytes + stage_bytes (0: none)
   int sm_count = 148;
   int cc_major = 0, cc_minor = 0;
   // BF16 tensor-core form: Omega~ and Psi~ stacked as one (k+s) x n
@@ -149,8 +150,9 @@ struct skema_ctx {
   double* res_sq = nullptr;
   bool res_ready = false;
   bool residual_pass = false;
-  // Device status word of the bounded waits in the tensor-core kernels
-  // (non-zero: a wait timed out); checked at the next synchronising call.
+  // Device status block of the bounded waits in the tensor-core kernels:
+  // dev_err[0] non-zero when a wait timed out (checked at the next
+  // synchronising call); dev_err[2..3] the wait limit in ns (64-bit).
   int* dev_err = nullptr;
   bool dev_err_armed = false;
   // stage timers
@@ -185,6 +187,10 @@ bool y_rows_clean(const skema_ctx* c, int64_t a, int64_t b);
 void y_rows_mark(skema_ctx* c, int64_t a, int64_t b);
 // Zero every Y row not written since the last reset.
 void y_materialize(skema_ctx* c);
+// The beta an update of Y rows [a, b) applies on the context stream: 0 when
+// no row of the range was written since the reset (the kernel then writes
+// without reading), else nu, after the range's unwritten rows were zeroed.
+float y_beta(skema_ctx* c, int64_t a, int64_t b, float nu);
 // Zero X and Z on `stream` if a reset left them pending.
 void xz_materialize(skema_ctx* c, cudaStream_t stream);
 
@@ -235,6 +241,8 @@ void tc_dense_update(skema_ctx* c, Mat A, int64_t row0, int64_t nrows);
 // Reads the tensor-core status word (synchronises the stream) and fails with
 // SKEMA_ETIMEOUT if a kernel gave up on a wait since the last check.
 void check_device_error(skema_ctx* c);
+// The default limit of one bounded device wait, in ns.
+unsigned long long tc_default_wait_ns();
 
 // ---- sparse paths (sparse.cu) ----
 void csr_update(skema_ctx* c, const int64_t* rowptr, const int32_t* col,

@@ -160,8 +160,7 @@ void rbf_tc_update(skema_ctx* c, Mat P, int64_t N, int64_t d, int64_t row0, int6
     const int64_t G = (nr + W - 1) / W;                      // windows of this group
     const int64_t ldT = pad8(nr);
     const float nuG = fold ? std::pow(nu, (float)G) : nu;    // G = 1 when not folded
-    if (!y_rows_clean(c, R0, R0 + nr)) y_materialize(c);    // rows written before get the nu term
-    const float ybeta = y_rows_clean(c, R0, R0 + nr) ? 0.f : nu;
+    const float ybeta = y_beta(c, R0, R0 + nr, nu);  // rows written before get the nu term
     char* sp = slice_sp;
     const TcSlices sl = tc_window_slices(c, R0, nr, &sp);
     {  // row pass: [Y | T] = K(rows, :) [Omega~; Psi~]^T, T rows weighted per window

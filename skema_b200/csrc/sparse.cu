@@ -459,12 +459,14 @@ void launch_csr_ssign_y_variant(skema_ctx* c, int warps_per_block, const int64_t
 }
 
 template <int U>
-static void launch_csr_ssign_y16(skema_ctx* c, int wpb, const int64_t* rowptr, const int32_t* col, const float* val,
+static void launch_csr_ssign_y16(skema_ctx* c, const int64_t* rowptr, const int32_t* col, const float* val,
                                  int64_t col_offset, int64_t nrows, const Map& O, float* Y, int64_t ldy, float alpha,
                                  float beta) {
   const int k = (int)c->k;
   // warps per block: the most warps within about 128 KB of bins per SM,
-  // in the fewest blocks (k = 81: 4 x 3 = 12 warps; k = 161: 2 x 3 = 6)
+  // in the fewest blocks (k = 81: 4 x 3 = 12 warps; k = 161: 2 x 3 = 6;
+  // k = 256: 4 x 1)
+  int wpb = 1;
   {
     const size_t per_warp = sizeof(float) * 32 * (size_t)k;
     int best = 0;
@@ -494,14 +496,17 @@ static void launch_csr_ssign_y16(skema_ctx* c, int wpb, const int64_t* rowptr, c
 static void launch_csr_ssign_y(skema_ctx* c, const int64_t* rowptr, const int32_t* col,
                                const float* val, int64_t col_offset, int64_t nrows, const Map& O,
                                float* Y, int64_t ldy, float alpha, float beta) {
+  if (O.packed16) {  // zeta = 8, k <= 256: at most 32 KB of bins per warp
+    launch_csr_ssign_y16<4>(c, rowptr, col, val, col_offset, nrows, O, Y, ldy, alpha, beta);
+    return;
+  }
+  // general form: up to 4 warps within 96 KB of bins per block; one warp's
+  // bins (32 k floats) must fit the 200 KB limit
   int wpb = 4;
   while (wpb > 1 && sizeof(float) * 32 * (size_t)c->k * wpb > 96 * 1024) wpb >>= 1;
   if (sizeof(float) * 32 * (size_t)c->k * wpb > 200 * 1024)
     fail(SKEMA_EUNSUPPORTED, "sketch range too large for the sparse-sign kernel");
-  if (O.packed16)
-    launch_csr_ssign_y16<4>(c, wpb, rowptr, col, val, col_offset, nrows, O, Y, ldy, alpha, beta);
-  else
-    launch_csr_ssign_y_variant<4>(c, wpb, rowptr, col, val, col_offset, nrows, O, Y, ldy, alpha, beta);
+  launch_csr_ssign_y_variant<4>(c, wpb, rowptr, col, val, col_offset, nrows, O, Y, ldy, alpha, beta);
 }
 
 // ---------------------------------------------------------------------------
@@ -514,8 +519,7 @@ void csr_update(skema_ctx* c, const int64_t* rowptr, const int32_t* col, const f
   const float eta = (float)c->p.sketch_eta, nu = (float)c->p.sketch_nu;
   const int64_t W = c->w;
   const int64_t nwin = (nrows + W - 1) / W;
-  const bool clean = y_rows_clean(c, row0, row0 + nrows);
-  const float ybeta = clean ? 0.f : nu;
+  const float ybeta = y_beta(c, row0, row0 + nrows, nu);
 
   if (c->p.dim_redux == SKEMA_MAP_SPARSE_SIGN) {
     // X / Z (zeroing after a reset, the nu scaling and the Upsilon / Phi
@@ -567,7 +571,7 @@ void csr_update(skema_ctx* c, const int64_t* rowptr, const int32_t* col, const f
   for (int64_t r = 0; r < nrows; r += W) {
     const int64_t wr = std::min(W, nrows - r);
     const int64_t R0 = row0 + r;
-    const float yb = y_rows_clean(c, R0, R0 + wr) ? 0.f : nu;
+    const float yb = y_beta(c, R0, R0 + wr, nu);
     {
       StageScope st(c, ST_OMEGA);
       csr_gauss_y_kernel<<<grid_cap(c, (wr + 7) / 8, 16), threads, 0, c->stream>>>(
@@ -601,7 +605,7 @@ void csr_update(skema_ctx* c, const int64_t* rowptr, const int32_t* col, const f
 
 void dense_ssign_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr) {
   const float eta = (float)c->p.sketch_eta, nu = (float)c->p.sketch_nu;
-  const float ybeta = y_rows_clean(c, R0, R0 + wr) ? 0.f : nu;
+  const float ybeta = y_beta(c, R0, R0 + wr, nu);
   {
     StageScope st(c, ST_OMEGA);
     dense_ssign_y_kernel<<<grid_cap(c, (wr * c->k + 255) / 256, 16), 256, 0, c->stream>>>(
@@ -625,7 +629,7 @@ void dense_ssign_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr) {
 
 void spd_ssign_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr) {
   const float eta = (float)c->p.sketch_eta, nu = (float)c->p.sketch_nu;
-  const float ybeta = y_rows_clean(c, R0, R0 + wr) ? 0.f : nu;
+  const float ybeta = y_beta(c, R0, R0 + wr, nu);
   int threads = 128;
   while (threads > 32 && sizeof(float) * (size_t)(threads * c->k) > 200 * 1024) threads >>= 1;
   const size_t smem = sizeof(float) * (size_t)(threads * c->k);

@@ -38,7 +38,10 @@ namespace tc {
 constexpr int BM = 128;      // tile rows (TMEM lanes)
 constexpr int BK = 64;       // K per stage (one 128-byte swizzle row of BF16)
 constexpr int kThreads = 192;
-constexpr unsigned long long kWaitNs = 2000000000ull;  // 2 s per wait
+// Every wait is bounded by the limit the context keeps in its device status
+// block (err[0] status, err[2..3] the limit in ns as one 64-bit word; 2 s
+// unless skema_set_wait_limit changed it).
+constexpr unsigned long long kWaitNs = 2000000000ull;  // default limit per wait
 
 // Where the A tile of a K step comes from.
 enum AMode : int {
@@ -110,10 +113,11 @@ __device__ __forceinline__ bool mbar_try(uint64_t* b, uint32_t parity) {
 __device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, int* err) {
   if (mbar_try(b, parity)) return true;
   const unsigned long long t0 = now_ns();
+  const unsigned long long limit = *reinterpret_cast<const unsigned long long*>(err + 2);
   while (true) {
     if (mbar_try(b, parity)) return true;
     if (*(volatile int*)err) return false;
-    if (now_ns() - t0 > kWaitNs) {
+    if (now_ns() - t0 > limit) {
       atomicExch(err, 1);
       return false;
     }
@@ -155,6 +159,23 @@ __device__ __forceinline__ void tc_fence_before() {
 }
 __device__ __forceinline__ void tc_fence_after() {
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+// End of a tensor-core kernel: every thread of the CTA meets here. When a
+// wait timed out anywhere (in this CTA or another), copies and tensor-core
+// operations this CTA issued may still be in flight, also where the thread
+// that issued them finished normally: they get a bounded 20 ms to land before
+// the shared memory and TMEM they target are released. The predicate is
+// reduced over the block, so every thread takes the same branch.
+__device__ __forceinline__ void drain_on_error(int* err) {
+  tc_fence_before();
+  if (__syncthreads_or(*(volatile int*)err != 0)) {
+    if (threadIdx.x == 0) {
+      const unsigned long long t0 = now_ns();
+      while (now_ns() - t0 < 20000000ull) __nanosleep(1000);
+    }
+    __syncthreads();
+  }
 }
 // Shared-memory matrix descriptor, 128-byte swizzle, sm_100 version field.
 __device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
@@ -503,15 +524,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       if (!epilogue_unit<NT, TCOLS>(o, tmem, acc, aph, tfull, tempty, mt, nt, warp, lane, err)) break;
     }
   }
-  if ((warp == 4 || warp == 5) && lane == 0 && *(volatile int*)err) {
-    // a wait timed out somewhere: give the copies and MMAs this CTA still
-    // has in flight a bounded time to land before its shared memory and
-    // TMEM are released
-    const unsigned long long t0 = now_ns();
-    while (now_ns() - t0 < 20000000ull) __nanosleep(1000);
-  }
-  tc_fence_before();
-  __syncthreads();
+  drain_on_error(err);
   if (warp == 5) {
     __syncwarp();
     tc_fence_after();
@@ -631,12 +644,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       if (!epilogue_unit<NT, TCOLS>(o, tmem, acc, aph, tfull, tempty, mt, nt, warp, lane, err)) break;
     }
   }
-  if ((warp == 4 || warp == 5) && lane == 0 && *(volatile int*)err) {
-    const unsigned long long t0 = now_ns();
-    while (now_ns() - t0 < 20000000ull) __nanosleep(1000);
-  }
-  tc_fence_before();
-  __syncthreads();
+  drain_on_error(err);
   if (warp == 5) {
     __syncwarp();
     tc_fence_after();
@@ -884,12 +892,7 @@ __global__ void __launch_bounds__(kThreadsA32, 1)
       if (!epilogue_unit<NT, TCOLS>(o, tmem, acc, aph, tfull, tempty, mt, nt, warp, lane, err)) break;
     }
   }
-  if ((warp == 4 || warp == 5 || threadIdx.x == 6 * 32) && lane == 0 && *(volatile int*)err) {
-    const unsigned long long t0 = now_ns();
-    while (now_ns() - t0 < 20000000ull) __nanosleep(1000);
-  }
-  tc_fence_before();
-  __syncthreads();
+  drain_on_error(err);
   if (warp == 5) {
     __syncwarp();
     tc_fence_after();

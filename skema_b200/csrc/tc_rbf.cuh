@@ -360,12 +360,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       if (!epilogue_unit<NC, 0>(o, tmem, 0, un & 1, ofull, ofree, qt, ch, warp, lane, err)) break;
     }
   }
-  if ((warp == 4 || warp == 5) && lane == 0 && *(volatile int*)err) {
-    const unsigned long long t0 = now_ns();
-    while (now_ns() - t0 < 20000000ull) __nanosleep(1000);
-  }
-  tc_fence_before();
-  __syncthreads();
+  drain_on_error(err);
   if (warp == 5) {
     __syncwarp();
     tc_fence_after();
@@ -702,12 +697,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       }
     }
   }
-  if ((warp == 4 || warp == 5) && lane == 0 && *(volatile int*)err) {
-    const unsigned long long t0 = now_ns();
-    while (now_ns() - t0 < 20000000ull) __nanosleep(1000);
-  }
-  tc_fence_before();
-  __syncthreads();
+  drain_on_error(err);
   if (warp == 5) {
     __syncwarp();
     tc_fence_after();

@@ -7,7 +7,8 @@ Gauss RBF kernel at gamma = 1 has the listed singular values). This script
 reads them from a reference checkout and stores them as one compressed
 numpy archive, so the tests run where the reference is not present.
 
-Usage: python tests/golden/make_golden.py [REFERENCE_ROOT]
+Usage: python tests/golden/make_golden.py REFERENCE_ROOT
+   or: SKEMA_REFERENCE=REFERENCE_ROOT python tests/golden/make_golden.py
 """
 import os
 import struct
@@ -15,7 +16,9 @@ import sys
 
 import numpy as np
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("SKEMA_REFERENCE", "")
+if not REF:
+    sys.exit("usage: make_golden.py REFERENCE_ROOT (or set SKEMA_REFERENCE)")
 DATA = os.path.join(REF, "test", "data")
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "kat_fixtures.npz")
 

@@ -251,6 +251,75 @@ def test_reset_then_read_or_update(sk, oracle, issparse):
         check_sketches(s, o)
 
 
+# name: (kind, issparse, precision, spd, window, row blocks, bar)
+OVERLAP_CASES = {
+    "csr-ssign": (1, True, 0, False, 40, [(0, 100), (50, 100)], TOL),
+    "csr-gauss": (0, True, 0, False, 40, [(0, 100), (50, 100)], TOL),
+    "dense-gauss": (0, False, 0, False, 40, [(0, 100), (50, 100)], TOL),
+    "dense-ssign": (1, False, 0, False, 40, [(0, 100), (50, 100)], TOL),
+    "dense-bf16-window": (0, False, 1, False, 40, [(0, 100), (50, 100)], 6e-3),
+    "dense-bf16-group": (0, False, 1, False, 64, [(0, 256), (128, 256)], 6e-3),
+    "spd-gauss": (0, False, 0, True, 40, [(0, 100), (50, 100)], TOL),
+    "spd-ssign": (1, False, 0, True, 40, [(0, 100), (50, 100)], TOL),
+}
+
+
+@pytest.mark.parametrize("case", sorted(OVERLAP_CASES))
+def test_reset_then_overlapping_row_blocks(sk, oracle, case):
+    # After a reset, Y rows that no update has written since are zero, also
+    # where a block overlaps rows written before: reset, update [0, 100),
+    # then [50, 150). Rows [100, 150) start from zero, not from what Y held
+    # before the reset; rows [50, 100) get nu * Y + eta * y twice.
+    import torch
+
+    kind, issparse, prec, spd, W, blocks, bar = OVERLAP_CASES[case]
+    m, n = (400, 400) if spd else (600, 300)
+    A = csr_input(m, n, nnz_row=7, seed=11) if issparse else dense_input(m, n, seed=11)
+    a = alg(sk, m, n, 5, W, kind, issparse, sketch_nu=0.5, sketch_eta=2.0, precision=prec)
+    if spd:
+        A = 0.5 * (A + A.T)
+        a.issymmetric = True
+    o = oracle_for(oracle, a, spd=spd)
+    cls = sk.SketchySPD if spd else sk.SketchySVD
+
+    def block(r0, nr):
+        if issparse:
+            return A[r0:r0 + nr]
+        return torch.from_numpy(np.ascontiguousarray(A[r0:r0 + nr], dtype=np.float32)).cuda()
+
+    with cls(a) as s:
+        s.update_rows(block(0, m), 0, m)  # Y holds data from before the reset
+        s.update_rows(block(0, m), 0, m)
+        s.reset()
+        for r0, nr in blocks:
+            s.update_rows(block(r0, nr), r0, nr)
+            o.update_rows(A, r0, nr)
+        if spd:
+            Y = s.get_sketches()
+            assert rel_fro(Y, o.Y) < bar, rel_fro(Y, o.Y)
+        else:
+            X, Y, Z = s.get_sketches()
+            for got, ref in ((X, o.X), (Y, o.Y), (Z, o.Z)):
+                assert rel_fro(got, ref) < bar, rel_fro(got, ref)
+        end = blocks[-1][0] + blocks[-1][1]
+        assert not np.any(np.asarray(Y)[end:])
+
+
+def test_csr_sparse_sign_top_bin(sk, oracle):
+    # k = 256: bin 255, whose 16-bit offset 255 * 128 = 32640 sits just under
+    # the sign bit, is used on the GPU.
+    m, n = 3000, 700
+    A = csr_input(m, n, nnz_row=9, seed=256)
+    a = alg(sk, m, n, 20, 1000, 1, issparse=True, sketch_range=256, sketch_nu=0.9)
+    o = oracle_for(oracle, a)
+    o.linear_update(A)
+    assert o.k == 256 and np.any(o.maps["omega"].idx == 255)
+    with sk.SketchySVD(a) as s:
+        assert s.range == 256
+        s.linear_update(A)
+        check_sketches(s, o)
+
+
 @pytest.mark.parametrize("rank", [32, 40, 63])
 def test_csr_sparse_sign_wide_range(sk, oracle, rank):
     # k = 4 r + 1 = 129, 161, 253: the 16-bit offset form with bins above 127

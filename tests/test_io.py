@@ -17,7 +17,10 @@ import scipy.sparse as sp
 from conftest import ROOT
 
 GOLD = os.path.join(ROOT, "tests", "golden", "kat_fixtures.npz")
-REF_DATA = "/root/reference/test/data"
+# A checkout of the reference, named by SKEMA_REFERENCE; the test that reads
+# its files is skipped when the variable is unset.
+_REF = os.environ.get("SKEMA_REFERENCE", "")
+REF_DATA = os.path.join(_REF, "test", "data") if _REF else ""
 
 
 @pytest.fixture(scope="module")
@@ -35,7 +38,7 @@ def csr_of(d, stem):
     return sp.csr_matrix((d[stem + "_val"], d[stem + "_col"], d[stem + "_rowptr"]), shape=tuple(d[stem + "_shape"]))
 
 
-@pytest.mark.skipif(not os.path.isdir(REF_DATA), reason="the reference checkout is not present")
+@pytest.mark.skipif(not REF_DATA or not os.path.isdir(REF_DATA), reason="SKEMA_REFERENCE does not name a reference checkout")
 def test_reference_files_read_to_the_fixtures(sk):
     d = golden()
     R = sk.read_matrix(os.path.join(REF_DATA, "rectangular_sparse.mtx"))
