@@ -127,32 +127,8 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------- synthetic ------
-def make_csr_torch(cfg, m_local, seed, device):
-    """Seeded CSR block on the device (torch RNG)."""
-    import torch
-
-    g = torch.Generator(device=device)
-    g.manual_seed(seed)
-    n, nr = cfg["n"], cfg["nnz_row"]
-    cols = torch.randint(0, n, (m_local, nr), generator=g, device=device)
-    cols, _ = cols.sort(dim=1)
-    keep = torch.ones_like(cols, dtype=torch.bool)
-    keep[:, 1:] = cols[:, 1:] != cols[:, :-1]
-    counts = keep.sum(1)
-    rowptr = torch.zeros(m_local + 1, dtype=torch.int64, device=device)
-    rowptr[1:] = torch.cumsum(counts, 0)
-    col = cols[keep].to(torch.int32)
-    rows = torch.repeat_interleave(torch.arange(m_local, device=device), counts)
-    p = cfg["planted"]
-    U = torch.randn(m_local, p, generator=g, device=device)
-    V = torch.randn(n, p, generator=g, device=device)
-    val = torch.randn(col.numel(), generator=g, device=device)
-    val += cfg["scale"] * (U[rows] * V[col.long()]).sum(1) / (p ** 0.5)
-    del U, V, rows, cols, keep, counts
-    return rowptr, col, val.float()
-
-
 def make_csr_numpy(cfg, m_local, seed):
+    """Seeded CSR block (numpy RNG): rowptr int64, col int32, val float32."""
     rng = np.random.default_rng(seed)
     n, nr = cfg["n"], cfg["nnz_row"]
     cols = rng.integers(0, n, size=(m_local, nr))
@@ -305,22 +281,10 @@ def run_vjp(args, cfg, peaks, peak_kind):
                 "kernel": "sgemm_kernel + rbf_tile_kernel (forward and adjoint)", "kernel_ms": ms,
                 "algorithmic_flops_per_step": flops, "traffic": None}
     acc = None
-    if prec == 1 and not args.no_accuracy:
-        # the same forward / adjoint through an FP32 context, as the yardstick
-        ref = _ctx_for_standalone(local, 0)
-        ref.set_stream(stream.cuda_stream)
-        Y32 = torch.empty_like(Y)
-        dX32 = torch.empty_like(dX)
-        dg32 = torch.zeros(1, dtype=torch.float64, device=dev)
-        ref._check(lib.skema_rbf_sketch_fwd(ref.h, P.data_ptr(), N, d, gamma, Om.data_ptr(), k, Y32.data_ptr()))
-        ref._check(lib.skema_rbf_sketch_vjp(ref.h, P.data_ptr(), N, d, gamma, Om.data_ptr(), k, Ybar.data_ptr(),
-                                            dX32.data_ptr(), dg32.data_ptr()))
+    if rank == 0 and world == 1 and not args.no_accuracy:
+        step()
         torch.cuda.synchronize()
-        rel = lambda a, b: float((a.double() - b.double()).norm() / b.double().norm())
-        acc = {"against": "the FP32 form on the same inputs",
-               "Y_rel_fro": rel(Y, Y32), "dX_rel_fro": rel(dX, dX32),
-               "dgamma_rel": float(abs(dg.item() - dg32.item()) / abs(dg32.item()))}
-        ref.close()
+        acc = vjp_accuracy(P, gamma, Om, Ybar, dX, float(dg.item()))
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         v, ns, thr = cpu_sample_vjp(cfg)
@@ -345,8 +309,7 @@ def run_vjp(args, cfg, peaks, peak_kind):
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
-    if rank == 0:
-        print(json.dumps(out), flush=True)
+    return out if rank == 0 else None
 
 
 def run_gpu(args, cfg, peaks, peak_kind):
@@ -365,6 +328,7 @@ def run_gpu(args, cfg, peaks, peak_kind):
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     rbf = bool(cfg.get("rbf"))
+    host_csr = None
     from skema_b200.distributed import reduce_partial_sketches, shard_rows
 
     if rbf:
@@ -395,7 +359,10 @@ def run_gpu(args, cfg, peaks, peak_kind):
         nnz = 0
         inp = P
     elif sparse:
-        rowptr, col, val = make_csr_torch(cfg, m_local, cfg["seed"] + rank, dev)
+        # generated once on the host (numpy) and uploaded: the FP64 oracle of
+        # the parity check reads the same matrix
+        host_csr = make_csr_numpy(cfg, m_local, cfg["seed"] + rank)
+        rowptr, col, val = (torch.from_numpy(x).to(dev) for x in host_csr)
         nnz = col.numel()
         inp = (rowptr, col, val)
     else:
@@ -426,12 +393,15 @@ def run_gpu(args, cfg, peaks, peak_kind):
     e1 = torch.cuda.Event(enable_timing=True)
     def load_for(seconds):
         # untimed steps of the same work, so the clock samples bracket the
-        # timed steps under continuous load
+        # timed steps under continuous load (batches of up to 8 short steps)
         t0 = time.perf_counter()
+        batch = 1
         while time.perf_counter() - t0 < seconds:
-            for _ in range(8):
+            t1 = time.perf_counter()
+            for _ in range(batch):
                 step()
             torch.cuda.synchronize()
+            batch = 8 if time.perf_counter() - t1 < 0.05 else 1
 
     with ClockSampler(local) as clk:
         load_for(args.clock_lead)
@@ -541,36 +511,27 @@ def run_gpu(args, cfg, peaks, peak_kind):
     elif rank == 0 and not sparse and not args.no_e2e:
         e2e = e2e_dense(ctx, inp, m_local, row0, k, s, n, args)
 
-    cpu = None
+    cpu = cpu_oracle = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_baseline(args, cfg, budget_s=args.cpu_budget)
+        cpu, cpu_oracle = cpu_baseline(args, cfg, budget_s=args.cpu_budget, csr=host_csr if sparse else None)
 
-    # accuracy of the reduced-precision form: top-r singular values of the
-    # fixed-rank approximation against the plain FP32 path on the same input
-    # and maps (the FP32 path is held to 1e-5 of the FP64 oracle by the tests)
-    acc = None
-    if rank == 0 and world == 1 and a.precision and not args.no_accuracy:
+    # parity of the timed workload at its full size: the device sketches of
+    # one step against the FP64 oracle's over every row of the same matrix
+    # and maps (the CPU baseline leg above ran it), outside the timed region
+    parity = None
+    if cpu_oracle is not None and not args.no_accuracy:
         step()
-        _, S_lp, _ = ctx.low_rank_approx()
-        import dataclasses
+        parity = sparse_parity(ctx, cpu_oracle)
 
-        a32 = dataclasses.replace(a, precision=0)
-        with sk.SketchySVD(a32) as c32:
-            c32.set_stream(stream.cuda_stream)
-            if a.precision == 2:
-                # the FP8 form holds its maps on the scaled E4M3 grid: the
-                # yardstick takes the same maps
-                from skema_b200 import _lib as L
-
-                for which in (L.UPSILON, L.OMEGA, L.PHI, L.PSI):
-                    c32.map_import(which, ctx.map_export(which)[0])
-            c32.reset()
-            c32.update_rows(inp, row0, m_local)
-            _, S32, _ = c32.low_rank_approx()
-        d = np.abs(S_lp - S32)
-        acc = {"vs": "plain FP32 path, same input and maps", "rank": int(len(S32)),
-               "max_rel_err_sigma_i": float(np.max(d / S32)), "max_err_over_sigma_1": float(np.max(d) / S32[0]),
-               "sigma_1": float(S32[0]), "sigma_r": float(S32[-1])}
+    # accuracy of every dense / kernel form: the top-r singular values of the
+    # fixed-rank approximation against FP64 SketchySVD on the same input and
+    # the context's own maps
+    acc = None
+    if rank == 0 and world == 1 and not sparse and not args.no_accuracy:
+        step()
+        _, S_dev, _ = ctx.low_rank_approx()
+        S64 = fp64_sigma(ctx, inp, cfg, cfg["rank"], gamma=cfg.get("gamma") if rbf else None)
+        acc = sigma_accuracy(S_dev, S64, {0: "fp32", 1: "bf16", 2: "fp8"}[a.precision])
 
     # the residual pass (compute_residuals, the second stream of A behind
     # Skema::sketchysvd): FP64 on the device, timed once after the bench
@@ -624,6 +585,8 @@ def run_gpu(args, cfg, peaks, peak_kind):
     }
     if acc is not None:
         out["accuracy"] = acc
+    if parity is not None:
+        out["parity"] = parity
     if respass is not None:
         out["residual_pass"] = respass
     if approx is not None:
@@ -632,8 +595,7 @@ def run_gpu(args, cfg, peaks, peak_kind):
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
-    if rank == 0:
-        print(json.dumps(out), flush=True)
+    return out if rank == 0 else None
 
 
 def config_of(args, cfg, world, nnz):
@@ -769,27 +731,191 @@ def e2e_dense(ctx, A, m_local, row0, k, s, n, args):
             "timer": "host wall clock around synchronous calls"}
 
 
+# ------------------------------------------------------- parity checks -----
+# The checker, outside every timed region: FP64 arithmetic on the same input
+# and the same maps as the device run. Large FP64 products run on the device
+# (torch, float64), the approximation and the sparse-sign sketches come from
+# the oracle's CPU restatement.
+def _rel_fro(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def sparse_parity(ctx, o):
+    """Device X, Y, Z of one step against the oracle's FP64 sketches of every
+    row, and the sparse-sign maps bit for bit."""
+    from skema_b200 import _lib as L
+
+    X, Y, Z = ctx.get_sketches()
+    maps_equal = True
+    for which, name in ((L.UPSILON, "upsilon"), (L.OMEGA, "omega"), (L.PHI, "phi"), (L.PSI, "psi")):
+        vals, idx = ctx.map_export(which)
+        om = o.maps[name]
+        maps_equal &= bool(np.array_equal(idx, om.idx) and np.array_equal(vals, om.val))
+    return {"vs": "FP64 oracle over every row of the same CSR matrix and maps (CSR x SparseSign restatement)",
+            "rows": int(o.m), "bar_rel_fro": 1e-5, "rel_fro_X": _rel_fro(X, o.X), "rel_fro_Y": _rel_fro(Y, o.Y),
+            "rel_fro_Z": _rel_fro(Z, o.Z), "maps_bitexact": maps_equal}
+
+
+class _LogicalMap:
+    """A map in the form the oracle's approximation reads (.logical)."""
+
+    def __init__(self, logical):
+        self.logical = logical
+
+
+def rbf_rows64(P64, sq, gamma, r0, wr):
+    """FP64 kernel rows [r0, r0 + wr): exp(-gamma d^2), d^2 >= 0, unit diagonal."""
+    import torch
+
+    d2 = (sq[r0:r0 + wr, None] + sq[None, :] - 2.0 * (P64[r0:r0 + wr] @ P64.T)).clamp_(min=0.0)
+    K = torch.exp(-gamma * d2)
+    idx = torch.arange(wr, device=K.device)
+    K[idx, r0 + idx] = 1.0
+    return K
+
+
+def fp64_sigma(ctx, inp, cfg, rank, gamma=None):
+    """Top-rank singular values of SketchySVD in FP64 on the same input (dense
+    A, or the points of a Gauss-RBF kernel) and the context's own maps (as
+    exported: FP32 values, or the BF16 / E4M3 grid of the precision forms).
+    Sketches X, Y, Z by FP64 products on the device, window by window with
+    eta = nu = 1; the approximation by the oracle (initial_approx +
+    low_rank_approx, FP64 LAPACK) on the host."""
+    import torch
+
+    from oracle import sketchy_oracle as O
+    from skema_b200 import _lib as L
+
+    dev = inp.device
+    M = {w: np.ascontiguousarray(ctx.map_export(w)[0]) for w in (L.UPSILON, L.OMEGA, L.PHI, L.PSI)}
+    U, Om, F, Ps = (torch.from_numpy(M[w]).to(dev) for w in (L.UPSILON, L.OMEGA, L.PHI, L.PSI))
+    k, s = U.shape[0], F.shape[0]
+    m = inp.shape[0]
+    n = m if gamma is not None else inp.shape[1]
+    W = cfg["window"]
+    X = torch.zeros((k, n), dtype=torch.float64, device=dev)
+    Y = torch.empty((m, k), dtype=torch.float64, device=dev)
+    Z = torch.zeros((s, s), dtype=torch.float64, device=dev)
+    if gamma is not None:
+        P64 = inp.double()
+        sq = (P64 * P64).sum(1)
+    for r0 in range(0, m, W):
+        wr = min(W, m - r0)
+        Aw = rbf_rows64(P64, sq, gamma, r0, wr) if gamma is not None else inp[r0:r0 + wr].double()
+        X += U[:, r0:r0 + wr] @ Aw
+        Y[r0:r0 + wr] = Aw @ Om.T
+        Z += F[:, r0:r0 + wr] @ (Aw @ Ps.T)
+        del Aw
+    o = O.OracleSketch.__new__(O.OracleSketch)
+    o.k, o.s, o.rank = k, s, rank
+    o.X, o.Y, o.Z = X.cpu().numpy(), Y.cpu().numpy(), Z.cpu().numpy()
+    o.maps = {"phi": _LogicalMap(M[L.PHI]), "psi": _LogicalMap(M[L.PSI])}
+    del X, Y, Z, U, Om, F, Ps
+    torch.cuda.empty_cache()
+    return o.low_rank_approx()[1]
+
+
+def sigma_accuracy(S, S64, form):
+    d = np.abs(np.asarray(S) - S64)
+    return {"vs": "FP64 SketchySVD on the same input and maps (FP64 device products, oracle approximation)",
+            "form": form, "rank": int(len(S64)), "max_rel_err_sigma_i": float(np.max(d / S64)),
+            "max_err_over_sigma_1": float(np.max(d) / S64[0]), "sigma_1": float(S64[0]),
+            "sigma_r": float(S64[-1])}
+
+
+def vjp64(P, gamma, Om, Ybar, want_grad=True, blk=2048):
+    """FP64 f = <Ybar, K Omega^T> of the RBF kernel sketch on the device, row
+    block by row block (K never whole), and with want_grad its exact gradient
+    w.r.t. the points and gamma (the unit diagonal contributes nothing)."""
+    import torch
+
+    P64 = P.double()
+    O64 = Om.double()
+    Yb = Ybar.double()
+    N = P64.shape[0]
+    sq = (P64 * P64).sum(1)
+    f = torch.zeros((), dtype=torch.float64, device=P.device)
+    if want_grad:
+        rows = torch.zeros(N, dtype=torch.float64, device=P.device)
+        cols = torch.zeros(N, dtype=torch.float64, device=P.device)
+        EX = torch.zeros_like(P64)
+        EtX = torch.zeros_like(P64)
+        dg = torch.zeros((), dtype=torch.float64, device=P.device)
+    for r0 in range(0, N, blk):
+        wr = min(blk, N - r0)
+        d2 = (sq[r0:r0 + wr, None] + sq[None, :] - 2.0 * (P64[r0:r0 + wr] @ P64.T)).clamp_(min=0.0)
+        K = torch.exp(-gamma * d2)
+        idx = torch.arange(wr, device=P.device)
+        K[idx, r0 + idx] = 1.0
+        f += (Yb[r0:r0 + wr] * (K @ O64.T)).sum()
+        if want_grad:
+            E = (Yb[r0:r0 + wr] @ O64) * K
+            E[idx, r0 + idx] = 0.0
+            dg -= (E * d2).sum()
+            rows[r0:r0 + wr] += E.sum(1)
+            cols += E.sum(0)
+            EX[r0:r0 + wr] += E @ P64
+            EtX += E.T @ P64[r0:r0 + wr]
+            del E
+        del d2, K
+    if not want_grad:
+        return float(f)
+    dX = -2.0 * gamma * ((rows + cols)[:, None] * P64 - EX - EtX)
+    return float(f), dX, float(dg)
+
+
+def vjp_accuracy(P, gamma, Om, Ybar, dX, dg, seed=7):
+    """The device VJP against the FP64 gradient and against central finite
+    differences of the FP64 forward (h = 1e-3 relative): along a seeded
+    random direction V of the points, and in gamma."""
+    import torch
+
+    _, dX64, dg64 = vjp64(P, gamma, Om, Ybar)
+    g = torch.Generator(device=P.device)
+    g.manual_seed(seed)
+    V = torch.randn(P.shape, generator=g, device=P.device, dtype=torch.float64)
+    h = 1e-3 * float(P.double().pow(2).mean().sqrt())
+    fp = vjp64(P.double() + h * V, gamma, Om, Ybar, want_grad=False)
+    fm = vjp64(P.double() - h * V, gamma, Om, Ybar, want_grad=False)
+    fd_x = (fp - fm) / (2 * h)
+    hg = 1e-3 * gamma
+    fd_g = (vjp64(P, gamma + hg, Om, Ybar, want_grad=False) - vjp64(P, gamma - hg, Om, Ybar, want_grad=False)) / (
+        2 * hg)
+    dir_dev = float((dX.double() * V).sum())
+    dir_64 = float((dX64 * V).sum())
+    rel = lambda a, b: abs(a - b) / max(abs(b), 1e-300)
+    return {"vs": "FP64 gradient on the device and central FD of the FP64 forward (h = 1e-3 relative)",
+            "dX_rel_fro_vs_fp64": float((dX.double() - dX64).norm() / dX64.norm()),
+            "dgamma_rel_vs_fp64": rel(dg, dg64),
+            "fd_direction_rel": rel(dir_dev, fd_x), "fd_gamma_rel": rel(dg, fd_g),
+            "fp64_vs_fd_direction_rel": rel(dir_64, fd_x), "fp64_vs_fd_gamma_rel": rel(dg64, fd_g)}
+
+
 # ------------------------------------------------------- CPU baseline ------
-def cpu_sample_sparse(cfg, budget_s, seed_rows=None):
+def cpu_sample_sparse(cfg, budget_s, seed_rows=None, csr=None):
     """Oracle (FP64 CRS x SparseSign restatement, OpenMP) on windows of the
-    workload until budget_s elapses; returns (rows/s, rows, threads)."""
+    workload until budget_s elapses (budget_s None: all rows); returns
+    (rows/s, rows, threads, oracle sketch). csr: the workload's host arrays,
+    when the caller already made them."""
     import scipy.sparse as sp
 
     from oracle import sketchy_oracle as O
 
     m, n, w = cfg["m"], cfg["n"], cfg["window"]
     rows_max = seed_rows or m
-    rowptr, col, val = make_csr_numpy(cfg, rows_max, cfg["seed"])
+    rowptr, col, val = csr if csr is not None else make_csr_numpy(cfg, rows_max, cfg["seed"])
     A = sp.csr_matrix((val.astype(np.float64), col, rowptr), shape=(rows_max, n))
     o = O.OracleSketch(m, n, cfg["rank"], w, kind=1, issparse=True, sketch_range=cfg["k"], sketch_core=cfg["s"])
     t0 = time.perf_counter()
     done = 0
-    while done < rows_max and time.perf_counter() - t0 < budget_s:
+    while done < rows_max and (budget_s is None or time.perf_counter() - t0 < budget_s):
         wr = min(w, rows_max - done)
         o.update_rows(A, done, wr)
         done += wr
     dt = time.perf_counter() - t0
-    return done / dt, done, O.num_threads()
+    return done / dt, done, O.num_threads(), o
 
 
 def cpu_sample_dense(cfg, budget_s):
@@ -845,18 +971,22 @@ def cpu_sample_vjp(cfg, ns=1000):
     return N / (ts * (N / ns) ** 2), ns, O.num_threads()
 
 
-def cpu_baseline(args, cfg, budget_s):
+def cpu_baseline(args, cfg, budget_s, csr=None):
+    """The CPU baseline leg; for the sparse workload it runs the oracle over
+    every row of the same matrix (csr) and also returns that oracle sketch,
+    which the parity check compares with the device's sketches."""
+    o = None
     if cfg.get("rbf"):
         v, rows, thr = cpu_sample_rbf(cfg, budget_s)
         sample = f"{rows} kernel rows (windows of 1024) of a same-recipe point set, FP64"
     elif args.workload.startswith("csr"):
-        v, rows, thr = cpu_sample_sparse(cfg, budget_s)
-        sample = f"first {rows} rows ({rows // cfg['window']} windows) of the workload, FP64"
+        v, rows, thr, o = cpu_sample_sparse(cfg, None, csr=csr)
+        sample = f"all {rows} rows ({rows // cfg['window']} windows) of the workload, FP64"
     else:
         v, rows, thr = cpu_sample_dense(cfg, budget_s)
         sample = f"{rows} rows (whole windows of {cfg['window']}) of a same-shape FP64 matrix"
     return {"value": v, "unit": "rows/s", "cores": thr, "kind": "port", "sample": sample,
-            "host_cpu": _cpu_model(), "nproc": os.cpu_count()}
+            "host_cpu": _cpu_model(), "nproc": os.cpu_count()}, o
 
 
 def _cpu_model():
@@ -885,7 +1015,7 @@ def run_reference(args, cfg):
         elif cfg.get("rbf"):
             v, r, thr = cpu_sample_rbf(cfg, budget)
         elif args.workload.startswith("csr"):
-            v, r, thr = cpu_sample_sparse(cfg, budget, seed_rows=min(cfg["m"], 200_000))
+            v, r, thr, _ = cpu_sample_sparse(cfg, budget, seed_rows=min(cfg["m"], 200_000))
         else:
             v, r, thr = cpu_sample_dense(cfg, budget)
         if i >= args.warmup:
@@ -906,6 +1036,46 @@ def run_reference(args, cfg):
     print(json.dumps(out), flush=True)
 
 
+# The other configurations, measured in the default run after the headline
+# (one GPU): the dense 200,000 x 20,000 Gaussian case in the plain FP32 form
+# and the BF16 / FP8 precision forms, the RBF kernel case in FP32 and BF16,
+# and the kernel-sketch forward / adjoint pair in FP32 and BF16. Steps per
+# workload are fewer for the slow plain forms.
+SECONDARY = (("dense-fp32", 3), ("dense-bf16", 10), ("dense-fp8", 10), ("rbf-fp32", 2), ("rbf-bf16", 5),
+             ("rbf-vjp", 3), ("rbf-vjp-bf16", 10))
+
+
+def run_secondary(args, peaks, peak_kind):
+    import torch
+
+    res = {}
+    for wl, steps in SECONDARY:
+        sub = argparse.Namespace(**vars(args))
+        sub.workload, sub.steps, sub.warmup = wl, steps, 3
+        sub.no_e2e = sub.no_cpu = sub.no_residuals = True
+        sub.clock_lead, sub.clock_tail = 0.5, 0.1
+        cfg = dict(WORKLOADS[wl])
+        out = run_vjp(sub, cfg, peaks, peak_kind) if cfg.get("vjp") else run_gpu(sub, cfg, peaks, peak_kind)
+        torch.cuda.empty_cache()
+        roof = out["roofline"]
+        keep = ("bound", "achieved", "peak", "unit", "frac", "kernel", "kernel_ms", "peak_source")
+        r = {key: roof[key] for key in keep if key in roof}
+        if "other_kernel" in roof:
+            r["other_kernel"] = {key: roof["other_kernel"][key] for key in keep if key in roof["other_kernel"]}
+        if "step_tflops" in roof:
+            r["step_tflops"] = roof["step_tflops"]
+        res[wl] = {"value": out["value"], "unit": out["unit"], "ms_per_step": out["ms_per_step"],
+                   "steps": steps, "warmup": 3, "dtype": out["dtype"], "config": out["config"], "roofline": r,
+                   "accuracy": out.get("accuracy"), "gpu_launches": out["gpu_launches"], "clocks": out["clocks"]}
+    sp = lambda a, b: res[a]["ms_per_step"] / res[b]["ms_per_step"]
+    res["speedups"] = {"dense_bf16_over_fp32": sp("dense-fp32", "dense-bf16"),
+                       "dense_fp8_over_fp32": sp("dense-fp32", "dense-fp8"),
+                       "rbf_bf16_over_fp32": sp("rbf-fp32", "rbf-bf16"),
+                       "vjp_bf16_over_fp32": sp("rbf-vjp", "rbf-vjp-bf16"),
+                       "note": "ms per step of the plain FP32 form over the precision form, same input"}
+    return res
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -917,12 +1087,15 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-residuals", action="store_true", help="skip the residual-pass timing")
     ap.add_argument("--no-accuracy", action="store_true",
-                    help="skip the reduced-precision forms' singular-value check against the FP32 path")
+                    help="skip the parity checks against FP64 (sketches, singular values, adjoint)")
     ap.add_argument("--cpu-budget", type=float, default=12.0)
     ap.add_argument("--clock-lead", type=float, default=1.0, help="seconds of load before the timed steps")
     ap.add_argument("--clock-tail", type=float, default=0.3, help="seconds of load after the timed steps")
     ap.add_argument("--rows", type=int, default=0,
                     help="rows per GPU instead of the workload's (small cases for profiling)")
+    ap.add_argument("--no-secondary", action="store_true",
+                    help="measure only the headline workload (the default run on one GPU also measures the "
+                         "dense, RBF and adjoint configurations after it)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     cfg = dict(WORKLOADS[args.workload])
@@ -932,10 +1105,13 @@ def main():
         run_reference(args, cfg)
         return
     peaks, kind = load_peaks()
-    if cfg.get("vjp"):
-        run_vjp(args, cfg, peaks, kind)
+    out = run_vjp(args, cfg, peaks, kind) if cfg.get("vjp") else run_gpu(args, cfg, peaks, kind)
+    if out is None:
         return
-    run_gpu(args, cfg, peaks, kind)
+    if (int(os.environ.get("WORLD_SIZE", "1")) == 1 and args.workload == "csr-sparse-sign" and args.rows == 0
+            and not args.no_secondary):
+        out["secondary"] = run_secondary(args, peaks, kind)
+    print(json.dumps(out), flush=True)
 
 
 if __name__ == "__main__":

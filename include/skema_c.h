@@ -50,7 +50,12 @@ typedef enum {
 /* ---- enums mirroring src/Skema_Utils.hpp:38-80 ------------------------- */
 enum { SKEMA_MAP_GAUSS = 0, SKEMA_MAP_SPARSE_SIGN = 1 };    /* DimRedux_Map */
 enum { SKEMA_KERNEL_NONE = 0, SKEMA_KERNEL_GAUSSRBF = 1 };  /* Kernel_Map   */
-/* Arithmetic of the sketch contractions (new; the reference is FP64 only). */
+/* Arithmetic of the sketch contractions (new; the reference is FP64 only).
+ * With Gauss maps on a dense or kernel input, the BF16 and FP8 forms hold the
+ * maps on the grid of their arithmetic (every value rounded to BF16, or to
+ * E4M3 times a power-of-two scale), at creation and after each map import:
+ * the tensor-core products, the FP32 kernels and the FP64 approximation then
+ * all use the same maps, and skema_map_export returns those values. */
 enum { SKEMA_PREC_FP32 = 0, SKEMA_PREC_BF16 = 1, SKEMA_PREC_FP8 = 2 };
 /* Which map, in the order of AlgParams::seeds (src/Skema_SketchySVD.cpp:37,54,70,87). */
 enum { SKEMA_UPSILON = 0, SKEMA_OMEGA = 1, SKEMA_PHI = 2, SKEMA_PSI = 3 };
@@ -255,6 +260,65 @@ int skema_rbf_sketch_vjp(skema_ctx* ctx, const float* pts, int64_t npts,
 int skema_rbf_sketch_fwd_noalloc(skema_ctx* ctx, const float* pts,
                                  int64_t npts, int64_t d, double gamma,
                                  const float* omega, int64_t k, float* Y);
+
+/* ---- standalone maps: GaussDimRedux / SparseSignDimRedux ---------------- */
+/* A random map with its lmap / rmap products (src/Skema_DimRedux.hpp:60-268).
+ * The map is generated on the device exactly as a context's map of the same
+ * kind, stored shape nrow x ncol and seed, so a caller can apply the sketch
+ * operators by hand. The products take FP32 operands and accumulate in FP32
+ * (the FP32 SIMT GEMM); a SparseSign map is expanded once into a dense FP32
+ * copy (duplicate entries summed) for them. The products are stated
+ * without the reference's conventions -- the C++ layer in skema.hpp maps the
+ * reference's calls (its init_transposed swap, its transposed CRS results)
+ * onto them:
+ *   lmap:  C = alpha op(M(:, idx)) op(B) + beta C   idx = stored columns
+ *   rmap:  C = alpha op(A) op(M(idx, :)) + beta C   idx = stored rows
+ * op(X) = X for 'N', X^T for 'T'; idx = [idx_first, idx_second), the whole
+ * map when idx_first == idx_second. `mem` says where A / B and C live; every
+ * descriptor's pointer follows it. */
+typedef struct skema_dimredux skema_dimredux;
+typedef struct {
+  float* p;        /* element (0, 0)                                       */
+  int64_t rows, cols, ld;
+  int32_t layout;  /* SKEMA_COL_MAJOR or SKEMA_ROW_MAJOR                    */
+} skema_matf;
+typedef struct {
+  const int64_t* rowptr; /* rows + 1 absolute offsets into col / val        */
+  const int32_t* col;    /* column indices in [0, cols) (others skipped)    */
+  const float* val;
+  int64_t rows, cols;
+} skema_csrf;
+/* GaussDimRedux / SparseSignDimRedux ctor (src/Skema_DimRedux.hpp:98-128,
+ * 191-268): kind SKEMA_MAP_*, stored shape nrow x ncol, seed. */
+int skema_dimredux_create(int32_t kind, int64_t nrow, int64_t ncol,
+                          int32_t seed, int32_t device, skema_dimredux** out);
+int skema_dimredux_destroy(skema_dimredux* map);
+/* Message of the last failed call on map ("" if none). */
+const char* skema_dimredux_last_error(const skema_dimredux* map);
+/* The map's values, as skema_map_export gives a context's map. */
+int skema_dimredux_export(skema_dimredux* map, double* values,
+                          int32_t* indices);
+/* DimRedux::lmap / rmap on a dense operand
+ * (src/Skema_DimRedux_Gauss.cpp:10-52, src/Skema_DimRedux_SparseSign.cpp:9-51). */
+int skema_dimredux_lmap(skema_dimredux* map, double alpha, const skema_matf* B,
+                        double beta, char transA, char transB,
+                        int64_t idx_first, int64_t idx_second, skema_matf* C,
+                        int32_t mem);
+int skema_dimredux_rmap(skema_dimredux* map, double alpha, const skema_matf* A,
+                        double beta, char transA, char transB,
+                        int64_t idx_first, int64_t idx_second, skema_matf* C,
+                        int32_t mem);
+/* DimRedux::lmap / rmap on a CRS operand
+ * (src/Skema_DimRedux_Gauss.cpp:54-99, src/Skema_DimRedux_SparseSign.cpp:53-111):
+ * B (lmap) or A (rmap) is the CSR matrix; C is dense. */
+int skema_dimredux_lmap_csr(skema_dimredux* map, double alpha,
+                            const skema_csrf* B, double beta, char transA,
+                            char transB, int64_t idx_first, int64_t idx_second,
+                            skema_matf* C, int32_t mem);
+int skema_dimredux_rmap_csr(skema_dimredux* map, double alpha,
+                            const skema_csrf* A, double beta, char transA,
+                            char transB, int64_t idx_first, int64_t idx_second,
+                            skema_matf* C, int32_t mem);
 
 /* ---- matrix files ----------------------------------------------------- */
 /* Skema::read_matrix / write_matrix (src/Skema_IO.hpp:10-40,

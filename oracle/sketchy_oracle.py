@@ -394,7 +394,10 @@ def rbf_vjp64(X, gamma, Omega, Ybar):
     unit diagonal contributing nothing."""
     X = np.asarray(X, dtype=np.float64)
     K = rbf_kernel(X, gamma)
-    D2 = ((X[:, None, :] - X[None, :, :]) ** 2).sum(-1)
+    N = X.shape[0]
+    D2 = np.empty((N, N))
+    for i0 in range(0, N, 64):  # explicit differences, 64 rows at a time
+        D2[i0:i0 + 64] = ((X[i0:i0 + 64, None, :] - X[None, :, :]) ** 2).sum(-1)
     M = Ybar @ Omega
     E = M * K
     np.fill_diagonal(E, 0.0)

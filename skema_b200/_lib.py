@@ -74,6 +74,20 @@ class Dense(C.Structure):
     _fields_ = [("nrow", C.c_int64), ("ncol", C.c_int64), ("data", C.POINTER(C.c_double))]
 
 
+class MatF(C.Structure):
+    """``skema_matf``: a dense FP32 operand of the map products."""
+
+    _fields_ = [("p", C.c_void_p), ("rows", C.c_int64), ("cols", C.c_int64), ("ld", C.c_int64),
+                ("layout", C.c_int32)]
+
+
+class CsrF(C.Structure):
+    """``skema_csrf``: a CSR FP32 operand of the map products."""
+
+    _fields_ = [("rowptr", C.c_void_p), ("col", C.c_void_p), ("val", C.c_void_p), ("rows", C.c_int64),
+                ("cols", C.c_int64)]
+
+
 _P = C.c_void_p
 _I64 = C.c_int64
 _I32 = C.c_int32
@@ -111,6 +125,18 @@ SIGNATURES = {
     "skema_launch_count": (_I64, [_P]),
     "skema_timing_enable": (C.c_int, [_P, _I32]),
     "skema_timing_get": (C.c_int, [_P, C.c_char_p, C.POINTER(C.c_double), C.POINTER(_I64)]),
+    "skema_dimredux_create": (C.c_int, [_I32, _I64, _I64, _I32, _I32, C.POINTER(_P)]),
+    "skema_dimredux_destroy": (C.c_int, [_P]),
+    "skema_dimredux_last_error": (C.c_char_p, [_P]),
+    "skema_dimredux_export": (C.c_int, [_P, _P, _P]),
+    "skema_dimredux_lmap": (C.c_int, [_P, _D, C.POINTER(MatF), _D, C.c_char, C.c_char, _I64, _I64,
+                                      C.POINTER(MatF), _I32]),
+    "skema_dimredux_rmap": (C.c_int, [_P, _D, C.POINTER(MatF), _D, C.c_char, C.c_char, _I64, _I64,
+                                      C.POINTER(MatF), _I32]),
+    "skema_dimredux_lmap_csr": (C.c_int, [_P, _D, C.POINTER(CsrF), _D, C.c_char, C.c_char, _I64, _I64,
+                                          C.POINTER(MatF), _I32]),
+    "skema_dimredux_rmap_csr": (C.c_int, [_P, _D, C.POINTER(CsrF), _D, C.c_char, C.c_char, _I64, _I64,
+                                          C.POINTER(MatF), _I32]),
     "skema_read_crs": (C.c_int, [C.c_char_p, C.POINTER(Crs)]),
     "skema_crs_free": (None, [C.POINTER(Crs)]),
     "skema_read_dense": (C.c_int, [C.c_char_p, C.POINTER(Dense)]),

@@ -371,6 +371,12 @@ __global__ void fp8_round_map_kernel(float* __restrict__ v, int64_t count, float
     v[q] = from_e4m3(to_e4m3(v[q] * sm)) * inv;
 }
 
+// Every map value rounded to the nearest BF16 value, kept in FP32.
+__global__ void bf16_round_map_kernel(float* __restrict__ v, int64_t count) {
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < count; q += (int64_t)gridDim.x * blockDim.x)
+    v[q] = __bfloat162float(__float2bfloat16(v[q]));
+}
+
 // Logical map rows [0, rows) -> E4M3(sm * map) at D[(r0 + r) * ld + j].
 __global__ void fp8_op_kernel(const float* __restrict__ f, int64_t rs, int64_t cs, int64_t rows, int64_t cols,
                               float sm, uint8_t* __restrict__ D, int64_t ld) {
@@ -586,6 +592,16 @@ void tc_prepare_maps(skema_ctx* c) {
     };
     conv8(c->omg, 0);
     conv8(c->psi, c->k);
+  } else {
+    // BF16 form: the maps themselves move onto the BF16 grid, so that the
+    // tensor-core products, the FP32 kernels and the FP64 approximation
+    // (Phi~ Q, Psi~ P) all use the same map values
+    for (Map* M : {&c->ups, &c->omg, &c->phi, &c->psi}) {
+      const int64_t cnt = M->lrows * M->lcols;
+      const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((cnt + 255) / 256, c->sm_count * 16));
+      bf16_round_map_kernel<<<grid, 256, 0, c->stream>>>(M->f32, cnt);
+      SKEMA_LAUNCHED(c);
+    }
   }
   const int64_t mp = pad8(c->m), np = pad8(c->n);
   if (!c->ups.lowp) {

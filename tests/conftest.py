@@ -63,3 +63,26 @@ def rel_fro(a, b) -> float:
     b = np.asarray(b, dtype=np.float64)
     nb = np.linalg.norm(b)
     return float(np.linalg.norm(a - b) / (nb if nb > 0 else 1.0))
+
+
+CPP_PROGRAMS = ("sketch_driver", "dimredux_check", "parse_params")
+
+
+@pytest.fixture(scope="session")
+def cpp_bins(lib_built, tmp_path_factory):
+    """The C++ programs under tests/cpp, compiled with g++ against
+    include/skema.hpp and linked with the CUDA library (name -> path)."""
+    import subprocess
+
+    out = tmp_path_factory.mktemp("cpp")
+    libdir = os.path.join(ROOT, "skema_b200")
+    bins = {}
+    for name in CPP_PROGRAMS:
+        exe = str(out / name)
+        cmd = ["g++", "-std=c++17", "-O1", "-Wall", "-Wextra", "-Werror", "-I" + os.path.join(ROOT, "include"),
+               os.path.join(ROOT, "tests", "cpp", name + ".cpp"), "-L" + libdir, "-lskema_b200",
+               "-Wl,-rpath," + libdir, "-o", exe]
+        res = subprocess.run(cmd, capture_output=True, text=True)
+        assert res.returncode == 0, res.stderr
+        bins[name] = exe
+    return bins

@@ -1,8 +1,10 @@
 """GPU parity tests of the BF16 tensor-core form of the dense Gauss sketch.
 
-The input window and the maps are rounded to BF16 (8-bit significand,
-unit roundoff 2^-9) and every product accumulates in FP32, so the sketches
-are compared with the FP64 oracle on the same inputs and maps at a relative
+The context holds its maps on the BF16 grid (every value rounded to BF16,
+also in the FP32 copies the approximation uses), so the oracle takes the
+same maps. The input window is rounded to BF16 (8-bit significand, unit
+roundoff 2^-9) and every product accumulates in FP32, so the sketches are
+compared with the FP64 oracle on the same inputs and maps at a relative
 Frobenius tolerance of 6e-3: about three times the error of one rounding of
 each operand of a sum of random-signed terms. Z sees two roundings (T is
 kept in BF16 between its two products) and gets 1e-2.
@@ -37,6 +39,32 @@ def bf16(a, sk):
     return a
 
 
+def bf16_grid(maps):
+    """The BF16 context's version of the oracle maps (dict name -> Map): the
+    FP64 values rounded to FP32, then to BF16 (round to nearest even)."""
+    import torch
+
+    for mp in maps.values():
+        mp._dense = torch.from_numpy(np.asarray(mp.dense)).float().bfloat16().double().numpy()
+
+
+def oracle_bf16(oracle, a, **kw):
+    o = oracle_for(oracle, a, **kw)
+    bf16_grid(o.maps)
+    return o
+
+
+def test_bf16_maps_on_the_bf16_grid(sk, oracle):
+    m, n = 600, 300
+    a = bf16(alg(sk, m, n, 5, 100, 0), sk)
+    o = oracle_bf16(oracle, a)
+    with sk.SketchySVD(a) as s:
+        for which, name in ((sk._lib.UPSILON, "upsilon"), (sk._lib.OMEGA, "omega"), (sk._lib.PHI, "phi"),
+                            (sk._lib.PSI, "psi")):
+            got = s.map_export(which)[0]
+            assert np.array_equal(got, o.maps[name].dense), name
+
+
 def check(s, o, tag=""):
     X, Y, Z = s.get_sketches()
     ex, ey, ez = rel_fro(X, o.X), rel_fro(Y, o.Y), rel_fro(Z, o.Z)
@@ -53,7 +81,7 @@ def test_dense_bf16_parity(sk, oracle, layout):
     A = dense_input(m, n).astype(np.float32)
     A = np.asfortranarray(A) if layout == "F" else np.ascontiguousarray(A)
     a = bf16(alg(sk, m, n, 10, 100, 0), sk)  # windows start at 100, 200, ...: both alignments
-    o = oracle_for(oracle, a)
+    o = oracle_bf16(oracle, a)
     o.linear_update(A.astype(np.float64))
     with sk.SketchySVD(a) as s:
         s.linear_update(A)
@@ -66,7 +94,7 @@ def test_dense_bf16_split_k_eta_nu_two_calls(sk, oracle):
     m, n = 4096, 3000
     A = dense_input(m, n, seed=11).astype(np.float32)
     a = bf16(alg(sk, m, n, 50, 2048, 0, sketch_eta=1.25, sketch_nu=0.8), sk)
-    o = oracle_for(oracle, a)
+    o = oracle_bf16(oracle, a)
     o.linear_update(A.astype(np.float64))
     At = torch.from_numpy(A).cuda()
     with sk.SketchySVD(a) as s:
@@ -86,7 +114,7 @@ def test_dense_bf16_ragged_window(sk, oracle, layout, n):
     A = dense_input(m, n, seed=5).astype(np.float32)
     A = np.asfortranarray(A) if layout == "F" else np.ascontiguousarray(A)
     a = bf16(alg(sk, m, n, 7, 129, 0, sketch_nu=0.5), sk)
-    o = oracle_for(oracle, a)
+    o = oracle_bf16(oracle, a)
     o.linear_update(A.astype(np.float64))
     with sk.SketchySVD(a) as s:
         s.linear_update(A)
@@ -101,7 +129,7 @@ def test_dense_bf16_device_column_major_offsets(sk, oracle):
     m, n = 252, 512
     A = dense_input(m, n, seed=12).astype(np.float32)
     a = bf16(alg(sk, m, n, 5, 96, 0, sketch_eta=0.5), sk)
-    o = oracle_for(oracle, a)
+    o = oracle_bf16(oracle, a)
     o.linear_update(A.astype(np.float64))
     At = torch.from_numpy(np.asfortranarray(A)).cuda().t().contiguous().t()
     assert At.stride() == (1, m)
@@ -115,7 +143,7 @@ def test_rbf_bf16_parity(sk, oracle):
     P = oracle.mixture_points(N, d, seed=1)
     gamma = oracle.median_gamma(P)
     a = bf16(alg(sk, N, N, 6, 128, 0, kernel_func=1, kernel_gamma=gamma, force_three_sketch=True), sk)
-    o = oracle_for(oracle, a, gamma=gamma)
+    o = oracle_bf16(oracle, a, gamma=gamma)
     o.linear_update(P.astype(np.float64))
     with sk.SketchySVD(a) as s:
         s.linear_update(P)
@@ -134,7 +162,7 @@ def test_rbf_bf16_tensor_core_parity(sk, oracle, N, d, rank, window, eta, nu):
     gamma = oracle.median_gamma(P)
     a = bf16(alg(sk, N, N, rank, window, 0, kernel_func=1, kernel_gamma=gamma, force_three_sketch=True,
                  sketch_eta=eta, sketch_nu=nu), sk)
-    o = oracle_for(oracle, a, gamma=gamma)
+    o = oracle_bf16(oracle, a, gamma=gamma)
     o.linear_update(P.astype(np.float64))
     with sk.SketchySVD(a) as s:
         s.linear_update(P)
@@ -151,7 +179,7 @@ def test_rbf_bf16_blocks_and_dirty_rows(sk, oracle, nu):
     gamma = oracle.median_gamma(P)
     a = bf16(alg(sk, N, N, 10, 300, 0, kernel_func=1, kernel_gamma=gamma, force_three_sketch=True,
                  sketch_eta=1.1, sketch_nu=nu), sk)
-    o = oracle_for(oracle, a, gamma=gamma)
+    o = oracle_bf16(oracle, a, gamma=gamma)
     o.reset()
     calls = [(0, 1000), (1000, 1000), (400, 600)]
     for r0, nr in calls:
