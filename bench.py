@@ -541,12 +541,25 @@ def run_gpu(args, cfg, peaks, peak_kind):
     if rank == 0 and world == 1 and not args.no_residuals and not (rbf and a.precision):
         step()
         # the fixed-rank approximation (FP64, on the device), timed on its
-        # own: CholeskyQR2 of Y and X^T, the core solve and the small SVD
+        # own: CholeskyQR2 of Y and X^T, the core solve and the small SVD,
+        # into device buffers (CUDA events), then once more into host memory
+        r = cfg["rank"]
+        n_out = m_glob if rbf else n
+        Ud = torch.empty((r, m_local), dtype=torch.float64, device=dev)  # column-major m x r
+        Vd = torch.empty((r, n_out), dtype=torch.float64, device=dev)
+        Sd = torch.empty(r, dtype=torch.float64, device=dev)
+        a0e = torch.cuda.Event(enable_timing=True)
+        a1e = torch.cuda.Event(enable_timing=True)
+        ctx.low_rank_approx(device_out=(Ud, Sd, Vd))  # warm
+        torch.cuda.synchronize()
+        a0e.record(stream)
+        ctx.low_rank_approx(device_out=(Ud, Sd, Vd))
+        a1e.record(stream)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         U, S, V = ctx.low_rank_approx()
-        approx = {"ms": (time.perf_counter() - t0) * 1e3,
-                  "timer": "host wall clock around the synchronous call, outputs copied to host"}
+        approx = {"ms": a0e.elapsed_time(a1e), "timer": "CUDA events, outputs in device memory",
+                  "ms_with_host_copy": (time.perf_counter() - t0) * 1e3}
         r0e = torch.cuda.Event(enable_timing=True)
         r1e = torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()

@@ -394,6 +394,7 @@ class _Context:
         self._stream(A, row0, nrows, "skema_linear_update")
 
     def _stream(self, A, row0, nrows, prefix):
+        self._torch_inputs_ready(*(A if isinstance(A, tuple) else (A,)))
         if self.alg.kernel_func == L.KERNEL_GAUSSRBF:
             ptr, ld, layout, mem, keep = _dense_arg(A)
             npts, d = A.shape
@@ -496,6 +497,34 @@ class _Context:
     def set_stream(self, stream_handle: int | None):
         """Launch on an external cudaStream_t (e.g. torch's current stream)."""
         self._check(self.lib.skema_set_stream(self.h, stream_handle))
+        self._stream_handle = stream_handle
+
+    # -- ordering against torch's stream ----------------------------------
+    # The library launches on the context's stream. Unless that is torch's
+    # current stream (set_stream), device tensors written by torch must be
+    # complete before a call reads them, and device tensors the library
+    # writes must be complete before torch reads them.
+    def _on_torch_stream(self, t) -> bool:
+        import torch
+
+        h = getattr(self, "_stream_handle", None)
+        return h is not None and h == torch.cuda.current_stream(t.device).cuda_stream
+
+    def _torch_inputs_ready(self, *tensors):
+        for t in tensors:
+            if _is_torch(t) and t.is_cuda:
+                if not self._on_torch_stream(t):
+                    import torch
+
+                    torch.cuda.current_stream(t.device).synchronize()
+                return
+
+    def _torch_outputs_ready(self, *tensors):
+        for t in tensors:
+            if _is_torch(t) and t.is_cuda:
+                if not self._on_torch_stream(t):
+                    self.synchronize()
+                return
 
     # -- sketches ---------------------------------------------------------
     def _sketch_shape(self, which):
@@ -508,6 +537,7 @@ class _Context:
             out = np.empty(shape, dtype=np.float32)
         if _is_torch(out):
             self._check(self.lib.skema_get_sketch(self.h, which, out.data_ptr(), shape[1], L.ROW_MAJOR, L.MEM_DEVICE))
+            self._torch_outputs_ready(out)
         else:
             self._check(self.lib.skema_get_sketch(self.h, which, out.ctypes.data, shape[1], L.ROW_MAJOR, L.MEM_HOST))
         return out
@@ -515,6 +545,7 @@ class _Context:
     def set_sketch(self, which, buf):
         shape = self._sketch_shape(which)
         if _is_torch(buf):
+            self._torch_inputs_ready(buf)
             self._check(self.lib.skema_set_sketch(self.h, which, buf.data_ptr(), shape[1], L.ROW_MAJOR, L.MEM_DEVICE))
         else:
             b = np.ascontiguousarray(buf, dtype=np.float32)
@@ -565,6 +596,7 @@ class SketchySVD(_Context):
         if device_out is not None:
             U, S, V = device_out
             self._check(self.lib.skema_low_rank_approx(self.h, U.data_ptr(), S.data_ptr(), V.data_ptr(), L.MEM_DEVICE))
+            self._torch_outputs_ready(U)
             return U, S, V
         U = np.empty((r, self.nrow), dtype=np.float64)
         V = np.empty((r, self.ncol), dtype=np.float64)
@@ -589,6 +621,7 @@ class SketchySPD(_Context):
         if device_out is not None:
             U, S = device_out
             self._check(self.lib.skema_low_rank_approx(self.h, U.data_ptr(), S.data_ptr(), None, L.MEM_DEVICE))
+            self._torch_outputs_ready(U)
             return U, S
         U = np.empty((r, self.nrow), dtype=np.float64)
         S = np.empty(r, dtype=np.float64)
@@ -725,6 +758,7 @@ def rbf_sketch_fwd(pts, gamma: float, omega, ctx: _Context | None = None, precis
         N, d = pts.shape
         k = omega.shape[0]
         Y = torch.empty((N, k), dtype=torch.float32, device=pts.device)
+        ctx._torch_inputs_ready(pts, omega, Y)
         ctx._check(ctx.lib.skema_rbf_sketch_fwd(ctx.h, pts.data_ptr(), N, d, float(gamma), omega.data_ptr(), k, Y.data_ptr()))
         ctx.synchronize()
         return Y
@@ -748,6 +782,7 @@ def rbf_sketch_vjp(pts, gamma: float, omega, Ybar, ctx: _Context | None = None, 
         k = omega.shape[0]
         dX = torch.empty_like(pts)
         dg = torch.zeros(1, dtype=torch.float64, device=pts.device)
+        ctx._torch_inputs_ready(pts, omega, Ybar, dg)
         ctx._check(ctx.lib.skema_rbf_sketch_vjp(ctx.h, pts.data_ptr(), N, d, float(gamma), omega.data_ptr(), k,
                                                 Ybar.data_ptr(), dX.data_ptr(), dg.data_ptr()))
         ctx.synchronize()

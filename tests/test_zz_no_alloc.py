@@ -49,6 +49,7 @@ def test_rbf_fwd_noalloc_matches_oracle_and_regular_entry_point(lib_built, oracl
             Xd, Od = torch.from_numpy(X).cuda(), torch.from_numpy(Om).cuda()
             Yd = torch.full((N, k), float("nan"), dtype=torch.float32, device="cuda")
             data.append((N, d, k, X, gamma, Om, Xd, Od, Yd))
+        torch.cuda.synchronize()  # the inputs' copies are complete before the library's stream reads them
         # warm-up call: the array's address is looked up on first use
         N, d, k, X, gamma, Om, Xd, Od, Yd = data[0]
         assert lib.skema_rbf_sketch_fwd_noalloc(ctx.h, Xd.data_ptr(), N, d, gamma, Od.data_ptr(), k,
