@@ -22,6 +22,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <initializer_list>
 #include <limits>
 #include <vector>
 
@@ -374,15 +375,26 @@ __global__ void svd_finish_kernel(const double* A, const double* V, int64_t k, d
 }
 
 // ------------------------------------------------------------ helpers ------
-struct DevBuf {
-  void* p = nullptr;
-  explicit DevBuf(size_t bytes) { SKEMA_CUDA(cudaMalloc(&p, std::max<size_t>(bytes, 16))); }
-  ~DevBuf() {
-    if (p) cudaFree(p);
+// Buffers of one approximation call, carved from the context's workspace
+// (grown once, then reused by every later call: no allocation per call).
+class Carve {
+ public:
+  Carve(skema_ctx* c, std::initializer_list<size_t> bytes) {
+    size_t total = 0;
+    for (size_t b : bytes) total += round(b);
+    base_ = static_cast<char*>(workspace(c, total));
+    at_ = base_;
   }
-  DevBuf(const DevBuf&) = delete;
-  DevBuf& operator=(const DevBuf&) = delete;
-  double* d() const { return (double*)p; }
+  double* take(size_t bytes) {
+    char* p = at_;
+    at_ += round(bytes);
+    return reinterpret_cast<double*>(p);
+  }
+
+ private:
+  static size_t round(size_t b) { return (std::max<size_t>(b, 16) + 255) / 256 * 256; }
+  char* base_;
+  char* at_;
 };
 
 int g1(const skema_ctx* c, int64_t total) {
@@ -402,9 +414,12 @@ void cholqr(skema_ctx* c, double* Qm, int64_t rows, int64_t k, double* Rout, dou
   SKEMA_LAUNCHED(c);
   int passes_left = 2;
   bool shifted = false;
+  // each pass writes Q R^{-1} into the other of the two buffers
+  double* cur = Qm;
+  double* nxt = work + 3 * k * k + 8;
   while (passes_left > 0) {
     // G = Q^T Q
-    dgemm<double, double>(c, k, k, rows, 1.0, Qm, rows, 1, Qm, 1, rows, 0.0, G, 1, k);
+    dgemm<double, double>(c, k, k, rows, 1.0, cur, rows, 1, cur, 1, rows, 0.0, G, 1, k);
     cholesky_kernel<<<1, 1024, 0, c->stream>>>(G, k, dstatus);
     SKEMA_LAUNCHED(c);
     int st = 0;
@@ -413,7 +428,7 @@ void cholqr(skema_ctx* c, double* Qm, int64_t rows, int64_t k, double* Rout, dou
     if (st != 0) {
       if (shifted) fail(SKEMA_ENOTPD, "Cholesky of the Gram matrix failed after the shifted pass");
       // shifted CholeskyQR: G + s I with s = 11 (rows*k + k(k+1)) u ||Q||_F^2
-      dgemm<double, double>(c, k, k, rows, 1.0, Qm, rows, 1, Qm, 1, rows, 0.0, G, 1, k);
+      dgemm<double, double>(c, k, k, rows, 1.0, cur, rows, 1, cur, 1, rows, 0.0, G, 1, k);
       trace_kernel<<<1, 256, 0, c->stream>>>(G, k, fro2);
       SKEMA_LAUNCHED(c);
       const double u = 1.1102230246251565e-16;
@@ -437,11 +452,9 @@ void cholqr(skema_ctx* c, double* Qm, int64_t rows, int64_t k, double* Rout, dou
     SKEMA_LAUNCHED(c);
     trsm_upper_kernel<<<(int)((k * 32 + 255) / 256), 256, 0, c->stream>>>(R, k, G, k, k);
     SKEMA_LAUNCHED(c);
-    // Qm <- Qm * Rinv  (rows x k) via a temporary in Rout's slot? use work tail
-    double* Qtmp = work + 3 * k * k + 8;
-    dgemm<double, double>(c, rows, k, k, 1.0, Qm, 1, rows, G, 1, k, 0.0, Qtmp, 1, rows, false);
-    SKEMA_CUDA(cudaMemcpyAsync(Qm, Qtmp, sizeof(double) * (size_t)(rows * k),
-                               cudaMemcpyDeviceToDevice, c->stream));
+    // next <- cur * Rinv  (rows x k)
+    dgemm<double, double>(c, rows, k, k, 1.0, cur, 1, rows, G, 1, k, 0.0, nxt, 1, rows, false);
+    std::swap(cur, nxt);
     // Racc <- R * Racc
     double* tmp = Rout;
     dgemm<double, double>(c, k, k, k, 1.0, R, 1, k, Racc, 1, k, 0.0, tmp, 1, k, false);
@@ -449,6 +462,8 @@ void cholqr(skema_ctx* c, double* Qm, int64_t rows, int64_t k, double* Rout, dou
                                cudaMemcpyDeviceToDevice, c->stream));
     --passes_left;
   }
+  if (cur != Qm)
+    SKEMA_CUDA(cudaMemcpyAsync(Qm, cur, sizeof(double) * (size_t)(rows * k), cudaMemcpyDeviceToDevice, c->stream));
   SKEMA_CUDA(cudaMemcpyAsync(Rout, Racc, sizeof(double) * (size_t)(k * k), cudaMemcpyDeviceToDevice,
                              c->stream));
 }
@@ -533,17 +548,15 @@ void spd_low_rank_approx(skema_ctx* c, double* Uout, double* Sout) {
   const bool ref_steps = c->p.spd_approx == SKEMA_SPD_REFERENCE_STEPS;
   const Map& O = c->omg;
   y_materialize(c);
-  DevBuf bY(sizeof(double) * (size_t)(m * k));
-  DevBuf bYe(sizeof(double) * (size_t)(m * k));
-  DevBuf bO(sizeof(double) * (size_t)(n * k));
-  DevBuf bW(sizeof(double) * cholqr_work_doubles(m, k));
-  DevBuf bsmall(sizeof(double) * (size_t)(8 * k * k + 4 * k + 64));
-  DevBuf bstat(sizeof(int) * 4);
-  double* Yd = bY.d();
-  double* Ye = bYe.d();
-  double* Od = bO.d();
-  double* W = bW.d();
-  double* G = bsmall.d();       // k x k
+  const size_t b_mk = sizeof(double) * (size_t)(m * k), b_nk = sizeof(double) * (size_t)(n * k);
+  const size_t b_w = sizeof(double) * cholqr_work_doubles(m, k);
+  const size_t b_small = sizeof(double) * (size_t)(8 * k * k + 4 * k + 64);
+  Carve cv(c, {b_mk, b_mk, b_nk, b_w, b_small, 16});
+  double* Yd = cv.take(b_mk);
+  double* Ye = cv.take(b_mk);
+  double* Od = cv.take(b_nk);
+  double* W = cv.take(b_w);
+  double* G = cv.take(b_small);  // k x k
   double* R = G + k * k;        // k x k
   double* Rinv = R + k * k;     // k x k
   double* Cw = Rinv + k * k;    // k x k
@@ -553,7 +566,7 @@ void spd_low_rank_approx(skema_ctx* c, double* Uout, double* Sout) {
   double* RE = Vt + k * k;      // k x k
   double* Sv = RE + k * k;      // k
   double* sig = Sv + k;         // k
-  int* st = (int*)bstat.p;
+  int* st = reinterpret_cast<int*>(cv.take(16));
 
   f2d_kernel<<<g1(c, m * k), 256, 0, c->stream>>>(c->Y, 1, m, Yd, 1, m, m, k);
   SKEMA_LAUNCHED(c);
@@ -621,7 +634,6 @@ void spd_low_rank_approx(skema_ctx* c, double* Uout, double* Sout) {
     spd_eig_kernel<<<1, 256, 0, c->stream>>>(Sv, Sout, r, ref_steps ? nu : eta);
     SKEMA_LAUNCHED(c);
   }
-  // the DevBufs are released at return: wait for the work that reads them
   SKEMA_CUDA(cudaStreamSynchronize(c->stream));
 }
 
@@ -634,19 +646,17 @@ void dgemm_f32_f64(skema_ctx* c, int64_t M, int64_t N, int64_t K, double alpha, 
 void low_rank_approx(skema_ctx* c, double* Uout, double* Sout, double* Vout) {
   const int64_t m = c->m, n = c->n, k = c->k, s = c->s, r = c->p.rank;
   y_materialize(c);
-  DevBuf bQ(sizeof(double) * (size_t)(m * k));
-  DevBuf bP(sizeof(double) * (size_t)(n * k));
-  DevBuf bW(sizeof(double) * cholqr_work_doubles(std::max(m, std::max(n, s)), k));
-  DevBuf bU1(sizeof(double) * (size_t)(s * k));
-  DevBuf bU2(sizeof(double) * (size_t)(s * k));
-  DevBuf bsmall(sizeof(double) * (size_t)(8 * k * k + s * s + k * s + 4 * k + 64));
-  DevBuf bstat(sizeof(int) * 4);
-  double* Q = bQ.d();
-  double* P = bP.d();
-  double* W = bW.d();
-  double* U1 = bU1.d();
-  double* U2 = bU2.d();
-  double* T1 = bsmall.d();
+  const size_t b_q = sizeof(double) * (size_t)(m * k), b_p = sizeof(double) * (size_t)(n * k);
+  const size_t b_w = sizeof(double) * cholqr_work_doubles(std::max(m, std::max(n, s)), k);
+  const size_t b_u = sizeof(double) * (size_t)(s * k);
+  const size_t b_small = sizeof(double) * (size_t)(8 * k * k + s * s + k * s + 4 * k + 64);
+  Carve cv(c, {b_q, b_p, b_w, b_u, b_u, b_small, 16});
+  double* Q = cv.take(b_q);
+  double* P = cv.take(b_p);
+  double* W = cv.take(b_w);
+  double* U1 = cv.take(b_u);
+  double* U2 = cv.take(b_u);
+  double* T1 = cv.take(b_small);
   double* T2 = T1 + k * k;
   double* Z1 = T2 + k * k;         // k x s
   double* Z2 = Z1 + k * s;         // k x k
@@ -656,7 +666,7 @@ void low_rank_approx(skema_ctx* c, double* Uout, double* Sout, double* Vout) {
   double* Sv = Vc + k * k;         // k
   double* sig = Sv + k;            // k
   double* Zd = sig + k;            // s x s
-  int* st = (int*)bstat.p;
+  int* st = reinterpret_cast<int*>(cv.take(16));
 
   // Q = Y (m x k, column-major, FP64); P = X^T (n x k, column-major)
   f2d_kernel<<<g1(c, m * k), 256, 0, c->stream>>>(c->Y, 1, m, Q, 1, m, m, k);
