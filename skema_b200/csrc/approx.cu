@@ -281,6 +281,35 @@ __global__ void colsparse_apply_kernel(const uint32_t* __restrict__ mp, int zeta
   }
 }
 
+// The same product with a private copy of out per CTA in shared memory: the
+// CTA's stored rows add into it with shared-memory atomics (few collisions:
+// out has R x k entries), then each entry goes to out with one global atomic
+// per CTA. Used when out fits in shared memory; the kernel above turns every
+// map entry into a global atomic on out's few entries.
+__global__ void colsparse_apply_smem_kernel(const uint32_t* __restrict__ mp, int zeta, int64_t n,
+                                            const double* __restrict__ P, int64_t ldp, int64_t k,
+                                            double* __restrict__ out, int64_t ldo, int64_t R) {
+  extern __shared__ double priv[];  // R x k, column-major (ld R)
+  for (int64_t q = threadIdx.x; q < R * k; q += blockDim.x) priv[q] = 0.0;
+  __syncthreads();
+  const int64_t per = (n + gridDim.x - 1) / gridDim.x;
+  const int64_t j0 = (int64_t)blockIdx.x * per, j1 = min(n, j0 + per);
+  const int64_t span = j1 > j0 ? j1 - j0 : 0;
+  for (int64_t q = threadIdx.x; q < span * k; q += blockDim.x) {
+    const int64_t j = j0 + q % span, col = q / span;  // consecutive threads: consecutive rows j
+    const double v = P[j + col * ldp];
+    for (int t = 0; t < zeta; ++t) {
+      const uint32_t w = mp[j * zeta + t];
+      atomicAdd(priv + (int64_t)(w & 0x7fffffffu) + col * R, (w >> 31) ? -v : v);
+    }
+  }
+  __syncthreads();
+  for (int64_t q = threadIdx.x; q < R * k; q += blockDim.x) {
+    const double a = priv[q];
+    if (a != 0.0) atomicAdd(out + (q % R) + (q / R) * ldo, a);
+  }
+}
+
 // ------------------------------------------------------ Jacobi SVD ---------
 // One-sided Jacobi on the column-major k x k A (overwritten by A V = U S),
 // V accumulated (column-major k x k). One CTA; each warp rotates pairs.
@@ -403,9 +432,11 @@ int g1(const skema_ctx* c, int64_t total) {
 
 // In-place CholeskyQR2 (+ shifted pre-pass if needed) of the column-major
 // rows x k matrix Qm (ld = rows). On return Rout (k x k, upper, column-major)
-// holds R with Q_in = Q_out R.
-void cholqr(skema_ctx* c, double* Qm, int64_t rows, int64_t k, double* Rout, double* work,
-            int* dstatus) {
+// holds R with Q_in = Q_out R. False when a Cholesky failed even after the
+// shifted pass (the columns are numerically dependent); Qm then holds the
+// input times an invertible upper-triangular matrix (the same column space).
+bool cholqr_try(skema_ctx* c, double* Qm, int64_t rows, int64_t k, double* Rout, double* work,
+                int* dstatus) {
   double* G = work;            // k x k
   double* R = work + k * k;    // k x k
   double* Racc = work + 2 * k * k;
@@ -426,7 +457,12 @@ void cholqr(skema_ctx* c, double* Qm, int64_t rows, int64_t k, double* Rout, dou
     SKEMA_CUDA(cudaMemcpyAsync(&st, dstatus, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     SKEMA_CUDA(cudaStreamSynchronize(c->stream));
     if (st != 0) {
-      if (shifted) fail(SKEMA_ENOTPD, "Cholesky of the Gram matrix failed after the shifted pass");
+      if (shifted) {
+        if (cur != Qm)
+          SKEMA_CUDA(cudaMemcpyAsync(Qm, cur, sizeof(double) * (size_t)(rows * k), cudaMemcpyDeviceToDevice,
+                                     c->stream));
+        return false;
+      }
       // shifted CholeskyQR: G + s I with s = 11 (rows*k + k(k+1)) u ||Q||_F^2
       dgemm<double, double>(c, k, k, rows, 1.0, cur, rows, 1, cur, 1, rows, 0.0, G, 1, k);
       trace_kernel<<<1, 256, 0, c->stream>>>(G, k, fro2);
@@ -439,7 +475,12 @@ void cholqr(skema_ctx* c, double* Qm, int64_t rows, int64_t k, double* Rout, dou
       SKEMA_LAUNCHED(c);
       SKEMA_CUDA(cudaMemcpyAsync(&st, dstatus, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
       SKEMA_CUDA(cudaStreamSynchronize(c->stream));
-      if (st != 0) fail(SKEMA_ENOTPD, "shifted Cholesky of the Gram matrix failed");
+      if (st != 0) {
+        if (cur != Qm)
+          SKEMA_CUDA(cudaMemcpyAsync(Qm, cur, sizeof(double) * (size_t)(rows * k), cudaMemcpyDeviceToDevice,
+                                     c->stream));
+        return false;
+      }
       shifted = true;
       passes_left = 3;  // shifted pass + CholeskyQR2
     }
@@ -466,9 +507,85 @@ void cholqr(skema_ctx* c, double* Qm, int64_t rows, int64_t k, double* Rout, dou
     SKEMA_CUDA(cudaMemcpyAsync(Qm, cur, sizeof(double) * (size_t)(rows * k), cudaMemcpyDeviceToDevice, c->stream));
   SKEMA_CUDA(cudaMemcpyAsync(Rout, Racc, sizeof(double) * (size_t)(k * k), cudaMemcpyDeviceToDevice,
                              c->stream));
+  return true;
 }
 
-size_t cholqr_work_doubles(int64_t rows, int64_t k) { return (size_t)(3 * k * k + 8 + rows * k); }
+void cholqr(skema_ctx* c, double* Qm, int64_t rows, int64_t k, double* Rout, double* work, int* dstatus) {
+  if (!cholqr_try(c, Qm, rows, k, Rout, work, dstatus))
+    fail(SKEMA_ENOTPD, "Cholesky of the Gram matrix failed after the shifted pass");
+}
+
+// 3 k^2 + 8 for cholqr's small matrices, rows x k for its second buffer,
+// 3 k^2 + 8 more for orth's eigen-decomposition.
+size_t cholqr_work_doubles(int64_t rows, int64_t k) { return (size_t)(6 * k * k + 16 + rows * k); }
+
+// Uniform values on [-1, 1) from SplitMix64 (Steele, Lea and Flood, OOPSLA
+// 2014) of (seed + index): the completion directions of orth.
+__global__ void fill_uniform_kernel(double* __restrict__ W, int64_t cnt, uint64_t seed) {
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < cnt; q += (int64_t)gridDim.x * blockDim.x) {
+    uint64_t z = seed + 0x9e3779b97f4a7c15ull * (uint64_t)(q + 1);
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    z ^= z >> 31;
+    W[q] = (double)(z >> 11) * (2.0 / 9007199254740992.0) - 1.0;
+  }
+}
+
+// An orthonormal basis Q (rows x k, in place) whose first columns span the
+// column space of the input, as dgeqrf + dorgqr give (src/Skema_SketchySVD.cpp:
+// 355-357, 381-383) also for inputs of rank below k. CholeskyQR2 first; when
+// the columns are numerically dependent, the eigen-decomposition of the
+// Gram matrix gives the independent directions (eigenvalues above 1e-12 of
+// the largest), which are orthonormalised, and the remaining columns are
+// completed with pseudo-random directions orthogonalised against them twice
+// (block Gram-Schmidt) and then among themselves. Householder QR completes
+// the basis with other orthonormal columns of the same complement; the
+// fixed-rank approximation does not depend on that choice beyond the rank
+// of the sketch.
+void orth(skema_ctx* c, double* Qm, int64_t rows, int64_t k, double* Rscratch, double* work, int* dstatus) {
+  if (cholqr_try(c, Qm, rows, k, Rscratch, work, dstatus)) return;
+  double* T = work + 3 * k * k + 8;              // rows x k
+  double* G = T + rows * k;                      // k x k
+  double* V = G + k * k;                         // k x k
+  double* Vs = V + k * k;                        // k x k (sorted)
+  double* Sv = Vs + k * k;                       // k
+  double* sig = Sv + k;                          // k
+  dgemm<double, double>(c, k, k, rows, 1.0, Qm, rows, 1, Qm, 1, rows, 0.0, G, 1, k);
+  jacobi_svd_kernel<<<1, 1024, 0, c->stream>>>(G, V, k, 60, 1e-15, dstatus + 1);
+  SKEMA_LAUNCHED(c);
+  // G V = U diag(lambda) with U = V for the symmetric positive semidefinite G
+  svd_finish_kernel<<<1, 256, 0, c->stream>>>(G, V, k, Rscratch /*U, unused*/, Vs, Sv, sig);
+  SKEMA_LAUNCHED(c);
+  std::vector<double> lam(k), vs((size_t)(k * k));
+  SKEMA_CUDA(cudaMemcpyAsync(lam.data(), Sv, sizeof(double) * (size_t)k, cudaMemcpyDeviceToHost, c->stream));
+  SKEMA_CUDA(cudaMemcpyAsync(vs.data(), Vs, sizeof(double) * (size_t)(k * k), cudaMemcpyDeviceToHost, c->stream));
+  SKEMA_CUDA(cudaStreamSynchronize(c->stream));
+  int64_t r = 0;
+  while (r < k && lam[r] > 1e-12 * lam[0]) ++r;
+  if (r == 0) fail(SKEMA_ENOTPD, "the sketch is zero: no direction to orthonormalise");
+  // B = V_r diag(lambda_r^-1/2): Q V_r B has orthonormal columns up to rounding
+  for (int64_t j = 0; j < r; ++j) {
+    const double sc = 1.0 / std::sqrt(lam[j]);
+    for (int64_t i = 0; i < k; ++i) vs[i + j * k] *= sc;
+  }
+  SKEMA_CUDA(cudaMemcpyAsync(G, vs.data(), sizeof(double) * (size_t)(k * r), cudaMemcpyHostToDevice, c->stream));
+  dgemm<double, double>(c, rows, r, k, 1.0, Qm, 1, rows, G, 1, k, 0.0, T, 1, rows, false);
+  SKEMA_CUDA(cudaMemcpyAsync(Qm, T, sizeof(double) * (size_t)(rows * r), cudaMemcpyDeviceToDevice, c->stream));
+  // stream order keeps the host vectors' copies complete before they go out of scope
+  SKEMA_CUDA(cudaStreamSynchronize(c->stream));
+  cholqr(c, Qm, rows, r, Rscratch, work, dstatus);  // well conditioned now
+  if (r == k) return;
+  double* W = Qm + r * rows;  // columns r .. k-1
+  const int64_t kr = k - r;
+  fill_uniform_kernel<<<g1(c, rows * kr), 256, 0, c->stream>>>(W, rows * kr, 0x5eed5eedull + (uint64_t)k);
+  SKEMA_LAUNCHED(c);
+  for (int pass = 0; pass < 2; ++pass) {
+    // W <- W - Q2 (Q2^T W)
+    dgemm<double, double>(c, r, kr, rows, 1.0, Qm, rows, 1, W, 1, rows, 0.0, G, 1, r);
+    dgemm<double, double>(c, rows, kr, r, -1.0, Qm, 1, rows, G, 1, r, 1.0, W, 1, rows, false);
+  }
+  cholqr(c, W, rows, kr, Rscratch, work, dstatus);
+}
 
 // out (R x k, column-major ld R) = Map~ (R x cols) * Qm (cols x k, column-major ld cols)
 void apply_map(skema_ctx* c, const Map& mp, const double* Qm, int64_t cols, int64_t k, double* out) {
@@ -483,8 +600,16 @@ void apply_map(skema_ctx* c, const Map& mp, const double* Qm, int64_t cols, int6
     SKEMA_LAUNCHED(c);
   } else {
     SKEMA_CUDA(cudaMemsetAsync(out, 0, sizeof(double) * (size_t)(R * k), c->stream));
-    colsparse_apply_kernel<<<g1(c, cols * k), 256, 0, c->stream>>>(mp.packed, mp.zeta, cols, Qm,
-                                                                    cols, k, out, R);
+    const size_t priv = sizeof(double) * (size_t)(R * k);
+    if (priv <= 200 * 1024) {
+      SKEMA_CUDA(cudaFuncSetAttribute(colsparse_apply_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)priv));
+      colsparse_apply_smem_kernel<<<c->sm_count, 1024, priv, c->stream>>>(mp.packed, mp.zeta, cols, Qm, cols, k,
+                                                                            out, R, R);
+    } else {
+      colsparse_apply_kernel<<<g1(c, cols * k), 256, 0, c->stream>>>(mp.packed, mp.zeta, cols, Qm, cols, k, out,
+                                                                      R);
+    }
     SKEMA_LAUNCHED(c);
   }
 }
@@ -675,8 +800,8 @@ void low_rank_approx(skema_ctx* c, double* Uout, double* Sout, double* Vout) {
   SKEMA_LAUNCHED(c);
   f2d_kernel<<<g1(c, s * s), 256, 0, c->stream>>>(c->Z, s, 1, Zd, 1, s, s, s);
   SKEMA_LAUNCHED(c);
-  cholqr(c, P, n, k, T1, W, st);  // T1 used as scratch R here
-  cholqr(c, Q, m, k, T1, W, st);
+  orth(c, P, n, k, T1, W, st);  // T1 used as scratch R here
+  orth(c, Q, m, k, T1, W, st);
   // U1 = Phi~ Q (s x k), U2 = Psi~ P (s x k)
   apply_map(c, c->phi, Q, m, k, U1);
   apply_map(c, c->psi, P, n, k, U2);

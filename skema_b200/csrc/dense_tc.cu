@@ -397,16 +397,78 @@ __global__ void amax_a16_kernel(const __nv_bfloat16* __restrict__ A16, int64_t c
   if ((threadIdx.x & 31) == 0) atomicMax(amax, wm);
 }
 
-// Per-window scales of the FP8 form from the windows' amax bits: sa[w] is
-// the largest power of two with amax * sa <= 448 (the E4M3 range) and
-// prod[w] = 1 / (sa[w] * scale_map) undoes both scales in the [Y | T]
-// epilogue.
-__global__ void fp8_window_scales_kernel(const uint32_t* __restrict__ amax, int64_t nwin, float smap,
-                                         float* __restrict__ sa, float* __restrict__ prod) {
-  for (int64_t w = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; w < nwin; w += (int64_t)gridDim.x * blockDim.x) {
-    const float s = pow2_scale_for(__uint_as_float(amax[w]));
-    sa[w] = s;
-    prod[w] = 1.f / (s * smap);
+// Row-blocked BF16 window (64-row blocks, a 128-byte line of 64 rows per
+// column) -> E4M3(scale_A a) row-major with row stride ld8 bytes, by tiles
+// of 64 rows x 128 columns through shared memory. A thread takes two 4 x 4
+// blocks (4 rows of 4 columns: four 8-byte loads), converts them and stores
+// each block row as one 32-bit word of the row-major tile; rows then leave
+// as 16-byte global stores. Within a warp the lanes cover 8 row quads x 4
+// column quads: the loads are 64-byte runs of 4 column lines, and with a
+// tile row stride of 33 words both the word stores and the row read-out
+// hit 32 distinct banks. scale_A comes from the window's amax (*amax);
+// block 0 also writes the [Y | T] product scale 1 / (scale_A scale_map)
+// into *scale_out.
+__global__ void __launch_bounds__(256)
+    a16_to_a8_kernel(const __nv_bfloat16* __restrict__ A16, int64_t rows, int64_t cols, uint8_t* __restrict__ A8,
+                     int64_t ld8, const uint32_t* amax, float* scale_out, float smap) {
+  constexpr int TC = 128, W = TC / 4 + 1;  // tile columns; shared row stride in 32-bit words
+  __shared__ uint32_t tile[64 * W];
+  const float sa = pow2_scale_for(__uint_as_float(*amax));
+  if (blockIdx.x == 0 && threadIdx.x == 0) *scale_out = 1.f / (sa * smap);
+  const int64_t nrb = (rows + 63) / 64, ncb = (cols + TC - 1) / TC;
+  for (int64_t t = blockIdx.x; t < nrb * ncb; t += gridDim.x) {
+    const int64_t rb = t / ncb, j0 = (t - rb * ncb) * TC;
+    uint2 w[2][4];
+#pragma unroll
+    for (int v = 0; v < 2; ++v) {
+      // rows 4g .. 4g+3 and columns 4cq .. 4cq+3 of the tile
+      const int b = threadIdx.x + 256 * v;
+      const int g = (b & 7) | (((b >> 5) & 1) << 3), cq = ((b >> 3) & 3) | ((b >> 6) << 2);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int64_t col = j0 + 4 * cq + j;
+        w[v][j] = make_uint2(0u, 0u);
+        if (col < cols) w[v][j] = *reinterpret_cast<const uint2*>(A16 + (rb * cols + col) * 64 + 4 * g);
+      }
+    }
+#pragma unroll
+    for (int v = 0; v < 2; ++v) {
+      const int b = threadIdx.x + 256 * v;
+      const int g = (b & 7) | (((b >> 5) & 1) << 3), cq = ((b >> 3) & 3) | ((b >> 6) << 2);
+      uint32_t row[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const __nv_bfloat162 lo = *reinterpret_cast<const __nv_bfloat162*>(&w[v][j].x);  // rows 4g, 4g+1
+        const __nv_bfloat162 hi = *reinterpret_cast<const __nv_bfloat162*>(&w[v][j].y);  // rows 4g+2, 4g+3
+        row[0] |= (uint32_t)to_e4m3(__low2float(lo) * sa) << (8 * j);
+        row[1] |= (uint32_t)to_e4m3(__high2float(lo) * sa) << (8 * j);
+        row[2] |= (uint32_t)to_e4m3(__low2float(hi) * sa) << (8 * j);
+        row[3] |= (uint32_t)to_e4m3(__high2float(hi) * sa) << (8 * j);
+      }
+#pragma unroll
+      for (int e = 0; e < 4; ++e) tile[(4 * g + e) * W + cq] = row[e];
+    }
+    __syncthreads();
+    // row r of the tile: TC bytes as TC / 16 pieces of 16 bytes
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      const int q = threadIdx.x + 256 * u, r = q >> 3, pc = q & 7;
+      const int64_t i = rb * 64 + r, j = j0 + 16 * pc;
+      if (i < rows && j < cols) {
+        const uint32_t* src = tile + r * W + 4 * pc;
+        const uint4 v = make_uint4(src[0], src[1], src[2], src[3]);
+        uint8_t* dst = A8 + i * ld8 + j;
+        if (j + 16 <= cols) {
+          *reinterpret_cast<uint4*>(dst) = v;
+        } else {
+          const uint32_t vw[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+          for (int e = 0; e < 16; ++e)
+            if (j + e < cols) dst[e] = (uint8_t)(vw[e >> 2] >> (8 * (e & 3)));
+        }
+      }
+    }
+    __syncthreads();
   }
 }
 
@@ -421,20 +483,17 @@ Plan plan_fp8(Plan pl, int64_t K) {
   return pl;
 }
 
-
-// The FP8 [Y | T] product from A16: E4M3 A made in shared memory (sa: the
-// windows' scales, wlen rows each).
-void launch_gemm_a16f8(skema_ctx* c, const CUtensorMap& ta16, const CUtensorMap& tb, int64_t M, int64_t N,
-                       int64_t K, Plan pl, const tc::OutSpec& o, const float* sa, int64_t wlen) {
-  constexpr int S1 = 2, S2 = 3;
+void launch_gemm_fp8(skema_ctx* c, const CUtensorMap& ta, const CUtensorMap& tb, int64_t M, int64_t N, int64_t K,
+                     Plan pl, const tc::OutSpec& o) {
+  constexpr int S = 5;
   constexpr uint32_t STAGE = ((tc::BM * 128 + kNT * 128 + 1023) / 1024) * 1024;
-  const size_t smem = (size_t)S1 * tc::BM * 128 * 2 + (size_t)S2 * STAGE + 1024 + 256;
-  auto kern = tc::gemm_a16f8_kernel<kNT, S1, S2>;
+  const size_t smem = (size_t)S * STAGE + 1024 + 256;
+  auto kern = tc::gemm_fp8_kernel<kNT, S>;
   SKEMA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int grid = 0;
   const tc::Grid3 g = grid_of(c, M, N, K, kNT, 128, pl, 0, &grid);
   if (grid <= 0) return;
-  kern<<<grid, tc::kThreadsA16F8, smem, c->stream>>>(ta16, tb, g, o, sa, wlen, c->dev_err);
+  kern<<<grid, tc::kThreads, smem, c->stream>>>(ta, tb, g, o, c->dev_err);
   SKEMA_LAUNCHED(c);
   c->dev_err_armed = true;
 }
@@ -520,7 +579,7 @@ void tc_prepare_maps(skema_ctx* c) {
     const int64_t n8 = (c->n + 15) / 16 * 16;
     if (!c->op8) {
       SKEMA_CUDA(cudaMalloc(&c->op8, (size_t)((c->k + c->s) * n8)));
-      SKEMA_CUDA(cudaMalloc(&c->fp8_win, 3 * sizeof(uint32_t)));
+      SKEMA_CUDA(cudaMalloc(&c->fp8_win, 2 * sizeof(uint32_t)));
     }
     c->ld_op8 = n8;
     SKEMA_CUDA(cudaMemsetAsync(c->op8, 0, (size_t)((c->k + c->s) * n8), c->stream));
@@ -568,6 +627,7 @@ size_t tc_scratch_bytes(const skema_ctx* c, int64_t wr) {
   b += sizeof(__nv_bfloat16) * (size_t)(wp * c->s) + 256;               // T16
   b += sizeof(float) * (size_t)(wp * c->s) + 256;                       // T32 (split-K)
   b += tc_slice_bytes(c, wr);                                           // map slices (unaligned R0)
+  if (c->p.precision == SKEMA_PREC_FP8) b += (size_t)(wr * ((c->n + 15) / 16 * 16)) + 256;  // A8
   return b;
 }
 
@@ -622,10 +682,13 @@ TcSlices xt_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr, __nv_bfloat16* 
   return sl;
 }
 
-// The FP8 scales of nwin windows from their amax (see fp8_window_scales_kernel).
-void fp8_scales(skema_ctx* c, const uint32_t* amax, int64_t nwin, float* sa, float* prod) {
-  fp8_window_scales_kernel<<<(int)std::max<int64_t>(1, std::min<int64_t>((nwin + 127) / 128, 64)), 128, 0,
-                             c->stream>>>(amax, nwin, c->fp8_map_scale, sa, prod);
+// A8 = e4m3(scale_A A16) row-major for rows rows, from the window's amax.
+void to_a8(skema_ctx* c, const __nv_bfloat16* A16, int64_t rows, uint8_t* A8, int64_t ld8, const uint32_t* amax,
+           float* scale_out) {
+  StageScope st(c, ST_WINDOW);
+  const int64_t tiles = ((rows + 63) / 64) * ((c->n + 127) / 128);
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(tiles, c->sm_count * 16));
+  a16_to_a8_kernel<<<grid, 256, 0, c->stream>>>(A16, rows, c->n, A8, ld8, amax, scale_out, c->fp8_map_scale);
   SKEMA_LAUNCHED(c);
 }
 
@@ -633,9 +696,10 @@ void fp8_scales(skema_ctx* c, const uint32_t* amax, int64_t nwin, float* sa, flo
 // Tdst (ld ldTd), rows weighted nu^(G-1-row/wlen); FP8 scales per wlen rows.
 struct YtSpec {
   int64_t R0, gr;
-  const __nv_bfloat16* A16;   // row-blocked BF16 copy of the rows
-  const float* scales;        // FP8: per-window product scales 1 / (sa * scale_map)
-  const float* sa;            // FP8: per-window scales of A
+  const __nv_bfloat16* A16;   // row-blocked BF16 (BF16 form)
+  const uint8_t* A8;          // row-major E4M3, ld8 (FP8 form)
+  int64_t ld8;
+  const float* scales;        // FP8: per-window product scales
   __nv_bfloat16* Tdst;
   int64_t ldTd;
   float log2w;
@@ -666,12 +730,9 @@ void yt_product(skema_ctx* c, const YtSpec& y) {
   }
   if (fp8) {
     o.scale = y.scales, o.scale_wlen = y.wlen;
-    // A16 as {64 rows, K, 64-row blocks}, one box = 64 rows x 128 columns
-    const uint64_t nrb = (uint64_t)((y.gr + 63) / 64);
-    const CUtensorMap ta = tmap_3d(CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, y.A16, 64, (uint64_t)n, nrb, 128,
-                                   (uint64_t)n * 128, 64, 128, 1, CU_TENSOR_MAP_SWIZZLE_NONE);
+    const CUtensorMap ta = tmap_u8(y.A8, (uint64_t)n, (uint64_t)y.gr, (uint64_t)y.ld8, 128, 128);
     const CUtensorMap tb = tmap_u8(c->op8, (uint64_t)n, (uint64_t)(k + s), (uint64_t)c->ld_op8, 128, kNT);
-    launch_gemm_a16f8(c, ta, tb, y.gr, k + s, n, pl, o, y.sa, y.wlen);
+    launch_gemm_fp8(c, ta, tb, y.gr, k + s, n, pl, o);
   } else {
     const CUtensorMap ta = tmap_bf16_blocked(y.A16, (uint64_t)n, (uint64_t)((y.gr + 63) / 64), 64);
     const CUtensorMap tb = tmap_bf16(c->op16, (uint64_t)n, (uint64_t)(k + s), (uint64_t)c->ld_op16 * 2, 64, kNT);
@@ -703,13 +764,14 @@ void tc_dense_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr, void* scratch
   // and the [Y | T] product runs E4M3 x E4M3 with the scales undone in its
   // epilogue. X^T and Z stay on the BF16 path.
   const bool fp8 = c->p.precision == SKEMA_PREC_FP8;
-  if (fp8) SKEMA_CUDA(cudaMemsetAsync(c->fp8_win, 0, 3 * sizeof(uint32_t), c->stream));
+  const int64_t ld8 = (n + 15) / 16 * 16;
+  uint8_t* A8 = fp8 ? reinterpret_cast<uint8_t*>(take((size_t)(wr * ld8))) : nullptr;
+  if (fp8) SKEMA_CUDA(cudaMemsetAsync(c->fp8_win, 0, 2 * sizeof(uint32_t), c->stream));
   const TcSlices sl = xt_window(c, Aw, R0, wr, A16, fp8 ? c->fp8_win : nullptr, &sp);
   float* scale = fp8 ? reinterpret_cast<float*>(c->fp8_win + 1) : nullptr;
-  float* sa = fp8 ? reinterpret_cast<float*>(c->fp8_win + 2) : nullptr;
-  if (fp8) fp8_scales(c, c->fp8_win, 1, sa, scale);
+  if (fp8) to_a8(c, A16, wr, A8, ld8, c->fp8_win, scale);
   YtSpec y{};
-  y.R0 = R0, y.gr = wr, y.A16 = A16, y.scales = scale, y.sa = sa, y.T32 = T32;
+  y.R0 = R0, y.gr = wr, y.A16 = A16, y.A8 = A8, y.ld8 = ld8, y.scales = scale, y.T32 = T32;
   y.Tdst = T16, y.ldTd = wp, y.log2w = 0.f, y.wlen = wr, y.nwin = 1;
   yt_product(c, y);
   y_rows_mark(c, R0, R0 + wr);
@@ -741,45 +803,43 @@ void tc_dense_update(skema_ctx* c, Mat A, int64_t row0, int64_t nrows) {
   const int64_t cap_a = ((int64_t)2 << 30) / (2 * n), cap_t = ((int64_t)512 << 20) / (2 * s);
   const int64_t grows = std::min(nrows, std::max<int64_t>(1, std::min(cap_a, cap_t) / W) * W);
   const int64_t gwin_max = (grows + W - 1) / W;
-  const int64_t ldT = pad8(grows);
+  const int64_t ldT = pad8(grows), ld8 = (n + 15) / 16 * 16;
   auto rup = [](size_t b) { return (b + 255) / 256 * 256; };
   const size_t b_a16 = rup(sizeof(__nv_bfloat16) * (size_t)(((grows + 63) / 64) * 64 * n));
+  const size_t b_a8 = fp8 ? rup((size_t)(grows * ld8)) : 0;
   const size_t b_t16 = rup(sizeof(__nv_bfloat16) * (size_t)(ldT * s));
   const size_t b_t32 = rup(sizeof(float) * (size_t)(ldT * s));
   const size_t b_sl = rup(tc_slice_bytes(c, grows)) + rup(tc_slice_bytes(c, W));
-  char* ws = static_cast<char*>(workspace(c, b_a16 + b_t16 + b_t32 + b_sl));
+  char* ws = static_cast<char*>(workspace(c, b_a16 + b_a8 + b_t16 + b_t32 + b_sl));
   __nv_bfloat16* A16 = reinterpret_cast<__nv_bfloat16*>(ws);
-  __nv_bfloat16* T16 = reinterpret_cast<__nv_bfloat16*>(ws + b_a16);
-  float* T32 = reinterpret_cast<float*>(ws + b_a16 + b_t16);
-  char* slice_sp = ws + b_a16 + b_t16 + b_t32;
+  uint8_t* A8 = reinterpret_cast<uint8_t*>(ws + b_a16);
+  __nv_bfloat16* T16 = reinterpret_cast<__nv_bfloat16*>(ws + b_a16 + b_a8);
+  float* T32 = reinterpret_cast<float*>(ws + b_a16 + b_a8 + b_t16);
+  char* slice_sp = ws + b_a16 + b_a8 + b_t16 + b_t32;
   uint32_t* amax = nullptr;
   float* scales = nullptr;
-  float* sa = nullptr;
   if (fp8) {
     if (c->fp8_win_cap < gwin_max) {
       if (c->fp8_win) cudaFree(c->fp8_win);
-      c->fp8_win = nullptr;
-      c->fp8_win_cap = 0;
-      SKEMA_CUDA(cudaMalloc(&c->fp8_win, sizeof(uint32_t) * (size_t)(3 * gwin_max)));
+      SKEMA_CUDA(cudaMalloc(&c->fp8_win, sizeof(uint32_t) * (size_t)(2 * gwin_max)));
       c->fp8_win_cap = gwin_max;
     }
     amax = c->fp8_win;
     scales = reinterpret_cast<float*>(c->fp8_win + gwin_max);
-    sa = reinterpret_cast<float*>(c->fp8_win + 2 * gwin_max);
   }
   const float log2nu = nu == 1.f ? 0.f : std::log2(nu);
   for (int64_t g0 = 0; g0 < nrows; g0 += grows) {
     const int64_t gr = std::min(grows, nrows - g0), G = (gr + W - 1) / W, R0 = row0 + g0;
-    if (fp8) SKEMA_CUDA(cudaMemsetAsync(amax, 0, sizeof(uint32_t) * (size_t)gwin_max, c->stream));
+    if (fp8) SKEMA_CUDA(cudaMemsetAsync(amax, 0, sizeof(uint32_t) * (size_t)(2 * gwin_max), c->stream));
     for (int64_t w = 0; w < G; ++w) {
       const int64_t r = g0 + w * W, wr = std::min(W, nrows - r);
       __nv_bfloat16* A16w = A16 + (w * W / 64) * 64 * n;
       char* sp = slice_sp + rup(tc_slice_bytes(c, grows));
       xt_window(c, Mat{A.p + r * A.rs, A.rs, A.cs}, row0 + r, wr, A16w, fp8 ? amax + w : nullptr, &sp);
+      if (fp8) to_a8(c, A16w, wr, A8 + w * W * ld8, ld8, amax + w, scales + w);
     }
-    if (fp8) fp8_scales(c, amax, G, sa, scales);
     YtSpec y{};
-    y.R0 = R0, y.gr = gr, y.A16 = A16, y.scales = scales, y.sa = sa, y.T32 = T32;
+    y.R0 = R0, y.gr = gr, y.A16 = A16, y.A8 = A8, y.ld8 = ld8, y.scales = scales, y.T32 = T32;
     y.Tdst = T16, y.ldTd = ldT, y.log2w = log2nu, y.wlen = W, y.nwin = G;
     yt_product(c, y);
     y_rows_mark(c, R0, R0 + gr);

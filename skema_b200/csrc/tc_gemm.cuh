@@ -29,7 +29,6 @@
 #pragma once
 #include <cuda.h>
 #include <cuda_bf16.h>
-#include <cuda_fp8.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -534,6 +533,126 @@ __global__ void __launch_bounds__(kThreads, 1)
 }
 
 // ---------------------------------------------------------------------------
+// The FP8 form of the same GEMM: E4M3 x E4M3 -> FP32 (tcgen05 kind::f8f6f4),
+// both operands K-major from 2-D maps, 128 K-elements (one 128-byte swizzle
+// row of bytes) per stage and four MMAs of K = 32 per stage. The operand
+// scales are folded into the epilogue through OutSpec::scale.
+template <int NT, int S>
+__global__ void __launch_bounds__(kThreads, 1)
+    gemm_fp8_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, Grid3 g,
+                    OutSpec o, int* err) {
+  constexpr int BK8 = 128;
+  constexpr uint32_t A_BYTES = BM * BK8;  // 16 KB
+  constexpr uint32_t B_BYTES = NT * BK8;
+  constexpr uint32_t STAGE = ((A_BYTES + B_BYTES + 1023) / 1024) * 1024;
+  constexpr uint32_t TCOLS = NT <= 32 ? 32 : NT <= 64 ? 64 : NT <= 128 ? 128 : 256;
+  static_assert(NT % 16 == 0 && NT <= 256, "N tile");
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char* smem = reinterpret_cast<unsigned char*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + S * STAGE);
+  uint64_t* empty = full + S;
+  uint64_t* tfull = empty + S;
+  uint64_t* tempty = tfull + 2;
+  uint32_t* tbase = reinterpret_cast<uint32_t*>(tempty + 2);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < S; ++s) {
+      mbar_init(full + s, 1);
+      mbar_init(empty + s, 1);
+    }
+    for (int a = 0; a < 2; ++a) {
+      mbar_init(tfull + a, 1);
+      mbar_init(tempty + a, 4 * 32);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 5) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tbase)),
+                 "r"(2 * TCOLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tbase;
+
+  if (warp == 4 && lane == 0) {
+    uint32_t it = 0;
+    bool ok = true;
+    Sched sc;
+    sched_init(g, sc);
+    int mt, nt, kt0, kt1;
+    while (ok && next_seg(g, sc, mt, nt, kt0, kt1)) {
+      const int KT = kt1 - kt0;
+      for (int kt = 0; kt < KT; ++kt, ++it) {
+        const int s = it % S;
+        const uint32_t ph = (it / S) & 1;
+        if (!mbar_wait(empty + s, ph ^ 1, err)) {
+          ok = false;
+          break;
+        }
+        unsigned char* sa = smem + s * STAGE;
+        mbar_expect_tx(full + s, A_BYTES + B_BYTES);
+        const int kc = (kt0 + kt) * BK8;
+        tma_load_2d(&tmA, full + s, sa, kc, mt * BM);
+        tma_load_2d(&tmB, full + s, sa + A_BYTES, kc, nt * NT);
+      }
+    }
+  } else if (warp == 5 && lane == 0) {
+    constexpr uint32_t idesc = idesc_e4m3(NT);
+    uint32_t it = 0, tcount = 0;
+    bool ok = true;
+    Sched sc;
+    sched_init(g, sc);
+    int mt, nt, kt0, kt1;
+    while (ok && next_seg(g, sc, mt, nt, kt0, kt1)) {
+      const int KT = kt1 - kt0;
+      const uint32_t acc = tcount & 1, aph = (tcount >> 1) & 1;
+      if (!mbar_wait(tempty + acc, aph ^ 1, err)) break;
+      tc_fence_after();
+      const uint32_t d = tmem + acc * TCOLS;
+      for (int kt = 0; kt < KT; ++kt, ++it) {
+        const int s = it % S;
+        const uint32_t ph = (it / S) & 1;
+        if (!mbar_wait(full + s, ph, err)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t sa = smem_u32(smem + s * STAGE);
+        const uint32_t sb = sa + A_BYTES;
+#pragma unroll
+        for (int kk = 0; kk < BK8 / 32; ++kk)
+          umma_f8(d, sdesc(sa + kk * 32, 16, 1024), sdesc(sb + kk * 32, 16, 1024), idesc,
+                  (kt > 0 || kk > 0) ? 1u : 0u);
+        umma_commit(empty + s);
+      }
+      if (ok) umma_commit(tfull + acc);
+      ++tcount;
+    }
+  } else if (warp < 4) {
+    uint32_t tcount = 0;
+    Sched sc;
+    sched_init(g, sc);
+    int mt, nt, kt0, kt1;
+    for (; next_seg(g, sc, mt, nt, kt0, kt1); ++tcount) {
+      const uint32_t acc = tcount & 1, aph = (tcount >> 1) & 1;
+      if (!epilogue_unit<NT, TCOLS>(o, tmem, acc, aph, tfull, tempty, mt, nt, warp, lane, err)) break;
+    }
+  }
+  drain_on_error(err);
+  if (warp == 5) {
+    __syncwarp();
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * TCOLS) : "memory");
+  }
+}
+
+// ---------------------------------------------------------------------------
 // The same GEMM with A read as FP32 and rounded to BF16 inside the kernel,
 // for X^T = A_w^T Upsilon~_w^T straight from the FP32 window: M runs over
 // the window's columns, K over its rows. Each K step's A tile (64 window
@@ -761,206 +880,6 @@ __global__ void __launch_bounds__(kThreadsA32, 1)
       // warp meets here.
       const uint32_t wm = __reduce_max_sync(0xffffffffu, __float_as_uint(mx));
       if ((ct & 31) == 0) atomicMax(amax, wm);
-    }
-  } else if (warp < 4) {
-    // ---------------- epilogue ----------------
-    uint32_t tcount = 0;
-    Sched sc;
-    sched_init(g, sc);
-    int mt, nt, kt0, kt1;
-    for (; next_seg(g, sc, mt, nt, kt0, kt1); ++tcount) {
-      const uint32_t acc = tcount & 1, aph = (tcount >> 1) & 1;
-      if (!epilogue_unit<NT, TCOLS>(o, tmem, acc, aph, tfull, tempty, mt, nt, warp, lane, err)) break;
-    }
-  }
-  drain_on_error(err);
-  if (warp == 5) {
-    __syncwarp();
-    tc_fence_after();
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * TCOLS) : "memory");
-  }
-}
-
-// ---------------------------------------------------------------------------
-// The FP8 form's [Y | T] product with the E4M3 operand made inside the
-// kernel: A is the BF16 copy of the windows (A16, row-blocked: per 64-row
-// block each column is 64 contiguous rows), read by TMA one K step of 128
-// columns at a time, then scaled by its window's power of two, rounded to
-// E4M3 and written by converter warps as the K-major 128-byte-swizzled A
-// operand of tcgen05 kind::f8f6f4. B (the E4M3 maps) arrives by TMA as in
-// gemm_fp8_kernel. So the window goes from A16 straight to the tensor cores:
-// no E4M3 copy of A is written to or read from memory. Each element gets the
-// same scaling and rounding as a separate conversion pass would give it.
-//   sa[w]: the scale of window w (rows w * wlen .. of the product), a power
-//          of two with max |a| * sa <= 448.
-// Threads: warps 0-3 epilogue, warp 4 TMA producer, warp 5 MMA issuer,
-// warps 6-13 converters (warp 6 + j: rows 32 (j % 4) .. + 31 of the tile,
-// K half j / 4; one row per lane). Rings: S1 BF16 stages (producer ->
-// converters) and S2 FP8 stages (A from the converters, B by TMA -> MMA).
-constexpr int kThreadsA16F8 = 448;
-
-template <int NT, int S1, int S2>
-__global__ void __launch_bounds__(kThreadsA16F8, 1)
-    gemm_a16f8_kernel(const __grid_constant__ CUtensorMap tmA16, const __grid_constant__ CUtensorMap tmB, Grid3 g,
-                      OutSpec o, const float* __restrict__ sa, int64_t wlen, int* err) {
-  constexpr int BK8 = 128;                      // K per stage (bytes of E4M3 per row)
-  constexpr uint32_t A16_BYTES = BM * BK8 * 2;  // 32 KB: two boxes {64 rows, 128 K}
-  constexpr uint32_t A_BYTES = BM * BK8;        // 16 KB
-  constexpr uint32_t B_BYTES = NT * BK8;
-  constexpr uint32_t STAGE = ((A_BYTES + B_BYTES + 1023) / 1024) * 1024;
-  constexpr uint32_t TCOLS = NT <= 32 ? 32 : NT <= 64 ? 64 : NT <= 128 ? 128 : 256;
-  constexpr int NCONV = kThreadsA16F8 - 6 * 32;  // 256 converter threads
-  static_assert(NT % 16 == 0 && NT <= 256, "N tile");
-  extern __shared__ __align__(1024) unsigned char smem_raw[];
-  unsigned char* smem = reinterpret_cast<unsigned char*>(
-      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
-  unsigned char* st16 = smem;                   // S1 x A16_BYTES
-  unsigned char* st8 = smem + S1 * A16_BYTES;   // S2 x STAGE
-  uint64_t* h16full = reinterpret_cast<uint64_t*>(st8 + S2 * STAGE);
-  uint64_t* h16empty = h16full + S1;
-  uint64_t* full = h16empty + S1;
-  uint64_t* empty = full + S2;
-  uint64_t* tfull = empty + S2;
-  uint64_t* tempty = tfull + 2;
-  uint32_t* tbase = reinterpret_cast<uint32_t*>(tempty + 2);
-
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-
-  if (threadIdx.x == 0) {
-    for (int s = 0; s < S1; ++s) {
-      mbar_init(h16full + s, 1);
-      mbar_init(h16empty + s, NCONV);
-    }
-    for (int s = 0; s < S2; ++s) {
-      mbar_init(full + s, 1 + NCONV);  // producer (B bytes) + converters (A tile)
-      mbar_init(empty + s, 1);         // MMA commit
-    }
-    for (int a = 0; a < 2; ++a) {
-      mbar_init(tfull + a, 1);
-      mbar_init(tempty + a, 4 * 32);
-    }
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  }
-  if (warp == 5) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tbase)),
-                 "r"(2 * TCOLS)
-                 : "memory");
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
-  }
-  tc_fence_before();
-  __syncthreads();
-  tc_fence_after();
-  const uint32_t tmem = *tbase;
-
-  if (warp == 4 && lane == 0) {
-    // ---------------- TMA producer ----------------
-    uint32_t it = 0;
-    bool ok = true;
-    Sched sc;
-    sched_init(g, sc);
-    int mt, nt, kt0, kt1;
-    while (ok && next_seg(g, sc, mt, nt, kt0, kt1)) {
-      const int KT = kt1 - kt0;
-      for (int kt = 0; kt < KT; ++kt, ++it) {
-        const int s1 = it % S1, s2 = it % S2;
-        const uint32_t ph1 = (it / S1) & 1, ph2 = (it / S2) & 1;
-        const int kc = (kt0 + kt) * BK8;
-        if (!mbar_wait(h16empty + s1, ph1 ^ 1, err)) {
-          ok = false;
-          break;
-        }
-        unsigned char* a16 = st16 + s1 * A16_BYTES;
-        mbar_expect_tx(h16full + s1, A16_BYTES);
-        tma_load_3d(&tmA16, h16full + s1, a16, 0, kc, 2 * mt);
-        tma_load_3d(&tmA16, h16full + s1, a16 + A16_BYTES / 2, 0, kc, 2 * mt + 1);
-        if (!mbar_wait(empty + s2, ph2 ^ 1, err)) {
-          ok = false;
-          break;
-        }
-        mbar_expect_tx(full + s2, B_BYTES);
-        tma_load_2d(&tmB, full + s2, st8 + s2 * STAGE + A_BYTES, kc, nt * NT);
-      }
-    }
-  } else if (warp == 5 && lane == 0) {
-    // ---------------- MMA issuer ----------------
-    constexpr uint32_t idesc = idesc_e4m3(NT);
-    uint32_t it = 0, tcount = 0;
-    bool ok = true;
-    Sched sc;
-    sched_init(g, sc);
-    int mt, nt, kt0, kt1;
-    while (ok && next_seg(g, sc, mt, nt, kt0, kt1)) {
-      const int KT = kt1 - kt0;
-      const uint32_t acc = tcount & 1, aph = (tcount >> 1) & 1;
-      if (!mbar_wait(tempty + acc, aph ^ 1, err)) break;
-      tc_fence_after();
-      const uint32_t d = tmem + acc * TCOLS;
-      for (int kt = 0; kt < KT; ++kt, ++it) {
-        const int s2 = it % S2;
-        const uint32_t ph2 = (it / S2) & 1;
-        if (!mbar_wait(full + s2, ph2, err)) {
-          ok = false;
-          break;
-        }
-        tc_fence_after();
-        const uint32_t sa8 = smem_u32(st8 + s2 * STAGE);
-        const uint32_t sb8 = sa8 + A_BYTES;
-#pragma unroll
-        for (int kk = 0; kk < BK8 / 32; ++kk)
-          umma_f8(d, sdesc(sa8 + kk * 32, 16, 1024), sdesc(sb8 + kk * 32, 16, 1024), idesc,
-                  (kt > 0 || kk > 0) ? 1u : 0u);
-        umma_commit(empty + s2);
-      }
-      if (ok) umma_commit(tfull + acc);
-      ++tcount;
-    }
-  } else if (warp >= 6) {
-    // ---------------- converters ----------------
-    const int cw = warp - 6;
-    const int R = 32 * (cw & 3) + lane;  // tile row of this lane
-    const int kh = cw >> 2;              // K half: columns 64 kh .. 64 kh + 63 of the stage
-    const int box = R >> 6, rr = R & 63;
-    const int sw = R & 7;
-    uint32_t it = 0;
-    bool ok = true;
-    Sched sc;
-    sched_init(g, sc);
-    int mt, nt, kt0, kt1;
-    while (ok && next_seg(g, sc, mt, nt, kt0, kt1)) {
-      const int64_t row = (int64_t)mt * BM + R;
-      const float scale = row < o.rows ? sa[row / wlen] : 1.f;
-      const int KT = kt1 - kt0;
-      for (int kt = 0; kt < KT; ++kt, ++it) {
-        const int s1 = it % S1, s2 = it % S2;
-        const uint32_t ph1 = (it / S1) & 1, ph2 = (it / S2) & 1;
-        if (!mbar_wait(h16full + s1, ph1, err) || !mbar_wait(empty + s2, ph2 ^ 1, err)) {
-          ok = false;
-          break;
-        }
-        const __nv_bfloat16* src =
-            reinterpret_cast<const __nv_bfloat16*>(st16 + s1 * A16_BYTES + box * (A16_BYTES / 2)) + rr;
-        unsigned char* dst = st8 + s2 * STAGE + R * 128;
-#pragma unroll
-        for (int c = 0; c < 4; ++c) {  // 16-byte chunk 4 kh + c of the row: K = 64 kh + 16 c .. + 15
-          const int k0 = 64 * kh + 16 * c;
-          uint32_t w[4];
-#pragma unroll
-          for (int q = 0; q < 4; ++q) {
-            uint32_t b = 0;
-#pragma unroll
-            for (int e = 0; e < 4; ++e) {
-              const float x = __bfloat162float(src[(k0 + 4 * q + e) * 64]) * scale;
-              b |= (uint32_t)__nv_cvt_float_to_fp8(x, __NV_SATFINITE, __NV_E4M3) << (8 * e);
-            }
-            w[q] = b;
-          }
-          const int chunk = 4 * kh + c;
-          *reinterpret_cast<uint4*>(dst + ((chunk ^ sw) << 4)) = make_uint4(w[0], w[1], w[2], w[3]);
-        }
-        fence_proxy_async();
-        mbar_arrive(h16empty + s1);
-        mbar_arrive(full + s2);
-      }
     }
   } else if (warp < 4) {
     // ---------------- epilogue ----------------

@@ -362,6 +362,47 @@ def test_csr_update_on_caller_stream(sk, oracle):
     assert rel_fro(Xh, o.X) < TOL
 
 
+def test_csr_long_rows_and_tail(sk, oracle):
+    # rows of 900 nonzeros among rows of 0-5, two empty 32-row tiles, and a
+    # nonzero count that is not a multiple of 4
+    rng = np.random.default_rng(31)
+    m, n = 2600, 2000
+    counts = np.where(np.arange(m) % 97 == 0, 900, rng.integers(0, 6, size=m))
+    counts[64:128] = 0  # two empty 32-row tiles
+    rows = np.repeat(np.arange(m), counts)
+    cols = np.concatenate([rng.choice(n, size=c, replace=False) for c in counts])
+    A = sp.csr_matrix((rng.normal(size=rows.size), (rows, cols)), shape=(m, n))
+    A.data = A.data.astype(np.float32).astype(np.float64)
+    if A.nnz % 4 == 0:
+        A = A[:-1]
+        m -= 1
+    assert A.nnz % 4 != 0
+    a = alg(sk, m, n, 20, 700, 1, issparse=True)
+    o = oracle_for(oracle, a)
+    o.linear_update(A)
+    with sk.SketchySVD(a) as s:
+        s.linear_update(A)
+        check_sketches(s, o)
+
+
+def test_csr_unaligned_device_arrays(sk, oracle):
+    # col / val device arrays that do not start on 16 bytes
+    import torch
+
+    m, n = 4000, 1300
+    A = csr_input(m, n, nnz_row=11, seed=23, empty_every=13)
+    a = alg(sk, m, n, 20, 900, 1, issparse=True, sketch_nu=0.75)
+    o = oracle_for(oracle, a)
+    o.linear_update(A)
+    rp = torch.from_numpy(A.indptr.astype(np.int64)).cuda()
+    cl = torch.from_numpy(np.concatenate([[0], A.indices]).astype(np.int32)).cuda()[1:]
+    vl = torch.from_numpy(np.concatenate([[0.0], A.data]).astype(np.float32)).cuda()[1:]
+    assert cl.data_ptr() % 16 != 0 and vl.data_ptr() % 16 != 0
+    with sk.SketchySVD(a) as s:
+        s.linear_update((rp, cl, vl))
+        check_sketches(s, o)
+
+
 def test_csr_imported_map_unsorted_duplicate_bins(sk):
     # The zeta = 8, k <= 128 kernel takes the map in a 16-bit offset form
     # sorted by bin with repeated bins flagged; an imported map may list its
