@@ -377,6 +377,12 @@ int skema_set_wait_limit(skema_ctx* ctx, int64_t ns);
  * reference counterpart. */
 int skema_set_workspace_limit(skema_ctx* ctx, int64_t bytes);
 
+/* The CUDA stream ctx launches on (cudaStream_t as void*): its own stream,
+ * or the one given to skema_set_stream. A caller that hands the library
+ * memory managed by a stream-ordered allocator records its use on this
+ * stream. */
+int skema_get_stream(const skema_ctx* ctx, void** stream);
+
 /* Number of this library's kernels launched on ctx so far (for accounting). */
 int64_t skema_launch_count(const skema_ctx* ctx);
 

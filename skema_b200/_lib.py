@@ -120,6 +120,7 @@ SIGNATURES = {
     "skema_rbf_sketch_fwd_noalloc": (C.c_int, [_P, _P, _I64, _I64, _D, _P, _I64, _P]),
     "skema_synchronize": (C.c_int, [_P]),
     "skema_set_stream": (C.c_int, [_P, _P]),
+    "skema_get_stream": (C.c_int, [_P, C.POINTER(_P)]),
     "skema_set_wait_limit": (C.c_int, [_P, _I64]),
     "skema_set_workspace_limit": (C.c_int, [_P, _I64]),
     "skema_launch_count": (_I64, [_P]),

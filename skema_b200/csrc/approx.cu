@@ -145,6 +145,167 @@ void dgemm(skema_ctx* c, int64_t M, int64_t N, int64_t K, double alpha, const TA
   SKEMA_LAUNCHED(c);
 }
 
+// ----------------------------------------- tall-skinny FP64 products -------
+// G += A^T A for a tall column-major A (rows x k, ld lda) with k <= 16 TPK:
+// each CTA takes a run of rows and accumulates the whole (padded) k x k
+// product in registers (16 x 16 threads, TPK x TPK each), eight rows of A
+// at a time through shared memory, then adds it to G (column-major k x k,
+// zeroed beforehand) with one atomic per entry. The general tile kernel
+// spends most of a 64 x 64 tile on padding at these k and splits K into
+// partial sums anyway.
+template <int TPK>
+__global__ void __launch_bounds__(256)
+    gram_kernel(const double* __restrict__ A, int64_t lda, int64_t rows, int k, double* __restrict__ G,
+                int64_t rows_per_cta) {
+  constexpr int KP = 16 * TPK;
+  __shared__ double S[8][KP + 1];
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  const int64_t r0 = (int64_t)blockIdx.x * rows_per_cta, r1 = min(rows, r0 + rows_per_cta);
+  double acc[TPK][TPK];
+#pragma unroll
+  for (int i = 0; i < TPK; ++i)
+#pragma unroll
+    for (int j = 0; j < TPK; ++j) acc[i][j] = 0.0;
+  for (int64_t c0 = r0; c0 < r1; c0 += 8) {
+    for (int q = tid; q < 8 * KP; q += 256) {
+      const int rr = q & 7, col = q >> 3;
+      const int64_t row = c0 + rr;
+      S[rr][col] = (row < r1 && col < k) ? A[row + (int64_t)col * lda] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int rr = 0; rr < 8; ++rr) {
+      double a[TPK], b[TPK];
+#pragma unroll
+      for (int i = 0; i < TPK; ++i) a[i] = S[rr][ty + 16 * i], b[i] = S[rr][tx + 16 * i];
+#pragma unroll
+      for (int i = 0; i < TPK; ++i)
+#pragma unroll
+        for (int j = 0; j < TPK; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < TPK; ++i)
+#pragma unroll
+    for (int j = 0; j < TPK; ++j) {
+      const int gi = ty + 16 * i, gj = tx + 16 * j;
+      if (gi < k && gj < k) atomicAdd(G + gi + (int64_t)gj * k, acc[i][j]);
+    }
+}
+
+// C = A B for a tall column-major A (rows x k, ld lda) and a small B (k x n2,
+// column-major ld ldb) with k, n2 <= 16 TPN: B stays in shared memory for the
+// CTA's life, A comes in blocks of 64 rows; thread (ty, tx) makes rows
+// 4 ty .. 4 ty + 3 and columns tx + 16 j of the block. C is column-major
+// (ld ldc) and written, not accumulated.
+template <int TPN>
+__global__ void __launch_bounds__(256)
+    tsm_kernel(const double* __restrict__ A, int64_t lda, int64_t rows, int k, const double* __restrict__ B,
+               int64_t ldb, int n2, double* __restrict__ C, int64_t ldc) {
+  constexpr int NP = 16 * TPN;
+  extern __shared__ double tsm_smem[];
+  double* Bs = tsm_smem;            // k x (NP + 1), row kk at kk * (NP + 1)
+  double* As = Bs + k * (NP + 1);   // k x 65, row kk at kk * 65
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  for (int q = tid; q < k * NP; q += 256) {
+    const int kk = q / NP, col = q - kk * NP;
+    Bs[kk * (NP + 1) + col] = col < n2 ? B[kk + (int64_t)col * ldb] : 0.0;
+  }
+  for (int64_t r0 = (int64_t)blockIdx.x * 64; r0 < rows; r0 += (int64_t)gridDim.x * 64) {
+    __syncthreads();
+    for (int q = tid; q < k * 64; q += 256) {
+      const int rr = q & 63, kk = q >> 6;
+      const int64_t row = r0 + rr;
+      As[kk * 65 + rr] = row < rows ? A[row + (int64_t)kk * lda] : 0.0;
+    }
+    __syncthreads();
+    double acc[4][TPN];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < TPN; ++j) acc[i][j] = 0.0;
+    for (int kk = 0; kk < k; ++kk) {
+      double a[4], b[TPN];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i] = As[kk * 65 + 4 * ty + i];
+#pragma unroll
+      for (int j = 0; j < TPN; ++j) b[j] = Bs[kk * (NP + 1) + tx + 16 * j];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < TPN; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int64_t row = r0 + 4 * ty + i;
+      if (row >= rows) continue;
+#pragma unroll
+      for (int j = 0; j < TPN; ++j) {
+        const int col = tx + 16 * j;
+        if (col < n2) C[row + (int64_t)col * ldc] = acc[i][j];
+      }
+    }
+  }
+}
+
+template <int T>
+void launch_gram(skema_ctx* c, const double* A, int64_t lda, int64_t rows, int64_t k, double* G) {
+  const int64_t ctas = std::max<int64_t>(1, std::min<int64_t>((rows + 255) / 256, 2 * (int64_t)c->sm_count));
+  const int64_t per = ((rows + ctas - 1) / ctas + 7) / 8 * 8;
+  gram_kernel<T><<<(unsigned)((rows + per - 1) / per), 256, 0, c->stream>>>(A, lda, rows, (int)k, G, per);
+  SKEMA_LAUNCHED(c);
+}
+
+template <int T>
+void launch_tsm(skema_ctx* c, const double* A, int64_t lda, int64_t rows, int64_t k, const double* B, int64_t ldb,
+                int64_t n2, double* C, int64_t ldc) {
+  const size_t smem = sizeof(double) * (size_t)(k * (16 * T + 1) + k * 65);
+  SKEMA_CUDA(cudaFuncSetAttribute(tsm_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int64_t blocks = (rows + 63) / 64;
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(blocks, 2 * (int64_t)c->sm_count));
+  tsm_kernel<T><<<grid, 256, smem, c->stream>>>(A, lda, rows, (int)k, B, ldb, (int)n2, C, ldc);
+  SKEMA_LAUNCHED(c);
+}
+
+// G (k x k, column-major) = A^T A for column-major A (rows x k, ld lda).
+void gram(skema_ctx* c, const double* A, int64_t lda, int64_t rows, int64_t k, double* G) {
+  if (k > 128) {
+    dgemm<double, double>(c, k, k, rows, 1.0, A, lda, 1, A, 1, lda, 0.0, G, 1, k);
+    return;
+  }
+  SKEMA_CUDA(cudaMemsetAsync(G, 0, sizeof(double) * (size_t)(k * k), c->stream));
+  switch ((k + 15) / 16) {
+    case 1: launch_gram<1>(c, A, lda, rows, k, G); break;
+    case 2: launch_gram<2>(c, A, lda, rows, k, G); break;
+    case 3: launch_gram<3>(c, A, lda, rows, k, G); break;
+    case 4: launch_gram<4>(c, A, lda, rows, k, G); break;
+    case 5: launch_gram<5>(c, A, lda, rows, k, G); break;
+    case 6: launch_gram<6>(c, A, lda, rows, k, G); break;
+    case 7: launch_gram<7>(c, A, lda, rows, k, G); break;
+    default: launch_gram<8>(c, A, lda, rows, k, G); break;
+  }
+}
+
+// C (rows x n2) = A (rows x k) B (k x n2), all column-major.
+void tall_times_small(skema_ctx* c, const double* A, int64_t lda, int64_t rows, int64_t k, const double* B,
+                      int64_t ldb, int64_t n2, double* C, int64_t ldc) {
+  if (k > 128 || n2 > 128) {
+    dgemm<double, double>(c, rows, n2, k, 1.0, A, 1, lda, B, 1, ldb, 0.0, C, 1, ldc, false);
+    return;
+  }
+  switch ((n2 + 15) / 16) {
+    case 1: launch_tsm<1>(c, A, lda, rows, k, B, ldb, n2, C, ldc); break;
+    case 2: launch_tsm<2>(c, A, lda, rows, k, B, ldb, n2, C, ldc); break;
+    case 3: launch_tsm<3>(c, A, lda, rows, k, B, ldb, n2, C, ldc); break;
+    case 4: launch_tsm<4>(c, A, lda, rows, k, B, ldb, n2, C, ldc); break;
+    case 5: launch_tsm<5>(c, A, lda, rows, k, B, ldb, n2, C, ldc); break;
+    case 6: launch_tsm<6>(c, A, lda, rows, k, B, ldb, n2, C, ldc); break;
+    case 7: launch_tsm<7>(c, A, lda, rows, k, B, ldb, n2, C, ldc); break;
+    default: launch_tsm<8>(c, A, lda, rows, k, B, ldb, n2, C, ldc); break;
+  }
+}
+
 // ----------------------------------------------------- conversions ----------
 __global__ void f2d_kernel(const float* __restrict__ S, int64_t srs, int64_t scs,
                            double* __restrict__ D, int64_t drs, int64_t dcs, int64_t M, int64_t N) {
@@ -313,10 +474,20 @@ __global__ void colsparse_apply_smem_kernel(const uint32_t* __restrict__ mp, int
 // ------------------------------------------------------ Jacobi SVD ---------
 // One-sided Jacobi on the column-major k x k A (overwritten by A V = U S),
 // V accumulated (column-major k x k). One CTA; each warp rotates pairs.
-__global__ void __launch_bounds__(1024) jacobi_svd_kernel(double* A, double* V, int64_t k,
-                                                          int max_sweeps, double tol,
-                                                          int* sweeps_out) {
+// SMEM: A and V are worked on in shared memory (2 k^2 doubles), copied in at
+// the start and out at the end; every rotation reads and writes two columns
+// of each, so global memory would put an L2 round trip on every step.
+template <bool SMEM>
+__global__ void __launch_bounds__(1024) jacobi_svd_kernel_t(double* Ag, double* Vg, int64_t k, int max_sweeps,
+                                                            double tol, int* sweeps_out) {
   __shared__ unsigned long long off_max;
+  extern __shared__ double jac_smem[];
+  double* A = SMEM ? jac_smem : Ag;
+  double* V = SMEM ? jac_smem + k * k : Vg;
+  if (SMEM) {
+    for (int64_t q = threadIdx.x; q < k * k; q += blockDim.x) A[q] = Ag[q];
+    __syncthreads();
+  }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
   for (int64_t q = threadIdx.x; q < k * k; q += blockDim.x) V[q] = (q % k == q / k) ? 1.0 : 0.0;
   const int64_t kp = (k + 1) & ~(int64_t)1;  // even number of players
@@ -377,6 +548,26 @@ __global__ void __launch_bounds__(1024) jacobi_svd_kernel(double* A, double* V, 
     __syncthreads();
   }
   if (threadIdx.x == 0) sweeps_out[0] = sweep;
+  if (SMEM) {
+    __syncthreads();
+    for (int64_t q = threadIdx.x; q < k * k; q += blockDim.x) {
+      Ag[q] = A[q];
+      Vg[q] = V[q];
+    }
+  }
+}
+
+// The SVD kernel for a k x k problem: shared memory when A and V fit.
+void jacobi_svd(skema_ctx* c, double* A, double* V, int64_t k, int max_sweeps, double tol, int* sweeps_out) {
+  const size_t smem = sizeof(double) * (size_t)(2 * k * k);
+  if (smem <= 200 * 1024) {
+    SKEMA_CUDA(cudaFuncSetAttribute(jacobi_svd_kernel_t<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem));
+    jacobi_svd_kernel_t<true><<<1, 1024, smem, c->stream>>>(A, V, k, max_sweeps, tol, sweeps_out);
+  } else {
+    jacobi_svd_kernel_t<false><<<1, 1024, 0, c->stream>>>(A, V, k, max_sweeps, tol, sweeps_out);
+  }
+  SKEMA_LAUNCHED(c);
 }
 
 // sigma_j = ||a_j||, ranks by descending sigma (ties by index), then
@@ -450,7 +641,7 @@ bool cholqr_try(skema_ctx* c, double* Qm, int64_t rows, int64_t k, double* Rout,
   double* nxt = work + 3 * k * k + 8;
   while (passes_left > 0) {
     // G = Q^T Q
-    dgemm<double, double>(c, k, k, rows, 1.0, cur, rows, 1, cur, 1, rows, 0.0, G, 1, k);
+    gram(c, cur, rows, rows, k, G);
     cholesky_kernel<<<1, 1024, 0, c->stream>>>(G, k, dstatus);
     SKEMA_LAUNCHED(c);
     int st = 0;
@@ -464,7 +655,7 @@ bool cholqr_try(skema_ctx* c, double* Qm, int64_t rows, int64_t k, double* Rout,
         return false;
       }
       // shifted CholeskyQR: G + s I with s = 11 (rows*k + k(k+1)) u ||Q||_F^2
-      dgemm<double, double>(c, k, k, rows, 1.0, cur, rows, 1, cur, 1, rows, 0.0, G, 1, k);
+      gram(c, cur, rows, rows, k, G);
       trace_kernel<<<1, 256, 0, c->stream>>>(G, k, fro2);
       SKEMA_LAUNCHED(c);
       const double u = 1.1102230246251565e-16;
@@ -494,7 +685,7 @@ bool cholqr_try(skema_ctx* c, double* Qm, int64_t rows, int64_t k, double* Rout,
     trsm_upper_kernel<<<(int)((k * 32 + 255) / 256), 256, 0, c->stream>>>(R, k, G, k, k);
     SKEMA_LAUNCHED(c);
     // next <- cur * Rinv  (rows x k)
-    dgemm<double, double>(c, rows, k, k, 1.0, cur, 1, rows, G, 1, k, 0.0, nxt, 1, rows, false);
+    tall_times_small(c, cur, rows, rows, k, G, k, k, nxt, rows);
     std::swap(cur, nxt);
     // Racc <- R * Racc
     double* tmp = Rout;
@@ -551,8 +742,7 @@ void orth(skema_ctx* c, double* Qm, int64_t rows, int64_t k, double* Rscratch, d
   double* Sv = Vs + k * k;                       // k
   double* sig = Sv + k;                          // k
   dgemm<double, double>(c, k, k, rows, 1.0, Qm, rows, 1, Qm, 1, rows, 0.0, G, 1, k);
-  jacobi_svd_kernel<<<1, 1024, 0, c->stream>>>(G, V, k, 60, 1e-15, dstatus + 1);
-  SKEMA_LAUNCHED(c);
+  jacobi_svd(c, G, V, k, 60, 1e-15, dstatus + 1);
   // G V = U diag(lambda) with U = V for the symmetric positive semidefinite G
   svd_finish_kernel<<<1, 256, 0, c->stream>>>(G, V, k, Rscratch /*U, unused*/, Vs, Sv, sig);
   SKEMA_LAUNCHED(c);
@@ -706,8 +896,7 @@ void spd_low_rank_approx(skema_ctx* c, double* Uout, double* Sout) {
 
   // nu = ||Y||_2 = sqrt(lambda_max(Y^T Y))
   dgemm<double, double>(c, k, k, m, 1.0, Yd, m, 1, Yd, 1, m, 0.0, G, 1, k);
-  jacobi_svd_kernel<<<1, 1024, 0, c->stream>>>(G, Vc, k, 60, 1e-15, st + 1);
-  SKEMA_LAUNCHED(c);
+  jacobi_svd(c, G, Vc, k, 60, 1e-15, st + 1);
   svd_finish_kernel<<<1, 256, 0, c->stream>>>(G, Vc, k, Uc, Vt, Sv, sig);
   SKEMA_LAUNCHED(c);
   double lmax = 0.0;
@@ -750,8 +939,7 @@ void spd_low_rank_approx(skema_ctx* c, double* Uout, double* Sout) {
   // svd(E) = Q svd(R_E)
   cholqr(c, E, m, k, RE, W, st);
   SKEMA_CUDA(cudaMemcpyAsync(Cw, RE, sizeof(double) * (size_t)(k * k), cudaMemcpyDeviceToDevice, c->stream));
-  jacobi_svd_kernel<<<1, 1024, 0, c->stream>>>(Cw, Vc, k, 60, 1e-15, st + 1);
-  SKEMA_LAUNCHED(c);
+  jacobi_svd(c, Cw, Vc, k, 60, 1e-15, st + 1);
   svd_finish_kernel<<<1, 256, 0, c->stream>>>(Cw, Vc, k, Uc, Vt, Sv, sig);
   SKEMA_LAUNCHED(c);
   if (Uout) dgemm<double, double>(c, m, r, k, 1.0, E, 1, m, Uc, 1, k, 0.0, Uout, 1, m, false);
@@ -824,14 +1012,13 @@ void low_rank_approx(skema_ctx* c, double* Uout, double* Sout, double* Vout) {
     double* Cw = W;  // k x k working copy
     dtranspose_kernel<<<g1(c, k * k), 256, 0, c->stream>>>(Z2t, Cw, k);
     SKEMA_LAUNCHED(c);
-    jacobi_svd_kernel<<<1, 1024, 0, c->stream>>>(Cw, Vc, k, 60, 1e-15, st + 1);
-    SKEMA_LAUNCHED(c);
+    jacobi_svd(c, Cw, Vc, k, 60, 1e-15, st + 1);
     svd_finish_kernel<<<1, 256, 0, c->stream>>>(Cw, Vc, k, C, Z2 /*Vout*/, Sv, sig);
     SKEMA_LAUNCHED(c);
   }
   // U = Q Uc(:, 1:r), V = P Vc(:, 1:r), S = S(1:r)
-  if (Uout) dgemm<double, double>(c, m, r, k, 1.0, Q, 1, m, C, 1, k, 0.0, Uout, 1, m, false);
-  if (Vout) dgemm<double, double>(c, n, r, k, 1.0, P, 1, n, Z2, 1, k, 0.0, Vout, 1, n, false);
+  if (Uout) tall_times_small(c, Q, m, m, k, C, k, r, Uout, m);
+  if (Vout) tall_times_small(c, P, n, n, k, Z2, k, r, Vout, n);
   if (Sout)
     SKEMA_CUDA(cudaMemcpyAsync(Sout, Sv, sizeof(double) * (size_t)r, cudaMemcpyDeviceToDevice, c->stream));
   SKEMA_CUDA(cudaStreamSynchronize(c->stream));

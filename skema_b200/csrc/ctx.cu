@@ -860,6 +860,12 @@ int skema_set_stream(skema_ctx* c, void* stream) {
   });
 }
 
+int skema_get_stream(const skema_ctx* c, void** stream) {
+  if (!c || !stream) return SKEMA_EINVAL;
+  *stream = (void*)c->stream;
+  return SKEMA_OK;
+}
+
 int skema_set_wait_limit(skema_ctx* c, int64_t ns) {
   return guarded(c, [&] {
     SKEMA_CUDA(cudaStreamSynchronize(c->stream));

@@ -497,34 +497,50 @@ class _Context:
     def set_stream(self, stream_handle: int | None):
         """Launch on an external cudaStream_t (e.g. torch's current stream)."""
         self._check(self.lib.skema_set_stream(self.h, stream_handle))
-        self._stream_handle = stream_handle
 
     # -- ordering against torch's stream ----------------------------------
-    # The library launches on the context's stream. Unless that is torch's
-    # current stream (set_stream), device tensors written by torch must be
-    # complete before a call reads them, and device tensors the library
-    # writes must be complete before torch reads them.
-    def _on_torch_stream(self, t) -> bool:
+    # The library launches on the context's stream (skema_get_stream). Unless
+    # that is torch's current stream, a call that reads device tensors first
+    # waits on the device for torch's current stream (the tensors' data are
+    # complete), and the tensors are recorded on the library's stream, so
+    # that torch's caching allocator reuses their memory only after the
+    # library's work on them is done. A call that writes device tensors makes
+    # torch's current stream wait for the library's.
+    def _lib_stream(self, device):
         import torch
 
-        h = getattr(self, "_stream_handle", None)
-        return h is not None and h == torch.cuda.current_stream(t.device).cuda_stream
+        h = C.c_void_p()
+        self._check(self.lib.skema_get_stream(self.h, C.byref(h)))
+        return torch.cuda.ExternalStream(h.value or 0, device=device)
+
+    def _cuda_tensors(self, tensors):
+        return [t for t in tensors if _is_torch(t) and t.is_cuda]
 
     def _torch_inputs_ready(self, *tensors):
-        for t in tensors:
-            if _is_torch(t) and t.is_cuda:
-                if not self._on_torch_stream(t):
-                    import torch
+        import torch
 
-                    torch.cuda.current_stream(t.device).synchronize()
-                return
+        ts = self._cuda_tensors(tensors)
+        if not ts:
+            return
+        lib_s, cur = self._lib_stream(ts[0].device), torch.cuda.current_stream(ts[0].device)
+        if lib_s.cuda_stream == cur.cuda_stream:
+            return
+        lib_s.wait_stream(cur)
+        for t in ts:
+            t.record_stream(lib_s)
 
     def _torch_outputs_ready(self, *tensors):
-        for t in tensors:
-            if _is_torch(t) and t.is_cuda:
-                if not self._on_torch_stream(t):
-                    self.synchronize()
-                return
+        import torch
+
+        ts = self._cuda_tensors(tensors)
+        if not ts:
+            return
+        lib_s, cur = self._lib_stream(ts[0].device), torch.cuda.current_stream(ts[0].device)
+        if lib_s.cuda_stream == cur.cuda_stream:
+            return
+        cur.wait_stream(lib_s)
+        for t in ts:
+            t.record_stream(lib_s)
 
     # -- sketches ---------------------------------------------------------
     def _sketch_shape(self, which):
@@ -536,6 +552,7 @@ class _Context:
         if out is None:
             out = np.empty(shape, dtype=np.float32)
         if _is_torch(out):
+            self._torch_inputs_ready(out)
             self._check(self.lib.skema_get_sketch(self.h, which, out.data_ptr(), shape[1], L.ROW_MAJOR, L.MEM_DEVICE))
             self._torch_outputs_ready(out)
         else:
@@ -595,8 +612,9 @@ class SketchySVD(_Context):
         r = self.rank
         if device_out is not None:
             U, S, V = device_out
+            self._torch_inputs_ready(U, S, V)
             self._check(self.lib.skema_low_rank_approx(self.h, U.data_ptr(), S.data_ptr(), V.data_ptr(), L.MEM_DEVICE))
-            self._torch_outputs_ready(U)
+            self._torch_outputs_ready(U, S, V)
             return U, S, V
         U = np.empty((r, self.nrow), dtype=np.float64)
         V = np.empty((r, self.ncol), dtype=np.float64)
@@ -620,8 +638,9 @@ class SketchySPD(_Context):
         r = self.rank
         if device_out is not None:
             U, S = device_out
+            self._torch_inputs_ready(U, S)
             self._check(self.lib.skema_low_rank_approx(self.h, U.data_ptr(), S.data_ptr(), None, L.MEM_DEVICE))
-            self._torch_outputs_ready(U)
+            self._torch_outputs_ready(U, S)
             return U, S
         U = np.empty((r, self.nrow), dtype=np.float64)
         S = np.empty(r, dtype=np.float64)
