@@ -13,6 +13,21 @@ rbf-bf16 / rbf-fp32 (Gauss-RBF kernel of 100,000 points in 128 dimensions,
 r = 64, k = 257, s = 515, windows of 4,096 rows; one step sketches all
 100,000 kernel rows, the kernel's rows split over the ranks).
 
+Parity (outside every timed region): the headline line carries `parity`,
+the device's X, Y, Z of one step against the FP64 oracle over every row of
+the same CSR matrix and maps (the CPU-baseline leg runs that oracle), and
+every dense / kernel line carries `accuracy`, its top-r singular values
+against FP64 SketchySVD on the same input and the context's own maps (FP64
+device products, the oracle's approximation), or for the adjoint pair the
+FP64 gradient and central finite differences of the FP64 forward.
+
+On one GPU the default run also measures the other configurations after
+the headline and reports them under `secondary`: the dense Gaussian case in
+the plain FP32 form and the BF16 / FP8 forms, the RBF kernel case in FP32
+and BF16, and the forward / adjoint pair in FP32 and BF16, each with its
+roofline and accuracy, and the speed-ups of the precision forms over the
+plain form (--no-secondary skips them).
+
 Multi-GPU (torchrun, one rank per GPU): weak scaling by contiguous row
 blocks; each rank sketches its own block of the global matrix and the
 partial X and Z sketches are summed with an NCCL all-reduce (Y rows are

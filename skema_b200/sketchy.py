@@ -495,8 +495,11 @@ class _Context:
         return ms.value, n.value
 
     def set_stream(self, stream_handle: int | None):
-        """Launch on an external cudaStream_t (e.g. torch's current stream)."""
+        """Launch on an external cudaStream_t (e.g. torch's current stream).
+        The stream must outlive every tensor this context has read or
+        written while it was set; None returns to the context's default."""
         self._check(self.lib.skema_set_stream(self.h, stream_handle))
+        self._user_stream = stream_handle or None
 
     # -- ordering against torch's stream ----------------------------------
     # The library launches on the context's stream (skema_get_stream). Unless
@@ -506,9 +509,22 @@ class _Context:
     # that torch's caching allocator reuses their memory only after the
     # library's work on them is done. A call that writes device tensors makes
     # torch's current stream wait for the library's.
+    #
+    # torch's allocator records an event on every recorded stream when such
+    # a tensor is freed, which may be after this context is destroyed. The
+    # stream the context creates for itself dies with it, so before the
+    # first call on torch tensors the context is moved onto a stream from
+    # torch's pool, which lives as long as the process.
     def _lib_stream(self, device):
         import torch
 
+        if getattr(self, "_user_stream", None) is None:
+            ts = getattr(self, "_torch_stream", None)
+            if ts is None or ts.device != device:
+                ts = torch.cuda.Stream(device=device)
+                self._check(self.lib.skema_set_stream(self.h, ts.cuda_stream))
+                self._torch_stream = ts
+            return ts
         h = C.c_void_p()
         self._check(self.lib.skema_get_stream(self.h, C.byref(h)))
         return torch.cuda.ExternalStream(h.value or 0, device=device)
