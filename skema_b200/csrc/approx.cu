@@ -373,6 +373,156 @@ __global__ void trsm_upper_kernel(const double* __restrict__ R, int64_t k, doubl
   }
 }
 
+// Packed triangles in shared memory. Upper: column j holds rows 0..j from
+// j (j + 1) / 2. Lower: column j holds rows j..k-1 from j k - j (j - 1) / 2.
+__device__ __forceinline__ int up_off(int j) { return j * (j + 1) / 2; }
+__device__ __forceinline__ int lo_off(int j, int k) { return j * k - j * (j - 1) / 2; }
+
+// Largest k for which one packed triangle plus k doubles fits the 200 KB
+// that the single-CTA kernels below use.
+constexpr int kPackedMaxK = 225;
+size_t packed_smem_bytes(int64_t k) { return sizeof(double) * (size_t)(k * (k + 1) / 2 + k); }
+
+// Value v of the register array b (v known only at run time) without a
+// local-memory copy: a chain of selects the compiler keeps in registers.
+template <int VMAX>
+__device__ __forceinline__ double pick(const double (&b)[VMAX], int v) {
+  double r = 0.0;
+#pragma unroll
+  for (int q = 0; q < VMAX; ++q)
+    if (q == v) r = b[q];
+  return r;
+}
+
+// Solve R X = B in place, R upper triangular (column-major k x k, k <=
+// min(32 VMAX, kPackedMaxK)) and B k x nrhs (column stride ldb). R is held
+// packed in shared memory with the reciprocals of its diagonal; one warp
+// per right-hand side keeps its column in registers (entry i in lane i % 32,
+// slot i / 32) and eliminates column by column: x_i = b_i / R(i, i), then
+// b_l -= R(l, i) x_i for l < i.
+template <int VMAX>
+__global__ void __launch_bounds__(256) trsm_upper_packed_kernel(const double* __restrict__ R, int k, double* B,
+                                                                int64_t ldb, int nrhs) {
+  extern __shared__ double tp_smem[];
+  double* Rp = tp_smem;
+  double* inv = Rp + k * (k + 1) / 2;
+  for (int q = threadIdx.x; q < k * k; q += blockDim.x) {
+    const int i = q % k, j = q / k;
+    if (i <= j) Rp[up_off(j) + i] = R[q];
+  }
+  for (int i = threadIdx.x; i < k; i += blockDim.x) inv[i] = 1.0 / R[i + (int64_t)i * k];
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int col = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (col >= nrhs) return;
+  double* x = B + (int64_t)col * ldb;
+  double b[VMAX];
+#pragma unroll
+  for (int v = 0; v < VMAX; ++v) {
+    const int i = lane + 32 * v;
+    b[v] = i < k ? x[i] : 0.0;
+  }
+  for (int i = k - 1; i >= 0; --i) {
+    const double xi = __shfl_sync(0xffffffffu, pick(b, i >> 5) * inv[i], i & 31);
+    const double* rc = Rp + up_off(i);
+#pragma unroll
+    for (int v = 0; v < VMAX; ++v) {
+      const int l = lane + 32 * v;
+      if (l < i)
+        b[v] = fma(-rc[l], xi, b[v]);
+      else if (l == i)
+        b[v] = xi;
+    }
+  }
+#pragma unroll
+  for (int v = 0; v < VMAX; ++v) {
+    const int i = lane + 32 * v;
+    if (i < k) x[i] = b[v];
+  }
+}
+
+// Cholesky of the symmetric positive definite G (column-major k x k, lower
+// triangle read) with its factor and inverse: R = L^T and Rinv = R^{-1}
+// (both upper, column-major k x k, zeros below the diagonal). One CTA of
+// 1024 threads, the lower triangle packed in shared memory. Right-looking:
+// step j subtracts L(a, j) L(b, j) / d_j from the trailing triangle using
+// the unscaled column, so one barrier per column suffices; the columns are
+// scaled by sqrt(d_j) afterwards. L^{-1} comes from forward substitution of
+// the unit vectors (one warp per column, the column in registers), and
+// Rinv(j, i) = L^{-1}(i, j). G is read completely before anything is
+// written, so Rinv may alias G. status[0] = 0, or j + 1 when the j-th pivot
+// is not positive (R and Rinv are then not written).
+template <int VMAX>
+__global__ void __launch_bounds__(1024) chol_factor_kernel(const double* G, int k, double* R, double* Rinv,
+                                                           int* status) {
+  extern __shared__ double cf_smem[];
+  double* L = cf_smem;
+  double* aux = L + k * (k + 1) / 2;  // pivots, then their reciprocals
+  for (int q = threadIdx.x; q < k * k; q += blockDim.x) {
+    const int i = q % k, j = q / k;
+    if (i >= j) L[lo_off(j, k) + i - j] = G[q];
+  }
+  __syncthreads();
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  int bad = 0;
+  for (int j = 0; j < k; ++j) {
+    const double d = L[lo_off(j, k)];
+    if (!(d > 0.0)) {  // every thread reads the same pivot: a uniform exit
+      bad = j + 1;
+      break;
+    }
+    const double dinv = 1.0 / d;
+    const double* colj = L + lo_off(j, k) - j;  // colj[a] = L(a, j)
+    for (int b = j + 1 + ty; b < k; b += 32) {
+      const double lbj = colj[b] * dinv;
+      double* colb = L + lo_off(b, k) - b;
+      for (int a = b + tx; a < k; a += 32) colb[a] = fma(-colj[a], lbj, colb[a]);
+    }
+    __syncthreads();
+  }
+  if (bad) {
+    if (threadIdx.x == 0) status[0] = bad;
+    return;
+  }
+  for (int j = threadIdx.x; j < k; j += blockDim.x) aux[j] = sqrt(L[lo_off(j, k)]);
+  __syncthreads();
+  for (int j = ty; j < k; j += 32) {
+    const double p = aux[j];
+    double* colj = L + lo_off(j, k) - j;
+    for (int i = j + tx; i < k; i += 32) colj[i] = (i == j) ? p : colj[i] / p;
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < k * k; q += blockDim.x) {
+    const int i = q % k, j = q / k;
+    R[q] = (i <= j) ? L[lo_off(i, k) + j - i] : 0.0;
+  }
+  for (int j = threadIdx.x; j < k; j += blockDim.x) aux[j] = 1.0 / aux[j];
+  __syncthreads();
+  for (int j = ty; j < k; j += 32) {
+    double b[VMAX];
+#pragma unroll
+    for (int v = 0; v < VMAX; ++v) b[v] = (tx + 32 * v == j) ? 1.0 : 0.0;
+    for (int l = j; l < k; ++l) {
+      const double yl = __shfl_sync(0xffffffffu, pick(b, l >> 5) * aux[l], l & 31);
+      const double* coll = L + lo_off(l, k) - l;
+#pragma unroll
+      for (int v = 0; v < VMAX; ++v) {
+        const int i = tx + 32 * v;
+        if (i > l && i < k)
+          b[v] = fma(-coll[i], yl, b[v]);
+        else if (i == l)
+          b[v] = yl;
+      }
+    }
+#pragma unroll
+    for (int v = 0; v < VMAX; ++v) {
+      const int i = tx + 32 * v;
+      if (i < k) Rinv[j + (int64_t)i * k] = (i >= j) ? b[v] : 0.0;
+    }
+  }
+  if (threadIdx.x == 0) status[0] = 0;
+}
+
 // D = S^T for column-major k x k matrices.
 __global__ void dtranspose_kernel(const double* __restrict__ S, double* __restrict__ D, int64_t k) {
   for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < k * k;
@@ -473,69 +623,81 @@ __global__ void colsparse_apply_smem_kernel(const uint32_t* __restrict__ mp, int
 
 // ------------------------------------------------------ Jacobi SVD ---------
 // One-sided Jacobi on the column-major k x k A (overwritten by A V = U S),
-// V accumulated (column-major k x k). One CTA; each warp rotates pairs.
+// V accumulated (column-major k x k). One CTA; each half-warp rotates one
+// pair of a round-robin round, and a sweep ends the loop when it made no
+// rotation (every pair within tol of orthogonal).
 // SMEM: A and V are worked on in shared memory (2 k^2 doubles), copied in at
 // the start and out at the end; every rotation reads and writes two columns
 // of each, so global memory would put an L2 round trip on every step.
 template <bool SMEM>
-__global__ void __launch_bounds__(1024) jacobi_svd_kernel_t(double* Ag, double* Vg, int64_t k, int max_sweeps,
+__global__ void __launch_bounds__(1024) jacobi_svd_kernel_t(double* Ag, double* Vg, int64_t k64, int max_sweeps,
                                                             double tol, int* sweeps_out) {
-  __shared__ unsigned long long off_max;
+  __shared__ int rotated;
   extern __shared__ double jac_smem[];
+  const int k = (int)k64;
   double* A = SMEM ? jac_smem : Ag;
-  double* V = SMEM ? jac_smem + k * k : Vg;
+  double* V = SMEM ? jac_smem + (size_t)k * k : Vg;
   if (SMEM) {
-    for (int64_t q = threadIdx.x; q < k * k; q += blockDim.x) A[q] = Ag[q];
-    __syncthreads();
+    for (int q = threadIdx.x; q < k * k; q += blockDim.x) A[q] = Ag[q];
   }
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-  for (int64_t q = threadIdx.x; q < k * k; q += blockDim.x) V[q] = (q % k == q / k) ? 1.0 : 0.0;
-  const int64_t kp = (k + 1) & ~(int64_t)1;  // even number of players
+  for (int q = threadIdx.x; q < k * k; q += blockDim.x) V[q] = (q % k == q / k) ? 1.0 : 0.0;
+  // a pair per half-warp: 64 pairs at a time, all of them for k <= 128
+  const int hl = threadIdx.x & 15, slot = threadIdx.x >> 4, nslot = blockDim.x >> 4;
+  const unsigned hmask = (threadIdx.x & 16) ? 0xffff0000u : 0x0000ffffu;
+  const int kp = (k + 1) & ~1;  // even number of players
   int sweep = 0;
   for (; sweep < max_sweeps; ++sweep) {
-    if (threadIdx.x == 0) off_max = 0ull;
+    if (threadIdx.x == 0) rotated = 0;
     __syncthreads();
-    for (int64_t round = 0; round < kp - 1; ++round) {
-      for (int64_t pr = warp; pr < kp / 2; pr += nwarp) {
-        int64_t p, qq;
+    for (int round = 0; round < kp - 1; ++round) {
+      for (int pr = slot; pr < kp / 2; pr += nslot) {
+        // round-robin pairing: player kp-1 stays, the others rotate
+        int p, q;
         if (pr == 0) {
           p = round;
-          qq = kp - 1;
+          q = kp - 1;
         } else {
-          p = (round + pr) % (kp - 1);
-          qq = (round - pr + (kp - 1)) % (kp - 1);
+          p = round + pr;
+          if (p >= kp - 1) p -= kp - 1;
+          q = round - pr;
+          if (q < 0) q += kp - 1;
         }
-        if (p > qq) { const int64_t t = p; p = qq; qq = t; }
-        if (qq >= k) continue;  // bye
-        double* ap = A + p * k;
-        double* aq = A + qq * k;
+        if (p > q) {
+          const int t = p;
+          p = q;
+          q = t;
+        }
+        if (q >= k) continue;  // bye
+        double* ap = A + (size_t)p * k;
+        double* aq = A + (size_t)q * k;
         double al = 0.0, be = 0.0, ga = 0.0;
-        for (int64_t i = lane; i < k; i += 32) {
+        for (int i = hl; i < k; i += 16) {
           const double x = ap[i], y = aq[i];
-          al += x * x;
-          be += y * y;
-          ga += x * y;
+          al = fma(x, x, al);
+          be = fma(y, y, be);
+          ga = fma(x, y, ga);
         }
-        for (int o = 16; o > 0; o >>= 1) {
-          al += __shfl_xor_sync(0xffffffffu, al, o);
-          be += __shfl_xor_sync(0xffffffffu, be, o);
-          ga += __shfl_xor_sync(0xffffffffu, ga, o);
+#pragma unroll
+        for (int o = 8; o > 0; o >>= 1) {
+          al += __shfl_xor_sync(hmask, al, o);
+          be += __shfl_xor_sync(hmask, be, o);
+          ga += __shfl_xor_sync(hmask, ga, o);
         }
         const double den = sqrt(al * be);
         if (den == 0.0 || fabs(ga) <= tol * den) continue;
-        const double rel = fabs(ga) / den;
-        if (lane == 0) atomicMax(&off_max, (unsigned long long)__double_as_longlong(rel));
+        if (hl == 0) rotated = 1;
+        // tan of the rotation angle, the smaller root of t^2 + 2 zeta t - 1
         const double zeta = (be - al) / (2.0 * ga);
-        const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
-        const double cs = 1.0 / sqrt(1.0 + t * t), sn = cs * t;
-        for (int64_t i = lane; i < k; i += 32) {
+        const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(fma(zeta, zeta, 1.0)));
+        const double cs = rsqrt(fma(t, t, 1.0)), sn = cs * t;
+        for (int i = hl; i < k; i += 16) {
           const double x = ap[i], y = aq[i];
           ap[i] = cs * x - sn * y;
           aq[i] = sn * x + cs * y;
         }
-        double* vp = V + p * k;
-        double* vq = V + qq * k;
-        for (int64_t i = lane; i < k; i += 32) {
+        double* vp = V + (size_t)p * k;
+        double* vq = V + (size_t)q * k;
+        for (int i = hl; i < k; i += 16) {
           const double x = vp[i], y = vq[i];
           vp[i] = cs * x - sn * y;
           vq[i] = sn * x + cs * y;
@@ -543,14 +705,14 @@ __global__ void __launch_bounds__(1024) jacobi_svd_kernel_t(double* Ag, double* 
       }
       __syncthreads();
     }
+    const bool more = rotated != 0;
     __syncthreads();
-    if (off_max == 0ull) break;
-    __syncthreads();
+    if (!more) break;
   }
   if (threadIdx.x == 0) sweeps_out[0] = sweep;
   if (SMEM) {
     __syncthreads();
-    for (int64_t q = threadIdx.x; q < k * k; q += blockDim.x) {
+    for (int q = threadIdx.x; q < k * k; q += blockDim.x) {
       Ag[q] = A[q];
       Vg[q] = V[q];
     }
@@ -621,6 +783,62 @@ int g1(const skema_ctx* c, int64_t total) {
   return (int)std::max<int64_t>(1, std::min<int64_t>((total + 255) / 256, (int64_t)c->sm_count * 16));
 }
 
+// R X = B in place for upper-triangular R (k x k) and B (k x nrhs, ld ldb):
+// the packed shared-memory kernel when R fits, else one warp per right-hand
+// side reading R from global memory.
+void trsm_upper(skema_ctx* c, const double* R, int64_t k, double* B, int64_t ldb, int64_t nrhs) {
+  if (nrhs <= 0 || k <= 0) return;
+  if (k <= kPackedMaxK) {
+    const size_t smem = packed_smem_bytes(k);
+    const int grid = (int)((nrhs + 7) / 8);
+    auto launch = [&](auto kern) {
+      SKEMA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      kern<<<grid, 256, smem, c->stream>>>(R, (int)k, B, ldb, (int)nrhs);
+    };
+    if (k <= 32)
+      launch(trsm_upper_packed_kernel<1>);
+    else if (k <= 64)
+      launch(trsm_upper_packed_kernel<2>);
+    else if (k <= 128)
+      launch(trsm_upper_packed_kernel<4>);
+    else
+      launch(trsm_upper_packed_kernel<8>);
+  } else {
+    trsm_upper_kernel<<<(int)((nrhs * 32 + 255) / 256), 256, 0, c->stream>>>(R, k, B, ldb, nrhs);
+  }
+  SKEMA_LAUNCHED(c);
+}
+
+// Cholesky G = L L^T of the k x k G with R = L^T and Rinv = R^{-1} (Rinv may
+// alias G); st[0] as chol_factor_kernel sets it, read by the caller. G is
+// consumed. When the factorisation fails R and Rinv hold no meaning.
+void chol_inverse(skema_ctx* c, double* G, int64_t k, double* R, double* Rinv, int* st) {
+  if (k <= kPackedMaxK) {
+    const size_t smem = packed_smem_bytes(k);
+    auto launch = [&](auto kern) {
+      SKEMA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      kern<<<1, 1024, smem, c->stream>>>(G, (int)k, R, Rinv, st);
+    };
+    if (k <= 32)
+      launch(chol_factor_kernel<1>);
+    else if (k <= 64)
+      launch(chol_factor_kernel<2>);
+    else if (k <= 128)
+      launch(chol_factor_kernel<4>);
+    else
+      launch(chol_factor_kernel<8>);
+    SKEMA_LAUNCHED(c);
+    return;
+  }
+  cholesky_kernel<<<1, 1024, 0, c->stream>>>(G, k, st);
+  SKEMA_LAUNCHED(c);
+  lower_to_upper_kernel<<<g1(c, k * k), 256, 0, c->stream>>>(G, R, k);
+  SKEMA_LAUNCHED(c);
+  identity_kernel<<<g1(c, k * k), 256, 0, c->stream>>>(Rinv, k);
+  SKEMA_LAUNCHED(c);
+  trsm_upper(c, R, k, Rinv, k, k);
+}
+
 // In-place CholeskyQR2 (+ shifted pre-pass if needed) of the column-major
 // rows x k matrix Qm (ld = rows). On return Rout (k x k, upper, column-major)
 // holds R with Q_in = Q_out R. False when a Cholesky failed even after the
@@ -642,8 +860,7 @@ bool cholqr_try(skema_ctx* c, double* Qm, int64_t rows, int64_t k, double* Rout,
   while (passes_left > 0) {
     // G = Q^T Q
     gram(c, cur, rows, rows, k, G);
-    cholesky_kernel<<<1, 1024, 0, c->stream>>>(G, k, dstatus);
-    SKEMA_LAUNCHED(c);
+    chol_inverse(c, G, k, R, G, dstatus);
     int st = 0;
     SKEMA_CUDA(cudaMemcpyAsync(&st, dstatus, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     SKEMA_CUDA(cudaStreamSynchronize(c->stream));
@@ -662,8 +879,7 @@ bool cholqr_try(skema_ctx* c, double* Qm, int64_t rows, int64_t k, double* Rout,
       shift_diag_kernel<<<(int)((k + 255) / 256), 256, 0, c->stream>>>(
           G, k, fro2, 11.0 * ((double)rows * k + (double)k * (k + 1)) * u);
       SKEMA_LAUNCHED(c);
-      cholesky_kernel<<<1, 1024, 0, c->stream>>>(G, k, dstatus);
-      SKEMA_LAUNCHED(c);
+      chol_inverse(c, G, k, R, G, dstatus);
       SKEMA_CUDA(cudaMemcpyAsync(&st, dstatus, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
       SKEMA_CUDA(cudaStreamSynchronize(c->stream));
       if (st != 0) {
@@ -675,16 +891,7 @@ bool cholqr_try(skema_ctx* c, double* Qm, int64_t rows, int64_t k, double* Rout,
       shifted = true;
       passes_left = 3;  // shifted pass + CholeskyQR2
     }
-    lower_to_upper_kernel<<<g1(c, k * k), 256, 0, c->stream>>>(G, R, k);
-    SKEMA_LAUNCHED(c);
-    // Q <- Q R^{-1}: solve R^T Q^T = ... via rows: transpose form R^T x = q_row
-    // done as Q^T <- R^{-T} Q^T; equivalently solve with the inverse:
-    // Rinv = R^{-1} (upper) then Q <- Q Rinv.
-    identity_kernel<<<g1(c, k * k), 256, 0, c->stream>>>(G, k);
-    SKEMA_LAUNCHED(c);
-    trsm_upper_kernel<<<(int)((k * 32 + 255) / 256), 256, 0, c->stream>>>(R, k, G, k, k);
-    SKEMA_LAUNCHED(c);
-    // next <- cur * Rinv  (rows x k)
+    // Q <- Q R^{-1} with G = R^{-1} (upper): next <- cur * Rinv (rows x k)
     tall_times_small(c, cur, rows, rows, k, G, k, k, nxt, rows);
     std::swap(cur, nxt);
     // Racc <- R * Racc
@@ -920,18 +1127,11 @@ void spd_low_rank_approx(skema_ctx* c, double* Uout, double* Sout) {
   dgemm<double, double>(c, k, k, n, 1.0, Od, n, 1, Ye, 1, m, 0.0, Cw, 1, k);
   symmetrize_kernel<<<g1(c, k * k), 256, 0, c->stream>>>(Cw, G, k);
   SKEMA_LAUNCHED(c);
-  cholesky_kernel<<<1, 1024, 0, c->stream>>>(G, k, st);
-  SKEMA_LAUNCHED(c);
+  chol_inverse(c, G, k, R, Rinv, st);
   int bad = 0;
   SKEMA_CUDA(cudaMemcpyAsync(&bad, st, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   SKEMA_CUDA(cudaStreamSynchronize(c->stream));
   if (bad != 0) fail(SKEMA_ENOTPD, "SketchySPD: (B + B^T) / 2 is not positive definite (dpotrf would fail)");
-  lower_to_upper_kernel<<<g1(c, k * k), 256, 0, c->stream>>>(G, R, k);
-  SKEMA_LAUNCHED(c);
-  identity_kernel<<<g1(c, k * k), 256, 0, c->stream>>>(Rinv, k);
-  SKEMA_LAUNCHED(c);
-  trsm_upper_kernel<<<(int)((k * 32 + 255) / 256), 256, 0, c->stream>>>(R, k, Rinv, k, k);
-  SKEMA_LAUNCHED(c);
   // E = (Y_eta or Y) R^{-1}, into Yd's buffer when it is no longer needed
   double* E = ref_steps ? Ye : Yd;
   const double* src = ref_steps ? Yd : Ye;
@@ -999,13 +1199,11 @@ void low_rank_approx(skema_ctx* c, double* Uout, double* Sout, double* Vout) {
   dgemm<double, double>(c, k, s, s, 1.0, U1, s, 1, Zd, 1, s, 0.0, Z1, 1, k);
   dgemm<double, double>(c, k, k, s, 1.0, Z1, 1, k, U2, 1, s, 0.0, Z2, 1, k);
   // Z2 = T1 \ Z2
-  trsm_upper_kernel<<<(int)((k * 32 + 255) / 256), 256, 0, c->stream>>>(T1, k, Z2, k, k);
-  SKEMA_LAUNCHED(c);
+  trsm_upper(c, T1, k, Z2, k, k);
   // C^T = T2 \ Z2^T
   dtranspose_kernel<<<g1(c, k * k), 256, 0, c->stream>>>(Z2, Z2t, k);
   SKEMA_LAUNCHED(c);
-  trsm_upper_kernel<<<(int)((k * 32 + 255) / 256), 256, 0, c->stream>>>(T2, k, Z2t, k, k);
-  SKEMA_LAUNCHED(c);
+  trsm_upper(c, T2, k, Z2t, k, k);
   // C = (Z2t)^T: copy into Uc's slot as the Jacobi working matrix
   double* C = Uc;
   {

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -235,6 +236,10 @@ static void free_all(skema_ctx* c) {
   if (c->side) cudaStreamDestroy(c->side);
   if (c->fork_ev) cudaEventDestroy(c->fork_ev);
   if (c->join_ev) cudaEventDestroy(c->join_ev);
+  for (cudaEvent_t& e : c->pipe_ev) {
+    if (e) cudaEventDestroy(e);
+    e = nullptr;
+  }
   c->side = nullptr;
   c->fork_ev = c->join_ev = nullptr;
 }
@@ -386,6 +391,12 @@ int skema_create(const skema_params* p, skema_ctx** out) {
     SKEMA_CUDA(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
     SKEMA_CUDA(cudaEventCreateWithFlags(&c->fork_ev, cudaEventDisableTiming));
     SKEMA_CUDA(cudaEventCreateWithFlags(&c->join_ev, cudaEventDisableTiming));
+    for (cudaEvent_t& e : c->pipe_ev) SKEMA_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    c->pipe_xt_sms = 0;
+    c->pipe_windows = 2;
+    if (const char* v = std::getenv("SKEMA_DENSE_PIPE_SMS")) c->pipe_xt_sms = std::max(0, std::atoi(v));
+    if (const char* v = std::getenv("SKEMA_DENSE_PIPE_WINDOWS")) c->pipe_windows = std::max(1, std::atoi(v));
+    if (c->pipe_xt_sms >= c->sm_count) c->pipe_xt_sms = 0;
     plan_maps(c);
     if (c->spd) {
       map_generate(c, c->omg, p->precision);

@@ -91,11 +91,12 @@ CUtensorMap tmap_bf16(const void* base, uint64_t d0, uint64_t d1, uint64_t st1, 
 
 Plan plan_split(const skema_ctx* c, int64_t tiles, int64_t K, int max_ks) {
   const int64_t ksteps = (K + tc::BK - 1) / tc::BK;
+  const int64_t ctas = c->tc_cta_cap > 0 ? std::min(c->tc_cta_cap, c->sm_count) : c->sm_count;
   int best = 1;
   double best_cost = 1e300;
   for (int ks = 1; ks <= max_ks; ++ks) {
     if (ks > 1 && ksteps / ks < 8) break;  // at least 8 k-steps per split
-    const int64_t waves = (tiles * ks + c->sm_count - 1) / c->sm_count;
+    const int64_t waves = (tiles * ks + ctas - 1) / ctas;
     // a split adds atomic partial sums to every output element; their cost
     // shows as about 12 k-steps per wave
     const double cost = (double)waves * ((double)ksteps / ks + 6.0 + (ks > 1 ? 12.0 : 0.0));
@@ -298,6 +299,7 @@ tc::Grid3 grid_of(const skema_ctx* c, int64_t M, int64_t N, int64_t K, int nt, i
   const int64_t units = (int64_t)g.mtiles * g.ntiles * (g.streamk ? g.ksteps : g.ksplit);
   if (units > 0x7fffffff) fail(SKEMA_EINVAL, "tensor-core grid too large");
   *grid = (int)std::min<int64_t>(units, g.streamk ? pl.streamk : c->sm_count);
+  if (c->tc_cta_cap > 0) *grid = std::min(*grid, c->tc_cta_cap);
   if (M <= 0 || N <= 0 || K <= 0) *grid = 0;
   return g;
 }
@@ -778,6 +780,29 @@ void tc_dense_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr, void* scratch
   tc_z_update(c, T16, wp, sl, wr, nu);
 }
 
+namespace {
+
+// Runs the launches of the helpers in its scope on `stream` with at most
+// `cap` CTAs each (0: one per SM), restoring the context's own on exit.
+class LaunchScope {
+ public:
+  LaunchScope(skema_ctx* c, cudaStream_t stream, int cap) : c_(c), stream_(c->stream), cap_(c->tc_cta_cap) {
+    c->stream = stream;
+    c->tc_cta_cap = cap;
+  }
+  ~LaunchScope() {
+    c_->stream = stream_;
+    c_->tc_cta_cap = cap_;
+  }
+
+ private:
+  skema_ctx* c_;
+  cudaStream_t stream_;
+  int cap_;
+};
+
+}  // namespace
+
 // The windows of one call. X^T runs per window (the recurrence X = nu X +
 // eta x_w); [Y | T] and Z run once per group of windows: Y rows are
 // disjoint, so a window's Y rows need only its own product, and Z = nu^G Z
@@ -787,9 +812,17 @@ void tc_dense_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr, void* scratch
 // tens of thousands of rows needs no K split (its tile count fills the SMs
 // many times over), and one Z^T product over the group avoids a product per
 // window that was bound by its split-K atomics. The group's BF16 (or E4M3)
-// window copies and T are kept: groups are capped at 2 GB of A16 and 512 MB
-// of T. Windows that do not start on 64-row blocks, or nu <= 0, take one
-// window at a time.
+// window copies and T are kept. Windows that do not start on 64-row blocks,
+// or nu <= 0, take one window at a time.
+//
+// Pipeline (pipe_xt_sms > 0): X^T streams the FP32 windows from HBM and
+// leaves the tensor pipe mostly idle, [Y | T] reads the BF16 copies and is
+// bound by the tensor pipe. X^T of group g + 1 therefore runs on the
+// context stream with pipe_xt_sms CTAs while [Y | T] and Z of group g run on
+// the side stream with the other SMs. Two copy buffers alternate: X^T of
+// group g + 2 waits for [Y | T] of group g to finish reading its buffer.
+// X and its per-window slices stay on the context stream; Y, T, Z and the
+// group's slices on the side stream, so every buffer has one writer.
 void tc_dense_update(skema_ctx* c, Mat A, int64_t row0, int64_t nrows) {
   const int64_t W = c->w, s = c->s, n = c->n;
   const float nu = (float)c->p.sketch_nu;
@@ -800,8 +833,12 @@ void tc_dense_update(skema_ctx* c, Mat A, int64_t row0, int64_t nrows) {
       tc_dense_window(c, Mat{A.p + r * A.rs, A.rs, A.cs}, row0 + r, std::min(W, nrows - r), ws);
     return;
   }
+  const bool pipe = c->pipe_xt_sms > 0 && c->pipe_xt_sms < c->sm_count;
+  const int nbuf = pipe ? 2 : 1;
   const int64_t cap_a = ((int64_t)2 << 30) / (2 * n), cap_t = ((int64_t)512 << 20) / (2 * s);
-  const int64_t grows = std::min(nrows, std::max<int64_t>(1, std::min(cap_a, cap_t) / W) * W);
+  int64_t gwin = std::max<int64_t>(1, std::min(cap_a, cap_t) / W);
+  if (pipe) gwin = std::min(gwin, c->pipe_windows);
+  const int64_t grows = std::min(nrows, gwin * W);
   const int64_t gwin_max = (grows + W - 1) / W;
   const int64_t ldT = pad8(grows), ld8 = (n + 15) / 16 * 16;
   auto rup = [](size_t b) { return (b + 255) / 256 * 256; };
@@ -809,43 +846,86 @@ void tc_dense_update(skema_ctx* c, Mat A, int64_t row0, int64_t nrows) {
   const size_t b_a8 = fp8 ? rup((size_t)(grows * ld8)) : 0;
   const size_t b_t16 = rup(sizeof(__nv_bfloat16) * (size_t)(ldT * s));
   const size_t b_t32 = rup(sizeof(float) * (size_t)(ldT * s));
-  const size_t b_sl = rup(tc_slice_bytes(c, grows)) + rup(tc_slice_bytes(c, W));
-  char* ws = static_cast<char*>(workspace(c, b_a16 + b_a8 + b_t16 + b_t32 + b_sl));
-  __nv_bfloat16* A16 = reinterpret_cast<__nv_bfloat16*>(ws);
-  uint8_t* A8 = reinterpret_cast<uint8_t*>(ws + b_a16);
-  __nv_bfloat16* T16 = reinterpret_cast<__nv_bfloat16*>(ws + b_a16 + b_a8);
-  float* T32 = reinterpret_cast<float*>(ws + b_a16 + b_a8 + b_t16);
-  char* slice_sp = ws + b_a16 + b_a8 + b_t16 + b_t32;
-  uint32_t* amax = nullptr;
-  float* scales = nullptr;
-  if (fp8) {
-    if (c->fp8_win_cap < gwin_max) {
-      if (c->fp8_win) cudaFree(c->fp8_win);
-      SKEMA_CUDA(cudaMalloc(&c->fp8_win, sizeof(uint32_t) * (size_t)(2 * gwin_max)));
-      c->fp8_win_cap = gwin_max;
-    }
-    amax = c->fp8_win;
-    scales = reinterpret_cast<float*>(c->fp8_win + gwin_max);
+  const size_t b_gsl = rup(tc_slice_bytes(c, grows)), b_wsl = rup(tc_slice_bytes(c, W));
+  char* ws = static_cast<char*>(workspace(c, nbuf * (b_a16 + b_a8) + b_t16 + b_t32 + b_gsl + b_wsl));
+  __nv_bfloat16* A16b[2];
+  uint8_t* A8b[2];
+  for (int b = 0; b < nbuf; ++b) {
+    A16b[b] = reinterpret_cast<__nv_bfloat16*>(ws + b * b_a16);
+    A8b[b] = reinterpret_cast<uint8_t*>(ws + nbuf * b_a16 + b * b_a8);
   }
-  const float log2nu = nu == 1.f ? 0.f : std::log2(nu);
-  for (int64_t g0 = 0; g0 < nrows; g0 += grows) {
-    const int64_t gr = std::min(grows, nrows - g0), G = (gr + W - 1) / W, R0 = row0 + g0;
-    if (fp8) SKEMA_CUDA(cudaMemsetAsync(amax, 0, sizeof(uint32_t) * (size_t)(2 * gwin_max), c->stream));
-    for (int64_t w = 0; w < G; ++w) {
-      const int64_t r = g0 + w * W, wr = std::min(W, nrows - r);
-      __nv_bfloat16* A16w = A16 + (w * W / 64) * 64 * n;
-      char* sp = slice_sp + rup(tc_slice_bytes(c, grows));
-      xt_window(c, Mat{A.p + r * A.rs, A.rs, A.cs}, row0 + r, wr, A16w, fp8 ? amax + w : nullptr, &sp);
-      if (fp8) to_a8(c, A16w, wr, A8 + w * W * ld8, ld8, amax + w, scales + w);
+  char* tail = ws + nbuf * (b_a16 + b_a8);
+  __nv_bfloat16* T16 = reinterpret_cast<__nv_bfloat16*>(tail);
+  float* T32 = reinterpret_cast<float*>(tail + b_t16);
+  char* gslice_sp = tail + b_t16 + b_t32;   // the group's slices (side stream)
+  char* wslice_sp = gslice_sp + b_gsl;      // one window's slices (context stream)
+  // FP8: per buffer, gwin_max window amax words then gwin_max scales
+  uint32_t* amaxb[2] = {nullptr, nullptr};
+  float* scalesb[2] = {nullptr, nullptr};
+  if (fp8) {
+    if (c->fp8_win_cap < 2 * gwin_max) {
+      if (c->fp8_win) cudaFree(c->fp8_win);
+      c->fp8_win = nullptr;
+      c->fp8_win_cap = 0;
+      SKEMA_CUDA(cudaMalloc(&c->fp8_win, sizeof(uint32_t) * (size_t)(4 * gwin_max)));
+      c->fp8_win_cap = 2 * gwin_max;
     }
-    YtSpec y{};
-    y.R0 = R0, y.gr = gr, y.A16 = A16, y.A8 = A8, y.ld8 = ld8, y.scales = scales, y.T32 = T32;
-    y.Tdst = T16, y.ldTd = ldT, y.log2w = log2nu, y.wlen = W, y.nwin = G;
-    yt_product(c, y);
-    y_rows_mark(c, R0, R0 + gr);
-    char* sp = slice_sp;
-    const TcSlices sl = tc_window_slices(c, R0, gr, &sp);
-    tc_z_update(c, T16, ldT, sl, gr, std::pow(nu, (float)G));
+    for (int b = 0; b < nbuf; ++b) {
+      amaxb[b] = c->fp8_win + b * 2 * gwin_max;
+      scalesb[b] = reinterpret_cast<float*>(amaxb[b] + gwin_max);
+    }
+  }
+  const cudaStream_t main_st = c->stream;
+  const cudaStream_t yt_st = pipe ? c->side : c->stream;
+  const int xt_cap = pipe ? c->pipe_xt_sms : 0, yt_cap = pipe ? c->sm_count - c->pipe_xt_sms : 0;
+  if (pipe) {
+    // the side stream starts after all earlier work of the context stream
+    SKEMA_CUDA(cudaEventRecord(c->fork_ev, main_st));
+    SKEMA_CUDA(cudaStreamWaitEvent(yt_st, c->fork_ev, 0));
+  }
+  // and the context stream continues after all of the side stream's work,
+  // also when a launch below fails
+  struct Join {
+    skema_ctx* c;
+    bool on;
+    ~Join() {
+      if (on && cudaEventRecord(c->join_ev, c->side) == cudaSuccess) cudaStreamWaitEvent(c->stream, c->join_ev, 0);
+    }
+  } join{c, pipe};
+  const float log2nu = nu == 1.f ? 0.f : std::log2(nu);
+  int64_t gi = 0;
+  for (int64_t g0 = 0; g0 < nrows; g0 += grows, ++gi) {
+    const int b = (int)(gi % nbuf);
+    const int64_t gr = std::min(grows, nrows - g0), G = (gr + W - 1) / W, R0 = row0 + g0;
+    __nv_bfloat16* A16 = A16b[b];
+    uint8_t* A8 = A8b[b];
+    {
+      LaunchScope ls(c, main_st, xt_cap);
+      // the buffer's previous group must have been read by its [Y | T]
+      if (pipe && gi >= nbuf) SKEMA_CUDA(cudaStreamWaitEvent(main_st, c->pipe_ev[2 + b], 0));
+      if (fp8) SKEMA_CUDA(cudaMemsetAsync(amaxb[b], 0, sizeof(uint32_t) * (size_t)(2 * gwin_max), main_st));
+      for (int64_t w = 0; w < G; ++w) {
+        const int64_t r = g0 + w * W, wr = std::min(W, nrows - r);
+        __nv_bfloat16* A16w = A16 + (w * W / 64) * 64 * n;
+        char* sp = wslice_sp;
+        xt_window(c, Mat{A.p + r * A.rs, A.rs, A.cs}, row0 + r, wr, A16w, fp8 ? amaxb[b] + w : nullptr, &sp);
+        if (fp8) to_a8(c, A16w, wr, A8 + w * W * ld8, ld8, amaxb[b] + w, scalesb[b] + w);
+      }
+      if (pipe) SKEMA_CUDA(cudaEventRecord(c->pipe_ev[b], main_st));
+    }
+    {
+      LaunchScope ls(c, yt_st, yt_cap);
+      if (pipe) SKEMA_CUDA(cudaStreamWaitEvent(yt_st, c->pipe_ev[b], 0));
+      YtSpec y{};
+      y.R0 = R0, y.gr = gr, y.A16 = A16, y.A8 = A8, y.ld8 = ld8, y.scales = scalesb[b], y.T32 = T32;
+      y.Tdst = T16, y.ldTd = ldT, y.log2w = log2nu, y.wlen = W, y.nwin = G;
+      yt_product(c, y);
+      y_rows_mark(c, R0, R0 + gr);
+      char* sp = gslice_sp;
+      const TcSlices sl = tc_window_slices(c, R0, gr, &sp);
+      tc_z_update(c, T16, ldT, sl, gr, std::pow(nu, (float)G));
+      if (pipe) SKEMA_CUDA(cudaEventRecord(c->pipe_ev[2 + b], yt_st));
+    }
   }
 }
 

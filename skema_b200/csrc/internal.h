@@ -99,6 +99,9 @@ struct skema_ctx {
   // call (forked from and joined back to `stream` before the call returns).
   cudaStream_t side = nullptr;
   cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
+  // Hand-offs between the two streams of the BF16 dense pipeline (window
+  // copies ready / released, one pair per copy buffer).
+  cudaEvent_t pipe_ev[4] = {nullptr, nullptr, nullptr, nullptr};
   std::string err;
   int64_t launches = 0;
   skema::Map ups, omg, phi, psi;
@@ -121,6 +124,15 @@ struct skema_ctx {
   size_t stage_bytes = 0;
   size_t ws_limit = 0;    // cap on ws_bytes + stage_bytes (0: none)
   int sm_count = 148;
+  // Upper bound on the CTAs of one tensor-core launch (0: one per SM); set
+  // while the dense pipeline splits the SMs between its two streams.
+  int tc_cta_cap = 0;
+  // Dense BF16 / FP8 pipeline: SMs given to the X^T product (0: no
+  // pipeline, the products run one after another on all SMs) and windows
+  // per [Y | T] group. Defaults set at creation; SKEMA_DENSE_PIPE_SMS and
+  // SKEMA_DENSE_PIPE_WINDOWS override them.
+  int pipe_xt_sms = 0;
+  int64_t pipe_windows = 2;
   int cc_major = 0, cc_minor = 0;
   // BF16 tensor-core form: Omega~ and Psi~ stacked as one (k+s) x n
   // row-major operand (ld_op16), Upsilon~ / Phi~ copies in Map::lowp with

@@ -365,3 +365,34 @@ def test_dense_tc_many_windows_one_call_nu(sk, oracle, prec, window):
             check(s, o, "six windows")
         else:
             check8(s, o, "six windows")
+
+
+@pytest.mark.parametrize("prec", ["bf16", "fp8"])
+@pytest.mark.parametrize("sms,windows", [(40, 1), (74, 2)])
+def test_dense_tc_two_stream_pipeline(sk, oracle, monkeypatch, prec, sms, windows):
+    # X^T on its own share of the SMs (context stream) beside [Y | T] and Z
+    # of the previous group (side stream), two window-copy buffers in turn:
+    # seven 256-row windows give four to seven groups, so each buffer is
+    # refilled while the other one's group is still being read; two calls,
+    # the second over rows the first wrote (its Y rows get the nu term)
+    import torch
+
+    monkeypatch.setenv("SKEMA_DENSE_PIPE_SMS", str(sms))
+    monkeypatch.setenv("SKEMA_DENSE_PIPE_WINDOWS", str(windows))
+    m, n = 1800, 600
+    A = dense_input(m, n, seed=33).astype(np.float32)
+    a = alg(sk, m, n, 8, 256, 0, sketch_eta=0.75, sketch_nu=0.9)
+    a = bf16(a, sk) if prec == "bf16" else fp8(a, sk)
+    o = oracle_for(oracle, a)
+    if prec == "fp8":
+        e4m3_grid(o.maps)
+    o.linear_update(A.astype(np.float64))
+    o.update_rows(A[:1024].astype(np.float64), 0, 1024)
+    with sk.SketchySVD(a) as s:
+        At = torch.from_numpy(A).cuda()
+        s.linear_update(At)
+        s.update_rows(At[:1024], 0)
+        if prec == "bf16":
+            check(s, o, f"pipeline {sms} SMs, {windows} windows per group")
+        else:
+            check8(s, o, f"pipeline {sms} SMs, {windows} windows per group")
