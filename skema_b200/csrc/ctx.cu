@@ -2,6 +2,7 @@
 // resolution, map orientation, sketch import/export and dispatch of the
 // linear update to the kernels of the other translation units.
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <cstdlib>
@@ -173,12 +174,16 @@ static cudaEvent_t pool_event(skema_ctx* c) {
 StageScope::StageScope(skema_ctx* c, int stage) : StageScope(c, stage, c->stream) {}
 
 StageScope::StageScope(skema_ctx* c, int stage, cudaStream_t stream) : c_(c), stage_(stage), stream_(stream) {
+  // an NVTX range per stage (host-side: a profiler that records NVTX shows
+  // the stage around its launches; without one the call is a no-op)
+  nvtxRangePushA(kStageNames[stage]);
   if (!c_->timing) return;
   a_ = pool_event(c_);
   SKEMA_CUDA(cudaEventRecord(a_, stream_));
 }
 
 StageScope::~StageScope() {
+  nvtxRangePop();
   if (!a_) return;
   cudaEvent_t b = nullptr;
   if (!c_->event_pool.empty()) {
@@ -397,6 +402,8 @@ int skema_create(const skema_params* p, skema_ctx** out) {
     if (const char* v = std::getenv("SKEMA_DENSE_PIPE_SMS")) c->pipe_xt_sms = std::max(0, std::atoi(v));
     if (const char* v = std::getenv("SKEMA_DENSE_PIPE_WINDOWS")) c->pipe_windows = std::max(1, std::atoi(v));
     if (c->pipe_xt_sms >= c->sm_count) c->pipe_xt_sms = 0;
+    c->xt_direct = false;
+    if (const char* v = std::getenv("SKEMA_XT_STORE")) c->xt_direct = std::strcmp(v, "direct") == 0;
     plan_maps(c);
     if (c->spd) {
       map_generate(c, c->omg, p->precision);

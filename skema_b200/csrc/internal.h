@@ -133,6 +133,10 @@ struct skema_ctx {
   // SKEMA_DENSE_PIPE_WINDOWS override them.
   int pipe_xt_sms = 0;
   int64_t pipe_windows = 2;
+  // X^T product from the FP32 window: the converter threads copy the BF16
+  // window copy out (true) or one TMA store per tile does (false).
+  // SKEMA_XT_STORE=tma|direct overrides the default.
+  bool xt_direct = false;
   int cc_major = 0, cc_minor = 0;
   // BF16 tensor-core form: Omega~ and Psi~ stacked as one (k+s) x n
   // row-major operand (ld_op16), Upsilon~ / Phi~ copies in Map::lowp with
