@@ -400,7 +400,12 @@ int64_t skema_launch_count(const skema_ctx* ctx);
  *   "update.window"  kernel-window generation
  *   "update.fused"   the fused tensor-core window kernel
  *   "update.daxpy"   sketch scaling by nu
- * Unknown names give SKEMA_EINVAL. */
+ *   "approx.orth"    orthonormal bases of Y and X^T (skema_low_rank_approx)
+ *   "approx.core"    the core matrix: Phi Q, Psi P, their QR and the solves
+ *   "approx.svd"     the core matrix's SVD
+ *   "approx.vectors" U = Q Uc and V = P Vc
+ * "approx.svd_sweeps" gives 0 ms and, as the count, the sweeps of the last
+ * core-matrix SVD (one-sided Jacobi). Unknown names give SKEMA_EINVAL. */
 int skema_timing_enable(skema_ctx* ctx, int32_t on);
 int skema_timing_get(skema_ctx* ctx, const char* stage, double* ms, int64_t* count);
 

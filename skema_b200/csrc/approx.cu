@@ -24,6 +24,7 @@
 #include <cmath>
 #include <initializer_list>
 #include <limits>
+#include <memory>
 #include <vector>
 
 #include "internal.h"
@@ -1181,6 +1182,7 @@ void low_rank_approx(skema_ctx* c, double* Uout, double* Sout, double* Vout) {
   double* Zd = sig + k;            // s x s
   int* st = reinterpret_cast<int*>(cv.take(16));
 
+  auto orth_scope = std::make_unique<StageScope>(c, ST_A_ORTH);
   // Q = Y (m x k, column-major, FP64); P = X^T (n x k, column-major)
   f2d_kernel<<<g1(c, m * k), 256, 0, c->stream>>>(c->Y, 1, m, Q, 1, m, m, k);
   SKEMA_LAUNCHED(c);
@@ -1190,6 +1192,8 @@ void low_rank_approx(skema_ctx* c, double* Uout, double* Sout, double* Vout) {
   SKEMA_LAUNCHED(c);
   orth(c, P, n, k, T1, W, st);  // T1 used as scratch R here
   orth(c, Q, m, k, T1, W, st);
+  orth_scope.reset();
+  auto core_scope = std::make_unique<StageScope>(c, ST_A_CORE);
   // U1 = Phi~ Q (s x k), U2 = Psi~ P (s x k)
   apply_map(c, c->phi, Q, m, k, U1);
   apply_map(c, c->psi, P, n, k, U2);
@@ -1206,7 +1210,9 @@ void low_rank_approx(skema_ctx* c, double* Uout, double* Sout, double* Vout) {
   trsm_upper(c, T2, k, Z2t, k, k);
   // C = (Z2t)^T: copy into Uc's slot as the Jacobi working matrix
   double* C = Uc;
+  core_scope.reset();
   {
+    StageScope sc(c, ST_A_SVD);
     double* Cw = W;  // k x k working copy
     dtranspose_kernel<<<g1(c, k * k), 256, 0, c->stream>>>(Z2t, Cw, k);
     SKEMA_LAUNCHED(c);
@@ -1214,12 +1220,18 @@ void low_rank_approx(skema_ctx* c, double* Uout, double* Sout, double* Vout) {
     svd_finish_kernel<<<1, 256, 0, c->stream>>>(Cw, Vc, k, C, Z2 /*Vout*/, Sv, sig);
     SKEMA_LAUNCHED(c);
   }
-  // U = Q Uc(:, 1:r), V = P Vc(:, 1:r), S = S(1:r)
-  if (Uout) tall_times_small(c, Q, m, m, k, C, k, r, Uout, m);
-  if (Vout) tall_times_small(c, P, n, n, k, Z2, k, r, Vout, n);
-  if (Sout)
-    SKEMA_CUDA(cudaMemcpyAsync(Sout, Sv, sizeof(double) * (size_t)r, cudaMemcpyDeviceToDevice, c->stream));
+  {
+    StageScope sc(c, ST_A_VECTORS);
+    // U = Q Uc(:, 1:r), V = P Vc(:, 1:r), S = S(1:r)
+    if (Uout) tall_times_small(c, Q, m, m, k, C, k, r, Uout, m);
+    if (Vout) tall_times_small(c, P, n, n, k, Z2, k, r, Vout, n);
+    if (Sout)
+      SKEMA_CUDA(cudaMemcpyAsync(Sout, Sv, sizeof(double) * (size_t)r, cudaMemcpyDeviceToDevice, c->stream));
+  }
+  int sweeps = 0;
+  SKEMA_CUDA(cudaMemcpyAsync(&sweeps, st + 1, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   SKEMA_CUDA(cudaStreamSynchronize(c->stream));
+  c->svd_sweeps = sweeps;
 }
 
 }  // namespace skema

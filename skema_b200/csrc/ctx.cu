@@ -158,7 +158,8 @@ void xz_materialize(skema_ctx* c, cudaStream_t stream) {
 
 const char* const kStageNames[ST_COUNT] = {"update.omega",   "update.psi",    "update.upsilon",
                                             "update.phi",     "update.entries", "update.window",
-                                            "update.fused",   "update.daxpy"};
+                                            "update.fused",   "update.daxpy",  "approx.orth",
+                                            "approx.core",    "approx.svd",    "approx.vectors"};
 
 static cudaEvent_t pool_event(skema_ctx* c) {
   if (!c->event_pool.empty()) {
@@ -402,8 +403,6 @@ int skema_create(const skema_params* p, skema_ctx** out) {
     if (const char* v = std::getenv("SKEMA_DENSE_PIPE_SMS")) c->pipe_xt_sms = std::max(0, std::atoi(v));
     if (const char* v = std::getenv("SKEMA_DENSE_PIPE_WINDOWS")) c->pipe_windows = std::max(1, std::atoi(v));
     if (c->pipe_xt_sms >= c->sm_count) c->pipe_xt_sms = 0;
-    c->xt_direct = false;
-    if (const char* v = std::getenv("SKEMA_XT_STORE")) c->xt_direct = std::strcmp(v, "direct") == 0;
     plan_maps(c);
     if (c->spd) {
       map_generate(c, c->omg, p->precision);
@@ -916,6 +915,11 @@ int skema_timing_get(skema_ctx* c, const char* stage, double* ms, int64_t* count
   return guarded(c, [&] {
     if (!stage) fail(SKEMA_EINVAL, "null stage name");
     drain_timers(c);
+    if (std::strcmp(stage, "approx.svd_sweeps") == 0) {
+      if (ms) *ms = 0.0;
+      if (count) *count = c->svd_sweeps;
+      return;
+    }
     for (int i = 0; i < ST_COUNT; ++i) {
       if (std::strcmp(stage, kStageNames[i]) == 0) {
         if (ms) *ms = c->stage_ms[i];

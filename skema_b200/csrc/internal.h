@@ -77,6 +77,10 @@ enum Stage {
   ST_WINDOW,
   ST_FUSED,
   ST_DAXPY,
+  ST_A_ORTH,     // orthonormal bases of Y and X^T
+  ST_A_CORE,     // the core matrix: Phi Q, Psi P, their QR and the solves
+  ST_A_SVD,      // the core matrix's SVD
+  ST_A_VECTORS,  // U = Q Uc, V = P Vc
   ST_COUNT
 };
 extern const char* const kStageNames[ST_COUNT];
@@ -133,10 +137,6 @@ struct skema_ctx {
   // SKEMA_DENSE_PIPE_WINDOWS override them.
   int pipe_xt_sms = 0;
   int64_t pipe_windows = 2;
-  // X^T product from the FP32 window: the converter threads copy the BF16
-  // window copy out (true) or one TMA store per tile does (false).
-  // SKEMA_XT_STORE=tma|direct overrides the default.
-  bool xt_direct = false;
   int cc_major = 0, cc_minor = 0;
   // BF16 tensor-core form: Omega~ and Psi~ stacked as one (k+s) x n
   // row-major operand (ld_op16), Upsilon~ / Phi~ copies in Map::lowp with
@@ -175,6 +175,8 @@ struct skema_ctx {
   bool timing = false;
   std::vector<skema::PendingTimer> pending;
   std::vector<cudaEvent_t> event_pool;
+  // Sweeps of the last core-matrix SVD (the Jacobi iteration's count).
+  int64_t svd_sweeps = 0;
   double stage_ms[skema::ST_COUNT] = {0};
   int64_t stage_n[skema::ST_COUNT] = {0};
 };
