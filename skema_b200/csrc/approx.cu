@@ -147,164 +147,231 @@ void dgemm(skema_ctx* c, int64_t M, int64_t N, int64_t K, double alpha, const TA
 }
 
 // ----------------------------------------- tall-skinny FP64 products -------
-// G += A^T A for a tall column-major A (rows x k, ld lda) with k <= 16 TPK:
-// each CTA takes a run of rows and accumulates the whole (padded) k x k
-// product in registers (16 x 16 threads, TPK x TPK each), eight rows of A
-// at a time through shared memory, then adds it to G (column-major k x k,
-// zeroed beforehand) with one atomic per entry. The general tile kernel
-// spends most of a 64 x 64 tile on padding at these k and splits K into
-// partial sums anyway.
-template <int TPK>
-__global__ void __launch_bounds__(256)
-    gram_kernel(const double* __restrict__ A, int64_t lda, int64_t rows, int k, double* __restrict__ G,
-                int64_t rows_per_cta) {
-  constexpr int KP = 16 * TPK;
-  __shared__ double S[8][KP + 1];
-  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
-  const int64_t r0 = (int64_t)blockIdx.x * rows_per_cta, r1 = min(rows, r0 + rows_per_cta);
-  double acc[TPK][TPK];
-#pragma unroll
-  for (int i = 0; i < TPK; ++i)
-#pragma unroll
-    for (int j = 0; j < TPK; ++j) acc[i][j] = 0.0;
-  for (int64_t c0 = r0; c0 < r1; c0 += 8) {
-    for (int q = tid; q < 8 * KP; q += 256) {
-      const int rr = q & 7, col = q >> 3;
-      const int64_t row = c0 + rr;
-      S[rr][col] = (row < r1 && col < k) ? A[row + (int64_t)col * lda] : 0.0;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int rr = 0; rr < 8; ++rr) {
-      double a[TPK], b[TPK];
-#pragma unroll
-      for (int i = 0; i < TPK; ++i) a[i] = S[rr][ty + 16 * i], b[i] = S[rr][tx + 16 * i];
-#pragma unroll
-      for (int i = 0; i < TPK; ++i)
-#pragma unroll
-        for (int j = 0; j < TPK; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
-    }
-    __syncthreads();
-  }
-#pragma unroll
-  for (int i = 0; i < TPK; ++i)
-#pragma unroll
-    for (int j = 0; j < TPK; ++j) {
-      const int gi = ty + 16 * i, gj = tx + 16 * j;
-      if (gi < k && gj < k) atomicAdd(G + gi + (int64_t)gj * k, acc[i][j]);
-    }
+// Both run on the FP64 tensor cores: mma.sync m8n8k4 (D = A B + C, 8 x 4 by
+// 4 x 8). Per lane: A holds element (lane / 4, lane % 4), B element
+// (lane % 4, lane / 4), C / D elements (lane / 4, 2 (lane % 4) + i), i < 2.
+__device__ __forceinline__ void dmma(double (&d)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+               : "+d"(d[0]), "+d"(d[1])
+               : "d"(a), "d"(b));
 }
 
-// C = A B for a tall column-major A (rows x k, ld lda) and a small B (k x n2,
-// column-major ld ldb) with k, n2 <= 16 TPN: B stays in shared memory for the
-// CTA's life, A comes in blocks of 64 rows; thread (ty, tx) makes rows
-// 4 ty .. 4 ty + 3 and columns tx + 16 j of the block. C is column-major
-// (ld ldc) and written, not accumulated.
-template <int TPN>
-__global__ void __launch_bounds__(256)
-    tsm_kernel(const double* __restrict__ A, int64_t lda, int64_t rows, int k, const double* __restrict__ B,
-               int64_t ldb, int n2, double* __restrict__ C, int64_t ldc) {
-  constexpr int NP = 16 * TPN;
-  extern __shared__ double tsm_smem[];
-  double* Bs = tsm_smem;            // k x (NP + 1), row kk at kk * (NP + 1)
-  double* As = Bs + k * (NP + 1);   // k x 65, row kk at kk * 65
-  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
-  for (int q = tid; q < k * NP; q += 256) {
-    const int kk = q / NP, col = q - kk * NP;
-    Bs[kk * (NP + 1) + col] = col < n2 ? B[kk + (int64_t)col * ldb] : 0.0;
+// G += A^T A for a tall column-major A (rows x k, ld lda, k <= 128; T float
+// or double, widened to FP64 exactly). The k x k product is cut into 32 x 32
+// tiles and only the tiles on or above the diagonal are formed (6 of 9 at
+// k <= 96), each by P warps of the CTA that split the CTA's rows four at a
+// time; a warp holds its tile as 4 x 4 MMA blocks. For a step of four rows
+// the A fragment of column block c is A(r + lane % 4, c + lane / 4) and
+// the B fragment of the same block is the same value, so a tile reads its
+// two column ranges once per step. The partial tiles go to G (column-major
+// k x k, zeroed beforehand) with atomics, mirrored below the diagonal.
+template <typename T>
+__global__ void __launch_bounds__(512) gram_mma_kernel(const T* __restrict__ A, int64_t lda, int64_t rows, int k,
+                                                       double* __restrict__ G, int64_t rows_per_cta, int P) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nsb = (k + 31) >> 5;
+  const int tile = warp / P, part = warp - tile * P;
+  int ti = 0, tj = tile;  // tile -> (ti, tj), ti <= tj, row-major over the upper triangle
+  while (tj >= nsb - ti) {
+    tj -= nsb - ti;
+    ++ti;
   }
-  for (int64_t r0 = (int64_t)blockIdx.x * 64; r0 < rows; r0 += (int64_t)gridDim.x * 64) {
-    __syncthreads();
-    for (int q = tid; q < k * 64; q += 256) {
-      const int rr = q & 63, kk = q >> 6;
-      const int64_t row = r0 + rr;
-      As[kk * 65 + rr] = row < rows ? A[row + (int64_t)kk * lda] : 0.0;
-    }
-    __syncthreads();
-    double acc[4][TPN];
+  tj += ti;
+  if (ti >= nsb) return;
+  const int64_t r0 = (int64_t)blockIdx.x * rows_per_cta, r1 = min(rows, r0 + rows_per_cta);
+  const int lr = lane & 3, lc = lane >> 2;
+  const T* ci[4];
+  const T* cj[4];
+  bool vi[4], vj[4];
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
+  for (int m = 0; m < 4; ++m) {
+    const int coli = 32 * ti + 8 * m + lc, colj = 32 * tj + 8 * m + lc;
+    vi[m] = coli < k;
+    vj[m] = colj < k;
+    ci[m] = A + (int64_t)(vi[m] ? coli : 0) * lda;
+    cj[m] = A + (int64_t)(vj[m] ? colj : 0) * lda;
+  }
+  double acc[4][4][2];
 #pragma unroll
-      for (int j = 0; j < TPN; ++j) acc[i][j] = 0.0;
-    for (int kk = 0; kk < k; ++kk) {
-      double a[4], b[TPN];
+  for (int m = 0; m < 4; ++m)
 #pragma unroll
-      for (int i = 0; i < 4; ++i) a[i] = As[kk * 65 + 4 * ty + i];
+    for (int n = 0; n < 4; ++n) acc[m][n][0] = acc[m][n][1] = 0.0;
+  // two steps of four rows per iteration: their 16 loads are in flight
+  // together before the 32 MMAs that use them
+  const bool diag = ti == tj;
+  for (int64_t r = r0 + 4 * part; r < r1; r += 8 * P) {
+    double a[2][4], b[2][4];
 #pragma unroll
-      for (int j = 0; j < TPN; ++j) b[j] = Bs[kk * (NP + 1) + tx + 16 * j];
+    for (int u = 0; u < 2; ++u) {
+      const int64_t row = r + 4 * P * u + lr;
+      const bool rv = row < r1;
 #pragma unroll
-      for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < TPN; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
-    }
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const int64_t row = r0 + 4 * ty + i;
-      if (row >= rows) continue;
-#pragma unroll
-      for (int j = 0; j < TPN; ++j) {
-        const int col = tx + 16 * j;
-        if (col < n2) C[row + (int64_t)col * ldc] = acc[i][j];
+      for (int m = 0; m < 4; ++m) {
+        a[u][m] = (rv && vi[m]) ? (double)ci[m][row] : 0.0;
+        b[u][m] = (!diag && rv && vj[m]) ? (double)cj[m][row] : 0.0;
       }
     }
+#pragma unroll
+    for (int u = 0; u < 2; ++u)
+#pragma unroll
+      for (int m = 0; m < 4; ++m)
+#pragma unroll
+        for (int n = 0; n < 4; ++n) dmma(acc[m][n], a[u][m], diag ? a[u][n] : b[u][n]);
+  }
+#pragma unroll
+  for (int m = 0; m < 4; ++m)
+#pragma unroll
+    for (int n = 0; n < 4; ++n)
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        const int gi = 32 * ti + 8 * m + lc, gj = 32 * tj + 8 * n + 2 * lr + i;
+        if (gi >= k || gj >= k) continue;
+        atomicAdd(G + gi + (int64_t)gj * k, acc[m][n][i]);
+        if (ti != tj) atomicAdd(G + gj + (int64_t)gi * k, acc[m][n][i]);
+      }
+}
+
+// C = A B for a tall column-major A (rows x k, ld lda; T float or double)
+// and a small B (k x n2, column-major ld ldb, k, n2 <= 8 NB). B stays in
+// shared memory for the CTA's life as 4-row slices laid out for its MMA
+// fragments; each warp takes 16-row tiles (two MMA row blocks) of C with
+// every column block in registers. UPPER: B is upper triangular, so column
+// block nb only needs the rows of B up to its last column and the K steps
+// past it are skipped (about half the work for Q R^{-1}). C is column-major
+// (ld ldc) and written, not accumulated.
+template <typename T, int NB, bool UPPER>
+__global__ void __launch_bounds__(256) tsm_mma_kernel(const T* __restrict__ A, int64_t lda, int64_t rows, int k,
+                                                      const double* __restrict__ B, int64_t ldb, int n2,
+                                                      double* __restrict__ C, int64_t ldc) {
+  extern __shared__ double tsm_smem[];
+  // Bs[kk * ldbs + col], ldbs = 8 NB + 4 (mod 16) so a fragment's 4 x 8
+  // reads hit 16 distinct bank pairs per half-warp
+  constexpr int ldbs = (8 * NB + 15) / 16 * 16 + 4;
+  const int kp = (k + 3) & ~3;
+  for (int q = threadIdx.x; q < kp * 8 * NB; q += blockDim.x) {
+    const int kk = q / (8 * NB), col = q - kk * (8 * NB);
+    tsm_smem[kk * ldbs + col] = (kk < k && col < n2) ? B[kk + (int64_t)col * ldb] : 0.0;
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarp = blockDim.x >> 5;
+  const int lr = lane & 3, lc = lane >> 2;
+  for (int64_t r0 = ((int64_t)blockIdx.x * nwarp + warp) * 16; r0 < rows; r0 += (int64_t)gridDim.x * nwarp * 16) {
+    double acc[2][NB][2];
+#pragma unroll
+    for (int m = 0; m < 2; ++m)
+#pragma unroll
+      for (int n = 0; n < NB; ++n) acc[m][n][0] = acc[m][n][1] = 0.0;
+    const int64_t ra = r0 + lc, rb = r0 + 8 + lc;
+    const bool va = ra < rows, vb = rb < rows;
+    // eight K steps per batch: their 16 loads of A are in flight together
+    for (int kb = 0; kb < kp; kb += 32) {
+      double a0[8], a1[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const int kk = kb + 4 * j + lr;
+        const bool kv = kk < k;
+        a0[j] = (va && kv) ? (double)A[ra + (int64_t)kk * lda] : 0.0;
+        a1[j] = (vb && kv) ? (double)A[rb + (int64_t)kk * lda] : 0.0;
+      }
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const int k0 = kb + 4 * j;
+        if (k0 >= kp) break;
+        const double* bs = tsm_smem + (k0 + lr) * ldbs + lc;
+#pragma unroll
+        for (int n = 0; n < NB; ++n) {
+          if (UPPER && 8 * n + 7 < k0) continue;  // B(k0.., block n) is zero
+          const double b = bs[8 * n];
+          dmma(acc[0][n], a0[j], b);
+          dmma(acc[1][n], a1[j], b);
+        }
+      }
+    }
+#pragma unroll
+    for (int m = 0; m < 2; ++m) {
+      const int64_t row = r0 + 8 * m + lc;
+      if (row >= rows) continue;
+#pragma unroll
+      for (int n = 0; n < NB; ++n)
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+          const int col = 8 * n + 2 * lr + i;
+          if (col < n2) C[row + (int64_t)col * ldc] = acc[m][n][i];
+        }
+    }
   }
 }
 
-template <int T>
-void launch_gram(skema_ctx* c, const double* A, int64_t lda, int64_t rows, int64_t k, double* G) {
-  const int64_t ctas = std::max<int64_t>(1, std::min<int64_t>((rows + 255) / 256, 2 * (int64_t)c->sm_count));
-  const int64_t per = ((rows + ctas - 1) / ctas + 7) / 8 * 8;
-  gram_kernel<T><<<(unsigned)((rows + per - 1) / per), 256, 0, c->stream>>>(A, lda, rows, (int)k, G, per);
+template <typename T>
+void launch_gram_mma(skema_ctx* c, const T* A, int64_t lda, int64_t rows, int64_t k, double* G) {
+  const int nsb = (int)((k + 31) / 32);
+  const int tiles = nsb * (nsb + 1) / 2;
+  const int P = std::max(1, std::min(16 / tiles, 16));
+  const int64_t ctas = std::max<int64_t>(1, std::min<int64_t>((rows + 1023) / 1024, (int64_t)c->sm_count));
+  const int64_t per = ((rows + ctas - 1) / ctas + 3) / 4 * 4;
+  gram_mma_kernel<T><<<(unsigned)((rows + per - 1) / per), 32 * tiles * P, 0, c->stream>>>(A, lda, rows, (int)k, G,
+                                                                                          per, P);
   SKEMA_LAUNCHED(c);
 }
 
-template <int T>
-void launch_tsm(skema_ctx* c, const double* A, int64_t lda, int64_t rows, int64_t k, const double* B, int64_t ldb,
-                int64_t n2, double* C, int64_t ldc) {
-  const size_t smem = sizeof(double) * (size_t)(k * (16 * T + 1) + k * 65);
-  SKEMA_CUDA(cudaFuncSetAttribute(tsm_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  const int64_t blocks = (rows + 63) / 64;
-  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(blocks, 2 * (int64_t)c->sm_count));
-  tsm_kernel<T><<<grid, 256, smem, c->stream>>>(A, lda, rows, (int)k, B, ldb, (int)n2, C, ldc);
+template <typename T, int NB>
+void launch_tsm_nb(skema_ctx* c, const T* A, int64_t lda, int64_t rows, int64_t k, const double* B, int64_t ldb,
+                   int64_t n2, double* C, int64_t ldc, bool upper) {
+  constexpr int ldbs = (8 * NB + 15) / 16 * 16 + 4;
+  const size_t smem = sizeof(double) * (size_t)(((k + 3) & ~3) * ldbs);
+  auto kern = upper ? tsm_mma_kernel<T, NB, true> : tsm_mma_kernel<T, NB, false>;
+  SKEMA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int64_t tiles = (rows + 15) / 16;
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((tiles + 7) / 8, 4 * (int64_t)c->sm_count));
+  kern<<<grid, 256, smem, c->stream>>>(A, lda, rows, (int)k, B, ldb, (int)n2, C, ldc);
   SKEMA_LAUNCHED(c);
 }
 
 // G (k x k, column-major) = A^T A for column-major A (rows x k, ld lda).
+template <typename T>
+void gram_t(skema_ctx* c, const T* A, int64_t lda, int64_t rows, int64_t k, double* G) {
+  SKEMA_CUDA(cudaMemsetAsync(G, 0, sizeof(double) * (size_t)(k * k), c->stream));
+  launch_gram_mma<T>(c, A, lda, rows, k, G);
+}
 void gram(skema_ctx* c, const double* A, int64_t lda, int64_t rows, int64_t k, double* G) {
   if (k > 128) {
     dgemm<double, double>(c, k, k, rows, 1.0, A, lda, 1, A, 1, lda, 0.0, G, 1, k);
     return;
   }
-  SKEMA_CUDA(cudaMemsetAsync(G, 0, sizeof(double) * (size_t)(k * k), c->stream));
-  switch ((k + 15) / 16) {
-    case 1: launch_gram<1>(c, A, lda, rows, k, G); break;
-    case 2: launch_gram<2>(c, A, lda, rows, k, G); break;
-    case 3: launch_gram<3>(c, A, lda, rows, k, G); break;
-    case 4: launch_gram<4>(c, A, lda, rows, k, G); break;
-    case 5: launch_gram<5>(c, A, lda, rows, k, G); break;
-    case 6: launch_gram<6>(c, A, lda, rows, k, G); break;
-    case 7: launch_gram<7>(c, A, lda, rows, k, G); break;
-    default: launch_gram<8>(c, A, lda, rows, k, G); break;
-  }
+  gram_t<double>(c, A, lda, rows, k, G);
 }
 
-// C (rows x n2) = A (rows x k) B (k x n2), all column-major.
+// C (rows x n2) = A (rows x k) B (k x n2), all column-major; upper: B is
+// upper triangular (its zeros below the diagonal are not read).
+template <typename T>
+void tall_times_small_t(skema_ctx* c, const T* A, int64_t lda, int64_t rows, int64_t k, const double* B,
+                        int64_t ldb, int64_t n2, double* C, int64_t ldc, bool upper) {
+  switch ((n2 + 7) / 8) {
+    case 1: launch_tsm_nb<T, 1>(c, A, lda, rows, k, B, ldb, n2, C, ldc, upper); break;
+    case 2: launch_tsm_nb<T, 2>(c, A, lda, rows, k, B, ldb, n2, C, ldc, upper); break;
+    case 3: launch_tsm_nb<T, 3>(c, A, lda, rows, k, B, ldb, n2, C, ldc, upper); break;
+    case 4: launch_tsm_nb<T, 4>(c, A, lda, rows, k, B, ldb, n2, C, ldc, upper); break;
+    case 5: launch_tsm_nb<T, 5>(c, A, lda, rows, k, B, ldb, n2, C, ldc, upper); break;
+    case 6: launch_tsm_nb<T, 6>(c, A, lda, rows, k, B, ldb, n2, C, ldc, upper); break;
+    case 7: launch_tsm_nb<T, 7>(c, A, lda, rows, k, B, ldb, n2, C, ldc, upper); break;
+    case 8: launch_tsm_nb<T, 8>(c, A, lda, rows, k, B, ldb, n2, C, ldc, upper); break;
+    case 9: launch_tsm_nb<T, 9>(c, A, lda, rows, k, B, ldb, n2, C, ldc, upper); break;
+    case 10: launch_tsm_nb<T, 10>(c, A, lda, rows, k, B, ldb, n2, C, ldc, upper); break;
+    case 11: launch_tsm_nb<T, 11>(c, A, lda, rows, k, B, ldb, n2, C, ldc, upper); break;
+    case 12: launch_tsm_nb<T, 12>(c, A, lda, rows, k, B, ldb, n2, C, ldc, upper); break;
+    case 13: launch_tsm_nb<T, 13>(c, A, lda, rows, k, B, ldb, n2, C, ldc, upper); break;
+    case 14: launch_tsm_nb<T, 14>(c, A, lda, rows, k, B, ldb, n2, C, ldc, upper); break;
+    case 15: launch_tsm_nb<T, 15>(c, A, lda, rows, k, B, ldb, n2, C, ldc, upper); break;
+    default: launch_tsm_nb<T, 16>(c, A, lda, rows, k, B, ldb, n2, C, ldc, upper); break;
+  }
+}
 void tall_times_small(skema_ctx* c, const double* A, int64_t lda, int64_t rows, int64_t k, const double* B,
-                      int64_t ldb, int64_t n2, double* C, int64_t ldc) {
+                      int64_t ldb, int64_t n2, double* C, int64_t ldc, bool upper = false) {
   if (k > 128 || n2 > 128) {
     dgemm<double, double>(c, rows, n2, k, 1.0, A, 1, lda, B, 1, ldb, 0.0, C, 1, ldc, false);
     return;
   }
-  switch ((n2 + 15) / 16) {
-    case 1: launch_tsm<1>(c, A, lda, rows, k, B, ldb, n2, C, ldc); break;
-    case 2: launch_tsm<2>(c, A, lda, rows, k, B, ldb, n2, C, ldc); break;
-    case 3: launch_tsm<3>(c, A, lda, rows, k, B, ldb, n2, C, ldc); break;
-    case 4: launch_tsm<4>(c, A, lda, rows, k, B, ldb, n2, C, ldc); break;
-    case 5: launch_tsm<5>(c, A, lda, rows, k, B, ldb, n2, C, ldc); break;
-    case 6: launch_tsm<6>(c, A, lda, rows, k, B, ldb, n2, C, ldc); break;
-    case 7: launch_tsm<7>(c, A, lda, rows, k, B, ldb, n2, C, ldc); break;
-    default: launch_tsm<8>(c, A, lda, rows, k, B, ldb, n2, C, ldc); break;
-  }
+  tall_times_small_t<double>(c, A, lda, rows, k, B, ldb, n2, C, ldc, upper);
 }
 
 // ----------------------------------------------------- conversions ----------
@@ -684,12 +751,15 @@ __global__ void __launch_bounds__(1024) jacobi_svd_kernel_t(double* Ag, double* 
           be += __shfl_xor_sync(hmask, be, o);
           ga += __shfl_xor_sync(hmask, ga, o);
         }
-        const double den = sqrt(al * be);
-        if (den == 0.0 || fabs(ga) <= tol * den) continue;
+        // converged pair: |gamma| <= tol sqrt(alpha beta), compared squared
+        if (ga == 0.0 || ga * ga <= (tol * tol) * (al * be)) continue;
         if (hl == 0) rotated = 1;
         // tan of the rotation angle, the smaller root of t^2 + 2 zeta t - 1
-        const double zeta = (be - al) / (2.0 * ga);
-        const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(fma(zeta, zeta, 1.0)));
+        // with zeta = d / h, d = beta - alpha, h = 2 gamma, written as
+        // t = sign(d) h / (|d| + sqrt(d^2 + h^2)): one square root and one
+        // division on the chain that every round waits for
+        const double d = be - al, h = 2.0 * ga;
+        const double t = (d >= 0.0 ? h : -h) / (fabs(d) + sqrt(fma(d, d, h * h)));
         const double cs = rsqrt(fma(t, t, 1.0)), sn = cs * t;
         for (int i = hl; i < k; i += 16) {
           const double x = ap[i], y = aq[i];
@@ -723,12 +793,14 @@ __global__ void __launch_bounds__(1024) jacobi_svd_kernel_t(double* Ag, double* 
 // The SVD kernel for a k x k problem: shared memory when A and V fit.
 void jacobi_svd(skema_ctx* c, double* A, double* V, int64_t k, int max_sweeps, double tol, int* sweeps_out) {
   const size_t smem = sizeof(double) * (size_t)(2 * k * k);
+  // a half-warp per pair of a round: (k + 1) / 2 pairs, at most 64 at a time
+  const int threads = (int)std::min<int64_t>(1024, ((k + 1) / 2 * 16 + 31) / 32 * 32);
   if (smem <= 200 * 1024) {
     SKEMA_CUDA(cudaFuncSetAttribute(jacobi_svd_kernel_t<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)smem));
-    jacobi_svd_kernel_t<true><<<1, 1024, smem, c->stream>>>(A, V, k, max_sweeps, tol, sweeps_out);
+    jacobi_svd_kernel_t<true><<<1, threads, smem, c->stream>>>(A, V, k, max_sweeps, tol, sweeps_out);
   } else {
-    jacobi_svd_kernel_t<false><<<1, 1024, 0, c->stream>>>(A, V, k, max_sweeps, tol, sweeps_out);
+    jacobi_svd_kernel_t<false><<<1, threads, 0, c->stream>>>(A, V, k, max_sweeps, tol, sweeps_out);
   }
   SKEMA_LAUNCHED(c);
 }
@@ -893,7 +965,7 @@ bool cholqr_try(skema_ctx* c, double* Qm, int64_t rows, int64_t k, double* Rout,
       passes_left = 3;  // shifted pass + CholeskyQR2
     }
     // Q <- Q R^{-1} with G = R^{-1} (upper): next <- cur * Rinv (rows x k)
-    tall_times_small(c, cur, rows, rows, k, G, k, k, nxt, rows);
+    tall_times_small(c, cur, rows, rows, k, G, k, k, nxt, rows, true);
     std::swap(cur, nxt);
     // Racc <- R * Racc
     double* tmp = Rout;
