@@ -1057,6 +1057,56 @@ void orth(skema_ctx* c, double* Qm, int64_t rows, int64_t k, double* Rscratch, d
   cholqr(c, W, rows, kr, Rscratch, work, dstatus);
 }
 
+// The orthonormal basis of orth() for the FP32 sketch S (rows x k,
+// column-major ld lds), left as Qm Tout with Tout upper triangular (k x k):
+// the first CholeskyQR pass reads S itself (its products are exact in
+// FP64) and writes Qm = S R1^{-1}; the second pass only factors
+// Qm^T Qm = R2^T R2 and returns Tout = R2^{-1}, so the last product with
+// the tall matrix is folded by the caller into the small matrices it
+// multiplies the basis by anyway. When a Cholesky factor does not exist,
+// orth() makes the basis explicit in Qm from the FP64 matrix at hand and
+// Tout = I.
+void orth_lazy(skema_ctx* c, const float* S, int64_t lds, double* Qm, int64_t rows, int64_t k, double* Tout,
+               double* Rscratch, double* work, int* dstatus) {
+  double* G = work;
+  double* R = work + k * k;
+  auto factor = [&] {
+    chol_inverse(c, G, k, R, G, dstatus);
+    int st = 0;
+    SKEMA_CUDA(cudaMemcpyAsync(&st, dstatus, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    SKEMA_CUDA(cudaStreamSynchronize(c->stream));
+    return st == 0;
+  };
+  auto explicit_basis = [&] {
+    orth(c, Qm, rows, k, Rscratch, work, dstatus);
+    identity_kernel<<<g1(c, k * k), 256, 0, c->stream>>>(Tout, k);
+    SKEMA_LAUNCHED(c);
+  };
+  if (k <= 128) {
+    gram_t<float>(c, S, lds, rows, k, G);
+  } else {
+    dgemm<float, float>(c, k, k, rows, 1.0, S, lds, 1, S, 1, lds, 0.0, G, 1, k);
+  }
+  if (!factor()) {
+    f2d_kernel<<<g1(c, rows * k), 256, 0, c->stream>>>(S, 1, lds, Qm, 1, rows, rows, k);
+    SKEMA_LAUNCHED(c);
+    explicit_basis();
+    return;
+  }
+  // Qm = S R1^{-1} (G holds R1^{-1})
+  if (k <= 128) {
+    tall_times_small_t<float>(c, S, lds, rows, k, G, k, k, Qm, rows, true);
+  } else {
+    dgemm<float, double>(c, rows, k, k, 1.0, S, 1, lds, G, 1, k, 0.0, Qm, 1, rows, false);
+  }
+  gram(c, Qm, rows, rows, k, G);
+  if (!factor()) {
+    explicit_basis();
+    return;
+  }
+  SKEMA_CUDA(cudaMemcpyAsync(Tout, G, sizeof(double) * (size_t)(k * k), cudaMemcpyDeviceToDevice, c->stream));
+}
+
 // out (R x k, column-major ld R) = Map~ (R x cols) * Qm (cols x k, column-major ld cols)
 void apply_map(skema_ctx* c, const Map& mp, const double* Qm, int64_t cols, int64_t k, double* out) {
   const int64_t R = mp.lrows;
@@ -1235,7 +1285,7 @@ void low_rank_approx(skema_ctx* c, double* Uout, double* Sout, double* Vout) {
   const size_t b_q = sizeof(double) * (size_t)(m * k), b_p = sizeof(double) * (size_t)(n * k);
   const size_t b_w = sizeof(double) * cholqr_work_doubles(std::max(m, std::max(n, s)), k);
   const size_t b_u = sizeof(double) * (size_t)(s * k);
-  const size_t b_small = sizeof(double) * (size_t)(8 * k * k + s * s + k * s + 4 * k + 64);
+  const size_t b_small = sizeof(double) * (size_t)(12 * k * k + s * s + k * s + 4 * k + 64);
   Carve cv(c, {b_q, b_p, b_w, b_u, b_u, b_small, 16});
   double* Q = cv.take(b_q);
   double* P = cv.take(b_p);
@@ -1252,23 +1302,26 @@ void low_rank_approx(skema_ctx* c, double* Uout, double* Sout, double* Vout) {
   double* Sv = Vc + k * k;         // k
   double* sig = Sv + k;            // k
   double* Zd = sig + k;            // s x s
+  double* TQ = Zd + s * s;         // k x k: the basis of Y is Q TQ
+  double* TP = TQ + k * k;         // k x k: the basis of X^T is P TP
+  double* WU = TP + k * k;         // k x r
+  double* WV = WU + k * k;         // k x r
   int* st = reinterpret_cast<int*>(cv.take(16));
 
   auto orth_scope = std::make_unique<StageScope>(c, ST_A_ORTH);
-  // Q = Y (m x k, column-major, FP64); P = X^T (n x k, column-major)
-  f2d_kernel<<<g1(c, m * k), 256, 0, c->stream>>>(c->Y, 1, m, Q, 1, m, m, k);
-  SKEMA_LAUNCHED(c);
-  f2d_kernel<<<g1(c, n * k), 256, 0, c->stream>>>(c->X, 1, n, P, 1, n, n, k);
-  SKEMA_LAUNCHED(c);
   f2d_kernel<<<g1(c, s * s), 256, 0, c->stream>>>(c->Z, s, 1, Zd, 1, s, s, s);
   SKEMA_LAUNCHED(c);
-  orth(c, P, n, k, T1, W, st);  // T1 used as scratch R here
-  orth(c, Q, m, k, T1, W, st);
+  // bases of Y (m x k, column-major) and X^T (n x k: X is k x n row-major),
+  // as Q TQ and P TP
+  orth_lazy(c, c->X, n, P, n, k, TP, T1, W, st);  // T1 used as scratch R here
+  orth_lazy(c, c->Y, m, Q, m, k, TQ, T1, W, st);
   orth_scope.reset();
   auto core_scope = std::make_unique<StageScope>(c, ST_A_CORE);
-  // U1 = Phi~ Q (s x k), U2 = Psi~ P (s x k)
-  apply_map(c, c->phi, Q, m, k, U1);
-  apply_map(c, c->psi, P, n, k, U2);
+  // U1 = Phi~ Q TQ (s x k), U2 = Psi~ P TP (s x k); W holds Phi~ Q, Psi~ P
+  apply_map(c, c->phi, Q, m, k, W);
+  tall_times_small(c, W, s, s, k, TQ, k, k, U1, s, true);
+  apply_map(c, c->psi, P, n, k, W);
+  tall_times_small(c, W, s, s, k, TP, k, k, U2, s, true);
   cholqr(c, U1, s, k, T1, W, st);
   cholqr(c, U2, s, k, T2, W, st);
   // Z1 = U1^T Z (k x s); Z2 = Z1 U2 (k x k)
@@ -1294,9 +1347,15 @@ void low_rank_approx(skema_ctx* c, double* Uout, double* Sout, double* Vout) {
   }
   {
     StageScope sc(c, ST_A_VECTORS);
-    // U = Q Uc(:, 1:r), V = P Vc(:, 1:r), S = S(1:r)
-    if (Uout) tall_times_small(c, Q, m, m, k, C, k, r, Uout, m);
-    if (Vout) tall_times_small(c, P, n, n, k, Z2, k, r, Vout, n);
+    // U = Q TQ Uc(:, 1:r), V = P TP Vc(:, 1:r), S = S(1:r)
+    if (Uout) {
+      tall_times_small(c, TQ, k, k, k, C, k, r, WU, k);
+      tall_times_small(c, Q, m, m, k, WU, k, r, Uout, m);
+    }
+    if (Vout) {
+      tall_times_small(c, TP, k, k, k, Z2, k, r, WV, k);
+      tall_times_small(c, P, n, n, k, WV, k, r, Vout, n);
+    }
     if (Sout)
       SKEMA_CUDA(cudaMemcpyAsync(Sout, Sv, sizeof(double) * (size_t)r, cudaMemcpyDeviceToDevice, c->stream));
   }
