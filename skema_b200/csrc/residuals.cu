@@ -93,40 +93,6 @@ __global__ void __launch_bounds__(256)
   }
 }
 
-// A^T U for a call's CSR rows without global atomics on A^T U: CTA b owns
-// columns [b cb, (b + 1) cb) and keeps their rows of A^T U (cb x r, row-major)
-// in shared memory. It walks every row of the call (a warp per row, lanes over
-// its nonzeros), adds a U(i, :) for the nonzeros in its columns with
-// shared-memory atomics, and adds its block to A^T U at the end, plainly: no
-// other CTA owns those columns. The col array of the call is read by every
-// CTA at about the same time, from L2.
-__global__ void __launch_bounds__(1024)
-    csr_atu_colblock_kernel(const int64_t* __restrict__ rowptr, const int32_t* __restrict__ col,
-                            const float* __restrict__ val, int64_t col_offset, int64_t nrows, int64_t R0,
-                            int64_t ncol, const double* __restrict__ U, int64_t r, double* __restrict__ AtU,
-                            int64_t cb) {
-  extern __shared__ double blk[];  // cb x r
-  const int64_t c0 = (int64_t)blockIdx.x * cb, c1 = min(ncol, c0 + cb);
-  if (c0 >= c1) return;
-  for (int64_t q = threadIdx.x; q < (c1 - c0) * r; q += blockDim.x) blk[q] = 0.0;
-  __syncthreads();
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  for (int64_t i = warp; i < nrows; i += nw) {
-    const int64_t b = rowptr[i] - col_offset, e = rowptr[i + 1] - col_offset;
-    const double* urow = U + (R0 + i) * r;
-    for (int64_t p = b + lane; p < e; p += 32) {
-      const int64_t cj = col[p];
-      if (cj < c0 || cj >= c1) continue;
-      const double a = (double)val[p];
-      double* out = blk + (cj - c0) * r;
-      for (int64_t j = 0; j < r; ++j) atomicAdd(out + j, a * urow[j]);
-    }
-  }
-  __syncthreads();
-  double* dst = AtU + c0 * r;
-  for (int64_t q = threadIdx.x; q < (c1 - c0) * r; q += blockDim.x) dst[q] += blk[q];
-}
-
 __global__ void sqrt_kernel(const double* __restrict__ a, double* __restrict__ out, int64_t r) {
   for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < r; j += (int64_t)gridDim.x * blockDim.x)
     out[j] = sqrt(a[j]);
@@ -194,25 +160,13 @@ void residual_csr(skema_ctx* c, const int64_t* rowptr, const int32_t* col, const
   need_ready(c);
   const int64_t r = c->p.rank;
   const int grid = grid_of(c, (nrows * 32 + 255) / 256, 16);
-  // A^T U by column blocks held in shared memory when a block of at least
-  // 64 columns fits, so that the A V pass below adds no atomics to it
-  const size_t smem_max = 200 * 1024;
-  const int64_t cb_fit = (int64_t)(smem_max / (sizeof(double) * (size_t)r));
-  const int64_t cb = std::min<int64_t>(cb_fit, (c->n + c->sm_count - 1) / c->sm_count);
-  const bool colblock = !c->spd && cb_fit >= 64;
+  // A^T U with FP64 atomics (a kernel that owned column blocks of A^T U in
+  // shared memory had every CTA walk all rows of the call and ran 2.5x
+  // longer)
   csr_residual_kernel<<<grid, 256, 0, c->stream>>>(rowptr, col, val, col_offset, nrows, row0, c->n,
                                                    c->spd ? c->res_V : c->res_U, c->res_V, c->res_S, r,
-                                                   (c->spd || colblock) ? nullptr : c->res_AtU, c->res_sq);
+                                                   c->spd ? nullptr : c->res_AtU, c->res_sq);
   SKEMA_LAUNCHED(c);
-  if (colblock && nrows > 0) {
-    const int64_t nb = (c->n + cb - 1) / cb;
-    const size_t smem = sizeof(double) * (size_t)(cb * r);
-    SKEMA_CUDA(cudaFuncSetAttribute(csr_atu_colblock_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)smem));
-    csr_atu_colblock_kernel<<<(unsigned)nb, 1024, smem, c->stream>>>(rowptr, col, val, col_offset, nrows, row0,
-                                                                     c->n, c->res_U, r, c->res_AtU, cb);
-    SKEMA_LAUNCHED(c);
-  }
 }
 
 // Kernel rows of the Gauss RBF input, a window at a time (the window of
