@@ -353,6 +353,28 @@ void skema_dense_free(skema_dense* a);
  * written as "coordinate real general" with 17 significant digits. */
 int skema_write_crs(const char* path, const skema_crs* a);
 
+/* Rows [row0, row0 + nrows) of a binary CRS file (.bin layout above; nrows
+ * < 0: to the last row), read from their offsets without loading the rest:
+ * the header and row map, then the block's entries and values. No
+ * counterpart in the reference, whose read_matrix (src/Skema_IO.cpp:53-74)
+ * reads the whole file; it lets each rank of a row-block sharding read
+ * only its own block. out->rowptr[0] = 0; the entries of a row keep their
+ * file order (not sorted, duplicates not summed: the sketch update takes
+ * them as they are); out->ncol is the file's row count, or the block's
+ * largest column + 1 when that is larger. Free with skema_crs_free. */
+int skema_read_crs_rows(const char* path, int64_t row0, int64_t nrows, skema_crs* out);
+
+/* Rows [row0, row0 + nrows) of a matrix file (nrows < 0: to the last row)
+ * streamed into the sketches: skema_linear_update_csr / _dense over those
+ * rows of A, as the reference's driver does after read_matrix
+ * (driver/main.cpp:79-150, src/Skema_IO.cpp:8-74). A binary CRS file is read one
+ * window of rows at a time (the context's window): the next window is read
+ * and converted to FP32 on the host, into one of two pinned buffers, while
+ * the device copies and sketches the previous one. A MatrixMarket file is
+ * read whole first (its entries are in no row order), then streamed.
+ * Kernel (Gauss-RBF) contexts take their points, not a file. */
+int skema_update_from_file(skema_ctx* ctx, const char* path, int64_t row0, int64_t nrows);
+
 /* Wait for all work queued on ctx's stream. */
 int skema_synchronize(skema_ctx* ctx);
 

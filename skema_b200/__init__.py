@@ -9,6 +9,7 @@ from .sketchy import (
     SparseSignDimRedux,
     rbf_sketch_fwd,
     rbf_sketch_vjp,
+    read_crs_rows,
     read_matrix,
     sketchysvd,
     write_matrix,
@@ -22,6 +23,7 @@ __all__ = [
     "SketchySPD",
     "sketchysvd",
     "read_matrix",
+    "read_crs_rows",
     "write_matrix",
     "rbf_sketch_fwd",
     "rbf_sketch_vjp",

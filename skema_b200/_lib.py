@@ -143,6 +143,8 @@ SIGNATURES = {
     "skema_read_dense": (C.c_int, [C.c_char_p, C.POINTER(Dense)]),
     "skema_dense_free": (None, [C.POINTER(Dense)]),
     "skema_write_crs": (C.c_int, [C.c_char_p, C.POINTER(Crs)]),
+    "skema_read_crs_rows": (C.c_int, [C.c_char_p, _I64, _I64, C.POINTER(Crs)]),
+    "skema_update_from_file": (C.c_int, [_P, C.c_char_p, _I64, _I64]),
 }
 
 _lib = None

@@ -403,8 +403,6 @@ int skema_create(const skema_params* p, skema_ctx** out) {
     if (const char* v = std::getenv("SKEMA_DENSE_PIPE_SMS")) c->pipe_xt_sms = std::max(0, std::atoi(v));
     if (const char* v = std::getenv("SKEMA_DENSE_PIPE_WINDOWS")) c->pipe_windows = std::max(1, std::atoi(v));
     if (c->pipe_xt_sms >= c->sm_count) c->pipe_xt_sms = 0;
-    c->ssign_red = false;
-    if (const char* v = std::getenv("SKEMA_SSIGN_RED")) c->ssign_red = std::atoi(v) != 0;
     plan_maps(c);
     if (c->spd) {
       map_generate(c, c->omg, p->precision);

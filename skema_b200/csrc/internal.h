@@ -137,9 +137,6 @@ struct skema_ctx {
   // SKEMA_DENSE_PIPE_WINDOWS override them.
   int pipe_xt_sms = 0;
   int64_t pipe_windows = 2;
-  // CSR x SparseSign Y kernel: bins updated with shared-memory reductions
-  // (true) or loads and stores (false); SKEMA_SSIGN_RED=1|0 overrides.
-  bool ssign_red = false;
   int cc_major = 0, cc_minor = 0;
   // BF16 tensor-core form: Omega~ and Psi~ stacked as one (k+s) x n
   // row-major operand (ld_op16), Upsilon~ / Phi~ copies in Map::lowp with

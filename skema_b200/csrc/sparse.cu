@@ -144,20 +144,9 @@ __device__ __forceinline__ void ssign_apply8(uint32_t base, uint4 wv, float a) {
   }
 }
 
-// The same update with one shared-memory reduction per entry (red.shared:
-// no load, no store, duplicates of a bin applied one after another).
-__device__ __forceinline__ void ssign_red8(uint32_t base, uint4 wv, float a) {
-  const uint32_t abits = __float_as_uint(a);
-  const uint32_t e[8] = {wv.x & 0xffffu, wv.x >> 16, wv.y & 0xffffu, wv.y >> 16,
-                         wv.z & 0xffffu, wv.z >> 16, wv.w & 0xffffu, wv.w >> 16};
-#pragma unroll
-  for (int t = 0; t < 8; ++t)
-    asm volatile("red.shared.add.f32 [%0], %1;" ::"r"(base + (e[t] & 0x7f80u)),
-                 "f"(__uint_as_float(abits ^ ((e[t] << 16) & 0x80000000u)))
-                 : "memory");
-}
-
-template <int U, bool RED>
+// (A form with one red.shared.add per map entry instead of the load and
+// store measured 30 % slower: 0.170 against 0.131 ms on the 1e6 x 1e5 case.)
+template <int U>
 __global__ void __launch_bounds__(128)
     csr_ssign_y16_kernel(const int64_t* __restrict__ rowptr, const int32_t* __restrict__ col,
                          const float* __restrict__ val, int64_t col_offset, int64_t nrows,
@@ -207,12 +196,7 @@ __global__ void __launch_bounds__(128)
       load_batch(more ? p + U : nb, more ? e : ne, j2, a2);
 #pragma unroll
       for (int u = 0; u < U; ++u)
-        if ((unsigned)jj[u] < (unsigned)ncol) {
-          if (RED)
-            ssign_red8(base, ww[u], aa[u] * alpha);
-          else
-            ssign_apply8(base, ww[u], aa[u] * alpha);
-        }
+        if ((unsigned)jj[u] < (unsigned)ncol) ssign_apply8(base, ww[u], aa[u] * alpha);
 #pragma unroll
       for (int u = 0; u < U; ++u) jj[u] = j2[u], aa[u] = a2[u];
       if (!more) break;
@@ -494,7 +478,7 @@ static void launch_csr_ssign_y16(skema_ctx* c, const int64_t* rowptr, const int3
     }
   }
   const size_t smem = sizeof(float) * 32 * (size_t)k * wpb;
-  auto kern = c->ssign_red ? csr_ssign_y16_kernel<U, true> : csr_ssign_y16_kernel<U, false>;
+  auto kern = csr_ssign_y16_kernel<U>;
   SKEMA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   // ~128 KB of bins per SM; the carve-out leaves the rest of the unified
   // L1 / shared memory to L1

@@ -393,6 +393,13 @@ class _Context:
         """Stream rows [row0, row0+nrows) (default: all rows of A)."""
         self._stream(A, row0, nrows, "skema_linear_update")
 
+    def update_from_file(self, path, row0: int = 0, nrows: int | None = None):
+        """Stream rows [row0, row0+nrows) of a matrix file (.bin CRS a window
+        at a time, MatrixMarket after a whole read) into the sketches
+        (skema_update_from_file). nrows None: to the last row of the file."""
+        self._check(self.lib.skema_update_from_file(self.h, str(path).encode(), int(row0),
+                                                    -1 if nrows is None else int(nrows)))
+
     def _stream(self, A, row0, nrows, prefix):
         self._torch_inputs_ready(*(A if isinstance(A, tuple) else (A,)))
         if self.alg.kernel_func == L.KERNEL_GAUSSRBF:
@@ -712,6 +719,27 @@ def read_matrix(path, sparse: bool | None = None):
     finally:
         lib.skema_dense_free(C.byref(d))
     return out
+
+
+def read_crs_rows(path, row0: int = 0, nrows: int = -1):
+    """Rows [row0, row0 + nrows) of a binary CRS file as a scipy CSR matrix
+    (FP64; entries of a row in file order), read without the rest of the
+    file (skema_read_crs_rows). nrows < 0 reads to the last row."""
+    import scipy.sparse as sp
+
+    lib = L.load()
+    a = L.Crs()
+    st = lib.skema_read_crs_rows(str(path).encode(), int(row0), int(nrows), C.byref(a))
+    if st != L.OK:
+        raise SkemaError(st, lib.skema_last_error(None).decode())
+    try:
+        nr, nc, nnz = a.nrow, a.ncol, a.nnz
+        rp = np.ctypeslib.as_array(a.rowptr, shape=(nr + 1,)).copy()
+        col = np.ctypeslib.as_array(a.col, shape=(nnz,)).copy() if nnz else np.zeros(0, np.int32)
+        val = np.ctypeslib.as_array(a.val, shape=(nnz,)).copy() if nnz else np.zeros(0)
+    finally:
+        lib.skema_crs_free(C.byref(a))
+    return sp.csr_matrix((val, col, rp), shape=(nr, nc))
 
 
 def write_matrix(A, path):

@@ -427,16 +427,6 @@ def test_csr_imported_map_unsorted_duplicate_bins(sk):
     assert rel_fro(Y, A @ OmT) < 1e-6
 
 
-@pytest.mark.parametrize("red", ["0", "1"])
-def test_csr_sparse_sign_bin_update_forms(sk, oracle, monkeypatch, red):
-    # the Y kernel's two bin-update forms (a load and a store per map entry,
-    # or one shared-memory reduction): oracle parity, and a map with
-    # repeated bins anywhere in a column
-    monkeypatch.setenv("SKEMA_SSIGN_RED", red)
-    test_csr_parity(sk, oracle, 1)
-    test_csr_imported_map_unsorted_duplicate_bins(sk)
-
-
 # ------------------------------------------------------------- SketchySPD ----
 @pytest.mark.parametrize("kind", [0, 1])
 @pytest.mark.parametrize("issparse", [False, True])

@@ -99,3 +99,53 @@ def test_coordinate_rules(sk, tmp_path):
     with pytest.raises(sk.SkemaError) as e:
         sk.read_matrix(str(q), sparse=False)
     assert "binary" in str(e.value)
+
+
+# ------------------------------------------------- row blocks of a .bin file --
+def _csr_with_empty_rows(m, n, seed):
+    rng = np.random.default_rng(seed)
+    A = sp.random(m, n, density=0.03, format="csr", random_state=seed, dtype=np.float64)
+    A.data = rng.standard_normal(A.nnz)
+    A = A.tolil()
+    for i in range(0, m, 7):
+        A.rows[i] = []
+        A.data[i] = []
+    return A.tocsr()
+
+
+@pytest.mark.parametrize("r0,nr", [(0, 300), (0, 1), (17, 50), (299, 1), (123, 0), (250, -1), (0, -1)])
+def test_read_crs_rows_blocks_match_the_whole_file(sk, tmp_path, r0, nr):
+    # rows of a binary CRS file read from their offsets equal the same rows
+    # of the whole-file read (the file's rows are sorted, so file order is
+    # sorted order here); the layout has no column count, so the block is
+    # as wide as the file has rows unless a column is larger
+    A = _csr_with_empty_rows(300, 120, seed=4)
+    path = str(tmp_path / "a.bin")
+    sk.write_matrix(A, path)
+    whole = sk.read_matrix(path)
+    B = sk.read_crs_rows(path, r0, nr)
+    end = 300 if nr < 0 else r0 + nr
+    assert B.shape == (end - r0, 300)
+    assert np.array_equal(B.indptr, whole[r0:end].indptr)
+    assert np.array_equal(B.indices, whole[r0:end].indices)
+    assert np.array_equal(B.data, whole[r0:end].data)
+    assert (B[:, :120] != A[r0:end]).nnz == 0
+
+
+def test_read_crs_rows_rejects_bad_ranges_and_files(sk, tmp_path):
+    from skema_b200 import SkemaError
+
+    A = _csr_with_empty_rows(40, 40, seed=5)
+    path = str(tmp_path / "a.bin")
+    sk.write_matrix(A, path)
+    for r0, nr in [(-1, 3), (39, 2), (41, -1)]:
+        with pytest.raises(SkemaError):
+            sk.read_crs_rows(path, r0, nr)
+    raw = open(path, "rb").read()
+    short = str(tmp_path / "short.bin")
+    with open(short, "wb") as f:
+        f.write(raw[:-8])  # one value missing
+    with pytest.raises(SkemaError):
+        sk.read_crs_rows(short, 0, 5)
+    with pytest.raises(SkemaError):
+        sk.read_crs_rows(str(tmp_path / "missing.bin"), 0, 1)
