@@ -44,7 +44,8 @@ typedef enum {
   SKEMA_ETIMEOUT = 5,     /* a bounded device-side wait ran out             */
   SKEMA_ESTATE = 6,       /* call not valid in the context's current state  */
   SKEMA_EUNSUPPORTED = 7, /* combination not provided by this build         */
-  SKEMA_ENOKERNEL = 8     /* no CUDA device / kernel image for this device  */
+  SKEMA_ENOKERNEL = 8,    /* no CUDA device / kernel image for this device  */
+  SKEMA_ECOLLECTIVE = 9   /* the caller's all-reduce callback failed         */
 } skema_status;
 
 /* ---- enums mirroring src/Skema_Utils.hpp:38-80 ------------------------- */
@@ -173,6 +174,31 @@ int skema_linear_update_rbf(skema_ctx* ctx, const float* pts, int64_t ld,
  * overwrites it with E). */
 int skema_low_rank_approx(skema_ctx* ctx, double* U, double* S, double* V,
                           int32_t mem);
+
+/* In-place sum over all ranks of count doubles at buf (device memory of
+ * the context's device; the context's stream has finished writing it and
+ * waits for the call to return). Returns 0 on success. Every rank's call
+ * sequence is the same, so the callback is a plain all-reduce (NCCL,
+ * MPI, ...) on the caller's communicator. */
+typedef int (*skema_allreduce_fn)(double* buf, int64_t count, void* user);
+
+/* skema_low_rank_approx for a sketch sharded by contiguous row blocks, one
+ * context per rank: this context holds Y's rows [row0, row0 + nrows) and
+ * X and Z already summed over the ranks (ν-weighted as the one-process
+ * window sequence has them). No counterpart in the reference, which runs
+ * on one process; it is SketchySVD::low_rank_approx
+ * (src/Skema_SketchySVD.cpp:338-664) with its two reductions over rows
+ * made collective: the k x k Gram matrices of both CholeskyQR passes of Y
+ * and the s x k product Phi~ Q are summed with `allreduce` (three calls,
+ * each rank in the same order); everything else is the same k-sized
+ * arithmetic on every rank. U receives the block's rows of U (nrows x
+ * rank, column-major, ld nrows); S and V (n x rank) are those of the whole
+ * matrix, the same on every rank up to FP64 summation order. A sketch of
+ * rank below the range fails with SKEMA_ENOTPD on every rank (the
+ * single-context call falls back to an eigen-decomposition that needs all
+ * of Y in one place). */
+int skema_low_rank_approx_rows(skema_ctx* ctx, int64_t row0, int64_t nrows, skema_allreduce_fn allreduce,
+                               void* user, double* U, double* S, double* V, int32_t mem);
 
 /* Residual norms of a fixed-rank approximation: SketchySVD::compute_residuals
  * (src/Skema_SketchySVD.cpp:719-727) with Skema::residuals and

@@ -13,10 +13,11 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libskema_b200.so")
 
 # status codes (skema_status)
-OK, EINVAL, ENOMEM, ECUDA, ENOTPD, ETIMEOUT, ESTATE, EUNSUPPORTED, ENOKERNEL = range(9)
+OK, EINVAL, ENOMEM, ECUDA, ENOTPD, ETIMEOUT, ESTATE, EUNSUPPORTED, ENOKERNEL, ECOLLECTIVE = range(10)
 STATUS_NAMES = {
     OK: "OK", EINVAL: "EINVAL", ENOMEM: "ENOMEM", ECUDA: "ECUDA", ENOTPD: "ENOTPD",
     ETIMEOUT: "ETIMEOUT", ESTATE: "ESTATE", EUNSUPPORTED: "EUNSUPPORTED", ENOKERNEL: "ENOKERNEL",
+    ECOLLECTIVE: "ECOLLECTIVE",
 }
 MAP_GAUSS, MAP_SPARSE_SIGN = 0, 1
 KERNEL_NONE, KERNEL_GAUSSRBF = 0, 1
@@ -68,6 +69,10 @@ class Crs(C.Structure):
                 ("rowptr", C.POINTER(C.c_int64)), ("col", C.POINTER(C.c_int32)), ("val", C.POINTER(C.c_double))]
 
 
+# skema_allreduce_fn: int (*)(double* buf, int64_t count, void* user)
+ALLREDUCE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int64, C.c_void_p)
+
+
 class Dense(C.Structure):
     """``skema_dense``: a column-major matrix returned by skema_read_dense."""
 
@@ -105,6 +110,7 @@ SIGNATURES = {
     "skema_linear_update_csr": (C.c_int, [_P, _P, _P, _P, _I64, _I64, _I32]),
     "skema_linear_update_rbf": (C.c_int, [_P, _P, _I64, _I32, _I64, _I64, _I64, _I64, _I32]),
     "skema_low_rank_approx": (C.c_int, [_P, _P, _P, _P, _I32]),
+    "skema_low_rank_approx_rows": (C.c_int, [_P, _I64, _I64, _P, _P, _P, _P, _P, _I32]),
     "skema_residuals_begin": (C.c_int, [_P, _P, _P, _P, _I32]),
     "skema_residuals_update_dense": (C.c_int, [_P, _P, _I64, _I32, _I64, _I64, _I32]),
     "skema_residuals_update_csr": (C.c_int, [_P, _P, _P, _P, _I64, _I64, _I32]),

@@ -331,9 +331,13 @@ void launch_tsm_nb(skema_ctx* c, const T* A, int64_t lda, int64_t rows, int64_t 
 template <typename T>
 void gram_t(skema_ctx* c, const T* A, int64_t lda, int64_t rows, int64_t k, double* G) {
   SKEMA_CUDA(cudaMemsetAsync(G, 0, sizeof(double) * (size_t)(k * k), c->stream));
-  launch_gram_mma<T>(c, A, lda, rows, k, G);
+  if (rows > 0) launch_gram_mma<T>(c, A, lda, rows, k, G);
 }
 void gram(skema_ctx* c, const double* A, int64_t lda, int64_t rows, int64_t k, double* G) {
+  if (rows <= 0) {  // an empty row block (a rank without rows) adds nothing
+    SKEMA_CUDA(cudaMemsetAsync(G, 0, sizeof(double) * (size_t)(k * k), c->stream));
+    return;
+  }
   if (k > 128) {
     dgemm<double, double>(c, k, k, rows, 1.0, A, lda, 1, A, 1, lda, 0.0, G, 1, k);
     return;
@@ -367,6 +371,7 @@ void tall_times_small_t(skema_ctx* c, const T* A, int64_t lda, int64_t rows, int
 }
 void tall_times_small(skema_ctx* c, const double* A, int64_t lda, int64_t rows, int64_t k, const double* B,
                       int64_t ldb, int64_t n2, double* C, int64_t ldc, bool upper = false) {
+  if (rows <= 0 || n2 <= 0) return;
   if (k > 128 || n2 > 128) {
     dgemm<double, double>(c, rows, n2, k, 1.0, A, 1, lda, B, 1, ldb, 0.0, C, 1, ldc, false);
     return;
@@ -630,14 +635,18 @@ __global__ void trace_kernel(const double* G, int64_t k, double* out) {
 // row); Q is m x k column-major (ldq), out R x k column-major (ldo).
 __global__ void rowsparse_apply_kernel(const uint32_t* __restrict__ mp, int zeta, int64_t R,
                                        const double* __restrict__ Q, int64_t ldq, int64_t k,
-                                       double* __restrict__ out, int64_t ldo) {
+                                       double* __restrict__ out, int64_t ldo, int64_t q0, int64_t qrows) {
+  // Q holds rows [q0, q0 + qrows) of the operand; map entries elsewhere
+  // belong to other row blocks
   for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < R * k;
        q += (int64_t)gridDim.x * blockDim.x) {
     const int64_t r = q % R, j = q / R;
     double a = 0.0;
     for (int t = 0; t < zeta; ++t) {
       const uint32_t w = mp[r * zeta + t];
-      const double v = Q[(int64_t)(w & 0x7fffffffu) + j * ldq];
+      const int64_t row = (int64_t)(w & 0x7fffffffu) - q0;
+      if ((uint64_t)row >= (uint64_t)qrows) continue;
+      const double v = Q[row + j * ldq];
       a += (w >> 31) ? -v : v;
     }
     out[r + j * ldo] = a;
@@ -1057,6 +1066,20 @@ void orth(skema_ctx* c, double* Qm, int64_t rows, int64_t k, double* Rscratch, d
   cholqr(c, W, rows, kr, Rscratch, work, dstatus);
 }
 
+// In-place sum over the ranks of a row-block sharded sketch (device
+// memory, after the context's stream has finished writing it), through the
+// caller's all-reduce; nothing for a single context.
+struct RankSum {
+  skema_allreduce_fn fn = nullptr;
+  void* user = nullptr;
+  bool on() const { return fn != nullptr; }
+  void operator()(skema_ctx* c, double* buf, int64_t count) const {
+    if (!fn) return;
+    SKEMA_CUDA(cudaStreamSynchronize(c->stream));
+    if (fn(buf, count, user) != 0) fail(SKEMA_ECOLLECTIVE, "the all-reduce callback reported a failure");
+  }
+};
+
 // The orthonormal basis of orth() for the FP32 sketch S (rows x k,
 // column-major ld lds), left as Qm Tout with Tout upper triangular (k x k):
 // the first CholeskyQR pass reads S itself (its products are exact in
@@ -1065,9 +1088,13 @@ void orth(skema_ctx* c, double* Qm, int64_t rows, int64_t k, double* Rscratch, d
 // the tall matrix is folded by the caller into the small matrices it
 // multiplies the basis by anyway. When a Cholesky factor does not exist,
 // orth() makes the basis explicit in Qm from the FP64 matrix at hand and
-// Tout = I.
+// Tout = I. With a rank sum, S is this rank's row block of a sharded
+// sketch: both Gram matrices are summed over the ranks before their
+// Cholesky, Qm is the block's rows of the basis, and a missing factor
+// fails (SKEMA_ENOTPD) on every rank alike, since the explicit fallback
+// needs the whole matrix.
 void orth_lazy(skema_ctx* c, const float* S, int64_t lds, double* Qm, int64_t rows, int64_t k, double* Tout,
-               double* Rscratch, double* work, int* dstatus) {
+               double* Rscratch, double* work, int* dstatus, const RankSum& rsum = RankSum{}) {
   double* G = work;
   double* R = work + k * k;
   auto factor = [&] {
@@ -1078,15 +1105,18 @@ void orth_lazy(skema_ctx* c, const float* S, int64_t lds, double* Qm, int64_t ro
     return st == 0;
   };
   auto explicit_basis = [&] {
+    if (rsum.on())
+      fail(SKEMA_ENOTPD, "the sharded sketch is rank deficient: CholeskyQR needs full column rank");
     orth(c, Qm, rows, k, Rscratch, work, dstatus);
     identity_kernel<<<g1(c, k * k), 256, 0, c->stream>>>(Tout, k);
     SKEMA_LAUNCHED(c);
   };
-  if (k <= 128) {
+  if (k <= 128 || rows <= 0) {
     gram_t<float>(c, S, lds, rows, k, G);
   } else {
     dgemm<float, float>(c, k, k, rows, 1.0, S, lds, 1, S, 1, lds, 0.0, G, 1, k);
   }
+  rsum(c, G, k * k);
   if (!factor()) {
     f2d_kernel<<<g1(c, rows * k), 256, 0, c->stream>>>(S, 1, lds, Qm, 1, rows, rows, k);
     SKEMA_LAUNCHED(c);
@@ -1094,12 +1124,14 @@ void orth_lazy(skema_ctx* c, const float* S, int64_t lds, double* Qm, int64_t ro
     return;
   }
   // Qm = S R1^{-1} (G holds R1^{-1})
-  if (k <= 128) {
+  if (rows <= 0) {
+  } else if (k <= 128) {
     tall_times_small_t<float>(c, S, lds, rows, k, G, k, k, Qm, rows, true);
   } else {
     dgemm<float, double>(c, rows, k, k, 1.0, S, 1, lds, G, 1, k, 0.0, Qm, 1, rows, false);
   }
   gram(c, Qm, rows, rows, k, G);
+  rsum(c, G, k * k);
   if (!factor()) {
     explicit_basis();
     return;
@@ -1108,30 +1140,43 @@ void orth_lazy(skema_ctx* c, const float* S, int64_t lds, double* Qm, int64_t ro
 }
 
 // out (R x k, column-major ld R) = Map~ (R x cols) * Qm (cols x k, column-major ld cols)
-void apply_map(skema_ctx* c, const Map& mp, const double* Qm, int64_t cols, int64_t k, double* out) {
+// out (R x k, column-major) = M Q for the map's logical R x cols matrix M
+// and rows [q0, q0 + qrows) of Q held in Qm (column-major, ld qrows): the
+// block's share of M Q, which sums over the row blocks to the whole.
+void apply_map_rows(skema_ctx* c, const Map& mp, const double* Qm, int64_t q0, int64_t qrows, int64_t k,
+                    double* out) {
   const int64_t R = mp.lrows;
+  if (qrows <= 0) {
+    SKEMA_CUDA(cudaMemsetAsync(out, 0, sizeof(double) * (size_t)(R * k), c->stream));
+    return;
+  }
   if (mp.kind == SKEMA_MAP_GAUSS) {
-    dgemm<float, double>(c, R, k, cols, 1.0, mp.f32, mp.rs, mp.cs, Qm, 1, cols, 0.0, out, 1, R);
+    dgemm<float, double>(c, R, k, qrows, 1.0, mp.f32 + q0 * mp.cs, mp.rs, mp.cs, Qm, 1, qrows, 0.0, out, 1, R);
     return;
   }
   if (!mp.transposed) {
-    rowsparse_apply_kernel<<<g1(c, R * k), 256, 0, c->stream>>>(mp.packed, mp.zeta, R, Qm, cols, k,
-                                                                 out, R);
+    rowsparse_apply_kernel<<<g1(c, R * k), 256, 0, c->stream>>>(mp.packed, mp.zeta, R, Qm, qrows, k, out, R, q0,
+                                                                 qrows);
     SKEMA_LAUNCHED(c);
   } else {
+    // stored rows are the operand's rows: the block's stored rows only
+    const uint32_t* mpb = mp.packed + q0 * mp.zeta;
     SKEMA_CUDA(cudaMemsetAsync(out, 0, sizeof(double) * (size_t)(R * k), c->stream));
     const size_t priv = sizeof(double) * (size_t)(R * k);
     if (priv <= 200 * 1024) {
       SKEMA_CUDA(cudaFuncSetAttribute(colsparse_apply_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)priv));
-      colsparse_apply_smem_kernel<<<c->sm_count, 1024, priv, c->stream>>>(mp.packed, mp.zeta, cols, Qm, cols, k,
-                                                                            out, R, R);
+      colsparse_apply_smem_kernel<<<c->sm_count, 1024, priv, c->stream>>>(mpb, mp.zeta, qrows, Qm, qrows, k, out,
+                                                                            R, R);
     } else {
-      colsparse_apply_kernel<<<g1(c, cols * k), 256, 0, c->stream>>>(mp.packed, mp.zeta, cols, Qm, cols, k, out,
-                                                                      R);
+      colsparse_apply_kernel<<<g1(c, qrows * k), 256, 0, c->stream>>>(mpb, mp.zeta, qrows, Qm, qrows, k, out, R);
     }
     SKEMA_LAUNCHED(c);
   }
+}
+
+void apply_map(skema_ctx* c, const Map& mp, const double* Qm, int64_t cols, int64_t k, double* out) {
+  apply_map_rows(c, mp, Qm, 0, cols, k, out);
 }
 
 // ---- SketchySPD pieces -----------------------------------------------------
@@ -1279,8 +1324,13 @@ void dgemm_f32_f64(skema_ctx* c, int64_t M, int64_t N, int64_t K, double alpha, 
   dgemm<float, double>(c, M, N, K, alpha, A, ars, acs, B, brs, bcs, beta, C, crs, ccs);
 }
 
-void low_rank_approx(skema_ctx* c, double* Uout, double* Sout, double* Vout) {
-  const int64_t m = c->m, n = c->n, k = c->k, s = c->s, r = c->p.rank;
+// The fixed-rank approximation from Y's rows [row0, row0 + nrows) with
+// the sums over row blocks taken by rsum (a row-block sharded sketch whose
+// X and Z are already summed), or from all of Y (rsum off, the whole
+// range). U (nrows x rank, column-major ld nrows) gets the block's rows.
+void low_rank_approx_rows(skema_ctx* c, int64_t row0, int64_t nrows, const RankSum& rsum, double* Uout,
+                          double* Sout, double* Vout) {
+  const int64_t m = nrows, n = c->n, k = c->k, s = c->s, r = c->p.rank;
   y_materialize(c);
   const size_t b_q = sizeof(double) * (size_t)(m * k), b_p = sizeof(double) * (size_t)(n * k);
   const size_t b_w = sizeof(double) * cholqr_work_doubles(std::max(m, std::max(n, s)), k);
@@ -1314,11 +1364,12 @@ void low_rank_approx(skema_ctx* c, double* Uout, double* Sout, double* Vout) {
   // bases of Y (m x k, column-major) and X^T (n x k: X is k x n row-major),
   // as Q TQ and P TP
   orth_lazy(c, c->X, n, P, n, k, TP, T1, W, st);  // T1 used as scratch R here
-  orth_lazy(c, c->Y, m, Q, m, k, TQ, T1, W, st);
+  orth_lazy(c, c->Y + row0, c->m, Q, m, k, TQ, T1, W, st, rsum);
   orth_scope.reset();
   auto core_scope = std::make_unique<StageScope>(c, ST_A_CORE);
   // U1 = Phi~ Q TQ (s x k), U2 = Psi~ P TP (s x k); W holds Phi~ Q, Psi~ P
-  apply_map(c, c->phi, Q, m, k, W);
+  apply_map_rows(c, c->phi, Q, row0, m, k, W);
+  rsum(c, W, s * k);
   tall_times_small(c, W, s, s, k, TQ, k, k, U1, s, true);
   apply_map(c, c->psi, P, n, k, W);
   tall_times_small(c, W, s, s, k, TP, k, k, U2, s, true);
@@ -1363,6 +1414,18 @@ void low_rank_approx(skema_ctx* c, double* Uout, double* Sout, double* Vout) {
   SKEMA_CUDA(cudaMemcpyAsync(&sweeps, st + 1, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   SKEMA_CUDA(cudaStreamSynchronize(c->stream));
   c->svd_sweeps = sweeps;
+}
+
+void low_rank_approx(skema_ctx* c, double* Uout, double* Sout, double* Vout) {
+  low_rank_approx_rows(c, 0, c->m, RankSum{}, Uout, Sout, Vout);
+}
+
+void low_rank_approx_sharded(skema_ctx* c, int64_t row0, int64_t nrows, skema_allreduce_fn fn, void* user,
+                             double* Uout, double* Sout, double* Vout) {
+  RankSum rs;
+  rs.fn = fn;
+  rs.user = user;
+  low_rank_approx_rows(c, row0, nrows, rs, Uout, Sout, Vout);
 }
 
 }  // namespace skema

@@ -584,6 +584,35 @@ int skema_linear_update_rbf(skema_ctx* c, const float* pts, int64_t ld, int32_t 
   });
 }
 
+int skema_low_rank_approx_rows(skema_ctx* c, int64_t row0, int64_t nrows, skema_allreduce_fn allreduce,
+                               void* user, double* U, double* S, double* V, int32_t mem) {
+  return guarded(c, [&] {
+    if (mem != SKEMA_MEM_DEVICE && mem != SKEMA_MEM_HOST) fail(SKEMA_EINVAL, "bad mem kind");
+    if (c->spd) fail(SKEMA_EUNSUPPORTED, "SketchySPD contexts take skema_low_rank_approx");
+    if (!allreduce) fail(SKEMA_EINVAL, "null all-reduce callback");
+    if (row0 < 0 || nrows < 0 || row0 + nrows > c->m) fail(SKEMA_EINVAL, "row range outside A");
+    if (c->k > c->n || c->k > c->m) fail(SKEMA_EINVAL, "range must not exceed min(m, n)");
+    if (c->s < c->k) fail(SKEMA_EINVAL, "core must be >= range");
+    const int64_t r = c->p.rank;
+    if (r > c->k) fail(SKEMA_EINVAL, "rank must not exceed range");
+    check_device_error(c);
+    if (mem == SKEMA_MEM_DEVICE) {
+      low_rank_approx_sharded(c, row0, nrows, allreduce, user, U, S, V);
+      return;
+    }
+    const size_t ub = sizeof(double) * (size_t)(nrows * r), vb = sizeof(double) * (size_t)(c->n * r);
+    char* buf = (char*)staging(c, ub + vb + sizeof(double) * (size_t)r + 512);
+    double* dU = (double*)buf;
+    double* dV = (double*)(buf + (ub + 255) / 256 * 256);
+    double* dS = (double*)(buf + (ub + 255) / 256 * 256 + (vb + 255) / 256 * 256);
+    low_rank_approx_sharded(c, row0, nrows, allreduce, user, U ? dU : nullptr, S ? dS : nullptr, V ? dV : nullptr);
+    if (U && ub) SKEMA_CUDA(cudaMemcpyAsync(U, dU, ub, cudaMemcpyDeviceToHost, c->stream));
+    if (V) SKEMA_CUDA(cudaMemcpyAsync(V, dV, vb, cudaMemcpyDeviceToHost, c->stream));
+    if (S) SKEMA_CUDA(cudaMemcpyAsync(S, dS, sizeof(double) * (size_t)r, cudaMemcpyDeviceToHost, c->stream));
+    SKEMA_CUDA(cudaStreamSynchronize(c->stream));
+  });
+}
+
 int skema_low_rank_approx(skema_ctx* c, double* U, double* S, double* V, int32_t mem) {
   return guarded(c, [&] {
     if (mem != SKEMA_MEM_DEVICE && mem != SKEMA_MEM_HOST) fail(SKEMA_EINVAL, "bad mem kind");

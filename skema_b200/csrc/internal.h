@@ -290,6 +290,10 @@ void rbf_vjp(skema_ctx* c, const float* pts, int64_t N, int64_t d,
 
 // ---- FP64 approximation (approx.cu) ----
 void low_rank_approx(skema_ctx* c, double* U, double* S, double* V);
+// Rows [row0, row0 + nrows) of a row-block sharded sketch, sums over the
+// ranks through fn (skema_low_rank_approx_rows).
+void low_rank_approx_sharded(skema_ctx* c, int64_t row0, int64_t nrows, skema_allreduce_fn fn, void* user,
+                             double* U, double* S, double* V);
 // SketchySPD: U (m x rank, column-major) and S (rank), device pointers (either may be NULL).
 void spd_low_rank_approx(skema_ctx* c, double* U, double* S);
 // C = alpha A B + beta C in FP64 (A FP32, exact in FP64), strided operands.

@@ -49,3 +49,37 @@ def reduce_partial_sketches(X, Z, m: int, window: int, nu: float, group=None) ->
         Z.mul_(w)
     dist.all_reduce(X, group=group)
     dist.all_reduce(Z, group=group)
+
+
+class _DeviceBuffer:
+    """A CUDA array interface over count FP64 values at a device pointer,
+    so that torch can view the library's buffer without a copy."""
+
+    def __init__(self, ptr: int, count: int):
+        self.__cuda_array_interface__ = {"shape": (count,), "typestr": "<f8", "data": (ptr, False),
+                                         "version": 3, "strides": None}
+
+
+def device_allreduce(group=None):
+    """allreduce(ptr, count) for SketchySVD.low_rank_approx_rows: sums
+    count FP64 values at a device pointer over the process group with
+    torch.distributed (NCCL) and waits for the sum before returning."""
+    import torch
+    import torch.distributed as dist
+
+    def allreduce(ptr: int, count: int) -> None:
+        t = torch.as_tensor(_DeviceBuffer(ptr, count), device="cuda")
+        dist.all_reduce(t, group=group)
+        torch.cuda.current_stream().synchronize()
+
+    return allreduce
+
+
+def low_rank_approx_sharded(ctx, m: int, window: int, group=None):
+    """The fixed-rank approximation of a row-block sharded sketch: this
+    rank's rows of U, and S, V of the whole matrix. X and Z must already be
+    summed over the ranks (reduce_partial_sketches). Every rank calls it."""
+    import torch.distributed as dist
+
+    row0, nrows = shard_rows(m, dist.get_world_size(group), dist.get_rank(group), window)
+    return ctx.low_rank_approx_rows(row0, nrows, device_allreduce(group))

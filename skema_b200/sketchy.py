@@ -646,6 +646,35 @@ class SketchySVD(_Context):
         self.uvecs, self.svals, self.vvecs = U.T, S, V.T
         return U.T, S, V.T
 
+    def low_rank_approx_rows(self, row0: int, nrows: int, allreduce):
+        """low_rank_approx of a sketch sharded by row blocks
+        (skema_low_rank_approx_rows): this context holds Y's rows [row0,
+        row0 + nrows) and X, Z summed over the ranks. allreduce(ptr, count)
+        sums count FP64 values at the device pointer ptr over the ranks in
+        place (it is called three times, in the same order on every rank).
+        Returns (U rows of the block, S, V) as numpy arrays."""
+        err = []
+
+        def cb(ptr, count, _user):
+            try:
+                allreduce(int(ptr), int(count))
+                return 0
+            except BaseException as e:  # reported as SKEMA_ECOLLECTIVE
+                err.append(e)
+                return 1
+
+        fn = L.ALLREDUCE_FN(cb)
+        r = self.rank
+        U = np.empty((r, max(nrows, 0)), dtype=np.float64)
+        V = np.empty((r, self.ncol), dtype=np.float64)
+        S = np.empty(r, dtype=np.float64)
+        st = self.lib.skema_low_rank_approx_rows(self.h, int(row0), int(nrows), C.cast(fn, C.c_void_p), None,
+                                                 U.ctypes.data, S.ctypes.data, V.ctypes.data, L.MEM_HOST)
+        if st != L.OK and err:
+            raise SkemaError(st, f"all-reduce callback: {err[0]!r}") from err[0]
+        self._check(st)
+        return U.T, S, V.T
+
 
 class SketchySPD(_Context):
     """SketchySPD<MatrixType, DimReduxT> (src/Skema_SketchySVD.hpp:67-108)."""
