@@ -567,13 +567,19 @@ def run_gpu(args, cfg, peaks, peak_kind):
         a1e = torch.cuda.Event(enable_timing=True)
         ctx.low_rank_approx(device_out=(Ud, Sd, Vd))  # warm
         torch.cuda.synchronize()
+        ctx.timing_enable(True)
         a0e.record(stream)
         ctx.low_rank_approx(device_out=(Ud, Sd, Vd))
         a1e.record(stream)
         torch.cuda.synchronize()
+        astages = {name: round(ctx.timing_get(name)[0], 3)
+                   for name in ("approx.orth", "approx.core", "approx.svd", "approx.vectors")}
+        sweeps = ctx.timing_get("approx.svd_sweeps")[1]
+        ctx.timing_enable(False)
         t0 = time.perf_counter()
         U, S, V = ctx.low_rank_approx()
         approx = {"ms": a0e.elapsed_time(a1e), "timer": "CUDA events, outputs in device memory",
+                  "stages_ms": astages, "core_svd_sweeps": sweeps,
                   "ms_with_host_copy": (time.perf_counter() - t0) * 1e3}
         r0e = torch.cuda.Event(enable_timing=True)
         r1e = torch.cuda.Event(enable_timing=True)
