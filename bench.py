@@ -1079,6 +1079,49 @@ SECONDARY = (("dense-fp32", 3), ("dense-bf16", 10), ("dense-fp8", 10), ("rbf-fp3
              ("rbf-vjp", 3), ("rbf-vjp-bf16", 10))
 
 
+def cublas_fp32_dense_ms(cfg, reps=3):
+    """ms per step of the dense FP32 sketch's products done by cuBLAS SGEMM
+    (torch.matmul in FP32, TF32 off) on the same shapes: per window of W rows
+    [Y_w | T] = A_w [Omega; Psi]^T, X += Upsilon_w A_w and Z += Phi_w T,
+    over the m / W windows of one step. A yardstick for the plain FP32 form
+    (the library's own SIMT GEMM), not a product path."""
+    import torch
+
+    dev = torch.device("cuda", 0)
+    m, n, k, s, W = cfg["m"], cfg["n"], cfg["k"], cfg["s"], cfg["window"]
+    g = torch.Generator(device=dev)
+    g.manual_seed(1)
+    A = torch.randn(W, n, generator=g, device=dev)
+    OP = torch.randn(n, k + s, generator=g, device=dev)
+    Ups = torch.randn(k, W, generator=g, device=dev)
+    Phi = torch.randn(s, W, generator=g, device=dev)
+    X = torch.zeros(k, n, device=dev)
+    Z = torch.zeros(s, s, device=dev)
+    prev = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    try:
+        def window():
+            YT = A @ OP
+            X.addmm_(Ups, A)
+            Z.addmm_(Phi, YT[:, k:])
+
+        for _ in range(2):
+            window()
+        nwin = (m + W - 1) // W
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(reps * nwin):
+            window()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+    finally:
+        torch.backends.cuda.matmul.allow_tf32 = prev
+        del A, OP, Ups, Phi, X, Z
+        torch.cuda.empty_cache()
+
+
 def run_secondary(args, peaks, peak_kind):
     import torch
 
@@ -1107,6 +1150,12 @@ def run_secondary(args, peaks, peak_kind):
                        "rbf_bf16_over_fp32": sp("rbf-fp32", "rbf-bf16"),
                        "vjp_bf16_over_fp32": sp("rbf-vjp", "rbf-vjp-bf16"),
                        "note": "ms per step of the plain FP32 form over the precision form, same input"}
+    # the same dense products by cuBLAS SGEMM, for the scale of the plain form
+    cb = cublas_fp32_dense_ms(dict(WORKLOADS["dense-fp32"]))
+    res["cublas_fp32_dense"] = {"ms_per_step": cb, "over_library_fp32": res["dense-fp32"]["ms_per_step"] / cb,
+                                "dense_bf16_speedup_over_it": cb / res["dense-bf16"]["ms_per_step"],
+                                "note": "cuBLAS SGEMM (TF32 off) on the dense-fp32 products and shapes, "
+                                        "a yardstick, not a product path"}
     return res
 
 
