@@ -403,6 +403,10 @@ int skema_create(const skema_params* p, skema_ctx** out) {
     if (const char* v = std::getenv("SKEMA_DENSE_PIPE_SMS")) c->pipe_xt_sms = std::max(0, std::atoi(v));
     if (const char* v = std::getenv("SKEMA_DENSE_PIPE_WINDOWS")) c->pipe_windows = std::max(1, std::atoi(v));
     if (c->pipe_xt_sms >= c->sm_count) c->pipe_xt_sms = 0;
+    c->ssign_bin_kb = 128;
+    if (const char* v = std::getenv("SKEMA_SSIGN_BIN_KB")) c->ssign_bin_kb = std::min(220, std::max(16, std::atoi(v)));
+    c->ssign_batch = 4;
+    if (const char* v = std::getenv("SKEMA_SSIGN_BATCH")) c->ssign_batch = std::atoi(v);
     plan_maps(c);
     if (c->spd) {
       map_generate(c, c->omg, p->precision);

@@ -137,6 +137,13 @@ struct skema_ctx {
   // SKEMA_DENSE_PIPE_WINDOWS override them.
   int pipe_xt_sms = 0;
   int64_t pipe_windows = 2;
+  // Shared memory per SM for the CSR x SparseSign Y kernel's bins, in KB
+  // (it sets the warps per SM; the rest of the unified L1 / shared memory
+  // stays L1). SKEMA_SSIGN_BIN_KB overrides the default.
+  int ssign_bin_kb = 128;
+  // Nonzeros each lane of that kernel loads ahead per step (2, 4, 6 or 8);
+  // SKEMA_SSIGN_BATCH overrides the default.
+  int ssign_batch = 4;
   int cc_major = 0, cc_minor = 0;
   // BF16 tensor-core form: Omega~ and Psi~ stacked as one (k+s) x n
   // row-major operand (ld_op16), Upsilon~ / Phi~ copies in Map::lowp with

@@ -465,26 +465,27 @@ static void launch_csr_ssign_y16(skema_ctx* c, const int64_t* rowptr, const int3
                                  int64_t col_offset, int64_t nrows, const Map& O, float* Y, int64_t ldy, float alpha,
                                  float beta) {
   const int k = (int)c->k;
-  // warps per block: the most warps within about 128 KB of bins per SM,
-  // in the fewest blocks (k = 81: 4 x 3 = 12 warps; k = 161: 2 x 3 = 6;
-  // k = 256: 4 x 1)
+  // warps per block: the most warps within the bin budget per SM (about
+  // 128 KB), in the fewest blocks (k = 81: 4 x 3 = 12 warps; k = 161:
+  // 2 x 3 = 6; k = 256: 4 x 1)
+  const size_t budget = (size_t)c->ssign_bin_kb * 1024;
   int wpb = 1;
   {
     const size_t per_warp = sizeof(float) * 32 * (size_t)k;
     int best = 0;
     for (int w = 4; w >= 1; w >>= 1) {
-      const int warps = w * (int)((size_t)(128 * 1024) / (per_warp * w));
+      const int warps = w * (int)(budget / (per_warp * w));
       if (warps > best) best = warps, wpb = w;
     }
   }
   const size_t smem = sizeof(float) * 32 * (size_t)k * wpb;
   auto kern = csr_ssign_y16_kernel<U>;
   SKEMA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  // ~128 KB of bins per SM; the carve-out leaves the rest of the unified
+  // the bin budget per SM; the carve-out leaves the rest of the unified
   // L1 / shared memory to L1
   int smem_sm = 0;
   SKEMA_CUDA(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, c->dev));
-  const int per_sm = (int)std::max<size_t>(1, (size_t)(128 * 1024) / smem);
+  const int per_sm = (int)std::max<size_t>(1, budget / smem);
   const int carve = (int)std::min<size_t>(100, (per_sm * (smem + 1024) * 100 + smem_sm - 1) / std::max(1, smem_sm) + 2);
   SKEMA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, carve));
   const int64_t tiles = (nrows + 31) / 32;
@@ -499,7 +500,12 @@ static void launch_csr_ssign_y(skema_ctx* c, const int64_t* rowptr, const int32_
                                const float* val, int64_t col_offset, int64_t nrows, const Map& O,
                                float* Y, int64_t ldy, float alpha, float beta) {
   if (O.packed16) {  // zeta = 8, k <= 256: at most 32 KB of bins per warp
-    launch_csr_ssign_y16<4>(c, rowptr, col, val, col_offset, nrows, O, Y, ldy, alpha, beta);
+    switch (c->ssign_batch) {
+      case 2: launch_csr_ssign_y16<2>(c, rowptr, col, val, col_offset, nrows, O, Y, ldy, alpha, beta); break;
+      case 6: launch_csr_ssign_y16<6>(c, rowptr, col, val, col_offset, nrows, O, Y, ldy, alpha, beta); break;
+      case 8: launch_csr_ssign_y16<8>(c, rowptr, col, val, col_offset, nrows, O, Y, ldy, alpha, beta); break;
+      default: launch_csr_ssign_y16<4>(c, rowptr, col, val, col_offset, nrows, O, Y, ldy, alpha, beta); break;
+    }
     return;
   }
   // general form: up to 4 warps within 96 KB of bins per block; one warp's
