@@ -321,10 +321,9 @@ void launch_gemm(skema_ctx* c, const CUtensorMap& ta, const CUtensorMap& tb, int
 }
 
 // X^T product straight from the FP32 window (converts it and writes A16).
-template <bool AROW>
-void launch_gemm_a32(skema_ctx* c, const CUtensorMap& ta32, const CUtensorMap& tb, const CUtensorMap& ta16,
-                     int64_t M, int64_t N, int64_t K, Plan pl, const tc::OutSpec& o, uint32_t* amax) {
-  constexpr int S1 = 3, S2 = 3;
+template <bool AROW, int S1, int S2>
+void launch_gemm_a32_s(skema_ctx* c, const CUtensorMap& ta32, const CUtensorMap& tb, const CUtensorMap& ta16,
+                       int64_t M, int64_t N, int64_t K, Plan pl, const tc::OutSpec& o, uint32_t* amax) {
   constexpr uint32_t STAGE = ((tc::BM * tc::BK * 2 + kNT * tc::BK * 2 + 1023) / 1024) * 1024;
   const size_t smem = (size_t)S1 * tc::BM * tc::BK * 4 + (size_t)S2 * STAGE + 1024 + 256;
   auto kern = amax ? tc::gemm_a32_kernel<kNT, S1, S2, AROW, true> : tc::gemm_a32_kernel<kNT, S1, S2, AROW, false>;
@@ -335,6 +334,17 @@ void launch_gemm_a32(skema_ctx* c, const CUtensorMap& ta32, const CUtensorMap& t
   kern<<<grid, tc::kThreadsA32, smem, c->stream>>>(ta32, tb, ta16, g, o, amax, c->dev_err);
   SKEMA_LAUNCHED(c);
   c->dev_err_armed = true;
+}
+
+// FP32 / BF16 stage counts of the X^T product (228 KB of shared memory at
+// 3 + 3 or 4 + 2)
+template <bool AROW>
+void launch_gemm_a32(skema_ctx* c, const CUtensorMap& ta32, const CUtensorMap& tb, const CUtensorMap& ta16,
+                     int64_t M, int64_t N, int64_t K, Plan pl, const tc::OutSpec& o, uint32_t* amax) {
+  if (c->xt_stages == 42)
+    launch_gemm_a32_s<AROW, 4, 2>(c, ta32, tb, ta16, M, N, K, pl, o, amax);
+  else
+    launch_gemm_a32_s<AROW, 3, 3>(c, ta32, tb, ta16, M, N, K, pl, o, amax);
 }
 
 // ---- FP8 form -------------------------------------------------------------

@@ -666,13 +666,17 @@ __global__ void __launch_bounds__(kThreads, 1)
 //                 two 128-byte-swizzled boxes {32 rows, 128 columns}.
 //   AROW = true:  row-major window (columns contiguous); four boxes
 //                 {32 columns, 64 rows}.
-// Threads: warps 0-3 epilogue, warp 4 TMA producer, warp 5 MMA issuer,
-// warps 6-9 converters. Rings: S1 FP32 stages (producer -> converters) and
+// Threads: warps 0-3 epilogue, warp 4 TMA producer of the FP32 tiles,
+// warp 5 MMA issuer, warps 6-9 converters, warp 10 TMA producer of the B
+// tiles. The two producers are separate so that the FP32 loads run up to S1
+// stages ahead whatever the state of the BF16 ring (one thread issuing
+// both waited for a free BF16 stage before each next FP32 load, which kept
+// fewer FP32 loads in flight). Rings: S1 FP32 stages (producer -> converters) and
 // S2 BF16 stages (A from the converters, B by TMA -> MMA); a BF16 stage is
 // free again when the MMAs that read it are done and the TMA store of its
 // A tile has read it. (Converters that copy the tile out themselves, with 4
 // FP32 + 2 BF16 stages and no bulk-store wait, measured 9 % slower.)
-constexpr int kThreadsA32 = 320;
+constexpr int kThreadsA32 = 352;
 
 template <int NT, int S1, int S2, bool AROW, bool AMAX>
 __global__ void __launch_bounds__(kThreadsA32, 1)
@@ -726,7 +730,7 @@ __global__ void __launch_bounds__(kThreadsA32, 1)
   const uint32_t tmem = *tbase;
 
   if (warp == 4 && lane == 0) {
-    // ---------------- TMA producer ----------------
+    // ---------------- TMA producer: FP32 tiles ----------------
     uint32_t it = 0;
     bool ok = true;
     Sched sc;
@@ -735,8 +739,8 @@ __global__ void __launch_bounds__(kThreadsA32, 1)
     while (ok && next_seg(g, sc, mt, nt, kt0, kt1)) {
       const int KT = kt1 - kt0;
       for (int kt = 0; kt < KT; ++kt, ++it) {
-        const int s1 = it % S1, s2 = it % S2;
-        const uint32_t ph1 = (it / S1) & 1, ph2 = (it / S2) & 1;
+        const int s1 = it % S1;
+        const uint32_t ph1 = (it / S1) & 1;
         const int kc = (kt0 + kt) * BK;
         if (!mbar_wait(f32empty + s1, ph1 ^ 1, err)) {
           ok = false;
@@ -751,6 +755,21 @@ __global__ void __launch_bounds__(kThreadsA32, 1)
 #pragma unroll
           for (int q = 0; q < 4; ++q) tma_load_2d(&tmA32, f32full + s1, a32 + q * 8192, mt * BM + 32 * q, kc);
         }
+      }
+    }
+  } else if (warp == 10 && lane == 0) {
+    // ---------------- TMA producer: B tiles ----------------
+    uint32_t it = 0;
+    bool ok = true;
+    Sched sc;
+    sched_init(g, sc);
+    int mt, nt, kt0, kt1;
+    while (ok && next_seg(g, sc, mt, nt, kt0, kt1)) {
+      const int KT = kt1 - kt0;
+      for (int kt = 0; kt < KT; ++kt, ++it) {
+        const int s2 = it % S2;
+        const uint32_t ph2 = (it / S2) & 1;
+        const int kc = (kt0 + kt) * BK;
         if (!mbar_wait(empty + s2, ph2 ^ 1, err)) {
           ok = false;
           break;
@@ -791,7 +810,7 @@ __global__ void __launch_bounds__(kThreadsA32, 1)
       if (ok) umma_commit(tfull + acc);
       ++tcount;
     }
-  } else if (warp >= 6) {
+  } else if (warp >= 6 && warp < 10) {
     // ---------------- converters ----------------
     const int ct = threadIdx.x - 6 * 32;  // A-tile line (window column) of this thread
     uint32_t it = 0;
