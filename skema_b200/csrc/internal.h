@@ -144,9 +144,6 @@ struct skema_ctx {
   // Nonzeros each lane of that kernel loads ahead per step (2, 4, 6 or 8);
   // SKEMA_SSIGN_BATCH overrides the default.
   int ssign_batch = 4;
-  // FP32 x 10 + BF16 stage counts of the X^T product from an FP32 window (33
-  // or 42); SKEMA_XT_STAGES overrides the default.
-  int xt_stages = 33;
   int cc_major = 0, cc_minor = 0;
   // BF16 tensor-core form: Omega~ and Psi~ stacked as one (k+s) x n
   // row-major operand (ld_op16), Upsilon~ / Phi~ copies in Map::lowp with
