@@ -321,20 +321,17 @@ void launch_gemm(skema_ctx* c, const CUtensorMap& ta, const CUtensorMap& tb, int
 }
 
 // X^T product straight from the FP32 window (converts it and writes A16).
-template <bool AROW, int S1, int S2, bool WST>
+template <bool AROW, int S1, int S2>
 void launch_gemm_a32_s(skema_ctx* c, const CUtensorMap& ta32, const CUtensorMap& tb, const CUtensorMap& ta16,
-                       __nv_bfloat16* a16, int64_t M, int64_t N, int64_t K, Plan pl, const tc::OutSpec& o,
-                       uint32_t* amax) {
+                       int64_t M, int64_t N, int64_t K, Plan pl, const tc::OutSpec& o, uint32_t* amax) {
   constexpr uint32_t STAGE = ((tc::BM * tc::BK * 2 + kNT * tc::BK * 2 + 1023) / 1024) * 1024;
   const size_t smem = (size_t)S1 * tc::BM * tc::BK * 4 + (size_t)S2 * STAGE + 1024 + 256;
-  auto kern = amax ? tc::gemm_a32_kernel<kNT, S1, S2, AROW, true, WST>
-                   : tc::gemm_a32_kernel<kNT, S1, S2, AROW, false, WST>;
+  auto kern = amax ? tc::gemm_a32_kernel<kNT, S1, S2, AROW, true> : tc::gemm_a32_kernel<kNT, S1, S2, AROW, false>;
   SKEMA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int grid = 0;
   const tc::Grid3 g = grid_of(c, M, N, K, kNT, tc::BK, pl, 1, &grid);
   if (grid <= 0) return;
-  kern<<<grid, WST ? tc::kThreadsA32St : tc::kThreadsA32, smem, c->stream>>>(ta32, tb, ta16, g, o, amax,
-                                                                            c->dev_err, a16, M);
+  kern<<<grid, tc::kThreadsA32, smem, c->stream>>>(ta32, tb, ta16, g, o, amax, c->dev_err);
   SKEMA_LAUNCHED(c);
   c->dev_err_armed = true;
 }
@@ -345,12 +342,8 @@ void launch_gemm_a32_s(skema_ctx* c, const CUtensorMap& ta32, const CUtensorMap&
 // of the two.
 template <bool AROW>
 void launch_gemm_a32(skema_ctx* c, const CUtensorMap& ta32, const CUtensorMap& tb, const CUtensorMap& ta16,
-                     __nv_bfloat16* a16, int64_t M, int64_t N, int64_t K, Plan pl, const tc::OutSpec& o,
-                     uint32_t* amax) {
-  if (c->xt_storer)
-    launch_gemm_a32_s<AROW, 3, 3, true>(c, ta32, tb, ta16, a16, M, N, K, pl, o, amax);
-  else
-    launch_gemm_a32_s<AROW, 3, 3, false>(c, ta32, tb, ta16, a16, M, N, K, pl, o, amax);
+                     int64_t M, int64_t N, int64_t K, Plan pl, const tc::OutSpec& o, uint32_t* amax) {
+  launch_gemm_a32_s<AROW, 3, 3>(c, ta32, tb, ta16, M, N, K, pl, o, amax);
 }
 
 // ---- FP8 form -------------------------------------------------------------
@@ -690,10 +683,10 @@ TcSlices xt_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr, __nv_bfloat16* 
   const CUtensorMap ta16 = tmap_bf16_blocked(A16, (uint64_t)n, (uint64_t)nrb, 128);
   if (a32_cm) {
     const CUtensorMap ta32 = tmap_f32(Aw.p, (uint64_t)wr, (uint64_t)n, (uint64_t)Aw.cs * 4, 32, 128);
-    launch_gemm_a32<false>(c, ta32, tb, ta16, A16, n, k, wr, pl, o, amax);
+    launch_gemm_a32<false>(c, ta32, tb, ta16, n, k, wr, pl, o, amax);
   } else if (a32_rm) {
     const CUtensorMap ta32 = tmap_f32(Aw.p, (uint64_t)n, (uint64_t)wr, (uint64_t)Aw.rs * 4, 32, 64);
-    launch_gemm_a32<true>(c, ta32, tb, ta16, A16, n, k, wr, pl, o, amax);
+    launch_gemm_a32<true>(c, ta32, tb, ta16, n, k, wr, pl, o, amax);
   } else {
     launch_gemm<tc::A_KMAJ_BLK>(c, ta16, tb, n, k, wr, pl, 1, o);
   }

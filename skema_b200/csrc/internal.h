@@ -144,10 +144,6 @@ struct skema_ctx {
   // Nonzeros each lane of that kernel loads ahead per step (2, 4, 6 or 8);
   // SKEMA_SSIGN_BATCH overrides the default.
   int ssign_batch = 4;
-  // X^T product from an FP32 window: a warp of its own copies the BF16
-  // window copy out of each stage (true) or one TMA store per tile does
-  // (false); SKEMA_XT_STORER=1|0 overrides the default.
-  bool xt_storer = false;
   int cc_major = 0, cc_minor = 0;
   // BF16 tensor-core form: Omega~ and Psi~ stacked as one (k+s) x n
   // row-major operand (ld_op16), Upsilon~ / Phi~ copies in Map::lowp with

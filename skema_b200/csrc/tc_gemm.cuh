@@ -676,21 +676,12 @@ __global__ void __launch_bounds__(kThreads, 1)
 // free again when the MMAs that read it are done and the TMA store of its
 // A tile has read it. (Converters that copy the tile out themselves, with 4
 // FP32 + 2 BF16 stages and no bulk-store wait, measured 9 % slower.)
-//   WST = false: one converter thread stores each A tile with TMA, and the
-//                stage is released once that store has read it (waited for
-//                one stage later).
-//   WST = true:  warp 11 copies each A tile out (16-byte loads from the
-//                swizzled stage, a warp writing 512 contiguous bytes of
-//                a16, columns a16_cols) as soon as the stage is full, and
-//                releases it with the MMA.
 constexpr int kThreadsA32 = 352;
-constexpr int kThreadsA32St = 384;
 
-template <int NT, int S1, int S2, bool AROW, bool AMAX, bool WST>
-__global__ void __launch_bounds__(kThreadsA32St, 1)
+template <int NT, int S1, int S2, bool AROW, bool AMAX>
+__global__ void __launch_bounds__(kThreadsA32, 1)
     gemm_a32_kernel(const __grid_constant__ CUtensorMap tmA32, const __grid_constant__ CUtensorMap tmB,
-                    const __grid_constant__ CUtensorMap tmA16, Grid3 g, OutSpec o, uint32_t* amax, int* err,
-                    __nv_bfloat16* a16, int64_t a16_cols) {
+                    const __grid_constant__ CUtensorMap tmA16, Grid3 g, OutSpec o, uint32_t* amax, int* err) {
   constexpr uint32_t A32_BYTES = BM * BK * 4;  // 32 KB
   constexpr uint32_t A_BYTES = BM * BK * 2;    // 16 KB
   constexpr uint32_t B_BYTES = NT * BK * 2;
@@ -877,7 +868,7 @@ __global__ void __launch_bounds__(kThreadsA32St, 1)
         fence_proxy_async();
         mbar_arrive(f32empty + s1);
         mbar_arrive(full + s2);
-        if (!WST && ct == 0) {
+        if (ct == 0) {
           // all 128 lines written (and the B tile landed): store the BF16
           // tile. The stage is released once TMA has read it; that is waited
           // for one stage later (the store before this one must be read by
@@ -898,7 +889,7 @@ __global__ void __launch_bounds__(kThreadsA32St, 1)
         }
       }
     }
-    if (!WST && ct == 0) {
+    if (ct == 0) {
       bulk_wait_all();
       if (pend >= 0) mbar_arrive(empty + pend);
     }
@@ -909,37 +900,6 @@ __global__ void __launch_bounds__(kThreadsA32St, 1)
       // warp meets here.
       const uint32_t wm = __reduce_max_sync(0xffffffffu, __float_as_uint(mx));
       if ((ct & 31) == 0) atomicMax(amax, wm);
-    }
-  } else if (WST && warp == 11) {
-    // ---------------- A16 storer ----------------
-    uint32_t it = 0;
-    bool ok = true;
-    Sched sc;
-    sched_init(g, sc);
-    int mt, nt, kt0, kt1;
-    while (ok && next_seg(g, sc, mt, nt, kt0, kt1)) {
-      const int KT = kt1 - kt0;
-      for (int kt = 0; kt < KT; ++kt, ++it) {
-        const int s2 = it % S2;
-        const uint32_t ph2 = (it / S2) & 1;
-        // every lane polls the stage's full barrier (bounded); the warp
-        // stops together if any lane's wait ran out
-        if (!__all_sync(0xffffffffu, mbar_wait(full + s2, ph2, err))) {
-          ok = false;
-          break;
-        }
-        const unsigned char* tile = stbf + s2 * STAGE;
-        const int64_t col0 = (int64_t)mt * BM;
-        uint4* gdst = reinterpret_cast<uint4*>(a16 + ((int64_t)(kt0 + kt) * a16_cols + col0) * BK);
-#pragma unroll 8
-        for (int q = 0; q < 32; ++q) {
-          const int idx = q * 32 + lane, line = idx >> 3, ch = idx & 7;
-          const uint4 v = *reinterpret_cast<const uint4*>(tile + line * 128 + ((ch ^ (line & 7)) << 4));
-          if (col0 + line < a16_cols) gdst[idx] = v;
-        }
-        __syncwarp();
-        if (lane == 0) mbar_arrive(empty + s2);
-      }
     }
   } else if (warp < 4) {
     // ---------------- epilogue ----------------
