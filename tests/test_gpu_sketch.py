@@ -499,10 +499,14 @@ def test_kat_kernel(sk, kat):
     assert np.max(np.abs(S - kat["kernel_svals"][:5])) / S[0] < 1e-5
 
 
-def test_low_rank_approx_vs_oracle(sk, oracle):
+@pytest.mark.parametrize("rank", [10, 50])
+def test_low_rank_approx_vs_oracle(sk, oracle, rank):
+    # rank 10: k = 41, the single-CTA shared-memory Jacobi and the tensor-core
+    # tall products; rank 50: k = 201, s = 403, the block Jacobi (A and V do
+    # not fit one CTA) and the general FP64 products for k > 128
     m, n = 2000, 1000
     A = dense_input(m, n).astype(np.float32)
-    a = alg(sk, m, n, 10, 100, 0)
+    a = alg(sk, m, n, rank, 100, 0)
     o = oracle_for(oracle, a)
     with sk.SketchySVD(a) as s:
         s.linear_update(A)
