@@ -156,7 +156,7 @@ __device__ __forceinline__ void dmma(double (&d)[2], double a, double b) {
                : "d"(a), "d"(b));
 }
 
-// G += A^T A for a tall column-major A (rows x k, ld lda, k <= 128; T float
+// G += A^T A for a tall column-major A (rows x k, ld lda, k <= 256; T float
 // or double, widened to FP64 exactly). The k x k product is cut into 32 x 32
 // tiles and only the tiles on or above the diagonal are formed (6 of 9 at
 // k <= 96), each by P warps of the CTA that split the CTA's rows four at a
@@ -170,7 +170,10 @@ __global__ void __launch_bounds__(512) gram_mma_kernel(const T* __restrict__ A, 
                                                        double* __restrict__ G, int64_t rows_per_cta, int P) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nsb = (k + 31) >> 5;
-  const int tile = warp / P, part = warp - tile * P;
+  // blockIdx.y takes a group of tiles when they do not all fit one CTA
+  const int per_cta = (int)(blockDim.x >> 5) / P;
+  const int tile = (int)blockIdx.y * per_cta + warp / P, part = warp % P;
+  if (tile >= nsb * (nsb + 1) / 2) return;
   int ti = 0, tj = tile;  // tile -> (ti, tj), ti <= tj, row-major over the upper triangle
   while (tj >= nsb - ti) {
     tj -= nsb - ti;
@@ -242,7 +245,9 @@ __global__ void __launch_bounds__(512) gram_mma_kernel(const T* __restrict__ A, 
 template <typename T, int NB, bool UPPER>
 __global__ void __launch_bounds__(256) tsm_mma_kernel(const T* __restrict__ A, int64_t lda, int64_t rows, int k,
                                                       const double* __restrict__ B, int64_t ldb, int n2,
-                                                      double* __restrict__ C, int64_t ldc) {
+                                                      double* __restrict__ C, int64_t ldc, int col0) {
+  // B and C are the columns [col0, col0 + n2) of the whole product (col0
+  // places them against the triangle for UPPER)
   extern __shared__ double tsm_smem[];
   // Bs[kk * ldbs + col], ldbs = 8 NB + 4 (mod 16) so a fragment's 4 x 8
   // reads hit 16 distinct bank pairs per half-warp
@@ -280,7 +285,7 @@ __global__ void __launch_bounds__(256) tsm_mma_kernel(const T* __restrict__ A, i
         const double* bs = tsm_smem + (k0 + lr) * ldbs + lc;
 #pragma unroll
         for (int n = 0; n < NB; ++n) {
-          if (UPPER && 8 * n + 7 < k0) continue;  // B(k0.., block n) is zero
+          if (UPPER && col0 + 8 * n + 7 < k0) continue;  // B(k0.., block n) is zero
           const double b = bs[8 * n];
           dmma(acc[0][n], a0[j], b);
           dmma(acc[1][n], a1[j], b);
@@ -306,28 +311,33 @@ template <typename T>
 void launch_gram_mma(skema_ctx* c, const T* A, int64_t lda, int64_t rows, int64_t k, double* G) {
   const int nsb = (int)((k + 31) / 32);
   const int tiles = nsb * (nsb + 1) / 2;
-  const int P = std::max(1, std::min(16 / tiles, 16));
+  // up to 16 warps per CTA: P warps per tile when the tiles leave room,
+  // else groups of 16 tiles over blockIdx.y (k > 160)
+  const int P = std::max(1, 16 / tiles);
+  const int per_cta = std::min(tiles, 16 / P);
+  const int groups = (tiles + per_cta - 1) / per_cta;
   const int64_t ctas = std::max<int64_t>(1, std::min<int64_t>((rows + 1023) / 1024, (int64_t)c->sm_count));
   const int64_t per = ((rows + ctas - 1) / ctas + 3) / 4 * 4;
-  gram_mma_kernel<T><<<(unsigned)((rows + per - 1) / per), 32 * tiles * P, 0, c->stream>>>(A, lda, rows, (int)k, G,
-                                                                                          per, P);
+  const dim3 grid((unsigned)((rows + per - 1) / per), (unsigned)groups);
+  gram_mma_kernel<T><<<grid, 32 * per_cta * P, 0, c->stream>>>(A, lda, rows, (int)k, G, per, P);
   SKEMA_LAUNCHED(c);
 }
 
 template <typename T, int NB>
 void launch_tsm_nb(skema_ctx* c, const T* A, int64_t lda, int64_t rows, int64_t k, const double* B, int64_t ldb,
-                   int64_t n2, double* C, int64_t ldc, bool upper) {
+                   int64_t n2, double* C, int64_t ldc, bool upper, int col0) {
   constexpr int ldbs = (8 * NB + 15) / 16 * 16 + 4;
   const size_t smem = sizeof(double) * (size_t)(((k + 3) & ~3) * ldbs);
   auto kern = upper ? tsm_mma_kernel<T, NB, true> : tsm_mma_kernel<T, NB, false>;
   SKEMA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int64_t tiles = (rows + 15) / 16;
   const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((tiles + 7) / 8, 4 * (int64_t)c->sm_count));
-  kern<<<grid, 256, smem, c->stream>>>(A, lda, rows, (int)k, B, ldb, (int)n2, C, ldc);
+  kern<<<grid, 256, smem, c->stream>>>(A, lda, rows, (int)k, B, ldb, (int)n2, C, ldc, col0);
   SKEMA_LAUNCHED(c);
 }
 
 // G (k x k, column-major) = A^T A for column-major A (rows x k, ld lda).
+constexpr int64_t kTallMaxK = 256;  // the tensor-core tall products take k up to this
 template <typename T>
 void gram_t(skema_ctx* c, const T* A, int64_t lda, int64_t rows, int64_t k, double* G) {
   SKEMA_CUDA(cudaMemsetAsync(G, 0, sizeof(double) * (size_t)(k * k), c->stream));
@@ -338,41 +348,60 @@ void gram(skema_ctx* c, const double* A, int64_t lda, int64_t rows, int64_t k, d
     SKEMA_CUDA(cudaMemsetAsync(G, 0, sizeof(double) * (size_t)(k * k), c->stream));
     return;
   }
-  if (k > 128) {
+  if (k > kTallMaxK) {
     dgemm<double, double>(c, k, k, rows, 1.0, A, lda, 1, A, 1, lda, 0.0, G, 1, k);
     return;
   }
   gram_t<double>(c, A, lda, rows, k, G);
 }
 
+// Column block width of the tall product: B's k x (8 NB) slice (padded)
+// stays in shared memory, at most 220 KB.
+int tsm_chunk_blocks(int64_t k) {
+  const int64_t kp = (k + 3) & ~3;
+  for (int nb = 16; nb > 1; --nb) {
+    const int64_t ldbs = (8 * nb + 15) / 16 * 16 + 4;
+    if (kp * ldbs * (int64_t)sizeof(double) <= 220 * 1024) return nb;
+  }
+  return 1;
+}
+
 // C (rows x n2) = A (rows x k) B (k x n2), all column-major; upper: B is
-// upper triangular (its zeros below the diagonal are not read).
+// upper triangular (its zeros below the diagonal are not read). Column
+// blocks of B beyond what shared memory holds go in further launches.
 template <typename T>
 void tall_times_small_t(skema_ctx* c, const T* A, int64_t lda, int64_t rows, int64_t k, const double* B,
                         int64_t ldb, int64_t n2, double* C, int64_t ldc, bool upper) {
-  switch ((n2 + 7) / 8) {
-    case 1: launch_tsm_nb<T, 1>(c, A, lda, rows, k, B, ldb, n2, C, ldc, upper); break;
-    case 2: launch_tsm_nb<T, 2>(c, A, lda, rows, k, B, ldb, n2, C, ldc, upper); break;
-    case 3: launch_tsm_nb<T, 3>(c, A, lda, rows, k, B, ldb, n2, C, ldc, upper); break;
-    case 4: launch_tsm_nb<T, 4>(c, A, lda, rows, k, B, ldb, n2, C, ldc, upper); break;
-    case 5: launch_tsm_nb<T, 5>(c, A, lda, rows, k, B, ldb, n2, C, ldc, upper); break;
-    case 6: launch_tsm_nb<T, 6>(c, A, lda, rows, k, B, ldb, n2, C, ldc, upper); break;
-    case 7: launch_tsm_nb<T, 7>(c, A, lda, rows, k, B, ldb, n2, C, ldc, upper); break;
-    case 8: launch_tsm_nb<T, 8>(c, A, lda, rows, k, B, ldb, n2, C, ldc, upper); break;
-    case 9: launch_tsm_nb<T, 9>(c, A, lda, rows, k, B, ldb, n2, C, ldc, upper); break;
-    case 10: launch_tsm_nb<T, 10>(c, A, lda, rows, k, B, ldb, n2, C, ldc, upper); break;
-    case 11: launch_tsm_nb<T, 11>(c, A, lda, rows, k, B, ldb, n2, C, ldc, upper); break;
-    case 12: launch_tsm_nb<T, 12>(c, A, lda, rows, k, B, ldb, n2, C, ldc, upper); break;
-    case 13: launch_tsm_nb<T, 13>(c, A, lda, rows, k, B, ldb, n2, C, ldc, upper); break;
-    case 14: launch_tsm_nb<T, 14>(c, A, lda, rows, k, B, ldb, n2, C, ldc, upper); break;
-    case 15: launch_tsm_nb<T, 15>(c, A, lda, rows, k, B, ldb, n2, C, ldc, upper); break;
-    default: launch_tsm_nb<T, 16>(c, A, lda, rows, k, B, ldb, n2, C, ldc, upper); break;
+  const int64_t chunk = 8 * (int64_t)tsm_chunk_blocks(k);
+  for (int64_t c0 = 0; c0 < n2; c0 += chunk) {
+    const int64_t w = std::min(chunk, n2 - c0);
+    const double* Bc = B + c0 * ldb;
+    double* Cc = C + c0 * ldc;
+    const int col0 = (int)c0;
+    switch ((w + 7) / 8) {
+      case 1: launch_tsm_nb<T, 1>(c, A, lda, rows, k, Bc, ldb, w, Cc, ldc, upper, col0); break;
+      case 2: launch_tsm_nb<T, 2>(c, A, lda, rows, k, Bc, ldb, w, Cc, ldc, upper, col0); break;
+      case 3: launch_tsm_nb<T, 3>(c, A, lda, rows, k, Bc, ldb, w, Cc, ldc, upper, col0); break;
+      case 4: launch_tsm_nb<T, 4>(c, A, lda, rows, k, Bc, ldb, w, Cc, ldc, upper, col0); break;
+      case 5: launch_tsm_nb<T, 5>(c, A, lda, rows, k, Bc, ldb, w, Cc, ldc, upper, col0); break;
+      case 6: launch_tsm_nb<T, 6>(c, A, lda, rows, k, Bc, ldb, w, Cc, ldc, upper, col0); break;
+      case 7: launch_tsm_nb<T, 7>(c, A, lda, rows, k, Bc, ldb, w, Cc, ldc, upper, col0); break;
+      case 8: launch_tsm_nb<T, 8>(c, A, lda, rows, k, Bc, ldb, w, Cc, ldc, upper, col0); break;
+      case 9: launch_tsm_nb<T, 9>(c, A, lda, rows, k, Bc, ldb, w, Cc, ldc, upper, col0); break;
+      case 10: launch_tsm_nb<T, 10>(c, A, lda, rows, k, Bc, ldb, w, Cc, ldc, upper, col0); break;
+      case 11: launch_tsm_nb<T, 11>(c, A, lda, rows, k, Bc, ldb, w, Cc, ldc, upper, col0); break;
+      case 12: launch_tsm_nb<T, 12>(c, A, lda, rows, k, Bc, ldb, w, Cc, ldc, upper, col0); break;
+      case 13: launch_tsm_nb<T, 13>(c, A, lda, rows, k, Bc, ldb, w, Cc, ldc, upper, col0); break;
+      case 14: launch_tsm_nb<T, 14>(c, A, lda, rows, k, Bc, ldb, w, Cc, ldc, upper, col0); break;
+      case 15: launch_tsm_nb<T, 15>(c, A, lda, rows, k, Bc, ldb, w, Cc, ldc, upper, col0); break;
+      default: launch_tsm_nb<T, 16>(c, A, lda, rows, k, Bc, ldb, w, Cc, ldc, upper, col0); break;
+    }
   }
 }
 void tall_times_small(skema_ctx* c, const double* A, int64_t lda, int64_t rows, int64_t k, const double* B,
                       int64_t ldb, int64_t n2, double* C, int64_t ldc, bool upper = false) {
   if (rows <= 0 || n2 <= 0) return;
-  if (k > 128 || n2 > 128) {
+  if (k > kTallMaxK) {
     dgemm<double, double>(c, rows, n2, k, 1.0, A, 1, lda, B, 1, ldb, 0.0, C, 1, ldc, false);
     return;
   }
@@ -1244,7 +1273,7 @@ void orth_lazy(skema_ctx* c, const float* S, int64_t lds, double* Qm, int64_t ro
     identity_kernel<<<g1(c, k * k), 256, 0, c->stream>>>(Tout, k);
     SKEMA_LAUNCHED(c);
   };
-  if (k <= 128 || rows <= 0) {
+  if (k <= kTallMaxK || rows <= 0) {
     gram_t<float>(c, S, lds, rows, k, G);
   } else {
     dgemm<float, float>(c, k, k, rows, 1.0, S, lds, 1, S, 1, lds, 0.0, G, 1, k);
@@ -1258,7 +1287,7 @@ void orth_lazy(skema_ctx* c, const float* S, int64_t lds, double* Qm, int64_t ro
   }
   // Qm = S R1^{-1} (G holds R1^{-1})
   if (rows <= 0) {
-  } else if (k <= 128) {
+  } else if (k <= kTallMaxK) {
     tall_times_small_t<float>(c, S, lds, rows, k, G, k, k, Qm, rows, true);
   } else {
     dgemm<float, double>(c, rows, k, k, 1.0, S, 1, lds, G, 1, k, 0.0, Qm, 1, rows, false);
