@@ -165,34 +165,45 @@ __device__ __forceinline__ void dmma(double (&d)[2], double a, double b) {
 // the B fragment of the same block is the same value, so a tile reads its
 // two column ranges once per step. The partial tiles go to G (column-major
 // k x k, zeroed beforehand) with atomics, mirrored below the diagonal.
-template <typename T>
-__global__ void __launch_bounds__(512) gram_mma_kernel(const T* __restrict__ A, int64_t lda, int64_t rows, int k,
-                                                       double* __restrict__ G, int64_t rows_per_cta, int P) {
+//
+// The same kernel forms C = A^T B for two tall matrices with the same rows
+// (SYM = false: A rows x ka, B rows x kb, every 32 x 32 tile of the ka x kb
+// product; C column-major with ld ka), which is how a dense map meets a
+// tall basis (Phi~ Q = (Phi~^T)^T Q).
+template <typename TA, typename TB, bool SYM>
+__global__ void __launch_bounds__(512) atb_mma_kernel(const TA* __restrict__ A, int64_t lda, int ka,
+                                                      const TB* __restrict__ B, int64_t ldb, int kb, int64_t rows,
+                                                      double* __restrict__ G, int64_t rows_per_cta, int P) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int nsb = (k + 31) >> 5;
+  const int nia = (ka + 31) >> 5, njb = (kb + 31) >> 5;
+  const int ntiles = SYM ? nia * (nia + 1) / 2 : nia * njb;
   // blockIdx.y takes a group of tiles when they do not all fit one CTA
   const int per_cta = (int)(blockDim.x >> 5) / P;
   const int tile = (int)blockIdx.y * per_cta + warp / P, part = warp % P;
-  if (tile >= nsb * (nsb + 1) / 2) return;
-  int ti = 0, tj = tile;  // tile -> (ti, tj), ti <= tj, row-major over the upper triangle
-  while (tj >= nsb - ti) {
-    tj -= nsb - ti;
-    ++ti;
+  if (tile >= ntiles) return;
+  int ti, tj;
+  if (SYM) {  // tile -> (ti, tj), ti <= tj, row-major over the upper triangle
+    ti = 0, tj = tile;
+    while (tj >= nia - ti) {
+      tj -= nia - ti;
+      ++ti;
+    }
+    tj += ti;
+  } else {
+    ti = tile / njb, tj = tile - (tile / njb) * njb;
   }
-  tj += ti;
-  if (ti >= nsb) return;
   const int64_t r0 = (int64_t)blockIdx.x * rows_per_cta, r1 = min(rows, r0 + rows_per_cta);
   const int lr = lane & 3, lc = lane >> 2;
-  const T* ci[4];
-  const T* cj[4];
+  const TA* ci[4];
+  const TB* cj[4];
   bool vi[4], vj[4];
 #pragma unroll
   for (int m = 0; m < 4; ++m) {
     const int coli = 32 * ti + 8 * m + lc, colj = 32 * tj + 8 * m + lc;
-    vi[m] = coli < k;
-    vj[m] = colj < k;
+    vi[m] = coli < ka;
+    vj[m] = colj < kb;
     ci[m] = A + (int64_t)(vi[m] ? coli : 0) * lda;
-    cj[m] = A + (int64_t)(vj[m] ? colj : 0) * lda;
+    cj[m] = B + (int64_t)(vj[m] ? colj : 0) * ldb;
   }
   double acc[4][4][2];
 #pragma unroll
@@ -201,7 +212,7 @@ __global__ void __launch_bounds__(512) gram_mma_kernel(const T* __restrict__ A, 
     for (int n = 0; n < 4; ++n) acc[m][n][0] = acc[m][n][1] = 0.0;
   // two steps of four rows per iteration: their 16 loads are in flight
   // together before the 32 MMAs that use them
-  const bool diag = ti == tj;
+  const bool diag = SYM && ti == tj;
   for (int64_t r = r0 + 4 * part; r < r1; r += 8 * P) {
     double a[2][4], b[2][4];
 #pragma unroll
@@ -228,9 +239,9 @@ __global__ void __launch_bounds__(512) gram_mma_kernel(const T* __restrict__ A, 
 #pragma unroll
       for (int i = 0; i < 2; ++i) {
         const int gi = 32 * ti + 8 * m + lc, gj = 32 * tj + 8 * n + 2 * lr + i;
-        if (gi >= k || gj >= k) continue;
-        atomicAdd(G + gi + (int64_t)gj * k, acc[m][n][i]);
-        if (ti != tj) atomicAdd(G + gj + (int64_t)gi * k, acc[m][n][i]);
+        if (gi >= ka || gj >= kb) continue;
+        atomicAdd(G + gi + (int64_t)gj * ka, acc[m][n][i]);
+        if (SYM && ti != tj) atomicAdd(G + gj + (int64_t)gi * ka, acc[m][n][i]);
       }
 }
 
@@ -307,19 +318,27 @@ __global__ void __launch_bounds__(256) tsm_mma_kernel(const T* __restrict__ A, i
   }
 }
 
-template <typename T>
-void launch_gram_mma(skema_ctx* c, const T* A, int64_t lda, int64_t rows, int64_t k, double* G) {
-  const int nsb = (int)((k + 31) / 32);
-  const int tiles = nsb * (nsb + 1) / 2;
+// C (ka x kb, column-major, zeroed beforehand) += A^T B, or the Gram matrix
+// A^T A when B is null (its upper tiles only).
+template <typename TA, typename TB>
+void launch_atb_mma(skema_ctx* c, const TA* A, int64_t lda, int64_t ka, const TB* B, int64_t ldb, int64_t kb,
+                    int64_t rows, double* G) {
+  const int nia = (int)((ka + 31) / 32), njb = (int)((kb + 31) / 32);
+  const int tiles = B ? nia * njb : nia * (nia + 1) / 2;
   // up to 16 warps per CTA: P warps per tile when the tiles leave room,
-  // else groups of 16 tiles over blockIdx.y (k > 160)
+  // else groups of 16 tiles over blockIdx.y
   const int P = std::max(1, 16 / tiles);
   const int per_cta = std::min(tiles, 16 / P);
   const int groups = (tiles + per_cta - 1) / per_cta;
   const int64_t ctas = std::max<int64_t>(1, std::min<int64_t>((rows + 1023) / 1024, (int64_t)c->sm_count));
   const int64_t per = ((rows + ctas - 1) / ctas + 3) / 4 * 4;
   const dim3 grid((unsigned)((rows + per - 1) / per), (unsigned)groups);
-  gram_mma_kernel<T><<<grid, 32 * per_cta * P, 0, c->stream>>>(A, lda, rows, (int)k, G, per, P);
+  if (B)
+    atb_mma_kernel<TA, TB, false><<<grid, 32 * per_cta * P, 0, c->stream>>>(A, lda, (int)ka, B, ldb, (int)kb, rows,
+                                                                             G, per, P);
+  else
+    atb_mma_kernel<TA, TA, true><<<grid, 32 * per_cta * P, 0, c->stream>>>(A, lda, (int)ka, A, lda, (int)ka, rows,
+                                                                            G, per, P);
   SKEMA_LAUNCHED(c);
 }
 
@@ -341,7 +360,7 @@ constexpr int64_t kTallMaxK = 256;  // the tensor-core tall products take k up t
 template <typename T>
 void gram_t(skema_ctx* c, const T* A, int64_t lda, int64_t rows, int64_t k, double* G) {
   SKEMA_CUDA(cudaMemsetAsync(G, 0, sizeof(double) * (size_t)(k * k), c->stream));
-  if (rows > 0) launch_gram_mma<T>(c, A, lda, rows, k, G);
+  if (rows > 0) launch_atb_mma<T, T>(c, A, lda, k, static_cast<const T*>(nullptr), 0, k, rows, G);
 }
 void gram(skema_ctx* c, const double* A, int64_t lda, int64_t rows, int64_t k, double* G) {
   if (rows <= 0) {  // an empty row block (a rank without rows) adds nothing
@@ -1313,6 +1332,13 @@ void apply_map_rows(skema_ctx* c, const Map& mp, const double* Qm, int64_t q0, i
     return;
   }
   if (mp.kind == SKEMA_MAP_GAUSS) {
+    if (mp.cs == 1 && R <= kTallMaxK * 4 && k <= kTallMaxK) {
+      // M(:, rows) Q = (M(:, rows)^T)^T Q: the map's logical rows are
+      // contiguous over the operand's rows, a tall column-major matrix
+      SKEMA_CUDA(cudaMemsetAsync(out, 0, sizeof(double) * (size_t)(R * k), c->stream));
+      launch_atb_mma<float, double>(c, mp.f32 + q0, mp.rs, R, Qm, qrows, k, qrows, out);
+      return;
+    }
     dgemm<float, double>(c, R, k, qrows, 1.0, mp.f32 + q0 * mp.cs, mp.rs, mp.cs, Qm, 1, qrows, 0.0, out, 1, R);
     return;
   }
