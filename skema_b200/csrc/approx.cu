@@ -856,12 +856,9 @@ __global__ void __launch_bounds__(1024) jacobi_svd_kernel_t(double* Ag, double* 
 // writes them back. rotated[0] is set when any rotation was made. nb - 1
 // outer rounds make an outer sweep, after which every pair of columns has
 // met; sweeps continue until one makes no rotation.
-template <int LP>
 __global__ void __launch_bounds__(1024) jacobi_block_kernel(double* __restrict__ Ag, double* __restrict__ Vg, int k,
                                                             int bs, int nb, int round, double tol,
                                                             int* __restrict__ rotated) {
-  // LP lanes per pair: a whole warp when the bs pairs of an inner round fit
-  // one per warp (shorter per-lane loops over the long columns)
   extern __shared__ double jb_smem[];
   __shared__ int any;
   // this CTA's pair of blocks in the round-robin round
@@ -888,8 +885,8 @@ __global__ void __launch_bounds__(1024) jacobi_block_kernel(double* __restrict__
   }
   if (threadIdx.x == 0) any = 0;
   __syncthreads();
-  const int hl = threadIdx.x & (LP - 1), slot = threadIdx.x / LP, nslot = blockDim.x / LP;
-  const unsigned hmask = LP == 32 ? 0xffffffffu : ((threadIdx.x & 16) ? 0xffff0000u : 0x0000ffffu);
+  const int hl = threadIdx.x & 15, slot = threadIdx.x >> 4, nslot = blockDim.x >> 4;
+  const unsigned hmask = (threadIdx.x & 16) ? 0xffff0000u : 0x0000ffffu;
   const int np = 2 * bs;  // even number of local players
   for (int r = 0; r < np - 1; ++r) {
     for (int pp = slot; pp < np / 2; pp += nslot) {
@@ -907,14 +904,14 @@ __global__ void __launch_bounds__(1024) jacobi_block_kernel(double* __restrict__
       double* ap = A + (size_t)p * k;
       double* aq = A + (size_t)q * k;
       double al = 0.0, be = 0.0, ga = 0.0;
-      for (int i = hl; i < k; i += LP) {
+      for (int i = hl; i < k; i += 16) {
         const double x = ap[i], y = aq[i];
         al = fma(x, x, al);
         be = fma(y, y, be);
         ga = fma(x, y, ga);
       }
 #pragma unroll
-      for (int o = LP / 2; o > 0; o >>= 1) {
+      for (int o = 8; o > 0; o >>= 1) {
         al += __shfl_xor_sync(hmask, al, o);
         be += __shfl_xor_sync(hmask, be, o);
         ga += __shfl_xor_sync(hmask, ga, o);
@@ -924,14 +921,14 @@ __global__ void __launch_bounds__(1024) jacobi_block_kernel(double* __restrict__
       const double d = be - al, h = 2.0 * ga;
       const double t = (d >= 0.0 ? h : -h) / (fabs(d) + sqrt(fma(d, d, h * h)));
       const double cs = rsqrt(fma(t, t, 1.0)), sn = cs * t;
-      for (int i = hl; i < k; i += LP) {
+      for (int i = hl; i < k; i += 16) {
         const double x = ap[i], y = aq[i];
         ap[i] = cs * x - sn * y;
         aq[i] = sn * x + cs * y;
       }
       double* vp = V + (size_t)p * k;
       double* vq = V + (size_t)q * k;
-      for (int i = hl; i < k; i += LP) {
+      for (int i = hl; i < k; i += 16) {
         const double x = vp[i], y = vq[i];
         vp[i] = cs * x - sn * y;
         vq[i] = sn * x + cs * y;
@@ -960,11 +957,7 @@ void jacobi_svd_blocked(skema_ctx* c, double* A, double* V, int64_t k, int max_s
   int nb = (int)((k + bs - 1) / bs);
   nb += nb & 1;  // an even number of players
   const size_t smem = sizeof(double) * (size_t)(4 * bs * k);
-  const bool warp_pairs = bs <= 32;  // bs pairs per inner round, one per warp of 1024 threads
-  if (warp_pairs)
-    SKEMA_CUDA(cudaFuncSetAttribute(jacobi_block_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  else
-    SKEMA_CUDA(cudaFuncSetAttribute(jacobi_block_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  SKEMA_CUDA(cudaFuncSetAttribute(jacobi_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   identity_kernel<<<(unsigned)std::min<int64_t>((k * k + 255) / 256, 4096), 256, 0, c->stream>>>(V, k);
   SKEMA_LAUNCHED(c);
   int* flag = sweeps_out + 2;  // the caller's status block has room after the sweep count
@@ -972,10 +965,7 @@ void jacobi_svd_blocked(skema_ctx* c, double* A, double* V, int64_t k, int max_s
   for (; sweep < max_sweeps; ++sweep) {
     SKEMA_CUDA(cudaMemsetAsync(flag, 0, sizeof(int), c->stream));
     for (int r = 0; r < nb - 1; ++r) {
-      if (warp_pairs)
-        jacobi_block_kernel<32><<<nb / 2, 1024, smem, c->stream>>>(A, V, (int)k, bs, nb, r, tol, flag);
-      else
-        jacobi_block_kernel<16><<<nb / 2, 1024, smem, c->stream>>>(A, V, (int)k, bs, nb, r, tol, flag);
+      jacobi_block_kernel<<<nb / 2, 1024, smem, c->stream>>>(A, V, (int)k, bs, nb, r, tol, flag);
       SKEMA_LAUNCHED(c);
     }
     int h = 0;
