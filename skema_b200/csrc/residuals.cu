@@ -93,87 +93,6 @@ __global__ void __launch_bounds__(256)
   }
 }
 
-// A^T U for a call's CSR rows through the transposed structure (CSC),
-// without atomics on A^T U: count the entries of each column, scan the
-// counts into column offsets, place each entry's row and value in its
-// column, then a warp per column sums a U(i, :) over the column's entries
-// (U row-major, r values per row, coalesced over the lanes) and adds the
-// sum to A^T U(c, :), which no other warp touches.
-__global__ void csr_col_count_kernel(const int32_t* __restrict__ col, int64_t b0, int64_t e0, int64_t ncol,
-                                     int* __restrict__ cnt) {
-  for (int64_t p = b0 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < e0; p += (int64_t)gridDim.x * blockDim.x) {
-    const int32_t c = col[p];
-    if ((uint64_t)c < (uint64_t)ncol) atomicAdd(cnt + c, 1);
-  }
-}
-
-// colptr[0..n] = exclusive prefix sum of cnt[0..n) (one CTA of 1024 threads:
-// each thread sums a contiguous chunk, the chunk sums are scanned in shared
-// memory, then each thread writes its chunk's offsets).
-__global__ void __launch_bounds__(1024) scan_counts_kernel(const int* __restrict__ cnt, int64_t n,
-                                                           int64_t* __restrict__ colptr) {
-  __shared__ int64_t part[1024];
-  const int64_t per = (n + blockDim.x - 1) / blockDim.x;
-  const int64_t a = threadIdx.x * per, b = min(n, a + per);
-  int64_t sum = 0;
-  for (int64_t q = a; q < b; ++q) sum += cnt[q];
-  part[threadIdx.x] = sum;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    int64_t run = 0;
-    for (int t = 0; t < (int)blockDim.x; ++t) {
-      const int64_t v = part[t];
-      part[t] = run;
-      run += v;
-    }
-    colptr[n] = run;
-  }
-  __syncthreads();
-  int64_t run = part[threadIdx.x];
-  for (int64_t q = a; q < b; ++q) {
-    colptr[q] = run;
-    run += cnt[q];
-  }
-}
-
-__global__ void csr_to_csc_kernel(const int64_t* __restrict__ rowptr, const int32_t* __restrict__ col,
-                                  const float* __restrict__ val, int64_t col_offset, int64_t nrows, int64_t ncol,
-                                  const int64_t* __restrict__ colptr, int* __restrict__ fill,
-                                  int32_t* __restrict__ rows_t, float* __restrict__ vals_t) {
-  const int lane = threadIdx.x & 31;
-  const int64_t w0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t i = w0; i < nrows; i += nw) {
-    const int64_t b = rowptr[i] - col_offset, e = rowptr[i + 1] - col_offset;
-    for (int64_t p = b + lane; p < e; p += 32) {
-      const int32_t c = col[p];
-      if ((uint64_t)c >= (uint64_t)ncol) continue;
-      const int64_t q = colptr[c] + atomicAdd(fill + c, 1);
-      rows_t[q] = (int32_t)i;
-      vals_t[q] = val[p];
-    }
-  }
-}
-
-__global__ void csc_atu_kernel(const int64_t* __restrict__ colptr, const int32_t* __restrict__ rows_t,
-                               const float* __restrict__ vals_t, int64_t ncol, int64_t R0,
-                               const double* __restrict__ U, int64_t r, double* __restrict__ AtU) {
-  const int lane = threadIdx.x & 31;
-  const int64_t w0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t c = w0; c < ncol; c += nw) {
-    const int64_t b = colptr[c], e = colptr[c + 1];
-    if (b == e) continue;
-    for (int64_t j0 = 0; j0 < r; j0 += 32) {
-      const int64_t j = j0 + lane;
-      if (j >= r) break;
-      double acc = 0.0;
-      for (int64_t q = b; q < e; ++q) acc = fma((double)vals_t[q], U[(R0 + rows_t[q]) * r + j], acc);
-      AtU[c * r + j] += acc;
-    }
-  }
-}
-
 __global__ void sqrt_kernel(const double* __restrict__ a, double* __restrict__ out, int64_t r) {
   for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < r; j += (int64_t)gridDim.x * blockDim.x)
     out[j] = sqrt(a[j]);
@@ -241,44 +160,12 @@ void residual_csr(skema_ctx* c, const int64_t* rowptr, const int32_t* col, const
   need_ready(c);
   const int64_t r = c->p.rank;
   const int grid = grid_of(c, (nrows * 32 + 255) / 256, 16);
-  // the transposed structure keeps call-local rows as int32
-  const bool transpose = !c->spd && nrows < ((int64_t)1 << 31);
-  // A V and its column sums of squares, a warp per row (with FP64 atomics
-  // into A^T U when the call is too large to transpose)
+  // A^T U with FP64 atomics (a kernel that owned column blocks of A^T U in
+  // shared memory had every CTA walk all rows of the call and ran 2.5x
+  // longer)
   csr_residual_kernel<<<grid, 256, 0, c->stream>>>(rowptr, col, val, col_offset, nrows, row0, c->n,
                                                    c->spd ? c->res_V : c->res_U, c->res_V, c->res_S, r,
-                                                   (c->spd || transpose) ? nullptr : c->res_AtU, c->res_sq);
-  SKEMA_LAUNCHED(c);
-  if (!transpose || nrows == 0) return;
-  // A^T U through the call's transposed structure (the FP64 atomics of one
-  // warp per row into A^T U took about 12 ms for 1e7 entries at r = 20; a
-  // kernel that owned column blocks of A^T U in shared memory had every CTA
-  // walk all rows of the call and ran 2.5x longer)
-  int64_t ends[2];
-  SKEMA_CUDA(cudaMemcpyAsync(&ends[0], rowptr, sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream));
-  SKEMA_CUDA(cudaMemcpyAsync(&ends[1], rowptr + nrows, sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream));
-  SKEMA_CUDA(cudaStreamSynchronize(c->stream));
-  const int64_t b0 = ends[0] - col_offset, e0 = ends[1] - col_offset, nnz = e0 - b0, n = c->n;
-  if (nnz <= 0) return;
-  auto rup = [](size_t b) { return (b + 255) / 256 * 256; };
-  const size_t b_cnt = rup(sizeof(int) * (size_t)n), b_ptr = rup(sizeof(int64_t) * (size_t)(n + 1));
-  const size_t b_rows = rup(sizeof(int32_t) * (size_t)nnz), b_vals = rup(sizeof(float) * (size_t)nnz);
-  char* ws = static_cast<char*>(workspace(c, 2 * b_cnt + b_ptr + b_rows + b_vals));
-  int* cnt = reinterpret_cast<int*>(ws);
-  int* fill = reinterpret_cast<int*>(ws + b_cnt);
-  int64_t* colptr = reinterpret_cast<int64_t*>(ws + 2 * b_cnt);
-  int32_t* rows_t = reinterpret_cast<int32_t*>(ws + 2 * b_cnt + b_ptr);
-  float* vals_t = reinterpret_cast<float*>(ws + 2 * b_cnt + b_ptr + b_rows);
-  SKEMA_CUDA(cudaMemsetAsync(cnt, 0, 2 * b_cnt, c->stream));  // cnt and fill
-  csr_col_count_kernel<<<grid_of(c, (nnz + 255) / 256, 16), 256, 0, c->stream>>>(col, b0, e0, n, cnt);
-  SKEMA_LAUNCHED(c);
-  scan_counts_kernel<<<1, 1024, 0, c->stream>>>(cnt, n, colptr);
-  SKEMA_LAUNCHED(c);
-  csr_to_csc_kernel<<<grid, 256, 0, c->stream>>>(rowptr, col, val, col_offset, nrows, n, colptr, fill, rows_t,
-                                                 vals_t);
-  SKEMA_LAUNCHED(c);
-  csc_atu_kernel<<<grid_of(c, (n * 32 + 255) / 256, 16), 256, 0, c->stream>>>(colptr, rows_t, vals_t, n, row0,
-                                                                               c->res_U, r, c->res_AtU);
+                                                   c->spd ? nullptr : c->res_AtU, c->res_sq);
   SKEMA_LAUNCHED(c);
 }
 
