@@ -584,26 +584,17 @@ __global__ void __launch_bounds__(1024) chol_factor_kernel(const double* G, int 
     if (i >= j) L[lo_off(j, k) + i - j] = G[q];
   }
   __syncthreads();
-  __shared__ double dinv_s;
-  __shared__ int bad_s;
-  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
   int bad = 0;
   for (int j = 0; j < k; ++j) {
-    // one thread forms the pivot's reciprocal (an FP64 division per
-    // column, not one per warp)
-    if (threadIdx.x == 0) {
-      const double d = L[lo_off(j, k)];
-      bad_s = (d > 0.0) ? 0 : j + 1;
-      dinv_s = (d > 0.0) ? 1.0 / d : 0.0;
-    }
-    __syncthreads();
-    if (bad_s) {  // the same value for every thread: a uniform exit
-      bad = bad_s;
+    const double d = L[lo_off(j, k)];
+    if (!(d > 0.0)) {  // every thread reads the same pivot: a uniform exit
+      bad = j + 1;
       break;
     }
-    const double dinv = dinv_s;
+    const double dinv = 1.0 / d;
     const double* colj = L + lo_off(j, k) - j;  // colj[a] = L(a, j)
-    for (int b = j + 1 + ty; b < k; b += nw) {
+    for (int b = j + 1 + ty; b < k; b += 32) {
       const double lbj = colj[b] * dinv;
       double* colb = L + lo_off(b, k) - b;
       for (int a = b + tx; a < k; a += 32) colb[a] = fma(-colj[a], lbj, colb[a]);
@@ -616,7 +607,7 @@ __global__ void __launch_bounds__(1024) chol_factor_kernel(const double* G, int 
   }
   for (int j = threadIdx.x; j < k; j += blockDim.x) aux[j] = sqrt(L[lo_off(j, k)]);
   __syncthreads();
-  for (int j = ty; j < k; j += nw) {
+  for (int j = ty; j < k; j += 32) {
     const double p = aux[j];
     double* colj = L + lo_off(j, k) - j;
     for (int i = j + tx; i < k; i += 32) colj[i] = (i == j) ? p : colj[i] / p;
@@ -628,7 +619,7 @@ __global__ void __launch_bounds__(1024) chol_factor_kernel(const double* G, int 
   }
   for (int j = threadIdx.x; j < k; j += blockDim.x) aux[j] = 1.0 / aux[j];
   __syncthreads();
-  for (int j = ty; j < k; j += nw) {
+  for (int j = ty; j < k; j += 32) {
     double b[VMAX];
 #pragma unroll
     for (int v = 0; v < VMAX; ++v) b[v] = (tx + 32 * v == j) ? 1.0 : 0.0;
@@ -757,113 +748,87 @@ __global__ void colsparse_apply_smem_kernel(const uint32_t* __restrict__ mp, int
 
 // ------------------------------------------------------ Jacobi SVD ---------
 // One-sided Jacobi on the column-major k x k A (overwritten by A V = U S),
-// V accumulated (column-major k x k), both in shared memory (2 k^2
-// doubles, k <= 114). One CTA. The first npairs half-warps each rotate one
-// pair of A's columns per round-robin round; the rotations (c, s) go to a
-// shared buffer, and the remaining warps apply the previous round's
-// rotations to V (eight lanes per pair) while A's next round runs, so V's
-// updates are off the chain that every round waits for. A sweep ends the
-// loop when it made no rotation (every pair within tol of orthogonal).
-__global__ void __launch_bounds__(1024) jacobi_svd_kernel(double* Ag, double* Vg, int k, int max_sweeps, double tol,
-                                                          int* sweeps_out, int awarps) {
+// V accumulated (column-major k x k). One CTA; each half-warp rotates one
+// pair of a round-robin round, and a sweep ends the loop when it made no
+// rotation (every pair within tol of orthogonal).
+// SMEM: A and V are worked on in shared memory (2 k^2 doubles), copied in at
+// the start and out at the end; every rotation reads and writes two columns
+// of each, so global memory would put an L2 round trip on every step.
+template <bool SMEM>
+__global__ void __launch_bounds__(1024) jacobi_svd_kernel_t(double* Ag, double* Vg, int64_t k64, int max_sweeps,
+                                                            double tol, int* sweeps_out) {
   __shared__ int rotated;
-  __shared__ double rot_c[2][64], rot_s[2][64];
-  __shared__ int rot_p[2][64], rot_q[2][64];
   extern __shared__ double jac_smem[];
-  double* A = jac_smem;
-  double* V = jac_smem + (size_t)k * k;
-  for (int q = threadIdx.x; q < k * k; q += blockDim.x) {
-    A[q] = Ag[q];
-    V[q] = (q % k == q / k) ? 1.0 : 0.0;
+  const int k = (int)k64;
+  double* A = SMEM ? jac_smem : Ag;
+  double* V = SMEM ? jac_smem + (size_t)k * k : Vg;
+  if (SMEM) {
+    for (int q = threadIdx.x; q < k * k; q += blockDim.x) A[q] = Ag[q];
   }
-  const int kp = (k + 1) & ~1;  // even number of players
-  const int npairs = kp / 2;    // <= 57
-  const int warp = threadIdx.x >> 5;
-  const bool agroup = warp < awarps;
-  // A group: a pair per half-warp; V group: a pair per 8 lanes
-  const int hl = threadIdx.x & 15, slot = threadIdx.x >> 4;
+  for (int q = threadIdx.x; q < k * k; q += blockDim.x) V[q] = (q % k == q / k) ? 1.0 : 0.0;
+  // a pair per half-warp: 64 pairs at a time, all of them for k <= 128
+  const int hl = threadIdx.x & 15, slot = threadIdx.x >> 4, nslot = blockDim.x >> 4;
   const unsigned hmask = (threadIdx.x & 16) ? 0xffff0000u : 0x0000ffffu;
-  const int vt = threadIdx.x - awarps * 32, vl = vt & 7, vslot = vt >> 3, nvslot = ((int)blockDim.x - awarps * 32) >> 3;
+  const int kp = (k + 1) & ~1;  // even number of players
   int sweep = 0;
   for (; sweep < max_sweeps; ++sweep) {
     if (threadIdx.x == 0) rotated = 0;
     __syncthreads();
-    // round r: A does round r (r < kp - 1), V applies round r - 1 (r >= 1)
-    for (int round = 0; round < kp; ++round) {
-      const int buf = round & 1;
-      if (agroup && round < kp - 1) {
-        for (int pr = slot; pr < npairs; pr += awarps * 2) {
-          // round-robin pairing: player kp-1 stays, the others rotate
-          int p, q;
-          if (pr == 0) {
-            p = round;
-            q = kp - 1;
-          } else {
-            p = round + pr;
-            if (p >= kp - 1) p -= kp - 1;
-            q = round - pr;
-            if (q < 0) q += kp - 1;
-          }
-          if (p > q) {
-            const int t = p;
-            p = q;
-            q = t;
-          }
-          double cs = 1.0, sn = 0.0;
-          if (q < k) {
-            double* ap = A + (size_t)p * k;
-            double* aq = A + (size_t)q * k;
-            double al = 0.0, be = 0.0, ga = 0.0;
-            for (int i = hl; i < k; i += 16) {
-              const double x = ap[i], y = aq[i];
-              al = fma(x, x, al);
-              be = fma(y, y, be);
-              ga = fma(x, y, ga);
-            }
-#pragma unroll
-            for (int o = 8; o > 0; o >>= 1) {
-              al += __shfl_xor_sync(hmask, al, o);
-              be += __shfl_xor_sync(hmask, be, o);
-              ga += __shfl_xor_sync(hmask, ga, o);
-            }
-            // converged pair: |gamma| <= tol sqrt(alpha beta), compared squared
-            if (!(ga == 0.0 || ga * ga <= (tol * tol) * (al * be))) {
-              if (hl == 0) rotated = 1;
-              // tan of the rotation angle, the smaller root of t^2 + 2 zeta t
-              // - 1 with zeta = d / h, d = beta - alpha, h = 2 gamma, written
-              // as t = sign(d) h / (|d| + sqrt(d^2 + h^2)): one square root
-              // and one division on the chain that every round waits for
-              const double d = be - al, h = 2.0 * ga;
-              const double t = (d >= 0.0 ? h : -h) / (fabs(d) + sqrt(fma(d, d, h * h)));
-              cs = rsqrt(fma(t, t, 1.0));
-              sn = cs * t;
-              for (int i = hl; i < k; i += 16) {
-                const double x = ap[i], y = aq[i];
-                ap[i] = cs * x - sn * y;
-                aq[i] = sn * x + cs * y;
-              }
-            }
-          }
-          if (hl == 0) {
-            rot_c[buf][pr] = cs;
-            rot_s[buf][pr] = sn;
-            rot_p[buf][pr] = p;
-            rot_q[buf][pr] = q;
-          }
+    for (int round = 0; round < kp - 1; ++round) {
+      for (int pr = slot; pr < kp / 2; pr += nslot) {
+        // round-robin pairing: player kp-1 stays, the others rotate
+        int p, q;
+        if (pr == 0) {
+          p = round;
+          q = kp - 1;
+        } else {
+          p = round + pr;
+          if (p >= kp - 1) p -= kp - 1;
+          q = round - pr;
+          if (q < 0) q += kp - 1;
         }
-      } else if (!agroup && round >= 1) {
-        const int pb = buf ^ 1;  // the previous round's rotations
-        for (int pr = vslot; pr < npairs; pr += nvslot) {
-          const int p = rot_p[pb][pr], q = rot_q[pb][pr];
-          const double cs = rot_c[pb][pr], sn = rot_s[pb][pr];
-          if (q >= k || sn == 0.0) continue;
-          double* vp = V + (size_t)p * k;
-          double* vq = V + (size_t)q * k;
-          for (int i = vl; i < k; i += 8) {
-            const double x = vp[i], y = vq[i];
-            vp[i] = cs * x - sn * y;
-            vq[i] = sn * x + cs * y;
-          }
+        if (p > q) {
+          const int t = p;
+          p = q;
+          q = t;
+        }
+        if (q >= k) continue;  // bye
+        double* ap = A + (size_t)p * k;
+        double* aq = A + (size_t)q * k;
+        double al = 0.0, be = 0.0, ga = 0.0;
+        for (int i = hl; i < k; i += 16) {
+          const double x = ap[i], y = aq[i];
+          al = fma(x, x, al);
+          be = fma(y, y, be);
+          ga = fma(x, y, ga);
+        }
+#pragma unroll
+        for (int o = 8; o > 0; o >>= 1) {
+          al += __shfl_xor_sync(hmask, al, o);
+          be += __shfl_xor_sync(hmask, be, o);
+          ga += __shfl_xor_sync(hmask, ga, o);
+        }
+        // converged pair: |gamma| <= tol sqrt(alpha beta), compared squared
+        if (ga == 0.0 || ga * ga <= (tol * tol) * (al * be)) continue;
+        if (hl == 0) rotated = 1;
+        // tan of the rotation angle, the smaller root of t^2 + 2 zeta t - 1
+        // with zeta = d / h, d = beta - alpha, h = 2 gamma, written as
+        // t = sign(d) h / (|d| + sqrt(d^2 + h^2)): one square root and one
+        // division on the chain that every round waits for
+        const double d = be - al, h = 2.0 * ga;
+        const double t = (d >= 0.0 ? h : -h) / (fabs(d) + sqrt(fma(d, d, h * h)));
+        const double cs = rsqrt(fma(t, t, 1.0)), sn = cs * t;
+        for (int i = hl; i < k; i += 16) {
+          const double x = ap[i], y = aq[i];
+          ap[i] = cs * x - sn * y;
+          aq[i] = sn * x + cs * y;
+        }
+        double* vp = V + (size_t)p * k;
+        double* vq = V + (size_t)q * k;
+        for (int i = hl; i < k; i += 16) {
+          const double x = vp[i], y = vq[i];
+          vp[i] = cs * x - sn * y;
+          vq[i] = sn * x + cs * y;
         }
       }
       __syncthreads();
@@ -873,10 +838,12 @@ __global__ void __launch_bounds__(1024) jacobi_svd_kernel(double* Ag, double* Vg
     if (!more) break;
   }
   if (threadIdx.x == 0) sweeps_out[0] = sweep;
-  __syncthreads();
-  for (int q = threadIdx.x; q < k * k; q += blockDim.x) {
-    Ag[q] = A[q];
-    Vg[q] = V[q];
+  if (SMEM) {
+    __syncthreads();
+    for (int q = threadIdx.x; q < k * k; q += blockDim.x) {
+      Ag[q] = A[q];
+      Vg[q] = V[q];
+    }
   }
 }
 
@@ -1013,15 +980,12 @@ void jacobi_svd_blocked(skema_ctx* c, double* A, double* V, int64_t k, int max_s
 // The SVD kernel for a k x k problem: shared memory when A and V fit.
 void jacobi_svd(skema_ctx* c, double* A, double* V, int64_t k, int max_sweeps, double tol, int* sweeps_out) {
   const size_t smem = sizeof(double) * (size_t)(2 * k * k);
-  if (smem <= 200 * 1024) {  // k <= 114: at most 57 pairs per round
-    // A: a half-warp per pair of a round; V: eight lanes per pair, in the
-    // warps left of 1024 threads (at least 3)
-    const int npairs = (int)((k + 1) / 2);
-    const int awarps = (npairs + 1) / 2;
-    const int vwarps = std::max(3, std::min(32 - awarps, (npairs + 3) / 4));
-    SKEMA_CUDA(cudaFuncSetAttribute(jacobi_svd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    jacobi_svd_kernel<<<1, 32 * (awarps + vwarps), smem, c->stream>>>(A, V, (int)k, max_sweeps, tol, sweeps_out,
-                                                                     awarps);
+  // a half-warp per pair of a round: (k + 1) / 2 pairs, at most 64 at a time
+  const int threads = (int)std::min<int64_t>(1024, ((k + 1) / 2 * 16 + 31) / 32 * 32);
+  if (smem <= 200 * 1024) {
+    SKEMA_CUDA(cudaFuncSetAttribute(jacobi_svd_kernel_t<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem));
+    jacobi_svd_kernel_t<true><<<1, threads, smem, c->stream>>>(A, V, k, max_sweeps, tol, sweeps_out);
     SKEMA_LAUNCHED(c);
     return;
   }
@@ -1114,12 +1078,9 @@ void trsm_upper(skema_ctx* c, const double* R, int64_t k, double* B, int64_t ldb
 void chol_inverse(skema_ctx* c, double* G, int64_t k, double* R, double* Rinv, int* st) {
   if (k <= kPackedMaxK) {
     const size_t smem = packed_smem_bytes(k);
-    // 8 warps up to k = 128 (at most 64 columns of trailing update per
-    // warp and step), 32 above
-    const int threads = k <= 128 ? 256 : 1024;
     auto launch = [&](auto kern) {
       SKEMA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      kern<<<1, threads, smem, c->stream>>>(G, (int)k, R, Rinv, st);
+      kern<<<1, 1024, smem, c->stream>>>(G, (int)k, R, Rinv, st);
     };
     if (k <= 32)
       launch(chol_factor_kernel<1>);
