@@ -110,28 +110,16 @@ __device__ __forceinline__ bool mbar_try(uint64_t* b, uint32_t parity) {
   return ok != 0;
 }
 // Bounded wait; false on time-out or when another thread already failed.
-// try_wait itself suspends the thread until the phase completes or a short
-// system time limit passes, so the loop polls the status word and the
-// clock (global loads, an L2 round trip each) only every eighth try: a
-// phase that completes during such a load would otherwise be seen that
-// much later.
 __device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, int* err) {
   if (mbar_try(b, parity)) return true;
-  unsigned long long t0 = 0, limit = 0;
-  bool timed = false;
-  for (uint32_t i = 1;; ++i) {
+  const unsigned long long t0 = now_ns();
+  const unsigned long long limit = *reinterpret_cast<const unsigned long long*>(err + 2);
+  while (true) {
     if (mbar_try(b, parity)) return true;
-    if ((i & 7) == 0) {
-      if (*(volatile int*)err) return false;
-      const unsigned long long t = now_ns();
-      if (!timed) {
-        t0 = t;
-        limit = *reinterpret_cast<const unsigned long long*>(err + 2);
-        timed = true;
-      } else if (t - t0 > limit) {
-        atomicExch(err, 1);
-        return false;
-      }
+    if (*(volatile int*)err) return false;
+    if (now_ns() - t0 > limit) {
+      atomicExch(err, 1);
+      return false;
     }
   }
 }
