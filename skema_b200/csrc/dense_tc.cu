@@ -321,17 +321,19 @@ void launch_gemm(skema_ctx* c, const CUtensorMap& ta, const CUtensorMap& tb, int
 }
 
 // X^T product straight from the FP32 window (converts it and writes A16).
-template <bool AROW, int S1, int S2>
+template <bool AROW, int S1, int S2, bool STT>
 void launch_gemm_a32_s(skema_ctx* c, const CUtensorMap& ta32, const CUtensorMap& tb, const CUtensorMap& ta16,
                        int64_t M, int64_t N, int64_t K, Plan pl, const tc::OutSpec& o, uint32_t* amax) {
   constexpr uint32_t STAGE = ((tc::BM * tc::BK * 2 + kNT * tc::BK * 2 + 1023) / 1024) * 1024;
   const size_t smem = (size_t)S1 * tc::BM * tc::BK * 4 + (size_t)S2 * STAGE + 1024 + 256;
-  auto kern = amax ? tc::gemm_a32_kernel<kNT, S1, S2, AROW, true> : tc::gemm_a32_kernel<kNT, S1, S2, AROW, false>;
+  auto kern = amax ? tc::gemm_a32_kernel<kNT, S1, S2, AROW, true, STT>
+                   : tc::gemm_a32_kernel<kNT, S1, S2, AROW, false, STT>;
   SKEMA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int grid = 0;
   const tc::Grid3 g = grid_of(c, M, N, K, kNT, tc::BK, pl, 1, &grid);
   if (grid <= 0) return;
-  kern<<<grid, tc::kThreadsA32, smem, c->stream>>>(ta32, tb, ta16, g, o, amax, c->dev_err);
+  kern<<<grid, STT ? tc::kThreadsA32St : tc::kThreadsA32, smem, c->stream>>>(ta32, tb, ta16, g, o, amax,
+                                                                            c->dev_err);
   SKEMA_LAUNCHED(c);
   c->dev_err_armed = true;
 }
@@ -343,7 +345,10 @@ void launch_gemm_a32_s(skema_ctx* c, const CUtensorMap& ta32, const CUtensorMap&
 template <bool AROW>
 void launch_gemm_a32(skema_ctx* c, const CUtensorMap& ta32, const CUtensorMap& tb, const CUtensorMap& ta16,
                      int64_t M, int64_t N, int64_t K, Plan pl, const tc::OutSpec& o, uint32_t* amax) {
-  launch_gemm_a32_s<AROW, 3, 3>(c, ta32, tb, ta16, M, N, K, pl, o, amax);
+  if (c->xt_store_thread)
+    launch_gemm_a32_s<AROW, 3, 3, true>(c, ta32, tb, ta16, M, N, K, pl, o, amax);
+  else
+    launch_gemm_a32_s<AROW, 3, 3, false>(c, ta32, tb, ta16, M, N, K, pl, o, amax);
 }
 
 // ---- FP8 form -------------------------------------------------------------

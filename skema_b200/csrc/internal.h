@@ -144,6 +144,10 @@ struct skema_ctx {
   // Nonzeros each lane of that kernel loads ahead per step (2, 4, 6 or 8);
   // SKEMA_SSIGN_BATCH overrides the default.
   int ssign_batch = 4;
+  // X^T product from an FP32 window: a thread of its own issues the BF16
+  // window copy's stores (true) or a converter thread does (false);
+  // SKEMA_XT_STORE_THREAD=1|0 overrides the default.
+  bool xt_store_thread = false;
   int cc_major = 0, cc_minor = 0;
   // BF16 tensor-core form: Omega~ and Psi~ stacked as one (k+s) x n
   // row-major operand (ld_op16), Upsilon~ / Phi~ copies in Map::lowp with

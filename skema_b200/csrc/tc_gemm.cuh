@@ -677,10 +677,16 @@ __global__ void __launch_bounds__(kThreads, 1)
 // A tile has read it. (Copying the tile out with plain 16-byte stores
 // measured slower both from the converter threads, with 4 FP32 + 2 BF16
 // stages, by 9 %, and from a warp of its own, by 27 %.)
+//   STT = false: converter thread 0 issues each A tile's TMA store after
+//                its stage is full and releases a stage one store later.
+//   STT = true:  warp 11's first lane does it: it waits for the stage to
+//                be full, issues the store, waits for the store to have
+//                read the stage and releases it at once.
 constexpr int kThreadsA32 = 352;
+constexpr int kThreadsA32St = 384;
 
-template <int NT, int S1, int S2, bool AROW, bool AMAX>
-__global__ void __launch_bounds__(kThreadsA32, 1)
+template <int NT, int S1, int S2, bool AROW, bool AMAX, bool STT>
+__global__ void __launch_bounds__(kThreadsA32St, 1)
     gemm_a32_kernel(const __grid_constant__ CUtensorMap tmA32, const __grid_constant__ CUtensorMap tmB,
                     const __grid_constant__ CUtensorMap tmA16, Grid3 g, OutSpec o, uint32_t* amax, int* err) {
   constexpr uint32_t A32_BYTES = BM * BK * 4;  // 32 KB
@@ -869,7 +875,7 @@ __global__ void __launch_bounds__(kThreadsA32, 1)
         fence_proxy_async();
         mbar_arrive(f32empty + s1);
         mbar_arrive(full + s2);
-        if (ct == 0) {
+        if (!STT && ct == 0) {
           // all 128 lines written (and the B tile landed): store the BF16
           // tile. The stage is released once TMA has read it; that is waited
           // for one stage later (the store before this one must be read by
@@ -890,7 +896,7 @@ __global__ void __launch_bounds__(kThreadsA32, 1)
         }
       }
     }
-    if (ct == 0) {
+    if (!STT && ct == 0) {
       bulk_wait_all();
       if (pend >= 0) mbar_arrive(empty + pend);
     }
@@ -902,6 +908,30 @@ __global__ void __launch_bounds__(kThreadsA32, 1)
       const uint32_t wm = __reduce_max_sync(0xffffffffu, __float_as_uint(mx));
       if ((ct & 31) == 0) atomicMax(amax, wm);
     }
+  } else if (STT && warp == 11 && lane == 0) {
+    // ---------------- A16 store thread ----------------
+    uint32_t it = 0;
+    bool ok = true;
+    Sched sc;
+    sched_init(g, sc);
+    int mt, nt, kt0, kt1;
+    while (ok && next_seg(g, sc, mt, nt, kt0, kt1)) {
+      const int KT = kt1 - kt0;
+      for (int kt = 0; kt < KT; ++kt, ++it) {
+        const int s2 = it % S2;
+        const uint32_t ph2 = (it / S2) & 1;
+        if (!mbar_wait(full + s2, ph2, err)) {
+          ok = false;
+          break;
+        }
+        fence_proxy_async();
+        tma_store_3d(&tmA16, stbf + s2 * STAGE, 0, mt * BM, kt0 + kt);
+        bulk_commit();
+        bulk_wait_read_all();
+        mbar_arrive(empty + s2);
+      }
+    }
+    bulk_wait_all();
   } else if (warp < 4) {
     // ---------------- epilogue ----------------
     uint32_t tcount = 0;
