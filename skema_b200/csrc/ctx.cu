@@ -406,7 +406,7 @@ int skema_create(const skema_params* p, skema_ctx** out) {
     c->ssign_bin_kb = 128;
     if (const char* v = std::getenv("SKEMA_SSIGN_BIN_KB")) c->ssign_bin_kb = std::min(220, std::max(16, std::atoi(v)));
     c->ssign_batch = 4;
-    c->xt_store_thread = false;
+    c->xt_store_thread = true;
     if (const char* v = std::getenv("SKEMA_XT_STORE_THREAD")) c->xt_store_thread = std::atoi(v) != 0;
     if (const char* v = std::getenv("SKEMA_SSIGN_BATCH")) c->ssign_batch = std::atoi(v);
     plan_maps(c);
