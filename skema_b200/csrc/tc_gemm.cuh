@@ -668,7 +668,7 @@ __global__ void __launch_bounds__(kThreads, 1)
 //                 {32 columns, 64 rows}.
 // Threads: warps 0-3 epilogue, warp 4 TMA producer of the FP32 tiles,
 // warp 5 MMA issuer, warps 6-9 converters, warp 10 TMA producer of the B
-// tiles. The two producers are separate so that the FP32 loads run up to S1
+// tiles, warp 11 (STT) the A16 store thread. The two producers are separate so that the FP32 loads run up to S1
 // stages ahead whatever the state of the BF16 ring (one thread issuing
 // both waited for a free BF16 stage before each next FP32 load, which kept
 // fewer FP32 loads in flight). Rings: S1 FP32 stages (producer -> converters) and
