@@ -751,21 +751,21 @@ __global__ void colsparse_apply_smem_kernel(const uint32_t* __restrict__ mp, int
 // V accumulated (column-major k x k). One CTA; each half-warp rotates one
 // pair of a round-robin round, and a sweep ends the loop when it made no
 // rotation (every pair within tol of orthogonal).
-// SMEM: A and V are worked on in shared memory (2 k^2 doubles), copied in at
-// the start and out at the end; every rotation reads and writes two columns
-// of each, so global memory would put an L2 round trip on every step.
-template <bool SMEM>
-__global__ void __launch_bounds__(1024) jacobi_svd_kernel_t(double* Ag, double* Vg, int64_t k64, int max_sweeps,
+// A and V are worked on in shared memory (2 k^2 doubles, k <= 114), copied
+// in at the start and out at the end; every rotation reads and writes two
+// columns of each, so global memory would put an L2 round trip on every
+// step.
+__global__ void __launch_bounds__(1024) jacobi_svd_kernel(double* Ag, double* Vg, int64_t k64, int max_sweeps,
                                                             double tol, int* sweeps_out) {
   __shared__ int rotated;
   extern __shared__ double jac_smem[];
   const int k = (int)k64;
-  double* A = SMEM ? jac_smem : Ag;
-  double* V = SMEM ? jac_smem + (size_t)k * k : Vg;
-  if (SMEM) {
-    for (int q = threadIdx.x; q < k * k; q += blockDim.x) A[q] = Ag[q];
+  double* A = jac_smem;
+  double* V = jac_smem + (size_t)k * k;
+  for (int q = threadIdx.x; q < k * k; q += blockDim.x) {
+    A[q] = Ag[q];
+    V[q] = (q % k == q / k) ? 1.0 : 0.0;
   }
-  for (int q = threadIdx.x; q < k * k; q += blockDim.x) V[q] = (q % k == q / k) ? 1.0 : 0.0;
   // a pair per half-warp: 64 pairs at a time, all of them for k <= 128
   const int hl = threadIdx.x & 15, slot = threadIdx.x >> 4, nslot = blockDim.x >> 4;
   const unsigned hmask = (threadIdx.x & 16) ? 0xffff0000u : 0x0000ffffu;
@@ -838,12 +838,10 @@ __global__ void __launch_bounds__(1024) jacobi_svd_kernel_t(double* Ag, double* 
     if (!more) break;
   }
   if (threadIdx.x == 0) sweeps_out[0] = sweep;
-  if (SMEM) {
-    __syncthreads();
-    for (int q = threadIdx.x; q < k * k; q += blockDim.x) {
-      Ag[q] = A[q];
-      Vg[q] = V[q];
-    }
+  __syncthreads();
+  for (int q = threadIdx.x; q < k * k; q += blockDim.x) {
+    Ag[q] = A[q];
+    Vg[q] = V[q];
   }
 }
 
@@ -983,9 +981,8 @@ void jacobi_svd(skema_ctx* c, double* A, double* V, int64_t k, int max_sweeps, d
   // a half-warp per pair of a round: (k + 1) / 2 pairs, at most 64 at a time
   const int threads = (int)std::min<int64_t>(1024, ((k + 1) / 2 * 16 + 31) / 32 * 32);
   if (smem <= 200 * 1024) {
-    SKEMA_CUDA(cudaFuncSetAttribute(jacobi_svd_kernel_t<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)smem));
-    jacobi_svd_kernel_t<true><<<1, threads, smem, c->stream>>>(A, V, k, max_sweeps, tol, sweeps_out);
+    SKEMA_CUDA(cudaFuncSetAttribute(jacobi_svd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    jacobi_svd_kernel<<<1, threads, smem, c->stream>>>(A, V, k, max_sweeps, tol, sweeps_out);
     SKEMA_LAUNCHED(c);
     return;
   }
