@@ -11,6 +11,7 @@ from .sketchy import (
     rbf_sketch_vjp,
     read_crs_rows,
     read_matrix,
+    read_reference_map_dump,
     sketchysvd,
     write_matrix,
 )
@@ -24,6 +25,7 @@ __all__ = [
     "sketchysvd",
     "read_matrix",
     "read_crs_rows",
+    "read_reference_map_dump",
     "write_matrix",
     "rbf_sketch_fwd",
     "rbf_sketch_vjp",

@@ -611,6 +611,23 @@ class _Context:
         self._check(self.lib.skema_map_export(self.h, which, vals.ctypes.data, idx.ctypes.data))
         return vals, idx
 
+    def map_import_reference_dumps(self, stem):
+        """Import the four maps from the reference's --debug-file dumps
+        <stem>_{Upsilon,Omega,Phi,Psi}.{txt,mtx} (one map for SketchySPD:
+        Omega), read by read_reference_map_dump in this context's stored
+        orientation."""
+        import os
+
+        for which, label in MAP_LABELS.items():
+            if self.spd and which != L.OMEGA:
+                continue
+            nr, nc, z, _ = self.map_info(which)
+            path = f"{stem}_{label}.mtx" if z else f"{stem}_{label}.txt"
+            if not os.path.exists(path):
+                raise FileNotFoundError(path)
+            vals, idx = read_reference_map_dump(path, nr, nc)
+            self.map_import(which, vals, idx)
+
     def map_import(self, which, values, indices=None):
         nr, nc, z, _ = self.map_info(which)
         if z == 0:
@@ -748,6 +765,55 @@ def read_matrix(path, sparse: bool | None = None):
     finally:
         lib.skema_dense_free(C.byref(d))
     return out
+
+
+MAP_LABELS = {L.UPSILON: "Upsilon", L.OMEGA: "Omega", L.PHI: "Phi", L.PSI: "Psi"}
+
+
+def read_reference_map_dump(path, nrow: int, ncol: int):
+    """A map written by the reference's --debug-file dumps
+    (src/Skema_DimRedux.hpp:124-127, 264-267; formats of Impl::write,
+    src/Skema_Common.hpp:175-190), in its stored orientation nrow x ncol:
+      <stem>_<label>.txt  GaussDimRedux: nrow lines of ncol values;
+      <stem>_<label>.mtx  SparseSignDimRedux: a MatrixMarket coordinate file
+                          (1-based), zeta entries per row kept as stored
+                          (repeated columns are not merged).
+    Returns (values, None) for Gauss (nrow x ncol float64) and
+    (values, indices) (nrow x zeta) for SparseSign, the map_import forms."""
+    p = str(path)
+    if p.lower().endswith(".txt"):
+        vals = np.loadtxt(p, dtype=np.float64, ndmin=2)
+        if vals.shape != (nrow, ncol):
+            raise ValueError(f"{p}: {vals.shape} values, the map is {nrow} x {ncol}")
+        return vals, None
+    rows, cols, vs = [], [], []
+    with open(p) as f:
+        header = f.readline().lower()
+        if "coordinate" not in header:
+            raise ValueError(f"{p}: not a MatrixMarket coordinate file")
+        line = f.readline()
+        while line.startswith("%") or not line.strip():
+            line = f.readline()
+        nr, nc, nnz = (int(t) for t in line.split()[:3])
+        if (nr, nc) != (nrow, ncol):
+            raise ValueError(f"{p}: {nr} x {nc}, the map is {nrow} x {ncol}")
+        for line in f:
+            t = line.split()
+            if not t or t[0].startswith("%"):
+                continue
+            rows.append(int(t[0]) - 1)
+            cols.append(int(t[1]) - 1)
+            vs.append(float(t[2]) if len(t) > 2 else 1.0)
+    if len(rows) != nnz or nnz % max(nrow, 1):
+        raise ValueError(f"{p}: {len(rows)} entries, not the same count in every one of {nrow} rows")
+    zeta = nnz // nrow
+    order = np.argsort(np.asarray(rows), kind="stable")  # rows in file order within each row
+    r = np.asarray(rows)[order]
+    if np.any(r != np.repeat(np.arange(nrow), zeta)):
+        raise ValueError(f"{p}: rows do not all hold {zeta} entries")
+    idx = np.asarray(cols, dtype=np.int32)[order].reshape(nrow, zeta)
+    val = np.asarray(vs, dtype=np.float64)[order].reshape(nrow, zeta)
+    return val, idx
 
 
 def read_crs_rows(path, row0: int = 0, nrows: int = -1):
