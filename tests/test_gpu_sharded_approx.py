@@ -158,3 +158,35 @@ def test_sharded_approx_reports_a_failed_allreduce(sk):
         assert ei.value.status == 9  # SKEMA_ECOLLECTIVE
         U, S, V = s.low_rank_approx()  # the context stays usable
         assert np.all(np.isfinite(S))
+
+
+def test_torch_distributed_callback_on_one_rank(sk):
+    # the torch.distributed binding (NCCL all_reduce on the library's device
+    # buffers) in a one-rank group: the sharded call over all rows equals
+    # the single-context approximation
+    import os
+    import socket
+
+    import torch.distributed as dist
+
+    from skema_b200 import distributed
+
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+    os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+    os.environ["MASTER_PORT"] = str(port)
+    rng = np.random.default_rng(5)
+    m, n = 2000, 600
+    A = (rng.standard_normal((m, 20)) @ rng.standard_normal((20, n))).astype(np.float32)
+    a = sk.AlgParams(matrix_m=m, matrix_n=n, rank=8, window=256, dim_redux=0)
+    dist.init_process_group("nccl", rank=0, world_size=1)
+    try:
+        with sk.SketchySVD(a) as s:
+            s.update_rows(A)
+            U0, S0, V0 = s.low_rank_approx()
+            U, S, V = distributed.low_rank_approx_sharded(s, m, 256)
+        assert np.max(np.abs(S - S0)) <= 1e-12 * S0[0]
+        assert np.max(np.abs(U - U0)) <= 1e-9 and np.max(np.abs(V - V0)) <= 1e-9
+    finally:
+        dist.destroy_process_group()
