@@ -14,6 +14,7 @@ from .sketchy import (
     read_reference_map_dump,
     sketchysvd,
     write_matrix,
+    write_reference_map_dump,
 )
 
 __all__ = [
@@ -27,6 +28,7 @@ __all__ = [
     "read_crs_rows",
     "read_reference_map_dump",
     "write_matrix",
+    "write_reference_map_dump",
     "rbf_sketch_fwd",
     "rbf_sketch_vjp",
     "SkemaError",

@@ -362,6 +362,26 @@ class _Context:
         self._check(self.lib.skema_get_dims(self.h, C.byref(k), C.byref(s), C.byref(spd)))
         self.range, self.core, self.spd = k.value, s.value, bool(spd.value)
         self.nrow, self.ncol, self.rank = alg.matrix_m, alg.matrix_n, alg.rank
+        stem = self.debug_stem()
+        if stem:
+            self.map_export_reference_dumps(stem)
+
+    def debug_stem(self):
+        """The stem of AlgParams.debug_filename, or None. Like the reference's
+        --debug-file dumps (debug_filename.filename().stem(),
+        src/Skema_DimRedux.hpp:124-127, src/Skema_SketchySVD.cpp:192-205), the
+        files are written as <stem>_<name> in the working directory."""
+        import os
+
+        f = getattr(self.alg, "debug_filename", "")
+        return os.path.splitext(os.path.basename(str(f)))[0] if f else None
+
+    def dump_sketches(self, stem, suffix=""):
+        """<stem>_X.txt, _Y.txt, _Z.txt (SketchySPD: _Y.txt) with the given
+        suffix, in the reference's text format (write_dense_text)."""
+        names = ((L.SKETCH_Y, "Y"),) if self.spd else ((L.SKETCH_X, "X"), (L.SKETCH_Y, "Y"), (L.SKETCH_Z, "Z"))
+        for which, name in names:
+            write_dense_text(f"{stem}_{name}.txt{suffix}", self.get_sketch(which))
 
     def _check(self, st):
         if st != L.OK:
@@ -470,21 +490,37 @@ class _Context:
         the rows go one window at a time and the top-rank singular values
         after each window are kept as self.traces[str(w)]["svals"]
         (src/Skema_SketchySVD.cpp:164-216); the approximation here does not
-        overwrite Y, so the later windows see the true sketch."""
+        overwrite Y, so the later windows see the true sketch.
+        With AlgParams.debug_filename the sketches are written after every
+        window (<stem>_X.txt.<w>, _Y.txt.<w>, _Z.txt.<w>) and at the end
+        (<stem>_X.txt, ...), as src/Skema_SketchySVD.cpp:191-205, 235-245
+        write them; SketchySPD writes <stem>_Y.txt at the end only
+        (src/Skema_SketchySVD.cpp:880-885). A single window of all rows
+        writes none, as the reference returns before its dumps."""
         self.reset()
         self.traces = {}
         W = int(self.alg.window)
-        if not getattr(self.alg, "sketch_compute_svals_iters", False) or W >= self.nrow or self.spd:
+        stem = self.debug_stem()
+        iters = bool(getattr(self.alg, "sketch_compute_svals_iters", False)) and not self.spd
+        if W >= self.nrow:
             self.update_rows(A, 0, None)
             return
-        for w, r0 in enumerate(range(0, self.nrow, W)):
-            wr = min(W, self.nrow - r0)
-            if self.alg.kernel_func == L.KERNEL_GAUSSRBF:
-                self.update_rows(A, r0, wr)
-            else:
-                self.update_rows(_row_block(A, r0, wr), r0, wr)
-            S = self.low_rank_approx()[1]
-            self.traces[str(w)] = {"svals": [float(x) for x in S]}
+        if self.spd or not (iters or stem):
+            self.update_rows(A, 0, None)
+        else:
+            for w, r0 in enumerate(range(0, self.nrow, W)):
+                wr = min(W, self.nrow - r0)
+                if self.alg.kernel_func == L.KERNEL_GAUSSRBF:
+                    self.update_rows(A, r0, wr)
+                else:
+                    self.update_rows(_row_block(A, r0, wr), r0, wr)
+                if stem:
+                    self.dump_sketches(stem, f".{w}")
+                if iters:
+                    S = self.low_rank_approx()[1]
+                    self.traces[str(w)] = {"svals": [float(x) for x in S]}
+        if stem:
+            self.dump_sketches(stem)
 
     def synchronize(self):
         self._check(self.lib.skema_synchronize(self.h))
@@ -610,6 +646,18 @@ class _Context:
         idx = np.empty((nr, z), dtype=np.int32)
         self._check(self.lib.skema_map_export(self.h, which, vals.ctypes.data, idx.ctypes.data))
         return vals, idx
+
+    def map_export_reference_dumps(self, stem):
+        """Write the maps as the reference's --debug-file dumps
+        <stem>_{Upsilon,Omega,Phi,Psi}.{txt,mtx} (SketchySPD: Omega), in this
+        context's stored orientation (write_reference_map_dump); the files
+        read back with map_import_reference_dumps."""
+        for which, label in MAP_LABELS.items():
+            if self.spd and which != L.OMEGA:
+                continue
+            _, nc, z, _ = self.map_info(which)
+            vals, idx = self.map_export(which)
+            write_reference_map_dump(f"{stem}_{label}.mtx" if z else f"{stem}_{label}.txt", vals, idx, nc)
 
     def map_import_reference_dumps(self, stem):
         """Import the four maps from the reference's --debug-file dumps
@@ -770,6 +818,40 @@ def read_matrix(path, sparse: bool | None = None):
 MAP_LABELS = {L.UPSILON: "Upsilon", L.OMEGA: "Omega", L.PHI: "Phi", L.PSI: "Psi"}
 
 
+def write_dense_text(path, M):
+    """Impl::write of a matrix or a vector (src/Skema_Common.hpp:164-184):
+    a matrix as one line per row, each entry "%.16f " ; a vector as one
+    "%.16f" value per line."""
+    a = np.asarray(M, dtype=np.float64)
+    with open(str(path), "w") as f:
+        if a.ndim == 1:
+            np.savetxt(f, a, fmt="%.16f", newline="\n")
+        else:
+            np.savetxt(f, a, fmt="%.16f", delimiter=" ", newline=" \n")
+
+
+def write_reference_map_dump(path, values, indices=None, ncol=None):
+    """A map in the reference's --debug-file dump formats (the writer side of
+    read_reference_map_dump): Gauss values (nrow x ncol) as text lines of
+    write_dense_text; SparseSign (values, indices), zeta entries per stored
+    row, as a MatrixMarket coordinate file with 1-based indices, the entries
+    of a row in stored order (repeated columns kept), ncol columns."""
+    if indices is None:
+        write_dense_text(path, values)
+        return
+    v = np.asarray(values, dtype=np.float64)
+    ix = np.asarray(indices, dtype=np.int64)
+    nr, z = v.shape
+    if ncol is None:
+        ncol = int(ix.max()) + 1 if ix.size else 0
+    rows = np.repeat(np.arange(1, nr + 1, dtype=np.int64), z)
+    with open(str(path), "w") as f:
+        f.write("%%MatrixMarket matrix coordinate real general\n")
+        f.write(f"{nr} {int(ncol)} {nr * z}\n")
+        for r, c, x in zip(rows.tolist(), (ix.reshape(-1) + 1).tolist(), v.reshape(-1).tolist()):
+            f.write(f"{r} {c} {x:.17g}\n")
+
+
 def read_reference_map_dump(path, nrow: int, ncol: int):
     """A map written by the reference's --debug-file dumps
     (src/Skema_DimRedux.hpp:124-127, 264-267; formats of Impl::write,
@@ -893,6 +975,11 @@ def sketchysvd(matrix, alg: AlgParams):
         sk.compute_residuals(matrix)
         if getattr(alg, "history_filename", ""):
             sk.save_history(alg.history_filename)
+        stem = sk.debug_stem()
+        if stem:  # src/Skema_SketchySVD.cpp:1386-1404, 1559-1576
+            for name, M in (("U", U), ("S", S), ("V", V)):
+                if M is not None and np.asarray(M).size:
+                    write_dense_text(f"{stem}_{name}.txt", M)
         return U, S, V
 
 

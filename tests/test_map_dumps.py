@@ -67,3 +67,30 @@ def test_sparse_dump_keeps_rows_and_repeats(sk, tmp_path):
         f.write("\n".join(lines[:2] + lines[2:-1]) + "\n")
     with pytest.raises(ValueError):
         sk.read_reference_map_dump(perm, nrow, ncol)
+
+
+def test_library_writers_use_the_reference_formats(sk, tmp_path):
+    from skema_b200.sketchy import write_dense_text, write_reference_map_dump
+
+    rng = np.random.default_rng(2)
+    # Gauss: byte for byte the "%.16f " lines of Impl::write
+    M = rng.uniform(-3, 3, size=(5, 11))
+    write_reference_map_dump(str(tmp_path / "a_Omega.txt"), M)
+    write_gauss_dump(str(tmp_path / "b_Omega.txt"), M)
+    assert open(tmp_path / "a_Omega.txt").read() == open(tmp_path / "b_Omega.txt").read()
+    # a vector: one "%.16f" value per line
+    v = rng.standard_normal(6)
+    write_dense_text(str(tmp_path / "run_S.txt"), v)
+    assert open(tmp_path / "run_S.txt").read() == "".join("%.16f\n" % x for x in v)
+    # SparseSign: a coordinate file that reads back exactly, repeats kept
+    nrow, ncol, zeta = 13, 7, 8
+    idx = rng.integers(0, ncol, size=(nrow, zeta)).astype(np.int32)
+    idx[::3, 2] = idx[::3, 1]
+    val = np.where(rng.random((nrow, zeta)) < 0.5, -1.0, 1.0)
+    p = str(tmp_path / "run_Psi.mtx")
+    write_reference_map_dump(p, val, idx, ncol)
+    lines = open(p).read().splitlines()
+    assert lines[0] == "%%MatrixMarket matrix coordinate real general"
+    assert lines[1] == f"{nrow} {ncol} {nrow * zeta}"
+    v2, i2 = sk.read_reference_map_dump(p, nrow, ncol)
+    assert np.array_equal(i2, idx) and np.array_equal(v2, val)
