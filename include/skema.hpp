@@ -35,6 +35,7 @@
 #include <cmath>
 #include <cstddef>
 #include <cstdint>
+#include <cstdio>
 #include <cstdlib>
 #include <filesystem>
 #include <fstream>
@@ -548,6 +549,59 @@ inline crs_matrix_type read_matrix<crs_matrix_type>(const std::filesystem::path&
   return A;
 }
 
+// ---- --debug-file dumps ----------------------------------------------------
+namespace detail {
+inline FILE* open_dump(const std::string& fname) {
+  FILE* f = std::fopen(fname.c_str(), "w");
+  if (!f) throw std::runtime_error("skema: cannot write " + fname);
+  return f;
+}
+// Impl::write (src/Skema_Common.hpp:164-184): a matrix as one line per row of
+// "%.16f " entries, a vector as one "%.16f" value per line.
+inline void write_text(const std::string& fname, const matrix_type& A) {
+  FILE* f = open_dump(fname);
+  for (size_type i = 0; i < A.extent(0); ++i) {
+    for (size_type j = 0; j < A.extent(1); ++j) std::fprintf(f, "%.16f ", A(i, j));
+    std::fprintf(f, "\n");
+  }
+  std::fclose(f);
+}
+inline void write_text(const std::string& fname, const vector_type& v) {
+  FILE* f = open_dump(fname);
+  for (size_type i = 0; i < v.extent(0); ++i) std::fprintf(f, "%.16f\n", v(i));
+  std::fclose(f);
+}
+// A map as the reference's constructors dump it (src/Skema_DimRedux.hpp:
+// 124-127, 264-267): Gauss values (nr x nc, column-major) to <stem>_<label>.txt
+// as write_text lines; SparseSign (z entries per stored row, row-major) to
+// <stem>_<label>.mtx as a MatrixMarket coordinate file with 1-based indices,
+// a row's entries in stored order (repeated columns kept).
+inline void write_map_dump(const std::string& stem, const std::string& label, int64_t nr, int64_t nc, int z,
+                           const std::vector<double>& vals, const std::vector<int32_t>& idx) {
+  if (z == 0) {
+    FILE* f = open_dump(stem + "_" + label + ".txt");
+    for (int64_t i = 0; i < nr; ++i) {
+      for (int64_t j = 0; j < nc; ++j) std::fprintf(f, "%.16f ", vals[(size_t)(i + j * nr)]);
+      std::fprintf(f, "\n");
+    }
+    std::fclose(f);
+    return;
+  }
+  FILE* f = open_dump(stem + "_" + label + ".mtx");
+  std::fprintf(f, "%%%%MatrixMarket matrix coordinate real general\n");
+  std::fprintf(f, "%lld %lld %lld\n", (long long)nr, (long long)nc, (long long)nr * z);
+  for (int64_t i = 0; i < nr; ++i)
+    for (int t = 0; t < z; ++t)
+      std::fprintf(f, "%lld %d %.17g\n", (long long)(i + 1), idx[(size_t)(i * z + t)] + 1, vals[(size_t)(i * z + t)]);
+  std::fclose(f);
+}
+// The file stem of --debug-file (debug_filename.filename().stem()); the
+// dumps go to the working directory, as the reference writes them.
+inline std::string debug_stem(const std::filesystem::path& debug_filename) {
+  return debug_filename.empty() ? std::string() : debug_filename.filename().stem().string();
+}
+}  // namespace detail
+
 // ---- DimRedux (src/Skema_DimRedux.hpp:60-268) -----------------------------
 struct DimReduxStats {
   scalar_type initialize{0.0};
@@ -569,6 +623,13 @@ class DimRedux {
     if (st != SKEMA_OK) detail::check(st, "skema_dimredux_create failed");
     map_ = std::shared_ptr<skema_dimredux>(h, Free{});
     stats.initialize = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (!debug_filename.empty()) {
+      std::vector<double> v;
+      std::vector<int32_t> ix;
+      export_map(v, ix);
+      const int z = KIND == SKEMA_MAP_SPARSE_SIGN ? (int)(v.size() / std::max<size_type>(nrow, 1)) : 0;
+      detail::write_map_dump(detail::debug_stem(debug_filename), label, (int64_t)nrow, (int64_t)ncol, z, v, ix);
+    }
   }
 
   // lmap: for a dense B, op(M(:, idx)) op(B), where op(M) is transposed when
@@ -773,6 +834,23 @@ class Context {
   static size_type rows_of(const matrix_type& A) { return A.extent(0); }
   static size_type rows_of(const crs_matrix_type& A) { return A.numRows(); }
 
+  // The context's maps as the reference's --debug-file dumps, in their
+  // stored orientation (SketchySPD: Omega only).
+  void dump_maps(const std::string& stem) const {
+    static const std::pair<int32_t, const char*> maps[4] = {
+        {SKEMA_UPSILON, "Upsilon"}, {SKEMA_OMEGA, "Omega"}, {SKEMA_PHI, "Phi"}, {SKEMA_PSI, "Psi"}};
+    for (const auto& [which, label] : maps) {
+      if (spd_ && which != SKEMA_OMEGA) continue;
+      int64_t nr = 0, nc = 0;
+      int32_t z = 0, tr = 0;
+      check_ctx(skema_map_info(get(), which, &nr, &nc, &z, &tr), get());
+      std::vector<double> v((size_t)(z ? nr * z : nr * nc));
+      std::vector<int32_t> ix((size_t)(z ? nr * z : 0));
+      check_ctx(skema_map_export(get(), which, v.data(), z ? ix.data() : nullptr), get());
+      write_map_dump(stem, label, nr, nc, z, v, ix);
+    }
+  }
+
  private:
   struct Free {
     void operator()(skema_ctx* c) const { skema_destroy(c); }
@@ -837,27 +915,38 @@ class SketchySVD {
  public:
   explicit SketchySVD(const AlgParams& p)
       : nrow(p.matrix_m), ncol(p.matrix_n), rank(p.rank), eta(p.sketch_eta), nu(p.sketch_nu), algParams(p),
-        ctx_(p, DimReduxT::kind, false), range(ctx_.range()), core(ctx_.core()) {}
+        ctx_(p, DimReduxT::kind, false), range(ctx_.range()), core(ctx_.core()) {
+    if (!p.debug_filename.empty()) ctx_.dump_maps(detail::debug_stem(p.debug_filename));
+  }
 
   // SketchySVD::linear_update (src/Skema_SketchySVD.cpp:120-246): zero the
   // sketches, stream every row window; with sketch_compute_svals_iters the
-  // top-rank singular values after each window go to the traces.
+  // top-rank singular values after each window go to the traces. With
+  // --debug-file the sketches are written after every window
+  // (<stem>_X.txt.<w>, _Y.txt.<w>, _Z.txt.<w>) and at the end (<stem>_X.txt,
+  // ...), as src/Skema_SketchySVD.cpp:191-205, 235-245 write them; a single
+  // window of all rows writes none, as the reference returns first.
   void linear_update(const MatrixType& A) {
     const auto t0 = std::chrono::steady_clock::now();
     skema_ctx* c = ctx_.get();
     detail::check_ctx(skema_reset(c), c);
     const size_type m = algParams.kernel_func == Kernel_Map::GAUSSRBF ? nrow : detail::Context::rows_of(A);
     const size_type W = std::max<size_type>(1, algParams.window);
-    if (!algParams.sketch_compute_svals_iters || W >= m) {
+    const std::string stem = W < m ? detail::debug_stem(algParams.debug_filename) : std::string();
+    if (W >= m || (!algParams.sketch_compute_svals_iters && stem.empty())) {
       ctx_.stream(A, 0, m, false);
     } else {
       for (size_type r0 = 0, w = 0; r0 < m; r0 += W, ++w) {
         ctx_.stream(A, r0, std::min(W, m - r0), false);
-        const auto S = std::get<1>(low_rank_approx(false));
-        std::vector<double> sv(S.data(), S.data() + S.extent(0));
-        traces[std::to_string(w)]["svals"] = sv;
+        if (!stem.empty()) dump_sketches(stem, "." + std::to_string(w));
+        if (algParams.sketch_compute_svals_iters) {
+          const auto S = std::get<1>(low_rank_approx(false));
+          std::vector<double> sv(S.data(), S.data() + S.extent(0));
+          traces[std::to_string(w)]["svals"] = sv;
+        }
       }
     }
+    if (!stem.empty()) dump_sketches(stem, "");
     detail::check_ctx(skema_synchronize(c), c);
     timings["update"]["total"] = detail::seconds_since(t0);
   }
@@ -915,6 +1004,12 @@ class SketchySVD {
   skema_ctx* context() const { return ctx_.get(); }
 
  private:
+  void dump_sketches(const std::string& stem, const std::string& suffix) const {
+    detail::write_text(stem + "_X.txt" + suffix, sketch(SKEMA_SKETCH_X));
+    detail::write_text(stem + "_Y.txt" + suffix, sketch(SKEMA_SKETCH_Y));
+    detail::write_text(stem + "_Z.txt" + suffix, sketch(SKEMA_SKETCH_Z));
+  }
+
   const size_type nrow, ncol, rank;
   const scalar_type eta, nu;
   const AlgParams algParams;
@@ -931,9 +1026,13 @@ class SketchySPD {
  public:
   explicit SketchySPD(const AlgParams& p)
       : nrow(p.matrix_m), ncol(p.matrix_n), rank(p.rank), algParams(p), ctx_(p, DimReduxT::kind, true),
-        range(ctx_.range()) {}
+        range(ctx_.range()) {
+    if (!p.debug_filename.empty()) ctx_.dump_maps(detail::debug_stem(p.debug_filename));
+  }
 
-  // SketchySPD::linear_update (src/Skema_SketchySVD.cpp:790-886).
+  // SketchySPD::linear_update (src/Skema_SketchySVD.cpp:790-886); with
+  // --debug-file, Y is written to <stem>_Y.txt at the end (:880-885), except
+  // for a single window of all rows.
   void linear_update(const MatrixType& A) {
     const auto t0 = std::chrono::steady_clock::now();
     skema_ctx* c = ctx_.get();
@@ -941,7 +1040,18 @@ class SketchySPD {
     const size_type m = algParams.kernel_func == Kernel_Map::GAUSSRBF ? nrow : detail::Context::rows_of(A);
     ctx_.stream(A, 0, m, false);
     detail::check_ctx(skema_synchronize(c), c);
+    if (!algParams.debug_filename.empty() && std::max<size_type>(1, algParams.window) < m)
+      detail::write_text(detail::debug_stem(algParams.debug_filename) + "_Y.txt", sketch());
     timings["update"]["total"] = detail::seconds_since(t0);
+  }
+
+  // The sketch Y (m x k), FP32 from the device.
+  matrix_type sketch() const {
+    std::vector<float> f(nrow * range);
+    detail::check_ctx(skema_get_sketch(ctx_.get(), SKEMA_SKETCH_Y, f.data(), (int64_t)std::max<size_type>(nrow, 1),
+                                       SKEMA_COL_MAJOR, SKEMA_MEM_HOST),
+                      ctx_.get());
+    return detail::from_f32(f, nrow, range, "sketch");
   }
 
   // SketchySPD::low_rank_approx (src/Skema_SketchySVD.cpp:935-1151): the
@@ -1043,17 +1153,6 @@ void run_spd(const MatrixType& matrix, const AlgParams& algParams, matrix_type& 
   if (!algParams.history_filename.empty()) sketch.save_history(algParams.history_filename);
 }
 
-inline void write_text(const std::string& fname, const matrix_type& A) {
-  std::ofstream f(fname);
-  for (size_type i = 0; i < A.extent(0); ++i) {
-    for (size_type j = 0; j < A.extent(1); ++j) f << (j ? " " : "") << num(A(i, j));
-    f << "\n";
-  }
-}
-inline void write_text(const std::string& fname, const vector_type& v) {
-  std::ofstream f(fname);
-  for (size_type i = 0; i < v.extent(0); ++i) f << num(v(i)) << "\n";
-}
 }  // namespace detail
 
 // Skema::sketchysvd: update, fixed-rank approximation, residuals and the

@@ -87,3 +87,41 @@ def test_dimredux_products(cpp_bins):
     res = subprocess.run([cpp_bins["dimredux_check"]], capture_output=True, text=True, timeout=300)
     print(res.stdout)
     assert res.returncode == 0, res.stdout + res.stderr
+
+
+@pytest.mark.parametrize("model,kind", [("gauss", 0), ("sparse-sign", 1)])
+def test_driver_debug_file_dumps(cpp_bins, kat, tmp_path, model, kind):
+    # --debug-file: the maps at construction, the sketches after each of the
+    # seven 5-row windows and at the end, and U / S / V, as <stem>_<name> in
+    # the working directory; the map dumps equal the Python mirror's maps
+    # for the same parameters
+    import skema_b200 as sk
+
+    write_array_mtx(tmp_path / "rect.mtx", kat["rect_dense"])
+    h = run_driver(cpp_bins["sketch_driver"], tmp_path, ["--input", "rect.mtx", "--rank", "10", "--window", "5",
+                                                          "--range", "12", "--core", "25", "--model", model,
+                                                          "--debug-file", "out/dbg.json"])
+    for name in "XYZ":
+        for w in range(7):
+            assert (tmp_path / f"dbg_{name}.txt.{w}").exists()
+        assert np.array_equal(np.loadtxt(tmp_path / f"dbg_{name}.txt.6", ndmin=2),
+                              np.loadtxt(tmp_path / f"dbg_{name}.txt", ndmin=2))
+    assert not (tmp_path / "dbg_X.txt.7").exists()
+    S = np.loadtxt(tmp_path / "dbg_S.txt")
+    assert np.max(np.abs(S - np.array(h["svals"]))) <= 1e-15 * S[0]
+    assert np.loadtxt(tmp_path / "dbg_U.txt", ndmin=2).shape == (32, 10)
+    assert np.loadtxt(tmp_path / "dbg_V.txt", ndmin=2).shape == (14, 10)
+    a = sk.AlgParams(matrix_m=32, matrix_n=14, rank=10, window=5, sketch_range=12, sketch_core=25, dim_redux=kind)
+    with sk.SketchySVD(a) as s:
+        for which, label in sk.sketchy.MAP_LABELS.items():
+            nr, nc, z, _ = s.map_info(which)
+            vals, idx = sk.read_reference_map_dump(str(tmp_path / f"dbg_{label}{'.mtx' if z else '.txt'}"), nr, nc)
+            v0, i0 = s.map_export(which)
+            if z:
+                assert np.array_equal(idx, i0) and np.array_equal(vals, v0)
+            else:
+                assert np.max(np.abs(vals - v0)) <= 1e-15 * max(1.0, np.abs(v0).max())
+        # the final Y dump is the sketch of the same input through the mirror
+        s.linear_update(np.asarray(kat["rect_dense"], dtype=np.float32))
+        y = np.loadtxt(tmp_path / "dbg_Y.txt", ndmin=2)
+        assert np.max(np.abs(y - s.get_sketch(1))) <= 1e-5 * np.abs(y).max()
