@@ -904,6 +904,46 @@ inline void write_history(const std::filesystem::path& fname, const std::vector<
   }
 }
 
+// The reference's timing keys (src/Skema_SketchySVD.cpp:101-116 for
+// SketchySVD, :776-786 for SketchySPD), in seconds, from the library's
+// device stage timers; zero where no stage corresponds or none ran. For
+// SketchySVD: update.{upsilon, omega, phi, psi, window, daxpy} from the
+// stages of the same names (the sparse-sign X / Z entry kernel counted under
+// upsilon, the fused tensor-core window kernel under omega), and
+// approx.{dgeqrf, dgels, dgesvd, dgemm} from approx.{orth, core, svd,
+// vectors}; the approximations taken for per-window traces are included.
+// For SketchySPD: update.{omega, window, daxpy}.
+inline Timings reference_timings(skema_ctx* c, bool spd) {
+  auto sec = [c](const char* stage) {
+    double ms = 0.0;
+    int64_t n = 0;
+    return skema_timing_get(c, stage, &ms, &n) == SKEMA_OK ? ms / 1e3 : 0.0;
+  };
+  Timings t;
+  if (spd) {
+    t["init"]["omega"] = 0.0;
+    t["update"]["omega"] = sec("update.omega") + sec("update.fused");
+    t["update"]["window"] = sec("update.window");
+    t["update"]["daxpy"] = sec("update.daxpy");
+    for (const char* k : {"omega", "daxpy", "norm2", "update", "dpotrf", "dgels", "dgesvd"}) t["approx"][k] = 0.0;
+    return t;
+  }
+  for (const char* k : {"upsilon", "omega", "phi", "psi"}) t["init"][k] = 0.0;
+  t["update"]["upsilon"] = sec("update.upsilon") + sec("update.entries");
+  t["update"]["omega"] = sec("update.omega") + sec("update.fused");
+  t["update"]["phi"] = sec("update.phi");
+  t["update"]["psi"] = sec("update.psi");
+  t["update"]["window"] = sec("update.window");
+  t["update"]["daxpy"] = sec("update.daxpy");
+  t["approx"]["phi"] = 0.0;
+  t["approx"]["psi"] = 0.0;
+  t["approx"]["dgeqrf"] = sec("approx.orth");
+  t["approx"]["dgels"] = sec("approx.core");
+  t["approx"]["dgesvd"] = sec("approx.svd");
+  t["approx"]["dgemm"] = sec("approx.vectors");
+  return t;
+}
+
 inline double seconds_since(std::chrono::steady_clock::time_point t0) {
   return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }
@@ -916,6 +956,7 @@ class SketchySVD {
   explicit SketchySVD(const AlgParams& p)
       : nrow(p.matrix_m), ncol(p.matrix_n), rank(p.rank), eta(p.sketch_eta), nu(p.sketch_nu), algParams(p),
         ctx_(p, DimReduxT::kind, false), range(ctx_.range()), core(ctx_.core()) {
+    detail::check_ctx(skema_timing_enable(ctx_.get(), 1), ctx_.get());  // the reference always times
     if (!p.debug_filename.empty()) ctx_.dump_maps(detail::debug_stem(p.debug_filename));
   }
 
@@ -927,7 +968,6 @@ class SketchySVD {
   // ...), as src/Skema_SketchySVD.cpp:191-205, 235-245 write them; a single
   // window of all rows writes none, as the reference returns first.
   void linear_update(const MatrixType& A) {
-    const auto t0 = std::chrono::steady_clock::now();
     skema_ctx* c = ctx_.get();
     detail::check_ctx(skema_reset(c), c);
     const size_type m = algParams.kernel_func == Kernel_Map::GAUSSRBF ? nrow : detail::Context::rows_of(A);
@@ -948,13 +988,11 @@ class SketchySVD {
     }
     if (!stem.empty()) dump_sketches(stem, "");
     detail::check_ctx(skema_synchronize(c), c);
-    timings["update"]["total"] = detail::seconds_since(t0);
   }
 
   // SketchySVD::low_rank_approx (src/Skema_SketchySVD.cpp:569-664): U (m x r),
   // S (r), V (n x r), FP64.
   std::tuple<matrix_type, vector_type, matrix_type> low_rank_approx(bool update_timers = true) {
-    const auto t0 = std::chrono::steady_clock::now();
     skema_ctx* c = ctx_.get();
     matrix_type U("U", nrow, rank), V("V", ncol, rank);
     vector_type S("S", rank);
@@ -963,7 +1001,6 @@ class SketchySVD {
       uvecs = U;
       svals = S;
       vvecs = V;
-      timings["approx"]["total"] = detail::seconds_since(t0);
     }
     return {U, S, V};
   }
@@ -988,7 +1025,7 @@ class SketchySVD {
       if (svals.extent(0) > i) s[i] = svals(i);
       if (rnrms.extent(0) > i) r[i] = rnrms(i);
     }
-    detail::write_history(fname, s, r, timings, traces);
+    detail::write_history(fname, s, r, detail::reference_timings(ctx_.get(), false), traces);
   }
 
   // The sketches (X k x n, Y m x k, Z s x s), FP32 from the device.
@@ -1017,7 +1054,6 @@ class SketchySVD {
   const size_type range, core;
   matrix_type uvecs, vvecs;
   vector_type svals, rnrms;
-  detail::Timings timings;
   detail::Traces traces;
 };
 
@@ -1027,6 +1063,7 @@ class SketchySPD {
   explicit SketchySPD(const AlgParams& p)
       : nrow(p.matrix_m), ncol(p.matrix_n), rank(p.rank), algParams(p), ctx_(p, DimReduxT::kind, true),
         range(ctx_.range()) {
+    detail::check_ctx(skema_timing_enable(ctx_.get(), 1), ctx_.get());
     if (!p.debug_filename.empty()) ctx_.dump_maps(detail::debug_stem(p.debug_filename));
   }
 
@@ -1034,7 +1071,6 @@ class SketchySPD {
   // --debug-file, Y is written to <stem>_Y.txt at the end (:880-885), except
   // for a single window of all rows.
   void linear_update(const MatrixType& A) {
-    const auto t0 = std::chrono::steady_clock::now();
     skema_ctx* c = ctx_.get();
     detail::check_ctx(skema_reset(c), c);
     const size_type m = algParams.kernel_func == Kernel_Map::GAUSSRBF ? nrow : detail::Context::rows_of(A);
@@ -1042,7 +1078,6 @@ class SketchySPD {
     detail::check_ctx(skema_synchronize(c), c);
     if (!algParams.debug_filename.empty() && std::max<size_type>(1, algParams.window) < m)
       detail::write_text(detail::debug_stem(algParams.debug_filename) + "_Y.txt", sketch());
-    timings["update"]["total"] = detail::seconds_since(t0);
   }
 
   // The sketch Y (m x k), FP32 from the device.
@@ -1057,7 +1092,6 @@ class SketchySPD {
   // SketchySPD::low_rank_approx (src/Skema_SketchySVD.cpp:935-1151): the
   // eigenvectors U (m x r) and eigenvalues S, per AlgParams::spd_approx.
   std::tuple<matrix_type, vector_type> low_rank_approx(bool update_timers = true) {
-    const auto t0 = std::chrono::steady_clock::now();
     skema_ctx* c = ctx_.get();
     matrix_type U("U", nrow, rank);
     vector_type S("S", rank);
@@ -1065,7 +1099,6 @@ class SketchySPD {
     if (update_timers) {
       uvecs = U;
       svals = S;
-      timings["approx"]["total"] = detail::seconds_since(t0);
     }
     return {U, S};
   }
@@ -1089,7 +1122,7 @@ class SketchySPD {
       if (svals.extent(0) > i) s[i] = svals(i);
       if (rnrms.extent(0) > i) r[i] = rnrms(i);
     }
-    detail::write_history(fname, s, r, timings, detail::Traces{});
+    detail::write_history(fname, s, r, detail::reference_timings(ctx_.get(), true), detail::Traces{});
   }
 
  private:
@@ -1099,7 +1132,6 @@ class SketchySPD {
   const size_type range;
   matrix_type uvecs;
   vector_type svals, rnrms;
-  detail::Timings timings;
 };
 
 // ---- the driver entry (src/Skema_SketchySVD.cpp:1244-1577) ---------------

@@ -466,23 +466,46 @@ class _Context:
 
     def save_history(self, path=None):
         """SketchySVD::save_history (src/Skema_SketchySVD.cpp:730-755): a JSON
-        object with "timings", "traces", "svals" and "rnrms", written with a
-        4-space indent to `path`, or returned as a string when path is None.
-        Timings hold this build's stage timers (milliseconds, when timing is
-        on) under the reference's keys; traces stay empty (no per-window
-        singular-value traces are taken)."""
-        upd = {}
-        for key, stage in (("upsilon", "update.upsilon"), ("omega", "update.omega"), ("phi", "update.phi"),
-                           ("psi", "update.psi"), ("window", "update.window"), ("daxpy", "update.daxpy")):
-            try:
-                upd[key] = self.timing_get(stage)[0] / 1e3
-            except SkemaError:
-                upd[key] = 0.0
+        object with "timings", "traces", "svals" and "rnrms", keys sorted and
+        a 4-space indent as the reference's JSON writer prints it, written to
+        `path`, or returned as a string when path is None. Timings hold the
+        reference's keys (reference_timings)."""
         r = self.rank
         sv = getattr(self, "svals", None)
         rn = getattr(self, "rnrms", None)
-        return write_history(path, np.zeros(r) if sv is None else sv, np.zeros(r) if rn is None else rn, upd,
-                             getattr(self, "traces", None))
+        return write_history(path, np.zeros(r) if sv is None else sv, np.zeros(r) if rn is None else rn,
+                             traces=getattr(self, "traces", None), timings=self.reference_timings())
+
+    def reference_timings(self):
+        """The reference's timing keys (src/Skema_SketchySVD.cpp:101-116;
+        SketchySPD :776-786), in seconds, from this context's device stage
+        timers (zero unless timing_enable was called, and where no stage
+        corresponds): update.{upsilon, omega, phi, psi, window, daxpy} from the
+        stages of the same names (the sparse-sign X / Z entry kernel under
+        upsilon, the fused tensor-core window kernel under omega) and
+        approx.{dgeqrf, dgels, dgesvd, dgemm} from approx.{orth, core, svd,
+        vectors}."""
+
+        def sec(*stages):
+            t = 0.0
+            for st in stages:
+                try:
+                    t += self.timing_get(st)[0] / 1e3
+                except SkemaError:
+                    pass
+            return t
+
+        if self.spd:
+            return {"init": {"omega": 0.0},
+                    "update": {"omega": sec("update.omega", "update.fused"), "window": sec("update.window"),
+                               "daxpy": sec("update.daxpy")},
+                    "approx": {k: 0.0 for k in ("omega", "daxpy", "norm2", "update", "dpotrf", "dgels", "dgesvd")}}
+        return {"init": {k: 0.0 for k in ("upsilon", "omega", "phi", "psi")},
+                "update": {"upsilon": sec("update.upsilon", "update.entries"),
+                           "omega": sec("update.omega", "update.fused"), "phi": sec("update.phi"),
+                           "psi": sec("update.psi"), "window": sec("update.window"), "daxpy": sec("update.daxpy")},
+                "approx": {"phi": 0.0, "psi": 0.0, "dgeqrf": sec("approx.orth"), "dgels": sec("approx.core"),
+                           "dgesvd": sec("approx.svd"), "dgemm": sec("approx.vectors")}}
 
     def linear_update(self, A):
         """SketchySVD::linear_update: zero the sketches, then stream all rows.
@@ -937,22 +960,24 @@ def write_matrix(A, path):
         raise SkemaError(st, lib.skema_last_error(None).decode())
 
 
-def write_history(path, svals, rnrms, update_seconds=None, traces=None):
+def write_history(path, svals, rnrms, update_seconds=None, traces=None, timings=None):
     """The JSON of SketchySVD::save_history (src/Skema_SketchySVD.cpp:730-755):
-    {"timings": {init, update, approx}, "traces": {}, "svals": [...],
-    "rnrms": [...]} with a 4-space indent, the reference's timing keys
-    (src/Skema_SketchySVD.cpp:101-116; update times in seconds where
-    given, else 0). Written to `path` (with a newline) unless path is None;
-    the text is returned."""
+    {"rnrms": [...], "svals": [...], "timings": {approx, init, update},
+    "traces": {...}}, keys sorted and a 4-space indent as the reference's JSON
+    writer prints them. timings: the nested dict to write; by default the
+    reference's SketchySVD keys (src/Skema_SketchySVD.cpp:101-116), zero
+    except the update times given in update_seconds. Written to `path`
+    (with a newline) unless path is None; the text is returned."""
     import json
 
-    upd = {k: 0.0 for k in ("upsilon", "omega", "phi", "psi", "window", "daxpy")}
-    upd.update(update_seconds or {})
-    timings = {"init": {k: 0.0 for k in ("upsilon", "omega", "phi", "psi")}, "update": upd,
-               "approx": {k: 0.0 for k in ("phi", "psi", "dgeqrf", "dgemm", "dgels", "dgesvd")}}
+    if timings is None:
+        upd = {k: 0.0 for k in ("upsilon", "omega", "phi", "psi", "window", "daxpy")}
+        upd.update(update_seconds or {})
+        timings = {"init": {k: 0.0 for k in ("upsilon", "omega", "phi", "psi")}, "update": upd,
+                   "approx": {k: 0.0 for k in ("phi", "psi", "dgeqrf", "dgemm", "dgels", "dgesvd")}}
     hist = {"timings": timings, "traces": dict(traces or {}), "svals": [float(x) for x in svals],
             "rnrms": [float(x) for x in rnrms]}
-    text = json.dumps(hist, indent=4)
+    text = json.dumps(hist, indent=4, sort_keys=True)
     if path is not None:
         with open(path, "w") as f:
             f.write(text + "\n")

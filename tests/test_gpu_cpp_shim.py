@@ -47,6 +47,11 @@ def test_driver_dense_rect(cpp_bins, kat, tmp_path):
         assert np.max(np.abs(S - kat["rect_svals"][:10])) / S[0] < BAR, (model, S)
         assert len(h["rnrms"]) == 10 and np.all(np.isfinite(h["rnrms"]))
         assert set(h) == {"rnrms", "svals", "timings", "traces"}
+        # the reference's timing keys (src/Skema_SketchySVD.cpp:101-116), from the device stage timers
+        t = h["timings"]
+        assert set(t["update"]) == {"upsilon", "omega", "phi", "psi", "window", "daxpy"}
+        assert set(t["approx"]) == {"phi", "psi", "dgeqrf", "dgemm", "dgels", "dgesvd"}
+        assert t["approx"]["dgesvd"] > 0 and t["approx"]["dgeqrf"] > 0
 
 
 def test_driver_sparse_rect(cpp_bins, kat, tmp_path):

@@ -18,5 +18,9 @@ def test_write_history_layout(tmp_path):
     assert set(d["timings"]["approx"]) == {"phi", "psi", "dgeqrf", "dgemm", "dgels", "dgesvd"}
     assert text.splitlines()[1].startswith("    \"")
     assert write_history(None, [1.0], [0.0]) == json.dumps(json.loads(write_history(None, [1.0], [0.0])), indent=4)
+    # keys in sorted order at every level, as the reference's JSON object prints them
+    assert list(json.loads(text)) == ["rnrms", "svals", "timings", "traces"]
+    assert list(json.loads(text)["timings"]) == ["approx", "init", "update"]
+    assert list(json.loads(text)["timings"]["update"]) == sorted(d["timings"]["update"])
     t = json.loads(write_history(None, [2.0], [0.0], None, {"0": {"svals": [2.5]}, "1": {"svals": [2.0]}}))
     assert t["traces"] == {"0": {"svals": [2.5]}, "1": {"svals": [2.0]}}
