@@ -520,11 +520,11 @@ def run_gpu(args, cfg, peaks, peak_kind):
     # end to end through the public API with pinned host buffers
     e2e = None
     if rank == 0 and sparse and not args.no_e2e:
-        e2e = e2e_sparse(ctx, inp, m_local, row0, k, s, n, args)
+        e2e = with_pcie_floor(e2e_sparse(ctx, inp, m_local, row0, k, s, n, args))
     elif rank == 0 and rbf and not args.no_e2e:
-        e2e = e2e_rbf(ctx, inp, m_local, row0, k, s, n, args)
+        e2e = with_pcie_floor(e2e_rbf(ctx, inp, m_local, row0, k, s, n, args))
     elif rank == 0 and not sparse and not args.no_e2e:
-        e2e = e2e_dense(ctx, inp, m_local, row0, k, s, n, args)
+        e2e = with_pcie_floor(e2e_dense(ctx, inp, m_local, row0, k, s, n, args))
 
     cpu = cpu_oracle = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -658,6 +658,46 @@ def config_of(args, cfg, world, nnz):
     else:
         c["l2"] = "A is 16 GB per step > 126 MB L2 (no flush needed)"
     return c
+
+
+_PCIE = {}
+
+
+def pcie_rates():
+    """Host<->device copy rates of this box (GB/s): one 1 GiB pinned buffer
+    copied to and from the device, best of 3 each, CUDA events."""
+    import torch
+
+    if not _PCIE:
+        nb = 1 << 30
+        h = torch.empty(nb, dtype=torch.uint8).pin_memory()
+        d = torch.empty(nb, dtype=torch.uint8, device="cuda")
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        for name, fn in (("h2d_gbs", lambda: d.copy_(h, non_blocking=True)),
+                         ("d2h_gbs", lambda: h.copy_(d, non_blocking=True))):
+            best = None
+            for _ in range(3):
+                torch.cuda.synchronize()
+                ev[0].record()
+                fn()
+                ev[1].record()
+                ev[1].synchronize()
+                ms = ev[0].elapsed_time(ev[1])
+                best = ms if best is None else min(best, ms)
+            _PCIE[name] = nb / (best / 1e3) / 1e9
+        del h, d
+    return dict(_PCIE)
+
+
+def with_pcie_floor(e2e):
+    """Adds the copy-only time of the step's host<->device bytes at this box's
+    measured rates, and its ratio to the e2e step."""
+    r = pcie_rates()
+    floor = (e2e["h2d_bytes_per_step"] / (r["h2d_gbs"] * 1e9) + e2e["d2h_bytes_per_step"] / (r["d2h_gbs"] * 1e9)) * 1e3
+    e2e["pcie"] = {"h2d_gbs": r["h2d_gbs"], "d2h_gbs": r["d2h_gbs"], "copy_floor_ms": floor,
+                   "floor_over_step": floor / e2e["ms_per_step"],
+                   "how": "1 GiB pinned buffer to and from the device, best of 3, CUDA events"}
+    return e2e
 
 
 def e2e_sparse(ctx, inp, m_local, row0, k, s, n, args):

@@ -81,6 +81,15 @@ void* workspace(skema_ctx* c, size_t bytes) {
   return c->ws;
 }
 
+// A pitched copy whose rows lie back to back on both sides goes as one
+// linear copy: the copy engines move one long run much faster than the same
+// bytes as many short rows (a 1e6 x 81 row-major sketch has 324-byte rows).
+static cudaError_t copy2d(void* dst, size_t dpitch, const void* src, size_t spitch, size_t width, size_t height,
+                          cudaMemcpyKind kind, cudaStream_t st) {
+  if (dpitch == width && spitch == width) return cudaMemcpyAsync(dst, src, width * height, kind, st);
+  return cudaMemcpy2DAsync(dst, dpitch, src, spitch, width, height, kind, st);
+}
+
 void* staging(skema_ctx* c, size_t bytes) {
   if (bytes <= c->stage_bytes) return c->stage;
   check_ws_limit(c, c->stage_bytes, std::max<size_t>(bytes, 1 << 20));
@@ -506,12 +515,12 @@ int skema_linear_update_dense(skema_ctx* c, const float* A, int64_t ld, int32_t 
     for (int64_t r = 0; r < nrows; r += W) {
       const int64_t wr = std::min(W, nrows - r);
       if (layout == SKEMA_COL_MAJOR) {
-        SKEMA_CUDA(cudaMemcpy2DAsync(buf, sizeof(float) * wr, A + r, sizeof(float) * ld,
+        SKEMA_CUDA(copy2d(buf, sizeof(float) * wr, A + r, sizeof(float) * ld,
                                      sizeof(float) * wr, c->n, cudaMemcpyHostToDevice, c->stream));
         Mat a{buf, 1, wr};
         dense_update(c, a, row0 + r, wr);
       } else {
-        SKEMA_CUDA(cudaMemcpy2DAsync(buf, sizeof(float) * c->n, A + r * ld, sizeof(float) * ld,
+        SKEMA_CUDA(copy2d(buf, sizeof(float) * c->n, A + r * ld, sizeof(float) * ld,
                                      sizeof(float) * c->n, wr, cudaMemcpyHostToDevice, c->stream));
         Mat a{buf, c->n, 1};
         dense_update(c, a, row0 + r, wr);
@@ -541,8 +550,6 @@ int skema_linear_update_csr(skema_ctx* c, const int64_t* rowptr, const int32_t* 
     const int64_t base = rowptr[0];
     const int64_t nnz = rowptr[nrows] - base;
     if (nnz < 0) fail(SKEMA_EINVAL, "rowptr is decreasing");
-    for (int64_t i = 0; i < nrows; ++i)
-      if (rowptr[i + 1] < rowptr[i]) fail(SKEMA_EINVAL, "rowptr is decreasing");
     if (nnz > 0 && (!col || !val)) fail(SKEMA_EINVAL, "null col/val");
     const size_t rp_bytes = sizeof(int64_t) * (size_t)(nrows + 1);
     const size_t rp_pad = (rp_bytes + 255) / 256 * 256;
@@ -558,6 +565,14 @@ int skema_linear_update_csr(skema_ctx* c, const int64_t* rowptr, const int32_t* 
       SKEMA_CUDA(cudaMemcpyAsync(d_val, val + base, sizeof(float) * (size_t)nnz,
                                  cudaMemcpyHostToDevice, c->stream));
     }
+    // the row map is checked on the host while the copies run (their sizes
+    // depend only on its ends); a decreasing map waits for them, so the
+    // caller's buffers are no longer read, and nothing is launched
+    for (int64_t i = 0; i < nrows; ++i)
+      if (rowptr[i + 1] < rowptr[i]) {
+        SKEMA_CUDA(cudaStreamSynchronize(c->stream));
+        fail(SKEMA_EINVAL, "rowptr is decreasing");
+      }
     csr_update(c, d_rp, d_col, d_val, base, row0, nrows);
   });
 }
@@ -579,11 +594,11 @@ int skema_linear_update_rbf(skema_ctx* c, const float* pts, int64_t ld, int32_t 
     }
     float* buf = (float*)staging(c, sizeof(float) * (size_t)(npts * d));
     if (layout == SKEMA_COL_MAJOR) {
-      SKEMA_CUDA(cudaMemcpy2DAsync(buf, sizeof(float) * npts, pts, sizeof(float) * ld,
+      SKEMA_CUDA(copy2d(buf, sizeof(float) * npts, pts, sizeof(float) * ld,
                                    sizeof(float) * npts, d, cudaMemcpyHostToDevice, c->stream));
       rbf_update(c, Mat{buf, 1, npts}, npts, d, row0, nrows);
     } else {
-      SKEMA_CUDA(cudaMemcpy2DAsync(buf, sizeof(float) * d, pts, sizeof(float) * ld,
+      SKEMA_CUDA(copy2d(buf, sizeof(float) * d, pts, sizeof(float) * ld,
                                    sizeof(float) * d, npts, cudaMemcpyHostToDevice, c->stream));
       rbf_update(c, Mat{buf, d, 1}, npts, d, row0, nrows);
     }
@@ -778,16 +793,40 @@ int skema_get_sketch(skema_ctx* c, int32_t which, float* buf, int64_t ld, int32_
     const bool want_row = layout == SKEMA_ROW_MAJOR;
     const cudaMemcpyKind kind = mem == SKEMA_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
     if (want_row == irow) {
-      SKEMA_CUDA(cudaMemcpy2DAsync(buf, sizeof(float) * ld, src, sizeof(float) * inner,
+      SKEMA_CUDA(copy2d(buf, sizeof(float) * ld, src, sizeof(float) * inner,
                                    sizeof(float) * inner, outer, kind, c->stream));
     } else if (mem == SKEMA_MEM_DEVICE) {
       copy_block(c, sm, want_row ? MatOut{buf, ld, 1} : MatOut{buf, 1, ld}, rows, cols);
     } else {
+      // The transposed copy goes out in chunks of the host layout's outer
+      // dimension through two staging slots: the side stream transposes
+      // chunk i + 1 while the context stream copies chunk i to the host, so
+      // the transposes hide behind the PCIe copy.
       const int64_t tin = want_row ? cols : rows, tout = want_row ? rows : cols;
-      float* tmp = (float*)staging(c, sizeof(float) * (size_t)(rows * cols));
-      copy_block(c, sm, want_row ? MatOut{tmp, cols, 1} : MatOut{tmp, 1, rows}, rows, cols);
-      SKEMA_CUDA(cudaMemcpy2DAsync(buf, sizeof(float) * ld, tmp, sizeof(float) * tin,
-                                   sizeof(float) * tin, tout, cudaMemcpyDeviceToHost, c->stream));
+      const int64_t och = std::max<int64_t>(1, std::min<int64_t>(tout, ((int64_t)8 << 20) / tin));
+      const size_t slot_bytes = (sizeof(float) * (size_t)(och * tin) + 255) / 256 * 256;
+      char* tmp = (char*)staging(c, 2 * slot_bytes);
+      cudaEvent_t tr_done[2] = {c->pipe_ev[0], c->pipe_ev[1]}, out_done[2] = {c->pipe_ev[2], c->pipe_ev[3]};
+      SKEMA_CUDA(cudaEventRecord(c->fork_ev, c->stream));
+      SKEMA_CUDA(cudaStreamWaitEvent(c->side, c->fork_ev, 0));
+      for (int64_t o0 = 0, i = 0; o0 < tout; o0 += och, ++i) {
+        const int64_t n = std::min(och, tout - o0);
+        const int sl = (int)(i & 1);
+        float* slot = (float*)(tmp + sl * slot_bytes);
+        if (i >= 2) SKEMA_CUDA(cudaStreamWaitEvent(c->side, out_done[sl], 0));
+        // the chunk's outer dimension is the one contiguous in the stored sketch
+        if (tin <= 256)
+          transpose_narrow(c, sm.p + o0, n, tin, want_row ? sm.cs : sm.rs, slot, c->side);
+        else if (want_row)
+          copy_block(c, Mat{sm.p + o0 * sm.rs, sm.rs, sm.cs}, MatOut{slot, cols, 1}, n, cols, c->side);
+        else
+          copy_block(c, Mat{sm.p + o0 * sm.cs, sm.rs, sm.cs}, MatOut{slot, 1, rows}, rows, n, c->side);
+        SKEMA_CUDA(cudaEventRecord(tr_done[sl], c->side));
+        SKEMA_CUDA(cudaStreamWaitEvent(c->stream, tr_done[sl], 0));
+        SKEMA_CUDA(copy2d(buf + o0 * ld, sizeof(float) * ld, slot, sizeof(float) * tin,
+                                     sizeof(float) * tin, n, cudaMemcpyDeviceToHost, c->stream));
+        SKEMA_CUDA(cudaEventRecord(out_done[sl], c->stream));
+      }
     }
     if (mem == SKEMA_MEM_HOST) SKEMA_CUDA(cudaStreamSynchronize(c->stream));
   });
@@ -806,14 +845,14 @@ int skema_set_sketch(skema_ctx* c, int32_t which, const float* buf, int64_t ld, 
     const bool have_row = layout == SKEMA_ROW_MAJOR;
     const cudaMemcpyKind kind = mem == SKEMA_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
     if (have_row == irow) {
-      SKEMA_CUDA(cudaMemcpy2DAsync(dst, sizeof(float) * inner, buf, sizeof(float) * ld,
+      SKEMA_CUDA(copy2d(dst, sizeof(float) * inner, buf, sizeof(float) * ld,
                                    sizeof(float) * inner, outer, kind, c->stream));
     } else if (mem == SKEMA_MEM_DEVICE) {
       copy_block(c, have_row ? Mat{buf, ld, 1} : Mat{buf, 1, ld}, dm, rows, cols);
     } else {
       const int64_t tin = have_row ? cols : rows, tout = have_row ? rows : cols;
       float* tmp = (float*)staging(c, sizeof(float) * (size_t)(rows * cols));
-      SKEMA_CUDA(cudaMemcpy2DAsync(tmp, sizeof(float) * tin, buf, sizeof(float) * ld,
+      SKEMA_CUDA(copy2d(tmp, sizeof(float) * tin, buf, sizeof(float) * ld,
                                    sizeof(float) * tin, tout, cudaMemcpyHostToDevice, c->stream));
       copy_block(c, have_row ? Mat{tmp, cols, 1} : Mat{tmp, 1, rows}, dm, rows, cols);
     }

@@ -256,13 +256,51 @@ void axpby_block(skema_ctx* c, Mat src, MatOut dst, int64_t M, int64_t N, float 
   SKEMA_LAUNCHED(c);
 }
 
-void copy_block(skema_ctx* c, Mat src, MatOut dst, int64_t M, int64_t N) {
+// dst[l * ns + s] = src[l + s * ss] for l < nl, s < ns (ns <= 256): a block
+// whose long dimension is contiguous in the source, written densely with the
+// short dimension innermost (a column-major m x k sketch into row-major rows,
+// or a row-major k x n one into column-major columns). A CTA takes 32 long
+// indices: a warp reads 128 contiguous bytes per short index into shared
+// memory (rows of an odd stride, so the stores do not collide), then the CTA
+// writes the 32 ns values as one contiguous run.
+__global__ void __launch_bounds__(256) narrow_transpose_kernel(const float* __restrict__ src, int64_t nl, int ns,
+                                                               int64_t ss, float* __restrict__ dst) {
+  extern __shared__ float nt[];  // 32 rows of ld >= ns
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  const int ld = ns | 1;
+  for (int64_t l0 = (int64_t)blockIdx.x * 32; l0 < nl; l0 += (int64_t)gridDim.x * 32) {
+    const int nr = (int)min((int64_t)32, nl - l0);
+    if (tx < nr)
+      for (int s = ty; s < ns; s += 8) nt[tx * ld + s] = src[l0 + tx + s * ss];
+    __syncthreads();
+    float* o = dst + l0 * ns;
+    const int tot = nr * ns;
+    for (int q = threadIdx.x; q < tot; q += blockDim.x) {
+      const int r = q / ns;
+      o[q] = nt[r * ld + (q - r * ns)];
+    }
+    __syncthreads();
+  }
+}
+
+void transpose_narrow(skema_ctx* c, const float* src, int64_t nl, int64_t ns, int64_t ss, float* dst,
+                      cudaStream_t st) {
+  if (nl <= 0 || ns <= 0) return;
+  if (ns > 256) fail(SKEMA_EINVAL, "transpose_narrow: short dimension above 256");
+  const int grid = (int)std::min<int64_t>((nl + 31) / 32, (int64_t)c->sm_count * 16);
+  const size_t smem = sizeof(float) * 32 * (size_t)(ns | 1);
+  narrow_transpose_kernel<<<grid, 256, smem, st>>>(src, nl, (int)ns, ss, dst);
+  SKEMA_LAUNCHED(c);
+}
+
+void copy_block(skema_ctx* c, Mat src, MatOut dst, int64_t M, int64_t N, cudaStream_t st) {
   if (M <= 0 || N <= 0) return;
   const int64_t tiles = ((M + 31) / 32) * ((N + 31) / 32);
   const int grid = (int)std::min<int64_t>(tiles, (int64_t)c->sm_count * 32);
-  copy_kernel<<<grid, dim3(32, 8), 0, c->stream>>>(src.p, src.rs, src.cs, dst.p, dst.rs, dst.cs, M,
-                                                   N);
+  copy_kernel<<<grid, dim3(32, 8), 0, st>>>(src.p, src.rs, src.cs, dst.p, dst.rs, dst.cs, M, N);
   SKEMA_LAUNCHED(c);
 }
+
+void copy_block(skema_ctx* c, Mat src, MatOut dst, int64_t M, int64_t N) { copy_block(c, src, dst, M, N, c->stream); }
 
 }  // namespace skema

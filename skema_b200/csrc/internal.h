@@ -250,6 +250,10 @@ void axpby_block(skema_ctx* c, Mat src, MatOut dst, int64_t M, int64_t N,
                  float alpha, float beta);
 // Copy a strided FP32 block into another strided block.
 void copy_block(skema_ctx* c, Mat src, MatOut dst, int64_t M, int64_t N);
+void copy_block(skema_ctx* c, Mat src, MatOut dst, int64_t M, int64_t N, cudaStream_t st);
+// dst[l * ns + s] = src[l + s * ss] (l < nl, s < ns <= 256) on stream st.
+void transpose_narrow(skema_ctx* c, const float* src, int64_t nl, int64_t ns, int64_t ss, float* dst,
+                      cudaStream_t st);
 
 // ---- dense update (dense.cu) ----
 // One call of skema_linear_update_dense on device data.
