@@ -255,6 +255,10 @@ static void free_all(skema_ctx* c) {
     if (e) cudaEventDestroy(e);
     e = nullptr;
   }
+  for (cudaEvent_t& e : c->stage_ev) {
+    if (e) cudaEventDestroy(e);
+    e = nullptr;
+  }
   c->side = nullptr;
   c->fork_ev = c->join_ev = nullptr;
 }
@@ -407,6 +411,7 @@ int skema_create(const skema_params* p, skema_ctx** out) {
     SKEMA_CUDA(cudaEventCreateWithFlags(&c->fork_ev, cudaEventDisableTiming));
     SKEMA_CUDA(cudaEventCreateWithFlags(&c->join_ev, cudaEventDisableTiming));
     for (cudaEvent_t& e : c->pipe_ev) SKEMA_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    for (cudaEvent_t& e : c->stage_ev) SKEMA_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     c->pipe_xt_sms = 0;
     c->pipe_windows = 2;
     if (const char* v = std::getenv("SKEMA_DENSE_PIPE_SMS")) c->pipe_xt_sms = std::max(0, std::atoi(v));
@@ -507,24 +512,35 @@ int skema_linear_update_dense(skema_ctx* c, const float* A, int64_t ld, int32_t 
       dense_update(c, a, row0, nrows);
       return;
     }
-    // Host input: stage window by window (the device path then sees a
-    // column-major w x n block with ld = w).
+    // Host input: staged window by window through two slots. The uploads
+    // run on the side stream and each window's update on the context stream
+    // once its upload has landed, so window w + 1 crosses PCIe while window
+    // w is sketched; a slot is refilled only after the update that read it.
+    // The device path sees a column-major w x n block (ld = w) or a
+    // row-major one (ld = n).
     const int64_t W = c->w;
-    const size_t win_bytes = sizeof(float) * (size_t)(std::min(W, nrows) * c->n);
-    float* buf = (float*)staging(c, win_bytes);
-    for (int64_t r = 0; r < nrows; r += W) {
+    const bool two = nrows > W;
+    const size_t win_bytes = (sizeof(float) * (size_t)(std::min(W, nrows) * c->n) + 255) / 256 * 256;
+    char* slots = (char*)staging(c, two ? 2 * win_bytes : win_bytes);
+    cudaEvent_t up[2] = {c->stage_ev[0], c->stage_ev[1]}, used[2] = {c->stage_ev[2], c->stage_ev[3]};
+    SKEMA_CUDA(cudaEventRecord(c->fork_ev, c->stream));
+    SKEMA_CUDA(cudaStreamWaitEvent(c->side, c->fork_ev, 0));
+    for (int64_t r = 0, i = 0; r < nrows; r += W, ++i) {
       const int64_t wr = std::min(W, nrows - r);
-      if (layout == SKEMA_COL_MAJOR) {
-        SKEMA_CUDA(copy2d(buf, sizeof(float) * wr, A + r, sizeof(float) * ld,
-                                     sizeof(float) * wr, c->n, cudaMemcpyHostToDevice, c->stream));
-        Mat a{buf, 1, wr};
-        dense_update(c, a, row0 + r, wr);
-      } else {
-        SKEMA_CUDA(copy2d(buf, sizeof(float) * c->n, A + r * ld, sizeof(float) * ld,
-                                     sizeof(float) * c->n, wr, cudaMemcpyHostToDevice, c->stream));
-        Mat a{buf, c->n, 1};
-        dense_update(c, a, row0 + r, wr);
-      }
+      const int sl = (int)(i & 1);
+      float* buf = (float*)(slots + sl * win_bytes);
+      if (i >= 2) SKEMA_CUDA(cudaStreamWaitEvent(c->side, used[sl], 0));
+      if (layout == SKEMA_COL_MAJOR)
+        SKEMA_CUDA(copy2d(buf, sizeof(float) * wr, A + r, sizeof(float) * ld, sizeof(float) * wr, c->n,
+                          cudaMemcpyHostToDevice, c->side));
+      else
+        SKEMA_CUDA(copy2d(buf, sizeof(float) * c->n, A + r * ld, sizeof(float) * ld, sizeof(float) * c->n, wr,
+                          cudaMemcpyHostToDevice, c->side));
+      SKEMA_CUDA(cudaEventRecord(up[sl], c->side));
+      SKEMA_CUDA(cudaStreamWaitEvent(c->stream, up[sl], 0));
+      const Mat a = layout == SKEMA_COL_MAJOR ? Mat{buf, 1, wr} : Mat{buf, c->n, 1};
+      dense_update(c, a, row0 + r, wr);
+      SKEMA_CUDA(cudaEventRecord(used[sl], c->stream));
     }
   });
 }
@@ -806,7 +822,7 @@ int skema_get_sketch(skema_ctx* c, int32_t which, float* buf, int64_t ld, int32_
       const int64_t och = std::max<int64_t>(1, std::min<int64_t>(tout, ((int64_t)8 << 20) / tin));
       const size_t slot_bytes = (sizeof(float) * (size_t)(och * tin) + 255) / 256 * 256;
       char* tmp = (char*)staging(c, 2 * slot_bytes);
-      cudaEvent_t tr_done[2] = {c->pipe_ev[0], c->pipe_ev[1]}, out_done[2] = {c->pipe_ev[2], c->pipe_ev[3]};
+      cudaEvent_t tr_done[2] = {c->stage_ev[0], c->stage_ev[1]}, out_done[2] = {c->stage_ev[2], c->stage_ev[3]};
       SKEMA_CUDA(cudaEventRecord(c->fork_ev, c->stream));
       SKEMA_CUDA(cudaStreamWaitEvent(c->side, c->fork_ev, 0));
       for (int64_t o0 = 0, i = 0; o0 < tout; o0 += och, ++i) {

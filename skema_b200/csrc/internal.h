@@ -106,6 +106,9 @@ struct skema_ctx {
   // Hand-offs between the two streams of the BF16 dense pipeline (window
   // copies ready / released, one pair per copy buffer).
   cudaEvent_t pipe_ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  // host staging through two slots (uploads and transposed fetches): slot i
+  // filled / slot i read, i = 0, 1
+  cudaEvent_t stage_ev[4] = {nullptr, nullptr, nullptr, nullptr};
   std::string err;
   int64_t launches = 0;
   skema::Map ups, omg, phi, psi;
