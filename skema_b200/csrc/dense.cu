@@ -26,8 +26,15 @@ static int splitk_for(const skema_ctx* c, int64_t M, int64_t N, int64_t K) {
   return (int)std::max<int64_t>(1, sk);
 }
 
-// The Gauss three-sketch body for one window. T is wr x s scratch.
+// Room for the K-split partial products of the window's three large
+// products (at most about 13 M values on the 200k x 20k case), after T.
+constexpr int64_t kSplitPartFloats = (int64_t)16 << 20;
+static int64_t t_floats(const skema_ctx* c, int64_t wr) { return (wr * c->s + 63) / 64 * 64; }
+
+// The Gauss three-sketch body for one window. T is wr x s scratch, followed
+// by kSplitPartFloats for sgemm_split.
 static void gauss_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr, float* T) {
+  float* part = T + t_floats(c, wr);
   const float eta = (float)c->p.sketch_eta, nu = (float)c->p.sketch_nu;
   const Map& U = c->ups;
   const Map& O = c->omg;
@@ -36,17 +43,19 @@ static void gauss_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr, float* T)
   const float ybeta = y_beta(c, R0, R0 + wr, nu);
   {  // Y rows: B(kk=j, col=r) = Omega~(r, j)
     StageScope st(c, ST_OMEGA);
-    sgemm(c, wr, c->k, c->n, eta, Aw, Mat{O.f32, O.cs, O.rs}, ybeta, MatOut{c->Y + R0, 1, c->m});
+    sgemm_split(c, wr, c->k, c->n, eta, Aw, Mat{O.f32, O.cs, O.rs}, ybeta, MatOut{c->Y + R0, 1, c->m}, part,
+                kSplitPartFloats);
   }
   y_rows_mark(c, R0, R0 + wr);
   {  // T = A_w Psi~^T
     StageScope st(c, ST_PSI);
-    sgemm(c, wr, c->s, c->n, 1.f, Aw, Mat{P.f32, P.cs, P.rs}, 0.f, MatOut{T, c->s, 1});
+    sgemm_split(c, wr, c->s, c->n, 1.f, Aw, Mat{P.f32, P.cs, P.rs}, 0.f, MatOut{T, c->s, 1}, part,
+                kSplitPartFloats);
   }
   {  // X = nu X + eta Upsilon~(:, R0:R0+wr) A_w
     StageScope st(c, ST_UPSILON);
-    sgemm(c, c->k, c->n, wr, eta, Mat{U.f32 + R0 * U.cs, U.rs, U.cs}, Aw, nu,
-          MatOut{c->X, c->n, 1});
+    sgemm_split(c, c->k, c->n, wr, eta, Mat{U.f32 + R0 * U.cs, U.rs, U.cs}, Aw, nu, MatOut{c->X, c->n, 1}, part,
+                kSplitPartFloats);
   }
   {  // Z = nu Z + eta Phi~(:, R0:R0+wr) T
     StageScope st(c, ST_PHI);
@@ -90,7 +99,7 @@ void dense_window(skema_ctx* c, Mat Aw, int64_t R0, int64_t wr, float* T) {
 size_t dense_scratch_bytes(const skema_ctx* c, int64_t wr) {
   if (c->spd || c->p.dim_redux == SKEMA_MAP_SPARSE_SIGN) return 256;
   if (tc_available(c)) return tc_scratch_bytes(c, wr);
-  return sizeof(float) * (size_t)(wr * c->s) + 256;
+  return sizeof(float) * (size_t)(t_floats(c, wr) + kSplitPartFloats) + 256;
 }
 
 void dense_update(skema_ctx* c, Mat A, int64_t row0, int64_t nrows) {

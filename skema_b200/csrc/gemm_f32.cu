@@ -20,12 +20,14 @@ namespace {
 
 constexpr int BM = 128, BN = 128, BK = 8, PAD = 4;
 
+// Two CTAs per SM (at most 128 registers a thread): one 256-thread CTA of
+// 8 warps does not hide the shared-memory and global-load latency.
 template <bool A_M_CONTIG, bool B_N_CONTIG, bool ATOMIC>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 2)
     sgemm_kernel(int64_t M, int64_t N, int64_t K, float alpha, const float* __restrict__ A,
                  int64_t a_rs, int64_t a_cs, const float* __restrict__ B, int64_t b_rs,
                  int64_t b_cs, float beta, float* __restrict__ C, int64_t c_rs, int64_t c_cs,
-                 int64_t kchunk) {
+                 int64_t kchunk, int64_t c_zs) {
   __shared__ __align__(16) float As[2][BK][BM + PAD];
   __shared__ __align__(16) float Bs[2][BK][BN + PAD];
   const int tid = threadIdx.x;
@@ -114,7 +116,7 @@ __global__ void __launch_bounds__(256)
     for (int j = 0; j < 8; ++j) {
       const int64_t gn = n0 + (j < 4 ? tx * 4 + j : 64 + tx * 4 + (j - 4));
       if (gn >= N) continue;
-      float* cp = C + gm * c_rs + gn * c_cs;
+      float* cp = C + blockIdx.z * c_zs + gm * c_rs + gn * c_cs;
       const float v = alpha * acc[i][j];
       if (ATOMIC) {
         atomicAdd(cp, v);
@@ -125,9 +127,10 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// C_zs: offset between the outputs of the K splits (0: all into C).
 template <bool AM, bool BN_, bool AT>
 void launch_sgemm(skema_ctx* c, int64_t M, int64_t N, int64_t K, float alpha, Mat A, Mat B,
-                  float beta, MatOut C, int splitk) {
+                  float beta, MatOut C, int splitk, int64_t c_zs = 0) {
   int64_t kchunk = (K + splitk - 1) / splitk;
   kchunk = (kchunk + BK - 1) / BK * BK;
   const int64_t gz = (K + kchunk - 1) / kchunk;
@@ -138,7 +141,7 @@ void launch_sgemm(skema_ctx* c, int64_t M, int64_t N, int64_t K, float alpha, Ma
     dim3 grid((unsigned)((M + BM - 1) / BM), (unsigned)((nn + BN - 1) / BN), (unsigned)gz);
     sgemm_kernel<AM, BN_, AT><<<grid, 256, 0, c->stream>>>(
         M, nn, K, alpha, A.p, A.rs, A.cs, B.p + nb * B.cs, B.rs, B.cs, beta, C.p + nb * C.cs, C.rs,
-        C.cs, kchunk);
+        C.cs, kchunk, c_zs);
     SKEMA_LAUNCHED(c);
   }
 }
@@ -216,6 +219,24 @@ __global__ void copy_kernel(const float* __restrict__ S, int64_t srs, int64_t sc
   }
 }
 
+// C = beta C + alpha sum_z P_z over M x N, the K-split partial products P_z
+// (strides p_rs, p_cs; p_zs apart) summed in z order, so the result does not
+// depend on scheduling. Consecutive threads follow C's unit stride.
+__global__ void splitk_reduce_kernel(const float* __restrict__ P, int64_t p_rs, int64_t p_cs, int64_t p_zs, int nz,
+                                     int64_t M, int64_t N, float alpha, float beta, float* __restrict__ C,
+                                     int64_t c_rs, int64_t c_cs) {
+  const int64_t total = M * N;
+  const bool cm = c_rs == 1;
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < total; q += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = cm ? q % M : q / N, j = cm ? q / M : q % N;
+    const float* pp = P + i * p_rs + j * p_cs;
+    float sum = 0.f;
+    for (int z = 0; z < nz; ++z) sum += pp[z * p_zs];
+    float* cp = C + i * c_rs + j * c_cs;
+    *cp = (beta == 0.f) ? alpha * sum : fmaf(beta, *cp, alpha * sum);
+  }
+}
+
 int grid1d(const skema_ctx* c, int64_t total, int threads) {
   const int64_t want = (total + threads - 1) / threads;
   return (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)c->sm_count * 16));
@@ -241,6 +262,41 @@ void sgemm(skema_ctx* c, int64_t M, int64_t N, int64_t K, float alpha, Mat A, Ma
   else if (bn) launch_sgemm<false, true, false>(c, M, N, K, alpha, A, B, beta, C, 1);
   else if (at) launch_sgemm<false, false, true>(c, M, N, K, alpha, A, B, beta, C, splitk);
   else launch_sgemm<false, false, false>(c, M, N, K, alpha, A, B, beta, C, 1);
+}
+
+void sgemm_split(skema_ctx* c, int64_t M, int64_t N, int64_t K, float alpha, Mat A, Mat B, float beta, MatOut C,
+                 float* part, int64_t part_floats) {
+  if (M <= 0 || N <= 0) return;
+  // Two 256-thread CTAs fit an SM. A grid of output tiles below two waves
+  // gets about three waves of (tile, K range) units, each range at least
+  // 1024 deep, as far as the partial buffer allows.
+  const int64_t tiles = ((M + BM - 1) / BM) * ((N + BN - 1) / BN);
+  const int64_t slots = 2 * (int64_t)c->sm_count;
+  int64_t sk = 1;
+  if (part && K > 0 && tiles < 2 * slots && N <= (int64_t)65535 * BN) {
+    sk = (3 * slots + tiles - 1) / tiles;
+    sk = std::min<int64_t>({sk, 16, K / 1024, part_floats / (M * N)});
+  }
+  if (sk < 2) {
+    sgemm(c, M, N, K, alpha, A, B, beta, C);
+    return;
+  }
+  int64_t kchunk = (K + sk - 1) / sk;
+  kchunk = (kchunk + BK - 1) / BK * BK;
+  const int nz = (int)((K + kchunk - 1) / kchunk);
+  // partial planes in C's orientation, so the reduction reads and writes
+  // along the same unit stride
+  const bool cm = C.rs == 1;
+  const MatOut P{part, cm ? 1 : N, cm ? M : 1};
+  const int64_t pz = M * N;
+  const bool am = (A.rs == 1), bn = (B.cs == 1);
+  if (am && bn) launch_sgemm<true, true, false>(c, M, N, K, 1.f, A, B, 0.f, P, (int)sk, pz);
+  else if (am) launch_sgemm<true, false, false>(c, M, N, K, 1.f, A, B, 0.f, P, (int)sk, pz);
+  else if (bn) launch_sgemm<false, true, false>(c, M, N, K, 1.f, A, B, 0.f, P, (int)sk, pz);
+  else launch_sgemm<false, false, false>(c, M, N, K, 1.f, A, B, 0.f, P, (int)sk, pz);
+  splitk_reduce_kernel<<<grid1d(c, pz, 256), 256, 0, c->stream>>>(part, P.rs, P.cs, pz, nz, M, N, alpha, beta, C.p,
+                                                                   C.rs, C.cs);
+  SKEMA_LAUNCHED(c);
 }
 
 void scale_block(skema_ctx* c, MatOut C, int64_t M, int64_t N, float beta, cudaStream_t stream) {

@@ -246,6 +246,12 @@ struct MatOut {
 };
 void sgemm(skema_ctx* c, int64_t M, int64_t N, int64_t K, float alpha, Mat A,
            Mat B, float beta, MatOut C, int splitk = 1);
+// The same product, with the K dimension split when the output tiles would
+// fill less than two waves: the splits write partial products into part
+// (capacity part_floats; at most 16 splits of 1024 or more) and one pass
+// sums them in a fixed order into C. Without room it falls back to sgemm.
+void sgemm_split(skema_ctx* c, int64_t M, int64_t N, int64_t K, float alpha, Mat A, Mat B, float beta, MatOut C,
+                 float* part, int64_t part_floats);
 // C = beta * C over an M x N strided block.
 void scale_block(skema_ctx* c, MatOut C, int64_t M, int64_t N, float beta, cudaStream_t stream = nullptr);
 // dst(i,j) = alpha * src(i,j) + beta * dst(i,j) over M x N (beta 0: no read).
