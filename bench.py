@@ -596,6 +596,29 @@ def run_gpu(args, cfg, peaks, peak_kind):
         respass = {"ms": rms, "fp64_tflops": fl / (rms / 1e3) / 1e12,
                    "rnorm_over_sigma1_max": float(np.max(rn) / S[0]),
                    "includes": "H2D of U, S, V (host FP64) + the FP64 products + D2H of the norms"}
+        # the same pass from the approximation's device-resident U, S, V
+        # (skema_residuals_begin with device buffers: no host copy of U),
+        # once untimed, then timed with CUDA events
+        import skema_b200._lib as L
+
+        def res_dev():
+            ctx._check(ctx.lib.skema_residuals_begin(ctx.h, Ud.data_ptr(), Sd.data_ptr(), Vd.data_ptr(),
+                                                     L.MEM_DEVICE))
+            ctx._stream(inp, row0, None, "skema_residuals_update")
+            out_n = np.empty(r, dtype=np.float64)
+            ctx._check(ctx.lib.skema_residuals_finish(ctx.h, out_n.ctypes.data, L.MEM_HOST))
+            return out_n
+
+        res_dev()
+        torch.cuda.synchronize()
+        r0e.record(stream)
+        rn_d = res_dev()
+        r1e.record(stream)
+        torch.cuda.synchronize()
+        dms = r0e.elapsed_time(r1e)
+        respass["device_inputs"] = {"ms": dms, "fp64_tflops": fl / (dms / 1e3) / 1e12,
+                                    "max_rel_diff_vs_host_inputs": float(np.max(np.abs(rn_d - rn) / np.abs(rn))),
+                                    "includes": "the FP64 products from device-resident U, S, V + D2H of the norms"}
 
     out = {
         "metric": "sketched rows/s",
