@@ -957,6 +957,8 @@ class SketchySVD {
       : nrow(p.matrix_m), ncol(p.matrix_n), rank(p.rank), eta(p.sketch_eta), nu(p.sketch_nu), algParams(p),
         ctx_(p, DimReduxT::kind, false), range(ctx_.range()), core(ctx_.core()) {
     detail::check_ctx(skema_timing_enable(ctx_.get(), 1), ctx_.get());  // the reference always times
+    // the last approximation's U, S, V stay on the device for compute_residuals
+    detail::check_ctx(skema_set_keep_factors(ctx_.get(), 1), ctx_.get());
     if (!p.debug_filename.empty()) ctx_.dump_maps(detail::debug_stem(p.debug_filename));
   }
 
@@ -1010,7 +1012,9 @@ class SketchySVD {
     const auto t0 = std::chrono::steady_clock::now();
     skema_ctx* c = ctx_.get();
     if (svals.extent(0) == 0) throw std::runtime_error("skema: compute_residuals needs a low_rank_approx first");
-    detail::check_ctx(skema_residuals_begin(c, uvecs.data(), svals.data(), vvecs.data(), SKEMA_MEM_HOST), c);
+    // the factors kept on the device, else (replaced since) the stored ones
+    if (skema_residuals_begin(c, nullptr, nullptr, nullptr, SKEMA_MEM_HOST) != SKEMA_OK)
+      detail::check_ctx(skema_residuals_begin(c, uvecs.data(), svals.data(), vvecs.data(), SKEMA_MEM_HOST), c);
     const size_type m = algParams.kernel_func == Kernel_Map::GAUSSRBF ? nrow : detail::Context::rows_of(A);
     ctx_.stream(A, 0, m, true);
     rnrms = vector_type("rnrms", rank);
@@ -1064,6 +1068,7 @@ class SketchySPD {
       : nrow(p.matrix_m), ncol(p.matrix_n), rank(p.rank), algParams(p), ctx_(p, DimReduxT::kind, true),
         range(ctx_.range()) {
     detail::check_ctx(skema_timing_enable(ctx_.get(), 1), ctx_.get());
+    detail::check_ctx(skema_set_keep_factors(ctx_.get(), 1), ctx_.get());
     if (!p.debug_filename.empty()) ctx_.dump_maps(detail::debug_stem(p.debug_filename));
   }
 
@@ -1108,7 +1113,8 @@ class SketchySPD {
     const auto t0 = std::chrono::steady_clock::now();
     skema_ctx* c = ctx_.get();
     if (svals.extent(0) == 0) throw std::runtime_error("skema: compute_residuals needs a low_rank_approx first");
-    detail::check_ctx(skema_residuals_begin(c, nullptr, svals.data(), uvecs.data(), SKEMA_MEM_HOST), c);
+    if (skema_residuals_begin(c, nullptr, nullptr, nullptr, SKEMA_MEM_HOST) != SKEMA_OK)
+      detail::check_ctx(skema_residuals_begin(c, nullptr, svals.data(), uvecs.data(), SKEMA_MEM_HOST), c);
     const size_type m = algParams.kernel_func == Kernel_Map::GAUSSRBF ? nrow : detail::Context::rows_of(A);
     ctx_.stream(A, 0, m, true);
     rnrms = vector_type("rnrms", rank);

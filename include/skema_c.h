@@ -213,7 +213,20 @@ int skema_low_rank_approx_rows(skema_ctx* ctx, int64_t row0, int64_t nrows, skem
  *   skema_residuals_finish(ctx, rnorms, mem)   rank doubles; closes the pass.
  * SketchySPD contexts take the one-sided form ||(A V - V S)(:, j)||_2
  * (src/Skema_Residuals.hpp:112-158); U may then be NULL. FP64 arithmetic.
- * An update or finish without an open pass fails with SKEMA_ESTATE. */
+ * An update or finish without an open pass fails with SKEMA_ESTATE.
+ * U, S and V all NULL open the pass on the factors of the last
+ * skema_low_rank_approx, kept on the device (skema_set_keep_factors), as
+ * the reference's compute_residuals uses the uvecs, svals and vvecs its
+ * low_rank_approx kept (src/Skema_SketchySVD.cpp:656-660, 719-727); without
+ * kept factors that fails with SKEMA_ESTATE. Factors passed explicitly
+ * replace the kept ones. */
+/* on = 1: every later skema_low_rank_approx (any mem) also keeps its U, S
+ * and V on the device, in buffers the context holds ((m + 2 n) rank + 2
+ * rank doubles, allocated by the first one), for a residual pass opened with
+ * NULL factors: no host copy of U is made. on = 0 stops keeping and drops
+ * the kept factors. Off by default. */
+int skema_set_keep_factors(skema_ctx* ctx, int32_t on);
+
 int skema_residuals_begin(skema_ctx* ctx, const double* U, const double* S,
                           const double* V, int32_t mem);
 int skema_residuals_update_dense(skema_ctx* ctx, const float* A, int64_t ld,

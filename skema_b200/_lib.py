@@ -112,6 +112,7 @@ SIGNATURES = {
     "skema_low_rank_approx": (C.c_int, [_P, _P, _P, _P, _I32]),
     "skema_low_rank_approx_rows": (C.c_int, [_P, _I64, _I64, _P, _P, _P, _P, _P, _I32]),
     "skema_residuals_begin": (C.c_int, [_P, _P, _P, _P, _I32]),
+    "skema_set_keep_factors": (C.c_int, [_P, _I32]),
     "skema_residuals_update_dense": (C.c_int, [_P, _P, _I64, _I32, _I64, _I64, _I32]),
     "skema_residuals_update_csr": (C.c_int, [_P, _P, _P, _P, _I64, _I64, _I32]),
     "skema_residuals_update_rbf": (C.c_int, [_P, _P, _I64, _I32, _I64, _I64, _I64, _I64, _I32]),

@@ -663,13 +663,16 @@ int skema_low_rank_approx(skema_ctx* c, double* U, double* S, double* V, int32_t
       const int64_t r = c->p.rank;
       if (mem == SKEMA_MEM_DEVICE) {
         spd_low_rank_approx(c, U, S);
+        if (c->keep_factors && U && S) residual_keep(c, nullptr, S, U);  // the one-sided form's V is U
         return;
       }
       const size_t ub = sizeof(double) * (size_t)(c->m * r);
       char* buf = (char*)staging(c, ub + sizeof(double) * (size_t)r + 512);
       double* dU = (double*)buf;
       double* dS = (double*)(buf + (ub + 255) / 256 * 256);
-      spd_low_rank_approx(c, U ? dU : nullptr, S ? dS : nullptr);
+      const bool keep = c->keep_factors;
+      spd_low_rank_approx(c, (U || keep) ? dU : nullptr, (S || keep) ? dS : nullptr);
+      if (keep) residual_keep(c, nullptr, dS, dU);
       if (U) SKEMA_CUDA(cudaMemcpyAsync(U, dU, ub, cudaMemcpyDeviceToHost, c->stream));
       if (S) SKEMA_CUDA(cudaMemcpyAsync(S, dS, sizeof(double) * (size_t)r, cudaMemcpyDeviceToHost, c->stream));
       SKEMA_CUDA(cudaStreamSynchronize(c->stream));
@@ -682,6 +685,7 @@ int skema_low_rank_approx(skema_ctx* c, double* U, double* S, double* V, int32_t
     check_device_error(c);
     if (mem == SKEMA_MEM_DEVICE) {
       low_rank_approx(c, U, S, V);
+      if (c->keep_factors && U && S && V) residual_keep(c, U, S, V);
       return;
     }
     const size_t ub = sizeof(double) * (size_t)(c->m * r), vb = sizeof(double) * (size_t)(c->n * r);
@@ -689,7 +693,9 @@ int skema_low_rank_approx(skema_ctx* c, double* U, double* S, double* V, int32_t
     double* dU = (double*)buf;
     double* dV = (double*)(buf + (ub + 255) / 256 * 256);
     double* dS = (double*)(buf + (ub + 255) / 256 * 256 + (vb + 255) / 256 * 256);
-    low_rank_approx(c, U ? dU : nullptr, S ? dS : nullptr, V ? dV : nullptr);
+    const bool keep = c->keep_factors;
+    low_rank_approx(c, (U || keep) ? dU : nullptr, (S || keep) ? dS : nullptr, (V || keep) ? dV : nullptr);
+    if (keep) residual_keep(c, dU, dS, dV);
     if (U) SKEMA_CUDA(cudaMemcpyAsync(U, dU, ub, cudaMemcpyDeviceToHost, c->stream));
     if (V) SKEMA_CUDA(cudaMemcpyAsync(V, dV, vb, cudaMemcpyDeviceToHost, c->stream));
     if (S) SKEMA_CUDA(cudaMemcpyAsync(S, dS, sizeof(double) * (size_t)r, cudaMemcpyDeviceToHost, c->stream));
@@ -698,9 +704,20 @@ int skema_low_rank_approx(skema_ctx* c, double* U, double* S, double* V, int32_t
 }
 
 // ---- residual pass ----------------------------------------------------------
+int skema_set_keep_factors(skema_ctx* c, int32_t on) {
+  return guarded(c, [&] {
+    c->keep_factors = on != 0;
+    if (!c->keep_factors) c->res_factors_kept = false;
+  });
+}
+
 int skema_residuals_begin(skema_ctx* c, const double* U, const double* S, const double* V, int32_t mem) {
   return guarded(c, [&] {
     if (mem != SKEMA_MEM_DEVICE && mem != SKEMA_MEM_HOST) fail(SKEMA_EINVAL, "bad mem kind");
+    if (!U && !S && !V) {  // the factors the last approximation kept on the device
+      residual_begin_kept(c);
+      return;
+    }
     if (!S || !V || (!c->spd && !U)) fail(SKEMA_EINVAL, "null U, S or V");
     const int64_t r = c->p.rank;
     if (mem == SKEMA_MEM_DEVICE) {

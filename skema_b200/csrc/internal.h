@@ -179,6 +179,11 @@ struct skema_ctx {
   double* res_AtU = nullptr;
   double* res_sq = nullptr;
   bool res_ready = false;
+  // skema_set_keep_factors: each low_rank_approx also loads its U, S, V into
+  // the residual buffers (res_factors_kept then holds), so a residual pass
+  // can open on them without a host copy
+  bool keep_factors = false;
+  bool res_factors_kept = false;
   bool residual_pass = false;
   // Device status block of the bounded waits in the tensor-core kernels:
   // dev_err[0] non-zero when a wait timed out (checked at the next
@@ -328,6 +333,11 @@ void dgemm_f32_f64(skema_ctx* c, int64_t M, int64_t N, int64_t K, double alpha, 
 // ---- residual norms (residuals.cu) ----
 // U (m x r), S (r), V (n x r) column-major, device pointers.
 void residual_begin(skema_ctx* c, const double* U, const double* S, const double* V);
+// Loads device U (m x r, column-major; unused for SketchySPD), S and V into
+// the residual buffers and marks them as the kept factors.
+void residual_keep(skema_ctx* c, const double* U, const double* S, const double* V);
+// Opens a residual pass on the kept factors (SKEMA_ESTATE without them).
+void residual_begin_kept(skema_ctx* c);
 void residual_dense(skema_ctx* c, Mat A, int64_t row0, int64_t nrows);
 void residual_csr(skema_ctx* c, const int64_t* rowptr, const int32_t* col, const float* val, int64_t col_offset,
                   int64_t row0, int64_t nrows);

@@ -112,7 +112,8 @@ void residual_free(skema_ctx* c) {
   c->res_ready = false;
 }
 
-void residual_begin(skema_ctx* c, const double* U, const double* S, const double* V) {
+// Allocates the residual buffers once and loads U, S, V into them.
+static void residual_load(skema_ctx* c, const double* U, const double* S, const double* V) {
   const int64_t m = c->m, n = c->n, r = c->p.rank;
   if (!c->res_V) {
     SKEMA_CUDA(cudaMalloc(&c->res_V, sizeof(double) * (size_t)(n * r)));
@@ -128,11 +129,33 @@ void residual_begin(skema_ctx* c, const double* U, const double* S, const double
   if (!c->spd) {
     cm_to_rm_kernel<<<grid_of(c, (m * r + 255) / 256, 16), 256, 0, c->stream>>>(U, m, m, r, c->res_U);
     SKEMA_LAUNCHED(c);
-    SKEMA_CUDA(cudaMemsetAsync(c->res_AtU, 0, sizeof(double) * (size_t)(n * r), c->stream));
   }
   SKEMA_CUDA(cudaMemcpyAsync(c->res_S, S, sizeof(double) * (size_t)r, cudaMemcpyDeviceToDevice, c->stream));
+}
+
+// Zeroes the pass's sums over the loaded factors and opens it.
+static void residual_open(skema_ctx* c) {
+  const int64_t n = c->n, r = c->p.rank;
+  if (!c->spd) SKEMA_CUDA(cudaMemsetAsync(c->res_AtU, 0, sizeof(double) * (size_t)(n * r), c->stream));
   SKEMA_CUDA(cudaMemsetAsync(c->res_sq, 0, sizeof(double) * (size_t)r, c->stream));
   c->res_ready = true;
+}
+
+void residual_begin(skema_ctx* c, const double* U, const double* S, const double* V) {
+  residual_load(c, U, S, V);
+  c->res_factors_kept = false;  // these factors are the caller's, not an approximation's
+  residual_open(c);
+}
+
+void residual_keep(skema_ctx* c, const double* U, const double* S, const double* V) {
+  residual_load(c, U, S, V);
+  c->res_factors_kept = true;
+}
+
+void residual_begin_kept(skema_ctx* c) {
+  if (!c->res_factors_kept)
+    fail(SKEMA_ESTATE, "no kept factors: enable skema_set_keep_factors before skema_low_rank_approx");
+  residual_open(c);
 }
 
 // Rows [row0, row0 + nrows) of a dense A, in windows of params.window rows

@@ -362,6 +362,10 @@ class _Context:
         self._check(self.lib.skema_get_dims(self.h, C.byref(k), C.byref(s), C.byref(spd)))
         self.range, self.core, self.spd = k.value, s.value, bool(spd.value)
         self.nrow, self.ncol, self.rank = alg.matrix_m, alg.matrix_n, alg.rank
+        # like the reference, which keeps the last approximation's uvecs,
+        # svals and vvecs for compute_residuals, the context keeps them on the
+        # device, so the residual pass needs no host copy of U
+        self._check(self.lib.skema_set_keep_factors(self.h, 1))
         stem = self.debug_stem()
         if stem:
             self.map_export_reference_dumps(stem)
@@ -444,12 +448,17 @@ class _Context:
         """Skema::residuals (src/Skema_Residuals.hpp:160-217): per-column
         ||[A^T U - V S; A V - U S]||_2 (SketchySPD: ||A V - V S||_2) for host
         FP64 U (m x r), S (r), V (n x r); A streamed again like the update.
-        row_blocks: optional list of (row0, A_block) pairs instead of A."""
-        Uc = None if U is None else np.asfortranarray(np.asarray(U, dtype=np.float64))
-        Sc = np.ascontiguousarray(np.asarray(S, dtype=np.float64))
-        Vc = np.asfortranarray(np.asarray(V, dtype=np.float64))
-        self._check(self.lib.skema_residuals_begin(self.h, None if Uc is None else Uc.ctypes.data, Sc.ctypes.data,
-                                                   Vc.ctypes.data, L.MEM_HOST))
+        U, S and V all None: the factors of the last low_rank_approx, kept
+        on the device. row_blocks: optional list of (row0, A_block) pairs
+        instead of A."""
+        if U is None and S is None and V is None:
+            self._check(self.lib.skema_residuals_begin(self.h, None, None, None, L.MEM_HOST))
+        else:
+            Uc = None if U is None else np.asfortranarray(np.asarray(U, dtype=np.float64))
+            Sc = np.ascontiguousarray(np.asarray(S, dtype=np.float64))
+            Vc = np.asfortranarray(np.asarray(V, dtype=np.float64))
+            self._check(self.lib.skema_residuals_begin(self.h, None if Uc is None else Uc.ctypes.data,
+                                                       Sc.ctypes.data, Vc.ctypes.data, L.MEM_HOST))
         for row0, blk in (row_blocks if row_blocks is not None else [(0, A)]):
             self._stream(blk, row0, None, "skema_residuals_update")
         out = np.empty(self.rank, dtype=np.float64)
@@ -461,7 +470,12 @@ class _Context:
         residual norms of the last low_rank_approx, kept as self.rnrms."""
         if getattr(self, "uvecs", None) is None:
             raise SkemaError(L.ESTATE, "compute_residuals needs a low_rank_approx first")
-        self.rnrms = self.residuals(A, self.uvecs, self.svals, self.vvecs)
+        try:  # the factors kept on the device
+            self.rnrms = self.residuals(A, None, None, None)
+        except SkemaError as e:  # replaced by factors passed to residuals() since
+            if e.status != L.ESTATE:
+                raise
+            self.rnrms = self.residuals(A, self.uvecs, self.svals, self.vvecs)
         return self.rnrms
 
     def save_history(self, path=None):
@@ -793,7 +807,12 @@ class SketchySPD(_Context):
         ||(A U - U S)(:, j)||_2 for the last low_rank_approx."""
         if getattr(self, "uvecs", None) is None:
             raise SkemaError(L.ESTATE, "compute_residuals needs a low_rank_approx first")
-        self.rnrms = self.residuals(A, None, self.svals, self.uvecs)
+        try:  # the factors kept on the device
+            self.rnrms = self.residuals(A, None, None, None)
+        except SkemaError as e:  # replaced by factors passed to residuals() since
+            if e.status != L.ESTATE:
+                raise
+            self.rnrms = self.residuals(A, None, self.svals, self.uvecs)
         return self.rnrms
 
 

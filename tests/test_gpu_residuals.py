@@ -105,3 +105,40 @@ def test_residuals_need_an_open_pass(sk):
         assert s.lib.skema_residuals_finish(s.h, out.ctypes.data, L.MEM_HOST) == L.ESTATE
         A = np.zeros((100, 50), np.float32)
         assert s.lib.skema_residuals_update_dense(s.h, A.ctypes.data, 50, L.ROW_MAJOR, 0, 100, L.MEM_HOST) == L.ESTATE
+
+
+def test_residuals_from_the_kept_factors(sk, oracle):
+    # skema_set_keep_factors: the last approximation's U, S, V stay on the
+    # device, and a pass opened with NULL factors equals one given them from
+    # the host; explicit factors replace the kept ones; keeping off drops them
+    import skema_b200._lib as L
+
+    rng = np.random.default_rng(12)
+    m, n = 3000, 400
+    A = ((rng.standard_normal((m, 12)) @ rng.standard_normal((12, n))) + 0.01 * rng.standard_normal((m, n))
+         ).astype(np.float32)
+    a = sk.AlgParams(matrix_m=m, matrix_n=n, rank=8, window=512, dim_redux=0)
+    with sk.SketchySVD(a) as s:
+        s.update_rows(A)
+        U, S, V = s.low_rank_approx()
+        kept = s.residuals(A, None, None, None)
+        host = s.residuals(A, U, S, V)
+        assert np.max(np.abs(kept - host) / np.abs(host)) < 1e-12
+        with pytest.raises(sk.SkemaError) as e:  # replaced by the explicit factors
+            s.residuals(A, None, None, None)
+        assert e.value.status == L.ESTATE
+        assert np.max(np.abs(s.compute_residuals(A) - host) / np.abs(host)) < 1e-12  # falls back to U, S, V
+        s.low_rank_approx()
+        assert np.max(np.abs(s.residuals(A, None, None, None) - host) / np.abs(host)) < 1e-12
+        assert s.lib.skema_set_keep_factors(s.h, 0) == L.OK
+        with pytest.raises(sk.SkemaError):
+            s.residuals(A, None, None, None)
+    b = sk.AlgParams(matrix_m=n, matrix_n=n, rank=5, window=128, dim_redux=0, issymmetric=True)
+    P = (rng.standard_normal((n, 20)) @ rng.standard_normal((20, n)) / n).astype(np.float64)
+    P = (P @ P.T).astype(np.float32)
+    with sk.SketchySPD(b) as s:
+        s.update_rows(P)
+        Us, Ss = s.low_rank_approx()
+        kept = s.residuals(P, None, None, None)
+        host = s.residuals(P, None, Ss, Us)
+        assert np.max(np.abs(kept - host) / np.maximum(np.abs(host), 1e-300)) < 1e-12
