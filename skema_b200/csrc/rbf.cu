@@ -203,6 +203,10 @@ void rbf_update(skema_ctx* c, Mat P, int64_t npts, int64_t d, int64_t row0, int6
   }
 }
 
+// Room for the K-split partial products of the FP32 forward and adjoint
+// (a window's rows times k or d, at most 16 splits).
+constexpr int64_t kRbfPartFloats = (int64_t)4 << 20;
+
 void rbf_fwd(skema_ctx* c, const float* pts, int64_t N, int64_t d, double gamma,
              const float* omega, int64_t k, float* Y) {
   if (rbf_pair_tc_supported(c, d, k, gamma)) {
@@ -211,12 +215,16 @@ void rbf_fwd(skema_ctx* c, const float* pts, int64_t N, int64_t d, double gamma,
   }
   const Mat P{pts, d, 1};
   const int64_t wb = rows_per_block(N, N);
-  float* Kw = (float*)workspace(c, sizeof(float) * (size_t)(wb * N));
+  const size_t kb = (sizeof(float) * (size_t)(wb * N) + 255) / 256 * 256;
+  char* ws = (char*)workspace(c, kb + sizeof(float) * (size_t)kRbfPartFloats);
+  float* Kw = (float*)ws;
+  float* part = (float*)(ws + kb);  // K-split partial products
   for (int64_t r = 0; r < N; r += wb) {
     const int64_t wr = std::min(wb, N - r);
     launch_tile(c, 0, P, N, d, (float)gamma, r, wr, Kw, N, nullptr, nullptr, nullptr);
     // Y(r:r+wr, :) = K_w Omega~^T ; B(kk=j, col=q) = omega[q*N + j]
-    sgemm(c, wr, k, N, 1.f, Mat{Kw, N, 1}, Mat{omega, 1, N}, 0.f, MatOut{Y + r * k, k, 1});
+    sgemm_split(c, wr, k, N, 1.f, Mat{Kw, N, 1}, Mat{omega, 1, N}, 0.f, MatOut{Y + r * k, k, 1}, part,
+                kRbfPartFloats);
   }
 }
 
@@ -231,11 +239,12 @@ void rbf_vjp(skema_ctx* c, const float* pts, int64_t N, int64_t d, double gamma,
   const size_t eb = (sizeof(float) * (size_t)(wb * N) + 255) / 256 * 256;
   const size_t vb = (sizeof(float) * (size_t)N + 255) / 256 * 256;
   const size_t sb = (sizeof(float) * (size_t)(N * d) + 255) / 256 * 256;
-  char* ws = (char*)workspace(c, eb + 2 * vb + sb);
+  char* ws = (char*)workspace(c, eb + 2 * vb + sb + sizeof(float) * (size_t)kRbfPartFloats);
   float* E = (float*)ws;
   float* rs = (float*)(ws + eb);
   float* cs = (float*)(ws + eb + vb);
   float* S = (float*)(ws + eb + 2 * vb);
+  float* part = (float*)(ws + eb + 2 * vb + sb);  // K-split partial products
   SKEMA_CUDA(cudaMemsetAsync(rs, 0, 2 * vb + sb, c->stream));
   SKEMA_CUDA(cudaMemsetAsync(dgamma, 0, sizeof(double), c->stream));
   for (int64_t r = 0; r < N; r += wb) {
@@ -245,7 +254,7 @@ void rbf_vjp(skema_ctx* c, const float* pts, int64_t N, int64_t d, double gamma,
     // E_w = M_w o K_w, with the gamma / row / column partial sums
     launch_tile(c, 1, P, N, d, (float)gamma, r, wr, E, N, dgamma, rs, cs);
     // S(r:r+wr, :) += E_w X ;  S += E_w^T X_w
-    sgemm(c, wr, d, N, 1.f, Mat{E, N, 1}, Mat{pts, d, 1}, 1.f, MatOut{S + r * d, d, 1});
+    sgemm_split(c, wr, d, N, 1.f, Mat{E, N, 1}, Mat{pts, d, 1}, 1.f, MatOut{S + r * d, d, 1}, part, kRbfPartFloats);
     sgemm(c, N, d, wr, 1.f, Mat{E, 1, N}, Mat{pts + r * d, d, 1}, 1.f, MatOut{S, d, 1});
   }
   rbf_dx_kernel<<<grid_cap(c, (N * d + 255) / 256, 16), 256, 0, c->stream>>>(
