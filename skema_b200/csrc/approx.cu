@@ -950,8 +950,13 @@ __global__ void store_int_kernel(int* dst, int v) { *dst = v; }
 // from the host, each outer sweep's rotation flag read back once.
 void jacobi_svd_blocked(skema_ctx* c, double* A, double* V, int64_t k, int max_sweeps, double tol,
                         int* sweeps_out) {
-  // columns per block: two blocks of A and V in about 200 KB
-  const int bs = (int)std::max<int64_t>(2, std::min<int64_t>(64, (200 * 1024) / (4 * (int64_t)sizeof(double) * k)));
+  // columns per block: 8, or fewer where two blocks of A and V would not fit
+  // about 200 KB. Small blocks put more CTAs on each round (nb / 2) for the
+  // same pairs per outer sweep: at k = 201, 8 columns (13 CTAs a round) took
+  // 10.5 ms against 15.1 ms for 31 columns (4 CTAs), 12 and 16 about 11.2 ms,
+  // 6 and 4 11.1 and 11.8 ms.
+  const int bs = (int)std::max<int64_t>(
+      2, std::min<int64_t>(8, (200 * 1024) / (4 * (int64_t)sizeof(double) * k)));
   int nb = (int)((k + bs - 1) / bs);
   nb += nb & 1;  // an even number of players
   const size_t smem = sizeof(double) * (size_t)(4 * bs * k);
