@@ -86,3 +86,18 @@ def test_host_csr_with_a_decreasing_row_map_is_rejected(sk):
         for x, y in zip(s.get_sketches(), ref.get_sketches()):
             assert np.array_equal(np.asarray(x), np.asarray(y)) or \
                 np.linalg.norm(np.asarray(x, np.float64) - y) <= 1e-6 * np.linalg.norm(y)
+
+
+def test_transposed_host_fetch_with_a_wide_range(sk):
+    # k = 4 r + 1 = 257 > 256: the chunks take the general tiled transpose
+    rng = np.random.default_rng(9)
+    m, n = 3000, 700
+    A = rng.standard_normal((m, n)).astype(np.float32)
+    a = sk.AlgParams(matrix_m=m, matrix_n=n, rank=64, window=1000, dim_redux=0)
+    with sk.SketchySVD(a) as s:
+        assert s.range == 257
+        s.update_rows(A)
+        for which in range(3):
+            r = _fetch(s, which, 1)
+            c = _fetch(s, which, 0)
+            assert np.array_equal(r, c), which
